@@ -1,0 +1,409 @@
+/*
+ * softbox_b200.h — C ABI of the B200 rigid-rod mechanics library (libsoftbox_b200.so).
+ *
+ * Drop-in boundary: each entry point below replaces the body of one public static
+ * method of the reference's System classes (package softbox/, notaboxllc/SoftBox). The
+ * Java side keeps its signatures and its planar SoA store layouts
+ * ([x0..xN-1 | y0..yN-1 | z0..zN-1], FilamentStore.java:10-22) and calls these
+ * functions through the Foreign Function & Memory API; INTEGRATION.md shows the
+ * binding. Conventions:
+ *   - every array argument is a DEVICE pointer owned by the caller (the store);
+ *     entry points allocate nothing except where a comment says "scratch";
+ *   - an argument `n`, `cap`, ... carries the length the Java code reads with
+ *     getSize() (divided by 3 for planar vectors);
+ *   - small parameter arrays (params, counts, kinParams, ...) are device arrays with
+ *     the reference's documented slot layout, exactly like the TornadoVM buffers;
+ *   - every call is asynchronous on the context's stream; results are ordered by
+ *     that stream; errors are returned as sbx_status and described by
+ *     sbx_ctx_last_error(). No C++ exception crosses this boundary.
+ *   - a context is not thread-safe; use one per host thread.
+ */
+#ifndef SOFTBOX_B200_H
+#define SOFTBOX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+typedef int32_t sbx_status;
+#define SBX_OK          0
+#define SBX_EINVAL     -1   /* bad argument / size */
+#define SBX_ECUDA      -2   /* CUDA runtime error */
+#define SBX_EOVERFLOW  -3   /* a capacity (MAX_CAND, contents) was exceeded; counts continue past it */
+#define SBX_ETIMEOUT   -4   /* a bounded device wait gave up */
+#define SBX_ENOMEM     -5
+#define SBX_ENONFINITE -6   /* a supplied-noise / state array holds NaN or Inf */
+#define SBX_ESTATE     -7   /* call out of order (e.g. plan not built) */
+
+/* reference constants (SpatialGrid.java:113-115, CrossBridgeSystem.java:36, ...) */
+#define SBX_MAX_CAND        256
+#define SBX_GRID_SCAN_CHUNK 512
+#define SBX_XB_STRIDE        13
+#define SBX_XL_STRIDE        12
+#define SBX_MINI_STRIDE       6
+#define SBX_STRAIN_WIN       10
+#define SBX_TORQUE_WIN        5
+#define SBX_FORCEDOT_WIN     10
+
+typedef struct sbx_ctx sbx_ctx;
+
+/* ---------------------------------------------------------------- context / memory */
+/* Creates a context on `device`. `stream` is a cudaStream_t to run on, or NULL to
+ * create a private non-blocking stream. */
+sbx_status sbx_ctx_create(int device, void* stream, sbx_ctx** out);
+sbx_status sbx_ctx_destroy(sbx_ctx* ctx);
+const char* sbx_ctx_last_error(sbx_ctx* ctx);
+sbx_status sbx_ctx_set_stream(sbx_ctx* ctx, void* stream);
+void* sbx_ctx_stream(sbx_ctx* ctx);
+sbx_status sbx_ctx_sync(sbx_ctx* ctx);
+/* number of kernels this context has launched (for launch accounting) */
+int64_t sbx_ctx_launch_count(sbx_ctx* ctx);
+
+/* DataTransferMode analogues: FIRST_EXECUTION / EVERY_EXECUTION uploads and
+ * UNDER_DEMAND pulls are plain async copies on the context stream. */
+sbx_status sbx_malloc(sbx_ctx* ctx, size_t bytes, void** dptr);
+sbx_status sbx_free(sbx_ctx* ctx, void* dptr);
+sbx_status sbx_upload(sbx_ctx* ctx, void* dst_dev, const void* src_host, size_t bytes);
+sbx_status sbx_download(sbx_ctx* ctx, void* dst_host, const void* src_dev, size_t bytes);
+sbx_status sbx_memset(sbx_ctx* ctx, void* dst_dev, int value, size_t bytes);
+
+/* ---------------------------------------------------------------- drag (host-init systems, run on device)
+ * DragTensorSystem.run(FilamentStore) (DragTensorSystem.java:71-97); `aeta` is the
+ * viscosity in Pa*s (the reference reads Constants.aeta = 0.1). */
+sbx_status sbx_drag_run_filament(sbx_ctx* ctx, int32_t n, const int32_t* monomerCount,
+                                 const int32_t* end1NbrSlot, const int32_t* end2NbrSlot, double aeta,
+                                 float* segLength, float* bTransGam, float* bRotGam,
+                                 float* bTransDiff, float* bRotDiff);
+/* DragTensorSystem.run(MotorStore) (DragTensorSystem.java:105-122) */
+sbx_status sbx_drag_run_motor(sbx_ctx* ctx, int32_t nMotors, double aeta, float* segLength,
+                              float* bTransGam, float* bRotGam, float* bTransDiff, float* bRotDiff);
+/* MiniFilamentStore.initBackboneDrag (MiniFilamentStore.java:294-307); backbone length is a parameter */
+sbx_status sbx_drag_run_backbone(sbx_ctx* ctx, int32_t nBb, double bbLenUm, double aeta, float* segLength,
+                                 float* bTransGam, float* bRotGam, float* bTransDiff, float* bRotDiff,
+                                 float* bbInvDragY);
+
+/* ---------------------------------------------------------------- Brownian forcing
+ * BrownianForceSystem.brownianForce (BrownianForceSystem.java:183-245): Wang-hash keyed
+ * (slot, counts[1]=step, counts[2]=seed), three Box-Muller pairs. params[1]=sqrt(2kT/dt). */
+sbx_status sbx_brownian_force(sbx_ctx* ctx, int32_t n, float* randForce, float* randTorque,
+                              const float* bTransGam, const float* bRotGam, const float* brownTransScale,
+                              const float* brownRotScale, const float* params, const int32_t* counts);
+/* Same amplitude law with Philox4x32-10 keyed (seed64, step, slot). */
+sbx_status sbx_brownian_force_philox(sbx_ctx* ctx, int32_t n, float* randForce, float* randTorque,
+                                     const float* bTransGam, const float* bRotGam,
+                                     const float* brownTransScale, const float* brownRotScale,
+                                     const float* params, const int32_t* counts, uint64_t seed);
+/* Supplied-noise mode: noise is planar [6][n] (gfx|gfy|gfz|gtx|gty|gtz) standard normals.
+ * Returns SBX_ENONFINITE (and writes nothing) if any entry is NaN/Inf. */
+sbx_status sbx_brownian_force_supplied(sbx_ctx* ctx, int32_t n, float* randForce, float* randTorque,
+                                       const float* bTransGam, const float* bRotGam,
+                                       const float* brownTransScale, const float* brownRotScale,
+                                       const float* params, const float* noise);
+
+/* ChainBendingForceSystem.zeroAccumulators (ChainBendingForceSystem.java:38-45) */
+sbx_status sbx_zero_accumulators(sbx_ctx* ctx, int32_t n, float* forceSum, float* torqueSum);
+
+/* ---------------------------------------------------------------- integration
+ * RigidRodLangevinIntegrationSystem.integrate (RigidRodLangevinIntegrationSystem.java:279-358).
+ * coord64 may be NULL; when given, centres accumulate in FP64 and coord receives the
+ * rounded projection (the per-step increment is the reference's FP32 dt*v). */
+sbx_status sbx_integrate(sbx_ctx* ctx, int32_t n, float* coord, double* coord64, float* uVec, float* yVec,
+                         const float* forceSum, const float* torqueSum, const float* randForce,
+                         const float* randTorque, const float* bTransGam, const float* bRotGam,
+                         const float* params);
+/* DerivedGeometrySystem.derive (DerivedGeometrySystem.java:386-432) */
+sbx_status sbx_derive(sbx_ctx* ctx, int32_t n, const float* coord, const float* uVec, float* yVec,
+                      float* zVec, float* end1, float* end2, const float* segLength);
+/* ContainmentSystem.confine (ContainmentSystem.java:390-458); boxParams[0..6] */
+sbx_status sbx_confine(sbx_ctx* ctx, int32_t n, const float* coord, const float* uVec,
+                       const float* segLength, const float* bTransGam, float* forceSum, float* torqueSum,
+                       const float* boxParams, const int32_t* counts);
+/* MechanicsFusion.forceBuild / integDerive / integDeriveConfined (MechanicsFusion.java:52-338) */
+sbx_status sbx_fusion_force_build(sbx_ctx* ctx, int32_t n, float* forceSum, float* torqueSum,
+                                  float* randForce, float* randTorque, const float* bTransGam,
+                                  const float* bRotGam, const float* brownTransScale,
+                                  const float* brownRotScale, const float* params, const int32_t* counts);
+sbx_status sbx_fusion_integ_derive(sbx_ctx* ctx, int32_t n, float* coord, double* coord64, float* uVec,
+                                   float* yVec, float* zVec, const float* segLength, float* end1, float* end2,
+                                   const float* forceSum, const float* torqueSum, const float* randForce,
+                                   const float* randTorque, const float* bTransGam, const float* bRotGam,
+                                   const float* params);
+sbx_status sbx_fusion_integ_derive_confined(sbx_ctx* ctx, int32_t n, float* coord, double* coord64,
+                                            float* uVec, float* yVec, float* zVec, const float* segLength,
+                                            float* end1, float* end2, float* forceSum, float* torqueSum,
+                                            const float* randForce, const float* randTorque,
+                                            const float* bTransGam, const float* bRotGam,
+                                            const float* boxParams, const int32_t* counts);
+
+/* ---------------------------------------------------------------- chain
+ * ChainBendingForceSystem.chainForces (ChainBendingForceSystem.java:105-331) */
+sbx_status sbx_chain_forces(sbx_ctx* ctx, int32_t n, const float* coord, const float* uVec,
+                            const float* segLength, const int32_t* end2NbrSlot, const int32_t* end2NbrSide,
+                            const int32_t* end1NbrSlot, const int32_t* end1NbrSide, const float* bTransGam,
+                            const float* bRotGam, float* forceSum, float* torqueSum, const float* chainParams);
+
+/* ---------------------------------------------------------------- body view publishing
+ * FilamentStore.publishToBodyView (FilamentStore.java:275-328); filState may be NULL (8-arg form) */
+sbx_status sbx_filament_publish(sbx_ctx* ctx, int32_t n, const float* coord, const float* segLength,
+                                int32_t cap, float* center, float* boundingRadius, int32_t* ownerStore,
+                                int32_t* ownerSlot, const float* viewParams, const int32_t* filState);
+/* MotorStore.publishHeadFromBody (MotorStore.java:300-314) */
+sbx_status sbx_motor_publish_head(sbx_ctx* ctx, int32_t nMotors, const float* bodyCoord,
+                                  const float* bodyUVec, const float* bodySegLength, float* head,
+                                  float* uVec, float* rodUVec);
+/* MotorStore.publishToBodyView (MotorStore.java:326-347); publishParams[0] = base slot */
+sbx_status sbx_motor_publish(sbx_ctx* ctx, int32_t nMotors, const float* head, const float* reach,
+                             int32_t cap, float* center, float* boundingRadius, int32_t* ownerStore,
+                             int32_t* ownerSlot, const int32_t* publishParams);
+
+/* ---------------------------------------------------------------- spatial grid
+ * SpatialGrid.bodyCell (SpatialGrid.java:118-142); counts[1] = S */
+sbx_status sbx_grid_body_cell(sbx_ctx* ctx, int32_t cap, const float* center, const float* gridParams,
+                              const int32_t* gridDims, const int32_t* counts, int32_t* bodyCell);
+/* The counting sort that replaces gridZero+gridHistogram+gridScanLocal/Chunks/Add+gridScatter
+ * (SpatialGrid.java:145-249) and the chunked gridChunk* variant (SpatialGrid.java:304-398):
+ * atomic cell histogram, block scan over GRID_SCAN_CHUNK tiles (chunkSum holds the tile
+ * sums, as in the reference), scatter, then an in-cell ascending sort so that the
+ * within-cell order is body-index order. Outputs equal the serial reference bit for bit:
+ * gridCellOffsets[0..totalCells] (terminator clamped to contentsCap), gridCellContents,
+ * cellCount (= per-cell counts, as the serial gridScatter leaves it), chunkSum. */
+sbx_status sbx_grid_build(sbx_ctx* ctx, const int32_t* bodyCell, const int32_t* counts,
+                          const int32_t* gridDims, int32_t totalCells, int32_t* cellCount,
+                          int32_t* chunkSum, int32_t* gridCellOffsets, int32_t* gridCellContents,
+                          int32_t contentsCap);
+/* SpatialGrid.broadPhase (SpatialGrid.java:407-473); candPartner is cap*SBX_MAX_CAND */
+sbx_status sbx_grid_broad_phase(sbx_ctx* ctx, int32_t cap, const float* center, const float* boundingRadius,
+                                const int32_t* bodyCell, const int32_t* gridCellOffsets,
+                                const int32_t* gridCellContents, const int32_t* gridDims,
+                                const float* gridParams, const int32_t* counts, int32_t* candPartner,
+                                int32_t* candCount);
+/* SpatialGrid.bruteForce (SpatialGrid.java:480-512) */
+sbx_status sbx_grid_brute_force(sbx_ctx* ctx, int32_t cap, const float* center, const float* boundingRadius,
+                                const float* gridParams, const int32_t* counts, int32_t* brutePartner,
+                                int32_t* bruteCount);
+
+/* ---------------------------------------------------------------- binding / unbinding
+ * BindingDetectionSystem.gridReachable (BindingDetectionSystem.java:143-228); counts[0]=nM */
+sbx_status sbx_binding_grid_reachable(sbx_ctx* ctx, const float* head, const float* uVec, const float* rodUVec,
+                                      int32_t nSeg, const float* segEnd1, const float* segEnd2,
+                                      const float* gridParams, const int32_t* gridDims,
+                                      const int32_t* gridCellOffsets, const int32_t* gridCellContents,
+                                      const int32_t* ownerStore, const int32_t* ownerSlot,
+                                      int32_t* motorReachSeg, int32_t* motorReachCount,
+                                      const float* kinParams, const int32_t* counts, int32_t nM);
+/* BindingDetectionSystem.bruteReachable (BindingDetectionSystem.java:260-283) */
+sbx_status sbx_binding_brute_reachable(sbx_ctx* ctx, const float* head, const float* uVec,
+                                       const float* rodUVec, int32_t nSeg, const float* segEnd1,
+                                       const float* segEnd2, int32_t* reachSeg, int32_t* reachCount,
+                                       const float* kinParams, int32_t nM);
+/* BindingDetectionSystem.bindNearest (BindingDetectionSystem.java:356-389) */
+sbx_status sbx_binding_bind_nearest(sbx_ctx* ctx, const float* head, const float* uVec, const float* rodUVec,
+                                    int32_t nSeg, const float* segEnd1, const float* segEnd2,
+                                    const int32_t* motorCandSeg, const int32_t* motorCandCount,
+                                    int32_t* boundSeg, float* bindArc, const float* kinParams, int32_t nM);
+/* NucleotideCycleSystem.catchSlipRelease (NucleotideCycleSystem.java:77-134) */
+sbx_status sbx_nucleotide_release(sbx_ctx* ctx, int32_t nM, int32_t* boundSeg, const float* forceDotFil,
+                                  const float* forceMag, int32_t* cooldown, int32_t* stats,
+                                  int32_t* capStats, const float* kinParams, const int32_t* counts);
+/* NucleotideCycleSystem.cycle (NucleotideCycleSystem.java:33-69) */
+sbx_status sbx_nucleotide_cycle(sbx_ctx* ctx, int32_t nM, int32_t* nucleotideState, const int32_t* boundSeg,
+                                const float* forceDotHist, const float* nucParams, const int32_t* counts);
+
+/* ---------------------------------------------------------------- cross-bridge
+ * CrossBridgeSystem.bondForces / applyHeadForce / registerForceDot (CrossBridgeSystem.java:58-187) */
+sbx_status sbx_xbridge_bond_forces(sbx_ctx* ctx, int32_t nB, const float* motorCoord, const float* motorUVec,
+                                   const float* motorYVec, const float* motorBRotGam, int32_t nSeg,
+                                   const float* filCoord, const float* filUVec, const float* filYVec,
+                                   const float* filBRotGam, const float* filSegLength, const int32_t* boundSeg,
+                                   const float* bindArc, const int32_t* nucleotideState, float* bondData,
+                                   const float* xbParams);
+sbx_status sbx_xbridge_apply_head_force(sbx_ctx* ctx, int32_t nB, const float* bondData,
+                                        float* bodyForceSum, float* bodyTorqueSum);
+sbx_status sbx_xbridge_register_force_dot(sbx_ctx* ctx, int32_t nM, const float* bondData,
+                                          const int32_t* boundSeg, float* forceDotFil, float* forceMag,
+                                          float* forceDotHist, int32_t* forceDotPlace);
+/* The CSR-inverse that replaces csrHistogram/csrScan/csrScatter and csrChunk*
+ * (CrossBridgeSystem.java:190-298): rows = key values, items in ascending index per row.
+ * Outputs equal the serial reference: rowOffsets[0..nRows], rowList, rowCount (= row
+ * lengths, as the serial csrScatter leaves it). Uses context scratch for the scan. */
+sbx_status sbx_csr_build(sbx_ctx* ctx, const int32_t* keys, int32_t nItems, int32_t nRows,
+                         int32_t* rowCount, int32_t* rowOffsets, int32_t* rowList);
+/* CrossBridgeSystem.segGather (CrossBridgeSystem.java:302-320) */
+sbx_status sbx_xbridge_seg_gather(sbx_ctx* ctx, int32_t nSeg, const int32_t* segMotorOffsets,
+                                  const int32_t* segMotorMyo, const float* bondData, float* filForceSum,
+                                  float* filTorqueSum);
+/* CrossBridgeSystem.bruteGather (CrossBridgeSystem.java:323-337) */
+sbx_status sbx_xbridge_brute_gather(sbx_ctx* ctx, int32_t nSeg, int32_t nM, const int32_t* boundSeg,
+                                    const float* bondData, float* bForceSum, float* bTorqueSum);
+
+/* ---------------------------------------------------------------- crosslinkers
+ * CrosslinkerSystem.linkForces / segGatherA / segGatherB / bruteGather / unbind /
+ * countActiveLinks / linkTorsion (CrosslinkerSystem.java:51-281, 694-808) */
+sbx_status sbx_xlink_count_active(sbx_ctx* ctx, int32_t nLinks, const int32_t* linkState,
+                                  const int32_t* linkFilA, const int32_t* linkFilB, int32_t nSeg,
+                                  int32_t* activeLinkCount);
+sbx_status sbx_xlink_forces(sbx_ctx* ctx, int32_t nSeg, const float* filCoord, const float* filUVec,
+                            const float* filEnd1, const float* filBTransGam, int32_t nLinks,
+                            const int32_t* linkFilA, const int32_t* linkFilB, const float* loc1,
+                            const float* loc2, const int32_t* filLinkCt, float* xlinkData,
+                            const float* xlParams);
+sbx_status sbx_xlink_torsion(sbx_ctx* ctx, int32_t nSeg, const float* filUVec, int32_t nLinks,
+                             const int32_t* linkFilA, const int32_t* linkFilB, const int32_t* linkState,
+                             const int32_t* linkOrientSame, float* torqueMagHist, int32_t* torqueMagPlace,
+                             float* xlinkData, const float* torsionParams);
+/* side = 0 gathers the A-side payload [0..5], side = 1 the B-side payload [6..11] */
+sbx_status sbx_xlink_seg_gather(sbx_ctx* ctx, int32_t side, int32_t nSeg, const int32_t* segOffsets,
+                                const int32_t* segLinkIdx, const float* xlinkData, const int32_t* linkState,
+                                float* filForceSum, float* filTorqueSum);
+sbx_status sbx_xlink_brute_gather(sbx_ctx* ctx, int32_t nSeg, int32_t nLinks, const int32_t* linkFilA,
+                                  const int32_t* linkFilB, const float* xlinkData, const int32_t* linkState,
+                                  float* bForceSum, float* bTorqueSum);
+sbx_status sbx_xlink_unbind(sbx_ctx* ctx, int32_t nSeg, const float* filUVec, const float* filEnd1,
+                            int32_t nLinks, const int32_t* linkFilA, const int32_t* linkFilB,
+                            const float* loc1, const float* loc2, int32_t* linkState, float* strainHist,
+                            int32_t* strainPlace, const float* offParams, const int32_t* counts);
+
+/* ---------------------------------------------------------------- myosin structure
+ * MotorJointSystem.joints (MotorJointSystem.java:72-197) */
+sbx_status sbx_motor_joints(sbx_ctx* ctx, int32_t nB, const float* coord, const float* uVec,
+                            const float* segLength, const float* bTransGam, const float* bRotGam,
+                            float* forceSum, float* torqueSum, const int32_t* nucleotideState,
+                            const float* jointParams);
+/* DimerCouplingSystem.couple (DimerCouplingSystem.java:83-184) */
+sbx_status sbx_dimer_couple(sbx_ctx* ctx, int32_t nB, const float* coord, const float* uVec,
+                            const float* segLength, const float* bTransGam, const float* bRotGam,
+                            float* forceSum, float* torqueSum, int32_t nD, const int32_t* motorA,
+                            const int32_t* motorB, const int32_t* parallel, const float* dimerParams,
+                            const int32_t* boundSeg);
+/* MiniFilamentSystem.tether / backboneGather (MiniFilamentSystem.java:65-155) */
+sbx_status sbx_mini_tether(sbx_ctx* ctx, int32_t nMB, const float* mCoord, const float* mUVec,
+                           const float* mSegLength, const float* mBTransGam, const float* mBRotGam,
+                           float* mForceSum, float* mTorqueSum, int32_t nBb, const float* bbCoord,
+                           const float* bbUVec, const float* bbInvDragY, int32_t nD,
+                           const int32_t* headBackboneSlot, const int32_t* motorA, const float* attachAxial,
+                           float* miniData, const float* miniParams);
+sbx_status sbx_mini_backbone_gather(sbx_ctx* ctx, int32_t nBb, const int32_t* bbDimerOffsets,
+                                    const int32_t* bbDimerList, const float* miniData, float* bbForceSum,
+                                    float* bbTorqueSum);
+
+/* ThermostatDiag.torsionalRestore (ThermostatDiag.java:127-145): diagnostic restore of
+ * every motor rod's uVec toward +z, used by the equipartition check. */
+sbx_status sbx_thermostat_torsional_restore(sbx_ctx* ctx, int32_t nMotors, const float* uVec,
+                                            const float* bRotGam, float* torqueSum, double coeff, double dt);
+
+/* ================================================================ store descriptors
+ * Mirrors of the reference stores (device pointers). Used by the fused step plans. */
+typedef struct sbx_rigid_body {           /* RigidRodBody.java:26-84 */
+    int32_t n;
+    float *coord, *uVec, *yVec, *zVec, *end1, *end2, *segLength;
+    float *bTransGam, *bRotGam, *bTransDiff, *bRotDiff;
+    float *forceSum, *torqueSum, *randForce, *randTorque;
+    float *brownTransScale, *brownRotScale;
+    double *coord64;                      /* optional FP64 centres (NULL = reference FP32) */
+} sbx_rigid_body;
+
+typedef struct sbx_filament_store {       /* FilamentStore.java:29-199 */
+    sbx_rigid_body body;
+    int32_t *monomerCount, *end1NbrSlot, *end1NbrSide, *end2NbrSlot, *end2NbrSide, *filState;
+    float *params;                        /* [0]=dt [1]=sqrt(2kT/dt) */
+    float *chainParams;                   /* ChainBendingForceSystem.java:31-32 */
+    int32_t *counts;                      /* [0]=n [1]=step [2]=seed [3]=loadOn */
+} sbx_filament_store;
+
+typedef struct sbx_motor_store {          /* MotorStore.java:32-161 */
+    sbx_rigid_body body;                  /* 3*nMotors sub-bodies: rod, lever, head */
+    int32_t nMotors;
+    float *head, *uVec, *rodUVec, *reach, *bindArc;
+    int32_t *boundSeg, *stats, *capStats, *cooldown;
+    int32_t *nucleotideState, *forceDotPlace;
+    float *forceDotFil, *forceMag, *forceDotHist;
+    float *bodyParams, *jointParams, *kinParams, *nucParams;
+    int32_t *counts;                      /* [0]=nMotors [1]=step [2]=seed [3]=nSeg */
+    int32_t *publishParams;               /* [0]=base body-view slot */
+} sbx_motor_store;
+
+typedef struct sbx_dimer_store {          /* DimerStore.java:211-252 */
+    int32_t nDimers;
+    int32_t *motorA, *motorB, *parallel;
+    float *dimerParams;
+} sbx_dimer_store;
+
+typedef struct sbx_minifilament_store {   /* MiniFilamentStore.java:201-308 */
+    sbx_rigid_body backbone;
+    int32_t nBackbones, nDimers;
+    float *bbBodyParams;
+    int32_t *bbCounts;                    /* [1]=step [2]=seed */
+    int32_t *headBackboneSlot, *motorA;
+    float *attachAxial, *miniData, *bbInvDragY, *miniParams;
+    int32_t *bbDimerCount, *bbDimerOffsets, *bbDimerList;
+} sbx_minifilament_store;
+
+typedef struct sbx_crosslinker_store {    /* CrosslinkerStore.java:31-179 */
+    int32_t nLinks;
+    int32_t *linkFilA, *linkFilB, *linkState, *linkOrientSame, *activeLinkCount;
+    float *loc1, *loc2, *xlinkData;
+    float *strainHist, *torqueMagHist;
+    int32_t *strainPlace, *torqueMagPlace;
+    float *xlParams, *offParams, *torsionParams;
+    int32_t *counts;                      /* [0]=nLinks [1]=step [2]=seed [3]=nSeg */
+    /* two-pass gather CSRs (DenseContractileHarness.java:82-83) */
+    int32_t *segCountA, *segOffsetsA, *segIdxA, *segCountB, *segOffsetsB, *segIdxB;
+} sbx_crosslinker_store;
+
+typedef struct sbx_grid_state {           /* SpatialBodyView.java:29-56 + SpatialGrid scratch */
+    int32_t cap, totalCells;
+    float *center, *boundingRadius;
+    int32_t *ownerStore, *ownerSlot;
+    float *gridParams, *viewParams;
+    int32_t *gridDims, *gridCounts;       /* gridCounts[1] = S */
+    int32_t *bodyCell, *cellCount, *chunkSum, *gridCellOffsets, *gridCellContents;
+    int32_t *reachSeg, *reachCount;       /* nMotors*SBX_MAX_CAND, nMotors */
+} sbx_grid_state;
+
+/* One dense contractile network: the composition and step order of
+ * DenseContractileHarness.cpuStep (DenseContractileHarness.java:350-429). */
+typedef struct sbx_dense_scene {
+    sbx_filament_store fil;
+    sbx_motor_store mot;
+    sbx_dimer_store dim;
+    sbx_minifilament_store mini;
+    sbx_crosslinker_store xl;
+    sbx_grid_state grid;
+    float *bondData, *xbParams, *boxParams;
+    int32_t *segMotorCount, *segMotorOffsets, *segMotorMyo;
+    int32_t seed, seedBb;                 /* SEED, SEED_BB */
+    int32_t xlinkOn, xlUnbind;
+} sbx_dense_scene;
+
+typedef struct sbx_dense_plan sbx_dense_plan;
+
+/* Builds the fused step for `scene` (pointers are kept; the scene's arrays must stay
+ * alive). The fused step is bit-identical to calling the per-system entry points in
+ * the DenseContractileHarness.cpuStep order. */
+sbx_status sbx_dense_plan_create(sbx_ctx* ctx, const sbx_dense_scene* scene, sbx_dense_plan** out);
+/* Advances steps t0, t0+1, ..., t0+nsteps-1 (the step index feeds every RNG key and
+ * the containment cadence). use_graph != 0 replays a captured CUDA graph per step. */
+sbx_status sbx_dense_plan_run(sbx_dense_plan* plan, int32_t t0, int32_t nsteps, int32_t use_graph);
+/* Runs one step as the unfused per-system call sequence (reference granularity). */
+sbx_status sbx_dense_step_unfused(sbx_ctx* ctx, const sbx_dense_scene* scene, int32_t t);
+/* Number of kernels one fused step launches. */
+int32_t sbx_dense_plan_kernels_per_step(sbx_dense_plan* plan);
+/* Overflow flags raised since the last call (bit0: reach list > MAX_CAND); clears them. */
+sbx_status sbx_dense_plan_overflow(sbx_dense_plan* plan, int32_t* flags);
+sbx_status sbx_dense_plan_destroy(sbx_dense_plan* plan);
+
+/* Free rods (DiffusionHarness cpuStepFdt order: brownian -> integrate -> derive).
+ * Runs nsteps steps (t0..) in one persistent launch that keeps each rod in registers.
+ * noise_mode 0 = Wang hash (reference), 1 = Philox (philox_seed), 2 = supplied
+ * (noise = planar [nsteps][6][n]). */
+sbx_status sbx_free_rods_run(sbx_ctx* ctx, sbx_filament_store* fil, int32_t t0, int32_t nsteps,
+                             int32_t noise_mode, uint64_t philox_seed, const float* noise);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SOFTBOX_B200_H */

@@ -1,0 +1,106 @@
+"""ctypes wrapper of the CPU oracle (test infrastructure only).
+
+Loads oracle/_build/liboracle.so (libm transcendentals, the reference's platform math)
+or liboracle_dm.so (the portable double functions the CUDA kernels evaluate). Only the
+tests, the smoke check and bench.py's CPU-baseline leg use this module.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_BUILD = os.path.join(_HERE, "_build")
+
+# argument codes: i int32, I uint64, d double, f float, p pointer, s struct pointer
+_SIGS = {
+    "orc_set_threads": "i", "orc_max_threads": "", "orc_accurate_acos": "d", "orc_angle_from_sin_cos": "dd",
+    "orc_kT": "", "orc_rod_drag_si": "dddp", "orc_sphere_drag_si": "ddp",
+    "orc_drag_run_filament": "ipppdppppp", "orc_drag_run_motor": "idppppp", "orc_backbone_drag": "iddpppppp",
+    "orc_brownian_force": "ipppppppp", "orc_brownian_force_philox": "ippppppppI",
+    "orc_brownian_force_supplied": "ipppppppp", "orc_gauss6_wang": "iiip", "orc_gauss6_philox": "iiIp",
+    "orc_zero_accumulators": "ipp", "orc_integrate": "ippppppppppp", "orc_derive": "ippppppp",
+    "orc_confine": "ipppppppp", "orc_force_build": "ipppppppppp", "orc_integ_derive": "ippppppppppppppp",
+    "orc_integ_derive_confined": "ipppppppppppppppp", "orc_chain_forces": "ipppppppppppp",
+    "orc_seed_accumulators": "ipppp", "orc_pin_endpoints": "ipppippp", "orc_fil_publish": "ippipppppp",
+    "orc_mot_publish_head": "ipppppp", "orc_mot_publish": "ippippppi", "orc_body_cell": "ipppip",
+    "orc_grid_zero": "ip", "orc_grid_histogram": "pip", "orc_grid_scan_local": "ippp",
+    "orc_grid_scan_chunks": "ip", "orc_grid_scan_add": "ipipp", "orc_grid_scatter": "pippip",
+    "orc_body_chunk_size": "ii", "orc_grid_chunk_zero": "iip", "orc_grid_chunk_histogram": "piiiip",
+    "orc_grid_chunk_reduce": "iipp", "orc_grid_chunk_scatter": "piiiippip", "orc_broad_phase": "ipppppppipp",
+    "orc_brute_force": "ipppipp", "orc_invert_candidates": "ppppiipp",
+    "orc_grid_reachable": "ipppippppppppppp", "orc_compute_reachable": "ipppippppppp",
+    "orc_brute_reachable": "ipppippppp", "orc_bind_nearest": "ipppippppppp",
+    "orc_bind_kinetics": "ipppippppppppp", "orc_cycle": "ippppp", "orc_catch_slip_release": "ipppppppp",
+    "orc_bond_forces": "ippppipppppppppp", "orc_apply_head_force": "ippp",
+    "orc_register_force_dot": "ipppppp", "orc_csr_histogram": "piip", "orc_csr_scan": "ipp",
+    "orc_csr_scatter": "pippp", "orc_csr_chunk_zero": "iip", "orc_csr_chunk_histogram": "piiiip",
+    "orc_csr_chunk_reduce": "iipp", "orc_csr_chunk_scatter": "piiiippp", "orc_seg_gather": "ippppp",
+    "orc_xb_brute_gather": "iipppp", "orc_link_forces": "ippppippppppp", "orc_seg_gather_a": "ipppppp",
+    "orc_seg_gather_b": "ipppppp", "orc_xl_brute_gather": "iipppppp", "orc_xl_unbind": "ippippppppppp",
+    "orc_count_active_links": "ipppip", "orc_link_torsion": "ipipppppppp",
+    "orc_compute_fil_link_ct": "ipppip", "orc_joints": "ippppppppp", "orc_dimer_couple": "ipppppppippppp",
+    "orc_mini_tether": "ipppppppipppippppp", "orc_backbone_gather": "ippppp",
+    "orc_mini_brute_gather": "iipppp", "orc_torsional_restore": "ipppdd", "orc_dense_step": "si",
+    "orc_dense_run": "sii", "orc_fdt_run": "sii", "orc_chain_run": "sii",
+    "orc_m_log": "d", "orc_m_exp": "d", "orc_m_sin": "d", "orc_m_cos": "d", "orc_m_eval": "iipp",
+}
+_CT = {"i": C.c_int32, "I": C.c_uint64, "d": C.c_double, "f": C.c_float, "p": C.c_void_p, "s": C.c_void_p}
+_RET = {"orc_max_threads": C.c_int, "orc_accurate_acos": C.c_double, "orc_angle_from_sin_cos": C.c_double,
+        "orc_kT": C.c_double, "orc_body_chunk_size": C.c_int32,
+        "orc_m_log": C.c_double, "orc_m_exp": C.c_double, "orc_m_sin": C.c_double, "orc_m_cos": C.c_double}
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+class Oracle:
+    """One loaded oracle library. Array arguments may be numpy arrays (passed by
+    pointer), None (NULL) or ctypes structures (passed by reference)."""
+
+    def __init__(self, devmath=False):
+        name = "liboracle_dm.so" if devmath else "liboracle.so"
+        path = os.path.join(_BUILD, name)
+        if not os.path.exists(path):
+            build()
+        self.lib = C.CDLL(path)
+        self.devmath = devmath
+        for fn, sig in _SIGS.items():
+            f = getattr(self.lib, fn)
+            f.argtypes = [_CT[c] for c in sig]
+            f.restype = _RET.get(fn, None)
+
+    def __getattr__(self, name):
+        fn = getattr(self.lib, "orc_" + name)
+        sig = _SIGS["orc_" + name]
+
+        def call(*args):
+            if len(args) != len(sig):
+                raise TypeError(f"orc_{name} takes {len(sig)} args, got {len(args)}")
+            conv = []
+            for a, c in zip(args, sig):
+                if c in "ps":
+                    if a is None:
+                        conv.append(None)
+                    elif isinstance(a, np.ndarray):
+                        assert a.flags["C_CONTIGUOUS"]
+                        conv.append(a.ctypes.data)
+                    elif isinstance(a, C.Structure):
+                        conv.append(C.addressof(a))
+                    else:
+                        raise TypeError(f"bad pointer arg {type(a)} for orc_{name}")
+                else:
+                    conv.append(a)
+            return fn(*conv)
+        return call
+
+
+_cache = {}
+
+
+def get(devmath=False):
+    if devmath not in _cache:
+        _cache[devmath] = Oracle(devmath)
+    return _cache[devmath]

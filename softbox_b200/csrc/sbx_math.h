@@ -1,0 +1,222 @@
+// sbx_math.h — scalar arithmetic shared by the CUDA kernels and by host code.
+//
+// Why this file exists: the reference evaluates Math.log / Math.sin / Math.cos /
+// Math.exp in double and rounds the result to float (BrownianForceSystem.java:88-104,
+// ChainBendingForceSystem.java:48-84, NucleotideCycleSystem.java:116). To make the
+// device and a CPU checker produce the SAME bits, both sides must evaluate the SAME
+// double-precision function. This header supplies one portable implementation of
+// log, exp, sin and cos written from textbook mathematics:
+//
+//   * Cody & Waite argument reduction (W. J. Cody, W. Waite, "Software Manual for
+//     the Elementary Functions", 1980): x = k*(pi/2) + r with pi/2 split into three
+//     doubles, and x = k*ln2 + r with ln2 split into two doubles. The split constants
+//     are derived by gen_math_constants.py (decimal arithmetic, 60 digits).
+//   * Taylor polynomials on the reduced range (coefficients are 1/n! and 1/(2k+1)),
+//     evaluated by Horner's rule.
+//   * log(m) = 2*atanh(f/(2+f)), f = m - 1, m in [sqrt(1/2), sqrt(2)).
+//
+// Accuracy (checked in tests/test_math.py against libm and, on the GPU, against
+// CUDA's own functions): <= 2 ulp in double for |x| <= 2^20 (sin/cos), all positive
+// normal x (log), |x| <= 700 (exp). Compiled with contraction disabled
+// (-ffp-contract=off on the host, -fmad=false on the device) every operation is a
+// single IEEE-754 round-to-nearest step, so host and device agree bit for bit.
+#pragma once
+#include <stdint.h>
+#include <string.h>
+
+#if defined(__CUDACC__)
+#define SBX_HD __host__ __device__ __forceinline__
+#else
+#define SBX_HD static inline
+#endif
+
+namespace sbxm {
+
+// ---- split constants (gen_math_constants.py) ----
+#define SBXM_PIO2_HI   0x1.921fb54400000p+0
+#define SBXM_PIO2_MID  0x1.0b4611a600000p-34
+#define SBXM_PIO2_LO   0x1.3198a2e037073p-69
+#define SBXM_2_OVER_PI 0x1.45f306dc9c883p-1
+#define SBXM_LN2_HI    0x1.62e42fee00000p-1
+#define SBXM_LN2_LO    0x1.a39ef35793c76p-33
+#define SBXM_INV_LN2   0x1.71547652b82fep+0
+#define SBXM_SQRT2     0x1.6a09e667f3bcdp+0
+
+SBX_HD uint64_t dbits(double x) { uint64_t u; memcpy(&u, &x, 8); return u; }
+SBX_HD double bitsd(uint64_t u) { double x; memcpy(&x, &u, 8); return x; }
+
+// nearest integer of a moderate-size double (ties away from zero)
+SBX_HD int nearest_int(double x) {
+    double t = (x >= 0.0) ? (x + 0.5) : (x - 0.5);
+    return (int)t;
+}
+
+// sin and cos of a reduced argument |r| <= ~pi/4 (Taylor, Horner in r^2)
+SBX_HD double sin_poly(double r) {
+    double r2 = r * r;
+    double p = 1.0 / 51090942171709440000.0;      //  1/21!
+    p = p * r2 - 1.0 / 121645100408832000.0;      // -1/19!
+    p = p * r2 + 1.0 / 355687428096000.0;         //  1/17!
+    p = p * r2 - 1.0 / 1307674368000.0;           // -1/15!
+    p = p * r2 + 1.0 / 6227020800.0;              //  1/13!
+    p = p * r2 - 1.0 / 39916800.0;                // -1/11!
+    p = p * r2 + 1.0 / 362880.0;                  //  1/9!
+    p = p * r2 - 1.0 / 5040.0;                    // -1/7!
+    p = p * r2 + 1.0 / 120.0;                     //  1/5!
+    p = p * r2 - 1.0 / 6.0;                       // -1/3!
+    return r + r * (r2 * p);
+}
+
+SBX_HD double cos_poly(double r) {
+    double r2 = r * r;
+    double p = -1.0 / 1124000727777607680000.0;   // -1/22!
+    p = p * r2 + 1.0 / 2432902008176640000.0;     //  1/20!
+    p = p * r2 - 1.0 / 6402373705728000.0;        // -1/18!
+    p = p * r2 + 1.0 / 20922789888000.0;          //  1/16!
+    p = p * r2 - 1.0 / 87178291200.0;             // -1/14!
+    p = p * r2 + 1.0 / 479001600.0;               //  1/12!
+    p = p * r2 - 1.0 / 3628800.0;                 // -1/10!
+    p = p * r2 + 1.0 / 40320.0;                   //  1/8!
+    p = p * r2 - 1.0 / 720.0;                     // -1/6!
+    p = p * r2 + 1.0 / 24.0;                      //  1/4!
+    p = p * r2 - 0.5;                             // -1/2!
+    return 1.0 + r2 * p;
+}
+
+// x = k*(pi/2) + r, |r| <= pi/4 (+ tiny); returns r, writes the quadrant k & 3
+SBX_HD double reduce_pio2(double x, int* quadrant) {
+    int k = nearest_int(x * SBXM_2_OVER_PI);
+    double kd = (double)k;
+    double r = x - kd * SBXM_PIO2_HI;
+    r = r - kd * SBXM_PIO2_MID;
+    r = r - kd * SBXM_PIO2_LO;
+    *quadrant = k & 3;
+    return r;
+}
+
+SBX_HD double sin(double x) {
+    int q; double r = reduce_pio2(x, &q);
+    switch (q) {
+        case 0: return sin_poly(r);
+        case 1: return cos_poly(r);
+        case 2: return -sin_poly(r);
+        default: return -cos_poly(r);
+    }
+}
+
+SBX_HD double cos(double x) {
+    int q; double r = reduce_pio2(x, &q);
+    switch (q) {
+        case 0: return cos_poly(r);
+        case 1: return -sin_poly(r);
+        case 2: return -cos_poly(r);
+        default: return sin_poly(r);
+    }
+}
+
+// natural log of a positive double (x <= 0 -> -inf / NaN like libm)
+SBX_HD double log(double x) {
+    if (!(x > 0.0)) return (x == 0.0) ? bitsd(0xfff0000000000000ULL) : bitsd(0x7ff8000000000000ULL);
+    uint64_t u = dbits(x);
+    int e = (int)((u >> 52) & 0x7ff);
+    if (e == 0x7ff) return x;                          // +inf
+    int adj = 0;
+    if (e == 0) {                                      // subnormal: scale into the normal range
+        x = x * 0x1p54; u = dbits(x); e = (int)((u >> 52) & 0x7ff); adj = -54;
+    }
+    e = e - 1023 + adj;
+    double m = bitsd((u & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL);   // [1,2)
+    if (m > SBXM_SQRT2) { m = m * 0.5; e = e + 1; }
+    double f = m - 1.0;
+    double s = f / (2.0 + f);
+    double s2 = s * s;
+    double q = 1.0 / 23.0;
+    q = q * s2 + 1.0 / 21.0;
+    q = q * s2 + 1.0 / 19.0;
+    q = q * s2 + 1.0 / 17.0;
+    q = q * s2 + 1.0 / 15.0;
+    q = q * s2 + 1.0 / 13.0;
+    q = q * s2 + 1.0 / 11.0;
+    q = q * s2 + 1.0 / 9.0;
+    q = q * s2 + 1.0 / 7.0;
+    q = q * s2 + 1.0 / 5.0;
+    q = q * s2 + 1.0 / 3.0;
+    double two_s = 2.0 * s;
+    double ed = (double)e;
+    double lo = ed * SBXM_LN2_LO + two_s * (s2 * q);
+    return ed * SBXM_LN2_HI + (two_s + lo);
+}
+
+// e^x
+SBX_HD double exp(double x) {
+    if (x != x) return x;
+    if (x > 709.782712893384) return bitsd(0x7ff0000000000000ULL);
+    if (x < -745.1332191019412) return 0.0;
+    int k = nearest_int(x * SBXM_INV_LN2);
+    double kd = (double)k;
+    double r = x - kd * SBXM_LN2_HI;
+    r = r - kd * SBXM_LN2_LO;
+    double p = 1.0 / 1307674368000.0;               // 1/15!
+    p = p * r + 1.0 / 87178291200.0;                // 1/14!
+    p = p * r + 1.0 / 6227020800.0;                 // 1/13!
+    p = p * r + 1.0 / 479001600.0;                  // 1/12!
+    p = p * r + 1.0 / 39916800.0;                   // 1/11!
+    p = p * r + 1.0 / 3628800.0;                    // 1/10!
+    p = p * r + 1.0 / 362880.0;                     // 1/9!
+    p = p * r + 1.0 / 40320.0;                      // 1/8!
+    p = p * r + 1.0 / 5040.0;                       // 1/7!
+    p = p * r + 1.0 / 720.0;                        // 1/6!
+    p = p * r + 1.0 / 120.0;                        // 1/5!
+    p = p * r + 1.0 / 24.0;                         // 1/4!
+    p = p * r + 1.0 / 6.0;                          // 1/3!
+    p = p * r + 0.5;                                // 1/2!
+    double er = 1.0 + (r + r * (r * p));
+    // scale by 2^k in two halves so that k down to -1074 stays representable
+    int k1 = k / 2, k2 = k - k1;
+    double s1 = bitsd((uint64_t)(k1 + 1023) << 52);
+    double s2 = bitsd((uint64_t)(k2 + 1023) << 52);
+    return (er * s1) * s2;
+}
+
+// ---- integer hashing and counter-based generators ----
+
+// 32-bit Wang hash (unsigned arithmetic == Java int wraparound with >>>)
+SBX_HD uint32_t wang_hash(uint32_t s) {
+    s = (s ^ 61u) ^ (s >> 16);
+    s = s * 9u;
+    s = s ^ (s >> 4);
+    s = s * 0x27d4eb2du;
+    s = s ^ (s >> 15);
+    return s;
+}
+
+// per-(slot, step, seed) base key: (i*1000003) ^ (step*999983) ^ (seed*7919), int32 wrap
+SBX_HD uint32_t rng_base(int32_t i, int32_t step, int32_t seed) {
+    return ((uint32_t)i * 1000003u) ^ ((uint32_t)step * 999983u) ^ ((uint32_t)seed * 7919u);
+}
+
+// (h >>> 1) / 2147483647.0f : the float literal 2147483647.0f is exactly 2^31
+SBX_HD float unit_from_hash(uint32_t h) {
+    return (float)(int32_t)(h >> 1) / 2147483648.0f;
+}
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as
+// 1, 2, 3", SC'11): counter c[4], key k[2], 10 rounds.
+SBX_HD void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+    const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+    for (int r = 0; r < 10; r++) {
+        uint64_t p0 = (uint64_t)M0 * c[0];
+        uint64_t p1 = (uint64_t)M1 * c[2];
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c[1] ^ k0;
+        uint32_t n1 = lo1;
+        uint32_t n2 = hi0 ^ c[3] ^ k1;
+        uint32_t n3 = lo0;
+        c[0] = n0; c[1] = n1; c[2] = n2; c[3] = n3;
+        k0 += W0; k1 += W1;
+    }
+}
+
+}  // namespace sbxm

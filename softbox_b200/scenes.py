@@ -1,0 +1,593 @@
+"""Host-side stores and scene builders.
+
+Arrays follow the reference's planar SoA store layouts (FilamentStore.java:10-22:
+[x0..xN-1 | y0..yN-1 | z0..zN-1]) and field names, so a scene built here is the same
+data a reference harness would hand to its System classes. Builders restate the
+reference harnesses' host set-up:
+
+  * free_rods_fdt      DiffusionHarness.freshStore        (DiffusionHarness.java:742-755)
+  * deflection_chain   DiffusionHarness.measureDeflection (DiffusionHarness.java:287-335)
+  * free_rods_box      the free-Brownian-rod workload (1,024 rods of 1.0 um in a 10 um box)
+  * dense_contractile  DenseContractileHarness.buildScene (DenseContractileHarness.java:112-280)
+                       with the network composition as a parameter set (DenseConfig)
+
+Host initialisation (drag tensors, Brownian amplitudes) runs here in double precision
+exactly as the reference's host code does (DragTensorSystem.java:33-97).
+"""
+import math
+from dataclasses import dataclass, field, replace
+
+import numpy as np
+
+from .javarandom import JavaRandom
+
+F32 = np.float32
+I32 = np.int32
+
+# Constants.java:25-67
+BOLTZ = 1.380662e-23
+TEMP_K = 298.15
+KT = BOLTZ * TEMP_K
+ACTIN_MONO_RADIUS = 0.0054 / 2.0
+ACTIN_RADIUS = 0.007 / 2.0
+STD_SEG_LENGTH = 32
+A_PARALLEL, A_ORTHOG, A_TURNING = -0.20, 0.84, -0.662
+BTRANS_COEFF, BROT_COEFF = 1.0, 0.5
+PERSISTENCE_LENGTH = 15.0
+EI = KT * (PERSISTENCE_LENGTH * 1.0e-6)
+# MotorStore.java:45-46, MiniFilamentStore.java:207-211, DimerStore.java:225-228
+ROD_LEN, LEVER_LEN, HEAD_LEN = 0.080, 0.008, 0.020
+ROD_R, LEVER_R, HEAD_R = 0.003, 0.002, 0.010
+BACKBONE_R = 0.005
+MINIFIL_FRAC_MOVE, MINIFIL_ALIGN = 0.07, 0.01
+DIMER_ROD_FRAC_MOVE, DIMER_LEVER_FMT, DIMER_LEVER_DEG = 0.2, 0.4, 160.0
+STORE_FILAMENT, STORE_MOTOR, STORE_NONE = 0, 1, -1
+MAX_CAND = 256
+GRID_SCAN_CHUNK = 512
+XB_STRIDE, XL_STRIDE, MINI_STRIDE = 13, 12, 6
+STRAIN_WIN, TORQUE_WIN = 10, 5
+NUC_NONE, NUC_ATP, NUC_ADPPI, NUC_ADP = 0, 1, 2, 3
+MYO_REBIND_TIME = 1.0e-5
+SIN80 = math.sin(math.radians(80.0))
+COS80 = math.cos(math.radians(80.0))
+
+
+def rod_drag_si(length_um, radius_um, aeta):
+    """DragTensorSystem.rodDragSI (DragTensorSystem.java:33-45)."""
+    LM = 1.0e-6 * length_um
+    RM = radius_um * 1.0e-6
+    logT = math.log(LM / (2 * RM))
+    bTGx = (2 * math.pi * aeta * LM) / (logT + A_PARALLEL)
+    bTGy = (4 * math.pi * aeta * LM) / (logT + A_ORTHOG)
+    bRGx = 4 * math.pi * aeta * RM * RM * LM
+    bRGy = (math.pi * aeta * (LM * LM * LM)) / (3 * (logT + A_TURNING))
+    return [bTGx, bTGy, bTGy, bRGx, bRGy, bRGy]
+
+
+def sphere_drag_si(radius_um, aeta):
+    """DragTensorSystem.sphereDragSI (DragTensorSystem.java:52-58)."""
+    RM = radius_um * 1.0e-6
+    bTG = 6 * math.pi * aeta * RM
+    bRG = 8 * math.pi * aeta * (RM * RM * RM)
+    return [bTG, bTG, bTG, bRG, bRG, bRG]
+
+
+def rigid_body(n):
+    """RigidRodBody.java:59-84 — all arrays zero."""
+    b = {k: np.zeros(3 * n, F32) for k in ("coord", "uVec", "yVec", "zVec", "end1", "end2", "bTransGam",
+                                           "bRotGam", "bTransDiff", "bRotDiff", "forceSum", "torqueSum",
+                                           "randForce", "randTorque")}
+    b["segLength"] = np.zeros(n, F32)
+    b["brownTransScale"] = np.zeros(n, F32)
+    b["brownRotScale"] = np.zeros(n, F32)
+    b["coord64"] = None
+    b["n"] = n
+    return b
+
+
+def store_drag(b, i, g):
+    """DragTensorSystem.storeDrag (DragTensorSystem.java:61-69)."""
+    n = b["n"]
+    for k in range(3):
+        b["bTransGam"][k * n + i] = F32(g[k])
+        b["bRotGam"][k * n + i] = F32(g[3 + k])
+        b["bTransDiff"][k * n + i] = F32(KT / g[k])
+        b["bRotDiff"][k * n + i] = F32(KT / g[3 + k])
+
+
+def set_vec(arr, n, i, x, y, z):
+    arr[i] = F32(x)
+    arr[n + i] = F32(y)
+    arr[2 * n + i] = F32(z)
+
+
+def derive_host(b):
+    """DerivedGeometrySystem.derive over host arrays (float32 arithmetic, as the reference)."""
+    n = b["n"]
+    u = b["uVec"].reshape(3, n)
+    y = b["yVec"].reshape(3, n)
+    c = b["coord"].reshape(3, n)
+    ux, uy, uz = u
+    yx, yy, yz = y
+    zx = uy * yz - uz * yy
+    zy = uz * yx - ux * yz
+    zz = ux * yy - uy * yx
+    m2 = zx * zx + zy * zy + zz * zz
+    inv = np.where(m2 > 0, F32(1.0) / np.sqrt(np.where(m2 > 0, m2, F32(1))), F32(1)).astype(F32)
+    zx = np.where(m2 > 0, zx * inv, zx)
+    zy = np.where(m2 > 0, zy * inv, zy)
+    zz = np.where(m2 > 0, zz * inv, zz)
+    b["zVec"][:] = np.concatenate([zx, zy, zz]).astype(F32)
+    b["yVec"][:] = np.concatenate([zy * uz - zz * uy, zz * ux - zx * uz, zx * uy - zy * ux]).astype(F32)
+    half = (b["segLength"] * F32(0.5)).astype(F32)
+    b["end1"][:] = np.concatenate([c[k] - half * u[k] for k in range(3)]).astype(F32)
+    b["end2"][:] = np.concatenate([c[k] + half * u[k] for k in range(3)]).astype(F32)
+
+
+def filament_store(n):
+    """FilamentStore.java:139-199."""
+    f = {"body": rigid_body(n)}
+    f["monomerCount"] = np.zeros(n, I32)
+    for k in ("end1NbrSlot", "end1NbrSide", "end2NbrSlot", "end2NbrSide"):
+        f[k] = np.full(n, -1, I32)
+    f["filState"] = np.zeros(n, I32)
+    f["params"] = np.zeros(2, F32)
+    f["counts"] = np.array([n, 0, 0, 1], I32)
+    f["chainParams"] = np.zeros(7, F32)
+    f["extForce"] = np.zeros(3 * n, F32)
+    return f
+
+
+def drag_run_filament(f, aeta):
+    """DragTensorSystem.run(FilamentStore) (DragTensorSystem.java:71-97), viscosity `aeta`."""
+    b = f["body"]
+    halfmono = ACTIN_MONO_RADIUS
+    for i in range(b["n"]):
+        length = (int(f["monomerCount"][i]) + 1) * ACTIN_MONO_RADIUS
+        b["segLength"][i] = F32(length)
+        at_end = f["end1NbrSlot"][i] == -1 or f["end2NbrSlot"][i] == -1
+        min_len = STD_SEG_LENGTH * halfmono if at_end else 30 * halfmono
+        as_if = length if length >= min_len else min_len
+        store_drag(b, i, rod_drag_si(as_if, ACTIN_RADIUS, aeta))
+
+
+def set_chain_params(f, dt, frac_move=0.5, frac_r=0.1, frac_move_torq=0.265, spring_active=0.0,
+                     spring=1.0e-20):
+    """FilamentStore.setChainParams (FilamentStore.java:345-353)."""
+    f["chainParams"][:] = np.array([dt, frac_move, frac_r, frac_move_torq, spring_active, spring,
+                                    ACTIN_MONO_RADIUS], F32)
+
+
+# ---------------------------------------------------------------------------- free rods
+def free_rods_fdt(n, monomer_ct=64, trans_scale=1.0, rot_scale=0.0, aeta=0.1, dt=1e-4, seed=12345):
+    """DiffusionHarness.freshStore (DiffusionHarness.java:742-755): n rods at the origin,
+    uVec = +x, yVec = +y; Config T uses (1, 0), Config R uses (0, 1)."""
+    f = filament_store(n)
+    b = f["body"]
+    f["monomerCount"][:] = monomer_ct
+    b["uVec"][:n] = 1.0
+    b["yVec"][n:2 * n] = 1.0
+    b["brownTransScale"][:] = F32(trans_scale)
+    b["brownRotScale"][:] = F32(rot_scale)
+    drag_run_filament(f, aeta)
+    f["params"][:] = np.array([dt, math.sqrt(2.0 * KT / dt)], F32)
+    f["counts"][:] = np.array([n, 0, seed, 1], I32)
+    return f
+
+
+def free_rods_box(n=1024, length_um=1.0, radius_um=0.004, box_um=10.0, aeta=1.0e-3, dt=1.0e-5,
+                  seed=0x5B0C0, trans_scale=1.0, rot_scale=1.0):
+    """Free Brownian rods: centres uniform in a cubic box, orientations uniform on the
+    sphere (normalised Gaussian triplet), slender-rod drag for (length, radius) in a
+    fluid of viscosity aeta."""
+    rng = np.random.default_rng(seed)
+    f = filament_store(n)
+    b = f["body"]
+    c = rng.uniform(0.0, box_um, size=(3, n))
+    u = rng.normal(size=(3, n))
+    u /= np.linalg.norm(u, axis=0)
+    a = np.where(np.abs(u[0]) < 0.9, 0, 1)                 # helper axis not parallel to u
+    helper = np.zeros((3, n))
+    helper[a, np.arange(n)] = 1.0
+    y = helper - (helper * u).sum(0) * u
+    y /= np.linalg.norm(y, axis=0)
+    b["coord"][:] = c.reshape(-1).astype(F32)
+    b["uVec"][:] = u.reshape(-1).astype(F32)
+    b["yVec"][:] = y.reshape(-1).astype(F32)
+    b["segLength"][:] = F32(length_um)
+    g = rod_drag_si(length_um, radius_um, aeta)
+    for i in range(n):
+        store_drag(b, i, g)
+    b["brownTransScale"][:] = F32(trans_scale)
+    b["brownRotScale"][:] = F32(rot_scale)
+    f["params"][:] = np.array([dt, math.sqrt(2.0 * KT / dt)], F32)
+    f["counts"][:] = np.array([n, 0, seed & 0x7FFFFFFF, 1], I32)
+    derive_host(b)
+    return f
+
+
+def deflection_chain(n_seg=11, frac_r=0.1, frac_move_torq=0.265, dt=1e-4):
+    """DiffusionHarness.measureDeflection set-up (DiffusionHarness.java:287-335): pinned
+    11-segment chain, Brownian off, midpoint load F = 48*EI*0.01/span^2."""
+    monomer_ct = STD_SEG_LENGTH
+    frac = 0.01
+    seg_len = (monomer_ct + 1) * ACTIN_MONO_RADIUS
+    total = n_seg * seg_len
+    span_m = total * 1.0e-6
+    force_n = 48.0 * EI * frac / (span_m * span_m)
+    mid = n_seg // 2
+    f = filament_store(n_seg)
+    b = f["body"]
+    x0 = -0.5 * total + 0.5 * seg_len
+    for k in range(n_seg):
+        f["monomerCount"][k] = monomer_ct
+        set_vec(b["uVec"], n_seg, k, 1, 0, 0)
+        set_vec(b["yVec"], n_seg, k, 0, 1, 0)
+        set_vec(b["coord"], n_seg, k, x0 + k * seg_len, 0, 0)
+        if k < n_seg - 1:
+            f["end2NbrSlot"][k] = k + 1
+            f["end2NbrSide"][k] = 0
+        if k > 0:
+            f["end1NbrSlot"][k] = k - 1
+            f["end1NbrSide"][k] = 1
+    drag_run_filament(f, 0.1)
+    f["params"][:] = np.array([dt, math.sqrt(2.0 * KT / dt)], F32)
+    set_chain_params(f, dt)
+    f["chainParams"][2] = F32(frac_r)
+    f["chainParams"][3] = F32(frac_move_torq)
+    f["extForce"][n_seg + mid] = F32(-force_n)
+    f["counts"][:] = np.array([n_seg, 0, 1, 1], I32)
+    f["pinSeg"] = np.array([0, n_seg - 1], I32)
+    f["pinEnd"] = np.array([1, 2], I32)
+    f["pinAnchor"] = np.array([-0.5 * total, 0, 0, 0.5 * total, 0, 0], F32)
+    f["analyticDefl"] = frac * total
+    f["mid"] = mid
+    return f
+
+
+# ---------------------------------------------------------------------------- dense network
+@dataclass
+class DenseConfig:
+    """Composition of a dense contractile network (DenseContractileHarness.java:42-63)."""
+    n_fil: int = 2000
+    segs_per_fil: int = 10
+    monomer_ct: int = 36            # (36+1)*0.0027 um = 0.0999 um rods
+    n_mini: int = 200
+    dimers_per_end: int = 8         # 16 heads per backbone end
+    backbone_len: float = 0.8
+    head_zone: float = 0.05
+    n_links: int = 4000
+    side: float = 20.0
+    box_z: float = 0.5
+    dt: float = 1.0e-5
+    aeta: float = 1.0e-3
+    myo_col_tol: float = 0.030
+    align_tol: float = -0.4
+    k_off: float = 20.0
+    myo_spring: float = 1.0e-9
+    j1_fmt: float = 0.4
+    brown_trans: float = 1.0
+    brown_rot: float = 0.3
+    chain_frac_move: float = 0.5
+    chain_frac_r: float = 0.1
+    chain_frac_move_torq: float = 0.2
+    xl_grab: float = 0.05
+    xl_rest: float = 0.035
+    xl_frac_move: float = 0.4
+    xl_off: tuple = (1.0, 0.0, 2.0)  # k_off = c + a*exp(b*strain): 1/s
+    xl_torsion_spring: float = 1.0e-19
+    xl_unbind: bool = True
+    seed: int = 0x0CDE5
+    seed_bb: int = 0x5C2F11
+    seed_fil: int = 0xF11A
+
+    @property
+    def n_seg(self):
+        return self.n_fil * self.segs_per_fil
+
+
+# The dense contractile network of the benchmark: 2,000 filaments x 10 rods of 0.1 um,
+# 200 minifilaments (0.8 um backbone, 16 heads per end), 4,000 crosslinkers, 20x20x0.5 um
+# slab with walls, water viscosity, dt = 10 us.
+C1 = DenseConfig()
+
+
+def dense_small(scale=0.05, **kw):
+    """The same composition scaled down (slab side scaled to keep density)."""
+    c = C1
+    n_fil = max(2, int(round(c.n_fil * scale)))
+    n_mini = max(1, int(round(c.n_mini * scale)))
+    n_links = max(1, int(round(c.n_links * scale)))
+    side = c.side * math.sqrt(scale)
+    return replace(c, n_fil=n_fil, n_mini=n_mini, n_links=n_links, side=side, **kw)
+
+
+def _place_arm(b, m, rc, d, p, e2, splay, cfg):
+    """ContractileAssayHarness.placeArm (ContractileAssayHarness.java:996-1016)."""
+    n = b["n"]
+    rod, lever, head = 3 * m, 3 * m + 1, 3 * m + 2
+    dx, dy, dz = d
+    px, py, pz = p
+    set_vec(b["coord"], n, rod, *rc)
+    set_vec(b["uVec"], n, rod, dx, dy, dz)
+    set_vec(b["yVec"], n, rod, px, py, pz)
+    lux = COS80 * dx + splay * SIN80 * px
+    luy = COS80 * dy + splay * SIN80 * py
+    luz = COS80 * dz + splay * SIN80 * pz
+    nx, ny, nz = dy * pz - dz * py, dz * px - dx * pz, dx * py - dy * px
+    ll, hl = LEVER_LEN, HEAD_LEN
+    set_vec(b["coord"], n, lever, e2[0] + 0.5 * ll * lux, e2[1] + 0.5 * ll * luy, e2[2] + 0.5 * ll * luz)
+    set_vec(b["uVec"], n, lever, lux, luy, luz)
+    set_vec(b["yVec"], n, lever, nx, ny, nz)
+    le2 = (e2[0] + ll * lux, e2[1] + ll * luy, e2[2] + ll * luz)
+    set_vec(b["coord"], n, head, le2[0] + 0.5 * hl * lux, le2[1] + 0.5 * hl * luy, le2[2] + 0.5 * hl * luz)
+    set_vec(b["uVec"], n, head, lux, luy, luz)
+    set_vec(b["yVec"], n, head, nx, ny, nz)
+    b["brownTransScale"][rod] = F32(cfg.brown_trans)
+    b["brownRotScale"][rod] = F32(cfg.brown_rot)
+    b["brownTransScale"][lever] = 0
+    b["brownRotScale"][lever] = 0
+    b["brownTransScale"][head] = F32(cfg.brown_trans)
+    b["brownRotScale"][head] = F32(cfg.brown_rot)
+
+
+def _place_dimer_along(b, mA, mB, e1, d, p, cfg):
+    """ContractileAssayHarness.placeDimerAlong (ContractileAssayHarness.java:982-995)."""
+    dx, dy, dz = d
+    dm = math.sqrt(dx * dx + dy * dy + dz * dz)
+    dx, dy, dz = dx / dm, dy / dm, dz / dm
+    px, py, pz = p
+    pm = math.sqrt(px * px + py * py + pz * pz)
+    px, py, pz = px / pm, py / pm, pz / pm
+    rl = ROD_LEN
+    rc = (e1[0] + 0.5 * rl * dx, e1[1] + 0.5 * rl * dy, e1[2] + 0.5 * rl * dz)
+    e2 = (e1[0] + rl * dx, e1[1] + rl * dy, e1[2] + rl * dz)
+    _place_arm(b, mA, rc, (dx, dy, dz), (px, py, pz), e2, +1, cfg)
+    _place_arm(b, mB, rc, (dx, dy, dz), (px, py, pz), e2, -1, cfg)
+
+
+def _pack_cell(x, y, z):
+    return ((x & 0x1FFFFF) << 42) | ((y & 0x1FFFFF) << 21) | (z & 0x1FFFFF)
+
+
+def dense_contractile(cfg: DenseConfig = C1):
+    """DenseContractileHarness.buildScene (DenseContractileHarness.java:112-280) for the
+    composition `cfg`. Returns a dict-of-stores scene (host numpy arrays)."""
+    rng = JavaRandom(cfg.seed)
+    side, box_z, dt = cfg.side, cfg.box_z, cfg.dt
+    n_fil, S = cfg.n_fil, cfg.segs_per_fil
+    n_seg = n_fil * S
+    n_mini = cfg.n_mini
+    n_dimers = n_mini * 2 * cfg.dimers_per_end
+    n_mot = 2 * n_dimers
+    L = (cfg.monomer_ct + 1) * ACTIN_MONO_RADIUS
+    half = 0.5 * side
+    hz = 0.5 * box_z
+    margin = 0.5 * (S * L)
+
+    # ---- filaments: free multi-segment chains ----
+    f = filament_store(n_seg)
+    fb = f["body"]
+    for p in range(n_fil):
+        cx = (rng.next_double() - 0.5) * (side - 2 * margin)
+        cy = (rng.next_double() - 0.5) * (side - 2 * margin)
+        cz = (rng.next_double() - 0.5) * (box_z - 0.1)
+        th = rng.next_double() * math.pi * 2
+        ux, uy, uz = math.cos(th), math.sin(th), 0.0
+        yx, yy, yz = -uy, ux, 0.0
+        g0 = p * S
+        for s in range(S):
+            g = g0 + s
+            off = (s - 0.5 * (S - 1)) * L
+            f["monomerCount"][g] = cfg.monomer_ct
+            set_vec(fb["uVec"], n_seg, g, ux, uy, uz)
+            set_vec(fb["yVec"], n_seg, g, yx, yy, yz)
+            set_vec(fb["coord"], n_seg, g, cx + off * ux, cy + off * uy, cz + off * uz)
+            fb["brownTransScale"][g] = F32(BTRANS_COEFF)
+            end = (s == 0 or s == S - 1)
+            fb["brownRotScale"][g] = F32(BROT_COEFF if end else 0.0)
+            if s < S - 1:
+                f["end2NbrSlot"][g] = g + 1
+                f["end2NbrSide"][g] = 0
+            if s > 0:
+                f["end1NbrSlot"][g] = g - 1
+                f["end1NbrSide"][g] = 1
+    drag_run_filament(f, cfg.aeta)
+    f["params"][:] = np.array([dt, math.sqrt(2.0 * KT / dt)], F32)
+    f["counts"][:] = np.array([n_seg, 0, cfg.seed_fil, 1], I32)
+    f["chainParams"][:] = np.array([dt, cfg.chain_frac_move, cfg.chain_frac_r, cfg.chain_frac_move_torq,
+                                    0.0, 1.0e-20, ACTIN_MONO_RADIUS], F32)
+    derive_host(fb)
+
+    # ---- minifilaments: backbones each owning 2*dimers_per_end splayed dimers ----
+    mot = {"body": rigid_body(3 * n_mot), "nMotors": n_mot}
+    mb = mot["body"]
+    dim = {"nDimers": n_dimers, "motorA": np.zeros(n_dimers, I32), "motorB": np.zeros(n_dimers, I32),
+           "parallel": np.ones(n_dimers, I32)}
+    mini = {"backbone": rigid_body(n_mini), "nBackbones": n_mini, "nDimers": n_dimers,
+            "headBackboneSlot": np.zeros(n_dimers, I32), "motorA": np.zeros(n_dimers, I32),
+            "attachAxial": np.zeros(n_dimers, F32), "miniData": np.zeros(MINI_STRIDE * n_dimers, F32),
+            "bbInvDragY": np.zeros(2 * n_mini, F32), "bbDimerCount": np.zeros(n_mini, I32),
+            "bbDimerOffsets": np.zeros(n_mini + 1, I32), "bbDimerList": np.zeros(n_dimers, I32)}
+    bbb = mini["backbone"]
+    reach = np.zeros(n_mot, F32)
+    d = 0
+    for mfi in range(n_mini):
+        bx = (rng.next_double() - 0.5) * (side - 2 * margin)
+        by = (rng.next_double() - 0.5) * (side - 2 * margin)
+        bz = (rng.next_double() - 0.5) * (box_z - 0.1)
+        th = rng.next_double() * math.pi * 2
+        ux, uy, uz = math.cos(th), math.sin(th), 0.0
+        yx, yy, yz = -uy, ux, 0.0
+        set_vec(bbb["coord"], n_mini, mfi, bx, by, bz)
+        set_vec(bbb["uVec"], n_mini, mfi, ux, uy, uz)
+        set_vec(bbb["yVec"], n_mini, mfi, yx, yy, yz)
+        bbb["brownTransScale"][mfi] = F32(cfg.brown_trans)
+        bbb["brownRotScale"][mfi] = F32(cfg.brown_rot)
+        for e in range(2):
+            sgn = -1.0 if e == 0 else 1.0
+            for j in range(cfg.dimers_per_end):
+                mag = cfg.backbone_len / 2.0 - (j + 0.5) / cfg.dimers_per_end * cfg.head_zone
+                ax = sgn * mag
+                e1 = (bx + ax * ux, by + ax * uy, bz + ax * uz)
+                phi = (j + 0.5) / cfg.dimers_per_end * math.pi
+                px = math.cos(phi) * yx + math.sin(phi) * (uy * yz - uz * yy)
+                py = math.cos(phi) * yy + math.sin(phi) * (uz * yx - ux * yz)
+                pz = math.cos(phi) * yz + math.sin(phi) * (ux * yy - uy * yx)
+                mA, mB = 2 * d, 2 * d + 1
+                _place_dimer_along(mb, mA, mB, e1, (sgn * ux, sgn * uy, sgn * uz), (px, py, pz), cfg)
+                dim["motorA"][d], dim["motorB"][d], dim["parallel"][d] = mA, mB, 1
+                mini["headBackboneSlot"][d], mini["motorA"][d] = mfi, mA
+                mini["attachAxial"][d] = F32(ax)
+                reach[mA] = reach[mB] = F32(cfg.myo_col_tol)
+                d += 1
+    # DragTensorSystem.run(MotorStore) (DragTensorSystem.java:105-122)
+    gr = rod_drag_si(ROD_LEN, ROD_R, cfg.aeta)
+    gl = rod_drag_si(LEVER_LEN, LEVER_R, cfg.aeta)
+    gh = sphere_drag_si(HEAD_R, cfg.aeta)
+    mb["segLength"][0::3] = F32(ROD_LEN)
+    mb["segLength"][1::3] = F32(LEVER_LEN)
+    mb["segLength"][2::3] = F32(HEAD_LEN)
+    for m in range(n_mot):
+        store_drag(mb, 3 * m, gr)
+        store_drag(mb, 3 * m + 1, gl)
+        store_drag(mb, 3 * m + 2, gh)
+    # MiniFilamentStore.initBackboneDrag (MiniFilamentStore.java:294-307)
+    gbb = rod_drag_si(cfg.backbone_len, BACKBONE_R, cfg.aeta)
+    for bbi in range(n_mini):
+        bbb["segLength"][bbi] = F32(cfg.backbone_len)
+        store_drag(bbb, bbi, gbb)
+        mini["bbInvDragY"][bbi] = F32(1.0 / gbb[1])
+        mini["bbInvDragY"][n_mini + bbi] = F32(1.0 / gbb[4])
+
+    # MotorStore set-up (MotorStore.java:190-263), DenseContractileHarness.java:210-215
+    mot.update({
+        "head": np.zeros(3 * n_mot, F32), "uVec": np.zeros(3 * n_mot, F32), "rodUVec": np.zeros(3 * n_mot, F32),
+        "reach": reach, "boundSeg": np.full(n_mot, -1, I32), "bindArc": np.zeros(n_mot, F32),
+        "stats": np.zeros(2 * n_mot, I32), "capStats": np.zeros(n_mot, I32), "cooldown": np.zeros(n_mot, I32),
+        "nucleotideState": np.zeros(n_mot, I32), "forceDotPlace": np.zeros(n_mot, I32),
+        "forceDotFil": np.zeros(n_mot, F32), "forceMag": np.zeros(n_mot, F32),
+        "forceDotHist": np.zeros(10 * n_mot, F32),
+        "bodyParams": np.array([dt, math.sqrt(2.0 * KT / dt)], F32),
+        "jointParams": np.array([dt, 0.4, 0.4, 0.4, 0.0, 0.4, 0.4, 0.0, 96.0, 0.4, 6.0], F32),
+        "kinParams": np.array([cfg.k_off, 0.92, 0.08, 2.5e-9, 0.4e-9, KT, dt, cfg.myo_col_tol, cfg.align_tol,
+                               0.0, math.ceil(MYO_REBIND_TIME / dt), 12.0e-12, 1.0, 1.0], F32),
+        "nucParams": np.array([dt, 2.0e4, 100.0, 100.0, 1.0e4, 0.0, 1.0e3, 1.0e3], F32),
+        "counts": np.array([n_mot, 0, cfg.seed, n_seg], I32),
+        "publishParams": np.array([n_seg], I32),
+    })
+    dim["dimerParams"] = np.array([dt, DIMER_ROD_FRAC_MOVE, DIMER_LEVER_FMT, DIMER_LEVER_DEG, ROD_LEN], F32)
+    mini["miniParams"] = np.array([dt, MINIFIL_FRAC_MOVE, MINIFIL_ALIGN], F32)
+    mini["bbBodyParams"] = np.array([dt, math.sqrt(2.0 * KT / dt)], F32)
+    mini["bbCounts"] = np.array([n_mini, 0, cfg.seed_bb, n_mini], I32)
+
+    # ---- grid + body view (filaments + heads) ----
+    cap = n_seg + n_mot
+    seg_bound_r = 0.5 * L + ACTIN_RADIUS
+    cutoff = cfg.myo_col_tol + 0.5 * ROD_LEN
+    cell = 2.0 * seg_bound_r + cutoff
+    gx = half + 1.0
+    gy = gx
+    gz = hz + 0.3
+    nX = 1 + int(math.ceil(2 * gx / cell))
+    nY = 1 + int(math.ceil(2 * gy / cell))
+    nZ = 1 + int(math.ceil(2 * gz / cell))
+    total_cells = nX * nY * nZ
+    grid = {
+        "cap": cap, "totalCells": total_cells,
+        "center": np.zeros(3 * cap, F32), "boundingRadius": np.zeros(cap, F32),
+        "ownerStore": np.full(cap, -1, I32), "ownerSlot": np.full(cap, -1, I32),
+        "gridParams": np.array([-gx, -gy, -gz, cell, 1.0 / cell, cutoff], F32),
+        "viewParams": np.array([ACTIN_RADIUS], F32),
+        "gridDims": np.array([nX, nY, nZ, total_cells], I32),
+        "gridCounts": np.array([0, cap, 0, 0], I32),
+        "bodyCell": np.full(cap, -1, I32), "cellCount": np.zeros(total_cells, I32),
+        "chunkSum": np.zeros((total_cells + GRID_SCAN_CHUNK - 1) // GRID_SCAN_CHUNK + 1, I32),
+        "gridCellOffsets": np.zeros(total_cells + 1, I32), "gridCellContents": np.full(cap, -1, I32),
+        "reachSeg": np.full(n_mot * MAX_CAND, -1, I32), "reachCount": np.zeros(n_mot, I32),
+    }
+
+    # ---- crosslinkers pre-placed between nearby segments of distinct filaments ----
+    xl = _build_crosslinkers(f, n_seg, S, cfg, rng)
+
+    check_int = max(1, int(round(1.0e-4 / dt)))
+    scene = {
+        "cfg": cfg, "fil": f, "mot": mot, "dim": dim, "mini": mini, "xl": xl, "grid": grid,
+        "bondData": np.zeros(n_mot * XB_STRIDE, F32),
+        "xbParams": np.array([cfg.myo_spring, 90.0, cfg.j1_fmt, dt, HEAD_LEN, 0.0], F32),
+        "boxParams": np.array([1.0e-4, side, side, box_z, ACTIN_RADIUS, 0.5, check_int, dt], F32),
+        "segMotorCount": np.zeros(n_seg, I32), "segMotorOffsets": np.zeros(n_seg + 1, I32),
+        "segMotorMyo": np.zeros(n_mot, I32),
+        "seed": cfg.seed, "seedBb": cfg.seed_bb, "xlinkOn": 1, "xlUnbind": 1 if cfg.xl_unbind else 0,
+    }
+    return scene
+
+
+def _build_crosslinkers(f, n_seg, segs_per_fil, cfg, rng):
+    """DenseContractileHarness.buildCrosslinkers (DenseContractileHarness.java:296-341)."""
+    n_links = cfg.n_links
+    xl = {"nLinks": n_links,
+          "linkFilA": np.full(n_links, -1, I32), "linkFilB": np.full(n_links, -1, I32),
+          "linkState": np.full(n_links, -1, I32), "linkOrientSame": np.zeros(n_links, I32),
+          "activeLinkCount": np.zeros(n_seg, I32),
+          "loc1": np.zeros(n_links, F32), "loc2": np.zeros(n_links, F32),
+          "xlinkData": np.zeros(n_links * XL_STRIDE, F32),
+          "strainHist": np.zeros(n_links * STRAIN_WIN, F32), "torqueMagHist": np.zeros(n_links * TORQUE_WIN, F32),
+          "strainPlace": np.zeros(n_links, I32), "torqueMagPlace": np.zeros(n_links, I32),
+          "counts": np.array([n_links, 0, 0, n_seg], I32)}
+    for k in ("segCountA", "segCountB"):
+        xl[k] = np.zeros(n_seg, I32)
+    for k in ("segOffsetsA", "segOffsetsB"):
+        xl[k] = np.zeros(n_seg + 1, I32)
+    for k in ("segIdxA", "segIdxB"):
+        xl[k] = np.zeros(n_links, I32)
+    fb = f["body"]
+    c = fb["coord"]
+    grab = cfg.xl_grab
+    cell = grab
+    buckets = {}
+    cx_all = np.floor(c[:n_seg].astype(np.float64) / cell).astype(np.int64)
+    cy_all = np.floor(c[n_seg:2 * n_seg].astype(np.float64) / cell).astype(np.int64)
+    cz_all = np.floor(c[2 * n_seg:].astype(np.float64) / cell).astype(np.int64)
+    for s in range(n_seg):
+        buckets.setdefault(_pack_cell(int(cx_all[s]), int(cy_all[s]), int(cz_all[s])), []).append(s)
+    placed = attempts = 0
+    while placed < n_links and attempts < n_links * 200:
+        attempts += 1
+        s = rng.next_int(n_seg)
+        fil_s = s // segs_per_fil
+        sx, sy, sz = float(c[s]), float(c[n_seg + s]), float(c[2 * n_seg + s])
+        best, best_d = -1, grab * grab
+        cx, cy, cz = math.floor(sx / cell), math.floor(sy / cell), math.floor(sz / cell)
+        dx = -1
+        while dx <= 1 and best < 0:
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    bucket = buckets.get(_pack_cell(cx + dx, cy + dy, cz + dz))
+                    if bucket is None:
+                        continue
+                    for t in bucket:
+                        if t // segs_per_fil == fil_s:
+                            continue
+                        ddx = float(c[t]) - sx
+                        ddy = float(c[n_seg + t]) - sy
+                        ddz = float(c[2 * n_seg + t]) - sz
+                        dd = ddx * ddx + ddy * ddy + ddz * ddz
+                        if dd < best_d:
+                            best_d, best = dd, t
+            dx += 1
+        if best < 0:
+            continue
+        xl["linkFilA"][placed] = s
+        xl["linkFilB"][placed] = best
+        xl["loc1"][placed] = F32(0.5 * float(fb["segLength"][s]))
+        xl["loc2"][placed] = F32(0.5 * float(fb["segLength"][best]))
+        xl["linkState"][placed] = 0
+        xl["linkOrientSame"][placed] = 1
+        placed += 1
+    xl["placed"] = placed
+    xl["xlParams"] = np.array([cfg.xl_rest, cfg.xl_frac_move, cfg.dt], F32)
+    xl["offParams"] = np.array([cfg.xl_off[0], cfg.xl_off[1], cfg.xl_off[2], cfg.dt, cfg.xl_rest], F32)
+    xl["torsionParams"] = np.array([cfg.xl_torsion_spring, 1.0], F32)
+    xl["counts"][2] = cfg.seed
+    return xl

@@ -1,0 +1,26 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+for p in (ROOT, os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built libsoftbox_b200.so")
+    config.addinivalue_line("markers", "slow: long CPU statistics run")
+
+
+@pytest.fixture(scope="session")
+def orc():
+    import oracle
+    return oracle.get(devmath=False)
+
+
+@pytest.fixture(scope="session")
+def orc_dm():
+    import oracle
+    return oracle.get(devmath=True)
