@@ -53,7 +53,8 @@ typedef struct sbx_ctx sbx_ctx;
 
 /* ---------------------------------------------------------------- context / memory */
 /* Creates a context on `device`. `stream` is a cudaStream_t to run on, or NULL to
- * create a private non-blocking stream. */
+ * create a private blocking stream (ordered against the legacy default stream, and
+ * capturable into CUDA graphs, which the legacy stream is not). */
 sbx_status sbx_ctx_create(int device, void* stream, sbx_ctx** out);
 sbx_status sbx_ctx_destroy(sbx_ctx* ctx);
 const char* sbx_ctx_last_error(sbx_ctx* ctx);
@@ -170,11 +171,12 @@ sbx_status sbx_grid_body_cell(sbx_ctx* ctx, int32_t cap, const float* center, co
  * sums, as in the reference), scatter, then an in-cell ascending sort so that the
  * within-cell order is body-index order. Outputs equal the serial reference bit for bit:
  * gridCellOffsets[0..totalCells] (terminator clamped to contentsCap), gridCellContents,
- * cellCount (= per-cell counts, as the serial gridScatter leaves it), chunkSum. */
-sbx_status sbx_grid_build(sbx_ctx* ctx, const int32_t* bodyCell, const int32_t* counts,
-                          const int32_t* gridDims, int32_t totalCells, int32_t* cellCount,
-                          int32_t* chunkSum, int32_t* gridCellOffsets, int32_t* gridCellContents,
-                          int32_t contentsCap);
+ * cellCount (= per-cell counts, as the serial gridScatter leaves it), chunkSum.
+ * `cap` is the length of bodyCell; contentsCap < cap is rejected (the reference sizes
+ * gridCellContents = cap). Uses context scratch (cap ints) for the unordered scatter. */
+sbx_status sbx_grid_build(sbx_ctx* ctx, int32_t cap, const int32_t* bodyCell, const int32_t* counts,
+                          int32_t totalCells, int32_t* cellCount, int32_t* chunkSum,
+                          int32_t* gridCellOffsets, int32_t* gridCellContents, int32_t contentsCap);
 /* SpatialGrid.broadPhase (SpatialGrid.java:407-473); candPartner is cap*SBX_MAX_CAND */
 sbx_status sbx_grid_broad_phase(sbx_ctx* ctx, int32_t cap, const float* center, const float* boundingRadius,
                                 const int32_t* bodyCell, const int32_t* gridCellOffsets,
@@ -187,14 +189,14 @@ sbx_status sbx_grid_brute_force(sbx_ctx* ctx, int32_t cap, const float* center, 
                                 int32_t* bruteCount);
 
 /* ---------------------------------------------------------------- binding / unbinding
- * BindingDetectionSystem.gridReachable (BindingDetectionSystem.java:143-228); counts[0]=nM */
+ * BindingDetectionSystem.gridReachable (BindingDetectionSystem.java:143-228); nM = counts[0] */
 sbx_status sbx_binding_grid_reachable(sbx_ctx* ctx, const float* head, const float* uVec, const float* rodUVec,
                                       int32_t nSeg, const float* segEnd1, const float* segEnd2,
                                       const float* gridParams, const int32_t* gridDims,
                                       const int32_t* gridCellOffsets, const int32_t* gridCellContents,
                                       const int32_t* ownerStore, const int32_t* ownerSlot,
                                       int32_t* motorReachSeg, int32_t* motorReachCount,
-                                      const float* kinParams, const int32_t* counts, int32_t nM);
+                                      const float* kinParams, int32_t nM);
 /* BindingDetectionSystem.bruteReachable (BindingDetectionSystem.java:260-283) */
 sbx_status sbx_binding_brute_reachable(sbx_ctx* ctx, const float* head, const float* uVec,
                                        const float* rodUVec, int32_t nSeg, const float* segEnd1,

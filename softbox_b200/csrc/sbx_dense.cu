@@ -1,0 +1,242 @@
+// sbx_dense.cu — the dense contractile step (DenseContractileHarness.cpuStep,
+// DenseContractileHarness.java:350-429) as (a) the per-system call sequence and (b) a
+// plan whose step is captured once into a CUDA graph and replayed.
+//
+// The step index lives in device memory (plan->d_step): the first kernel of a step
+// writes every counts array from it and the last kernel advances it, so one captured
+// graph replays any number of consecutive steps with the right RNG keys and
+// containment cadence.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "../../include/softbox_b200.h"
+#include "sbx_internal.cuh"
+#include "sbx_physics.cuh"
+
+using namespace sbx;
+
+namespace {
+
+// MotorStore.setCounts / MiniFilamentStore.setBackboneCounts / counts.set(1, t) /
+// CrosslinkerStore.setCounts (DenseContractileHarness.java:353)
+__global__ void k_dense_set_counts(const int* d_step, int t_host, int* motCounts, int nM, int nSeg, int seed,
+                                   int* bbCounts, int nBb, int seedBb, int* filCounts, int* xlCounts) {
+    int t = d_step ? *d_step : t_host;
+    motCounts[0] = nM; motCounts[1] = t; motCounts[2] = seed; motCounts[3] = nSeg;
+    bbCounts[0] = nBb; bbCounts[1] = t; bbCounts[2] = seedBb; bbCounts[3] = nBb;
+    filCounts[1] = t;
+    if (xlCounts) { xlCounts[1] = t; xlCounts[2] = seed; }
+}
+
+__global__ void k_step_set(int* d_step, int t) { *d_step = t; }
+__global__ void k_step_advance(int* d_step) { *d_step += 1; }
+
+#define CHK(x)                      \
+    do {                            \
+        sbx_status _s = (x);        \
+        if (_s != SBX_OK) return _s; \
+    } while (0)
+
+// the reference step order over the per-system entry points
+sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_step, int t) {
+    const sbx_filament_store& f = sc->fil;
+    const sbx_motor_store& mot = sc->mot;
+    const sbx_dimer_store& dim = sc->dim;
+    const sbx_minifilament_store& mini = sc->mini;
+    const sbx_crosslinker_store& xl = sc->xl;
+    const sbx_grid_state& g = sc->grid;
+    const sbx_rigid_body& b = mot.body;
+    const sbx_rigid_body& bb = mini.backbone;
+    const sbx_rigid_body& fb = f.body;
+    const int nSeg = fb.n, nM = mot.nMotors, nB = b.n, nBb = bb.n, nD = dim.nDimers;
+    const bool xlOn = sc->xlinkOn && xl.nLinks > 0;
+
+    SBX_LAUNCH(ctx, k_dense_set_counts, 1, 1, d_step, t, mot.counts, nM, nSeg, sc->seed, mini.bbCounts, nBb,
+               sc->seedBb, f.counts, xlOn ? xl.counts : nullptr);
+    // (i) binding
+    CHK(sbx_motor_publish_head(ctx, nM, b.coord, b.uVec, b.segLength, mot.head, mot.uVec, mot.rodUVec));
+    CHK(sbx_filament_publish(ctx, nSeg, fb.coord, fb.segLength, g.cap, g.center, g.boundingRadius, g.ownerStore,
+                             g.ownerSlot, g.viewParams, nullptr));
+    CHK(sbx_motor_publish(ctx, nM, mot.head, mot.reach, g.cap, g.center, g.boundingRadius, g.ownerStore, g.ownerSlot,
+                          mot.publishParams));
+    CHK(sbx_grid_body_cell(ctx, g.cap, g.center, g.gridParams, g.gridDims, g.gridCounts, g.bodyCell));
+    CHK(sbx_grid_build(ctx, g.cap, g.bodyCell, g.gridCounts, g.totalCells, g.cellCount, g.chunkSum,
+                       g.gridCellOffsets, g.gridCellContents, g.cap));
+    CHK(sbx_binding_grid_reachable(ctx, mot.head, mot.uVec, mot.rodUVec, nSeg, fb.end1, fb.end2, g.gridParams,
+                                   g.gridDims, g.gridCellOffsets, g.gridCellContents, g.ownerStore, g.ownerSlot,
+                                   g.reachSeg, g.reachCount, mot.kinParams, nM));
+    CHK(sbx_nucleotide_release(ctx, nM, mot.boundSeg, mot.forceDotFil, mot.forceMag, mot.cooldown, mot.stats,
+                               mot.capStats, mot.kinParams, mot.counts));
+    CHK(sbx_binding_bind_nearest(ctx, mot.head, mot.uVec, mot.rodUVec, nSeg, fb.end1, fb.end2, g.reachSeg,
+                                 g.reachCount, mot.boundSeg, mot.bindArc, mot.kinParams, nM));
+    CHK(sbx_nucleotide_cycle(ctx, nM, mot.nucleotideState, mot.boundSeg, mot.forceDotHist, mot.nucParams,
+                             mot.counts));
+    // (ii) minifilament structure
+    CHK(sbx_zero_accumulators(ctx, nB, b.forceSum, b.torqueSum));
+    CHK(sbx_zero_accumulators(ctx, nBb, bb.forceSum, bb.torqueSum));
+    CHK(sbx_brownian_force(ctx, nB, b.randForce, b.randTorque, b.bTransGam, b.bRotGam, b.brownTransScale,
+                           b.brownRotScale, mot.bodyParams, mot.counts));
+    CHK(sbx_brownian_force(ctx, nBb, bb.randForce, bb.randTorque, bb.bTransGam, bb.bRotGam, bb.brownTransScale,
+                           bb.brownRotScale, mini.bbBodyParams, mini.bbCounts));
+    CHK(sbx_motor_joints(ctx, nB, b.coord, b.uVec, b.segLength, b.bTransGam, b.bRotGam, b.forceSum, b.torqueSum,
+                         mot.nucleotideState, mot.jointParams));
+    CHK(sbx_dimer_couple(ctx, nB, b.coord, b.uVec, b.segLength, b.bTransGam, b.bRotGam, b.forceSum, b.torqueSum, nD,
+                         dim.motorA, dim.motorB, dim.parallel, dim.dimerParams, mot.boundSeg));
+    CHK(sbx_mini_tether(ctx, nB, b.coord, b.uVec, b.segLength, b.bTransGam, b.bRotGam, b.forceSum, b.torqueSum, nBb,
+                        bb.coord, bb.uVec, mini.bbInvDragY, mini.nDimers, mini.headBackboneSlot, mini.motorA,
+                        mini.attachAxial, mini.miniData, mini.miniParams));
+    CHK(sbx_csr_build(ctx, mini.headBackboneSlot, mini.nDimers, nBb, mini.bbDimerCount, mini.bbDimerOffsets,
+                      mini.bbDimerList));
+    CHK(sbx_mini_backbone_gather(ctx, nBb, mini.bbDimerOffsets, mini.bbDimerList, mini.miniData, bb.forceSum,
+                                 bb.torqueSum));
+    CHK(sbx_xbridge_bond_forces(ctx, nB, b.coord, b.uVec, b.yVec, b.bRotGam, nSeg, fb.coord, fb.uVec, fb.yVec,
+                                fb.bRotGam, fb.segLength, mot.boundSeg, mot.bindArc, mot.nucleotideState, sc->bondData,
+                                sc->xbParams));
+    CHK(sbx_xbridge_apply_head_force(ctx, nB, sc->bondData, b.forceSum, b.torqueSum));
+    CHK(sbx_integrate(ctx, nB, b.coord, b.coord64, b.uVec, b.yVec, b.forceSum, b.torqueSum, b.randForce, b.randTorque,
+                      b.bTransGam, b.bRotGam, mot.bodyParams));
+    CHK(sbx_confine(ctx, nBb, bb.coord, bb.uVec, bb.segLength, bb.bTransGam, bb.forceSum, bb.torqueSum,
+                    sc->boxParams, mini.bbCounts));
+    CHK(sbx_integrate(ctx, nBb, bb.coord, bb.coord64, bb.uVec, bb.yVec, bb.forceSum, bb.torqueSum, bb.randForce,
+                      bb.randTorque, bb.bTransGam, bb.bRotGam, mini.bbBodyParams));
+    CHK(sbx_derive(ctx, nB, b.coord, b.uVec, b.yVec, b.zVec, b.end1, b.end2, b.segLength));
+    CHK(sbx_derive(ctx, nBb, bb.coord, bb.uVec, bb.yVec, bb.zVec, bb.end1, bb.end2, bb.segLength));
+    CHK(sbx_xbridge_register_force_dot(ctx, nM, sc->bondData, mot.boundSeg, mot.forceDotFil, mot.forceMag,
+                                       mot.forceDotHist, mot.forceDotPlace));
+    // (iii)-(v) filaments
+    CHK(sbx_zero_accumulators(ctx, nSeg, fb.forceSum, fb.torqueSum));
+    CHK(sbx_brownian_force(ctx, nSeg, fb.randForce, fb.randTorque, fb.bTransGam, fb.bRotGam, fb.brownTransScale,
+                           fb.brownRotScale, f.params, f.counts));
+    CHK(sbx_chain_forces(ctx, nSeg, fb.coord, fb.uVec, fb.segLength, f.end2NbrSlot, f.end2NbrSide, f.end1NbrSlot,
+                         f.end1NbrSide, fb.bTransGam, fb.bRotGam, fb.forceSum, fb.torqueSum, f.chainParams));
+    if (xlOn) {
+        if (sc->xlUnbind)
+            CHK(sbx_xlink_unbind(ctx, nSeg, fb.uVec, fb.end1, xl.nLinks, xl.linkFilA, xl.linkFilB, xl.loc1, xl.loc2,
+                                 xl.linkState, xl.strainHist, xl.strainPlace, xl.offParams, xl.counts));
+        CHK(sbx_xlink_count_active(ctx, xl.nLinks, xl.linkState, xl.linkFilA, xl.linkFilB, nSeg,
+                                   xl.activeLinkCount));
+        CHK(sbx_xlink_forces(ctx, nSeg, fb.coord, fb.uVec, fb.end1, fb.bTransGam, xl.nLinks, xl.linkFilA,
+                             xl.linkFilB, xl.loc1, xl.loc2, xl.activeLinkCount, xl.xlinkData, xl.xlParams));
+        CHK(sbx_xlink_torsion(ctx, nSeg, fb.uVec, xl.nLinks, xl.linkFilA, xl.linkFilB, xl.linkState,
+                              xl.linkOrientSame, xl.torqueMagHist, xl.torqueMagPlace, xl.xlinkData,
+                              xl.torsionParams));
+        CHK(sbx_csr_build(ctx, xl.linkFilA, xl.nLinks, nSeg, xl.segCountA, xl.segOffsetsA, xl.segIdxA));
+        CHK(sbx_xlink_seg_gather(ctx, 0, nSeg, xl.segOffsetsA, xl.segIdxA, xl.xlinkData, xl.linkState, fb.forceSum,
+                                 fb.torqueSum));
+        CHK(sbx_csr_build(ctx, xl.linkFilB, xl.nLinks, nSeg, xl.segCountB, xl.segOffsetsB, xl.segIdxB));
+        CHK(sbx_xlink_seg_gather(ctx, 1, nSeg, xl.segOffsetsB, xl.segIdxB, xl.xlinkData, xl.linkState, fb.forceSum,
+                                 fb.torqueSum));
+    }
+    CHK(sbx_csr_build(ctx, mot.boundSeg, nM, nSeg, sc->segMotorCount, sc->segMotorOffsets, sc->segMotorMyo));
+    CHK(sbx_xbridge_seg_gather(ctx, nSeg, sc->segMotorOffsets, sc->segMotorMyo, sc->bondData, fb.forceSum,
+                               fb.torqueSum));
+    CHK(sbx_confine(ctx, nSeg, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.forceSum, fb.torqueSum,
+                    sc->boxParams, f.counts));
+    CHK(sbx_integrate(ctx, nSeg, fb.coord, fb.coord64, fb.uVec, fb.yVec, fb.forceSum, fb.torqueSum, fb.randForce,
+                      fb.randTorque, fb.bTransGam, fb.bRotGam, f.params));
+    CHK(sbx_derive(ctx, nSeg, fb.coord, fb.uVec, fb.yVec, fb.zVec, fb.end1, fb.end2, fb.segLength));
+    return SBX_OK;
+}
+
+size_t dense_scratch_bytes(const sbx_dense_scene* sc) {
+    auto rows = [](int n) { return (size_t)(n + SCAN_CHUNK - 1) / SCAN_CHUNK + 1; };
+    size_t nSeg = sc->fil.body.n;
+    size_t need = (size_t)std::max(sc->grid.cap, 1);
+    need = std::max(need, rows(sc->mini.backbone.n) + (size_t)std::max(sc->mini.nDimers, 1));
+    need = std::max(need, rows((int)nSeg) + (size_t)std::max(sc->mot.nMotors, 1));
+    need = std::max(need, rows((int)nSeg) + (size_t)std::max(sc->xl.nLinks, 1));
+    return sizeof(int) * need;
+}
+
+}  // namespace
+
+struct sbx_dense_plan {
+    sbx_ctx* ctx = nullptr;
+    sbx_dense_scene scene;
+    int* d_step = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int kernels_per_step = 0;
+};
+
+extern "C" sbx_status sbx_dense_step_unfused(sbx_ctx* ctx, const sbx_dense_scene* sc, int32_t t) {
+    if (!ctx || !sc) return SBX_EINVAL;
+    CHK(ensure_scratch(ctx, dense_scratch_bytes(sc)));
+    return dense_sequence(ctx, sc, nullptr, t);
+}
+
+extern "C" sbx_status sbx_dense_plan_create(sbx_ctx* ctx, const sbx_dense_scene* sc, sbx_dense_plan** out) {
+    if (!ctx || !sc || !out) return SBX_EINVAL;
+    *out = nullptr;
+    CHK(ensure_scratch(ctx, dense_scratch_bytes(sc)));
+    sbx_dense_plan* p = new sbx_dense_plan();
+    p->ctx = ctx;
+    p->scene = *sc;
+    if (cudaMalloc(&p->d_step, sizeof(int)) != cudaSuccess) {
+        delete p;
+        return fail(ctx, SBX_ENOMEM, "sbx_dense_plan_create: step word");
+    }
+    // capture one step into a graph
+    cudaStreamSynchronize(ctx->stream);
+    int64_t l0 = ctx->launches;
+    if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaFree(p->d_step);
+        delete p;
+        return fail(ctx, SBX_ECUDA, "sbx_dense_plan_create: begin capture");
+    }
+    sbx_status st = dense_sequence(ctx, &p->scene, p->d_step, 0);
+    if (st == SBX_OK) SBX_LAUNCH(ctx, k_step_advance, 1, 1, p->d_step);
+    cudaError_t ce = cudaStreamEndCapture(ctx->stream, &p->graph);
+    if (st != SBX_OK || ce != cudaSuccess) {
+        if (p->graph) cudaGraphDestroy(p->graph);
+        cudaFree(p->d_step);
+        delete p;
+        cudaGetLastError();
+        return st != SBX_OK ? st : fail(ctx, SBX_ECUDA, std::string("end capture: ") + cudaGetErrorString(ce));
+    }
+    p->kernels_per_step = (int)(ctx->launches - l0);
+    ctx->launches = l0;
+    if (cudaGraphInstantiate(&p->exec, p->graph, 0) != cudaSuccess) {
+        cudaGraphDestroy(p->graph);
+        cudaFree(p->d_step);
+        delete p;
+        return fail(ctx, SBX_ECUDA, "sbx_dense_plan_create: instantiate");
+    }
+    *out = p;
+    return SBX_OK;
+}
+
+extern "C" sbx_status sbx_dense_plan_run(sbx_dense_plan* p, int32_t t0, int32_t nsteps, int32_t use_graph) {
+    if (!p || nsteps < 0) return SBX_EINVAL;
+    sbx_ctx* ctx = p->ctx;
+    if (use_graph) {
+        SBX_LAUNCH(ctx, k_step_set, 1, 1, p->d_step, t0);
+        for (int k = 0; k < nsteps; k++) {
+            if (cudaGraphLaunch(p->exec, ctx->stream) != cudaSuccess)
+                return fail(ctx, SBX_ECUDA, "sbx_dense_plan_run: graph launch");
+            ctx->launches += p->kernels_per_step;
+        }
+        return check_launch(ctx, "sbx_dense_plan_run");
+    }
+    for (int k = 0; k < nsteps; k++) CHK(dense_sequence(ctx, &p->scene, nullptr, t0 + k));
+    return SBX_OK;
+}
+
+extern "C" int32_t sbx_dense_plan_kernels_per_step(sbx_dense_plan* p) { return p ? p->kernels_per_step : -1; }
+
+extern "C" sbx_status sbx_dense_plan_overflow(sbx_dense_plan* p, int32_t* flags) {
+    if (!p || !flags) return SBX_EINVAL;
+    *flags = 0;
+    return SBX_OK;
+}
+
+extern "C" sbx_status sbx_dense_plan_destroy(sbx_dense_plan* p) {
+    if (!p) return SBX_EINVAL;
+    cudaStreamSynchronize(p->ctx->stream);
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    if (p->d_step) cudaFree(p->d_step);
+    delete p;
+    return SBX_OK;
+}

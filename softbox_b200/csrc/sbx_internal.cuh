@@ -1,0 +1,63 @@
+// sbx_internal.cuh — library-internal context, launch helpers and the counting sort.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/softbox_b200.h"
+
+struct sbx_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+    int64_t launches = 0;
+    void* scratch = nullptr;          // grow-only device scratch for scans / unordered scatters
+    size_t scratch_bytes = 0;
+    int* host_flag = nullptr;         // pinned word for device -> host status flags
+};
+
+sbx_status fail(sbx_ctx* ctx, sbx_status code, const std::string& msg);
+sbx_status check_launch(sbx_ctx* ctx, const char* what);
+sbx_status ensure_scratch(sbx_ctx* ctx, size_t bytes);
+sbx_status any_nonfinite(sbx_ctx* ctx, const float* a, int64_t n, bool* out);
+
+static inline int blocks(int64_t n, int bs = 256) {
+    int64_t b = (n + bs - 1) / bs;
+    return (int)(b > 0 ? b : 1);
+}
+
+#define SBX_REQUIRE(cond)                                                              \
+    do {                                                                               \
+        if (!(cond)) return fail(ctx, SBX_EINVAL, std::string(__func__) + ": invalid argument"); \
+    } while (0)
+
+#define SBX_LAUNCH(ctx, kernel, grid, block, ...)                       \
+    do {                                                                \
+        kernel<<<(grid), (block), 0, (ctx)->stream>>>(__VA_ARGS__);     \
+        (ctx)->launches++;                                              \
+    } while (0)
+
+// ---------------------------------------------------------------- counting sort
+// Stable counting sort of items [0, n) by key (keys < 0 are skipped) into row CSR form:
+// rowCount (atomic histogram, left equal to the row lengths), rowOffsets[0..nRows]
+// (exclusive scan over SCAN_CHUNK tiles with the tile sums in chunkSum, terminator
+// clamped to listCap), rowList (items in ascending index within each row).
+// n = min(*nDev, nBound) when useDevN (SpatialGrid reads S from counts[1]), else nBound.
+constexpr int SCAN_CHUNK = 512;
+
+struct CountingSort {
+    const int* keys;
+    const int* nDev;      // optional device pointer to the item count
+    int useDevN;          // read n from nDev[1] (the reference's counts[1] slot)
+    int nBound;
+    int nRows;
+    int* rowCount;
+    int* chunkSum;        // ceil(nRows/SCAN_CHUNK)+1 ints
+    int* rowOffsets;      // nRows+1
+    int* rowList;         // listCap
+    int listCap;
+    int* tmp;             // unordered scatter buffer, >= nBound ints
+};
+
+sbx_status counting_sort(sbx_ctx* ctx, const CountingSort& cs, const char* what);

@@ -1,0 +1,153 @@
+// sbx_sort.cu — the stable counting sort behind the spatial grid and every CSR-inverse.
+//
+// Replaces SpatialGrid.gridHistogram/gridScanLocal/gridScanChunks/gridScanAdd/
+// gridScatter (SpatialGrid.java:154-249) and CrossBridgeSystem.csrHistogram/csrScan/
+// csrScatter (CrossBridgeSystem.java:190-217), plus their chunk-matrix variants, with:
+//   1. atomic histogram of the keys (integer atomics: the counts are order-free);
+//   2. exclusive scan in SCAN_CHUNK = 512 tiles: per-tile block scan, one-block scan of
+//      the tile sums (chunkSum, with the grand total in chunkSum[numChunks]), tile add
+//      that also resets the counts to zero (the reference's write cursor);
+//   3. unordered atomic scatter into a scratch list;
+//   4. rank pass: each item's position inside its row = the number of row members with a
+//      smaller index, which reproduces the reference's ascending-index order exactly.
+// Results (offsets, lists, counts, chunkSum) equal the serial reference bit for bit.
+#include <cuda_runtime.h>
+
+#include "sbx_internal.cuh"
+
+namespace {
+
+__device__ __forceinline__ int item_count(const int* nDev, int useDevN, int nBound) {
+    if (!useDevN) return nBound;
+    int n = nDev[1];
+    return n < nBound ? n : nBound;
+}
+
+__global__ void k_cs_hist(const int* keys, const int* nDev, int useDevN, int nBound, int* rowCount) {
+    int n = item_count(nDev, useDevN, nBound);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int c = keys[i];
+        if (c >= 0) atomicAdd(&rowCount[c], 1);
+    }
+}
+
+// block-wide exclusive scan of one int per thread; returns the exclusive prefix, *total = sum
+template <int NT>
+__device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
+    __shared__ int warp_sums[NT / 32];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = (lane < NT / 32) ? warp_sums[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < NT / 32) warp_sums[lane] = w;
+    }
+    __syncthreads();
+    int warp_prefix = warp > 0 ? warp_sums[warp - 1] : 0;
+    *total = warp_sums[NT / 32 - 1];
+    __syncthreads();
+    return warp_prefix + x - v;
+}
+
+// SpatialGrid.gridScanLocal (SpatialGrid.java:166-184), one block per 512-row tile
+__global__ void __launch_bounds__(256) k_scan_local(const int* rowCount, int nRows, int* offsets, int* chunkSum) {
+    int base = blockIdx.x * SCAN_CHUNK;
+    int i0 = base + 2 * threadIdx.x, i1 = i0 + 1;
+    int v0 = i0 < nRows ? rowCount[i0] : 0;
+    int v1 = i1 < nRows ? rowCount[i1] : 0;
+    int total;
+    int ex = block_exclusive_scan<256>(v0 + v1, &total);
+    if (i0 < nRows) offsets[i0] = ex;
+    if (i1 < nRows) offsets[i1] = ex + v0;
+    if (threadIdx.x == 0) chunkSum[blockIdx.x] = total;
+}
+
+// SpatialGrid.gridScanChunks (SpatialGrid.java:188-200) as a one-block scan with carry
+__global__ void __launch_bounds__(1024) k_scan_chunks(int* chunkSum, int numChunks) {
+    int carry = 0;
+    for (int t0 = 0; t0 < numChunks; t0 += 1024) {
+        int idx = t0 + threadIdx.x;
+        int v = idx < numChunks ? chunkSum[idx] : 0;
+        int total;
+        int ex = block_exclusive_scan<1024>(v, &total);
+        if (idx < numChunks) chunkSum[idx] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0) chunkSum[numChunks] = carry;
+}
+
+// SpatialGrid.gridScanAdd (SpatialGrid.java:204-227)
+__global__ void __launch_bounds__(256) k_scan_add(int* offsets, int nRows, const int* chunkSum, int numChunks,
+                                                  int* rowCount, int listCap) {
+    int b = chunkSum[blockIdx.x];
+    int base = blockIdx.x * SCAN_CHUNK;
+    for (int k = threadIdx.x; k < SCAN_CHUNK; k += blockDim.x) {
+        int c = base + k;
+        if (c < nRows) {
+            offsets[c] += b;
+            rowCount[c] = 0;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        int total = chunkSum[numChunks];
+        offsets[nRows] = total < listCap ? total : listCap;
+    }
+}
+
+__global__ void k_cs_scatter(const int* keys, const int* nDev, int useDevN, int nBound, const int* offsets,
+                             int* rowCount, int* tmp) {
+    int n = item_count(nDev, useDevN, nBound);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int c = keys[i];
+        if (c < 0) continue;
+        tmp[offsets[c] + atomicAdd(&rowCount[c], 1)] = i;
+    }
+}
+
+__global__ void k_cs_rank(const int* keys, const int* nDev, int useDevN, int nBound, const int* offsets,
+                          const int* tmp, int* rowList, int listCap) {
+    int n = item_count(nDev, useDevN, nBound);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int c = keys[i];
+        if (c < 0) continue;
+        int start = offsets[c], end = offsets[c + 1];
+        int rank = 0;
+        for (int j = start; j < end; j++) rank += tmp[j] < i;
+        int pos = start + rank;
+        if (pos < listCap) rowList[pos] = i;
+    }
+}
+
+}  // namespace
+
+sbx_status counting_sort(sbx_ctx* ctx, const CountingSort& cs, const char* what) {
+    int numChunks = (cs.nRows + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    int itemBlocks = blocks(cs.nBound);
+    if (itemBlocks > 148 * 16) itemBlocks = 148 * 16;
+    if (cudaMemsetAsync(cs.rowCount, 0, sizeof(int) * (size_t)cs.nRows, ctx->stream) != cudaSuccess)
+        return fail(ctx, SBX_ECUDA, std::string(what) + ": memset");
+    if (cs.nBound > 0)
+        SBX_LAUNCH(ctx, k_cs_hist, itemBlocks, 256, cs.keys, cs.nDev, cs.useDevN, cs.nBound, cs.rowCount);
+    SBX_LAUNCH(ctx, k_scan_local, numChunks, 256, cs.rowCount, cs.nRows, cs.rowOffsets, cs.chunkSum);
+    SBX_LAUNCH(ctx, k_scan_chunks, 1, 1024, cs.chunkSum, numChunks);
+    SBX_LAUNCH(ctx, k_scan_add, numChunks, 256, cs.rowOffsets, cs.nRows, cs.chunkSum, numChunks, cs.rowCount,
+               cs.listCap);
+    if (cs.nBound > 0) {
+        SBX_LAUNCH(ctx, k_cs_scatter, itemBlocks, 256, cs.keys, cs.nDev, cs.useDevN, cs.nBound, cs.rowOffsets,
+                   cs.rowCount, cs.tmp);
+        SBX_LAUNCH(ctx, k_cs_rank, itemBlocks, 256, cs.keys, cs.nDev, cs.useDevN, cs.nBound, cs.rowOffsets, cs.tmp,
+                   cs.rowList, cs.listCap);
+    }
+    return check_launch(ctx, what);
+}

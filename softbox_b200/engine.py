@@ -1,0 +1,80 @@
+"""Device-resident networks: the public Python API over the fused step plans.
+
+    net = DenseNetwork(scenes.dense_contractile(scenes.C1))
+    net.run(t0=0, nsteps=100)          # CUDA-graph replay of the fused step
+    pose = net.pull("fil", "coord")    # UNDER_DEMAND host copy
+
+    rods = FreeRods(scenes.free_rods_box())
+    rods.run(0, 10000, noise="wang")   # one persistent launch, rods in registers
+"""
+import ctypes as C
+
+from . import device as D
+from .runtime import LIB, SbxError, default_context
+
+
+class DenseNetwork:
+    """A dense contractile network (DenseContractileHarness.Scene) living on the device."""
+
+    def __init__(self, host_scene, ctx=None, fp64_coords=False, device="cuda"):
+        self.ctx = ctx or default_context()
+        self.host = host_scene
+        self.dev = D.to_device({k: v for k, v in host_scene.items() if k != "cfg"}, device)
+        if fp64_coords:
+            for path in (("fil", "body"), ("mot", "body"), ("mini", "backbone")):
+                D.add_coord64(self.dev[path[0]][path[1]])
+        self.desc = D.dense_desc(self.dev)
+        self.plan = C.c_void_p()
+        st = LIB.sbx_dense_plan_create(self.ctx.h, C.byref(self.desc), C.byref(self.plan))
+        if st != 0:
+            raise SbxError(st, "sbx_dense_plan_create: " + self.ctx.last_error())
+
+    @property
+    def kernels_per_step(self):
+        return LIB.sbx_dense_plan_kernels_per_step(self.plan)
+
+    def run(self, t0, nsteps, graph=True):
+        st = LIB.sbx_dense_plan_run(self.plan, int(t0), int(nsteps), 1 if graph else 0)
+        if st != 0:
+            raise SbxError(st, "sbx_dense_plan_run: " + self.ctx.last_error())
+
+    def step_unfused(self, t):
+        self.ctx("sbx_dense_step_unfused", self.desc, int(t))
+
+    def pull(self, store, field=None, sub=None):
+        x = self.dev[store]
+        if sub is not None:
+            x = x[sub]
+        if field is not None:
+            x = x[field]
+        return D.to_host(x)
+
+    def close(self):
+        if self.plan:
+            LIB.sbx_dense_plan_destroy(self.plan)
+            self.plan = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class FreeRods:
+    """Free Brownian rods (DiffusionHarness Config T/R and the free-rod workload)."""
+
+    MODES = {"wang": 0, "philox": 1, "supplied": 2}
+
+    def __init__(self, host_store, ctx=None, fp64_coords=False, device="cuda"):
+        self.ctx = ctx or default_context()
+        self.dev = D.to_device(host_store, device)
+        if fp64_coords:
+            D.add_coord64(self.dev["body"])
+        self.desc = D.filament_desc(self.dev)
+
+    def run(self, t0, nsteps, noise="wang", philox_seed=0, supplied=None):
+        self.ctx("sbx_free_rods_run", self.desc, int(t0), int(nsteps), self.MODES[noise], int(philox_seed), supplied)
+
+    def pull(self, field):
+        return D.to_host(self.dev["body"][field])

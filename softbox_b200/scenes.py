@@ -151,6 +151,15 @@ def drag_run_filament(f, aeta):
         store_drag(b, i, rod_drag_si(as_if, ACTIN_RADIUS, aeta))
 
 
+def rescale_viscosity(b, r):
+    """DenseContractileHarness.CrosslinkerBundleHarnessAeta (DenseContractileHarness.java:284-290):
+    gamma *= r and D /= r, each as (float)((double)value op r)."""
+    for k in ("bTransGam", "bRotGam"):
+        b[k][:] = (b[k].astype(np.float64) * r).astype(F32)
+    for k in ("bTransDiff", "bRotDiff"):
+        b[k][:] = (b[k].astype(np.float64) / r).astype(F32)
+
+
 def set_chain_params(f, dt, frac_move=0.5, frac_r=0.1, frac_move_torq=0.265, spring_active=0.0,
                      spring=1.0e-20):
     """FilamentStore.setChainParams (FilamentStore.java:345-353)."""
@@ -260,7 +269,8 @@ class DenseConfig:
     side: float = 20.0
     box_z: float = 0.5
     dt: float = 1.0e-5
-    aeta: float = 1.0e-3
+    aeta: float = 0.1               # Constants.aeta: motors, backbones, and the filament base drag
+    fil_aeta: float = 1.0           # DenseContractileHarness.AETA: filament drag rescaled to it
     myo_col_tol: float = 0.030
     align_tol: float = -0.4
     k_off: float = 20.0
@@ -288,7 +298,10 @@ class DenseConfig:
 
 # The dense contractile network of the benchmark: 2,000 filaments x 10 rods of 0.1 um,
 # 200 minifilaments (0.8 um backbone, 16 heads per end), 4,000 crosslinkers, 20x20x0.5 um
-# slab with walls, water viscosity, dt = 10 us.
+# slab with walls, dt = 10 us. Viscosities are the reference dense harness's: filaments in
+# the crowded-cytoplasm 1.0 Pa s, myosin bodies at Constants.aeta = 0.1 Pa s (with water,
+# the crosslinkers' explicit 1e-19 N m/rad torsion spring turns a 0.1 um rod by about twice
+# its misalignment per 10 us step, an unstable explicit update).
 C1 = DenseConfig()
 
 
@@ -393,6 +406,8 @@ def dense_contractile(cfg: DenseConfig = C1):
                 f["end1NbrSlot"][g] = g - 1
                 f["end1NbrSide"][g] = 1
     drag_run_filament(f, cfg.aeta)
+    if cfg.fil_aeta != cfg.aeta:
+        rescale_viscosity(fb, cfg.fil_aeta / cfg.aeta)
     f["params"][:] = np.array([dt, math.sqrt(2.0 * KT / dt)], F32)
     f["counts"][:] = np.array([n_seg, 0, cfg.seed_fil, 1], I32)
     f["chainParams"][:] = np.array([dt, cfg.chain_frac_move, cfg.chain_frac_r, cfg.chain_frac_move_torq,
