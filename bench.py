@@ -1,0 +1,330 @@
+"""Benchmark: rod-steps/s of the dense contractile network on B200.
+
+Workload (one step = one DenseContractileHarness.cpuStep of the whole network):
+2,000 filaments x 10 rigid rods of 0.1 um (20,000 rods), 200 minifilaments with a 0.8 um
+backbone and 16 heads per end (6,400 heads, 19,200 myosin sub-bodies), 4,000
+crosslinkers (Bell unbinding on), 20 x 20 x 0.5 um slab with confining walls, dt = 10 us,
+forces FP32, rod centres accumulated in FP64. Synthetic seeded scene (the reference's
+scene builder with these counts); no dataset.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm: each step is one launch of the fused persistent kernel; timed with CUDA events
+on the library's stream, one step at a time, with L2 flushed (a 256 MiB write) between
+timed steps. The reference arm times the reference's CPU path: the C++ restatement of
+the Java System classes (oracle/), on all host threads, on the same workload.
+Multi-GPU: one process per GPU (torchrun), each advancing its own independent network
+(replicas; the single network does not shard), value = all ranks' rod-steps / max time.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "rod-steps/s"
+WORKLOAD = ("dense contractile network: 2000 filaments x 10 rods of 0.1 um (20000 rods), 200 minifilaments "
+            "(0.8 um backbone, 16 heads/end: 6400 heads), 4000 crosslinkers, 20x20x0.5 um slab with walls, "
+            "dt 10 us, FP32 forces, FP64 rod centres")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# --------------------------------------------------------------------------- byte model
+def step_bytes(sc, fp64=True):
+    """Algorithmic bytes of one step: every array the step reads counted once at its stored
+    size, every array it writes counted once (the compulsory traffic of the step)."""
+    f, m, mini, xl, g = sc["fil"], sc["mot"], sc["mini"], sc["xl"], sc["grid"]
+    fb, mb, bb = f["body"], m["body"], mini["backbone"]
+    nb = lambda a: int(a.nbytes)
+    total = 0
+    for b in (fb, mb, bb):
+        rd = ["coord", "uVec", "yVec", "segLength", "bTransGam", "bRotGam", "brownTransScale", "brownRotScale"]
+        wr = ["coord", "uVec", "yVec", "zVec", "end1", "end2", "forceSum", "torqueSum", "randForce", "randTorque"]
+        total += sum(nb(b[k]) for k in rd) + sum(nb(b[k]) for k in wr)
+        if fp64:
+            total += 2 * 8 * b["coord"].size
+    total += sum(nb(f[k]) for k in ("end1NbrSlot", "end1NbrSide", "end2NbrSlot", "end2NbrSide"))
+    total += nb(fb["end1"]) + nb(fb["end2"])                      # read by binding and links
+    mot_rw = ["boundSeg", "bindArc", "stats", "capStats", "cooldown", "nucleotideState", "forceDotPlace",
+              "forceDotFil", "forceMag", "forceDotHist"]
+    total += 2 * sum(nb(m[k]) for k in mot_rw) + 3 * nb(m["head"]) + nb(m["reach"])
+    total += nb(sc["bondData"]) * 2 + nb(mini["miniData"]) * 2 + nb(mini["attachAxial"])
+    total += 2 * sum(nb(xl[k]) for k in ("linkState", "strainHist", "strainPlace", "torqueMagHist",
+                                          "torqueMagPlace", "xlinkData"))
+    total += sum(nb(xl[k]) for k in ("linkFilA", "linkFilB", "loc1", "loc2", "linkOrientSame"))
+    # grid + CSRs (written once, read once)
+    total += 2 * sum(nb(g[k]) for k in ("center", "boundingRadius", "ownerStore", "ownerSlot", "bodyCell",
+                                         "cellCount", "gridCellOffsets", "gridCellContents"))
+    total += 2 * (4 * m["nMotors"] * 4)                           # reach lists actually used (~4 per head)
+    for k in ("segCountA", "segOffsetsA", "segIdxA", "segCountB", "segOffsetsB", "segIdxB"):
+        total += 2 * nb(xl[k])
+    for k in ("segMotorCount", "segMotorOffsets", "segMotorMyo"):
+        total += 2 * nb(sc[k])
+    return total
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- CPU arm
+def cpu_oracle_rate(sc_host, steps, threads):
+    """rod-steps/s of the oracle (C++ restatement of the reference's Java System classes)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import copy
+    import oracle
+    from softbox_b200 import device as D
+    orc = oracle.get(devmath=False)
+    orc.set_threads(threads)
+    sc = copy.deepcopy(sc_host)
+    for s_, b_ in (("fil", "body"), ("mot", "body"), ("mini", "backbone")):
+        D.add_coord64(sc[s_][b_])
+    desc = D.dense_desc(sc)
+    orc.dense_run(desc, 0, 2)                      # warm
+    t0 = time.perf_counter()
+    orc.dense_run(desc, 2, steps)
+    dt = time.perf_counter() - t0
+    return sc["fil"]["body"]["n"] * steps / dt, dt
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from softbox_b200 import scenes
+    sc = scenes.dense_contractile(scenes.C1)
+    threads = os.cpu_count() or 1
+    rate, dt = cpu_oracle_rate(sc, max(1, args.warmup + args.steps), threads)
+    line = {"metric": METRIC, "value": rate, "unit": "rod-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sc["fil"]["body"]["n"] / rate, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 forces, f64 centres", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "parallelism": "host threads"}, "impl": "reference",
+            "cpu_baseline": {"value": rate, "unit": "rod-steps/s", "cores": threads, "kind": "port",
+                             "sample": f"{args.warmup + args.steps} full steps of the workload, "
+                                       f"{dt:.1f} s, C++ restatement of the Java System classes (no JVM on the box)"},
+            "e2e": {"value": rate, "unit": "rod-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- GPU arm
+def run_ours(args):
+    import torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    from softbox_b200 import scenes
+    from softbox_b200.engine import DenseNetwork
+    from softbox_b200.runtime import LIB, Context
+
+    ctx = Context(local)
+    sc_host = scenes.dense_contractile(scenes.C1)
+    net = DenseNetwork(sc_host, ctx=ctx, fp64_coords=True)
+    assert net.fused_available, "the benchmark network must qualify for the fused path"
+    stream = torch.cuda.ExternalStream(LIB.sbx_ctx_stream(ctx.h))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    nrods = sc_host["fil"]["body"]["n"]
+
+    def one_step(t):
+        net.run(t, 1, mode="fused")
+
+    t = 0
+    with torch.cuda.stream(stream):
+        for _ in range(max(3, args.warmup)):
+            flush.zero_()
+            one_step(t)
+            t += 1
+    torch.cuda.synchronize()
+    net.status()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        time.sleep(0.3)
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.zero_()
+                starts[k].record(stream)
+                one_step(t)
+                ends[k].record(stream)
+                t += 1
+        torch.cuda.synchronize()
+    net.status()
+    step_ms = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
+    total_ms = float(step_ms.sum())
+    if pg:
+        tt = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    value = ws * nrods * args.steps / (total_ms / 1e3)
+
+    # e2e through the C ABI: per step, H2D of the step's counts blocks (the reference's
+    # EVERY_EXECUTION upload: motor, backbone and filament counts, 3 x 16 B) from pinned
+    # memory, one fused step, D2H of the step's binding state (boundSeg) into pinned memory
+    d = net.dev
+    counts_host = torch.zeros(12, dtype=torch.int32).pin_memory()
+    bound_host = torch.empty(sc_host["mot"]["nMotors"], dtype=torch.int32).pin_memory()
+    cfg = sc_host["cfg"]
+    h2d = 3 * 16
+    d2h = bound_host.numel() * 4
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    e2e_steps = args.steps
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        c = counts_host.numpy()
+        c[:] = [sc_host["mot"]["nMotors"], t, cfg.seed, nrods, sc_host["mini"]["nBackbones"], t, cfg.seed_bb,
+                sc_host["mini"]["nBackbones"], nrods, t, cfg.seed_fil, 1]
+        for j, dst in enumerate((d["mot"]["counts"], d["mini"]["bbCounts"], d["fil"]["counts"])):
+            ctx("sbx_upload", C.c_void_p(dst.data_ptr()), C.c_void_p(counts_host.data_ptr() + 16 * j), 16)
+        st = LIB.sbx_dense_plan_run(net.plan, t, 1, 2)
+        assert st == 0, ctx.last_error()
+        ctx("sbx_download", C.c_void_p(bound_host.data_ptr()), C.c_void_p(d["mot"]["boundSeg"].data_ptr()), d2h)
+        t += 1
+    e2e_s = time.perf_counter() - t0
+    if pg:
+        tt = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e = ws * nrods * e2e_steps / e2e_s
+
+    # roofline of the dominant (only) kernel: the fused step
+    hbm, how = peaks()
+    bytes_step = step_bytes(sc_host, fp64=True)
+    achieved = bytes_step / (float(np.mean(step_ms)) / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "fused_step_traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        rate, dt = cpu_oracle_rate(sc_host, args.cpu_steps, 1)
+        cpu = {"value": rate, "unit": "rod-steps/s", "cores": 1, "kind": "port",
+               "sample": f"{args.cpu_steps} full steps of the workload on 1 host core ({dt:.1f} s), C++ "
+                         f"restatement of the Java System classes' single-threaded -cpu runner"}
+    clocks = clk.summary()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "rod-steps/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32 forces, f64 centres", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "rods": nrods, "heads": sc_host["mot"]["nMotors"],
+                           "crosslinks": sc_host["xl"]["nLinks"], "parallelism": f"replicas x{ws}",
+                           "l2": "flushed between timed steps (256 MiB write)",
+                           "path": "fused persistent cooperative kernel, 1 launch per step",
+                           "grid_ctas": net.fused_grid},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                             "frac": achieved / hbm, "traffic": traffic, "peak_source": how,
+                             "kernel": "k_dense_fused", "algorithmic_bytes_per_launch": bytes_step},
+                "cpu_baseline": cpu,
+                "e2e": {"value": e2e, "unit": "rod-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "gpu_launches": args.steps,
+                "clocks": clocks,
+                "step_ms_median": float(np.median(step_ms)), "step_ms_p90": float(np.percentile(step_ms, 90))}
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=600)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

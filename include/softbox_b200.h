@@ -388,14 +388,32 @@ typedef struct sbx_dense_plan sbx_dense_plan;
  * the DenseContractileHarness.cpuStep order. */
 sbx_status sbx_dense_plan_create(sbx_ctx* ctx, const sbx_dense_scene* scene, sbx_dense_plan** out);
 /* Advances steps t0, t0+1, ..., t0+nsteps-1 (the step index feeds every RNG key and
- * the containment cadence). use_graph != 0 replays a captured CUDA graph per step. */
-sbx_status sbx_dense_plan_run(sbx_dense_plan* plan, int32_t t0, int32_t nsteps, int32_t use_graph);
+ * the containment cadence). mode 0: the per-system call sequence; 1: one CUDA-graph
+ * replay per step of that sequence; 2: the fused persistent kernel (all nsteps in one
+ * cooperative launch; available when the scene has the harness layout, see
+ * sbx_dense_plan_fused_available). All three give the same bits. */
+sbx_status sbx_dense_plan_run(sbx_dense_plan* plan, int32_t t0, int32_t nsteps, int32_t mode);
 /* Runs one step as the unfused per-system call sequence (reference granularity). */
 sbx_status sbx_dense_step_unfused(sbx_ctx* ctx, const sbx_dense_scene* scene, int32_t t);
 /* Number of kernels one fused step launches. */
 int32_t sbx_dense_plan_kernels_per_step(sbx_dense_plan* plan);
-/* Overflow flags raised since the last call (bit0: reach list > MAX_CAND); clears them. */
-sbx_status sbx_dense_plan_overflow(sbx_dense_plan* plan, int32_t* flags);
+/* Synchronises and reports the fused path's flags for the last run: bit0 a grid-barrier
+ * wait ran out (SBX_ETIMEOUT; the state of that run is partial), bit1 a reach list
+ * exceeded SBX_MAX_CAND (SBX_EOVERFLOW; counts continue past the cap, as the reference),
+ * bit2 a bulk-copy wait ran out (SBX_ETIMEOUT). */
+sbx_status sbx_dense_plan_status(sbx_dense_plan* plan, int32_t* flags);
+/* 1 when the fused persistent path is available for this scene (else mode 2 returns SBX_ESTATE) */
+int32_t sbx_dense_plan_fused_available(sbx_dense_plan* plan);
+/* cooperative grid size (CTAs) of the fused path */
+int32_t sbx_dense_plan_fused_grid(sbx_dense_plan* plan);
+/* Phase timing of the fused path: when dev_times (device int64 array of nsteps*11) is
+ * set, each run writes the %globaltimer value (ns) after every phase barrier of every
+ * step; NULL switches it off. */
+sbx_status sbx_dense_plan_phase_times(sbx_dense_plan* plan, int64_t* dev_times);
+/* Test hook for failure detection: the fused kernel's grid barrier waits for `extra`
+ * arrivals that never come, so its bounded wait runs out and the run reports
+ * SBX_ETIMEOUT. 0 restores normal operation. */
+sbx_status sbx_dense_plan_test_barrier_extra(sbx_dense_plan* plan, int32_t extra);
 sbx_status sbx_dense_plan_destroy(sbx_dense_plan* plan);
 
 /* Free rods (DiffusionHarness cpuStepFdt order: brownian -> integrate -> derive).

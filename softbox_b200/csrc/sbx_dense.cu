@@ -11,8 +11,11 @@
 #include <algorithm>
 
 #include "../../include/softbox_b200.h"
+#include "sbx_fused.cuh"
 #include "sbx_internal.cuh"
 #include "sbx_physics.cuh"
+
+#include <vector>
 
 using namespace sbx;
 
@@ -158,7 +161,116 @@ struct sbx_dense_plan {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int kernels_per_step = 0;
+    // fused persistent path
+    bool fused_ok = false;
+    bool fused_dirty = true;     // scratch must be (re)initialised before the next fused run
+    std::string fused_why;
+    FusedArgs fa{};
+    int fused_grid = 0;
+    std::vector<void*> allocs;
 };
+
+namespace {
+
+template <class T>
+std::vector<T> d2h(const T* d, size_t n, cudaStream_t s) {
+    std::vector<T> h(n);
+    if (n) cudaMemcpyAsync(h.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    return h;
+}
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+// Checks that the scene has the harness's structure the fused kernel relies on and fills
+// the kernel arguments; on failure records why (the graph path remains available).
+bool fused_prepare(sbx_dense_plan* p) {
+    const sbx_dense_scene& sc = p->scene;
+    cudaStream_t st = p->ctx->stream;
+    FusedArgs& a = p->fa;
+    a.sc = sc;
+    a.nSeg = sc.fil.body.n; a.nM = sc.mot.nMotors; a.nB = sc.mot.body.n; a.nBb = sc.mini.backbone.n;
+    a.nD = sc.dim.nDimers; a.nL = sc.xl.nLinks; a.cap = sc.grid.cap; a.C = sc.grid.totalCells;
+    a.xlOn = (sc.xlinkOn && sc.xl.nLinks > 0) ? 1 : 0;
+    a.xlUnbind = sc.xlUnbind ? 1 : 0;
+    auto why = [&](const char* w) { p->fused_why = w; return false; };
+    if (a.nSeg <= 0 || a.nM <= 0 || a.nBb <= 0) return why("empty stores");
+    if (a.nB != 3 * a.nM || a.nM != 2 * a.nD || sc.mini.nDimers != a.nD) return why("motor/dimer counts");
+    if (a.nD % a.nBb) return why("dimers per backbone not uniform");
+    a.dpm = a.nD / a.nBb;
+    if (6 * a.dpm > FUSED_MAX_SUB || 2 * a.dpm > 32) return why("too many dimers per backbone");
+    auto mA = d2h(sc.dim.motorA, a.nD, st), mB = d2h(sc.dim.motorB, a.nD, st);
+    auto hbs = d2h(sc.mini.headBackboneSlot, a.nD, st), mmA = d2h(sc.mini.motorA, a.nD, st);
+    for (int d = 0; d < a.nD; d++)
+        if (mA[d] != 2 * d || mB[d] != 2 * d + 1 || hbs[d] != d / a.dpm || mmA[d] != 2 * d)
+            return why("dimer/minifilament topology is not the harness layout");
+    auto pub = d2h(sc.mot.publishParams, 1, st);
+    if (pub[0] != a.nSeg || a.cap < a.nSeg + a.nM) return why("body-view layout");
+    auto gc = d2h(sc.grid.gridCounts, 4, st);
+    a.S = gc[1];
+    if (a.S < 0 || a.S > a.cap) return why("grid counts");
+    auto gd = d2h(sc.grid.gridDims, 4, st);
+    a.nX = gd[0]; a.nY = gd[1]; a.nZ = gd[2];
+    if (gd[3] != a.C || (long long)a.nX * a.nY * a.nZ != a.C) return why("grid dims");
+    // chain topology: filaments must be contiguous slot ranges; pick the largest group
+    // of whole filaments (<= FUSED_MAX_ROD, a multiple of 4 segments)
+    auto e1 = d2h(sc.fil.end1NbrSlot, a.nSeg, st), e2 = d2h(sc.fil.end2NbrSlot, a.nSeg, st);
+    std::vector<int> lo(a.nSeg), hi(a.nSeg);
+    for (int i = 0; i < a.nSeg; i++) {
+        lo[i] = i; hi[i] = i;
+        int nb[2] = {e1[i], e2[i]};
+        for (int j : nb) {
+            if (j < -1 || j >= a.nSeg) return why("neighbour slot out of range");
+            if (j >= 0) { lo[i] = std::min(lo[i], j); hi[i] = std::max(hi[i], j); }
+        }
+    }
+    a.G = 0;
+    for (int G = FUSED_MAX_ROD - FUSED_MAX_ROD % 4; G >= 4 && !a.G; G -= 4) {
+        bool ok = true;
+        for (int i = 0; i < a.nSeg && ok; i++) ok = (lo[i] / G == i / G) && (hi[i] / G == i / G);
+        if (ok) a.G = G;
+    }
+    if (!a.G) return why("chain neighbours cross every segment grouping");
+    a.nRodUnits = (a.nSeg + a.G - 1) / a.G;
+    a.tilesC = (a.C + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    a.tilesS = (a.nSeg + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    auto fc = d2h(sc.fil.counts, 4, st);
+    a.filSeed = fc[2];
+    const sbx_rigid_body& fb = sc.fil.body;
+    a.useTma = (a.nSeg % 4 == 0) && (a.G % 4 == 0) && aligned16(fb.coord) && aligned16(fb.uVec) &&
+               aligned16(fb.segLength) && aligned16(fb.bTransGam) && aligned16(fb.bRotGam);
+    // plan-owned scratch
+    auto alloc = [&](size_t bytes) -> void* {
+        void* q = nullptr;
+        if (cudaMalloc(&q, bytes ? bytes : 4) != cudaSuccess) return nullptr;
+        p->allocs.push_back(q);
+        return q;
+    };
+    size_t nS = a.nSeg;
+    a.cntCell = (int*)alloc(4 * (size_t)a.C);
+    a.cntAct = (int*)alloc(4 * nS); a.cntA = (int*)alloc(4 * nS); a.cntB = (int*)alloc(4 * nS);
+    a.cntM = (int*)alloc(4 * nS);
+    a.tileSum = (int*)alloc(4 * (size_t)(a.tilesC + 2 * a.tilesS + 1));
+    a.tmpCell = (int*)alloc(4 * (size_t)a.cap);
+    a.tmpA = (int*)alloc(4 * (size_t)std::max(a.nL, 1)); a.tmpB = (int*)alloc(4 * (size_t)std::max(a.nL, 1));
+    a.tmpM = (int*)alloc(4 * (size_t)a.nM);
+    a.sortedE1 = (float4*)alloc(16 * (size_t)a.cap); a.sortedE2 = (float4*)alloc(16 * (size_t)a.cap);
+    a.bar = (unsigned*)alloc(16);
+    a.err = (int*)alloc(16);
+    a.d_step = p->d_step;
+    for (void* q : p->allocs)
+        if (!q) return why("scratch allocation failed");
+    int dev = 0, sms = 0, coop = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    int per = fused_max_blocks_per_sm();
+    if (!coop || per <= 0) return why("cooperative launch unavailable");
+    p->fused_grid = sms * per;
+    return true;
+}
+
+}  // namespace
 
 extern "C" sbx_status sbx_dense_step_unfused(sbx_ctx* ctx, const sbx_dense_scene* sc, int32_t t) {
     if (!ctx || !sc) return SBX_EINVAL;
@@ -203,14 +315,31 @@ extern "C" sbx_status sbx_dense_plan_create(sbx_ctx* ctx, const sbx_dense_scene*
         delete p;
         return fail(ctx, SBX_ECUDA, "sbx_dense_plan_create: instantiate");
     }
+    p->fused_ok = fused_prepare(p);
+    cudaGetLastError();
     *out = p;
     return SBX_OK;
 }
 
-extern "C" sbx_status sbx_dense_plan_run(sbx_dense_plan* p, int32_t t0, int32_t nsteps, int32_t use_graph) {
-    if (!p || nsteps < 0) return SBX_EINVAL;
+extern "C" sbx_status sbx_dense_plan_run(sbx_dense_plan* p, int32_t t0, int32_t nsteps, int32_t mode) {
+    if (!p || nsteps < 0 || mode < 0 || mode > 2) return SBX_EINVAL;
     sbx_ctx* ctx = p->ctx;
-    if (use_graph) {
+    if (nsteps == 0) return SBX_OK;
+    if (mode == 2) {
+        if (!p->fused_ok) return fail(ctx, SBX_ESTATE, "fused path unavailable: " + p->fused_why);
+        // the kernel leaves its histograms zeroed and its barrier words consistent at the
+        // end of every completed run; they are reset here only after a failed run
+        if (p->fused_dirty) {
+            FusedArgs& a = p->fa;
+            cudaMemsetAsync(a.cntCell, 0, 4 * (size_t)a.C, ctx->stream);
+            for (int* q : {a.cntAct, a.cntA, a.cntB, a.cntM}) cudaMemsetAsync(q, 0, 4 * (size_t)a.nSeg, ctx->stream);
+            cudaMemsetAsync(a.bar, 0, 16, ctx->stream);
+            cudaMemsetAsync(a.err, 0, 16, ctx->stream);
+            p->fused_dirty = false;
+        }
+        return fused_launch(ctx, p->fa, p->fused_grid, t0, nsteps);
+    }
+    if (mode == 1) {
         SBX_LAUNCH(ctx, k_step_set, 1, 1, p->d_step, t0);
         for (int k = 0; k < nsteps; k++) {
             if (cudaGraphLaunch(p->exec, ctx->stream) != cudaSuccess)
@@ -225,9 +354,35 @@ extern "C" sbx_status sbx_dense_plan_run(sbx_dense_plan* p, int32_t t0, int32_t 
 
 extern "C" int32_t sbx_dense_plan_kernels_per_step(sbx_dense_plan* p) { return p ? p->kernels_per_step : -1; }
 
-extern "C" sbx_status sbx_dense_plan_overflow(sbx_dense_plan* p, int32_t* flags) {
+extern "C" sbx_status sbx_dense_plan_status(sbx_dense_plan* p, int32_t* flags) {
     if (!p || !flags) return SBX_EINVAL;
     *flags = 0;
+    if (!p->fused_ok) return SBX_OK;
+    int h = 0;
+    cudaMemcpyAsync(&h, p->fa.err, sizeof(int), cudaMemcpyDeviceToHost, p->ctx->stream);
+    CHK(sbx_ctx_sync(p->ctx));
+    *flags = h;
+    if (h) p->fused_dirty = true;
+    if (h & 1) return fail(p->ctx, SBX_ETIMEOUT, "fused step: grid barrier wait ran out");
+    if (h & 4) return fail(p->ctx, SBX_ETIMEOUT, "fused step: bulk-copy wait ran out");
+    if (h & 2) return fail(p->ctx, SBX_EOVERFLOW, "fused step: a reach list exceeded SBX_MAX_CAND");
+    return SBX_OK;
+}
+
+extern "C" int32_t sbx_dense_plan_fused_available(sbx_dense_plan* p) { return p && p->fused_ok ? 1 : 0; }
+
+extern "C" int32_t sbx_dense_plan_fused_grid(sbx_dense_plan* p) { return p ? p->fused_grid : 0; }
+
+extern "C" sbx_status sbx_dense_plan_phase_times(sbx_dense_plan* p, int64_t* dev_times) {
+    if (!p) return SBX_EINVAL;
+    p->fa.phaseTimes = (long long*)dev_times;
+    return SBX_OK;
+}
+
+extern "C" sbx_status sbx_dense_plan_test_barrier_extra(sbx_dense_plan* p, int32_t extra) {
+    if (!p || extra < 0) return SBX_EINVAL;
+    p->fa.barrierExtra = extra;
+    p->fused_dirty = true;
     return SBX_OK;
 }
 
@@ -237,6 +392,7 @@ extern "C" sbx_status sbx_dense_plan_destroy(sbx_dense_plan* p) {
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
     if (p->d_step) cudaFree(p->d_step);
+    for (void* q : p->allocs) cudaFree(q);
     delete p;
     return SBX_OK;
 }

@@ -1,0 +1,722 @@
+// sbx_fused.cu — the dense contractile step as ONE persistent cooperative kernel.
+//
+// A launch advances nsteps steps. Within a step, phases are separated by a grid-wide
+// barrier (bounded spin: a barrier that does not complete within the limit raises
+// error bit 0 and every CTA returns, so a fault cannot hang the device):
+//
+//   A  publish the body view (FilamentStore/MotorStore.publish*), bin bodies
+//      (SpatialGrid.bodyCell) + atomic cell histogram; crosslinker Bell unbind and the
+//      active-link / CSR-key histograms
+//   B  tile sums of the three histograms (cells, link A keys, link B keys)
+//   C  exclusive scans -> gridCellOffsets / segOffsetsA / segOffsetsB / chunkSum
+//   D  unordered atomic scatter into scratch lists
+//   E  rank pass -> stable gridCellContents / segIdxA / segIdxB, plus cell-sorted
+//      float4 copies of the segment endpoints for the reach walk
+//   F  one CTA per minifilament: reach walk, release, bind, nucleotide cycle for its 32
+//      heads, then Brownian, joints, dimer coupling, tether, backbone gather, cross-
+//      bridge bonds, integrate + derive of its 96 sub-bodies and backbone, force-dot
+//      registry — all sub-body force sums kept in shared memory; other CTAs compute
+//      crosslinker forces + torsion
+//   G  motor->segment histogram tile sums; filament Brownian forcing
+//   H  motor CSR scan -> segMotorOffsets
+//   I  motor scatter
+//   J  motor rank -> segMotorMyo
+//   K  one CTA per group of whole filaments, poses staged in shared memory with TMA
+//      bulk copies: chain forces, crosslinker A/B gathers, motor gather (CSR order, FP64
+//      sums), containment, integrate + derive
+//
+// Every slot is computed by the same device functions as the per-system kernels, in the
+// reference's accumulation order, so the result is bit-identical to
+// DenseContractileHarness.cpuStep (DenseContractileHarness.java:350-429).
+#include <cuda_runtime.h>
+
+#include "../../include/softbox_b200.h"
+#include "sbx_fused.cuh"
+#include "sbx_internal.cuh"
+#include "sbx_physics.cuh"
+
+using namespace sbx;
+
+namespace {
+
+constexpr long long SPIN_LIMIT = 1LL << 24;    // x ~64 ns sleeps: about one second
+constexpr int ERR_BARRIER = 1, ERR_REACH_OVERFLOW = 2, ERR_TMA = 4;
+
+__device__ __forceinline__ int vload(const int* p) { return *(const volatile int*)p; }
+
+// Grid barrier (the cooperative-groups pattern: block barrier, one thread per CTA
+// publishes with a device fence, waits on a generation word, fences again).
+__device__ bool grid_sync(const FusedArgs& a) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = a.bar + 1;
+        unsigned g = *gen;
+        __threadfence();
+        unsigned arrived = atomicAdd(a.bar, 1u);
+        if (arrived == gridDim.x - 1 + (unsigned)a.barrierExtra) {
+            a.bar[0] = 0;
+            __threadfence();
+            atomicAdd(a.bar + 1, 1u);
+        } else {
+            long long it = 0;
+            while (*gen == g) {
+                if (vload(a.err) & ERR_BARRIER) break;
+                if (++it > SPIN_LIMIT) {
+                    atomicOr(a.err, ERR_BARRIER);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = (vload(a.err) & ERR_BARRIER) == 0;
+    }
+    __syncthreads();
+    return s_ok;
+}
+
+__device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ int gthreads() { return gridDim.x * blockDim.x; }
+
+// ---------------------------------------------------------------- phase A
+__device__ void phase_publish_bin(const FusedArgs& a, int t) {
+    const sbx_dense_scene& sc = a.sc;
+    const sbx_grid_state& g = sc.grid;
+    const sbx_rigid_body& fb = sc.fil.body;
+    const sbx_rigid_body& mb = sc.mot.body;
+    const sbx_crosslinker_store& xl = sc.xl;
+    const int nSeg = a.nSeg, nM = a.nM, nB = a.nB, cap = a.cap;
+    const float* gp = g.gridParams;
+    const int nX = a.nX, nY = a.nY, nZ = a.nZ;
+    const int total = cap + (a.xlOn ? a.nL : 0);
+    for (int i = gtid(); i < total; i += gthreads()) {
+        if (i < nSeg) {
+            float c[3] = {fb.coord[i], fb.coord[nSeg + i], fb.coord[2 * nSeg + i]};
+            g.center[i] = c[0]; g.center[cap + i] = c[1]; g.center[2 * cap + i] = c[2];
+            g.boundingRadius[i] = 0.5f * fb.segLength[i] + g.viewParams[0];
+            g.ownerStore[i] = STORE_FILAMENT;
+            g.ownerSlot[i] = i;
+            if (i < a.S) {
+                int cell = cell_coord(c[0], gp[0], gp[4], nX) + cell_coord(c[1], gp[1], gp[4], nY) * nX +
+                           cell_coord(c[2], gp[2], gp[4], nZ) * (nX * nY);
+                g.bodyCell[i] = cell;
+                atomicAdd(&a.cntCell[cell], 1);
+            } else {
+                g.bodyCell[i] = -1;
+            }
+        } else if (i < nSeg + nM) {
+            int m = i - nSeg, h = 3 * m + 2, r = 3 * m;
+            float hl = mb.segLength[h];
+            float hd[3];
+            for (int k = 0; k < 3; k++) {
+                hd[k] = mb.coord[k * nB + h] + 0.5f * hl * mb.uVec[k * nB + h];
+                sc.mot.head[k * nM + m] = hd[k];
+                sc.mot.uVec[k * nM + m] = mb.uVec[k * nB + h];
+                sc.mot.rodUVec[k * nM + m] = mb.uVec[k * nB + r];
+            }
+            int b = i;   // base slot == nSeg (checked at plan creation)
+            g.center[b] = hd[0]; g.center[cap + b] = hd[1]; g.center[2 * cap + b] = hd[2];
+            g.boundingRadius[b] = sc.mot.reach[m];
+            g.ownerStore[b] = STORE_MOTOR;
+            g.ownerSlot[b] = m;
+            if (b < a.S) {
+                int cell = cell_coord(hd[0], gp[0], gp[4], nX) + cell_coord(hd[1], gp[1], gp[4], nY) * nX +
+                           cell_coord(hd[2], gp[2], gp[4], nZ) * (nX * nY);
+                g.bodyCell[b] = cell;
+                atomicAdd(&a.cntCell[cell], 1);
+            } else {
+                g.bodyCell[b] = -1;
+            }
+        } else if (i < cap) {
+            g.bodyCell[i] = -1;
+        } else {
+            int k = i - cap;
+            int la = xl.linkFilA[k], lb = xl.linkFilB[k];
+            int state = xl.linkState[k];
+            if (a.xlUnbind && state >= 0 &&
+                unbind_one(k, nSeg, fb.uVec, fb.end1, la, lb, xl.loc1[k], xl.loc2[k], xl.strainHist, xl.strainPlace,
+                           xl.offParams, t, sc.seed)) {
+                state = LINK_FREE;
+                xl.linkState[k] = state;
+            }
+            if (state >= 0) {
+                atomicAdd(&a.cntAct[la], 1);
+                atomicAdd(&a.cntAct[lb], 1);
+            }
+            if (la >= 0) atomicAdd(&a.cntA[la], 1);
+            if (lb >= 0) atomicAdd(&a.cntB[lb], 1);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- scans (B, C, G, H)
+struct ScanArr {
+    const int* cnt;   // histogram
+    int n;            // rows
+    int tile0;        // first tile index in the shared tile-sum array
+};
+
+__device__ __forceinline__ int warp_sum(int v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ void tile_sums(const ScanArr* arrs, int narr, int* tileSum) {
+    int lane = threadIdx.x & 31;
+    int warp = gtid() >> 5, nwarps = gthreads() >> 5;
+    int total = arrs[narr - 1].tile0 + (arrs[narr - 1].n + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    for (int tl = warp; tl < total; tl += nwarps) {
+        int ai = 0;
+        while (ai + 1 < narr && tl >= arrs[ai + 1].tile0) ai++;
+        const ScanArr& s = arrs[ai];
+        int base = (tl - s.tile0) * SCAN_CHUNK;
+        int v = 0;
+        for (int j = lane; j < SCAN_CHUNK; j += 32) v += (base + j < s.n) ? s.cnt[base + j] : 0;
+        v = warp_sum(v);
+        if (lane == 0) tileSum[tl] = v;
+    }
+}
+
+// exclusive scan of each array into out[ai][0..n] (terminator = min(total, clamp[ai])),
+// zeroing zero[ai][...] (the write cursors); chunkOut (optional, array 0) gets the
+// tile-prefix layout of SpatialGrid.gridScanChunks.
+__device__ void tile_scan(const ScanArr* arrs, int narr, const int* tileSum, int* const* out, int* const* zero,
+                          const int* clampTotal, int* chunkOut) {
+    int lane = threadIdx.x & 31;
+    int warp = gtid() >> 5, nwarps = gthreads() >> 5;
+    int total = arrs[narr - 1].tile0 + (arrs[narr - 1].n + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    for (int tl = warp; tl < total; tl += nwarps) {
+        int ai = 0;
+        while (ai + 1 < narr && tl >= arrs[ai + 1].tile0) ai++;
+        const ScanArr& s = arrs[ai];
+        int ntiles = (s.n + SCAN_CHUNK - 1) / SCAN_CHUNK;
+        int local = tl - s.tile0;
+        int b = 0;
+        for (int j = lane; j < local; j += 32) b += tileSum[s.tile0 + j];
+        b = warp_sum(b);
+        int base = local * SCAN_CHUNK;
+        constexpr int PER = SCAN_CHUNK / 32;
+        int vals[PER];
+        int lsum = 0;
+        for (int j = 0; j < PER; j++) {
+            int r = base + lane * PER + j;
+            vals[j] = r < s.n ? s.cnt[r] : 0;
+            lsum += vals[j];
+        }
+        int x = lsum;
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        int run = b + x - lsum;
+        for (int j = 0; j < PER; j++) {
+            int r = base + lane * PER + j;
+            if (r < s.n) {
+                out[ai][r] = run;
+                if (zero[ai]) zero[ai][r] = 0;
+            }
+            run += vals[j];
+        }
+        if (lane == 0 && ai == 0 && chunkOut) chunkOut[local] = b;
+        if (local == ntiles - 1) {
+            int tot = __shfl_sync(0xffffffffu, run, 31);
+            if (lane == 0) {
+                out[ai][s.n] = tot < clampTotal[ai] ? tot : clampTotal[ai];
+                if (ai == 0 && chunkOut) chunkOut[ntiles] = tot;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- D / E (grid + link CSRs)
+__device__ void phase_scatter(const FusedArgs& a) {
+    const sbx_dense_scene& sc = a.sc;
+    const sbx_grid_state& g = sc.grid;
+    const sbx_crosslinker_store& xl = sc.xl;
+    int total = a.cap + (a.xlOn ? a.nL : 0);
+    for (int i = gtid(); i < total; i += gthreads()) {
+        if (i < a.cap) {
+            int c = g.bodyCell[i];
+            if (c >= 0) a.tmpCell[g.gridCellOffsets[c] + atomicAdd(&g.cellCount[c], 1)] = i;
+        } else {
+            int k = i - a.cap;
+            int la = xl.linkFilA[k], lb = xl.linkFilB[k];
+            if (la >= 0) a.tmpA[xl.segOffsetsA[la] + atomicAdd(&xl.segCountA[la], 1)] = k;
+            if (lb >= 0) a.tmpB[xl.segOffsetsB[lb] + atomicAdd(&xl.segCountB[lb], 1)] = k;
+        }
+    }
+}
+
+__device__ __forceinline__ int rank_in(const int* tmp, int start, int end, int i) {
+    int r = 0;
+    for (int j = start; j < end; j++) r += tmp[j] < i;
+    return r;
+}
+
+__device__ void phase_rank(const FusedArgs& a) {
+    const sbx_dense_scene& sc = a.sc;
+    const sbx_grid_state& g = sc.grid;
+    const sbx_crosslinker_store& xl = sc.xl;
+    const sbx_rigid_body& fb = sc.fil.body;
+    const int nSeg = a.nSeg;
+    int total = a.cap + (a.xlOn ? a.nL : 0);
+    for (int i = gtid(); i < total; i += gthreads()) {
+        if (i < a.cap) {
+            int c = g.bodyCell[i];
+            if (c < 0) continue;
+            int s0 = g.gridCellOffsets[c], s1 = g.gridCellOffsets[c + 1];
+            int pos = s0 + rank_in(a.tmpCell, s0, s1, i);
+            g.gridCellContents[pos] = i;
+            // cell-sorted endpoint copy for the reach walk (w = segment slot, -1 = not a segment)
+            float4 e1, e2;
+            if (i < nSeg) {
+                e1 = make_float4(fb.end1[i], fb.end1[nSeg + i], fb.end1[2 * nSeg + i], __int_as_float(i));
+                e2 = make_float4(fb.end2[i], fb.end2[nSeg + i], fb.end2[2 * nSeg + i], 0.f);
+            } else {
+                e1 = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+                e2 = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            a.sortedE1[pos] = e1;
+            a.sortedE2[pos] = e2;
+        } else {
+            int k = i - a.cap;
+            int la = xl.linkFilA[k], lb = xl.linkFilB[k];
+            if (la >= 0) {
+                int s0 = xl.segOffsetsA[la], s1 = xl.segOffsetsA[la + 1];
+                xl.segIdxA[s0 + rank_in(a.tmpA, s0, s1, k)] = k;
+            }
+            if (lb >= 0) {
+                int s0 = xl.segOffsetsB[lb], s1 = xl.segOffsetsB[lb + 1];
+                xl.segIdxB[s0 + rank_in(a.tmpB, s0, s1, k)] = k;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- F: minifilaments + links
+// BindingDetectionSystem.gridReachable over the cell-sorted float4 endpoints: the same
+// 27 cells, the same order, the same predicate as grid_reach_walk.
+__device__ int reach_walk_sorted(const FusedArgs& a, int m, float mx, float my, float mz, float mux, float muy,
+                                 float muz, float rux, float ruy, float ruz, int* out, float tol, float align) {
+    const float* gp = a.sc.grid.gridParams;
+    const int* off = a.sc.grid.gridCellOffsets;
+    int nX = a.nX, nY = a.nY, nZ = a.nZ, nXY = nX * nY;
+    int cx = cell_coord(mx, gp[0], gp[4], nX), cy = cell_coord(my, gp[1], gp[4], nY),
+        cz = cell_coord(mz, gp[2], gp[4], nZ);
+    int x0 = max(cx - 1, 0), x1 = min(cx + 1, nX - 1);
+    int y0 = max(cy - 1, 0), y1 = min(cy + 1, nY - 1);
+    int z0 = max(cz - 1, 0), z1 = min(cz + 1, nZ - 1);
+    int cnt = 0;
+    for (int zz = z0; zz <= z1; zz++)
+        for (int yy = y0; yy <= y1; yy++) {
+            // cells x0..x1 of one row are consecutive: one contiguous CSR range
+            int c0 = x0 + yy * nX + zz * nXY;
+            int start = off[c0], end = off[c0 + (x1 - x0) + 1];
+            for (int idx = start; idx < end; idx++) {
+                float4 e1 = a.sortedE1[idx];
+                int s = __float_as_int(e1.w);
+                if (s < 0) continue;
+                float4 e2 = a.sortedE2[idx];
+                float d = reach_test_dist_sq(mx, my, mz, mux, muy, muz, rux, ruy, ruz, e1.x, e1.y, e1.z, e2.x, e2.y,
+                                             e2.z, tol, align);
+                if (d >= 0.f) {
+                    if (cnt < MAX_CAND) out[cnt] = s;
+                    cnt++;
+                }
+            }
+        }
+    return cnt;
+}
+
+__device__ void mini_unit(const FusedArgs& a, int u, int t) {
+    const sbx_dense_scene& sc = a.sc;
+    const sbx_motor_store& mot = sc.mot;
+    const sbx_rigid_body& mb = mot.body;
+    const sbx_minifilament_store& mini = sc.mini;
+    const sbx_rigid_body& bb = mini.backbone;
+    const sbx_rigid_body& fb = sc.fil.body;
+    const int nB = a.nB, nM = a.nM, nSeg = a.nSeg, nBb = a.nBb;
+    const int dpm = a.dpm, mpm = 2 * dpm, spm = 6 * dpm;
+    const int m0 = u * mpm, s0 = u * spm, d0 = u * dpm;
+    const int tid = threadIdx.x;
+    __shared__ float sF[3 * FUSED_MAX_SUB], sT[3 * FUSED_MAX_SUB];
+    LocalAcc acc{sF, sT, s0, spm};
+    const float* kp = mot.kinParams;
+
+    // F1: binding for this minifilament's heads
+    if (tid < mpm) {
+        int m = m0 + tid;
+        float mx = mot.head[m], my = mot.head[nM + m], mz = mot.head[2 * nM + m];
+        float mux = mot.uVec[m], muy = mot.uVec[nM + m], muz = mot.uVec[2 * nM + m];
+        float rux = mot.rodUVec[m], ruy = mot.rodUVec[nM + m], ruz = mot.rodUVec[2 * nM + m];
+        int* slice = sc.grid.reachSeg + (int64_t)m * MAX_CAND;
+        int rc = reach_walk_sorted(a, m, mx, my, mz, mux, muy, muz, rux, ruy, ruz, slice, kp[7], kp[8]);
+        sc.grid.reachCount[m] = rc;
+        if (rc > MAX_CAND) atomicOr(a.err, ERR_REACH_OVERFLOW);
+        int bs = mot.boundSeg[m], cd = mot.cooldown[m], sb = mot.stats[2 * m], sr = mot.stats[2 * m + 1],
+            cs = mot.capStats[m];
+        release_one(m, bs, cd, sb, sr, cs, mot.forceDotFil[m], mot.forceMag[m], kp, t, sc.seed);
+        if (bs == FREE_BINDABLE) {
+            int best;
+            float arc;
+            if (bind_nearest_scan(m, nM, mot.head, mot.uVec, mot.rodUVec, nSeg, fb.end1, fb.end2, slice, rc, kp[7],
+                                  kp[8], &best, &arc)) {
+                bs = best;
+                mot.bindArc[m] = arc;
+            }
+        }
+        mot.boundSeg[m] = bs; mot.cooldown[m] = cd; mot.stats[2 * m] = sb; mot.stats[2 * m + 1] = sr;
+        mot.capStats[m] = cs;
+        mot.nucleotideState[m] = cycle_one(m, mot.nucleotideState[m], bs >= 0, mot.forceDotHist + 10 * m,
+                                           mot.nucParams, t, sc.seed);
+        if (bs >= 0) atomicAdd(&a.cntM[bs], 1);
+    }
+    __syncthreads();
+    // F2: Brownian forcing + joints of the 96 sub-bodies; backbone Brownian
+    if (tid < spm) {
+        int s = s0 + tid;
+        float g[6];
+        gauss6_wang(s, t, sc.seed, g);
+        float gT[3] = {mb.bTransGam[s], mb.bTransGam[nB + s], mb.bTransGam[2 * nB + s]};
+        float gR[3] = {mb.bRotGam[s], mb.bRotGam[nB + s], mb.bRotGam[2 * nB + s]};
+        float rf[3], rt[3];
+        brownian_amplitudes(g, mb.brownTransScale[s], mb.brownRotScale[s], mot.bodyParams[1], gT, gR, rf, rt);
+        for (int k = 0; k < 3; k++) { mb.randForce[k * nB + s] = rf[k]; mb.randTorque[k * nB + s] = rt[k]; }
+        double f[3], tq[3];
+        joints_one(s, nB, mb.coord, mb.uVec, mb.segLength, mb.bTransGam, mb.bRotGam, mot.nucleotideState[s / 3],
+                   mot.jointParams, f, tq);
+        for (int k = 0; k < 3; k++) {
+            sF[k * spm + tid] = (float)(0.0 + f[k]);
+            sT[k * spm + tid] = (float)(0.0 + tq[k]);
+        }
+    } else if (tid == spm) {
+        float g[6];
+        gauss6_wang(u, t, sc.seedBb, g);
+        float gT[3] = {bb.bTransGam[u], bb.bTransGam[nBb + u], bb.bTransGam[2 * nBb + u]};
+        float gR[3] = {bb.bRotGam[u], bb.bRotGam[nBb + u], bb.bRotGam[2 * nBb + u]};
+        float rf[3], rt[3];
+        brownian_amplitudes(g, bb.brownTransScale[u], bb.brownRotScale[u], mini.bbBodyParams[1], gT, gR, rf, rt);
+        for (int k = 0; k < 3; k++) { bb.randForce[k * nBb + u] = rf[k]; bb.randTorque[k * nBb + u] = rt[k]; }
+    }
+    __syncthreads();
+    // F3: dimer coupling then tether (per dimer; disjoint sub-bodies)
+    if (tid < dpm) {
+        int d = d0 + tid;
+        couple_one(nB, mb.coord, mb.uVec, mb.segLength, mb.bTransGam, mb.bRotGam, acc, 2 * d, 2 * d + 1,
+                   sc.dim.parallel[d] != 0, sc.dim.dimerParams, mot.boundSeg);
+        tether_one(d, nB, mb.coord, mb.uVec, mb.segLength, mb.bTransGam, mb.bRotGam, acc, nBb, bb.coord, bb.uVec,
+                   mini.bbInvDragY, u, 2 * d, mini.attachAxial[d], mini.miniData, mini.miniParams);
+        // backbone CSR of the reference (rows = backbones, items = dimers in index order)
+        mini.bbDimerList[d] = d;
+    }
+    __syncthreads();
+    // F4 (backbone thread): gather its dimers' reactions, confine, integrate, derive
+    if (tid == spm) {
+        mini.bbDimerCount[u] = dpm;
+        mini.bbDimerOffsets[u] = d0;
+        if (u == nBb - 1) mini.bbDimerOffsets[nBb] = d0 + dpm;
+        // MiniFilamentSystem.backboneGather over this backbone's CSR row (its dimers, ascending)
+        double f[3] = {0, 0, 0}, tq[3] = {0, 0, 0};
+        for (int d = d0; d < d0 + dpm; d++) {
+            const float* p = mini.miniData + (int64_t)d * MINI_STRIDE;
+            f[0] += p[0]; f[1] += p[1]; f[2] += p[2];
+            tq[0] += p[3]; tq[1] += p[4]; tq[2] += p[5];
+        }
+        float F[3], T[3];
+        for (int k = 0; k < 3; k++) { F[k] = (float)(0.0f + f[k]); T[k] = (float)(0.0f + tq[k]); }
+        BoxParams bx = box_params(sc.boxParams, t);
+        float c[3] = {bb.coord[u], bb.coord[nBb + u], bb.coord[2 * nBb + u]};
+        float uu[3] = {bb.uVec[u], bb.uVec[nBb + u], bb.uVec[2 * nBb + u]};
+        if (bx.active) confine_one(bx, c, uu, bb.segLength[u], bb.bTransGam[u], F, T);
+        integrate_derive_store(bb, u, F, T, mini.bbBodyParams[0]);
+    }
+    // F5 (heads): cross-bridge bond, head self-write into the shared sums
+    if (tid < mpm) {
+        int m = m0 + tid;
+        float out[XB_STRIDE];
+        bond_one(m, nB, mb.coord, mb.uVec, mb.yVec, mb.bRotGam, nSeg, fb.coord, fb.uVec, fb.yVec, fb.bRotGam,
+                 fb.segLength, mot.boundSeg[m], mot.bindArc[m], mot.nucleotideState[m], sc.xbParams, out);
+        for (int k = 0; k < XB_STRIDE; k++) sc.bondData[m * XB_STRIDE + k] = out[k];
+        int hl = 3 * m + 2 - s0;
+        for (int k = 0; k < 3; k++) {
+            sF[k * spm + hl] = sF[k * spm + hl] + out[k];
+            sT[k * spm + hl] = sT[k * spm + hl] + out[3 + k];
+        }
+    }
+    __syncthreads();
+    // F6: integrate + derive the sub-bodies; F7: force-dot registry
+    if (tid < spm) {
+        int s = s0 + tid;
+        float F[3] = {sF[tid], sF[spm + tid], sF[2 * spm + tid]};
+        float T[3] = {sT[tid], sT[spm + tid], sT[2 * spm + tid]};
+        integrate_derive_store(mb, s, F, T, mot.bodyParams[0]);
+    }
+    if (tid < mpm) {
+        int m = m0 + tid;
+        register_force_dot_one(m, sc.bondData, mot.boundSeg[m] >= 0, mot.forceDotFil, mot.forceMag,
+                               mot.forceDotHist, mot.forceDotPlace);
+    }
+    __syncthreads();
+}
+
+__device__ void link_item(const FusedArgs& a, int k) {
+    const sbx_dense_scene& sc = a.sc;
+    const sbx_crosslinker_store& xl = sc.xl;
+    const sbx_rigid_body& fb = sc.fil.body;
+    float out[XL_STRIDE];
+    int la = xl.linkFilA[k], lb = xl.linkFilB[k];
+    link_forces_one(k, a.nSeg, fb.coord, fb.uVec, fb.end1, fb.bTransGam, la, lb, xl.loc1[k], xl.loc2[k], a.cntAct,
+                    xl.xlParams, out);
+    for (int j = 0; j < XL_STRIDE; j++) xl.xlinkData[k * XL_STRIDE + j] = out[j];
+    if (xl.torsionParams[1] >= 0.5f)
+        link_torsion_one(k, a.nSeg, fb.uVec, la, lb, xl.linkState[k], xl.linkOrientSame[k], xl.torqueMagHist,
+                         xl.torqueMagPlace, xl.xlinkData, xl.torsionParams[0]);
+}
+
+__device__ void phase_motors_links(const FusedArgs& a, int t) {
+    int linkChunks = a.xlOn ? (a.nL + blockDim.x - 1) / blockDim.x : 0;
+    int units = a.nBb + linkChunks;
+    for (int w = blockIdx.x; w < units; w += gridDim.x) {
+        if (w < a.nBb) {
+            mini_unit(a, w, t);
+        } else {
+            int k = (w - a.nBb) * blockDim.x + threadIdx.x;
+            if (k < a.nL) link_item(a, k);
+        }
+    }
+    // the reference's activeLinkCount array holds this step's counts
+    if (a.xlOn)
+        for (int s = gtid(); s < a.nSeg; s += gthreads()) a.sc.xl.activeLinkCount[s] = a.cntAct[s];
+}
+
+// ---------------------------------------------------------------- G: filament Brownian
+__device__ void phase_fil_brownian(const FusedArgs& a, int t) {
+    const sbx_rigid_body& fb = a.sc.fil.body;
+    int n = a.nSeg;
+    int seed = a.filSeed;
+    float mag = a.sc.fil.params[1];
+    for (int i = gtid(); i < n; i += gthreads()) {
+        float g[6];
+        gauss6_wang(i, t, seed, g);
+        float gT[3] = {fb.bTransGam[i], fb.bTransGam[n + i], fb.bTransGam[2 * n + i]};
+        float gR[3] = {fb.bRotGam[i], fb.bRotGam[n + i], fb.bRotGam[2 * n + i]};
+        float rf[3], rt[3];
+        brownian_amplitudes(g, fb.brownTransScale[i], fb.brownRotScale[i], mag, gT, gR, rf, rt);
+        for (int k = 0; k < 3; k++) { fb.randForce[k * n + i] = rf[k]; fb.randTorque[k * n + i] = rt[k]; }
+    }
+}
+
+__device__ void phase_motor_scatter(const FusedArgs& a) {
+    const sbx_dense_scene& sc = a.sc;
+    for (int m = gtid(); m < a.nM; m += gthreads()) {
+        int s = sc.mot.boundSeg[m];
+        if (s >= 0) a.tmpM[sc.segMotorOffsets[s] + atomicAdd(&sc.segMotorCount[s], 1)] = m;
+    }
+}
+
+__device__ void phase_motor_rank(const FusedArgs& a) {
+    const sbx_dense_scene& sc = a.sc;
+    for (int m = gtid(); m < a.nM; m += gthreads()) {
+        int s = sc.mot.boundSeg[m];
+        if (s < 0) continue;
+        int s0 = sc.segMotorOffsets[s], s1 = sc.segMotorOffsets[s + 1];
+        sc.segMotorMyo[s0 + rank_in(a.tmpM, s0, s1, m)] = m;
+    }
+}
+
+// ---------------------------------------------------------------- K: rods
+// TMA bulk copy global -> shared, completion on an mbarrier (no multicast)
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* mbar) {
+    unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    unsigned b = (unsigned)__cvta_generic_to_shared(mbar);
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                 :: "r"(d), "l"(src), "r"(bytes), "r"(b) : "memory");
+}
+
+__device__ void rod_unit(const FusedArgs& a, int u, int t, uint64_t* mbar, unsigned& phase) {
+    const sbx_dense_scene& sc = a.sc;
+    const sbx_filament_store& f = sc.fil;
+    const sbx_rigid_body& fb = f.body;
+    const sbx_crosslinker_store& xl = sc.xl;
+    const int n = a.nSeg, G = a.G;
+    const int g0 = u * G;
+    const int cnt = min(G, n - g0);
+    const int tid = threadIdx.x;
+    // staged rod geometry: coord xyz, uVec xyz, segLength, bTransGam x y, bRotGam y
+    __shared__ __align__(16) float st[10 * FUSED_MAX_ROD];
+    float* sc_[10];
+    for (int k = 0; k < 10; k++) sc_[k] = st + k * FUSED_MAX_ROD;
+    const float* src[10] = {fb.coord + g0, fb.coord + n + g0, fb.coord + 2 * n + g0, fb.uVec + g0, fb.uVec + n + g0,
+                            fb.uVec + 2 * n + g0, fb.segLength + g0, fb.bTransGam + g0, fb.bTransGam + n + g0,
+                            fb.bRotGam + n + g0};
+    __syncthreads();
+    bool tma = a.useTma && (cnt % 4 == 0);
+    if (tma) {
+        // order earlier generic-proxy accesses of the staging buffer before the async writes
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        unsigned bytes = (unsigned)cnt * 4u;
+        if (tid == 0) {
+            unsigned mb = (unsigned)__cvta_generic_to_shared(mbar);
+            asm volatile("mbarrier.arrive.expect_tx.shared.b64 _, [%0], %1;\n" :: "r"(mb), "r"(bytes * 10u) : "memory");
+            for (int k = 0; k < 10; k++) bulk_g2s(sc_[k], src[k], bytes, mbar);
+        }
+        // bounded wait on the transaction barrier
+        unsigned mb = (unsigned)__cvta_generic_to_shared(mbar);
+        long long it = 0;
+        unsigned done = 0;
+        while (!done) {
+            asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                         : "=r"(done) : "r"(mb), "r"(phase) : "memory");
+            if (!done && ++it > SPIN_LIMIT) {
+                atomicOr(a.err, ERR_TMA);
+                break;
+            }
+        }
+        phase ^= 1u;
+        if (!done) tma = false;
+    }
+    if (!tma) {
+        for (int k = 0; k < 10; k++)
+            for (int j = tid; j < cnt; j += blockDim.x) sc_[k][j] = src[k][j];
+    }
+    __syncthreads();
+    if (tid < cnt) {
+        int i = g0 + tid;
+        ChainParams cp = chain_params(f.chainParams);
+        auto rod = [&](int j) {
+            int l = j - g0;
+            RodGeom r;
+            r.cx = sc_[0][l]; r.cy = sc_[1][l]; r.cz = sc_[2][l];
+            r.ux = sc_[3][l]; r.uy = sc_[4][l]; r.uz = sc_[5][l];
+            r.len = sc_[6][l];
+            r.bTGx = sc_[7][l]; r.bTGy = sc_[8][l]; r.bRGy = sc_[9][l];
+            return r;
+        };
+        RodGeom me = rod(i);
+        double fd[3] = {0, 0, 0}, td[3] = {0, 0, 0};
+        int s2 = f.end2NbrSlot[i];
+        if (s2 >= 0) chain_side(cp, i, 0, s2, f.end2NbrSide[i], me, rod(s2), fd, td);
+        int s1 = f.end1NbrSlot[i];
+        if (s1 >= 0) chain_side(cp, i, 1, s1, f.end1NbrSide[i], me, rod(s1), fd, td);
+        float F[3], T[3];
+        for (int k = 0; k < 3; k++) { F[k] = (float)(0.0f + fd[k]); T[k] = (float)(0.0f + td[k]); }
+        double gf[3], gt[3];
+        if (a.xlOn) {
+            csr_gather_row(i, xl.segOffsetsA, xl.segIdxA, xl.xlinkData, XL_STRIDE, 0, xl.linkState, gf, gt);
+            for (int k = 0; k < 3; k++) { F[k] = (float)(F[k] + gf[k]); T[k] = (float)(T[k] + gt[k]); }
+            csr_gather_row(i, xl.segOffsetsB, xl.segIdxB, xl.xlinkData, XL_STRIDE, 6, xl.linkState, gf, gt);
+            for (int k = 0; k < 3; k++) { F[k] = (float)(F[k] + gf[k]); T[k] = (float)(T[k] + gt[k]); }
+        }
+        csr_gather_row(i, sc.segMotorOffsets, sc.segMotorMyo, sc.bondData, XB_STRIDE, 6, nullptr, gf, gt);
+        for (int k = 0; k < 3; k++) { F[k] = (float)(F[k] + gf[k]); T[k] = (float)(T[k] + gt[k]); }
+        BoxParams bx = box_params(sc.boxParams, t);
+        float c[3] = {sc_[0][tid], sc_[1][tid], sc_[2][tid]};
+        float uu[3] = {sc_[3][tid], sc_[4][tid], sc_[5][tid]};
+        if (bx.active) confine_one(bx, c, uu, sc_[6][tid], sc_[7][tid], F, T);
+        integrate_derive_store(fb, i, F, T, f.params[0]);
+    }
+}
+
+__device__ void phase_rods(const FusedArgs& a, int t, uint64_t* mbar, unsigned& phase) {
+    for (int u = blockIdx.x; u < a.nRodUnits; u += gridDim.x) rod_unit(a, u, t, mbar, phase);
+    // reset the private histograms for the next step
+    for (int i = gtid(); i < a.C; i += gthreads()) a.cntCell[i] = 0;
+    for (int i = gtid(); i < a.nSeg; i += gthreads()) {
+        a.cntAct[i] = 0; a.cntA[i] = 0; a.cntB[i] = 0; a.cntM[i] = 0;
+    }
+}
+
+__global__ void __launch_bounds__(FUSED_THREADS) k_dense_fused(FusedArgs a, int t0, int nsteps) {
+    __shared__ __align__(8) uint64_t mbar;
+    unsigned phase = 0;
+    if (threadIdx.x == 0) {
+        unsigned mb = (unsigned)__cvta_generic_to_shared(&mbar);
+        asm volatile("mbarrier.init.shared.b64 [%0], 1;\n" :: "r"(mb) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    const sbx_dense_scene& sc = a.sc;
+    ScanArr first[3] = {{a.cntCell, a.C, 0}, {a.cntA, a.nSeg, a.tilesC}, {a.cntB, a.nSeg, a.tilesC + a.tilesS}};
+    int narr1 = a.xlOn ? 3 : 1;
+    int* out1[3] = {sc.grid.gridCellOffsets, sc.xl.segOffsetsA, sc.xl.segOffsetsB};
+    int* zero1[3] = {sc.grid.cellCount, sc.xl.segCountA, sc.xl.segCountB};
+    int clamp1[3] = {a.cap, a.nL, a.nL};
+    ScanArr second[1] = {{a.cntM, a.nSeg, 0}};
+    int* out2[1] = {sc.segMotorOffsets};
+    int* zero2[1] = {sc.segMotorCount};
+    int clamp2[1] = {a.nM};
+    int ph = 0;
+    auto stamp = [&](int s_) {
+        if (a.phaseTimes && gtid() == 0) {
+            long long ns;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(ns));
+            a.phaseTimes[(long long)s_ * FUSED_PHASES + ph] = ns;
+        }
+        ph++;
+    };
+    for (int s = 0; s < nsteps; s++) {
+        int t = t0 + s;
+        ph = 0;
+        if (gtid() == 0) {
+            // MotorStore.setCounts, MiniFilamentStore.setBackboneCounts, counts.set(1, t), xl.setCounts
+            int* mc = sc.mot.counts; mc[0] = a.nM; mc[1] = t; mc[2] = sc.seed; mc[3] = a.nSeg;
+            int* bc = sc.mini.bbCounts; bc[0] = a.nBb; bc[1] = t; bc[2] = sc.seedBb; bc[3] = a.nBb;
+            sc.fil.counts[1] = t;
+            if (a.xlOn) { sc.xl.counts[1] = t; sc.xl.counts[2] = sc.seed; }
+        }
+        phase_publish_bin(a, t);
+        if (!grid_sync(a)) return;
+        stamp(s);
+        tile_sums(first, narr1, a.tileSum);
+        if (!grid_sync(a)) return;
+        stamp(s);
+        tile_scan(first, narr1, a.tileSum, out1, zero1, clamp1, sc.grid.chunkSum);
+        if (!grid_sync(a)) return;
+        stamp(s);
+        phase_scatter(a);
+        if (!grid_sync(a)) return;
+        stamp(s);
+        phase_rank(a);
+        if (!grid_sync(a)) return;
+        stamp(s);
+        phase_motors_links(a, t);
+        if (!grid_sync(a)) return;
+        stamp(s);
+        tile_sums(second, 1, a.tileSum);
+        phase_fil_brownian(a, t);
+        if (!grid_sync(a)) return;
+        stamp(s);
+        tile_scan(second, 1, a.tileSum, out2, zero2, clamp2, nullptr);
+        if (!grid_sync(a)) return;
+        stamp(s);
+        phase_motor_scatter(a);
+        if (!grid_sync(a)) return;
+        stamp(s);
+        phase_motor_rank(a);
+        if (!grid_sync(a)) return;
+        stamp(s);
+        phase_rods(a, t, &mbar, phase);
+        if (!grid_sync(a)) return;
+        stamp(s);
+    }
+    if (gtid() == 0 && a.d_step) *a.d_step = t0 + nsteps;
+}
+
+}  // namespace
+
+sbx_status fused_launch(sbx_ctx* ctx, FusedArgs& a, int grid, int t0, int nsteps) {
+    void* args[] = {&a, &t0, &nsteps};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_dense_fused, grid, FUSED_THREADS, args, 0, ctx->stream);
+    ctx->launches++;
+    if (e != cudaSuccess) return fail(ctx, SBX_ECUDA, std::string("fused launch: ") + cudaGetErrorString(e));
+    return SBX_OK;
+}
+
+int fused_max_blocks_per_sm() {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_dense_fused, FUSED_THREADS, 0);
+    return nb;
+}
+
+const void* fused_kernel_ptr() { return (const void*)k_dense_fused; }

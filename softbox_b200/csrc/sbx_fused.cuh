@@ -1,0 +1,33 @@
+// sbx_fused.cuh — arguments of the fused persistent dense-step kernel (sbx_fused.cu).
+#pragma once
+#include "../../include/softbox_b200.h"
+#include "sbx_internal.cuh"
+
+constexpr int FUSED_THREADS = 128;
+constexpr int FUSED_MAX_SUB = 120;    // sub-bodies per minifilament CTA (6 per dimer)
+constexpr int FUSED_MAX_ROD = 128;    // segments per rod CTA
+
+struct FusedArgs {
+    sbx_dense_scene sc;
+    int nSeg, nM, nB, nBb, nD, nL, cap, S, C;
+    int nX, nY, nZ;
+    int dpm;                 // dimers per minifilament
+    int G, nRodUnits;        // segments per rod unit (whole filaments), units
+    int tilesC, tilesS;
+    int xlOn, xlUnbind, useTma, filSeed;
+    // private scratch (plan-owned)
+    int *cntCell, *cntAct, *cntA, *cntB, *cntM;
+    int* tileSum;
+    int *tmpCell, *tmpA, *tmpB, *tmpM;
+    float4 *sortedE1, *sortedE2;
+    unsigned* bar;           // [0] arrivals, [1] generation
+    int* err;                // bit0 barrier timeout, bit1 reach overflow, bit2 TMA wait timeout
+    int* d_step;
+    int barrierExtra;        // test hook: arrivals the barrier waits for beyond gridDim.x
+    long long* phaseTimes;   // optional: %globaltimer after each phase barrier, [nsteps][FUSED_PHASES]
+};
+
+constexpr int FUSED_PHASES = 11;
+
+sbx_status fused_launch(sbx_ctx* ctx, FusedArgs& a, int grid, int t0, int nsteps);
+int fused_max_blocks_per_sm();

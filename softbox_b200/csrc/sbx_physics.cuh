@@ -9,6 +9,7 @@
 #pragma once
 #include <stdint.h>
 #include "sbx_math.h"
+#include "../../include/softbox_b200.h"
 
 #define SBX_DEV __device__ __forceinline__
 
@@ -886,8 +887,22 @@ SBX_DEV void joints_one(int s, int nB, const float* coord, const float* uVec, co
 }
 
 // DimerCouplingSystem.couple per dimer (DimerCouplingSystem.java:99-182); self-writes rods/levers
+// Force/torque accumulators addressed as (component k, body s): planar global arrays or a
+// shared-memory window of them (the fused kernels keep a minifilament's sums on chip).
+struct GlobalAcc {
+    float* F; float* T; int n;
+    SBX_DEV float& f(int k, int s) const { return F[k * n + s]; }
+    SBX_DEV float& t(int k, int s) const { return T[k * n + s]; }
+};
+struct LocalAcc {
+    float* F; float* T; int base, stride;
+    SBX_DEV float& f(int k, int s) const { return F[k * stride + (s - base)]; }
+    SBX_DEV float& t(int k, int s) const { return T[k * stride + (s - base)]; }
+};
+
+template <class Acc>
 SBX_DEV void couple_one(int nB, const float* coord, const float* uVec, const float* segLength, const float* bTG,
-                        const float* bRG, float* F, float* T, int mA, int mB, bool par, const float* dp,
+                        const float* bRG, const Acc& acc, int mA, int mB, bool par, const float* dp,
                         const int* boundSeg) {
     double dt = dp[0], fracMove = dp[1], leverTorq = dp[2], leverDeg = dp[3], rodLen = dp[4];
     int rodA = 3 * mA, rodB = 3 * mB;
@@ -917,22 +932,22 @@ SBX_DEV void couple_one(int nB, const float* coord, const float* uVec, const flo
             double TAx = (RsA * aUy) * FAz - (RsA * aUz) * FAy;
             double TAy = (RsA * aUz) * FAx - (RsA * aUx) * FAz;
             double TAz = (RsA * aUx) * FAy - (RsA * aUy) * FAx;
-            F[rodA] = (float)(F[rodA] + FAx);
-            F[nB + rodA] = (float)(F[nB + rodA] + FAy);
-            F[2 * nB + rodA] = (float)(F[2 * nB + rodA] + FAz);
-            T[rodA] = (float)(T[rodA] + TAx);
-            T[nB + rodA] = (float)(T[nB + rodA] + TAy);
-            T[2 * nB + rodA] = (float)(T[2 * nB + rodA] + TAz);
+            acc.f(0, rodA) = (float)(acc.f(0, rodA) + FAx);
+            acc.f(1, rodA) = (float)(acc.f(1, rodA) + FAy);
+            acc.f(2, rodA) = (float)(acc.f(2, rodA) + FAz);
+            acc.t(0, rodA) = (float)(acc.t(0, rodA) + TAx);
+            acc.t(1, rodA) = (float)(acc.t(1, rodA) + TAy);
+            acc.t(2, rodA) = (float)(acc.t(2, rodA) + TAz);
             double RsB = 0.5e-6 * rodLen * endSelB;
             double TBx = (RsB * bUy) * (-FAz) - (RsB * bUz) * (-FAy);
             double TBy = (RsB * bUz) * (-FAx) - (RsB * bUx) * (-FAz);
             double TBz = (RsB * bUx) * (-FAy) - (RsB * bUy) * (-FAx);
-            F[rodB] = (float)(F[rodB] - FAx);
-            F[nB + rodB] = (float)(F[nB + rodB] - FAy);
-            F[2 * nB + rodB] = (float)(F[2 * nB + rodB] - FAz);
-            T[rodB] = (float)(T[rodB] + TBx);
-            T[nB + rodB] = (float)(T[nB + rodB] + TBy);
-            T[2 * nB + rodB] = (float)(T[2 * nB + rodB] + TBz);
+            acc.f(0, rodB) = (float)(acc.f(0, rodB) - FAx);
+            acc.f(1, rodB) = (float)(acc.f(1, rodB) - FAy);
+            acc.f(2, rodB) = (float)(acc.f(2, rodB) - FAz);
+            acc.t(0, rodB) = (float)(acc.t(0, rodB) + TBx);
+            acc.t(1, rodB) = (float)(acc.t(1, rodB) + TBy);
+            acc.t(2, rodB) = (float)(acc.t(2, rodB) + TBz);
         }
     }
     bool bothBound = boundSeg[mA] >= 0 && boundSeg[mB] >= 0;
@@ -951,19 +966,20 @@ SBX_DEV void couple_one(int nB, const float* coord, const float* uVec, const flo
             double ang = accurate_acos(dot) * 180.0 / PI_D;
             double invBRG = 1.0 / bRG[nB + leverA] + 1.0 / bRG[nB + leverB];
             double torsionMag = leverTorq * (PI_D / 180.0) * (ang - leverDeg) / (invBRG * dt);
-            T[leverA] = (float)(T[leverA] + tvx * torsionMag);
-            T[nB + leverA] = (float)(T[nB + leverA] + tvy * torsionMag);
-            T[2 * nB + leverA] = (float)(T[2 * nB + leverA] + tvz * torsionMag);
-            T[leverB] = (float)(T[leverB] - tvx * torsionMag);
-            T[nB + leverB] = (float)(T[nB + leverB] - tvy * torsionMag);
-            T[2 * nB + leverB] = (float)(T[2 * nB + leverB] - tvz * torsionMag);
+            acc.t(0, leverA) = (float)(acc.t(0, leverA) + tvx * torsionMag);
+            acc.t(1, leverA) = (float)(acc.t(1, leverA) + tvy * torsionMag);
+            acc.t(2, leverA) = (float)(acc.t(2, leverA) + tvz * torsionMag);
+            acc.t(0, leverB) = (float)(acc.t(0, leverB) - tvx * torsionMag);
+            acc.t(1, leverB) = (float)(acc.t(1, leverB) - tvy * torsionMag);
+            acc.t(2, leverB) = (float)(acc.t(2, leverB) - tvz * torsionMag);
         }
     }
 }
 
 // MiniFilamentSystem.tether per dimer (MiniFilamentSystem.java:77-131)
+template <class Acc>
 SBX_DEV void tether_one(int d, int nMB, const float* mC, const float* mU, const float* mL, const float* mBTG,
-                        const float* mBRG, float* mF, float* mT, int nBb, const float* bbC, const float* bbU,
+                        const float* mBRG, const Acc& acc, int nBb, const float* bbC, const float* bbU,
                         const float* inv, int bb, int mA, float axf, float* miniData, const float* mp) {
     double dt = mp[0], fracMove = mp[1], align = mp[2];
     int rodA = 3 * mA;
@@ -984,9 +1000,9 @@ SBX_DEV void tether_one(int d, int nMB, const float* mC, const float* mU, const 
         double denom = dt * (1.0 / mBTG[nMB + rodA] + inv[bb]);
         double forceMag = (denom > 0.0) ? (fracMove * 1.0e-6 * strain / denom) : 0.0;
         double Frx = forceMag * lx, Fry = forceMag * ly, Frz = forceMag * lz;
-        mF[rodA] = (float)(mF[rodA] + Frx);
-        mF[nMB + rodA] = (float)(mF[nMB + rodA] + Fry);
-        mF[2 * nMB + rodA] = (float)(mF[2 * nMB + rodA] + Frz);
+        acc.f(0, rodA) = (float)(acc.f(0, rodA) + Frx);
+        acc.f(1, rodA) = (float)(acc.f(1, rodA) + Fry);
+        acc.f(2, rodA) = (float)(acc.f(2, rodA) + Frz);
         fbx = -Frx; fby = -Fry; fbz = -Frz;
     }
     double alignSign = (ax < 0.0) ? -1.0 : 1.0;
@@ -1002,14 +1018,44 @@ SBX_DEV void tether_one(int d, int nMB, const float* mC, const float* mU, const 
         double angDeg = accurate_acos(dot) * 180.0 / PI_D;
         double denomR = (1.0 / mBRG[nMB + rodA] + inv[nBb + bb]) * dt;
         double tmag = align * (PI_D / 180.0) * angDeg / denomR;
-        mT[rodA] = (float)(mT[rodA] + tvx * tmag);
-        mT[nMB + rodA] = (float)(mT[nMB + rodA] + tvy * tmag);
-        mT[2 * nMB + rodA] = (float)(mT[2 * nMB + rodA] + tvz * tmag);
+        acc.t(0, rodA) = (float)(acc.t(0, rodA) + tvx * tmag);
+        acc.t(1, rodA) = (float)(acc.t(1, rodA) + tvy * tmag);
+        acc.t(2, rodA) = (float)(acc.t(2, rodA) + tvz * tmag);
         tbx = -tvx * tmag; tby = -tvy * tmag; tbz = -tvz * tmag;
     }
     float* o = miniData + (int64_t)MINI_STRIDE * d;
     o[0] = (float)fbx; o[1] = (float)fby; o[2] = (float)fbz;
     o[3] = (float)tbx; o[4] = (float)tby; o[5] = (float)tbz;
+}
+
+
+// integrate + derive one body slot from accumulated F/T (registers), the slot's stored
+// Brownian draws and drag, then store pose, derived geometry and the final F/T sums
+// (MechanicsFusion.integDerive, MechanicsFusion.java:129-200)
+SBX_DEV void integrate_derive_store(const sbx_rigid_body& b, int s, const float F[3], const float T[3], float dt) {
+    const int n = b.n;
+    Pose p, q;
+    float rf[3], rt[3], gT[3], gR[3], dc[3];
+    for (int k = 0; k < 3; k++) {
+        p.c[k] = b.coord[k * n + s]; p.u[k] = b.uVec[k * n + s]; p.y[k] = b.yVec[k * n + s];
+        rf[k] = b.randForce[k * n + s]; rt[k] = b.randTorque[k * n + s];
+        gT[k] = b.bTransGam[k * n + s]; gR[k] = b.bRotGam[k * n + s];
+    }
+    integrate_pose(p, F, T, rf, rt, gT, gR, dt, q, dc);
+    if (b.coord64) {
+        for (int k = 0; k < 3; k++) {
+            double c = b.coord64[k * n + s] + (double)dc[k];
+            b.coord64[k * n + s] = c;
+            q.c[k] = (float)c;
+        }
+    }
+    float z[3], e1[3], e2[3];
+    derive_pose(q.c, q.u, q.y, z, e1, e2, b.segLength[s]);
+    for (int k = 0; k < 3; k++) {
+        b.coord[k * n + s] = q.c[k]; b.uVec[k * n + s] = q.u[k]; b.yVec[k * n + s] = q.y[k];
+        b.zVec[k * n + s] = z[k]; b.end1[k * n + s] = e1[k]; b.end2[k * n + s] = e2[k];
+        b.forceSum[k * n + s] = F[k]; b.torqueSum[k * n + s] = T[k];
+    }
 }
 
 }  // namespace sbx

@@ -1061,7 +1061,7 @@ __global__ void k_couple(int nB, const float* coord, const float* uVec, const fl
                          const float* dp, const int* boundSeg) {
     int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= nD) return;
-    couple_one(nB, coord, uVec, segLength, bTG, bRG, F, T, mA[d], mB[d], par[d] != 0, dp, boundSeg);
+    couple_one(nB, coord, uVec, segLength, bTG, bRG, GlobalAcc{F, T, nB}, mA[d], mB[d], par[d] != 0, dp, boundSeg);
 }
 
 extern "C" sbx_status sbx_dimer_couple(sbx_ctx* ctx, int32_t nB, const float* coord, const float* uVec,
@@ -1082,7 +1082,7 @@ __global__ void k_tether(int nMB, const float* mC, const float* mU, const float*
                          const float* mp) {
     int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= nD) return;
-    tether_one(d, nMB, mC, mU, mL, mBTG, mBRG, mF, mT, nBb, bbC, bbU, inv, hbs[d], mA[d], ax[d], miniData, mp);
+    tether_one(d, nMB, mC, mU, mL, mBTG, mBRG, GlobalAcc{mF, mT, nMB}, nBb, bbC, bbU, inv, hbs[d], mA[d], ax[d], miniData, mp);
 }
 
 extern "C" sbx_status sbx_mini_tether(sbx_ctx* ctx, int32_t nMB, const float* mC, const float* mU, const float* mL,

@@ -29,14 +29,38 @@ class DenseNetwork:
         if st != 0:
             raise SbxError(st, "sbx_dense_plan_create: " + self.ctx.last_error())
 
+    MODES = {"unfused": 0, "graph": 1, "fused": 2}
+
     @property
     def kernels_per_step(self):
+        """Kernels one step launches on the graph path (the fused path launches one kernel per run)."""
         return LIB.sbx_dense_plan_kernels_per_step(self.plan)
 
-    def run(self, t0, nsteps, graph=True):
-        st = LIB.sbx_dense_plan_run(self.plan, int(t0), int(nsteps), 1 if graph else 0)
+    @property
+    def fused_available(self):
+        return bool(LIB.sbx_dense_plan_fused_available(self.plan))
+
+    @property
+    def fused_grid(self):
+        return LIB.sbx_dense_plan_fused_grid(self.plan)
+
+    def run(self, t0, nsteps, mode=None):
+        """Advance steps t0..t0+nsteps-1. mode: "fused" (default when available: one
+        persistent cooperative launch for all steps), "graph" (one CUDA-graph replay per
+        step) or "unfused" (the per-system call sequence). All give the same bits."""
+        if mode is None:
+            mode = "fused" if self.fused_available else "graph"
+        st = LIB.sbx_dense_plan_run(self.plan, int(t0), int(nsteps), self.MODES[mode])
         if st != 0:
             raise SbxError(st, "sbx_dense_plan_run: " + self.ctx.last_error())
+
+    def status(self):
+        """Synchronise and return the fused path's flags; raises on a timeout/overflow."""
+        flags = C.c_int32(0)
+        st = LIB.sbx_dense_plan_status(self.plan, C.byref(flags))
+        if st != 0:
+            raise SbxError(st, "sbx_dense_plan_status: " + self.ctx.last_error())
+        return flags.value
 
     def step_unfused(self, t):
         self.ctx("sbx_dense_step_unfused", self.desc, int(t))

@@ -37,7 +37,7 @@ def host(x):
 
 
 # ----------------------------------------------------------------------------- whole step
-@pytest.mark.parametrize("mode", ["unfused", "graph"])
+@pytest.mark.parametrize("mode", ["unfused", "graph", "fused"])
 def test_dense_steps_bitwise(orc_dm, warm_scene, mode):
     from softbox_b200.engine import DenseNetwork
     ref = copy.deepcopy(warm_scene)
@@ -47,7 +47,9 @@ def test_dense_steps_bitwise(orc_dm, warm_scene, mode):
         for t in range(300, 300 + nsteps):
             net.step_unfused(t)
     else:
-        net.run(300, nsteps, graph=True)
+        assert mode != "fused" or net.fused_available
+        net.run(300, nsteps, mode=mode)
+        assert net.status() == 0
     torch.cuda.synchronize()
     oracle_dense_run(orc_dm, ref, 300, nsteps)
     got = host(net.dev)
@@ -55,13 +57,14 @@ def test_dense_steps_bitwise(orc_dm, warm_scene, mode):
     assert len(names) > 80
 
 
-def test_dense_fp64_coords(orc_dm, warm_scene):
+@pytest.mark.parametrize("mode", ["graph", "fused"])
+def test_dense_fp64_coords(orc_dm, warm_scene, mode):
     from softbox_b200.engine import DenseNetwork
     ref = copy.deepcopy(warm_scene)
     for s, b in (("fil", "body"), ("mot", "body"), ("mini", "backbone")):
         D.add_coord64(ref[s][b])
     net = DenseNetwork(copy.deepcopy(warm_scene), fp64_coords=True)
-    net.run(300, 25, graph=True)
+    net.run(300, 25, mode=mode)
     torch.cuda.synchronize()
     oracle_dense_run(orc_dm, ref, 300, 25)
     got = host(net.dev)
@@ -536,3 +539,40 @@ def test_thermostat_equipartition():
     bRGy = float(b["bRotGam"][nB + 0])
     pred = 4.0 * scenes.KT * dt / (bRGy * coeff * (2.0 - coeff))
     assert abs(meas / pred - 1.0) < 0.03, (meas, pred)
+
+
+def test_fused_equals_graph_on_full_network():
+    """The full 20,000-rod network: 60 fused steps (one launch) == 60 graph-replayed steps."""
+    from softbox_b200.engine import DenseNetwork
+    sc = scenes.dense_contractile(scenes.C1)
+    a = DenseNetwork(copy.deepcopy(sc))
+    b = DenseNetwork(copy.deepcopy(sc))
+    assert a.fused_available, "fused path must qualify for the benchmark network"
+    a.run(0, 60, mode="fused")
+    b.run(0, 60, mode="graph")
+    assert a.status() == 0
+    torch.cuda.synchronize()
+    names = compare_scenes(host(a.dev), host(b.dev))
+    assert len(names) > 80
+
+
+def test_fused_barrier_timeout_reports_and_recovers(warm_scene):
+    """Failure detection without a GPU fault: the test hook makes the grid barrier wait for
+    an arrival that never comes; the bounded wait runs out, every CTA returns, the run
+    reports SBX_ETIMEOUT, and the context and plan stay usable."""
+    from softbox_b200.engine import DenseNetwork
+    from softbox_b200.runtime import LIB, SbxError
+    net = DenseNetwork(copy.deepcopy(warm_scene))
+    assert LIB.sbx_dense_plan_test_barrier_extra(net.plan, 1) == 0
+    net.run(300, 1, mode="fused")
+    with pytest.raises(SbxError) as e:
+        net.status()
+    assert e.value.code == -4
+    assert LIB.sbx_dense_plan_test_barrier_extra(net.plan, 0) == 0
+    fresh = DenseNetwork(copy.deepcopy(warm_scene))
+    fresh.run(300, 5, mode="fused")
+    assert fresh.status() == 0
+    ref = DenseNetwork(copy.deepcopy(warm_scene))
+    ref.run(300, 5, mode="graph")
+    torch.cuda.synchronize()
+    compare_scenes(host(ref.dev), host(fresh.dev))
