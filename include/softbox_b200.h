@@ -234,6 +234,19 @@ sbx_status sbx_xbridge_register_force_dot(sbx_ctx* ctx, int32_t nM, const float*
  * lengths, as the serial csrScatter leaves it). Uses context scratch for the scan. */
 sbx_status sbx_csr_build(sbx_ctx* ctx, const int32_t* keys, int32_t nItems, int32_t nRows,
                          int32_t* rowCount, int32_t* rowOffsets, int32_t* rowList);
+/* No counterpart in the reference. Same outputs as sbx_csr_build, but it allocates no
+ * device memory: its scratch is a fixed array inside the library (about 4 MB per device),
+ * for callers that cannot let a call allocate or synchronise (a host that owns the device
+ * heap under a fixed budget, a step sequence that must not stall). Inputs above
+ * SBX_CSR_NOALLOC_MAX_ITEMS items or SBX_CSR_NOALLOC_MAX_ROWS rows return SBX_EINVAL.
+ * Nothing needs to start at zero. The scratch is shared by every context on a device:
+ * calls that overlap in time on one device (different streams) race; calls on one stream
+ * are safe. The first call on each device sets the scratch up; make it before any stream
+ * capture begins. */
+#define SBX_CSR_NOALLOC_MAX_ITEMS (1 << 20)
+#define SBX_CSR_NOALLOC_MAX_ROWS (1 << 22)
+sbx_status sbx_csr_build_noalloc(sbx_ctx* ctx, const int32_t* keys, int32_t nItems, int32_t nRows,
+                                 int32_t* rowCount, int32_t* rowOffsets, int32_t* rowList);
 /* CrossBridgeSystem.segGather (CrossBridgeSystem.java:302-320) */
 sbx_status sbx_xbridge_seg_gather(sbx_ctx* ctx, int32_t nSeg, const int32_t* segMotorOffsets,
                                   const int32_t* segMotorMyo, const float* bondData, float* filForceSum,
