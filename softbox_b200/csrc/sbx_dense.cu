@@ -212,9 +212,18 @@ bool fused_prepare(sbx_dense_plan* p) {
     auto gd = d2h(sc.grid.gridDims, 4, st);
     a.nX = gd[0]; a.nY = gd[1]; a.nZ = gd[2];
     if (gd[3] != a.C || (long long)a.nX * a.nY * a.nZ != a.C) return why("grid dims");
-    // chain topology: filaments must be contiguous slot ranges; pick the largest group
-    // of whole filaments (<= FUSED_MAX_ROD, a multiple of 4 segments)
+    int dev = 0, sms = 0, coop = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    int per = fused_max_blocks_per_sm();
+    if (!coop || per <= 0) return why("cooperative launch unavailable");
+    p->fused_grid = sms * per;
+    // chain topology: filaments must be contiguous slot ranges. A rod group is a run of
+    // whole filaments (a multiple of 4 segments, <= FUSED_MAX_ROD); the smallest group
+    // size whose groups fit one wave of CTAs, else the largest valid one.
     auto e1 = d2h(sc.fil.end1NbrSlot, a.nSeg, st), e2 = d2h(sc.fil.end2NbrSlot, a.nSeg, st);
+    auto d1 = d2h(sc.fil.end1NbrSide, a.nSeg, st), d2 = d2h(sc.fil.end2NbrSide, a.nSeg, st);
     std::vector<int> lo(a.nSeg), hi(a.nSeg);
     for (int i = 0; i < a.nSeg; i++) {
         lo[i] = i; hi[i] = i;
@@ -225,12 +234,27 @@ bool fused_prepare(sbx_dense_plan* p) {
         }
     }
     a.G = 0;
-    for (int G = FUSED_MAX_ROD - FUSED_MAX_ROD % 4; G >= 4 && !a.G; G -= 4) {
+    int largest = 0;
+    for (int G = 4; G <= FUSED_MAX_ROD; G += 4) {
         bool ok = true;
         for (int i = 0; i < a.nSeg && ok; i++) ok = (lo[i] / G == i / G) && (hi[i] / G == i / G);
-        if (ok) a.G = G;
+        if (!ok) continue;
+        largest = G;
+        if (!a.G && (a.nSeg + G - 1) / G <= p->fused_grid) a.G = G;
     }
+    if (!a.G) a.G = largest;
     if (!a.G) return why("chain neighbours cross every segment grouping");
+    // joint sharing needs every neighbour link to point back: rod i's side s (0 = end2) to
+    // slot j at nside means j's side 1 - nside points to i at nside 1 - s
+    a.jointShare = 1;
+    for (int i = 0; i < a.nSeg && a.jointShare; i++)
+        for (int side = 0; side < 2; side++) {
+            int j = side == 0 ? e2[i] : e1[i], ns = side == 0 ? d2[i] : d1[i];
+            if (j < 0) continue;
+            if (j == i || (ns != 0 && ns != 1)) { a.jointShare = 0; break; }
+            int back = ns == 0 ? e1[j] : e2[j], backSide = ns == 0 ? d1[j] : d2[j];
+            if (back != i || backSide != 1 - side) { a.jointShare = 0; break; }
+        }
     a.nRodUnits = (a.nSeg + a.G - 1) / a.G;
     a.tilesC = (a.C + SCAN_CHUNK - 1) / SCAN_CHUNK;
     a.tilesS = (a.nSeg + SCAN_CHUNK - 1) / SCAN_CHUNK;
@@ -260,13 +284,6 @@ bool fused_prepare(sbx_dense_plan* p) {
     a.d_step = p->d_step;
     for (void* q : p->allocs)
         if (!q) return why("scratch allocation failed");
-    int dev = 0, sms = 0, coop = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-    int per = fused_max_blocks_per_sm();
-    if (!coop || per <= 0) return why("cooperative launch unavailable");
-    p->fused_grid = sms * per;
     return true;
 }
 

@@ -42,6 +42,26 @@ namespace {
 constexpr long long SPIN_LIMIT = 1LL << 24;    // x ~64 ns sleeps: about one second
 constexpr int ERR_BARRIER = 1, ERR_REACH_OVERFLOW = 2, ERR_TMA = 4;
 
+// shared memory of one CTA, reused by the phases
+struct RodSmem {
+    float st[10 * FUSED_MAX_ROD];                 // staged rod geometry planes (TMA destination)
+    int off[3][FUSED_MAX_ROD + 1];                // the group's CSR row offsets: links A, links B, motors
+    ChainJoint js[2 * FUSED_MAX_ROD];             // joints, at (owner rod, owner side)
+    float ent[FUSED_ENT_CAP][6];                  // the group's CSR payloads, in CSR order
+    int entOk[FUSED_ENT_CAP];                     // guard passed (active link)
+};
+struct MiniSmem {
+    float sF[3 * FUSED_MAX_SUB], sT[3 * FUSED_MAX_SUB];
+    MotorJoint mj[4 * FUSED_MAX_DPM];            // [local motor][joint 2, joint 1]
+    CoupleTerm ct[2 * FUSED_MAX_DPM];            // [local dimer][end variant]
+    LeverTerm lt[FUSED_MAX_DPM];
+    TetherTerm tt[FUSED_MAX_DPM];
+};
+union FusedSmem {
+    RodSmem rod;
+    MiniSmem mini;
+};
+
 __device__ __forceinline__ int vload(const int* p) { return *(const volatile int*)p; }
 
 // Grid barrier (the cooperative-groups pattern: block barrier, one thread per CTA
@@ -79,6 +99,18 @@ __device__ bool grid_sync(const FusedArgs& a) {
 __device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
 __device__ __forceinline__ int gthreads() { return gridDim.x * blockDim.x; }
 
+// BrownianForceSystem.brownianForces for one slot (BrownianForceSystem.java:183-245)
+__device__ __forceinline__ void brownian_slot(const sbx_rigid_body& b, int s, int t, int seed, float mag) {
+    const int n = b.n;
+    float g[6];
+    gauss6_wang(s, t, seed, g);
+    float gT[3] = {b.bTransGam[s], b.bTransGam[n + s], b.bTransGam[2 * n + s]};
+    float gR[3] = {b.bRotGam[s], b.bRotGam[n + s], b.bRotGam[2 * n + s]};
+    float rf[3], rt[3];
+    brownian_amplitudes(g, b.brownTransScale[s], b.brownRotScale[s], mag, gT, gR, rf, rt);
+    for (int k = 0; k < 3; k++) { b.randForce[k * n + s] = rf[k]; b.randTorque[k * n + s] = rt[k]; }
+}
+
 // ---------------------------------------------------------------- phase A
 __device__ void phase_publish_bin(const FusedArgs& a, int t) {
     const sbx_dense_scene& sc = a.sc;
@@ -89,8 +121,16 @@ __device__ void phase_publish_bin(const FusedArgs& a, int t) {
     const int nSeg = a.nSeg, nM = a.nM, nB = a.nB, cap = a.cap;
     const float* gp = g.gridParams;
     const int nX = a.nX, nY = a.nY, nZ = a.nZ;
-    const int total = cap + (a.xlOn ? a.nL : 0);
+    const int nLk = a.xlOn ? a.nL : 0;
+    const int total = cap + nLk + nB + a.nBb;
     for (int i = gtid(); i < total; i += gthreads()) {
+        if (i >= cap + nLk) {
+            // BrownianForceSystem for the motor sub-bodies, then the backbones
+            int j = i - cap - nLk;
+            if (j < nB) brownian_slot(mb, j, t, sc.seed, sc.mot.bodyParams[1]);
+            else brownian_slot(sc.mini.backbone, j - nB, t, sc.seedBb, sc.mini.bbBodyParams[1]);
+            continue;
+        }
         if (i < nSeg) {
             float c[3] = {fb.coord[i], fb.coord[nSeg + i], fb.coord[2 * nSeg + i]};
             g.center[i] = c[0]; g.center[cap + i] = c[1]; g.center[2 * cap + i] = c[2];
@@ -329,7 +369,12 @@ __device__ int reach_walk_sorted(const FusedArgs& a, int m, float mx, float my, 
     return cnt;
 }
 
-__device__ void mini_unit(const FusedArgs& a, int u, int t) {
+// One minifilament per CTA. Stage 1: warp 0 runs binding for the heads while warps 1-3
+// evaluate every position-only term of the myosin mechanics (motor joints, dimer coupling
+// variants and lever torsion, tethers), none of which depends on this step's binding.
+// Stage 2: each sub-body accumulates its terms in the order of the reference's System
+// sequence (joints, coupling, tether; the head's bond after its joint). Stage 3: integrate.
+__device__ void mini_unit(const FusedArgs& a, MiniSmem& ms, int u, int t) {
     const sbx_dense_scene& sc = a.sc;
     const sbx_motor_store& mot = sc.mot;
     const sbx_rigid_body& mb = mot.body;
@@ -340,112 +385,144 @@ __device__ void mini_unit(const FusedArgs& a, int u, int t) {
     const int dpm = a.dpm, mpm = 2 * dpm, spm = 6 * dpm;
     const int m0 = u * mpm, s0 = u * spm, d0 = u * dpm;
     const int tid = threadIdx.x;
-    __shared__ float sF[3 * FUSED_MAX_SUB], sT[3 * FUSED_MAX_SUB];
+    float* sF = ms.sF;
+    float* sT = ms.sT;
     LocalAcc acc{sF, sT, s0, spm};
     const float* kp = mot.kinParams;
 
-    // F1: binding for this minifilament's heads
-    if (tid < mpm) {
-        int m = m0 + tid;
-        float mx = mot.head[m], my = mot.head[nM + m], mz = mot.head[2 * nM + m];
-        float mux = mot.uVec[m], muy = mot.uVec[nM + m], muz = mot.uVec[2 * nM + m];
-        float rux = mot.rodUVec[m], ruy = mot.rodUVec[nM + m], ruz = mot.rodUVec[2 * nM + m];
-        int* slice = sc.grid.reachSeg + (int64_t)m * MAX_CAND;
-        int rc = reach_walk_sorted(a, m, mx, my, mz, mux, muy, muz, rux, ruy, ruz, slice, kp[7], kp[8]);
-        sc.grid.reachCount[m] = rc;
-        if (rc > MAX_CAND) atomicOr(a.err, ERR_REACH_OVERFLOW);
-        int bs = mot.boundSeg[m], cd = mot.cooldown[m], sb = mot.stats[2 * m], sr = mot.stats[2 * m + 1],
-            cs = mot.capStats[m];
-        release_one(m, bs, cd, sb, sr, cs, mot.forceDotFil[m], mot.forceMag[m], kp, t, sc.seed);
-        if (bs == FREE_BINDABLE) {
-            int best;
-            float arc;
-            if (bind_nearest_scan(m, nM, mot.head, mot.uVec, mot.rodUVec, nSeg, fb.end1, fb.end2, slice, rc, kp[7],
-                                  kp[8], &best, &arc)) {
-                bs = best;
-                mot.bindArc[m] = arc;
+    // ---- stage 1
+    if (tid < 32) {
+        if (tid < mpm) {
+            // BindingDetectionSystem / NucleotideCycleSystem for this head
+            int m = m0 + tid;
+            float mx = mot.head[m], my = mot.head[nM + m], mz = mot.head[2 * nM + m];
+            float mux = mot.uVec[m], muy = mot.uVec[nM + m], muz = mot.uVec[2 * nM + m];
+            float rux = mot.rodUVec[m], ruy = mot.rodUVec[nM + m], ruz = mot.rodUVec[2 * nM + m];
+            int* slice = sc.grid.reachSeg + (int64_t)m * MAX_CAND;
+            int rc = reach_walk_sorted(a, m, mx, my, mz, mux, muy, muz, rux, ruy, ruz, slice, kp[7], kp[8]);
+            sc.grid.reachCount[m] = rc;
+            if (rc > MAX_CAND) atomicOr(a.err, ERR_REACH_OVERFLOW);
+            int bs = mot.boundSeg[m], cd = mot.cooldown[m], sb = mot.stats[2 * m], sr = mot.stats[2 * m + 1],
+                cs = mot.capStats[m];
+            release_one(m, bs, cd, sb, sr, cs, mot.forceDotFil[m], mot.forceMag[m], kp, t, sc.seed);
+            if (bs == FREE_BINDABLE) {
+                int best;
+                float arc;
+                if (bind_nearest_scan(m, nM, mot.head, mot.uVec, mot.rodUVec, nSeg, fb.end1, fb.end2, slice, rc,
+                                      kp[7], kp[8], &best, &arc)) {
+                    bs = best;
+                    mot.bindArc[m] = arc;
+                }
+            }
+            mot.boundSeg[m] = bs; mot.cooldown[m] = cd; mot.stats[2 * m] = sb; mot.stats[2 * m + 1] = sr;
+            mot.capStats[m] = cs;
+            mot.nucleotideState[m] = cycle_one(m, mot.nucleotideState[m], bs >= 0, mot.forceDotHist + 10 * m,
+                                               mot.nucParams, t, sc.seed);
+            if (bs >= 0) atomicAdd(&a.cntM[bs], 1);
+        }
+    } else if (tid < 96) {
+        // warps 1-2: motor joints (local motor k/2, joint k&1), then a lever (warp 1) or a tether (warp 2)
+        int k = tid - 32;
+        if (k < 2 * mpm)
+            ms.mj[k] = motor_joint(m0 + (k >> 1), k & 1, nB, mb.coord, mb.uVec, mb.segLength, mb.bTransGam,
+                                   mb.bRotGam, mot.jointParams);
+        int dl = k & 31;
+        if (dl < dpm) {
+            int d = d0 + dl;
+            if (k < 32) {
+                ms.lt[dl] = couple_lever(nB, mb.uVec, mb.bRotGam, 2 * d, 2 * d + 1, sc.dim.dimerParams);
+            } else {
+                TetherTerm T = tether_terms(nB, mb.coord, mb.uVec, mb.segLength, mb.bTransGam, mb.bRotGam, nBb,
+                                            bb.coord, bb.uVec, mini.bbInvDragY, u, 2 * d, mini.attachAxial[d],
+                                            mini.miniParams);
+                ms.tt[dl] = T;
+                float* o = mini.miniData + (int64_t)MINI_STRIDE * d;
+                for (int j = 0; j < 6; j++) o[j] = T.row[j];
+                // backbone CSR of the reference (rows = backbones, items = dimers in index order)
+                mini.bbDimerList[d] = d;
             }
         }
-        mot.boundSeg[m] = bs; mot.cooldown[m] = cd; mot.stats[2 * m] = sb; mot.stats[2 * m + 1] = sr;
-        mot.capStats[m] = cs;
-        mot.nucleotideState[m] = cycle_one(m, mot.nucleotideState[m], bs >= 0, mot.forceDotHist + 10 * m,
-                                           mot.nucParams, t, sc.seed);
-        if (bs >= 0) atomicAdd(&a.cntM[bs], 1);
-    }
-    __syncthreads();
-    // F2: Brownian forcing + joints of the 96 sub-bodies; backbone Brownian
-    if (tid < spm) {
-        int s = s0 + tid;
-        float g[6];
-        gauss6_wang(s, t, sc.seed, g);
-        float gT[3] = {mb.bTransGam[s], mb.bTransGam[nB + s], mb.bTransGam[2 * nB + s]};
-        float gR[3] = {mb.bRotGam[s], mb.bRotGam[nB + s], mb.bRotGam[2 * nB + s]};
-        float rf[3], rt[3];
-        brownian_amplitudes(g, mb.brownTransScale[s], mb.brownRotScale[s], mot.bodyParams[1], gT, gR, rf, rt);
-        for (int k = 0; k < 3; k++) { mb.randForce[k * nB + s] = rf[k]; mb.randTorque[k * nB + s] = rt[k]; }
-        double f[3], tq[3];
-        joints_one(s, nB, mb.coord, mb.uVec, mb.segLength, mb.bTransGam, mb.bRotGam, mot.nucleotideState[s / 3],
-                   mot.jointParams, f, tq);
-        for (int k = 0; k < 3; k++) {
-            sF[k * spm + tid] = (float)(0.0 + f[k]);
-            sT[k * spm + tid] = (float)(0.0 + tq[k]);
-        }
-    } else if (tid == spm) {
-        float g[6];
-        gauss6_wang(u, t, sc.seedBb, g);
-        float gT[3] = {bb.bTransGam[u], bb.bTransGam[nBb + u], bb.bTransGam[2 * nBb + u]};
-        float gR[3] = {bb.bRotGam[u], bb.bRotGam[nBb + u], bb.bRotGam[2 * nBb + u]};
-        float rf[3], rt[3];
-        brownian_amplitudes(g, bb.brownTransScale[u], bb.brownRotScale[u], mini.bbBodyParams[1], gT, gR, rf, rt);
-        for (int k = 0; k < 3; k++) { bb.randForce[k * nBb + u] = rf[k]; bb.randTorque[k * nBb + u] = rt[k]; }
-    }
-    __syncthreads();
-    // F3: dimer coupling then tether (per dimer; disjoint sub-bodies)
-    if (tid < dpm) {
-        int d = d0 + tid;
-        couple_one(nB, mb.coord, mb.uVec, mb.segLength, mb.bTransGam, mb.bRotGam, acc, 2 * d, 2 * d + 1,
-                   sc.dim.parallel[d] != 0, sc.dim.dimerParams, mot.boundSeg);
-        tether_one(d, nB, mb.coord, mb.uVec, mb.segLength, mb.bTransGam, mb.bRotGam, acc, nBb, bb.coord, bb.uVec,
-                   mini.bbInvDragY, u, 2 * d, mini.attachAxial[d], mini.miniData, mini.miniParams);
-        // backbone CSR of the reference (rows = backbones, items = dimers in index order)
-        mini.bbDimerList[d] = d;
-    }
-    __syncthreads();
-    // F4 (backbone thread): gather its dimers' reactions, confine, integrate, derive
-    if (tid == spm) {
-        mini.bbDimerCount[u] = dpm;
-        mini.bbDimerOffsets[u] = d0;
-        if (u == nBb - 1) mini.bbDimerOffsets[nBb] = d0 + dpm;
-        // MiniFilamentSystem.backboneGather over this backbone's CSR row (its dimers, ascending)
-        double f[3] = {0, 0, 0}, tq[3] = {0, 0, 0};
-        for (int d = d0; d < d0 + dpm; d++) {
-            const float* p = mini.miniData + (int64_t)d * MINI_STRIDE;
-            f[0] += p[0]; f[1] += p[1]; f[2] += p[2];
-            tq[0] += p[3]; tq[1] += p[4]; tq[2] += p[5];
-        }
-        float F[3], T[3];
-        for (int k = 0; k < 3; k++) { F[k] = (float)(0.0f + f[k]); T[k] = (float)(0.0f + tq[k]); }
-        BoxParams bx = box_params(sc.boxParams, t);
-        float c[3] = {bb.coord[u], bb.coord[nBb + u], bb.coord[2 * nBb + u]};
-        float uu[3] = {bb.uVec[u], bb.uVec[nBb + u], bb.uVec[2 * nBb + u]};
-        if (bx.active) confine_one(bx, c, uu, bb.segLength[u], bb.bTransGam[u], F, T);
-        integrate_derive_store(bb, u, F, T, mini.bbBodyParams[0]);
-    }
-    // F5 (heads): cross-bridge bond, head self-write into the shared sums
-    if (tid < mpm) {
-        int m = m0 + tid;
-        float out[XB_STRIDE];
-        bond_one(m, nB, mb.coord, mb.uVec, mb.yVec, mb.bRotGam, nSeg, fb.coord, fb.uVec, fb.yVec, fb.bRotGam,
-                 fb.segLength, mot.boundSeg[m], mot.bindArc[m], mot.nucleotideState[m], sc.xbParams, out);
-        for (int k = 0; k < XB_STRIDE; k++) sc.bondData[m * XB_STRIDE + k] = out[k];
-        int hl = 3 * m + 2 - s0;
-        for (int k = 0; k < 3; k++) {
-            sF[k * spm + hl] = sF[k * spm + hl] + out[k];
-            sT[k * spm + hl] = sT[k * spm + hl] + out[3 + k];
+    } else {
+        // warp 3: the two end variants of each dimer's rod-rod coupling
+        int q = tid - 96;
+        if (q < 2 * dpm) {
+            int d = d0 + (q >> 1);
+            ms.ct[q] = couple_variant(nB, mb.coord, mb.uVec, mb.segLength, mb.bTransGam, mb.bRotGam, 2 * d,
+                                      2 * d + 1, sc.dim.parallel[d] != 0, sc.dim.dimerParams, q & 1);
         }
     }
     __syncthreads();
-    // F6: integrate + derive the sub-bodies; F7: force-dot registry
+    // ---- stage 2
+    if (tid < 32) {
+        if (tid < mpm) {
+            // CrossBridgeSystem.bondForces, then the head's sums: joint 1, then the bond
+            int m = m0 + tid;
+            float out[XB_STRIDE];
+            bond_one(m, nB, mb.coord, mb.uVec, mb.yVec, mb.bRotGam, nSeg, fb.coord, fb.uVec, fb.yVec, fb.bRotGam,
+                     fb.segLength, mot.boundSeg[m], mot.bindArc[m], mot.nucleotideState[m], sc.xbParams, out);
+            for (int k = 0; k < XB_STRIDE; k++) sc.bondData[m * XB_STRIDE + k] = out[k];
+            int hl = 3 * tid + 2;
+            double f[3] = {0.0, 0.0, 0.0}, tq[3] = {0.0, 0.0, 0.0};
+            motor_joint_apply(ms.mj[2 * tid + 1], 1, true, mot.nucleotideState[m], s0 + hl, nB, mb.uVec,
+                              mb.segLength, mot.jointParams, f, tq);
+            for (int k = 0; k < 3; k++) {
+                float F = (float)(0.0 + f[k]), T = (float)(0.0 + tq[k]);
+                sF[k * spm + hl] = F + out[k];
+                sT[k * spm + hl] = T + out[3 + k];
+            }
+        }
+    } else {
+        int w = tid - 32;
+        if (w < 2 * mpm) {
+            // rods (role 0) and levers (role 1): joints, then dimer coupling, then the tether
+            int ml = w >> 1, role = w & 1;
+            int m = m0 + ml, sl = 3 * ml + role, s = s0 + sl;
+            int nuc = mot.nucleotideState[m];
+            double f[3] = {0.0, 0.0, 0.0}, tq[3] = {0.0, 0.0, 0.0};
+            if (role == 0) {
+                motor_joint_apply(ms.mj[2 * ml], 0, false, nuc, s, nB, mb.uVec, mb.segLength, mot.jointParams, f, tq);
+            } else {
+                motor_joint_apply(ms.mj[2 * ml], 0, true, nuc, s, nB, mb.uVec, mb.segLength, mot.jointParams, f, tq);
+                motor_joint_apply(ms.mj[2 * ml + 1], 1, false, nuc, s, nB, mb.uVec, mb.segLength, mot.jointParams, f,
+                                  tq);
+            }
+            for (int k = 0; k < 3; k++) {
+                sF[k * spm + sl] = (float)(0.0 + f[k]);
+                sT[k * spm + sl] = (float)(0.0 + tq[k]);
+            }
+            int dl = ml >> 1, d = d0 + dl;
+            bool isA = (ml & 1) == 0;            // motorA = 2d, motorB = 2d + 1
+            if (role == 0) {
+                couple_apply_rod(acc, s, isA, ms.ct[2 * dl]);
+                couple_apply_rod(acc, s, isA, ms.ct[2 * dl + 1]);
+                if (isA) tether_apply(acc, s, ms.tt[dl]);
+            } else {
+                bool bothBound = mot.boundSeg[2 * d] >= 0 && mot.boundSeg[2 * d + 1] >= 0;
+                if (sc.dim.parallel[d] != 0 && !bothBound) couple_apply_lever(acc, s, isA, ms.lt[dl]);
+            }
+        } else if (w == 2 * mpm) {
+            // the backbone: gather its dimers' reactions, confine, integrate, derive
+            mini.bbDimerCount[u] = dpm;
+            mini.bbDimerOffsets[u] = d0;
+            if (u == nBb - 1) mini.bbDimerOffsets[nBb] = d0 + dpm;
+            // MiniFilamentSystem.backboneGather over this backbone's CSR row (its dimers, ascending)
+            double f[3] = {0, 0, 0}, tq[3] = {0, 0, 0};
+            for (int d = d0; d < d0 + dpm; d++) {
+                const float* p = mini.miniData + (int64_t)d * MINI_STRIDE;
+                f[0] += p[0]; f[1] += p[1]; f[2] += p[2];
+                tq[0] += p[3]; tq[1] += p[4]; tq[2] += p[5];
+            }
+            float F[3], T[3];
+            for (int k = 0; k < 3; k++) { F[k] = (float)(0.0f + f[k]); T[k] = (float)(0.0f + tq[k]); }
+            BoxParams bx = box_params(sc.boxParams, t);
+            float c[3] = {bb.coord[u], bb.coord[nBb + u], bb.coord[2 * nBb + u]};
+            float uu[3] = {bb.uVec[u], bb.uVec[nBb + u], bb.uVec[2 * nBb + u]};
+            if (bx.active) confine_one(bx, c, uu, bb.segLength[u], bb.bTransGam[u], F, T);
+            integrate_derive_store(bb, u, F, T, mini.bbBodyParams[0]);
+        }
+    }
+    __syncthreads();
+    // ---- stage 3: integrate + derive the sub-bodies; force-dot registry
     if (tid < spm) {
         int s = s0 + tid;
         float F[3] = {sF[tid], sF[spm + tid], sF[2 * spm + tid]};
@@ -474,37 +551,27 @@ __device__ void link_item(const FusedArgs& a, int k) {
                          xl.torqueMagPlace, xl.xlinkData, xl.torsionParams[0]);
 }
 
-__device__ void phase_motors_links(const FusedArgs& a, int t) {
+__device__ void phase_motors_links(const FusedArgs& a, FusedSmem& sm, int t) {
     int linkChunks = a.xlOn ? (a.nL + blockDim.x - 1) / blockDim.x : 0;
     int units = a.nBb + linkChunks;
     for (int w = blockIdx.x; w < units; w += gridDim.x) {
         if (w < a.nBb) {
-            mini_unit(a, w, t);
+            mini_unit(a, sm.mini, w, t);
         } else {
             int k = (w - a.nBb) * blockDim.x + threadIdx.x;
             if (k < a.nL) link_item(a, k);
         }
     }
+    // filament Brownian forcing on the CTAs without a unit (all CTAs when there are none)
+    const sbx_filament_store& fs = a.sc.fil;
+    int helpers = (int)gridDim.x - units, h0 = units;
+    if (helpers <= 0) { helpers = gridDim.x; h0 = 0; }
+    if ((int)blockIdx.x >= h0)
+        for (int i = ((int)blockIdx.x - h0) * blockDim.x + threadIdx.x; i < a.nSeg; i += helpers * blockDim.x)
+            brownian_slot(fs.body, i, t, a.filSeed, fs.params[1]);
     // the reference's activeLinkCount array holds this step's counts
     if (a.xlOn)
         for (int s = gtid(); s < a.nSeg; s += gthreads()) a.sc.xl.activeLinkCount[s] = a.cntAct[s];
-}
-
-// ---------------------------------------------------------------- G: filament Brownian
-__device__ void phase_fil_brownian(const FusedArgs& a, int t) {
-    const sbx_rigid_body& fb = a.sc.fil.body;
-    int n = a.nSeg;
-    int seed = a.filSeed;
-    float mag = a.sc.fil.params[1];
-    for (int i = gtid(); i < n; i += gthreads()) {
-        float g[6];
-        gauss6_wang(i, t, seed, g);
-        float gT[3] = {fb.bTransGam[i], fb.bTransGam[n + i], fb.bTransGam[2 * n + i]};
-        float gR[3] = {fb.bRotGam[i], fb.bRotGam[n + i], fb.bRotGam[2 * n + i]};
-        float rf[3], rt[3];
-        brownian_amplitudes(g, fb.brownTransScale[i], fb.brownRotScale[i], mag, gT, gR, rf, rt);
-        for (int k = 0; k < 3; k++) { fb.randForce[k * n + i] = rf[k]; fb.randTorque[k * n + i] = rt[k]; }
-    }
 }
 
 __device__ void phase_motor_scatter(const FusedArgs& a) {
@@ -534,7 +601,31 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                  :: "r"(d), "l"(src), "r"(bytes), "r"(b) : "memory");
 }
 
-__device__ void rod_unit(const FusedArgs& a, int u, int t, uint64_t* mbar, unsigned& phase) {
+// FP64 row sum of CSR c for local rod l, from the fetched entries (global past the cap);
+// the arithmetic of csr_gather_row
+__device__ __forceinline__ void gather_staged(const RodSmem& rs, int c, int l, int eBase, const int* list,
+                                              const float* payload, int stride, int poff, const int* guard,
+                                              double f[3], double t[3]) {
+    f[0] = f[1] = f[2] = 0.0;
+    t[0] = t[1] = t[2] = 0.0;
+    int k0 = rs.off[c][0];
+    for (int k = rs.off[c][l]; k < rs.off[c][l + 1]; k++) {
+        int e = eBase + (k - k0);
+        const float* p;
+        if (e < FUSED_ENT_CAP) {
+            if (!rs.entOk[e]) continue;
+            p = rs.ent[e];
+        } else {
+            int li = list[k];
+            if (guard && guard[li] < 0) continue;
+            p = payload + (int64_t)li * stride + poff;
+        }
+        f[0] += p[0]; f[1] += p[1]; f[2] += p[2];
+        t[0] += p[3]; t[1] += p[4]; t[2] += p[5];
+    }
+}
+
+__device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t* mbar, unsigned& phase) {
     const sbx_dense_scene& sc = a.sc;
     const sbx_filament_store& f = sc.fil;
     const sbx_rigid_body& fb = f.body;
@@ -544,9 +635,8 @@ __device__ void rod_unit(const FusedArgs& a, int u, int t, uint64_t* mbar, unsig
     const int cnt = min(G, n - g0);
     const int tid = threadIdx.x;
     // staged rod geometry: coord xyz, uVec xyz, segLength, bTransGam x y, bRotGam y
-    __shared__ __align__(16) float st[10 * FUSED_MAX_ROD];
     float* sc_[10];
-    for (int k = 0; k < 10; k++) sc_[k] = st + k * FUSED_MAX_ROD;
+    for (int k = 0; k < 10; k++) sc_[k] = rs.st + k * FUSED_MAX_ROD;
     const float* src[10] = {fb.coord + g0, fb.coord + n + g0, fb.coord + 2 * n + g0, fb.uVec + g0, fb.uVec + n + g0,
                             fb.uVec + 2 * n + g0, fb.segLength + g0, fb.bTransGam + g0, fb.bTransGam + n + g0,
                             fb.bRotGam + n + g0};
@@ -561,6 +651,20 @@ __device__ void rod_unit(const FusedArgs& a, int u, int t, uint64_t* mbar, unsig
             asm volatile("mbarrier.arrive.expect_tx.shared.b64 _, [%0], %1;\n" :: "r"(mb), "r"(bytes * 10u) : "memory");
             for (int k = 0; k < 10; k++) bulk_g2s(sc_[k], src[k], bytes, mbar);
         }
+    }
+    // the group's CSR row offsets, while the bulk copies run
+    const int* offSrc[3] = {xl.segOffsetsA, xl.segOffsetsB, sc.segMotorOffsets};
+    for (int j = tid; j < 3 * (cnt + 1); j += blockDim.x) {
+        int c = j / (cnt + 1), r = j - c * (cnt + 1);
+        if (c == 2 || a.xlOn) rs.off[c][r] = offSrc[c][g0 + r];
+    }
+    int i = g0 + tid;
+    int s2 = -1, n2 = 0, s1 = -1, n1 = 0;
+    if (tid < cnt) {
+        s2 = f.end2NbrSlot[i]; n2 = f.end2NbrSide[i];
+        s1 = f.end1NbrSlot[i]; n1 = f.end1NbrSide[i];
+    }
+    if (tma) {
         // bounded wait on the transaction barrier
         unsigned mb = (unsigned)__cvta_generic_to_shared(mbar);
         long long it = 0;
@@ -581,34 +685,72 @@ __device__ void rod_unit(const FusedArgs& a, int u, int t, uint64_t* mbar, unsig
             for (int j = tid; j < cnt; j += blockDim.x) sc_[k][j] = src[k][j];
     }
     __syncthreads();
+    ChainParams cp = chain_params(f.chainParams);
+    auto rod = [&](int j) {
+        int l = j - g0;
+        RodGeom r;
+        r.cx = sc_[0][l]; r.cy = sc_[1][l]; r.cz = sc_[2][l];
+        r.ux = sc_[3][l]; r.uy = sc_[4][l]; r.uz = sc_[5][l];
+        r.len = sc_[6][l];
+        r.bTGx = sc_[7][l]; r.bTGy = sc_[8][l]; r.bRGy = sc_[9][l];
+        return r;
+    };
+    // each joint once, by its lower-slot rod
+    if (a.jointShare && tid < cnt) {
+        RodGeom me = rod(i);
+        if (s2 > i) rs.js[2 * tid + 0] = chain_joint(cp, i, 0, s2, n2, me, rod(s2));
+        if (s1 > i) rs.js[2 * tid + 1] = chain_joint(cp, i, 1, s1, n1, me, rod(s1));
+    }
+    // the CSR payloads of the group's rows (link A, link B, motor), one entry per thread
+    const int eA = a.xlOn ? rs.off[0][cnt] - rs.off[0][0] : 0;
+    const int eB = a.xlOn ? rs.off[1][cnt] - rs.off[1][0] : 0;
+    const int eM = rs.off[2][cnt] - rs.off[2][0];
+    const int eLim = min(eA + eB + eM, FUSED_ENT_CAP);
+    for (int e = (tid - cnt + (int)blockDim.x) % (int)blockDim.x; e < eLim; e += blockDim.x) {
+        const float* p;
+        bool ok = true;
+        if (e < eA) {
+            int li = xl.segIdxA[rs.off[0][0] + e];
+            ok = xl.linkState[li] >= 0;
+            p = xl.xlinkData + (int64_t)li * XL_STRIDE;
+        } else if (e < eA + eB) {
+            int li = xl.segIdxB[rs.off[1][0] + (e - eA)];
+            ok = xl.linkState[li] >= 0;
+            p = xl.xlinkData + (int64_t)li * XL_STRIDE + 6;
+        } else {
+            int li = sc.segMotorMyo[rs.off[2][0] + (e - eA - eB)];
+            p = sc.bondData + (int64_t)li * XB_STRIDE + 6;
+        }
+        float v[6];
+        for (int k = 0; k < 6; k++) v[k] = p[k];
+        for (int k = 0; k < 6; k++) rs.ent[e][k] = ok ? v[k] : 0.f;
+        rs.entOk[e] = ok;
+    }
+    __syncthreads();
     if (tid < cnt) {
-        int i = g0 + tid;
-        ChainParams cp = chain_params(f.chainParams);
-        auto rod = [&](int j) {
-            int l = j - g0;
-            RodGeom r;
-            r.cx = sc_[0][l]; r.cy = sc_[1][l]; r.cz = sc_[2][l];
-            r.ux = sc_[3][l]; r.uy = sc_[4][l]; r.uz = sc_[5][l];
-            r.len = sc_[6][l];
-            r.bTGx = sc_[7][l]; r.bTGy = sc_[8][l]; r.bRGy = sc_[9][l];
-            return r;
-        };
         RodGeom me = rod(i);
         double fd[3] = {0, 0, 0}, td[3] = {0, 0, 0};
-        int s2 = f.end2NbrSlot[i];
-        if (s2 >= 0) chain_side(cp, i, 0, s2, f.end2NbrSide[i], me, rod(s2), fd, td);
-        int s1 = f.end1NbrSlot[i];
-        if (s1 >= 0) chain_side(cp, i, 1, s1, f.end1NbrSide[i], me, rod(s1), fd, td);
+        if (a.jointShare) {
+            if (s2 >= 0)
+                chain_apply(cp, i, 0, s2, n2, me, rod(s2), s2 > i ? rs.js[2 * tid] : rs.js[2 * (s2 - g0) + (1 - n2)],
+                            fd, td);
+            if (s1 >= 0)
+                chain_apply(cp, i, 1, s1, n1, me, rod(s1),
+                            s1 > i ? rs.js[2 * tid + 1] : rs.js[2 * (s1 - g0) + (1 - n1)], fd, td);
+        } else {
+            if (s2 >= 0) chain_side(cp, i, 0, s2, n2, me, rod(s2), fd, td);
+            if (s1 >= 0) chain_side(cp, i, 1, s1, n1, me, rod(s1), fd, td);
+        }
         float F[3], T[3];
         for (int k = 0; k < 3; k++) { F[k] = (float)(0.0f + fd[k]); T[k] = (float)(0.0f + td[k]); }
         double gf[3], gt[3];
         if (a.xlOn) {
-            csr_gather_row(i, xl.segOffsetsA, xl.segIdxA, xl.xlinkData, XL_STRIDE, 0, xl.linkState, gf, gt);
+            gather_staged(rs, 0, tid, 0, xl.segIdxA, xl.xlinkData, XL_STRIDE, 0, xl.linkState, gf, gt);
             for (int k = 0; k < 3; k++) { F[k] = (float)(F[k] + gf[k]); T[k] = (float)(T[k] + gt[k]); }
-            csr_gather_row(i, xl.segOffsetsB, xl.segIdxB, xl.xlinkData, XL_STRIDE, 6, xl.linkState, gf, gt);
+            gather_staged(rs, 1, tid, eA, xl.segIdxB, xl.xlinkData, XL_STRIDE, 6, xl.linkState, gf, gt);
             for (int k = 0; k < 3; k++) { F[k] = (float)(F[k] + gf[k]); T[k] = (float)(T[k] + gt[k]); }
         }
-        csr_gather_row(i, sc.segMotorOffsets, sc.segMotorMyo, sc.bondData, XB_STRIDE, 6, nullptr, gf, gt);
+        gather_staged(rs, 2, tid, eA + eB, sc.segMotorMyo, sc.bondData, XB_STRIDE, 6, nullptr, gf, gt);
         for (int k = 0; k < 3; k++) { F[k] = (float)(F[k] + gf[k]); T[k] = (float)(T[k] + gt[k]); }
         BoxParams bx = box_params(sc.boxParams, t);
         float c[3] = {sc_[0][tid], sc_[1][tid], sc_[2][tid]};
@@ -618,8 +760,8 @@ __device__ void rod_unit(const FusedArgs& a, int u, int t, uint64_t* mbar, unsig
     }
 }
 
-__device__ void phase_rods(const FusedArgs& a, int t, uint64_t* mbar, unsigned& phase) {
-    for (int u = blockIdx.x; u < a.nRodUnits; u += gridDim.x) rod_unit(a, u, t, mbar, phase);
+__device__ void phase_rods(const FusedArgs& a, FusedSmem& sm, int t, uint64_t* mbar, unsigned& phase) {
+    for (int u = blockIdx.x; u < a.nRodUnits; u += gridDim.x) rod_unit(a, sm.rod, u, t, mbar, phase);
     // reset the private histograms for the next step
     for (int i = gtid(); i < a.C; i += gthreads()) a.cntCell[i] = 0;
     for (int i = gtid(); i < a.nSeg; i += gthreads()) {
@@ -629,6 +771,7 @@ __device__ void phase_rods(const FusedArgs& a, int t, uint64_t* mbar, unsigned& 
 
 __global__ void __launch_bounds__(FUSED_THREADS) k_dense_fused(FusedArgs a, int t0, int nsteps) {
     __shared__ __align__(8) uint64_t mbar;
+    __shared__ __align__(16) FusedSmem sm;
     unsigned phase = 0;
     if (threadIdx.x == 0) {
         unsigned mb = (unsigned)__cvta_generic_to_shared(&mbar);
@@ -680,11 +823,10 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_dense_fused(FusedArgs a, int 
         phase_rank(a);
         if (!grid_sync(a)) return;
         stamp(s);
-        phase_motors_links(a, t);
+        phase_motors_links(a, sm, t);
         if (!grid_sync(a)) return;
         stamp(s);
         tile_sums(second, 1, a.tileSum);
-        phase_fil_brownian(a, t);
         if (!grid_sync(a)) return;
         stamp(s);
         tile_scan(second, 1, a.tileSum, out2, zero2, clamp2, nullptr);
@@ -696,7 +838,7 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_dense_fused(FusedArgs a, int 
         phase_motor_rank(a);
         if (!grid_sync(a)) return;
         stamp(s);
-        phase_rods(a, t, &mbar, phase);
+        phase_rods(a, sm, t, &mbar, phase);
         if (!grid_sync(a)) return;
         stamp(s);
     }

@@ -6,6 +6,8 @@
 constexpr int FUSED_THREADS = 128;
 constexpr int FUSED_MAX_SUB = 120;    // sub-bodies per minifilament CTA (6 per dimer)
 constexpr int FUSED_MAX_ROD = 128;    // segments per rod CTA
+constexpr int FUSED_MAX_DPM = 16;     // dimers per minifilament (32 heads: one warp)
+constexpr int FUSED_ENT_CAP = 256;    // CSR payload entries a rod CTA stages in shared memory
 
 struct FusedArgs {
     sbx_dense_scene sc;
@@ -15,6 +17,7 @@ struct FusedArgs {
     int G, nRodUnits;        // segments per rod unit (whole filaments), units
     int tilesC, tilesS;
     int xlOn, xlUnbind, useTma, filSeed;
+    int jointShare;          // chain neighbours are symmetric: each joint computed once
     // private scratch (plan-owned)
     int *cntCell, *cntAct, *cntA, *cntB, *cntM;
     int* tileSum;

@@ -96,22 +96,35 @@ SBX_HD double reduce_pio2(double x, int* quadrant) {
 
 SBX_HD double sin(double x) {
     int q; double r = reduce_pio2(x, &q);
+#ifdef __CUDA_ARCH__
+    // both polynomials and a select: lanes in different quadrants do not diverge
+    double sp = sin_poly(r), cp = cos_poly(r);
+    double v = (q & 1) ? cp : sp;
+    return (q & 2) ? -v : v;
+#else
     switch (q) {
         case 0: return sin_poly(r);
         case 1: return cos_poly(r);
         case 2: return -sin_poly(r);
         default: return -cos_poly(r);
     }
+#endif
 }
 
 SBX_HD double cos(double x) {
     int q; double r = reduce_pio2(x, &q);
+#ifdef __CUDA_ARCH__
+    double sp = sin_poly(r), cp = cos_poly(r);
+    double v = (q & 1) ? sp : cp;
+    return ((q + 1) & 2) ? -v : v;
+#else
     switch (q) {
         case 0: return cos_poly(r);
         case 1: return -sin_poly(r);
         case 2: return -cos_poly(r);
         default: return sin_poly(r);
     }
+#endif
 }
 
 // natural log of a positive double (x <= 0 -> -inf / NaN like libm)

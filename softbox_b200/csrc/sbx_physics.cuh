@@ -306,12 +306,22 @@ struct RodGeom {        // the per-rod reads of ChainBendingForceSystem.java:136
     double cx, cy, cz, ux, uy, uz, len, bTGx, bTGy, bRGy;
 };
 
-// One joint side (side 0 = end2 block :152-235, side 1 = end1 block :237-321) of rod i
-// with neighbour `slot` attached at its `nside`; accumulates into f/t (double).
-SBX_DEV void chain_side(const ChainParams& cp, int i, int side, int slot, int nside, const RodGeom& r,
-                        const RodGeom& nb, double f[3], double t[3]) {
-    const double DEG2RAD = PI_D / 180.0;
+// A chain joint seen from rod i's `side` (side 0 = end2 block :152-235, side 1 = end1 block
+// :237-321) with neighbour `slot` attached at its `nside` (0 = the neighbour's end1).
+// chain_joint holds the costly scalars of the joint; both rods of a joint get the same
+// values: seen from the neighbour (side' = 1 - nside, nside' = 1 - side) the strain points,
+// the two moveC terms (swapped, and summed commutatively), the torsion axis (negated) and
+// the bend angle come out bit-identical.
+struct ChainJoint {
+    double forceMag, luX, luY, luZ, invMag, torsionMag;
+    int tvOK;
+};
+
+SBX_DEV ChainJoint chain_joint(const ChainParams& cp, int i, int side, int slot, int nside, const RodGeom& r,
+                               const RodGeom& nb) {
     const double RAD2DEG = 180.0 / PI_D;
+    const double DEG2RAD = PI_D / 180.0;
+    ChainJoint J;
     double halfLen_um = 0.5 * r.len;
     double lSqSelf = 1.0e-12 * r.len * r.len;
     double nHalfLen_um = 0.5 * nb.len;
@@ -353,34 +363,57 @@ SBX_DEV void chain_side(const ChainParams& cp, int i, int side, int slot, int ns
     double cosA2_2 = cosA2 * cosA2;
     double moveC2 = cosB2 * cosB2 / nb.bTGx + cosA2_2 / nb.bTGy + lSqN * cosA2_2 / (4.0 * nb.bRGy);
     double denom = cp.dt * (moveC1 + moveC2);
-    double forceMag = (denom > 0.0) ? (cp.fracMove * 1.0e-6 * strainDist / denom) : 0.0;
-    double fSign = owner ? 1.0 : -1.0;
-    double Fx = fSign * forceMag * luX, Fy = fSign * forceMag * luY, Fz = fSign * forceMag * luZ;
-    f[0] += Fx; f[1] += Fy; f[2] += Fz;
-    double Rscale = (side == 0) ? (0.5e-6 * r.len * cp.fracR) : (-0.5e-6 * r.len * cp.fracR);
-    double Rx = Rscale * r.ux, Ry = Rscale * r.uy, Rz = Rscale * r.uz;
-    t[0] += Ry * Fz - Rz * Fy; t[1] += Rz * Fx - Rx * Fz; t[2] += Rx * Fy - Ry * Fx;
+    J.forceMag = (denom > 0.0) ? (cp.fracMove * 1.0e-6 * strainDist / denom) : 0.0;
+    J.luX = luX; J.luY = luY; J.luZ = luZ;
 
     double nxE = (nside == 0) ? nb.ux : -nb.ux, nyE = (nside == 0) ? nb.uy : -nb.uy, nzE = (nside == 0) ? nb.uz : -nb.uz;
     double mux = (side == 0) ? r.ux : -r.ux, muy = (side == 0) ? r.uy : -r.uy, muz = (side == 0) ? r.uz : -r.uz;
     double tvx = muy * nzE - muz * nyE, tvy = muz * nxE - mux * nzE, tvz = mux * nyE - muy * nxE;
     double tvMag2 = tvx * tvx + tvy * tvy + tvz * tvz;
-    if (tvMag2 > 1.0e-30) {
-        double invMag = 1.0 / sqrt(tvMag2);
-        tvx *= invMag; tvy *= invMag; tvz *= invMag;
+    J.tvOK = tvMag2 > 1.0e-30;
+    J.invMag = 0.0;
+    J.torsionMag = 0.0;
+    if (J.tvOK) {
+        J.invMag = 1.0 / sqrt(tvMag2);
         double dotV = mux * nxE + muy * nyE + muz * nzE;
         if (dotV > 1.0) dotV = 1.0;
         if (dotV < -1.0) dotV = -1.0;
         double angTween = angle_from_sin_cos(tvMag2, dotV) * RAD2DEG;
-        double torsionMag;
         if (cp.springActive > 0.5) {
-            torsionMag = cp.fracMoveTorq * cp.spring * angTween;
+            J.torsionMag = cp.fracMoveTorq * cp.spring * angTween;
         } else {
             double invBRG = 1.0 / r.bRGy + 1.0 / nb.bRGy;
-            torsionMag = cp.fracMoveTorq * DEG2RAD * angTween / (invBRG * cp.dt);
+            J.torsionMag = cp.fracMoveTorq * DEG2RAD * angTween / (invBRG * cp.dt);
         }
-        t[0] += tvx * torsionMag; t[1] += tvy * torsionMag; t[2] += tvz * torsionMag;
     }
+    return J;
+}
+
+// Accumulates joint J into rod i's double force/torque sums from its own side.
+SBX_DEV void chain_apply(const ChainParams& cp, int i, int side, int slot, int nside, const RodGeom& r,
+                         const RodGeom& nb, const ChainJoint& J, double f[3], double t[3]) {
+    bool owner = i < slot;
+    double fSign = owner ? 1.0 : -1.0;
+    double Fx = fSign * J.forceMag * J.luX, Fy = fSign * J.forceMag * J.luY, Fz = fSign * J.forceMag * J.luZ;
+    f[0] += Fx; f[1] += Fy; f[2] += Fz;
+    double Rscale = (side == 0) ? (0.5e-6 * r.len * cp.fracR) : (-0.5e-6 * r.len * cp.fracR);
+    double Rx = Rscale * r.ux, Ry = Rscale * r.uy, Rz = Rscale * r.uz;
+    t[0] += Ry * Fz - Rz * Fy; t[1] += Rz * Fx - Rx * Fz; t[2] += Rx * Fy - Ry * Fx;
+    if (J.tvOK) {
+        double nxE = (nside == 0) ? nb.ux : -nb.ux, nyE = (nside == 0) ? nb.uy : -nb.uy,
+               nzE = (nside == 0) ? nb.uz : -nb.uz;
+        double mux = (side == 0) ? r.ux : -r.ux, muy = (side == 0) ? r.uy : -r.uy, muz = (side == 0) ? r.uz : -r.uz;
+        double tvx = muy * nzE - muz * nyE, tvy = muz * nxE - mux * nzE, tvz = mux * nyE - muy * nxE;
+        tvx *= J.invMag; tvy *= J.invMag; tvz *= J.invMag;
+        t[0] += tvx * J.torsionMag; t[1] += tvy * J.torsionMag; t[2] += tvz * J.torsionMag;
+    }
+}
+
+// One joint side of rod i, accumulated into f/t (ChainBendingForceSystem.java:152-321)
+SBX_DEV void chain_side(const ChainParams& cp, int i, int side, int slot, int nside, const RodGeom& r,
+                        const RodGeom& nb, double f[3], double t[3]) {
+    ChainJoint J = chain_joint(cp, i, side, slot, nside, r, nb);
+    chain_apply(cp, i, side, slot, nside, r, nb, J, f, t);
 }
 
 SBX_DEV RodGeom load_rod(int n, int i, const float* coord, const float* uVec, const float* segLength,
@@ -785,104 +818,104 @@ SBX_DEV bool unbind_one(int k, int nSeg, const float* fU, const float* fE1, int 
 }
 
 // MotorJointSystem.joints per sub-body (MotorJointSystem.java:88-190) -> f, t (double)
-SBX_DEV void joints_one(int s, int nB, const float* coord, const float* uVec, const float* segLength,
-                        const float* bTG, const float* bRG, int nucState, const float* jp, double f[3], double t[3]) {
+// One motor joint (MotorJointSystem.java:86-197): which = 0 is joint 2 (rod-lever),
+// which = 1 is joint 1 (lever-head). The position-only part, shared by the joint's two
+// bodies; tm[0] / tm[1] are the torsion magnitudes for a nucleotide state other than /
+// equal to ADP.Pi (joint 1's rest angle 60 / 0 degrees; joint 2 has one rest angle).
+struct MotorJoint {
+    double forceMag, lx, ly, lz, tvx, tvy, tvz, tm[2];
+};
+
+SBX_DEV MotorJoint motor_joint(int m, int which, int nB, const float* coord, const float* uVec,
+                               const float* segLength, const float* bTG, const float* bRG, const float* jp) {
     const double DEG2RAD = PI_D / 180.0, RAD2DEG = 180.0 / PI_D;
     double dt = jp[0];
-    double j1FracMove = jp[1], j1FracR = jp[2], j1FracMoveTorq = jp[3];
-    double j2FracMove = jp[5], j2FracR = jp[6], j2FracMoveTorq = jp[7], j2Rest = jp[8];
-    double stallPN = jp[10];
+    int a = 3 * m + which, b = a + 1;           // (rod, lever) or (lever, head)
+    double fracMove = which == 0 ? (double)jp[5] : (double)jp[1];
+    double fracMoveTorq = which == 0 ? (double)jp[7] : (double)jp[3];
+    double acx = coord[a], acy = coord[nB + a], acz = coord[2 * nB + a];
+    double aux = uVec[a], auy = uVec[nB + a], auz = uVec[2 * nB + a];
+    double alen = segLength[a];
+    double bcx = coord[b], bcy = coord[nB + b], bcz = coord[2 * nB + b];
+    double bux = uVec[b], buy = uVec[nB + b], buz = uVec[2 * nB + b];
+    double blen = segLength[b];
+    MotorJoint J;
+    double aEx = acx + 0.5 * alen * aux, aEy = acy + 0.5 * alen * auy, aEz = acz + 0.5 * alen * auz;
+    double bEx = bcx - 0.5 * blen * bux, bEy = bcy - 0.5 * blen * buy, bEz = bcz - 0.5 * blen * buz;
+    double dx = aEx - bEx, dy = aEy - bEy, dz = aEz - bEz;
+    double strain = sqrt(dx * dx + dy * dy + dz * dz);
+    double inv = (strain > 0.0) ? 1.0 / strain : 0.0;
+    double lx = dx * inv, ly = dy * inv, lz = dz * inv;
+    double mcA = move_c(aux, auy, auz, lx, ly, lz, bTG[a], bTG[nB + a], bRG[nB + a], alen);
+    double mcB = move_c(bux, buy, buz, lx, ly, lz, bTG[b], bTG[nB + b], bRG[nB + b], blen);
+    double denom = dt * (mcA + mcB);
+    J.forceMag = (denom > 0.0) ? (fracMove * 1.0e-6 * strain / denom) : 0.0;
+    J.lx = lx; J.ly = ly; J.lz = lz;
+    double tvx = auy * buz - auz * buy, tvy = auz * bux - aux * buz, tvz = aux * buy - auy * bux;
+    double tvm2 = tvx * tvx + tvy * tvy + tvz * tvz;
+    J.tm[0] = J.tm[1] = 0.0;
+    if (tvm2 > 1.0e-30) {
+        double im = 1.0 / sqrt(tvm2);
+        tvx *= im; tvy *= im; tvz *= im;
+        double dotV = aux * bux + auy * buy + auz * buz;
+        if (dotV > 1.0) dotV = 1.0;
+        if (dotV < -1.0) dotV = -1.0;
+        double ang = accurate_acos(dotV) * RAD2DEG;
+        double invBRG = 1.0 / bRG[nB + a] + 1.0 / bRG[nB + b];
+        if (which == 0) {
+            double j2Rest = jp[8];
+            J.tm[0] = J.tm[1] = fracMoveTorq * DEG2RAD * (ang - j2Rest) / (invBRG * dt);
+        } else {
+            double maxMag = (double)jp[10] * 0.5 * blen * 1.0e-18;
+            for (int r = 0; r < 2; r++) {
+                double j1Rest = r == 0 ? 60.0 : 0.0;
+                double tmag = fracMoveTorq * DEG2RAD * (ang - j1Rest) / (invBRG * dt);
+                if (tmag > maxMag) tmag = maxMag;
+                J.tm[r] = tmag;
+            }
+        }
+    }
+    J.tvx = tvx; J.tvy = tvy; J.tvz = tvz;
+    return J;
+}
+
+// Adds joint J to body `s` (one of its two bodies; `second` = the lever of joint 2 or the
+// head of joint 1) in double, the sequence of MotorJointSystem.java:124-137 / :175-188.
+SBX_DEV void motor_joint_apply(const MotorJoint& J, int which, bool second, int nucState, int s, int nB,
+                               const float* uVec, const float* segLength, const float* jp, double f[3],
+                               double t[3]) {
+    double fracR = which == 0 ? (double)jp[6] : (double)jp[2];
+    double tm = J.tm[(which == 1 && nucState == NUC_ADPPI) ? 1 : 0];
+    double ux = uVec[s], uy = uVec[nB + s], uz = uVec[2 * nB + s];
+    double len = segLength[s];
+    if (!second) {
+        double Fx = -J.forceMag * J.lx, Fy = -J.forceMag * J.ly, Fz = -J.forceMag * J.lz;
+        f[0] += Fx; f[1] += Fy; f[2] += Fz;
+        double Rs = 0.5e-6 * len * fracR, Rx = Rs * ux, Ry = Rs * uy, Rz = Rs * uz;
+        t[0] += Ry * Fz - Rz * Fy; t[1] += Rz * Fx - Rx * Fz; t[2] += Rx * Fy - Ry * Fx;
+        t[0] += J.tvx * tm; t[1] += J.tvy * tm; t[2] += J.tvz * tm;
+    } else {
+        double Fx = J.forceMag * J.lx, Fy = J.forceMag * J.ly, Fz = J.forceMag * J.lz;
+        f[0] += Fx; f[1] += Fy; f[2] += Fz;
+        double Rs = -0.5e-6 * len * fracR, Rx = Rs * ux, Ry = Rs * uy, Rz = Rs * uz;
+        t[0] += Ry * Fz - Rz * Fy; t[1] += Rz * Fx - Rx * Fz; t[2] += Rx * Fy - Ry * Fx;
+        t[0] -= J.tvx * tm; t[1] -= J.tvy * tm; t[2] -= J.tvz * tm;
+    }
+}
+
+// MotorJointSystem.joints for one sub-body (role 0 rod, 1 lever, 2 head), from zero
+SBX_DEV void joints_one(int s, int nB, const float* coord, const float* uVec, const float* segLength,
+                        const float* bTG, const float* bRG, int nucState, const float* jp, double f[3], double t[3]) {
     int m = s / 3, role = s - 3 * m;
-    double j1Rest = (nucState != NUC_ADPPI) ? 60.0 : 0.0;
-    int rod = 3 * m, lever = 3 * m + 1, head = 3 * m + 2;
-    double rcx = coord[rod], rcy = coord[nB + rod], rcz = coord[2 * nB + rod];
-    double rux = uVec[rod], ruy = uVec[nB + rod], ruz = uVec[2 * nB + rod];
-    double rlen = segLength[rod];
-    double lcx = coord[lever], lcy = coord[nB + lever], lcz = coord[2 * nB + lever];
-    double lux = uVec[lever], luy = uVec[nB + lever], luz = uVec[2 * nB + lever];
-    double llen = segLength[lever];
-    double hcx = coord[head], hcy = coord[nB + head], hcz = coord[2 * nB + head];
-    double hux = uVec[head], huy = uVec[nB + head], huz = uVec[2 * nB + head];
-    double hlen = segLength[head];
     f[0] = f[1] = f[2] = 0.0;
     t[0] = t[1] = t[2] = 0.0;
     if (role == 0 || role == 1) {
-        double aEx = rcx + 0.5 * rlen * rux, aEy = rcy + 0.5 * rlen * ruy, aEz = rcz + 0.5 * rlen * ruz;
-        double bEx = lcx - 0.5 * llen * lux, bEy = lcy - 0.5 * llen * luy, bEz = lcz - 0.5 * llen * luz;
-        double dx = aEx - bEx, dy = aEy - bEy, dz = aEz - bEz;
-        double strain = sqrt(dx * dx + dy * dy + dz * dz);
-        double inv = (strain > 0.0) ? 1.0 / strain : 0.0;
-        double lx = dx * inv, ly = dy * inv, lz = dz * inv;
-        double mcRod = move_c(rux, ruy, ruz, lx, ly, lz, bTG[rod], bTG[nB + rod], bRG[nB + rod], rlen);
-        double mcLever = move_c(lux, luy, luz, lx, ly, lz, bTG[lever], bTG[nB + lever], bRG[nB + lever], llen);
-        double denom = dt * (mcRod + mcLever);
-        double forceMag = (denom > 0.0) ? (j2FracMove * 1.0e-6 * strain / denom) : 0.0;
-        double tvx = ruy * luz - ruz * luy, tvy = ruz * lux - rux * luz, tvz = rux * luy - ruy * lux;
-        double tvm2 = tvx * tvx + tvy * tvy + tvz * tvz;
-        double torsionMag = 0.0;
-        if (tvm2 > 1.0e-30) {
-            double im = 1.0 / sqrt(tvm2);
-            tvx *= im; tvy *= im; tvz *= im;
-            double dotV = rux * lux + ruy * luy + ruz * luz;
-            if (dotV > 1.0) dotV = 1.0;
-            if (dotV < -1.0) dotV = -1.0;
-            double ang = accurate_acos(dotV) * RAD2DEG;
-            double invBRG = 1.0 / bRG[nB + rod] + 1.0 / bRG[nB + lever];
-            torsionMag = j2FracMoveTorq * DEG2RAD * (ang - j2Rest) / (invBRG * dt);
-        }
-        if (role == 0) {
-            double Fx = -forceMag * lx, Fy = -forceMag * ly, Fz = -forceMag * lz;
-            f[0] += Fx; f[1] += Fy; f[2] += Fz;
-            double Rs = 0.5e-6 * rlen * j2FracR, Rx = Rs * rux, Ry = Rs * ruy, Rz = Rs * ruz;
-            t[0] += Ry * Fz - Rz * Fy; t[1] += Rz * Fx - Rx * Fz; t[2] += Rx * Fy - Ry * Fx;
-            t[0] += tvx * torsionMag; t[1] += tvy * torsionMag; t[2] += tvz * torsionMag;
-        } else {
-            double Fx = forceMag * lx, Fy = forceMag * ly, Fz = forceMag * lz;
-            f[0] += Fx; f[1] += Fy; f[2] += Fz;
-            double Rs = -0.5e-6 * llen * j2FracR, Rx = Rs * lux, Ry = Rs * luy, Rz = Rs * luz;
-            t[0] += Ry * Fz - Rz * Fy; t[1] += Rz * Fx - Rx * Fz; t[2] += Rx * Fy - Ry * Fx;
-            t[0] -= tvx * torsionMag; t[1] -= tvy * torsionMag; t[2] -= tvz * torsionMag;
-        }
+        MotorJoint J = motor_joint(m, 0, nB, coord, uVec, segLength, bTG, bRG, jp);
+        motor_joint_apply(J, 0, role == 1, nucState, s, nB, uVec, segLength, jp, f, t);
     }
     if (role == 1 || role == 2) {
-        double aEx = lcx + 0.5 * llen * lux, aEy = lcy + 0.5 * llen * luy, aEz = lcz + 0.5 * llen * luz;
-        double bEx = hcx - 0.5 * hlen * hux, bEy = hcy - 0.5 * hlen * huy, bEz = hcz - 0.5 * hlen * huz;
-        double dx = aEx - bEx, dy = aEy - bEy, dz = aEz - bEz;
-        double strain = sqrt(dx * dx + dy * dy + dz * dz);
-        double inv = (strain > 0.0) ? 1.0 / strain : 0.0;
-        double lx = dx * inv, ly = dy * inv, lz = dz * inv;
-        double mcLever = move_c(lux, luy, luz, lx, ly, lz, bTG[lever], bTG[nB + lever], bRG[nB + lever], llen);
-        double mcHead = move_c(hux, huy, huz, lx, ly, lz, bTG[head], bTG[nB + head], bRG[nB + head], hlen);
-        double denom = dt * (mcLever + mcHead);
-        double forceMag = (denom > 0.0) ? (j1FracMove * 1.0e-6 * strain / denom) : 0.0;
-        double tvx = luy * huz - luz * huy, tvy = luz * hux - lux * huz, tvz = lux * huy - luy * hux;
-        double tvm2 = tvx * tvx + tvy * tvy + tvz * tvz;
-        double torsionMag = 0.0;
-        if (tvm2 > 1.0e-30) {
-            double im = 1.0 / sqrt(tvm2);
-            tvx *= im; tvy *= im; tvz *= im;
-            double dotV = lux * hux + luy * huy + luz * huz;
-            if (dotV > 1.0) dotV = 1.0;
-            if (dotV < -1.0) dotV = -1.0;
-            double ang = accurate_acos(dotV) * RAD2DEG;
-            double invBRG = 1.0 / bRG[nB + lever] + 1.0 / bRG[nB + head];
-            torsionMag = j1FracMoveTorq * DEG2RAD * (ang - j1Rest) / (invBRG * dt);
-            double maxMag = stallPN * 0.5 * hlen * 1.0e-18;
-            if (torsionMag > maxMag) torsionMag = maxMag;
-        }
-        if (role == 1) {
-            double Fx = -forceMag * lx, Fy = -forceMag * ly, Fz = -forceMag * lz;
-            f[0] += Fx; f[1] += Fy; f[2] += Fz;
-            double Rs = 0.5e-6 * llen * j1FracR, Rx = Rs * lux, Ry = Rs * luy, Rz = Rs * luz;
-            t[0] += Ry * Fz - Rz * Fy; t[1] += Rz * Fx - Rx * Fz; t[2] += Rx * Fy - Ry * Fx;
-            t[0] += tvx * torsionMag; t[1] += tvy * torsionMag; t[2] += tvz * torsionMag;
-        } else {
-            double Fx = forceMag * lx, Fy = forceMag * ly, Fz = forceMag * lz;
-            f[0] += Fx; f[1] += Fy; f[2] += Fz;
-            double Rs = -0.5e-6 * hlen * j1FracR, Rx = Rs * hux, Ry = Rs * huy, Rz = Rs * huz;
-            t[0] += Ry * Fz - Rz * Fy; t[1] += Rz * Fx - Rx * Fz; t[2] += Rx * Fy - Ry * Fx;
-            t[0] -= tvx * torsionMag; t[1] -= tvy * torsionMag; t[2] -= tvz * torsionMag;
-        }
+        MotorJoint J = motor_joint(m, 1, nB, coord, uVec, segLength, bTG, bRG, jp);
+        motor_joint_apply(J, 1, role == 2, nucState, s, nB, uVec, segLength, jp, f, t);
     }
 }
 
@@ -900,90 +933,149 @@ struct LocalAcc {
     SBX_DEV float& t(int k, int s) const { return T[k * stride + (s - base)]; }
 };
 
+// DimerCouplingSystem.couple split into its position-only terms and their ordered
+// accumulation: two end variants (rod-rod pull) and the lever torsion.
+struct CoupleTerm {
+    double FAx, FAy, FAz, TAx, TAy, TAz, TBx, TBy, TBz;
+    int ok;                                      // strain > 0
+};
+struct LeverTerm {
+    double px, py, pz;                           // tv * torsionMag
+    int ok;                                      // tvm2 > 1e-30
+};
+
+SBX_DEV CoupleTerm couple_variant(int nB, const float* coord, const float* uVec, const float* segLength,
+                                  const float* bTG, const float* bRG, int mA, int mB, bool par, const float* dp,
+                                  int variant) {
+    double dt = dp[0], fracMove = dp[1], rodLen = dp[4];
+    int rodA = 3 * mA, rodB = 3 * mB;
+    CoupleTerm C;
+    double endSelA = (variant == 0) ? -1.0 : 1.0;
+    double endSelB = par ? endSelA : -endSelA;
+    double aCx = coord[rodA], aCy = coord[nB + rodA], aCz = coord[2 * nB + rodA];
+    double aUx = uVec[rodA], aUy = uVec[nB + rodA], aUz = uVec[2 * nB + rodA];
+    double bCx = coord[rodB], bCy = coord[nB + rodB], bCz = coord[2 * nB + rodB];
+    double bUx = uVec[rodB], bUy = uVec[nB + rodB], bUz = uVec[2 * nB + rodB];
+    double aLen = segLength[rodA], bLen = segLength[rodB];
+    double pAx = aCx + endSelA * 0.5 * aLen * aUx, pAy = aCy + endSelA * 0.5 * aLen * aUy,
+           pAz = aCz + endSelA * 0.5 * aLen * aUz;
+    double pBx = bCx + endSelB * 0.5 * bLen * bUx, pBy = bCy + endSelB * 0.5 * bLen * bUy,
+           pBz = bCz + endSelB * 0.5 * bLen * bUz;
+    double dx = pBx - pAx, dy = pBy - pAy, dz = pBz - pAz;
+    double strain = sqrt(dx * dx + dy * dy + dz * dz);
+    C.ok = strain > 0.0;
+    if (C.ok) {
+        double inv = 1.0 / strain;
+        double lx = dx * inv, ly = dy * inv, lz = dz * inv;
+        double mcA = move_c(aUx, aUy, aUz, lx, ly, lz, bTG[rodA], bTG[nB + rodA], bRG[nB + rodA], aLen);
+        double mcB = move_c(bUx, bUy, bUz, lx, ly, lz, bTG[rodB], bTG[nB + rodB], bRG[nB + rodB], bLen);
+        double denom = dt * (mcA + mcB);
+        double forceMag = (denom > 0.0) ? (fracMove * 1.0e-6 * strain / denom) : 0.0;
+        double FAx = forceMag * lx, FAy = forceMag * ly, FAz = forceMag * lz;
+        double RsA = 0.5e-6 * rodLen * endSelA;
+        C.TAx = (RsA * aUy) * FAz - (RsA * aUz) * FAy;
+        C.TAy = (RsA * aUz) * FAx - (RsA * aUx) * FAz;
+        C.TAz = (RsA * aUx) * FAy - (RsA * aUy) * FAx;
+        double RsB = 0.5e-6 * rodLen * endSelB;
+        C.TBx = (RsB * bUy) * (-FAz) - (RsB * bUz) * (-FAy);
+        C.TBy = (RsB * bUz) * (-FAx) - (RsB * bUx) * (-FAz);
+        C.TBz = (RsB * bUx) * (-FAy) - (RsB * bUy) * (-FAx);
+        C.FAx = FAx; C.FAy = FAy; C.FAz = FAz;
+    }
+    return C;
+}
+
+SBX_DEV LeverTerm couple_lever(int nB, const float* uVec, const float* bRG, int mA, int mB, const float* dp) {
+    double dt = dp[0], leverTorq = dp[2], leverDeg = dp[3];
+    int leverA = 3 * mA + 1, leverB = 3 * mB + 1;
+    LeverTerm L;
+    double u1x = uVec[leverA], u1y = uVec[nB + leverA], u1z = uVec[2 * nB + leverA];
+    double u2x = uVec[leverB], u2y = uVec[nB + leverB], u2z = uVec[2 * nB + leverB];
+    double tvx = u1y * u2z - u1z * u2y, tvy = u1z * u2x - u1x * u2z, tvz = u1x * u2y - u1y * u2x;
+    double tvm2 = tvx * tvx + tvy * tvy + tvz * tvz;
+    L.ok = tvm2 > 1.0e-30;
+    if (L.ok) {
+        double im = 1.0 / sqrt(tvm2);
+        tvx *= im; tvy *= im; tvz *= im;
+        double dot = u1x * u2x + u1y * u2y + u1z * u2z;
+        if (dot > 1.0) dot = 1.0;
+        if (dot < -1.0) dot = -1.0;
+        double ang = accurate_acos(dot) * 180.0 / PI_D;
+        double invBRG = 1.0 / bRG[nB + leverA] + 1.0 / bRG[nB + leverB];
+        double torsionMag = leverTorq * (PI_D / 180.0) * (ang - leverDeg) / (invBRG * dt);
+        L.px = tvx * torsionMag; L.py = tvy * torsionMag; L.pz = tvz * torsionMag;
+    }
+    return L;
+}
+
+// the variant's float accumulation into rod A (sign +) or rod B (force -, torque TB)
+template <class Acc>
+SBX_DEV void couple_apply_rod(const Acc& acc, int body, bool isA, const CoupleTerm& C) {
+    if (!C.ok) return;
+    if (isA) {
+        acc.f(0, body) = (float)(acc.f(0, body) + C.FAx);
+        acc.f(1, body) = (float)(acc.f(1, body) + C.FAy);
+        acc.f(2, body) = (float)(acc.f(2, body) + C.FAz);
+        acc.t(0, body) = (float)(acc.t(0, body) + C.TAx);
+        acc.t(1, body) = (float)(acc.t(1, body) + C.TAy);
+        acc.t(2, body) = (float)(acc.t(2, body) + C.TAz);
+    } else {
+        acc.f(0, body) = (float)(acc.f(0, body) - C.FAx);
+        acc.f(1, body) = (float)(acc.f(1, body) - C.FAy);
+        acc.f(2, body) = (float)(acc.f(2, body) - C.FAz);
+        acc.t(0, body) = (float)(acc.t(0, body) + C.TBx);
+        acc.t(1, body) = (float)(acc.t(1, body) + C.TBy);
+        acc.t(2, body) = (float)(acc.t(2, body) + C.TBz);
+    }
+}
+
+template <class Acc>
+SBX_DEV void couple_apply_lever(const Acc& acc, int body, bool isA, const LeverTerm& L) {
+    if (!L.ok) return;
+    if (isA) {
+        acc.t(0, body) = (float)(acc.t(0, body) + L.px);
+        acc.t(1, body) = (float)(acc.t(1, body) + L.py);
+        acc.t(2, body) = (float)(acc.t(2, body) + L.pz);
+    } else {
+        acc.t(0, body) = (float)(acc.t(0, body) - L.px);
+        acc.t(1, body) = (float)(acc.t(1, body) - L.py);
+        acc.t(2, body) = (float)(acc.t(2, body) - L.pz);
+    }
+}
+
+// DimerCouplingSystem.couple per dimer (DimerCouplingSystem.java:99-182); self-writes rods/levers
 template <class Acc>
 SBX_DEV void couple_one(int nB, const float* coord, const float* uVec, const float* segLength, const float* bTG,
                         const float* bRG, const Acc& acc, int mA, int mB, bool par, const float* dp,
                         const int* boundSeg) {
-    double dt = dp[0], fracMove = dp[1], leverTorq = dp[2], leverDeg = dp[3], rodLen = dp[4];
-    int rodA = 3 * mA, rodB = 3 * mB;
     for (int variant = 0; variant < 2; variant++) {
-        double endSelA = (variant == 0) ? -1.0 : 1.0;
-        double endSelB = par ? endSelA : -endSelA;
-        double aCx = coord[rodA], aCy = coord[nB + rodA], aCz = coord[2 * nB + rodA];
-        double aUx = uVec[rodA], aUy = uVec[nB + rodA], aUz = uVec[2 * nB + rodA];
-        double bCx = coord[rodB], bCy = coord[nB + rodB], bCz = coord[2 * nB + rodB];
-        double bUx = uVec[rodB], bUy = uVec[nB + rodB], bUz = uVec[2 * nB + rodB];
-        double aLen = segLength[rodA], bLen = segLength[rodB];
-        double pAx = aCx + endSelA * 0.5 * aLen * aUx, pAy = aCy + endSelA * 0.5 * aLen * aUy,
-               pAz = aCz + endSelA * 0.5 * aLen * aUz;
-        double pBx = bCx + endSelB * 0.5 * bLen * bUx, pBy = bCy + endSelB * 0.5 * bLen * bUy,
-               pBz = bCz + endSelB * 0.5 * bLen * bUz;
-        double dx = pBx - pAx, dy = pBy - pAy, dz = pBz - pAz;
-        double strain = sqrt(dx * dx + dy * dy + dz * dz);
-        if (strain > 0.0) {
-            double inv = 1.0 / strain;
-            double lx = dx * inv, ly = dy * inv, lz = dz * inv;
-            double mcA = move_c(aUx, aUy, aUz, lx, ly, lz, bTG[rodA], bTG[nB + rodA], bRG[nB + rodA], aLen);
-            double mcB = move_c(bUx, bUy, bUz, lx, ly, lz, bTG[rodB], bTG[nB + rodB], bRG[nB + rodB], bLen);
-            double denom = dt * (mcA + mcB);
-            double forceMag = (denom > 0.0) ? (fracMove * 1.0e-6 * strain / denom) : 0.0;
-            double FAx = forceMag * lx, FAy = forceMag * ly, FAz = forceMag * lz;
-            double RsA = 0.5e-6 * rodLen * endSelA;
-            double TAx = (RsA * aUy) * FAz - (RsA * aUz) * FAy;
-            double TAy = (RsA * aUz) * FAx - (RsA * aUx) * FAz;
-            double TAz = (RsA * aUx) * FAy - (RsA * aUy) * FAx;
-            acc.f(0, rodA) = (float)(acc.f(0, rodA) + FAx);
-            acc.f(1, rodA) = (float)(acc.f(1, rodA) + FAy);
-            acc.f(2, rodA) = (float)(acc.f(2, rodA) + FAz);
-            acc.t(0, rodA) = (float)(acc.t(0, rodA) + TAx);
-            acc.t(1, rodA) = (float)(acc.t(1, rodA) + TAy);
-            acc.t(2, rodA) = (float)(acc.t(2, rodA) + TAz);
-            double RsB = 0.5e-6 * rodLen * endSelB;
-            double TBx = (RsB * bUy) * (-FAz) - (RsB * bUz) * (-FAy);
-            double TBy = (RsB * bUz) * (-FAx) - (RsB * bUx) * (-FAz);
-            double TBz = (RsB * bUx) * (-FAy) - (RsB * bUy) * (-FAx);
-            acc.f(0, rodB) = (float)(acc.f(0, rodB) - FAx);
-            acc.f(1, rodB) = (float)(acc.f(1, rodB) - FAy);
-            acc.f(2, rodB) = (float)(acc.f(2, rodB) - FAz);
-            acc.t(0, rodB) = (float)(acc.t(0, rodB) + TBx);
-            acc.t(1, rodB) = (float)(acc.t(1, rodB) + TBy);
-            acc.t(2, rodB) = (float)(acc.t(2, rodB) + TBz);
-        }
+        CoupleTerm C = couple_variant(nB, coord, uVec, segLength, bTG, bRG, mA, mB, par, dp, variant);
+        couple_apply_rod(acc, 3 * mA, true, C);
+        couple_apply_rod(acc, 3 * mB, false, C);
     }
     bool bothBound = boundSeg[mA] >= 0 && boundSeg[mB] >= 0;
     if (par && !bothBound) {
-        int leverA = 3 * mA + 1, leverB = 3 * mB + 1;
-        double u1x = uVec[leverA], u1y = uVec[nB + leverA], u1z = uVec[2 * nB + leverA];
-        double u2x = uVec[leverB], u2y = uVec[nB + leverB], u2z = uVec[2 * nB + leverB];
-        double tvx = u1y * u2z - u1z * u2y, tvy = u1z * u2x - u1x * u2z, tvz = u1x * u2y - u1y * u2x;
-        double tvm2 = tvx * tvx + tvy * tvy + tvz * tvz;
-        if (tvm2 > 1.0e-30) {
-            double im = 1.0 / sqrt(tvm2);
-            tvx *= im; tvy *= im; tvz *= im;
-            double dot = u1x * u2x + u1y * u2y + u1z * u2z;
-            if (dot > 1.0) dot = 1.0;
-            if (dot < -1.0) dot = -1.0;
-            double ang = accurate_acos(dot) * 180.0 / PI_D;
-            double invBRG = 1.0 / bRG[nB + leverA] + 1.0 / bRG[nB + leverB];
-            double torsionMag = leverTorq * (PI_D / 180.0) * (ang - leverDeg) / (invBRG * dt);
-            acc.t(0, leverA) = (float)(acc.t(0, leverA) + tvx * torsionMag);
-            acc.t(1, leverA) = (float)(acc.t(1, leverA) + tvy * torsionMag);
-            acc.t(2, leverA) = (float)(acc.t(2, leverA) + tvz * torsionMag);
-            acc.t(0, leverB) = (float)(acc.t(0, leverB) - tvx * torsionMag);
-            acc.t(1, leverB) = (float)(acc.t(1, leverB) - tvy * torsionMag);
-            acc.t(2, leverB) = (float)(acc.t(2, leverB) - tvz * torsionMag);
-        }
+        LeverTerm L = couple_lever(nB, uVec, bRG, mA, mB, dp);
+        couple_apply_lever(acc, 3 * mA + 1, true, L);
+        couple_apply_lever(acc, 3 * mB + 1, false, L);
     }
 }
 
-// MiniFilamentSystem.tether per dimer (MiniFilamentSystem.java:77-131)
-template <class Acc>
-SBX_DEV void tether_one(int d, int nMB, const float* mC, const float* mU, const float* mL, const float* mBTG,
-                        const float* mBRG, const Acc& acc, int nBb, const float* bbC, const float* bbU,
-                        const float* inv, int bb, int mA, float axf, float* miniData, const float* mp) {
+// MiniFilamentSystem.tether per dimer (MiniFilamentSystem.java:77-131): the rod-A terms
+// (force if strain > 0, torque tv * tmag if tvm2 > 1e-30) and the backbone reaction row.
+struct TetherTerm {
+    double Fx, Fy, Fz, Tx, Ty, Tz;
+    int fOK, tOK;
+    float row[6];                                // miniData row (reaction on the backbone)
+};
+
+SBX_DEV TetherTerm tether_terms(int nMB, const float* mC, const float* mU, const float* mL, const float* mBTG,
+                                const float* mBRG, int nBb, const float* bbC, const float* bbU, const float* inv,
+                                int bb, int mA, float axf, const float* mp) {
     double dt = mp[0], fracMove = mp[1], align = mp[2];
     int rodA = 3 * mA;
     double ax = axf;
+    TetherTerm T;
     double bcx = bbC[bb], bcy = bbC[nBb + bb], bcz = bbC[2 * nBb + bb];
     double bux = bbU[bb], buy = bbU[nBb + bb], buz = bbU[2 * nBb + bb];
     double pax = bcx + ax * bux, pay = bcy + ax * buy, paz = bcz + ax * buz;
@@ -994,22 +1086,21 @@ SBX_DEV void tether_one(int d, int nMB, const float* mC, const float* mU, const 
     double fbx = 0, fby = 0, fbz = 0, tbx = 0, tby = 0, tbz = 0;
     double dx = pax - re1x, dy = pay - re1y, dz = paz - re1z;
     double strain = sqrt(dx * dx + dy * dy + dz * dz);
-    if (strain > 0.0) {
+    T.fOK = strain > 0.0;
+    if (T.fOK) {
         double iv = 1.0 / strain;
         double lx = dx * iv, ly = dy * iv, lz = dz * iv;
         double denom = dt * (1.0 / mBTG[nMB + rodA] + inv[bb]);
         double forceMag = (denom > 0.0) ? (fracMove * 1.0e-6 * strain / denom) : 0.0;
-        double Frx = forceMag * lx, Fry = forceMag * ly, Frz = forceMag * lz;
-        acc.f(0, rodA) = (float)(acc.f(0, rodA) + Frx);
-        acc.f(1, rodA) = (float)(acc.f(1, rodA) + Fry);
-        acc.f(2, rodA) = (float)(acc.f(2, rodA) + Frz);
-        fbx = -Frx; fby = -Fry; fbz = -Frz;
+        T.Fx = forceMag * lx; T.Fy = forceMag * ly; T.Fz = forceMag * lz;
+        fbx = -T.Fx; fby = -T.Fy; fbz = -T.Fz;
     }
     double alignSign = (ax < 0.0) ? -1.0 : 1.0;
     double tux = alignSign * bux, tuy = alignSign * buy, tuz = alignSign * buz;
     double tvx = ruy * tuz - ruz * tuy, tvy = ruz * tux - rux * tuz, tvz = rux * tuy - ruy * tux;
     double tvm2 = tvx * tvx + tvy * tvy + tvz * tvz;
-    if (tvm2 > 1.0e-30) {
+    T.tOK = tvm2 > 1.0e-30;
+    if (T.tOK) {
         double im = 1.0 / sqrt(tvm2);
         tvx *= im; tvy *= im; tvz *= im;
         double dot = rux * tux + ruy * tuy + ruz * tuz;
@@ -1018,16 +1109,37 @@ SBX_DEV void tether_one(int d, int nMB, const float* mC, const float* mU, const 
         double angDeg = accurate_acos(dot) * 180.0 / PI_D;
         double denomR = (1.0 / mBRG[nMB + rodA] + inv[nBb + bb]) * dt;
         double tmag = align * (PI_D / 180.0) * angDeg / denomR;
-        acc.t(0, rodA) = (float)(acc.t(0, rodA) + tvx * tmag);
-        acc.t(1, rodA) = (float)(acc.t(1, rodA) + tvy * tmag);
-        acc.t(2, rodA) = (float)(acc.t(2, rodA) + tvz * tmag);
+        T.Tx = tvx * tmag; T.Ty = tvy * tmag; T.Tz = tvz * tmag;
         tbx = -tvx * tmag; tby = -tvy * tmag; tbz = -tvz * tmag;
     }
-    float* o = miniData + (int64_t)MINI_STRIDE * d;
-    o[0] = (float)fbx; o[1] = (float)fby; o[2] = (float)fbz;
-    o[3] = (float)tbx; o[4] = (float)tby; o[5] = (float)tbz;
+    T.row[0] = (float)fbx; T.row[1] = (float)fby; T.row[2] = (float)fbz;
+    T.row[3] = (float)tbx; T.row[4] = (float)tby; T.row[5] = (float)tbz;
+    return T;
 }
 
+template <class Acc>
+SBX_DEV void tether_apply(const Acc& acc, int rodA, const TetherTerm& T) {
+    if (T.fOK) {
+        acc.f(0, rodA) = (float)(acc.f(0, rodA) + T.Fx);
+        acc.f(1, rodA) = (float)(acc.f(1, rodA) + T.Fy);
+        acc.f(2, rodA) = (float)(acc.f(2, rodA) + T.Fz);
+    }
+    if (T.tOK) {
+        acc.t(0, rodA) = (float)(acc.t(0, rodA) + T.Tx);
+        acc.t(1, rodA) = (float)(acc.t(1, rodA) + T.Ty);
+        acc.t(2, rodA) = (float)(acc.t(2, rodA) + T.Tz);
+    }
+}
+
+template <class Acc>
+SBX_DEV void tether_one(int d, int nMB, const float* mC, const float* mU, const float* mL, const float* mBTG,
+                        const float* mBRG, const Acc& acc, int nBb, const float* bbC, const float* bbU,
+                        const float* inv, int bb, int mA, float axf, float* miniData, const float* mp) {
+    TetherTerm T = tether_terms(nMB, mC, mU, mL, mBTG, mBRG, nBb, bbC, bbU, inv, bb, mA, axf, mp);
+    tether_apply(acc, 3 * mA, T);
+    float* o = miniData + (int64_t)MINI_STRIDE * d;
+    for (int k = 0; k < 6; k++) o[k] = T.row[k];
+}
 
 // integrate + derive one body slot from accumulated F/T (registers), the slot's stored
 // Brownian draws and drag, then store pose, derived geometry and the final F/T sums
