@@ -272,13 +272,15 @@ bool fused_prepare(sbx_dense_plan* p) {
     };
     size_t nS = a.nSeg;
     a.cntCell = (int*)alloc(4 * (size_t)a.C);
+    a.cntSeg = (int*)alloc(4 * (size_t)a.C);
+    a.segCellOff = (int*)alloc(4 * ((size_t)a.C + 1));
     a.cntAct = (int*)alloc(4 * nS); a.cntA = (int*)alloc(4 * nS); a.cntB = (int*)alloc(4 * nS);
     a.cntM = (int*)alloc(4 * nS);
-    a.tileSum = (int*)alloc(4 * (size_t)(a.tilesC + 2 * a.tilesS + 1));
+    a.tileSum = (int*)alloc(4 * (size_t)(2 * a.tilesC + 2 * a.tilesS + 1));
     a.tmpCell = (int*)alloc(4 * (size_t)a.cap);
     a.tmpA = (int*)alloc(4 * (size_t)std::max(a.nL, 1)); a.tmpB = (int*)alloc(4 * (size_t)std::max(a.nL, 1));
     a.tmpM = (int*)alloc(4 * (size_t)a.nM);
-    a.sortedE1 = (float4*)alloc(16 * (size_t)a.cap); a.sortedE2 = (float4*)alloc(16 * (size_t)a.cap);
+    a.segE1 = (float4*)alloc(16 * nS); a.segE2 = (float4*)alloc(16 * nS);
     a.bar = (unsigned*)alloc(16);
     a.err = (int*)alloc(16);
     a.d_step = p->d_step;
@@ -349,6 +351,7 @@ extern "C" sbx_status sbx_dense_plan_run(sbx_dense_plan* p, int32_t t0, int32_t 
         if (p->fused_dirty) {
             FusedArgs& a = p->fa;
             cudaMemsetAsync(a.cntCell, 0, 4 * (size_t)a.C, ctx->stream);
+            cudaMemsetAsync(a.cntSeg, 0, 4 * (size_t)a.C, ctx->stream);
             for (int* q : {a.cntAct, a.cntA, a.cntB, a.cntM}) cudaMemsetAsync(q, 0, 4 * (size_t)a.nSeg, ctx->stream);
             cudaMemsetAsync(a.bar, 0, 16, ctx->stream);
             cudaMemsetAsync(a.err, 0, 16, ctx->stream);

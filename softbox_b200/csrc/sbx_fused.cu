@@ -142,6 +142,7 @@ __device__ void phase_publish_bin(const FusedArgs& a, int t) {
                            cell_coord(c[2], gp[2], gp[4], nZ) * (nX * nY);
                 g.bodyCell[i] = cell;
                 atomicAdd(&a.cntCell[cell], 1);
+                atomicAdd(&a.cntSeg[cell], 1);
             } else {
                 g.bodyCell[i] = -1;
             }
@@ -308,17 +309,14 @@ __device__ void phase_rank(const FusedArgs& a) {
             int s0 = g.gridCellOffsets[c], s1 = g.gridCellOffsets[c + 1];
             int pos = s0 + rank_in(a.tmpCell, s0, s1, i);
             g.gridCellContents[pos] = i;
-            // cell-sorted endpoint copy for the reach walk (w = segment slot, -1 = not a segment)
-            float4 e1, e2;
+            // segment endpoints in cell order for the reach walk: within a cell the segments
+            // (slots below nSeg) precede the motor heads, so a segment's rank among the
+            // segments of its cell equals its rank in the cell
             if (i < nSeg) {
-                e1 = make_float4(fb.end1[i], fb.end1[nSeg + i], fb.end1[2 * nSeg + i], __int_as_float(i));
-                e2 = make_float4(fb.end2[i], fb.end2[nSeg + i], fb.end2[2 * nSeg + i], 0.f);
-            } else {
-                e1 = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
-                e2 = make_float4(0.f, 0.f, 0.f, 0.f);
+                int q = a.segCellOff[c] + (pos - s0);
+                a.segE1[q] = make_float4(fb.end1[i], fb.end1[nSeg + i], fb.end1[2 * nSeg + i], __int_as_float(i));
+                a.segE2[q] = make_float4(fb.end2[i], fb.end2[nSeg + i], fb.end2[2 * nSeg + i], 0.f);
             }
-            a.sortedE1[pos] = e1;
-            a.sortedE2[pos] = e2;
         } else {
             int k = i - a.cap;
             int la = xl.linkFilA[k], lb = xl.linkFilB[k];
@@ -335,37 +333,54 @@ __device__ void phase_rank(const FusedArgs& a) {
 }
 
 // ---------------------------------------------------------------- F: minifilaments + links
-// BindingDetectionSystem.gridReachable over the cell-sorted float4 endpoints: the same
-// 27 cells, the same order, the same predicate as grid_reach_walk.
-__device__ int reach_walk_sorted(const FusedArgs& a, int m, float mx, float my, float mz, float mux, float muy,
-                                 float muz, float rux, float ruy, float ruz, int* out, float tol, float align) {
+// BindingDetectionSystem.gridReachable (BindingDetectionSystem.java:161-227) over the
+// segment-only cell-ordered endpoints, fused with bindNearest's selection
+// (BindingDetectionSystem.java:366-388): the same 27 cells in the same order, the same
+// predicate, and the first nearest among the first MAX_CAND candidates. The nine row
+// ranges (three consecutive x-cells each) are loaded before the walk starts.
+__device__ int reach_walk_bind(const FusedArgs& a, float mx, float my, float mz, float mux, float muy, float muz,
+                               float rux, float ruy, float ruz, int* out, float tol, float align, int* bestSeg,
+                               float* bestArc) {
     const float* gp = a.sc.grid.gridParams;
-    const int* off = a.sc.grid.gridCellOffsets;
+    const int* off = a.segCellOff;
     int nX = a.nX, nY = a.nY, nZ = a.nZ, nXY = nX * nY;
     int cx = cell_coord(mx, gp[0], gp[4], nX), cy = cell_coord(my, gp[1], gp[4], nY),
         cz = cell_coord(mz, gp[2], gp[4], nZ);
     int x0 = max(cx - 1, 0), x1 = min(cx + 1, nX - 1);
-    int y0 = max(cy - 1, 0), y1 = min(cy + 1, nY - 1);
-    int z0 = max(cz - 1, 0), z1 = min(cz + 1, nZ - 1);
-    int cnt = 0;
-    for (int zz = z0; zz <= z1; zz++)
-        for (int yy = y0; yy <= y1; yy++) {
-            // cells x0..x1 of one row are consecutive: one contiguous CSR range
-            int c0 = x0 + yy * nX + zz * nXY;
-            int start = off[c0], end = off[c0 + (x1 - x0) + 1];
-            for (int idx = start; idx < end; idx++) {
-                float4 e1 = a.sortedE1[idx];
-                int s = __float_as_int(e1.w);
-                if (s < 0) continue;
-                float4 e2 = a.sortedE2[idx];
-                float d = reach_test_dist_sq(mx, my, mz, mux, muy, muz, rux, ruy, ruz, e1.x, e1.y, e1.z, e2.x, e2.y,
-                                             e2.z, tol, align);
-                if (d >= 0.f) {
-                    if (cnt < MAX_CAND) out[cnt] = s;
-                    cnt++;
+    int rs[9], re[9];
+#pragma unroll
+    for (int r = 0; r < 9; r++) {
+        int zz = cz - 1 + r / 3, yy = cy - 1 + r % 3;
+        bool ok = zz >= 0 && zz < nZ && yy >= 0 && yy < nY;
+        int c0 = x0 + yy * nX + zz * nXY;
+        rs[r] = ok ? off[c0] : 0;
+        re[r] = ok ? off[c0 + (x1 - x0) + 1] : 0;
+    }
+    int cnt = 0, best = -1;
+    float bestD = 1.0e30f, arc = 0.f;
+#pragma unroll
+    for (int r = 0; r < 9; r++) {
+        for (int idx = rs[r]; idx < re[r]; idx++) {
+            float4 e1 = a.segE1[idx];
+            float4 e2 = a.segE2[idx];
+            float d = reach_test_dist_sq(mx, my, mz, mux, muy, muz, rux, ruy, ruz, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z,
+                                         tol, align);
+            if (d >= 0.f) {
+                if (cnt < MAX_CAND) {
+                    int sg = __float_as_int(e1.w);
+                    out[cnt] = sg;
+                    if (d < bestD) {
+                        bestD = d;
+                        best = sg;
+                        arc = bind_arc(mx, my, mz, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z);
+                    }
                 }
+                cnt++;
             }
         }
+    }
+    *bestSeg = best;
+    *bestArc = arc;
     return cnt;
 }
 
@@ -399,20 +414,17 @@ __device__ void mini_unit(const FusedArgs& a, MiniSmem& ms, int u, int t) {
             float mux = mot.uVec[m], muy = mot.uVec[nM + m], muz = mot.uVec[2 * nM + m];
             float rux = mot.rodUVec[m], ruy = mot.rodUVec[nM + m], ruz = mot.rodUVec[2 * nM + m];
             int* slice = sc.grid.reachSeg + (int64_t)m * MAX_CAND;
-            int rc = reach_walk_sorted(a, m, mx, my, mz, mux, muy, muz, rux, ruy, ruz, slice, kp[7], kp[8]);
-            sc.grid.reachCount[m] = rc;
-            if (rc > MAX_CAND) atomicOr(a.err, ERR_REACH_OVERFLOW);
             int bs = mot.boundSeg[m], cd = mot.cooldown[m], sb = mot.stats[2 * m], sr = mot.stats[2 * m + 1],
                 cs = mot.capStats[m];
             release_one(m, bs, cd, sb, sr, cs, mot.forceDotFil[m], mot.forceMag[m], kp, t, sc.seed);
-            if (bs == FREE_BINDABLE) {
-                int best;
-                float arc;
-                if (bind_nearest_scan(m, nM, mot.head, mot.uVec, mot.rodUVec, nSeg, fb.end1, fb.end2, slice, rc,
-                                      kp[7], kp[8], &best, &arc)) {
-                    bs = best;
-                    mot.bindArc[m] = arc;
-                }
+            int best;
+            float arc;
+            int rc = reach_walk_bind(a, mx, my, mz, mux, muy, muz, rux, ruy, ruz, slice, kp[7], kp[8], &best, &arc);
+            sc.grid.reachCount[m] = rc;
+            if (rc > MAX_CAND) atomicOr(a.err, ERR_REACH_OVERFLOW);
+            if (bs == FREE_BINDABLE && best >= 0) {
+                bs = best;
+                mot.bindArc[m] = arc;
             }
             mot.boundSeg[m] = bs; mot.cooldown[m] = cd; mot.stats[2 * m] = sb; mot.stats[2 * m + 1] = sr;
             mot.capStats[m] = cs;
@@ -763,7 +775,7 @@ __device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
 __device__ void phase_rods(const FusedArgs& a, FusedSmem& sm, int t, uint64_t* mbar, unsigned& phase) {
     for (int u = blockIdx.x; u < a.nRodUnits; u += gridDim.x) rod_unit(a, sm.rod, u, t, mbar, phase);
     // reset the private histograms for the next step
-    for (int i = gtid(); i < a.C; i += gthreads()) a.cntCell[i] = 0;
+    for (int i = gtid(); i < a.C; i += gthreads()) { a.cntCell[i] = 0; a.cntSeg[i] = 0; }
     for (int i = gtid(); i < a.nSeg; i += gthreads()) {
         a.cntAct[i] = 0; a.cntA[i] = 0; a.cntB[i] = 0; a.cntM[i] = 0;
     }
@@ -780,11 +792,12 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_dense_fused(FusedArgs a, int 
     }
     __syncthreads();
     const sbx_dense_scene& sc = a.sc;
-    ScanArr first[3] = {{a.cntCell, a.C, 0}, {a.cntA, a.nSeg, a.tilesC}, {a.cntB, a.nSeg, a.tilesC + a.tilesS}};
-    int narr1 = a.xlOn ? 3 : 1;
-    int* out1[3] = {sc.grid.gridCellOffsets, sc.xl.segOffsetsA, sc.xl.segOffsetsB};
-    int* zero1[3] = {sc.grid.cellCount, sc.xl.segCountA, sc.xl.segCountB};
-    int clamp1[3] = {a.cap, a.nL, a.nL};
+    ScanArr first[4] = {{a.cntCell, a.C, 0}, {a.cntSeg, a.C, a.tilesC}, {a.cntA, a.nSeg, 2 * a.tilesC},
+                        {a.cntB, a.nSeg, 2 * a.tilesC + a.tilesS}};
+    int narr1 = a.xlOn ? 4 : 2;
+    int* out1[4] = {sc.grid.gridCellOffsets, a.segCellOff, sc.xl.segOffsetsA, sc.xl.segOffsetsB};
+    int* zero1[4] = {sc.grid.cellCount, nullptr, sc.xl.segCountA, sc.xl.segCountB};
+    int clamp1[4] = {a.cap, a.nSeg, a.nL, a.nL};
     ScanArr second[1] = {{a.cntM, a.nSeg, 0}};
     int* out2[1] = {sc.segMotorOffsets};
     int* zero2[1] = {sc.segMotorCount};

@@ -19,10 +19,11 @@ struct FusedArgs {
     int xlOn, xlUnbind, useTma, filSeed;
     int jointShare;          // chain neighbours are symmetric: each joint computed once
     // private scratch (plan-owned)
-    int *cntCell, *cntAct, *cntA, *cntB, *cntM;
+    int *cntCell, *cntSeg, *cntAct, *cntA, *cntB, *cntM;   // cntSeg: segments per cell
+    int* segCellOff;         // segment-only exclusive prefix over cells (C + 1)
     int* tileSum;
     int *tmpCell, *tmpA, *tmpB, *tmpM;
-    float4 *sortedE1, *sortedE2;
+    float4 *segE1, *segE2;   // segment endpoints in cell order: {end1, slot}, {end2, 0}
     unsigned* bar;           // [0] arrivals, [1] generation
     int* err;                // bit0 barrier timeout, bit1 reach overflow, bit2 TMA wait timeout
     int* d_step;
