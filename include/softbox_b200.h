@@ -413,15 +413,17 @@ int32_t sbx_dense_plan_kernels_per_step(sbx_dense_plan* plan);
 /* Synchronises and reports the fused path's flags for the last run: bit0 a grid-barrier
  * wait ran out (SBX_ETIMEOUT; the state of that run is partial), bit1 a reach list
  * exceeded SBX_MAX_CAND (SBX_EOVERFLOW; counts continue past the cap, as the reference),
- * bit2 a bulk-copy wait ran out (SBX_ETIMEOUT). */
+ * bit2 a bulk-copy wait ran out (SBX_ETIMEOUT), bit3 a linked-list walk ran past its bound
+ * (SBX_ESTATE). */
 sbx_status sbx_dense_plan_status(sbx_dense_plan* plan, int32_t* flags);
 /* 1 when the fused persistent path is available for this scene (else mode 2 returns SBX_ESTATE) */
 int32_t sbx_dense_plan_fused_available(sbx_dense_plan* plan);
 /* cooperative grid size (CTAs) of the fused path */
 int32_t sbx_dense_plan_fused_grid(sbx_dense_plan* plan);
-/* Phase timing of the fused path: when dev_times (device int64 array of nsteps*11) is
- * set, each run writes the %globaltimer value (ns) after every phase barrier of every
- * step; NULL switches it off. */
+/* Phase timing of the fused path: when dev_times (device int64 array of
+ * nsteps*SBX_FUSED_PHASES) is set, each run writes the %globaltimer value (ns) after every
+ * phase barrier of every step; NULL switches it off. */
+#define SBX_FUSED_PHASES 6
 sbx_status sbx_dense_plan_phase_times(sbx_dense_plan* plan, int64_t* dev_times);
 /* Test hook for failure detection: the fused kernel's grid barrier waits for `extra`
  * arrivals that never come, so its bounded wait runs out and the run reports

@@ -240,7 +240,7 @@ bool fused_prepare(sbx_dense_plan* p) {
         for (int i = 0; i < a.nSeg && ok; i++) ok = (lo[i] / G == i / G) && (hi[i] / G == i / G);
         if (!ok) continue;
         largest = G;
-        if (!a.G && (a.nSeg + G - 1) / G <= p->fused_grid) a.G = G;
+        if (!a.G && (a.nSeg + G - 1) / G <= p->fused_grid - FUSED_MIN_HELPERS) a.G = G;
     }
     if (!a.G) a.G = largest;
     if (!a.G) return why("chain neighbours cross every segment grouping");
@@ -256,6 +256,8 @@ bool fused_prepare(sbx_dense_plan* p) {
             if (back != i || backSide != 1 - side) { a.jointShare = 0; break; }
         }
     a.nRodUnits = (a.nSeg + a.G - 1) / a.G;
+    // helper CTAs of the rod phase: those without a rod unit, at least FUSED_MIN_HELPERS
+    a.kHelp0 = std::max(0, std::min(a.nRodUnits, p->fused_grid - FUSED_MIN_HELPERS));
     a.tilesC = (a.C + SCAN_CHUNK - 1) / SCAN_CHUNK;
     a.tilesS = (a.nSeg + SCAN_CHUNK - 1) / SCAN_CHUNK;
     auto fc = d2h(sc.fil.counts, 4, st);
@@ -277,11 +279,14 @@ bool fused_prepare(sbx_dense_plan* p) {
     a.cntAct = (int*)alloc(4 * nS); a.cntA = (int*)alloc(4 * nS); a.cntB = (int*)alloc(4 * nS);
     a.cntM = (int*)alloc(4 * nS);
     a.tileSum = (int*)alloc(4 * (size_t)(2 * a.tilesC + 2 * a.tilesS + 1));
-    a.tmpCell = (int*)alloc(4 * (size_t)a.cap);
-    a.tmpA = (int*)alloc(4 * (size_t)std::max(a.nL, 1)); a.tmpB = (int*)alloc(4 * (size_t)std::max(a.nL, 1));
-    a.tmpM = (int*)alloc(4 * (size_t)a.nM);
+    a.mTileSum = (int*)alloc(4 * (size_t)(a.tilesS + 1));
+    a.cellHead = (int*)alloc(4 * (size_t)a.C); a.cellNext = (int*)alloc(4 * (size_t)a.cap);
+    size_t nLk = (size_t)std::max(a.nL, 1);
+    a.headA = (int*)alloc(4 * nS); a.nextA = (int*)alloc(4 * nLk);
+    a.headB = (int*)alloc(4 * nS); a.nextB = (int*)alloc(4 * nLk);
+    a.headM = (int*)alloc(4 * nS); a.nextM = (int*)alloc(4 * (size_t)a.nM);
     a.segE1 = (float4*)alloc(16 * nS); a.segE2 = (float4*)alloc(16 * nS);
-    a.bar = (unsigned*)alloc(16);
+    a.bar = (unsigned long long*)alloc(32);
     a.err = (int*)alloc(16);
     a.d_step = p->d_step;
     for (void* q : p->allocs)
@@ -353,7 +358,9 @@ extern "C" sbx_status sbx_dense_plan_run(sbx_dense_plan* p, int32_t t0, int32_t 
             cudaMemsetAsync(a.cntCell, 0, 4 * (size_t)a.C, ctx->stream);
             cudaMemsetAsync(a.cntSeg, 0, 4 * (size_t)a.C, ctx->stream);
             for (int* q : {a.cntAct, a.cntA, a.cntB, a.cntM}) cudaMemsetAsync(q, 0, 4 * (size_t)a.nSeg, ctx->stream);
-            cudaMemsetAsync(a.bar, 0, 16, ctx->stream);
+            cudaMemsetAsync(a.cellHead, 0xff, 4 * (size_t)a.C, ctx->stream);
+            for (int* q : {a.headA, a.headB, a.headM}) cudaMemsetAsync(q, 0xff, 4 * (size_t)a.nSeg, ctx->stream);
+            cudaMemsetAsync(a.bar, 0, 32, ctx->stream);
             cudaMemsetAsync(a.err, 0, 16, ctx->stream);
             p->fused_dirty = false;
         }
@@ -385,6 +392,7 @@ extern "C" sbx_status sbx_dense_plan_status(sbx_dense_plan* p, int32_t* flags) {
     if (h) p->fused_dirty = true;
     if (h & 1) return fail(p->ctx, SBX_ETIMEOUT, "fused step: grid barrier wait ran out");
     if (h & 4) return fail(p->ctx, SBX_ETIMEOUT, "fused step: bulk-copy wait ran out");
+    if (h & 8) return fail(p->ctx, SBX_ESTATE, "fused step: a linked-list walk ran past its bound");
     if (h & 2) return fail(p->ctx, SBX_EOVERFLOW, "fused step: a reach list exceeded SBX_MAX_CAND");
     return SBX_OK;
 }

@@ -1,29 +1,29 @@
 // sbx_fused.cu — the dense contractile step as ONE persistent cooperative kernel.
 //
-// A launch advances nsteps steps. Within a step, phases are separated by a grid-wide
+// A launch advances nsteps steps. Within a step, six phases are separated by a grid-wide
 // barrier (bounded spin: a barrier that does not complete within the limit raises
 // error bit 0 and every CTA returns, so a fault cannot hang the device):
 //
 //   A  publish the body view (FilamentStore/MotorStore.publish*), bin bodies
-//      (SpatialGrid.bodyCell) + atomic cell histogram; crosslinker Bell unbind and the
-//      active-link / CSR-key histograms
-//   B  tile sums of the three histograms (cells, link A keys, link B keys)
-//   C  exclusive scans -> gridCellOffsets / segOffsetsA / segOffsetsB / chunkSum
-//   D  unordered atomic scatter into scratch lists
-//   E  rank pass -> stable gridCellContents / segIdxA / segIdxB, plus cell-sorted
-//      float4 copies of the segment endpoints for the reach walk
-//   F  one CTA per minifilament: reach walk, release, bind, nucleotide cycle for its 32
-//      heads, then Brownian, joints, dimer coupling, tether, backbone gather, cross-
-//      bridge bonds, integrate + derive of its 96 sub-bodies and backbone, force-dot
-//      registry — all sub-body force sums kept in shared memory; other CTAs compute
-//      crosslinker forces + torsion
-//   G  motor->segment histogram tile sums; filament Brownian forcing
-//   H  motor CSR scan -> segMotorOffsets
-//   I  motor scatter
-//   J  motor rank -> segMotorMyo
+//      (SpatialGrid.bodyCell): cell histogram, segments-per-cell histogram and a list
+//      per cell; crosslinker Bell unbind, active-link counts, link-key histograms and
+//      lists; Brownian draws of the motor sub-bodies and backbones
+//   B  tile sums of the four histograms
+//   C  exclusive scans -> gridCellOffsets (+ chunkSum, cellCount), the segment-only cell
+//      prefix, segOffsetsA / segOffsetsB (+ counts)
+//   E  stable placement by list rank -> gridCellContents, segIdxA, segIdxB and the
+//      segment endpoints in cell order (float4) for the reach walk
+//   F  one CTA per minifilament: binding of its 32 heads (reach walk fused with the
+//      nearest-segment choice; bound heads join their segment's motor list) alongside
+//      every position-only myosin term, then the ordered sums, the cross-bridge bonds
+//      and integrate + derive of its 96 sub-bodies and backbone, all force sums in
+//      shared memory; other CTAs compute crosslinker forces + torsion and the filament
+//      Brownian draws
 //   K  one CTA per group of whole filaments, poses staged in shared memory with TMA
-//      bulk copies: chain forces, crosslinker A/B gathers, motor gather (CSR order, FP64
-//      sums), containment, integrate + derive
+//      bulk copies: chain forces (each joint once), crosslinker A/B gathers, motor
+//      gather from the segment's motor list in ascending slot order (FP64 sums),
+//      containment, integrate + derive; helper CTAs build the motor CSR arrays and reset
+//      the step's histograms and lists
 //
 // Every slot is computed by the same device functions as the per-system kernels, in the
 // reference's accumulation order, so the result is bit-identical to
@@ -39,16 +39,20 @@ using namespace sbx;
 
 namespace {
 
-constexpr long long SPIN_LIMIT = 1LL << 24;    // x ~64 ns sleeps: about one second
-constexpr int ERR_BARRIER = 1, ERR_REACH_OVERFLOW = 2, ERR_TMA = 4;
+constexpr long long SPIN_LIMIT = 1LL << 24;    // x ~64 ns sleeps: about one second (bulk-copy waits)
+constexpr unsigned long long WAIT_NS = 1000000000ULL;   // barrier waits give up after one second
+constexpr int ERR_BARRIER = 1, ERR_REACH_OVERFLOW = 2, ERR_TMA = 4, ERR_LIST = 8;
 
 // shared memory of one CTA, reused by the phases
 struct RodSmem {
     float st[10 * FUSED_MAX_ROD];                 // staged rod geometry planes (TMA destination)
     int off[3][FUSED_MAX_ROD + 1];                // the group's CSR row offsets: links A, links B, motors
     ChainJoint js[2 * FUSED_MAX_ROD];             // joints, at (owner rod, owner side)
-    float ent[FUSED_ENT_CAP][6];                  // the group's CSR payloads, in CSR order
+    float ent[FUSED_ENT_CAP][6];                  // the group's link CSR payloads, in CSR order
     int entOk[FUSED_ENT_CAP];                     // guard passed (active link)
+    int mCnt[FUSED_MAX_ROD];                      // motors bound to each rod
+    int mIds[FUSED_MAX_ROD][FUSED_MIDS];          // their slots, ascending (the first FUSED_MIDS)
+    float mPay[FUSED_MAX_ROD][FUSED_MCAP][6];     // the first FUSED_MCAP bond reactions
 };
 struct MiniSmem {
     float sF[3 * FUSED_MAX_SUB], sT[3 * FUSED_MAX_SUB];
@@ -64,36 +68,52 @@ union FusedSmem {
 
 __device__ __forceinline__ int vload(const int* p) { return *(const volatile int*)p; }
 
-// Grid barrier (the cooperative-groups pattern: block barrier, one thread per CTA
-// publishes with a device fence, waits on a generation word, fences again).
-__device__ bool grid_sync(const FusedArgs& a) {
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long ns;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(ns));
+    return ns;
+}
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void red_release_add(unsigned long long* p, unsigned long long v) {
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+}
+
+// Barrier over `n` CTAs on a monotonic 64-bit arrival counter: after the block barrier,
+// thread 0 adds one arrival with release semantics and polls with acquire loads until
+// the counter reaches this barrier's target (the previous target + n). A wait longer
+// than WAIT_NS, or an error raised elsewhere, sets/sees ERR_BARRIER and returns false.
+__device__ bool counter_sync(unsigned long long* ctr, unsigned long long& target, unsigned n, int* err) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned* gen = a.bar + 1;
-        unsigned g = *gen;
-        __threadfence();
-        unsigned arrived = atomicAdd(a.bar, 1u);
-        if (arrived == gridDim.x - 1 + (unsigned)a.barrierExtra) {
-            a.bar[0] = 0;
-            __threadfence();
-            atomicAdd(a.bar + 1, 1u);
-        } else {
-            long long it = 0;
-            while (*gen == g) {
-                if (vload(a.err) & ERR_BARRIER) break;
-                if (++it > SPIN_LIMIT) {
-                    atomicOr(a.err, ERR_BARRIER);
-                    break;
-                }
-                __nanosleep(64);
+        target += n;
+        red_release_add(ctr, 1ULL);
+        unsigned long long t0 = 0;
+        unsigned it = 0;
+        bool ok = true;
+        while (ld_acquire(ctr) < target) {
+            if ((++it & 63u) == 0) {
+                if (vload(err) & ERR_BARRIER) { ok = false; break; }
+                unsigned long long now = gtimer();
+                if (t0 == 0) t0 = now;
+                else if (now - t0 > WAIT_NS) { atomicOr(err, ERR_BARRIER); ok = false; break; }
             }
         }
-        __threadfence();
-        s_ok = (vload(a.err) & ERR_BARRIER) == 0;
+        s_ok = ok && (vload(err) & ERR_BARRIER) == 0;
     }
     __syncthreads();
     return s_ok;
+}
+
+// the counter value at which this launch's barriers start: every completed barrier adds
+// exactly n arrivals, and no barrier completes before every CTA has read the counter
+__device__ __forceinline__ unsigned long long counter_base(const unsigned long long* ctr, unsigned n) {
+    unsigned long long c = ld_acquire(ctr);
+    return c - c % n;
 }
 
 __device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
@@ -122,8 +142,15 @@ __device__ void phase_publish_bin(const FusedArgs& a, int t) {
     const float* gp = g.gridParams;
     const int nX = a.nX, nY = a.nY, nZ = a.nZ;
     const int nLk = a.xlOn ? a.nL : 0;
-    const int total = cap + nLk + nB + a.nBb;
+    const int total = cap + nLk + nB + a.nBb + nSeg;
     for (int i = gtid(); i < total; i += gthreads()) {
+        if (i >= cap + nLk + nB + a.nBb) {
+            // the motor lists and counts of the previous step were last read by its rod phase
+            int s = i - (cap + nLk + nB + a.nBb);
+            a.headM[s] = -1;
+            a.cntM[s] = 0;
+            continue;
+        }
         if (i >= cap + nLk) {
             // BrownianForceSystem for the motor sub-bodies, then the backbones
             int j = i - cap - nLk;
@@ -143,6 +170,7 @@ __device__ void phase_publish_bin(const FusedArgs& a, int t) {
                 g.bodyCell[i] = cell;
                 atomicAdd(&a.cntCell[cell], 1);
                 atomicAdd(&a.cntSeg[cell], 1);
+                a.cellNext[i] = atomicExch(&a.cellHead[cell], i);
             } else {
                 g.bodyCell[i] = -1;
             }
@@ -166,6 +194,7 @@ __device__ void phase_publish_bin(const FusedArgs& a, int t) {
                            cell_coord(hd[2], gp[2], gp[4], nZ) * (nX * nY);
                 g.bodyCell[b] = cell;
                 atomicAdd(&a.cntCell[cell], 1);
+                a.cellNext[b] = atomicExch(&a.cellHead[cell], b);
             } else {
                 g.bodyCell[b] = -1;
             }
@@ -185,8 +214,8 @@ __device__ void phase_publish_bin(const FusedArgs& a, int t) {
                 atomicAdd(&a.cntAct[la], 1);
                 atomicAdd(&a.cntAct[lb], 1);
             }
-            if (la >= 0) atomicAdd(&a.cntA[la], 1);
-            if (lb >= 0) atomicAdd(&a.cntB[lb], 1);
+            if (la >= 0) { atomicAdd(&a.cntA[la], 1); a.nextA[k] = atomicExch(&a.headA[la], k); }
+            if (lb >= 0) { atomicAdd(&a.cntB[lb], 1); a.nextB[k] = atomicExch(&a.headB[lb], k); }
         }
     }
 }
@@ -203,9 +232,8 @@ __device__ __forceinline__ int warp_sum(int v) {
     return v;
 }
 
-__device__ void tile_sums(const ScanArr* arrs, int narr, int* tileSum) {
+__device__ void tile_sums(const ScanArr* arrs, int narr, int* tileSum, int warp, int nwarps) {
     int lane = threadIdx.x & 31;
-    int warp = gtid() >> 5, nwarps = gthreads() >> 5;
     int total = arrs[narr - 1].tile0 + (arrs[narr - 1].n + SCAN_CHUNK - 1) / SCAN_CHUNK;
     for (int tl = warp; tl < total; tl += nwarps) {
         int ai = 0;
@@ -219,13 +247,13 @@ __device__ void tile_sums(const ScanArr* arrs, int narr, int* tileSum) {
     }
 }
 
-// exclusive scan of each array into out[ai][0..n] (terminator = min(total, clamp[ai])),
-// zeroing zero[ai][...] (the write cursors); chunkOut (optional, array 0) gets the
-// tile-prefix layout of SpatialGrid.gridScanChunks.
-__device__ void tile_scan(const ScanArr* arrs, int narr, const int* tileSum, int* const* out, int* const* zero,
-                          const int* clampTotal, int* chunkOut) {
+// exclusive scan of each array into out[ai][0..n] (terminator = min(total, clamp[ai]));
+// copy[ai] (optional) receives the counts — the row lengths the reference's serial
+// scatter leaves in its write cursors; chunkOut (optional, array 0) gets the tile-prefix
+// layout of SpatialGrid.gridScanChunks.
+__device__ void tile_scan(const ScanArr* arrs, int narr, const int* tileSum, int* const* out, int* const* copy,
+                          const int* clampTotal, int* chunkOut, int warp, int nwarps) {
     int lane = threadIdx.x & 31;
-    int warp = gtid() >> 5, nwarps = gthreads() >> 5;
     int total = arrs[narr - 1].tile0 + (arrs[narr - 1].n + SCAN_CHUNK - 1) / SCAN_CHUNK;
     for (int tl = warp; tl < total; tl += nwarps) {
         int ai = 0;
@@ -233,35 +261,43 @@ __device__ void tile_scan(const ScanArr* arrs, int narr, const int* tileSum, int
         const ScanArr& s = arrs[ai];
         int ntiles = (s.n + SCAN_CHUNK - 1) / SCAN_CHUNK;
         int local = tl - s.tile0;
+        // the preceding tiles' sums: 16 predicated loads per lane in flight together
         int b = 0;
-        for (int j = lane; j < local; j += 32) b += tileSum[s.tile0 + j];
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            int j = lane + 32 * q;
+            b += (j < local) ? tileSum[s.tile0 + j] : 0;
+        }
+        for (int j = lane + 512; j < local; j += 32) b += tileSum[s.tile0 + j];
         b = warp_sum(b);
         int base = local * SCAN_CHUNK;
         constexpr int PER = SCAN_CHUNK / 32;
+        // coalesced: row j of the tile is elements base + 32 j + lane
         int vals[PER];
-        int lsum = 0;
+#pragma unroll
         for (int j = 0; j < PER; j++) {
-            int r = base + lane * PER + j;
+            int r = base + 32 * j + lane;
             vals[j] = r < s.n ? s.cnt[r] : 0;
-            lsum += vals[j];
         }
-        int x = lsum;
-        for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        int run = b + x - lsum;
+        int run = b;
+#pragma unroll
         for (int j = 0; j < PER; j++) {
-            int r = base + lane * PER + j;
-            if (r < s.n) {
-                out[ai][r] = run;
-                if (zero[ai]) zero[ai][r] = 0;
+            int v = vals[j], x = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
             }
-            run += vals[j];
+            int r = base + 32 * j + lane;
+            if (r < s.n) {
+                out[ai][r] = run + x - v;
+                if (copy[ai]) copy[ai][r] = v;
+            }
+            run += __shfl_sync(0xffffffffu, x, 31);
         }
         if (lane == 0 && ai == 0 && chunkOut) chunkOut[local] = b;
         if (local == ntiles - 1) {
-            int tot = __shfl_sync(0xffffffffu, run, 31);
+            int tot = run;
             if (lane == 0) {
                 out[ai][s.n] = tot < clampTotal[ai] ? tot : clampTotal[ai];
                 if (ai == 0 && chunkOut) chunkOut[ntiles] = tot;
@@ -270,32 +306,23 @@ __device__ void tile_scan(const ScanArr* arrs, int narr, const int* tileSum, int
     }
 }
 
-// ---------------------------------------------------------------- D / E (grid + link CSRs)
-__device__ void phase_scatter(const FusedArgs& a) {
-    const sbx_dense_scene& sc = a.sc;
-    const sbx_grid_state& g = sc.grid;
-    const sbx_crosslinker_store& xl = sc.xl;
-    int total = a.cap + (a.xlOn ? a.nL : 0);
-    for (int i = gtid(); i < total; i += gthreads()) {
-        if (i < a.cap) {
-            int c = g.bodyCell[i];
-            if (c >= 0) a.tmpCell[g.gridCellOffsets[c] + atomicAdd(&g.cellCount[c], 1)] = i;
-        } else {
-            int k = i - a.cap;
-            int la = xl.linkFilA[k], lb = xl.linkFilB[k];
-            if (la >= 0) a.tmpA[xl.segOffsetsA[la] + atomicAdd(&xl.segCountA[la], 1)] = k;
-            if (lb >= 0) a.tmpB[xl.segOffsetsB[lb] + atomicAdd(&xl.segCountB[lb], 1)] = k;
+// ---------------------------------------------------------------- E: stable placement
+// Rank of `self` in a row = the number of the row's items with a smaller index, counted
+// along the row's list: the position the reference's serial scatter gives it (items are
+// scattered in ascending index). A walk longer than `bound` marks the list corrupt.
+__device__ __forceinline__ int list_rank(const FusedArgs& a, int head, const int* next, int self, int bound) {
+    int r = 0, it = 0;
+    for (int j = head; j >= 0; j = next[j]) {
+        r += j < self;
+        if (++it > bound) {
+            atomicOr(a.err, ERR_LIST);
+            break;
         }
     }
-}
-
-__device__ __forceinline__ int rank_in(const int* tmp, int start, int end, int i) {
-    int r = 0;
-    for (int j = start; j < end; j++) r += tmp[j] < i;
     return r;
 }
 
-__device__ void phase_rank(const FusedArgs& a) {
+__device__ void phase_place(const FusedArgs& a) {
     const sbx_dense_scene& sc = a.sc;
     const sbx_grid_state& g = sc.grid;
     const sbx_crosslinker_store& xl = sc.xl;
@@ -306,28 +333,21 @@ __device__ void phase_rank(const FusedArgs& a) {
         if (i < a.cap) {
             int c = g.bodyCell[i];
             if (c < 0) continue;
-            int s0 = g.gridCellOffsets[c], s1 = g.gridCellOffsets[c + 1];
-            int pos = s0 + rank_in(a.tmpCell, s0, s1, i);
-            g.gridCellContents[pos] = i;
+            int rank = list_rank(a, a.cellHead[c], a.cellNext, i, a.cap);
+            g.gridCellContents[g.gridCellOffsets[c] + rank] = i;
             // segment endpoints in cell order for the reach walk: within a cell the segments
             // (slots below nSeg) precede the motor heads, so a segment's rank among the
             // segments of its cell equals its rank in the cell
             if (i < nSeg) {
-                int q = a.segCellOff[c] + (pos - s0);
+                int q = a.segCellOff[c] + rank;
                 a.segE1[q] = make_float4(fb.end1[i], fb.end1[nSeg + i], fb.end1[2 * nSeg + i], __int_as_float(i));
                 a.segE2[q] = make_float4(fb.end2[i], fb.end2[nSeg + i], fb.end2[2 * nSeg + i], 0.f);
             }
         } else {
             int k = i - a.cap;
             int la = xl.linkFilA[k], lb = xl.linkFilB[k];
-            if (la >= 0) {
-                int s0 = xl.segOffsetsA[la], s1 = xl.segOffsetsA[la + 1];
-                xl.segIdxA[s0 + rank_in(a.tmpA, s0, s1, k)] = k;
-            }
-            if (lb >= 0) {
-                int s0 = xl.segOffsetsB[lb], s1 = xl.segOffsetsB[lb + 1];
-                xl.segIdxB[s0 + rank_in(a.tmpB, s0, s1, k)] = k;
-            }
+            if (la >= 0) xl.segIdxA[xl.segOffsetsA[la] + list_rank(a, a.headA[la], a.nextA, k, a.nL)] = k;
+            if (lb >= 0) xl.segIdxB[xl.segOffsetsB[lb] + list_rank(a, a.headB[lb], a.nextB, k, a.nL)] = k;
         }
     }
 }
@@ -430,7 +450,10 @@ __device__ void mini_unit(const FusedArgs& a, MiniSmem& ms, int u, int t) {
             mot.capStats[m] = cs;
             mot.nucleotideState[m] = cycle_one(m, mot.nucleotideState[m], bs >= 0, mot.forceDotHist + 10 * m,
                                                mot.nucParams, t, sc.seed);
-            if (bs >= 0) atomicAdd(&a.cntM[bs], 1);
+            if (bs >= 0) {
+                atomicAdd(&a.cntM[bs], 1);
+                a.nextM[m] = atomicExch(&a.headM[bs], m);
+            }
         }
     } else if (tid < 96) {
         // warps 1-2: motor joints (local motor k/2, joint k&1), then a lever (warp 1) or a tether (warp 2)
@@ -586,24 +609,6 @@ __device__ void phase_motors_links(const FusedArgs& a, FusedSmem& sm, int t) {
         for (int s = gtid(); s < a.nSeg; s += gthreads()) a.sc.xl.activeLinkCount[s] = a.cntAct[s];
 }
 
-__device__ void phase_motor_scatter(const FusedArgs& a) {
-    const sbx_dense_scene& sc = a.sc;
-    for (int m = gtid(); m < a.nM; m += gthreads()) {
-        int s = sc.mot.boundSeg[m];
-        if (s >= 0) a.tmpM[sc.segMotorOffsets[s] + atomicAdd(&sc.segMotorCount[s], 1)] = m;
-    }
-}
-
-__device__ void phase_motor_rank(const FusedArgs& a) {
-    const sbx_dense_scene& sc = a.sc;
-    for (int m = gtid(); m < a.nM; m += gthreads()) {
-        int s = sc.mot.boundSeg[m];
-        if (s < 0) continue;
-        int s0 = sc.segMotorOffsets[s], s1 = sc.segMotorOffsets[s + 1];
-        sc.segMotorMyo[s0 + rank_in(a.tmpM, s0, s1, m)] = m;
-    }
-}
-
 // ---------------------------------------------------------------- K: rods
 // TMA bulk copy global -> shared, completion on an mbarrier (no multicast)
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* mbar) {
@@ -664,11 +669,13 @@ __device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
             for (int k = 0; k < 10; k++) bulk_g2s(sc_[k], src[k], bytes, mbar);
         }
     }
-    // the group's CSR row offsets, while the bulk copies run
-    const int* offSrc[3] = {xl.segOffsetsA, xl.segOffsetsB, sc.segMotorOffsets};
-    for (int j = tid; j < 3 * (cnt + 1); j += blockDim.x) {
-        int c = j / (cnt + 1), r = j - c * (cnt + 1);
-        if (c == 2 || a.xlOn) rs.off[c][r] = offSrc[c][g0 + r];
+    // the group's link CSR row offsets, while the bulk copies run
+    if (a.xlOn) {
+        const int* offSrc[2] = {xl.segOffsetsA, xl.segOffsetsB};
+        for (int j = tid; j < 2 * (cnt + 1); j += blockDim.x) {
+            int c = j / (cnt + 1), r = j - c * (cnt + 1);
+            rs.off[c][r] = offSrc[c][g0 + r];
+        }
     }
     int i = g0 + tid;
     int s2 = -1, n2 = 0, s1 = -1, n1 = 0;
@@ -713,30 +720,47 @@ __device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
         if (s2 > i) rs.js[2 * tid + 0] = chain_joint(cp, i, 0, s2, n2, me, rod(s2));
         if (s1 > i) rs.js[2 * tid + 1] = chain_joint(cp, i, 1, s1, n1, me, rod(s1));
     }
-    // the CSR payloads of the group's rows (link A, link B, motor), one entry per thread
+    // the link CSR payloads of the group's rows (link A, link B), one entry per thread
     const int eA = a.xlOn ? rs.off[0][cnt] - rs.off[0][0] : 0;
     const int eB = a.xlOn ? rs.off[1][cnt] - rs.off[1][0] : 0;
-    const int eM = rs.off[2][cnt] - rs.off[2][0];
-    const int eLim = min(eA + eB + eM, FUSED_ENT_CAP);
-    for (int e = (tid - cnt + (int)blockDim.x) % (int)blockDim.x; e < eLim; e += blockDim.x) {
+    const int eLim = min(eA + eB, FUSED_ENT_CAP);
+    const int first = (tid - cnt + (int)blockDim.x) % (int)blockDim.x;
+    for (int e = first; e < eLim; e += blockDim.x) {
         const float* p;
-        bool ok = true;
+        bool ok;
         if (e < eA) {
             int li = xl.segIdxA[rs.off[0][0] + e];
             ok = xl.linkState[li] >= 0;
             p = xl.xlinkData + (int64_t)li * XL_STRIDE;
-        } else if (e < eA + eB) {
+        } else {
             int li = xl.segIdxB[rs.off[1][0] + (e - eA)];
             ok = xl.linkState[li] >= 0;
             p = xl.xlinkData + (int64_t)li * XL_STRIDE + 6;
-        } else {
-            int li = sc.segMotorMyo[rs.off[2][0] + (e - eA - eB)];
-            p = sc.bondData + (int64_t)li * XB_STRIDE + 6;
         }
         float v[6];
         for (int k = 0; k < 6; k++) v[k] = p[k];
         for (int k = 0; k < 6; k++) rs.ent[e][k] = ok ? v[k] : 0.f;
         rs.entOk[e] = ok;
+    }
+    // each rod's bound motors (its list, sorted ascending = the motor CSR row order)
+    for (int l = first; l < cnt; l += blockDim.x) {
+        int* ids = rs.mIds[l];
+        int nm = 0, it = 0;
+        for (int m = a.headM[g0 + l]; m >= 0; m = a.nextM[m]) {
+            if (nm < FUSED_MIDS) {
+                int q = nm;
+                while (q > 0 && ids[q - 1] > m) { ids[q] = ids[q - 1]; q--; }
+                ids[q] = m;
+            }
+            nm++;
+            if (++it > a.nM) { atomicOr(a.err, ERR_LIST); nm = 0; break; }
+        }
+        rs.mCnt[l] = nm;
+        int np = nm < FUSED_MCAP ? nm : FUSED_MCAP;
+        for (int q = 0; q < np; q++) {
+            const float* p = sc.bondData + (int64_t)ids[q] * XB_STRIDE + 6;
+            for (int k = 0; k < 6; k++) rs.mPay[l][q][k] = p[k];
+        }
     }
     __syncthreads();
     if (tid < cnt) {
@@ -762,7 +786,34 @@ __device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
             gather_staged(rs, 1, tid, eA, xl.segIdxB, xl.xlinkData, XL_STRIDE, 6, xl.linkState, gf, gt);
             for (int k = 0; k < 3; k++) { F[k] = (float)(F[k] + gf[k]); T[k] = (float)(T[k] + gt[k]); }
         }
-        gather_staged(rs, 2, tid, eA + eB, sc.segMotorMyo, sc.bondData, XB_STRIDE, 6, nullptr, gf, gt);
+        // CrossBridgeSystem.segGather: FP64 sums of the bound motors' reactions, ascending slot
+        gf[0] = gf[1] = gf[2] = 0.0;
+        gt[0] = gt[1] = gt[2] = 0.0;
+        int nm = rs.mCnt[tid];
+        if (nm <= FUSED_MIDS) {
+            for (int q = 0; q < nm; q++) {
+                const float* p = q < FUSED_MCAP ? rs.mPay[tid][q]
+                                                : sc.bondData + (int64_t)rs.mIds[tid][q] * XB_STRIDE + 6;
+                gf[0] += p[0]; gf[1] += p[1]; gf[2] += p[2];
+                gt[0] += p[3]; gt[1] += p[4]; gt[2] += p[5];
+            }
+        } else {
+            // a long row: take the list's members in ascending order by repeated minimum
+            int last = -1;
+            for (int q = 0; q < nm; q++) {
+                int next = 0x7fffffff, it = 0;
+                for (int m = a.headM[i]; m >= 0 && it <= a.nM; m = a.nextM[m], it++)
+                    if (m > last && m < next) next = m;
+                if (next == 0x7fffffff) {
+                    atomicOr(a.err, ERR_LIST);
+                    break;
+                }
+                const float* p = sc.bondData + (int64_t)next * XB_STRIDE + 6;
+                gf[0] += p[0]; gf[1] += p[1]; gf[2] += p[2];
+                gt[0] += p[3]; gt[1] += p[4]; gt[2] += p[5];
+                last = next;
+            }
+        }
         for (int k = 0; k < 3; k++) { F[k] = (float)(F[k] + gf[k]); T[k] = (float)(T[k] + gt[k]); }
         BoxParams bx = box_params(sc.boxParams, t);
         float c[3] = {sc_[0][tid], sc_[1][tid], sc_[2][tid]};
@@ -772,19 +823,56 @@ __device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
     }
 }
 
-__device__ void phase_rods(const FusedArgs& a, FusedSmem& sm, int t, uint64_t* mbar, unsigned& phase) {
-    for (int u = blockIdx.x; u < a.nRodUnits; u += gridDim.x) rod_unit(a, sm.rod, u, t, mbar, phase);
-    // reset the private histograms for the next step
-    for (int i = gtid(); i < a.C; i += gthreads()) { a.cntCell[i] = 0; a.cntSeg[i] = 0; }
-    for (int i = gtid(); i < a.nSeg; i += gthreads()) {
-        a.cntAct[i] = 0; a.cntA[i] = 0; a.cntB[i] = 0; a.cntM[i] = 0;
+// The motor CSR of the reference's cpuStep (CrossBridgeSystem.csrHistogram/csrScan/
+// csrScatter, CrossBridgeSystem.java:190-217) built by the helper CTAs while the rod units
+// gather from the lists: tile sums, scan (segMotorOffsets, segMotorCount = row lengths),
+// then each bound motor placed at its rank in its segment's list.
+__device__ void motor_csr(const FusedArgs& a, int h, int nH, unsigned long long& hTarget) {
+    const sbx_dense_scene& sc = a.sc;
+    int wpc = blockDim.x >> 5;
+    int hw = h * wpc + (threadIdx.x >> 5), nhw = nH * wpc;
+    ScanArr arr[1] = {{a.cntM, a.nSeg, 0}};
+    tile_sums(arr, 1, a.mTileSum, hw, nhw);
+    if (!counter_sync(a.bar + 1, hTarget, nH, a.err)) return;
+    int* out[1] = {sc.segMotorOffsets};
+    int* copy[1] = {sc.segMotorCount};
+    int clamp[1] = {a.nM};
+    tile_scan(arr, 1, a.mTileSum, out, copy, clamp, nullptr, hw, nhw);
+    if (!counter_sync(a.bar + 1, hTarget, nH, a.err)) return;
+    for (int m = h * blockDim.x + threadIdx.x; m < a.nM; m += nH * blockDim.x) {
+        int bs = sc.mot.boundSeg[m];
+        if (bs < 0) continue;
+        int pos = sc.segMotorOffsets[bs] + list_rank(a, a.headM[bs], a.nextM, m, a.nM);
+        if (pos < a.nM) sc.segMotorMyo[pos] = m;
     }
 }
 
-__global__ void __launch_bounds__(FUSED_THREADS) k_dense_fused(FusedArgs a, int t0, int nsteps) {
+__device__ void phase_rods(const FusedArgs& a, FusedSmem& sm, int t, uint64_t* mbar, unsigned& phase,
+                           unsigned long long& hTarget) {
+    for (int u = blockIdx.x; u < a.nRodUnits; u += gridDim.x) rod_unit(a, sm.rod, u, t, mbar, phase);
+    if ((int)blockIdx.x >= a.kHelp0) motor_csr(a, blockIdx.x - a.kHelp0, gridDim.x - a.kHelp0, hTarget);
+    // reset the histograms and lists of this step's grid and link CSRs for the next step
+    for (int i = gtid(); i < a.C; i += gthreads()) { a.cntCell[i] = 0; a.cntSeg[i] = 0; a.cellHead[i] = -1; }
+    for (int i = gtid(); i < a.nSeg; i += gthreads()) {
+        a.cntAct[i] = 0; a.cntA[i] = 0; a.cntB[i] = 0; a.headA[i] = -1; a.headB[i] = -1;
+    }
+}
+
+__global__ void __launch_bounds__(FUSED_THREADS, 4) k_dense_fused(FusedArgs a, int t0, int nsteps) {
     __shared__ __align__(8) uint64_t mbar;
-    __shared__ __align__(16) FusedSmem sm;
+    extern __shared__ __align__(16) unsigned char fused_dsm[];
+    FusedSmem& sm = *reinterpret_cast<FusedSmem*>(fused_dsm);
     unsigned phase = 0;
+    // a run after an unreported failure (barrier, bulk-copy or list fault) does nothing
+    // until the plan status has been read, which re-initialises the scratch
+    if (vload(a.err) & (ERR_BARRIER | ERR_TMA | ERR_LIST)) return;
+    const unsigned nGrid = gridDim.x + (unsigned)a.barrierExtra;
+    const unsigned nHelp = gridDim.x - (unsigned)a.kHelp0;
+    unsigned long long gTarget = 0, hTarget = 0;
+    if (threadIdx.x == 0) {
+        gTarget = counter_base(a.bar, nGrid);
+        hTarget = counter_base(a.bar + 1, nHelp);
+    }
     if (threadIdx.x == 0) {
         unsigned mb = (unsigned)__cvta_generic_to_shared(&mbar);
         asm volatile("mbarrier.init.shared.b64 [%0], 1;\n" :: "r"(mb) : "memory");
@@ -796,12 +884,9 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_dense_fused(FusedArgs a, int 
                         {a.cntB, a.nSeg, 2 * a.tilesC + a.tilesS}};
     int narr1 = a.xlOn ? 4 : 2;
     int* out1[4] = {sc.grid.gridCellOffsets, a.segCellOff, sc.xl.segOffsetsA, sc.xl.segOffsetsB};
-    int* zero1[4] = {sc.grid.cellCount, nullptr, sc.xl.segCountA, sc.xl.segCountB};
+    int* copy1[4] = {sc.grid.cellCount, nullptr, sc.xl.segCountA, sc.xl.segCountB};
     int clamp1[4] = {a.cap, a.nSeg, a.nL, a.nL};
-    ScanArr second[1] = {{a.cntM, a.nSeg, 0}};
-    int* out2[1] = {sc.segMotorOffsets};
-    int* zero2[1] = {sc.segMotorCount};
-    int clamp2[1] = {a.nM};
+    const int gw = gtid() >> 5, nw = gthreads() >> 5;
     int ph = 0;
     auto stamp = [&](int s_) {
         if (a.phaseTimes && gtid() == 0) {
@@ -821,38 +906,28 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_dense_fused(FusedArgs a, int 
             sc.fil.counts[1] = t;
             if (a.xlOn) { sc.xl.counts[1] = t; sc.xl.counts[2] = sc.seed; }
         }
+        // A: body view, bins, histograms and lists, crosslinker unbind, motor Brownian
         phase_publish_bin(a, t);
-        if (!grid_sync(a)) return;
+        if (!counter_sync(a.bar, gTarget, nGrid, a.err)) return;
         stamp(s);
-        tile_sums(first, narr1, a.tileSum);
-        if (!grid_sync(a)) return;
+        // B, C: scans of the cell, segment-per-cell and link-key histograms
+        tile_sums(first, narr1, a.tileSum, gw, nw);
+        if (!counter_sync(a.bar, gTarget, nGrid, a.err)) return;
         stamp(s);
-        tile_scan(first, narr1, a.tileSum, out1, zero1, clamp1, sc.grid.chunkSum);
-        if (!grid_sync(a)) return;
+        tile_scan(first, narr1, a.tileSum, out1, copy1, clamp1, sc.grid.chunkSum, gw, nw);
+        if (!counter_sync(a.bar, gTarget, nGrid, a.err)) return;
         stamp(s);
-        phase_scatter(a);
-        if (!grid_sync(a)) return;
+        // E: stable placement (grid contents, segment endpoints, link CSR lists)
+        phase_place(a);
+        if (!counter_sync(a.bar, gTarget, nGrid, a.err)) return;
         stamp(s);
-        phase_rank(a);
-        if (!grid_sync(a)) return;
-        stamp(s);
+        // F: minifilaments (binding + myosin mechanics), crosslinker forces, filament Brownian
         phase_motors_links(a, sm, t);
-        if (!grid_sync(a)) return;
+        if (!counter_sync(a.bar, gTarget, nGrid, a.err)) return;
         stamp(s);
-        tile_sums(second, 1, a.tileSum);
-        if (!grid_sync(a)) return;
-        stamp(s);
-        tile_scan(second, 1, a.tileSum, out2, zero2, clamp2, nullptr);
-        if (!grid_sync(a)) return;
-        stamp(s);
-        phase_motor_scatter(a);
-        if (!grid_sync(a)) return;
-        stamp(s);
-        phase_motor_rank(a);
-        if (!grid_sync(a)) return;
-        stamp(s);
-        phase_rods(a, sm, t, &mbar, phase);
-        if (!grid_sync(a)) return;
+        // K: rods; helpers build the motor CSR and reset the step's histograms and lists
+        phase_rods(a, sm, t, &mbar, phase, hTarget);
+        if (!counter_sync(a.bar, gTarget, nGrid, a.err)) return;
         stamp(s);
     }
     if (gtid() == 0 && a.d_step) *a.d_step = t0 + nsteps;
@@ -862,7 +937,8 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_dense_fused(FusedArgs a, int 
 
 sbx_status fused_launch(sbx_ctx* ctx, FusedArgs& a, int grid, int t0, int nsteps) {
     void* args[] = {&a, &t0, &nsteps};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_dense_fused, grid, FUSED_THREADS, args, 0, ctx->stream);
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_dense_fused, grid, FUSED_THREADS, args,
+                                                sizeof(FusedSmem), ctx->stream);
     ctx->launches++;
     if (e != cudaSuccess) return fail(ctx, SBX_ECUDA, std::string("fused launch: ") + cudaGetErrorString(e));
     return SBX_OK;
@@ -870,7 +946,12 @@ sbx_status fused_launch(sbx_ctx* ctx, FusedArgs& a, int grid, int t0, int nsteps
 
 int fused_max_blocks_per_sm() {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_dense_fused, FUSED_THREADS, 0);
+    if (cudaFuncSetAttribute(k_dense_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FusedSmem)) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_dense_fused, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+        return 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_dense_fused, FUSED_THREADS, sizeof(FusedSmem));
     return nb;
 }
 

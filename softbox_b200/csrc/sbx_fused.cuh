@@ -5,9 +5,12 @@
 
 constexpr int FUSED_THREADS = 128;
 constexpr int FUSED_MAX_SUB = 120;    // sub-bodies per minifilament CTA (6 per dimer)
-constexpr int FUSED_MAX_ROD = 128;    // segments per rod CTA
+constexpr int FUSED_MAX_ROD = 64;     // segments per rod CTA (whole filaments)
 constexpr int FUSED_MAX_DPM = 16;     // dimers per minifilament (32 heads: one warp)
 constexpr int FUSED_ENT_CAP = 256;    // CSR payload entries a rod CTA stages in shared memory
+constexpr int FUSED_MCAP = 4;         // motor reactions per segment a rod CTA stages in shared memory
+constexpr int FUSED_MIDS = 16;        // motor slots per segment a rod CTA sorts (more: repeated-minimum walk)
+constexpr int FUSED_MIN_HELPERS = 16; // CTAs kept free of rod units in the rod phase
 
 struct FusedArgs {
     sbx_dense_scene sc;
@@ -18,20 +21,24 @@ struct FusedArgs {
     int tilesC, tilesS;
     int xlOn, xlUnbind, useTma, filSeed;
     int jointShare;          // chain neighbours are symmetric: each joint computed once
+    int kHelp0;              // first CTA of the rod phase's helpers (motor CSR build, resets)
     // private scratch (plan-owned)
     int *cntCell, *cntSeg, *cntAct, *cntA, *cntB, *cntM;   // cntSeg: segments per cell
     int* segCellOff;         // segment-only exclusive prefix over cells (C + 1)
-    int* tileSum;
-    int *tmpCell, *tmpA, *tmpB, *tmpM;
+    int* tileSum;            // tile sums of the step's scans (cells, segments, link A, link B)
+    int* mTileSum;           // tile sums of the motor CSR scan
+    // singly linked lists (head per row, next per item; -1 ends): cells, link A/B keys,
+    // motors per bound segment
+    int *cellHead, *cellNext, *headA, *nextA, *headB, *nextB, *headM, *nextM;
     float4 *segE1, *segE2;   // segment endpoints in cell order: {end1, slot}, {end2, 0}
-    unsigned* bar;           // [0] arrivals, [1] generation
-    int* err;                // bit0 barrier timeout, bit1 reach overflow, bit2 TMA wait timeout
+    unsigned long long* bar; // arrival counters (monotonic): [0] grid barrier, [1] rod-phase helpers
+    int* err;                // bit0 barrier timeout, bit1 reach overflow, bit2 TMA wait timeout, bit3 list walk
     int* d_step;
     int barrierExtra;        // test hook: arrivals the barrier waits for beyond gridDim.x
     long long* phaseTimes;   // optional: %globaltimer after each phase barrier, [nsteps][FUSED_PHASES]
 };
 
-constexpr int FUSED_PHASES = 11;
+constexpr int FUSED_PHASES = SBX_FUSED_PHASES;
 
 sbx_status fused_launch(sbx_ctx* ctx, FusedArgs& a, int grid, int t0, int nsteps);
 int fused_max_blocks_per_sm();

@@ -16,10 +16,10 @@ from . import scenes
 from .engine import DenseNetwork
 from .runtime import LIB
 
-PHASES = ["A publish, bin, histograms, crosslinker unbind",   # measured as K(prev) -> A
-          "B tile sums", "C scans", "D scatter", "E rank + sorted endpoints",
-          "F minifilaments + crosslinker forces", "G motor tile sums + filament Brownian", "H motor scan",
-          "I motor scatter", "J motor rank", "K rods"]
+PHASES = ["A publish, bin, histograms + lists, crosslinker unbind, motor Brownian",   # K(prev) -> A
+          "B tile sums", "C scans", "E stable placement",
+          "F minifilaments + crosslinker forces + filament Brownian",
+          "K rods (+ motor CSR helpers, resets)"]
 
 
 def phase_times(steps=200, fp64_coords=False, cfg=None):
