@@ -280,12 +280,16 @@ bool fused_prepare(sbx_dense_plan* p) {
     a.cntM = (int*)alloc(4 * nS);
     a.tileSum = (int*)alloc(4 * (size_t)(2 * a.tilesC + 2 * a.tilesS + 1));
     a.mTileSum = (int*)alloc(4 * (size_t)(a.tilesS + 1));
+    a.cellSlot = (int*)alloc(4 * (size_t)a.C * FUSED_CELL_SLOTS);
+    a.slotA = (int*)alloc(4 * nS * FUSED_ROW_SLOTS); a.slotB = (int*)alloc(4 * nS * FUSED_ROW_SLOTS);
+    a.slotM = (int*)alloc(4 * nS * FUSED_ROW_SLOTS);
     a.cellHead = (int*)alloc(4 * (size_t)a.C); a.cellNext = (int*)alloc(4 * (size_t)a.cap);
     size_t nLk = (size_t)std::max(a.nL, 1);
     a.headA = (int*)alloc(4 * nS); a.nextA = (int*)alloc(4 * nLk);
     a.headB = (int*)alloc(4 * nS); a.nextB = (int*)alloc(4 * nLk);
     a.headM = (int*)alloc(4 * nS); a.nextM = (int*)alloc(4 * (size_t)a.nM);
     a.segE1 = (float4*)alloc(16 * nS); a.segE2 = (float4*)alloc(16 * nS);
+    a.joints = alloc(2 * nS * FUSED_JOINT_BYTES);
     a.bar = (unsigned long long*)alloc(32);
     a.err = (int*)alloc(16);
     a.d_step = p->d_step;

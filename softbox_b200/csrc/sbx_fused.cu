@@ -5,12 +5,13 @@
 // error bit 0 and every CTA returns, so a fault cannot hang the device):
 //
 //   A  publish the body view (FilamentStore/MotorStore.publish*), bin bodies
-//      (SpatialGrid.bodyCell): cell histogram, segments-per-cell histogram and a list
-//      per cell; crosslinker Bell unbind, active-link counts, link-key histograms and
-//      lists; Brownian draws of the motor sub-bodies and backbones
-//   B  tile sums of the four histograms
+//      (SpatialGrid.bodyCell): cell histogram (+ row slots), segments-per-cell
+//      histogram; link-key histograms (+ row slots)
+//   B  tile sums of the four histograms; the warps without a tile run the crosslinker
+//      Bell unbind and count the active links
 //   C  exclusive scans -> gridCellOffsets (+ chunkSum, cellCount), the segment-only cell
-//      prefix, segOffsetsA / segOffsetsB (+ counts)
+//      prefix, segOffsetsA / segOffsetsB (+ counts); the warps without a tile draw the
+//      Brownian forces of the motor sub-bodies and backbones
 //   E  stable placement by list rank -> gridCellContents, segIdxA, segIdxB and the
 //      segment endpoints in cell order (float4) for the reach walk
 //   F  one CTA per minifilament: binding of its 32 heads (reach walk fused with the
@@ -47,7 +48,6 @@ constexpr int ERR_BARRIER = 1, ERR_REACH_OVERFLOW = 2, ERR_TMA = 4, ERR_LIST = 8
 struct RodSmem {
     float st[10 * FUSED_MAX_ROD];                 // staged rod geometry planes (TMA destination)
     int off[3][FUSED_MAX_ROD + 1];                // the group's CSR row offsets: links A, links B, motors
-    ChainJoint js[2 * FUSED_MAX_ROD];             // joints, at (owner rod, owner side)
     float ent[FUSED_ENT_CAP][6];                  // the group's link CSR payloads, in CSR order
     int entOk[FUSED_ENT_CAP];                     // guard passed (active link)
     int mCnt[FUSED_MAX_ROD];                      // motors bound to each rod
@@ -61,6 +61,8 @@ struct MiniSmem {
     LeverTerm lt[FUSED_MAX_DPM];
     TetherTerm tt[FUSED_MAX_DPM];
 };
+static_assert(sizeof(ChainJoint) <= FUSED_JOINT_BYTES, "joint slot size");
+
 union FusedSmem {
     RodSmem rod;
     MiniSmem mini;
@@ -131,6 +133,43 @@ __device__ __forceinline__ void brownian_slot(const sbx_rigid_body& b, int s, in
     for (int k = 0; k < 3; k++) { b.randForce[k * n + s] = rf[k]; b.randTorque[k * n + s] = rt[k]; }
 }
 
+// ---------------------------------------------------------------- rows: slots + overflow lists
+// Rank of `self` in a row = the number of the row's items with a smaller index, counted
+// along the row's list: the position the reference's serial scatter gives it (items are
+// scattered in ascending index). A walk longer than `bound` marks the list corrupt.
+__device__ __forceinline__ int list_rank(const FusedArgs& a, int head, const int* next, int self, int bound) {
+    int r = 0, it = 0;
+    for (int j = head; j >= 0; j = next[j]) {
+        r += j < self;
+        if (++it > bound) {
+            atomicOr(a.err, ERR_LIST);
+            break;
+        }
+    }
+    return r;
+}
+
+// Appends `item` to row r: the histogram's old count is its arrival index; the first S
+// arrivals take the row's fixed slots, later ones join the row's overflow list.
+__device__ __forceinline__ void row_insert(int* cnt, int* slot, int S, int* head, int* next, int r, int item) {
+    int j = atomicAdd(&cnt[r], 1);
+    if (j < S) slot[(size_t)r * S + j] = item;
+    else next[item] = atomicExch(&head[r], item);
+}
+
+// rank of `item` in row r: the row's members with a smaller index (slots, then the list)
+template <int S>
+__device__ __forceinline__ int row_rank(const FusedArgs& a, const int* cnt, const int* slot, const int* head,
+                                        const int* next, int r, int item, int bound) {
+    int n = cnt[r];
+    int rank = 0;
+#pragma unroll
+    for (int j = 0; j < S; j++)
+        if (j < n) rank += slot[(size_t)r * S + j] < item;
+    if (n > S) rank += list_rank(a, head[r], next, item, bound);
+    return rank;
+}
+
 // ---------------------------------------------------------------- phase A
 __device__ void phase_publish_bin(const FusedArgs& a, int t) {
     const sbx_dense_scene& sc = a.sc;
@@ -142,20 +181,13 @@ __device__ void phase_publish_bin(const FusedArgs& a, int t) {
     const float* gp = g.gridParams;
     const int nX = a.nX, nY = a.nY, nZ = a.nZ;
     const int nLk = a.xlOn ? a.nL : 0;
-    const int total = cap + nLk + nB + a.nBb + nSeg;
+    const int total = cap + nLk + nSeg;
     for (int i = gtid(); i < total; i += gthreads()) {
-        if (i >= cap + nLk + nB + a.nBb) {
+        if (i >= cap + nLk) {
             // the motor lists and counts of the previous step were last read by its rod phase
-            int s = i - (cap + nLk + nB + a.nBb);
+            int s = i - (cap + nLk);
             a.headM[s] = -1;
             a.cntM[s] = 0;
-            continue;
-        }
-        if (i >= cap + nLk) {
-            // BrownianForceSystem for the motor sub-bodies, then the backbones
-            int j = i - cap - nLk;
-            if (j < nB) brownian_slot(mb, j, t, sc.seed, sc.mot.bodyParams[1]);
-            else brownian_slot(sc.mini.backbone, j - nB, t, sc.seedBb, sc.mini.bbBodyParams[1]);
             continue;
         }
         if (i < nSeg) {
@@ -168,9 +200,8 @@ __device__ void phase_publish_bin(const FusedArgs& a, int t) {
                 int cell = cell_coord(c[0], gp[0], gp[4], nX) + cell_coord(c[1], gp[1], gp[4], nY) * nX +
                            cell_coord(c[2], gp[2], gp[4], nZ) * (nX * nY);
                 g.bodyCell[i] = cell;
-                atomicAdd(&a.cntCell[cell], 1);
                 atomicAdd(&a.cntSeg[cell], 1);
-                a.cellNext[i] = atomicExch(&a.cellHead[cell], i);
+                row_insert(a.cntCell, a.cellSlot, FUSED_CELL_SLOTS, a.cellHead, a.cellNext, cell, i);
             } else {
                 g.bodyCell[i] = -1;
             }
@@ -193,8 +224,7 @@ __device__ void phase_publish_bin(const FusedArgs& a, int t) {
                 int cell = cell_coord(hd[0], gp[0], gp[4], nX) + cell_coord(hd[1], gp[1], gp[4], nY) * nX +
                            cell_coord(hd[2], gp[2], gp[4], nZ) * (nX * nY);
                 g.bodyCell[b] = cell;
-                atomicAdd(&a.cntCell[cell], 1);
-                a.cellNext[b] = atomicExch(&a.cellHead[cell], b);
+                row_insert(a.cntCell, a.cellSlot, FUSED_CELL_SLOTS, a.cellHead, a.cellNext, cell, b);
             } else {
                 g.bodyCell[b] = -1;
             }
@@ -203,20 +233,49 @@ __device__ void phase_publish_bin(const FusedArgs& a, int t) {
         } else {
             int k = i - cap;
             int la = xl.linkFilA[k], lb = xl.linkFilB[k];
-            int state = xl.linkState[k];
-            if (a.xlUnbind && state >= 0 &&
-                unbind_one(k, nSeg, fb.uVec, fb.end1, la, lb, xl.loc1[k], xl.loc2[k], xl.strainHist, xl.strainPlace,
-                           xl.offParams, t, sc.seed)) {
-                state = LINK_FREE;
-                xl.linkState[k] = state;
-            }
-            if (state >= 0) {
-                atomicAdd(&a.cntAct[la], 1);
-                atomicAdd(&a.cntAct[lb], 1);
-            }
-            if (la >= 0) { atomicAdd(&a.cntA[la], 1); a.nextA[k] = atomicExch(&a.headA[la], k); }
-            if (lb >= 0) { atomicAdd(&a.cntB[lb], 1); a.nextB[k] = atomicExch(&a.headB[lb], k); }
+            if (la >= 0) row_insert(a.cntA, a.slotA, FUSED_ROW_SLOTS, a.headA, a.nextA, la, k);
+            if (lb >= 0) row_insert(a.cntB, a.slotB, FUSED_ROW_SLOTS, a.headB, a.nextB, lb, k);
         }
+    }
+}
+
+// CrosslinkerSystem.unbind (Bell law over the strain window, CrosslinkerSystem.java:
+// 727-756) and countActiveLinks (:694-708), on the warps from `firstWarp` on (all warps
+// when there are none). The link CSR keys (linkFilA/B) do not depend on the state.
+__device__ void link_unbind(const FusedArgs& a, int t, int firstWarp) {
+    const sbx_dense_scene& sc = a.sc;
+    const sbx_crosslinker_store& xl = sc.xl;
+    const sbx_rigid_body& fb = sc.fil.body;
+    int w = gtid() >> 5, nw = gthreads() >> 5;
+    if (firstWarp >= nw) firstWarp = 0;
+    if (w < firstWarp) return;
+    for (int k = (w - firstWarp) * 32 + (threadIdx.x & 31); k < a.nL; k += (nw - firstWarp) * 32) {
+        int la = xl.linkFilA[k], lb = xl.linkFilB[k];
+        int state = xl.linkState[k];
+        if (a.xlUnbind && state >= 0 &&
+            unbind_one(k, a.nSeg, fb.uVec, fb.end1, la, lb, xl.loc1[k], xl.loc2[k], xl.strainHist, xl.strainPlace,
+                       xl.offParams, t, sc.seed)) {
+            state = LINK_FREE;
+            xl.linkState[k] = state;
+        }
+        if (state >= 0) {
+            atomicAdd(&a.cntAct[la], 1);
+            atomicAdd(&a.cntAct[lb], 1);
+        }
+    }
+}
+
+// BrownianForceSystem for the motor sub-bodies, then the backbones, on the warps from
+// `firstWarp` on (all warps when there are none)
+__device__ void motor_brownian(const FusedArgs& a, int t, int firstWarp) {
+    const sbx_dense_scene& sc = a.sc;
+    int w = gtid() >> 5, nw = gthreads() >> 5;
+    if (firstWarp >= nw) firstWarp = 0;
+    if (w < firstWarp) return;
+    const int nB = a.nB, n = nB + a.nBb;
+    for (int j = (w - firstWarp) * 32 + (threadIdx.x & 31); j < n; j += (nw - firstWarp) * 32) {
+        if (j < nB) brownian_slot(sc.mot.body, j, t, sc.seed, sc.mot.bodyParams[1]);
+        else brownian_slot(sc.mini.backbone, j - nB, t, sc.seedBb, sc.mini.bbBodyParams[1]);
     }
 }
 
@@ -307,21 +366,6 @@ __device__ void tile_scan(const ScanArr* arrs, int narr, const int* tileSum, int
 }
 
 // ---------------------------------------------------------------- E: stable placement
-// Rank of `self` in a row = the number of the row's items with a smaller index, counted
-// along the row's list: the position the reference's serial scatter gives it (items are
-// scattered in ascending index). A walk longer than `bound` marks the list corrupt.
-__device__ __forceinline__ int list_rank(const FusedArgs& a, int head, const int* next, int self, int bound) {
-    int r = 0, it = 0;
-    for (int j = head; j >= 0; j = next[j]) {
-        r += j < self;
-        if (++it > bound) {
-            atomicOr(a.err, ERR_LIST);
-            break;
-        }
-    }
-    return r;
-}
-
 __device__ void phase_place(const FusedArgs& a) {
     const sbx_dense_scene& sc = a.sc;
     const sbx_grid_state& g = sc.grid;
@@ -333,7 +377,7 @@ __device__ void phase_place(const FusedArgs& a) {
         if (i < a.cap) {
             int c = g.bodyCell[i];
             if (c < 0) continue;
-            int rank = list_rank(a, a.cellHead[c], a.cellNext, i, a.cap);
+            int rank = row_rank<FUSED_CELL_SLOTS>(a, a.cntCell, a.cellSlot, a.cellHead, a.cellNext, c, i, a.cap);
             g.gridCellContents[g.gridCellOffsets[c] + rank] = i;
             // segment endpoints in cell order for the reach walk: within a cell the segments
             // (slots below nSeg) precede the motor heads, so a segment's rank among the
@@ -346,8 +390,12 @@ __device__ void phase_place(const FusedArgs& a) {
         } else {
             int k = i - a.cap;
             int la = xl.linkFilA[k], lb = xl.linkFilB[k];
-            if (la >= 0) xl.segIdxA[xl.segOffsetsA[la] + list_rank(a, a.headA[la], a.nextA, k, a.nL)] = k;
-            if (lb >= 0) xl.segIdxB[xl.segOffsetsB[lb] + list_rank(a, a.headB[lb], a.nextB, k, a.nL)] = k;
+            if (la >= 0)
+                xl.segIdxA[xl.segOffsetsA[la] +
+                           row_rank<FUSED_ROW_SLOTS>(a, a.cntA, a.slotA, a.headA, a.nextA, la, k, a.nL)] = k;
+            if (lb >= 0)
+                xl.segIdxB[xl.segOffsetsB[lb] +
+                           row_rank<FUSED_ROW_SLOTS>(a, a.cntB, a.slotB, a.headB, a.nextB, lb, k, a.nL)] = k;
         }
     }
 }
@@ -376,23 +424,42 @@ __device__ int reach_walk_bind(const FusedArgs& a, float mx, float my, float mz,
         rs[r] = ok ? off[c0] : 0;
         re[r] = ok ? off[c0 + (x1 - x0) + 1] : 0;
     }
+    // the nine ranges as one sequence k = 0..total-1 (row order, then index order), taken
+    // four items at a time so that their loads are in flight together
+    int pre[10];
+    pre[0] = 0;
+#pragma unroll
+    for (int r = 0; r < 9; r++) pre[r + 1] = pre[r] + (re[r] - rs[r]);
+    const int total = pre[9];
     int cnt = 0, best = -1;
     float bestD = 1.0e30f, arc = 0.f;
+    for (int k0 = 0; k0 < total; k0 += 4) {
+        float4 e1[4], e2[4];
 #pragma unroll
-    for (int r = 0; r < 9; r++) {
-        for (int idx = rs[r]; idx < re[r]; idx++) {
-            float4 e1 = a.segE1[idx];
-            float4 e2 = a.segE2[idx];
-            float d = reach_test_dist_sq(mx, my, mz, mux, muy, muz, rux, ruy, ruz, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z,
-                                         tol, align);
+        for (int q = 0; q < 4; q++) {
+            int k = k0 + q;
+            if (k < total) {
+                int idx = rs[0] + k;
+#pragma unroll
+                for (int r = 1; r < 9; r++)
+                    if (k >= pre[r]) idx = rs[r] + (k - pre[r]);
+                e1[q] = a.segE1[idx];
+                e2[q] = a.segE2[idx];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (k0 + q >= total) break;
+            float d = reach_test_dist_sq(mx, my, mz, mux, muy, muz, rux, ruy, ruz, e1[q].x, e1[q].y, e1[q].z, e2[q].x,
+                                         e2[q].y, e2[q].z, tol, align);
             if (d >= 0.f) {
                 if (cnt < MAX_CAND) {
-                    int sg = __float_as_int(e1.w);
+                    int sg = __float_as_int(e1[q].w);
                     out[cnt] = sg;
                     if (d < bestD) {
                         bestD = d;
                         best = sg;
-                        arc = bind_arc(mx, my, mz, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z);
+                        arc = bind_arc(mx, my, mz, e1[q].x, e1[q].y, e1[q].z, e2[q].x, e2[q].y, e2[q].z);
                     }
                 }
                 cnt++;
@@ -450,10 +517,7 @@ __device__ void mini_unit(const FusedArgs& a, MiniSmem& ms, int u, int t) {
             mot.capStats[m] = cs;
             mot.nucleotideState[m] = cycle_one(m, mot.nucleotideState[m], bs >= 0, mot.forceDotHist + 10 * m,
                                                mot.nucParams, t, sc.seed);
-            if (bs >= 0) {
-                atomicAdd(&a.cntM[bs], 1);
-                a.nextM[m] = atomicExch(&a.headM[bs], m);
-            }
+            if (bs >= 0) row_insert(a.cntM, a.slotM, FUSED_ROW_SLOTS, a.headM, a.nextM, bs, m);
         }
     } else if (tid < 96) {
         // warps 1-2: motor joints (local motor k/2, joint k&1), then a lever (warp 1) or a tether (warp 2)
@@ -597,13 +661,34 @@ __device__ void phase_motors_links(const FusedArgs& a, FusedSmem& sm, int t) {
             if (k < a.nL) link_item(a, k);
         }
     }
-    // filament Brownian forcing on the CTAs without a unit (all CTAs when there are none)
+    // on the CTAs without a unit (all CTAs when there are none): the chain joints of the
+    // filaments (ChainBendingForceSystem's costly part, from this step's start poses; each
+    // joint once, by its lower-slot rod) and the filament Brownian forcing
     const sbx_filament_store& fs = a.sc.fil;
+    const sbx_rigid_body& fb = fs.body;
     int helpers = (int)gridDim.x - units, h0 = units;
     if (helpers <= 0) { helpers = gridDim.x; h0 = 0; }
-    if ((int)blockIdx.x >= h0)
-        for (int i = ((int)blockIdx.x - h0) * blockDim.x + threadIdx.x; i < a.nSeg; i += helpers * blockDim.x)
-            brownian_slot(fs.body, i, t, a.filSeed, fs.params[1]);
+    if ((int)blockIdx.x >= h0) {
+        ChainJoint* J = reinterpret_cast<ChainJoint*>(a.joints);
+        const int n = a.nSeg;
+        ChainParams cp = chain_params(fs.chainParams);
+        for (int i = ((int)blockIdx.x - h0) * blockDim.x + threadIdx.x; i < n; i += helpers * blockDim.x) {
+            if (a.jointShare) {
+                int s2 = fs.end2NbrSlot[i], s1 = fs.end1NbrSlot[i];
+                if (s2 > i || s1 > i) {
+                    RodGeom me = load_rod(n, i, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.bRotGam);
+                    if (s2 > i)
+                        J[2 * i] = chain_joint(cp, i, 0, s2, fs.end2NbrSide[i], me,
+                                               load_rod(n, s2, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.bRotGam));
+                    if (s1 > i)
+                        J[2 * i + 1] =
+                            chain_joint(cp, i, 1, s1, fs.end1NbrSide[i], me,
+                                        load_rod(n, s1, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.bRotGam));
+                }
+            }
+            brownian_slot(fb, i, t, a.filSeed, fs.params[1]);
+        }
+    }
     // the reference's activeLinkCount array holds this step's counts
     if (a.xlOn)
         for (int s = gtid(); s < a.nSeg; s += gthreads()) a.sc.xl.activeLinkCount[s] = a.cntAct[s];
@@ -714,17 +799,18 @@ __device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
         r.bTGx = sc_[7][l]; r.bTGy = sc_[8][l]; r.bRGy = sc_[9][l];
         return r;
     };
-    // each joint once, by its lower-slot rod
+    // this rod's two joints (computed in the minifilament phase), loaded ahead of use
+    const ChainJoint* Jg = reinterpret_cast<const ChainJoint*>(a.joints);
+    ChainJoint j2, j1;
     if (a.jointShare && tid < cnt) {
-        RodGeom me = rod(i);
-        if (s2 > i) rs.js[2 * tid + 0] = chain_joint(cp, i, 0, s2, n2, me, rod(s2));
-        if (s1 > i) rs.js[2 * tid + 1] = chain_joint(cp, i, 1, s1, n1, me, rod(s1));
+        if (s2 >= 0) j2 = Jg[s2 > i ? 2 * i : 2 * s2 + (1 - n2)];
+        if (s1 >= 0) j1 = Jg[s1 > i ? 2 * i + 1 : 2 * s1 + (1 - n1)];
     }
     // the link CSR payloads of the group's rows (link A, link B), one entry per thread
     const int eA = a.xlOn ? rs.off[0][cnt] - rs.off[0][0] : 0;
     const int eB = a.xlOn ? rs.off[1][cnt] - rs.off[1][0] : 0;
     const int eLim = min(eA + eB, FUSED_ENT_CAP);
-    const int first = (tid - cnt + (int)blockDim.x) % (int)blockDim.x;
+    const int first = tid;
     for (int e = first; e < eLim; e += blockDim.x) {
         const float* p;
         bool ok;
@@ -742,21 +828,37 @@ __device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
         for (int k = 0; k < 6; k++) rs.ent[e][k] = ok ? v[k] : 0.f;
         rs.entOk[e] = ok;
     }
-    // each rod's bound motors (its list, sorted ascending = the motor CSR row order)
+    // each rod's bound motors (its row's slots and overflow list), sorted ascending = the
+    // motor CSR row order
     for (int l = first; l < cnt; l += blockDim.x) {
         int* ids = rs.mIds[l];
-        int nm = 0, it = 0;
-        for (int m = a.headM[g0 + l]; m >= 0; m = a.nextM[m]) {
-            if (nm < FUSED_MIDS) {
-                int q = nm;
+        const int r = g0 + l;
+        const int nm = a.cntM[r];
+        int got = 0;
+        auto put = [&](int m) {
+            if (got < FUSED_MIDS) {
+                int q = got;
                 while (q > 0 && ids[q - 1] > m) { ids[q] = ids[q - 1]; q--; }
                 ids[q] = m;
             }
-            nm++;
-            if (++it > a.nM) { atomicOr(a.err, ERR_LIST); nm = 0; break; }
+            got++;
+        };
+        int sl[FUSED_ROW_SLOTS];
+#pragma unroll
+        for (int j = 0; j < FUSED_ROW_SLOTS; j++) sl[j] = j < nm ? a.slotM[(size_t)r * FUSED_ROW_SLOTS + j] : 0;
+#pragma unroll
+        for (int j = 0; j < FUSED_ROW_SLOTS; j++)
+            if (j < nm) put(sl[j]);
+        if (nm > FUSED_ROW_SLOTS) {
+            int it = 0;
+            for (int m = a.headM[r]; m >= 0; m = a.nextM[m]) {
+                put(m);
+                if (++it > a.nM) { atomicOr(a.err, ERR_LIST); break; }
+            }
         }
-        rs.mCnt[l] = nm;
+        rs.mCnt[l] = got == nm ? nm : 0;
         int np = nm < FUSED_MCAP ? nm : FUSED_MCAP;
+        if (got != nm) np = 0;
         for (int q = 0; q < np; q++) {
             const float* p = sc.bondData + (int64_t)ids[q] * XB_STRIDE + 6;
             for (int k = 0; k < 6; k++) rs.mPay[l][q][k] = p[k];
@@ -767,12 +869,8 @@ __device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
         RodGeom me = rod(i);
         double fd[3] = {0, 0, 0}, td[3] = {0, 0, 0};
         if (a.jointShare) {
-            if (s2 >= 0)
-                chain_apply(cp, i, 0, s2, n2, me, rod(s2), s2 > i ? rs.js[2 * tid] : rs.js[2 * (s2 - g0) + (1 - n2)],
-                            fd, td);
-            if (s1 >= 0)
-                chain_apply(cp, i, 1, s1, n1, me, rod(s1),
-                            s1 > i ? rs.js[2 * tid + 1] : rs.js[2 * (s1 - g0) + (1 - n1)], fd, td);
+            if (s2 >= 0) chain_apply(cp, i, 0, s2, n2, me, rod(s2), j2, fd, td);
+            if (s1 >= 0) chain_apply(cp, i, 1, s1, n1, me, rod(s1), j1, fd, td);
         } else {
             if (s2 >= 0) chain_side(cp, i, 0, s2, n2, me, rod(s2), fd, td);
             if (s1 >= 0) chain_side(cp, i, 1, s1, n1, me, rod(s1), fd, td);
@@ -798,10 +896,14 @@ __device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
                 gt[0] += p[3]; gt[1] += p[4]; gt[2] += p[5];
             }
         } else {
-            // a long row: take the list's members in ascending order by repeated minimum
+            // a long row: take its members in ascending order by repeated minimum
             int last = -1;
             for (int q = 0; q < nm; q++) {
                 int next = 0x7fffffff, it = 0;
+                for (int j = 0; j < FUSED_ROW_SLOTS; j++) {
+                    int m = a.slotM[(size_t)i * FUSED_ROW_SLOTS + j];
+                    if (m > last && m < next) next = m;
+                }
                 for (int m = a.headM[i]; m >= 0 && it <= a.nM; m = a.nextM[m], it++)
                     if (m > last && m < next) next = m;
                 if (next == 0x7fffffff) {
@@ -842,7 +944,7 @@ __device__ void motor_csr(const FusedArgs& a, int h, int nH, unsigned long long&
     for (int m = h * blockDim.x + threadIdx.x; m < a.nM; m += nH * blockDim.x) {
         int bs = sc.mot.boundSeg[m];
         if (bs < 0) continue;
-        int pos = sc.segMotorOffsets[bs] + list_rank(a, a.headM[bs], a.nextM, m, a.nM);
+        int pos = sc.segMotorOffsets[bs] + row_rank<FUSED_ROW_SLOTS>(a, a.cntM, a.slotM, a.headM, a.nextM, bs, m, a.nM);
         if (pos < a.nM) sc.segMotorMyo[pos] = m;
     }
 }
@@ -883,6 +985,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_dense_fused(FusedArgs a, i
     ScanArr first[4] = {{a.cntCell, a.C, 0}, {a.cntSeg, a.C, a.tilesC}, {a.cntA, a.nSeg, 2 * a.tilesC},
                         {a.cntB, a.nSeg, 2 * a.tilesC + a.tilesS}};
     int narr1 = a.xlOn ? 4 : 2;
+    const int nTiles1 = first[narr1 - 1].tile0 + (first[narr1 - 1].n + SCAN_CHUNK - 1) / SCAN_CHUNK;
     int* out1[4] = {sc.grid.gridCellOffsets, a.segCellOff, sc.xl.segOffsetsA, sc.xl.segOffsetsB};
     int* copy1[4] = {sc.grid.cellCount, nullptr, sc.xl.segCountA, sc.xl.segCountB};
     int clamp1[4] = {a.cap, a.nSeg, a.nL, a.nL};
@@ -906,15 +1009,17 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_dense_fused(FusedArgs a, i
             sc.fil.counts[1] = t;
             if (a.xlOn) { sc.xl.counts[1] = t; sc.xl.counts[2] = sc.seed; }
         }
-        // A: body view, bins, histograms and lists, crosslinker unbind, motor Brownian
+        // A: body view, bins, histograms and lists, crosslinker unbind
         phase_publish_bin(a, t);
         if (!counter_sync(a.bar, gTarget, nGrid, a.err)) return;
         stamp(s);
-        // B, C: scans of the cell, segment-per-cell and link-key histograms
+        // B, C: scans of the cell, segment-per-cell and link-key histograms (+ motor Brownian)
         tile_sums(first, narr1, a.tileSum, gw, nw);
+        if (a.xlOn) link_unbind(a, t, nTiles1);
         if (!counter_sync(a.bar, gTarget, nGrid, a.err)) return;
         stamp(s);
         tile_scan(first, narr1, a.tileSum, out1, copy1, clamp1, sc.grid.chunkSum, gw, nw);
+        motor_brownian(a, t, nTiles1);
         if (!counter_sync(a.bar, gTarget, nGrid, a.err)) return;
         stamp(s);
         // E: stable placement (grid contents, segment endpoints, link CSR lists)

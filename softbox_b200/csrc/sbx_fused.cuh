@@ -10,6 +10,9 @@ constexpr int FUSED_MAX_DPM = 16;     // dimers per minifilament (32 heads: one 
 constexpr int FUSED_ENT_CAP = 256;    // CSR payload entries a rod CTA stages in shared memory
 constexpr int FUSED_MCAP = 4;         // motor reactions per segment a rod CTA stages in shared memory
 constexpr int FUSED_MIDS = 16;        // motor slots per segment a rod CTA sorts (more: repeated-minimum walk)
+constexpr int FUSED_CELL_SLOTS = 4;   // fixed slots per grid cell
+constexpr int FUSED_JOINT_BYTES = 64; // one chain joint (ChainJoint, padded)
+constexpr int FUSED_ROW_SLOTS = 4;    // fixed slots per segment (link A ends, link B ends, motors)
 constexpr int FUSED_MIN_HELPERS = 16; // CTAs kept free of rod units in the rod phase
 
 struct FusedArgs {
@@ -25,10 +28,13 @@ struct FusedArgs {
     // private scratch (plan-owned)
     int *cntCell, *cntSeg, *cntAct, *cntA, *cntB, *cntM;   // cntSeg: segments per cell
     int* segCellOff;         // segment-only exclusive prefix over cells (C + 1)
+    void* joints;            // chain joints at (owner rod, owner side): 2 * nSeg slots of FUSED_JOINT_BYTES
     int* tileSum;            // tile sums of the step's scans (cells, segments, link A, link B)
     int* mTileSum;           // tile sums of the motor CSR scan
-    // singly linked lists (head per row, next per item; -1 ends): cells, link A/B keys,
-    // motors per bound segment
+    // rows of the step's inverse maps (cells -> bodies, segments -> link A/B ends,
+    // segments -> bound motors): the first arrivals of a row sit in its fixed slots, the
+    // rest in a singly linked overflow list (head per row, next per item; -1 ends)
+    int *cellSlot, *slotA, *slotB, *slotM;
     int *cellHead, *cellNext, *headA, *nextA, *headB, *nextB, *headM, *nextM;
     float4 *segE1, *segE2;   // segment endpoints in cell order: {end1, slot}, {end2, 0}
     unsigned long long* bar; // arrival counters (monotonic): [0] grid barrier, [1] rod-phase helpers

@@ -806,10 +806,13 @@ SBX_DEV bool unbind_one(int k, int nSeg, const float* fU, const float* fE1, int 
     double strain = stretch / restLength;
     int base = k * STRAIN_WIN;
     int p = place[k];
+    // the window with this step's entry replaced, summed in slot order
+    float w[STRAIN_WIN];
+    for (int j = 0; j < STRAIN_WIN; j++) w[j] = hist[base + j];
     hist[base + p] = (float)strain;
     place[k] = (p + 1) % STRAIN_WIN;
     double ave = 0.0;
-    for (int j = 0; j < STRAIN_WIN; j++) ave += hist[base + j];
+    for (int j = 0; j < STRAIN_WIN; j++) ave += (j == p) ? (float)strain : w[j];
     ave /= STRAIN_WIN;
     double kOff = offConst + offCoeff * sbxm::exp(ave * offExp);
     double pBreak = kOff * dt;
@@ -817,7 +820,6 @@ SBX_DEV bool unbind_one(int k, int nSeg, const float* fU, const float* fE1, int 
     return u < pBreak;
 }
 
-// MotorJointSystem.joints per sub-body (MotorJointSystem.java:88-190) -> f, t (double)
 // One motor joint (MotorJointSystem.java:86-197): which = 0 is joint 2 (rod-lever),
 // which = 1 is joint 1 (lever-head). The position-only part, shared by the joint's two
 // bodies; tm[0] / tm[1] are the torsion magnitudes for a nucleotide state other than /

@@ -16,8 +16,8 @@ from . import scenes
 from .engine import DenseNetwork
 from .runtime import LIB
 
-PHASES = ["A publish, bin, histograms + lists, crosslinker unbind, motor Brownian",   # K(prev) -> A
-          "B tile sums", "C scans", "E stable placement",
+PHASES = ["A publish, bin, histograms + lists, crosslinker unbind",   # K(prev) -> A
+          "B tile sums", "C scans + motor Brownian", "E stable placement",
           "F minifilaments + crosslinker forces + filament Brownian",
           "K rods (+ motor CSR helpers, resets)"]
 
