@@ -282,6 +282,67 @@ sbx_status sbx_xlink_unbind(sbx_ctx* ctx, int32_t nSeg, const float* filUVec, co
                             const float* loc1, const float* loc2, int32_t* linkState, float* strainHist,
                             int32_t* strainPlace, const float* offParams, const int32_t* counts);
 
+/* ---------------------------------------------------------------- crosslinker formation + allocator
+ * CrosslinkerSystem formation (CrosslinkerSystem.java:417-752) and the scan-rank free-list
+ * allocator (:297-345). formParams: [0] maxXLinkBondAngle (rad) [1] crossLinkGrabDist^2
+ * [2] minSepBetweenXLinks [3] maxXLinksOnSeg [4] P_form [5] loc jitter half-range
+ * [6] crossLinkGrabDist; formCounts: [0] nCand (written) [1] step [2] seed [3] xLinkMode
+ * (0 both, 1 parallel, -1 antiparallel) (CrosslinkerStore.java:108-112). The formation grid
+ * (FormationGrid.java) is built with sbx_filament_publish + sbx_grid_body_cell + sbx_grid_build. */
+/* filFilCandidates (:431-452): all cross-filament pairs i<j within the coarse capsule bound,
+ * lexicographic, capped at reqCap, unused tail keyed -1. Uses context scratch. */
+sbx_status sbx_xlink_fil_fil_candidates(sbx_ctx* ctx, int32_t nSeg, const float* coord, const float* segLength,
+                                        const int32_t* filID, int32_t reqCap, int32_t* reqFilA, int32_t* reqFilB,
+                                        const float* formParams, int32_t* formCounts);
+/* gridFormCount (:474-516): per segment, partners j>i in its 27 formation-grid cells (<= 256) */
+sbx_status sbx_xlink_grid_form_count(sbx_ctx* ctx, int32_t nSeg, const float* coord, const float* segLength,
+                                     const int32_t* filID, const float* gridParams, const int32_t* gridDims,
+                                     const int32_t* gridCellOffsets, const int32_t* gridCellContents,
+                                     int32_t* candCountSeg, const float* formParams);
+/* gridFormScan (:520-532): candBaseSeg = exclusive prefix (candBaseSeg[nSeg] = total),
+ * formCounts[0] = min(total, reqCap), unused tail keyed -1. Uses context scratch. */
+sbx_status sbx_xlink_grid_form_scan(sbx_ctx* ctx, int32_t nSeg, const int32_t* candCountSeg, int32_t* candBaseSeg,
+                                    int32_t reqCap, int32_t* reqFilA, int32_t* reqFilB, int32_t* formCounts);
+/* gridFormEmit (:538-595): partners ascending into each segment's region (== filFilCandidates) */
+sbx_status sbx_xlink_grid_form_emit(sbx_ctx* ctx, int32_t nSeg, const float* coord, const float* segLength,
+                                    const int32_t* filID, const float* gridParams, const int32_t* gridDims,
+                                    const int32_t* gridCellOffsets, const int32_t* gridCellContents,
+                                    const int32_t* candBaseSeg, const int32_t* candCountSeg, int32_t reqCap,
+                                    int32_t* reqFilA, int32_t* reqFilB, const float* formParams);
+/* formGates (:600-665): alignment, closest approach, loc + jitter, P_form -> gatePass, reqLoc1/2, reqOrient */
+sbx_status sbx_xlink_form_gates(sbx_ctx* ctx, int32_t nSeg, const float* filUVec, const float* filEnd1,
+                                const float* filEnd2, const float* filSegLength, int32_t reqCap,
+                                const int32_t* reqFilA, const int32_t* reqFilB, float* reqLoc1, float* reqLoc2,
+                                int32_t* reqOrient, int32_t* gatePass, const float* formParams,
+                                const int32_t* formCounts);
+/* formAdmitReduce (:670-682): per segment, the minimum gate-passing candidate index (sentinel reqCap) */
+sbx_status sbx_xlink_form_admit_reduce(sbx_ctx* ctx, int32_t reqCap, const int32_t* reqFilA, const int32_t* reqFilB,
+                                       const int32_t* gatePass, int32_t nSeg, int32_t* minCand);
+/* formAdmit (:713-735): one new link per segment, saturation and spacing vs start-of-step links */
+sbx_status sbx_xlink_form_admit(sbx_ctx* ctx, int32_t reqCap, const int32_t* reqFilA, const int32_t* reqFilB,
+                                const float* reqLoc1, const float* reqLoc2, const int32_t* gatePass,
+                                const int32_t* minCand, const int32_t* activeLinkCount, int32_t nLinks,
+                                const int32_t* linkState, const int32_t* linkFilA, const int32_t* linkFilB,
+                                const float* loc1, const float* loc2, int32_t* acceptFlag, const float* formParams);
+/* freeFlags (:297-302): freeCount[s] = linkState[s] < 0 */
+sbx_status sbx_xlink_free_flags(sbx_ctx* ctx, int32_t C, const int32_t* linkState, int32_t* freeCount);
+/* CrossBridgeSystem.csrScan (CrossBridgeSystem.java:198-205): offsets = exclusive prefix of
+ * counts, offsets[n] = total, counts reset to 0. Uses context scratch. */
+sbx_status sbx_csr_scan(sbx_ctx* ctx, int32_t n, int32_t* counts, int32_t* offsets);
+/* freeScatter (:306-314): freeList[freeOffsets[s]] = s for each FREE slot */
+sbx_status sbx_xlink_free_scatter(sbx_ctx* ctx, int32_t C, const int32_t* linkState, const int32_t* freeOffsets,
+                                  int32_t* freeList);
+/* allocate (:322-341): accepted request r claims freeList[rankOffsets[r]] (below nFree) */
+sbx_status sbx_xlink_allocate(sbx_ctx* ctx, int32_t K, const int32_t* reqFilA, const int32_t* reqFilB,
+                              const float* reqLoc1, const float* reqLoc2, const int32_t* rankOffsets,
+                              const int32_t* freeList, const int32_t* freeOffsets, int32_t C, int32_t* linkFilA,
+                              int32_t* linkFilB, float* loc1, float* loc2, int32_t* linkState, float* strainHist,
+                              int32_t* strainPlace);
+/* placeOrient (:740-752): orientSame and a fresh torsion ring in each claimed slot */
+sbx_status sbx_xlink_place_orient(sbx_ctx* ctx, int32_t K, const int32_t* reqOrient, const int32_t* rankOffsets,
+                                  const int32_t* freeList, const int32_t* freeOffsets, int32_t C,
+                                  int32_t* linkOrientSame, float* torqueMagHist, int32_t* torqueMagPlace);
+
 /* ---------------------------------------------------------------- myosin structure
  * MotorJointSystem.joints (MotorJointSystem.java:72-197) */
 sbx_status sbx_motor_joints(sbx_ctx* ctx, int32_t nB, const float* coord, const float* uVec,

@@ -45,6 +45,11 @@ _SIGS = {
     "orc_mini_brute_gather": "iipppp", "orc_torsional_restore": "ipppdd", "orc_dense_step": "si",
     "orc_dense_run": "sii", "orc_fdt_run": "sii", "orc_chain_run": "sii",
     "orc_m_log": "d", "orc_m_exp": "d", "orc_m_sin": "d", "orc_m_cos": "d", "orc_m_eval": "iipp",
+    "orc_xl_fil_fil_candidates": "ipppipppp", "orc_xl_grid_form_count": "ippppppppp",
+    "orc_xl_grid_form_scan": "ippippp", "orc_xl_grid_form_emit": "ipppppppppippp",
+    "orc_xl_form_gates": "ippppipppppppp", "orc_xl_form_admit_reduce": "ipppip",
+    "orc_xl_form_admit": "ipppppppippppppp", "orc_xl_free_flags": "ipp", "orc_xl_free_scatter": "ippp",
+    "orc_xl_allocate": "ipppppppippppppp", "orc_xl_place_orient": "ippppippp",
 }
 _CT = {"i": C.c_int32, "I": C.c_uint64, "d": C.c_double, "f": C.c_float, "p": C.c_void_p, "s": C.c_void_p}
 _RET = {"orc_max_threads": C.c_int, "orc_accurate_acos": C.c_double, "orc_angle_from_sin_cos": C.c_double,

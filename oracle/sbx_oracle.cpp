@@ -70,7 +70,7 @@ const int XB_STRIDE = 13;          // CrossBridgeSystem.java:36
 const int XL_STRIDE = 12;          // CrosslinkerStore.java:33
 const int STRAIN_WIN = 10, TORQUE_WIN = 5;   // CrosslinkerStore.java:64,118
 const int MINI_STRIDE = 6;         // MiniFilamentStore.java:224
-const int LINK_FREE = -1;
+const int LINK_FREE = -1, LINK_ACTIVE = 0;   // CrosslinkerStore.java:58-59
 
 // Java (int) cast of a float / double
 inline i32 jf2i(float f) {
@@ -1979,5 +1979,289 @@ EXPORT void orc_m_eval(int which, int n, const double* x, double* y) {
     PAR for (int i = 0; i < n; i++) {
         double v = x[i];
         y[i] = which == 0 ? sbxm::log(v) : which == 1 ? sbxm::exp(v) : which == 2 ? sbxm::sin(v) : sbxm::cos(v);
+    }
+}
+
+// ============================================================================
+// Crosslinker formation (CrosslinkerSystem.java:417-752) and the scan-rank free-list
+// allocator (CrosslinkerSystem.java:297-345); FormationGrid.java:28-109 builds its grid
+// with the SpatialGrid functions above.
+// formParams: [0] maxXLinkBondAngle (rad) [1] crossLinkGrabDist^2 [2] minSepBetweenXLinks
+//             [3] maxXLinksOnSeg [4] P_form [5] loc jitter half-range [6] crossLinkGrabDist
+// formCounts: [0] nCand [1] step [2] seed [3] xLinkMode (0 both, 1 parallel, -1 antiparallel)
+// ============================================================================
+namespace {
+const int FORM_MAXC = 256;   // CrosslinkerSystem.java:472
+
+// the coarse capsule bound of filFilCandidates / gridFormCount (CrosslinkerSystem.java:444-448)
+inline bool form_pair_ok(i32 nSeg, const float* coord, const float* segLength, const i32* filID, int i, int j,
+                         double cix, double ciy, double ciz, double hi, double grab) {
+    if (filID[j] == filID[i]) return false;
+    double dx = cix - coord[j], dy = ciy - coord[nSeg + j], dz = ciz - coord[2 * nSeg + j];
+    double cd = std::sqrt(dx * dx + dy * dy + dz * dz);
+    double bound = hi + 0.5 * segLength[j] + grab;
+    return !(cd > bound);
+}
+
+inline void form_cell_range(double cix, double ciy, double ciz, const float* gp, const i32* gd, int* lo, int* hi) {
+    float xMin = gp[0], yMin = gp[1], zMin = gp[2], invCell = gp[4];
+    int n[3] = {gd[0], gd[1], gd[2]};
+    int c[3] = {jf2i(((float)cix - xMin) * invCell), jf2i(((float)ciy - yMin) * invCell),
+                jf2i(((float)ciz - zMin) * invCell)};
+    for (int k = 0; k < 3; k++) {
+        if (c[k] < 0) c[k] = 0;
+        if (c[k] >= n[k]) c[k] = n[k] - 1;
+        lo[k] = c[k] - 1; if (lo[k] < 0) lo[k] = 0;
+        hi[k] = c[k] + 1; if (hi[k] >= n[k]) hi[k] = n[k] - 1;
+    }
+}
+}  // namespace
+
+// CrosslinkerSystem.filFilCandidates (CrosslinkerSystem.java:431-452): all distinct
+// cross-filament pairs i<j within the coarse bound, lexicographic, capped at reqCap
+EXPORT void orc_xl_fil_fil_candidates(i32 nSeg, const float* coord, const float* segLength, const i32* filID,
+                                      i32 reqCap, i32* reqFilA, i32* reqFilB, const float* formParams,
+                                      i32* formCounts) {
+    double grab = formParams[6];
+    int c = 0;
+    for (int i = 0; i < nSeg; i++) {
+        double cix = coord[i], ciy = coord[nSeg + i], ciz = coord[2 * nSeg + i];
+        double hi = 0.5 * segLength[i];
+        for (int j = i + 1; j < nSeg; j++) {
+            if (!form_pair_ok(nSeg, coord, segLength, filID, i, j, cix, ciy, ciz, hi, grab)) continue;
+            if (c < reqCap) { reqFilA[c] = i; reqFilB[c] = j; c++; }
+        }
+    }
+    formCounts[0] = c;
+    for (int k = c; k < reqCap; k++) { reqFilA[k] = -1; reqFilB[k] = -1; }
+}
+
+// CrosslinkerSystem.gridFormCount (CrosslinkerSystem.java:474-516)
+EXPORT void orc_xl_grid_form_count(i32 nSeg, const float* coord, const float* segLength, const i32* filID,
+                                   const float* gridParams, const i32* gridDims, const i32* offsets,
+                                   const i32* contents, i32* candCountSeg, const float* formParams) {
+    double grab = formParams[6];
+    int nX = gridDims[0], nY = gridDims[1], nXY = nX * nY;
+    (void)nY;
+    PAR for (int i = 0; i < nSeg; i++) {
+        double cix = coord[i], ciy = coord[nSeg + i], ciz = coord[2 * nSeg + i];
+        double hi = 0.5 * segLength[i];
+        int lo[3], up[3];
+        form_cell_range(cix, ciy, ciz, gridParams, gridDims, lo, up);
+        int cnt = 0;
+        for (int zz = lo[2]; zz <= up[2]; zz++)
+            for (int yy = lo[1]; yy <= up[1]; yy++)
+                for (int xx = lo[0]; xx <= up[0]; xx++) {
+                    int cc = xx + yy * nX + zz * nXY;
+                    for (int idx = offsets[cc]; idx < offsets[cc + 1]; idx++) {
+                        int j = contents[idx];
+                        if (j <= i) continue;
+                        if (!form_pair_ok(nSeg, coord, segLength, filID, i, j, cix, ciy, ciz, hi, grab)) continue;
+                        cnt++;
+                    }
+                }
+        candCountSeg[i] = cnt < FORM_MAXC ? cnt : FORM_MAXC;
+    }
+}
+
+// CrosslinkerSystem.gridFormScan (CrosslinkerSystem.java:520-532)
+EXPORT void orc_xl_grid_form_scan(i32 nSeg, const i32* candCountSeg, i32* candBaseSeg, i32 reqCap, i32* reqFilA,
+                                  i32* reqFilB, i32* formCounts) {
+    int acc = 0;
+    for (int s = 0; s < nSeg; s++) { candBaseSeg[s] = acc; acc += candCountSeg[s]; }
+    candBaseSeg[nSeg] = acc;
+    int total = acc < reqCap ? acc : reqCap;
+    formCounts[0] = total;
+    for (int k = total; k < reqCap; k++) { reqFilA[k] = -1; reqFilB[k] = -1; }
+}
+
+// CrosslinkerSystem.gridFormEmit (CrosslinkerSystem.java:538-595): partners ascending in
+// each segment's owned region; a full region keeps the smallest FORM_MAXC
+EXPORT void orc_xl_grid_form_emit(i32 nSeg, const float* coord, const float* segLength, const i32* filID,
+                                  const float* gridParams, const i32* gridDims, const i32* offsets,
+                                  const i32* contents, const i32* candBaseSeg, const i32* candCountSeg, i32 reqCap,
+                                  i32* reqFilA, i32* reqFilB, const float* formParams) {
+    double grab = formParams[6];
+    int nX = gridDims[0], nXY = nX * gridDims[1];
+    PAR for (int i = 0; i < nSeg; i++) {
+        int base = candBaseSeg[i];
+        int cap = candCountSeg[i];
+        if (base >= reqCap) cap = 0;
+        else if (base + cap > reqCap) cap = reqCap - base;
+        if (cap <= 0) continue;
+        double cix = coord[i], ciy = coord[nSeg + i], ciz = coord[2 * nSeg + i];
+        double hi = 0.5 * segLength[i];
+        int lo[3], up[3];
+        form_cell_range(cix, ciy, ciz, gridParams, gridDims, lo, up);
+        int cnt = 0;
+        for (int zz = lo[2]; zz <= up[2]; zz++)
+            for (int yy = lo[1]; yy <= up[1]; yy++)
+                for (int xx = lo[0]; xx <= up[0]; xx++) {
+                    int cc = xx + yy * nX + zz * nXY;
+                    for (int idx = offsets[cc]; idx < offsets[cc + 1]; idx++) {
+                        int j = contents[idx];
+                        if (j <= i) continue;
+                        if (!form_pair_ok(nSeg, coord, segLength, filID, i, j, cix, ciy, ciz, hi, grab)) continue;
+                        if (cnt < cap) {
+                            int p = base + cnt;
+                            while (p > base && reqFilB[p - 1] > j) { reqFilB[p] = reqFilB[p - 1]; p--; }
+                            reqFilB[p] = j;
+                            cnt++;
+                        } else if (j < reqFilB[base + cap - 1]) {
+                            int p = base + cap - 1;
+                            while (p > base && reqFilB[p - 1] > j) { reqFilB[p] = reqFilB[p - 1]; p--; }
+                            reqFilB[p] = j;
+                        }
+                    }
+                }
+        for (int k = 0; k < cap; k++) reqFilA[base + k] = i;
+    }
+}
+
+// CrosslinkerSystem.formGates (CrosslinkerSystem.java:600-665)
+EXPORT void orc_xl_form_gates(i32 nSeg, const float* fU, const float* fE1, const float* fE2, const float* segLength,
+                              i32 reqCap, const i32* reqFilA, const i32* reqFilB, float* reqLoc1, float* reqLoc2,
+                              i32* reqOrient, i32* gatePass, const float* formParams, const i32* formCounts) {
+    i32 step = formCounts[1], seed = formCounts[2], mode = formCounts[3];
+    double maxAngle = formParams[0], grabSq = formParams[1];
+    double pForm = formParams[4], jit = formParams[5];
+    PAR for (int c = 0; c < reqCap; c++) {
+        gatePass[c] = 0; reqOrient[c] = 0;
+        int a = reqFilA[c], b = reqFilB[c];
+        if (a < 0 || b < 0) continue;
+        double uax = fU[a], uay = fU[nSeg + a], uaz = fU[2 * nSeg + a];
+        double ubx = fU[b], uby = fU[nSeg + b], ubz = fU[2 * nSeg + b];
+        double dot = uax * ubx + uay * uby + uaz * ubz;
+        double angT = fast_acos(dot), angTR = fast_acos(-dot);
+        bool alignOk;
+        if (mode == 1) alignOk = angT <= maxAngle;
+        else if (mode == -1) alignOk = angTR <= maxAngle;
+        else alignOk = (angT <= maxAngle) || (angTR <= maxAngle);
+        if (!alignOk) continue;
+        reqOrient[c] = dot >= 0.0 ? 1 : 0;
+        double e1ax = fE1[a], e1ay = fE1[nSeg + a], e1az = fE1[2 * nSeg + a];
+        double e2ax = fE2[a], e2ay = fE2[nSeg + a], e2az = fE2[2 * nSeg + a];
+        double e1bx = fE1[b], e1by = fE1[nSeg + b], e1bz = fE1[2 * nSeg + b];
+        double e2bx = fE2[b], e2by = fE2[nSeg + b], e2bz = fE2[2 * nSeg + b];
+        double r1x = e2ax - e1ax, r1y = e2ay - e1ay, r1z = e2az - e1az;
+        double r2x = e2bx - e1bx, r2y = e2by - e1by, r2z = e2bz - e1bz;
+        double r3x = e1bx - e1ax, r3y = e1by - e1ay, r3z = e1bz - e1az;
+        double r4x = r1y * r2z - r1z * r2y, r4y = r1z * r2x - r1x * r2z, r4z = r1x * r2y - r1y * r2x;
+        double smallNum = 1e-20;
+        if (r4x < smallNum && r4y < smallNum && r4z < smallNum) continue;
+        double denom = r4x * r4x + r4y * r4y + r4z * r4z;
+        double c32x = r3y * r2z - r3z * r2y, c32y = r3z * r2x - r3x * r2z, c32z = r3x * r2y - r3y * r2x;
+        double alpha = (r4x * c32x + r4y * c32y + r4z * c32z) / denom;
+        if (alpha < 0.0 || alpha > 1.0) continue;
+        double c31x = r3y * r1z - r3z * r1y, c31y = r3z * r1x - r3x * r1z, c31z = r3x * r1y - r3y * r1x;
+        double beta = (r4x * c31x + r4y * c31y + r4z * c31z) / denom;
+        if (beta < 0.0 || beta > 1.0) continue;
+        double p1x = e1ax + alpha * r1x, p1y = e1ay + alpha * r1y, p1z = e1az + alpha * r1z;
+        double p2x = e1bx + beta * r2x, p2y = e1by + beta * r2y, p2z = e1bz + beta * r2z;
+        double ddx = p1x - p2x, ddy = p1y - p2y, ddz = p1z - p2z;
+        double conDistSq = ddx * ddx + ddy * ddy + ddz * ddz;
+        if (conDistSq >= grabSq) continue;
+        uint32_t base = sbxm::rng_base(c, step, seed);
+        double da = std::sqrt((p1x - e1ax) * (p1x - e1ax) + (p1y - e1ay) * (p1y - e1ay) + (p1z - e1az) * (p1z - e1az));
+        double db = std::sqrt((p2x - e1bx) * (p2x - e1bx) + (p2y - e1by) * (p2y - e1by) + (p2z - e1bz) * (p2z - e1bz));
+        float uj1 = sbxm::unit_from_hash(sbxm::wang_hash(base ^ 0x584C4A31u));
+        float uj2 = sbxm::unit_from_hash(sbxm::wang_hash(base ^ 0x584C4A32u));
+        double loc1 = da + (2.0 * uj1 - 1.0) * jit;
+        double loc2 = db + (2.0 * uj2 - 1.0) * jit;
+        double lenA = segLength[a], lenB = segLength[b];
+        if (loc1 > lenA) loc1 = lenA;
+        if (loc1 < 0.0) loc1 = 0.0;
+        if (loc2 > lenB) loc2 = lenB;
+        if (loc2 < 0.0) loc2 = 0.0;
+        reqLoc1[c] = (float)loc1; reqLoc2[c] = (float)loc2;
+        float up = sbxm::unit_from_hash(sbxm::wang_hash(base ^ 0x584C4650u));
+        if (up < pForm) gatePass[c] = 1;
+    }
+}
+
+// CrosslinkerSystem.formAdmitReduce (CrosslinkerSystem.java:670-682)
+EXPORT void orc_xl_form_admit_reduce(i32 reqCap, const i32* reqFilA, const i32* reqFilB, const i32* gatePass,
+                                     i32 nSeg, i32* minCand) {
+    for (int s = 0; s < nSeg; s++) minCand[s] = reqCap;
+    for (int c = 0; c < reqCap; c++) {
+        if (gatePass[c] == 0) continue;
+        int a = reqFilA[c], b = reqFilB[c];
+        if (c < minCand[a]) minCand[a] = c;
+        if (c < minCand[b]) minCand[b] = c;
+    }
+}
+
+// CrosslinkerSystem.formAdmit (CrosslinkerSystem.java:713-735)
+EXPORT void orc_xl_form_admit(i32 reqCap, const i32* reqFilA, const i32* reqFilB, const float* reqLoc1,
+                              const float* reqLoc2, const i32* gatePass, const i32* minCand,
+                              const i32* activeLinkCount, i32 nLinks, const i32* linkState, const i32* linkFilA,
+                              const i32* linkFilB, const float* loc1, const float* loc2, i32* acceptFlag,
+                              const float* formParams) {
+    double minSep = formParams[2];
+    int maxLinks = jf2i(formParams[3]);
+    PAR for (int c = 0; c < reqCap; c++) {
+        acceptFlag[c] = 0;
+        if (gatePass[c] == 0) continue;
+        int segA = reqFilA[c], segB = reqFilB[c];
+        if (minCand[segA] != c || minCand[segB] != c) continue;
+        if (activeLinkCount[segA] >= maxLinks || activeLinkCount[segB] >= maxLinks) continue;
+        double la = reqLoc1[c], lb = reqLoc2[c];
+        bool ok = true;
+        for (int L = 0; L < nLinks; L++) {
+            if (linkState[L] < 0) continue;
+            int fa = linkFilA[L], fb = linkFilB[L];
+            if (fa == segA && std::fabs(la - loc1[L]) < minSep) ok = false;
+            if (fb == segA && std::fabs(la - loc2[L]) < minSep) ok = false;
+            if (fa == segB && std::fabs(lb - loc1[L]) < minSep) ok = false;
+            if (fb == segB && std::fabs(lb - loc2[L]) < minSep) ok = false;
+        }
+        if (ok) acceptFlag[c] = 1;
+    }
+}
+
+// CrosslinkerSystem.freeFlags (:297-302), CrossBridgeSystem.csrScan, freeScatter (:306-314)
+EXPORT void orc_xl_free_flags(i32 C, const i32* linkState, i32* freeCount) {
+    for (int s = 0; s < C; s++) freeCount[s] = linkState[s] < 0 ? 1 : 0;
+}
+EXPORT void orc_xl_free_scatter(i32 C, const i32* linkState, const i32* freeOffsets, i32* freeList) {
+    for (int s = 0; s < C; s++)
+        if (linkState[s] < 0) freeList[freeOffsets[s]] = s;
+}
+
+// CrosslinkerSystem.allocate (:322-341) then placeOrient (:740-752)
+EXPORT void orc_xl_allocate(i32 K, const i32* reqFilA, const i32* reqFilB, const float* reqLoc1,
+                            const float* reqLoc2, const i32* rankOffsets, const i32* freeList,
+                            const i32* freeOffsets, i32 C, i32* linkFilA, i32* linkFilB, float* loc1, float* loc2,
+                            i32* linkState, float* strainHist, i32* strainPlace) {
+    int nFree = freeOffsets[C];
+    for (int r = 0; r < K; r++) {
+        int rank = rankOffsets[r];
+        bool accepted = rankOffsets[r + 1] > rank;
+        if (!accepted) continue;
+        if (rank >= nFree) continue;
+        int slot = freeList[rank];
+        linkFilA[slot] = reqFilA[r];
+        linkFilB[slot] = reqFilB[r];
+        loc1[slot] = reqLoc1[r];
+        loc2[slot] = reqLoc2[r];
+        int base = slot * STRAIN_WIN;
+        for (int j = 0; j < STRAIN_WIN; j++) strainHist[base + j] = 0.f;
+        strainPlace[slot] = 0;
+        linkState[slot] = LINK_ACTIVE;
+    }
+}
+EXPORT void orc_xl_place_orient(i32 K, const i32* reqOrient, const i32* rankOffsets, const i32* freeList,
+                                const i32* freeOffsets, i32 C, i32* linkOrientSame, float* torqueMagHist,
+                                i32* torqueMagPlace) {
+    int nFree = freeOffsets[C];
+    for (int r = 0; r < K; r++) {
+        int rank = rankOffsets[r];
+        if (rankOffsets[r + 1] <= rank) continue;
+        if (rank >= nFree) continue;
+        int slot = freeList[rank];
+        linkOrientSame[slot] = reqOrient[r];
+        torqueMagPlace[slot] = 0;
+        int b = slot * TORQUE_WIN;
+        for (int j = 0; j < TORQUE_WIN; j++) torqueMagHist[b + j] = 0.f;
     }
 }

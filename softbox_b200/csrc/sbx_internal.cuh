@@ -61,3 +61,7 @@ struct CountingSort {
 };
 
 sbx_status counting_sort(sbx_ctx* ctx, const CountingSort& cs, const char* what);
+
+// Exclusive prefix sum of in[0..n) into out[0..n), total into out[n]; zeroIn resets in[]
+// (CrossBridgeSystem.csrScan's cursor side effect). chunkSum: ceil(n/SCAN_CHUNK)+1 ints.
+sbx_status exclusive_scan(sbx_ctx* ctx, int* in, int n, int* out, bool zeroIn, int* chunkSum, const char* what);

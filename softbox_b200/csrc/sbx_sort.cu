@@ -129,7 +129,36 @@ __global__ void k_cs_rank(const int* keys, const int* nDev, int useDevN, int nBo
     }
 }
 
+// exclusive_scan's tile add: out += tile prefix; the input optionally reset (csrScan's
+// cursor side effect); out[n] = total
+__global__ void __launch_bounds__(256) k_scan_add_plain(int* out, int n, const int* chunkSum, int numChunks, int* in,
+                                                        int zeroIn) {
+    int b = chunkSum[blockIdx.x];
+    int base = blockIdx.x * SCAN_CHUNK;
+    for (int k = threadIdx.x; k < SCAN_CHUNK; k += blockDim.x) {
+        int c = base + k;
+        if (c < n) {
+            out[c] += b;
+            if (zeroIn) in[c] = 0;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = chunkSum[numChunks];
+}
+
 }  // namespace
+
+sbx_status exclusive_scan(sbx_ctx* ctx, int* in, int n, int* out, bool zeroIn, int* chunkSum, const char* what) {
+    int numChunks = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    if (numChunks == 0) {
+        if (cudaMemsetAsync(out, 0, sizeof(int), ctx->stream) != cudaSuccess)
+            return fail(ctx, SBX_ECUDA, std::string(what) + ": memset");
+        return SBX_OK;
+    }
+    SBX_LAUNCH(ctx, k_scan_local, numChunks, 256, in, n, out, chunkSum);
+    SBX_LAUNCH(ctx, k_scan_chunks, 1, 1024, chunkSum, numChunks);
+    SBX_LAUNCH(ctx, k_scan_add_plain, numChunks, 256, out, n, chunkSum, numChunks, in, zeroIn ? 1 : 0);
+    return check_launch(ctx, what);
+}
 
 sbx_status counting_sort(sbx_ctx* ctx, const CountingSort& cs, const char* what) {
     int numChunks = (cs.nRows + SCAN_CHUNK - 1) / SCAN_CHUNK;

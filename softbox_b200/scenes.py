@@ -606,3 +606,77 @@ def _build_crosslinkers(f, n_seg, segs_per_fil, cfg, rng):
     xl["torsionParams"] = np.array([cfg.xl_torsion_spring, 1.0], F32)
     xl["counts"][2] = cfg.seed
     return xl
+
+
+# ---------------------------------------------------------------- crosslinker formation scene
+XL_BUNDLE_REST_LEN = 0.0125                  # CrosslinkerBundleHarness.java:46 (FilLink.restLength)
+XL_GRAB_DIST = 2.0 * 0.0054                  # crossLinkGrabDist = 2 actinMonoDiam (:51)
+XL_MIN_SEP = 5.0 * 0.0054                    # minSepBetweenXLinks (:52)
+XL_MIN_FILLINK_SEP = 2.0 * 0.0054            # loc jitter half-range (:53)
+XL_MAX_LINKS_ON_SEG = 10                     # (:54)
+
+
+def xlink_form_params(max_angle, p_form, grab=XL_GRAB_DIST, min_sep=XL_MIN_SEP, max_links=XL_MAX_LINKS_ON_SEG,
+                      jitter=XL_MIN_FILLINK_SEP):
+    """CrosslinkerStore.setFormParams (CrosslinkerStore.java:190-199)."""
+    return np.array([max_angle, grab * grab, min_sep, max_links, p_form, jitter, grab, 0.0], F32)
+
+
+def xlink_bundle(n_fil=200, box=(0.7, 0.7, 0.3), dt=1.0e-4, seed=7, pos_sigma=0.2, max_angle=0.6, p_form=0.5,
+                 aeta=1.0, mode=0):
+    """A dense bundle of single-segment filaments for crosslinker formation, composed like
+    CrosslinkerBundleHarness.buildBundle (CrosslinkerBundleHarness.java:260-311): lengths
+    uniform in [0.1, 0.3] um, directions uniform on the sphere, centres Gaussian (sigma
+    0.2 um) clamped to the box, filID = index, an empty link pool of max(64, 4 n) slots and
+    all-pairs request capacity. Seeded numpy draws stand in for java.util.Random."""
+    rng = np.random.default_rng(seed)
+    n = n_fil
+    f = filament_store(n)
+    b = f["body"]
+    lens = 0.1 + rng.random(n) * 0.2
+    f["monomerCount"][:] = np.maximum(1, np.rint(lens / ACTIN_MONO_RADIUS).astype(np.int64) - 1).astype(I32)
+    z = 2.0 * rng.random(n) - 1.0
+    phi = 2.0 * math.pi * rng.random(n)
+    r = np.sqrt(np.maximum(0.0, 1.0 - z * z))
+    u = np.stack([r * np.cos(phi), r * np.sin(phi), z])
+    y = np.stack([-u[1], u[0], np.zeros(n)])
+    yn = np.linalg.norm(y, axis=0)
+    small = yn < 1e-9
+    y[:, small] = np.stack([np.zeros(small.sum()), -u[2, small], u[1, small]])
+    y /= np.linalg.norm(y, axis=0)
+    c = np.stack([np.clip(rng.normal(size=n) * pos_sigma, -0.5 * bx, 0.5 * bx) for bx in box])
+    b["coord"][:] = c.reshape(-1).astype(F32)
+    b["uVec"][:] = u.reshape(-1).astype(F32)
+    b["yVec"][:] = y.reshape(-1).astype(F32)
+    b["brownTransScale"][:] = F32(1.0)
+    b["brownRotScale"][:] = F32(0.5)
+    drag_run_filament(f, 0.1)
+    rescale_viscosity(b, aeta / 0.1)
+    f["params"][:] = np.array([dt, math.sqrt(2.0 * KT / dt)], F32)
+    f["counts"][:] = np.array([n, 0, seed, 1], I32)
+    derive_host(b)
+    C = max(64, 4 * n)
+    req_cap = max(1, n * (n - 1) // 2)
+    xl = {"nLinks": C,
+          "linkFilA": np.full(C, -1, I32), "linkFilB": np.full(C, -1, I32),
+          "linkState": np.full(C, -1, I32), "linkOrientSame": np.zeros(C, I32),
+          "activeLinkCount": np.zeros(n, I32),
+          "loc1": np.zeros(C, F32), "loc2": np.zeros(C, F32),
+          "xlinkData": np.zeros(C * XL_STRIDE, F32),
+          "strainHist": np.zeros(C * STRAIN_WIN, F32), "torqueMagHist": np.zeros(C * TORQUE_WIN, F32),
+          "strainPlace": np.zeros(C, I32), "torqueMagPlace": np.zeros(C, I32),
+          "counts": np.array([C, 0, seed, n], I32),
+          "reqFilA": np.full(req_cap, -1, I32), "reqFilB": np.full(req_cap, -1, I32),
+          "reqLoc1": np.zeros(req_cap, F32), "reqLoc2": np.zeros(req_cap, F32),
+          "reqOrient": np.zeros(req_cap, I32), "gatePass": np.zeros(req_cap, I32),
+          "acceptFlag": np.zeros(req_cap, I32), "rankOffsets": np.zeros(req_cap + 1, I32),
+          "minCand": np.zeros(n, I32),
+          "freeCount": np.zeros(C, I32), "freeOffsets": np.zeros(C + 1, I32), "freeList": np.zeros(C, I32),
+          "formParams": xlink_form_params(max_angle, p_form),
+          "formCounts": np.array([0, 0, seed, mode], I32)}
+    seg_len = b["segLength"].astype(np.float64)
+    max_c = float(np.abs(b["coord"]).max())
+    cell = 2.0 * (0.5 * float(seg_len.max()) + ACTIN_RADIUS) + XL_GRAB_DIST
+    g = max(2.0, max_c * 4.0 + cell + 0.5)
+    grid = {"half": g, "cell": cell, "grab": XL_GRAB_DIST, "radius": ACTIN_RADIUS}
+    return {"fil": f, "xl": xl, "filID": np.arange(n, dtype=I32), "grid": grid, "reqCap": req_cap, "C": C}

@@ -204,6 +204,12 @@ class CrossBridgeSystem:                     # CrossBridgeSystem.java
                forceDotHist, forceDotPlace)
 
     @staticmethod
+    def csrScan(counts, segMotorCount, segMotorOffsets):
+        """CrossBridgeSystem.csrScan (CrossBridgeSystem.java:198-205): n = counts[3] rows (host value)."""
+        n = int(counts[3]) if not hasattr(counts, "device") or counts.device.type == "cpu" else int(counts[3].item())
+        _ctx()("sbx_csr_scan", n, segMotorCount, segMotorOffsets)
+
+    @staticmethod
     def csrBuild(keys, nRows, rowCount, rowOffsets, rowList):
         """csrHistogram + csrScan + csrScatter (and the csrChunk* variant) in one call."""
         _ctx()("sbx_csr_build", keys, keys.numel(), int(nRows), rowCount, rowOffsets, rowList)
@@ -257,6 +263,119 @@ class CrosslinkerSystem:                     # CrosslinkerSystem.java
                offParams, counts):
         _ctx()("sbx_xlink_unbind", _n3(filCoord), filUVec, filEnd1, linkFilA.numel(), linkFilA, linkFilB, loc1, loc2,
                linkState, strainHist, strainPlace, offParams, counts)
+
+    # ---- formation (CrosslinkerSystem.java:417-752) and the free-list allocator (:297-345)
+    FORM_MAXC = 256
+
+    @staticmethod
+    def filFilCandidates(filCoord, filSegLength, filID, reqFilA, reqFilB, formParams, formCounts):
+        _ctx()("sbx_xlink_fil_fil_candidates", _n3(filCoord), filCoord, filSegLength, filID, reqFilA.numel(),
+               reqFilA, reqFilB, formParams, formCounts)
+
+    @staticmethod
+    def gridFormCount(filCoord, filSegLength, filID, gridParams, gridDims, gridCellOffsets, gridCellContents,
+                      candCountSeg, formParams, formCounts=None):
+        _ctx()("sbx_xlink_grid_form_count", _n3(filCoord), filCoord, filSegLength, filID, gridParams, gridDims,
+               gridCellOffsets, gridCellContents, candCountSeg, formParams)
+
+    @staticmethod
+    def gridFormScan(candCountSeg, candBaseSeg, reqFilA, reqFilB, formCounts):
+        _ctx()("sbx_xlink_grid_form_scan", candCountSeg.numel(), candCountSeg, candBaseSeg, reqFilA.numel(), reqFilA,
+               reqFilB, formCounts)
+
+    @staticmethod
+    def gridFormEmit(filCoord, filSegLength, filID, gridParams, gridDims, gridCellOffsets, gridCellContents,
+                     candBaseSeg, candCountSeg, reqFilA, reqFilB, formParams, formCounts=None):
+        _ctx()("sbx_xlink_grid_form_emit", _n3(filCoord), filCoord, filSegLength, filID, gridParams, gridDims,
+               gridCellOffsets, gridCellContents, candBaseSeg, candCountSeg, reqFilA.numel(), reqFilA, reqFilB,
+               formParams)
+
+    @staticmethod
+    def formGates(filUVec, filEnd1, filEnd2, filSegLength, reqFilA, reqFilB, reqLoc1, reqLoc2, reqOrient, gatePass,
+                  formParams, formCounts):
+        _ctx()("sbx_xlink_form_gates", _n3(filUVec), filUVec, filEnd1, filEnd2, filSegLength, reqFilA.numel(),
+               reqFilA, reqFilB, reqLoc1, reqLoc2, reqOrient, gatePass, formParams, formCounts)
+
+    @staticmethod
+    def formAdmitReduce(reqFilA, reqFilB, gatePass, minCand, formCounts=None):
+        _ctx()("sbx_xlink_form_admit_reduce", reqFilA.numel(), reqFilA, reqFilB, gatePass, minCand.numel(), minCand)
+
+    @staticmethod
+    def formAdmit(reqFilA, reqFilB, reqLoc1, reqLoc2, gatePass, minCand, activeLinkCount, linkState, linkFilA,
+                  linkFilB, loc1, loc2, acceptFlag, formParams, formCounts=None):
+        _ctx()("sbx_xlink_form_admit", reqFilA.numel(), reqFilA, reqFilB, reqLoc1, reqLoc2, gatePass, minCand,
+               activeLinkCount, linkState.numel(), linkState, linkFilA, linkFilB, loc1, loc2, acceptFlag, formParams)
+
+    @staticmethod
+    def freeFlags(linkState, freeCount, allocCounts=None):
+        _ctx()("sbx_xlink_free_flags", freeCount.numel(), linkState, freeCount)
+
+    @staticmethod
+    def freeScatter(linkState, freeOffsets, freeList, allocCounts=None):
+        _ctx()("sbx_xlink_free_scatter", freeList.numel(), linkState, freeOffsets, freeList)
+
+    @staticmethod
+    def allocate(reqFilA, reqFilB, reqLoc1, reqLoc2, rankOffsets, freeList, freeOffsets, linkFilA, linkFilB, loc1,
+                 loc2, linkState, strainHist, strainPlace, allocCounts=None, K=None):
+        K = reqFilA.numel() if K is None else K
+        _ctx()("sbx_xlink_allocate", K, reqFilA, reqFilB, reqLoc1, reqLoc2, rankOffsets, freeList, freeOffsets,
+               freeList.numel(), linkFilA, linkFilB, loc1, loc2, linkState, strainHist, strainPlace)
+
+    @staticmethod
+    def placeOrient(reqOrient, rankOffsets, freeList, freeOffsets, linkOrientSame, torqueMagHist, torqueMagPlace,
+                    allocCounts=None, K=None):
+        K = reqOrient.numel() if K is None else K
+        _ctx()("sbx_xlink_place_orient", K, reqOrient, rankOffsets, freeList, freeOffsets, freeList.numel(),
+               linkOrientSame, torqueMagHist, torqueMagPlace)
+
+
+class FormationGrid:                         # FormationGrid.java:28-109
+    """The dedicated crosslinker-formation grid: one body per segment, cell size
+    >= max segment length + grab so the 27-cell stencil is complete."""
+
+    def __init__(self, n_seg, gx, gy, gz, cell_size, grab, actin_radius, device="cuda"):
+        import math
+        import torch
+        i32 = dict(dtype=torch.int32, device=device)
+        f32 = dict(dtype=torch.float32, device=device)
+        self.nSeg = n_seg
+        nX = 1 + int(math.ceil(2 * gx / cell_size))
+        nY = 1 + int(math.ceil(2 * gy / cell_size))
+        nZ = 1 + int(math.ceil(2 * gz / cell_size))
+        self.totalCells = nX * nY * nZ
+        self.viewParams = torch.tensor([actin_radius], **f32)
+        self.gridParams = torch.tensor([-gx, -gy, -gz, cell_size, 1.0 / cell_size, grab], **f32)
+        self.gridDims = torch.tensor([nX, nY, nZ, self.totalCells], **i32)
+        self.gridCounts = torch.tensor([0, n_seg, 0, 0], **i32)
+        self.center = torch.zeros(3 * n_seg, **f32)
+        self.boundingRadius = torch.zeros(n_seg, **f32)
+        self.ownerStore = torch.zeros(n_seg, **i32)
+        self.ownerSlot = torch.zeros(n_seg, **i32)
+        self.bodyCell = torch.full((n_seg,), -1, **i32)
+        self.cellCount = torch.zeros(self.totalCells, **i32)
+        self.chunkSum = torch.zeros((self.totalCells + 511) // 512 + 1, **i32)
+        self.gridCellOffsets = torch.zeros(self.totalCells + 1, **i32)
+        self.gridCellContents = torch.full((n_seg,), -1, **i32)
+        self.candCountSeg = torch.zeros(n_seg, **i32)
+        self.candBaseSeg = torch.zeros(n_seg + 1, **i32)
+
+    def build(self, filCoord, filSegLength, filState=None):
+        """publishToBodyView -> bodyCell -> counting sort (FormationGrid.buildCpu)."""
+        c = _ctx()
+        c("sbx_filament_publish", self.nSeg, filCoord, filSegLength, self.nSeg, self.center, self.boundingRadius,
+          self.ownerStore, self.ownerSlot, self.viewParams, filState)
+        SpatialGrid.bodyCell(self.center, self.gridParams, self.gridDims, self.gridCounts, self.bodyCell)
+        SpatialGrid.build(self.bodyCell, self.gridCounts, self.gridDims, self.cellCount, self.chunkSum,
+                          self.gridCellOffsets, self.gridCellContents)
+
+    def formCandidates(self, filCoord, filSegLength, filID, reqFilA, reqFilB, formParams, formCounts):
+        """gridFormCount -> gridFormScan -> gridFormEmit (FormationGrid.formCandidatesCpu)."""
+        CrosslinkerSystem.gridFormCount(filCoord, filSegLength, filID, self.gridParams, self.gridDims,
+                                        self.gridCellOffsets, self.gridCellContents, self.candCountSeg, formParams)
+        CrosslinkerSystem.gridFormScan(self.candCountSeg, self.candBaseSeg, reqFilA, reqFilB, formCounts)
+        CrosslinkerSystem.gridFormEmit(filCoord, filSegLength, filID, self.gridParams, self.gridDims,
+                                       self.gridCellOffsets, self.gridCellContents, self.candBaseSeg,
+                                       self.candCountSeg, reqFilA, reqFilB, formParams)
 
 
 class MotorJointSystem:                      # MotorJointSystem.java:72

@@ -57,3 +57,73 @@ def compare_scenes(host, dev_host, skip=()):
 
 def small_dense(scale=0.05, **kw):
     return scenes.dense_contractile(scenes.dense_small(scale, **kw))
+
+
+# ---------------------------------------------------------------- crosslinker formation
+def oracle_formation_grid(orc, sc):
+    """FormationGrid.buildCpu (FormationGrid.java:90-101) on host arrays; returns the grid."""
+    f = sc["fil"]
+    b = f["body"]
+    n = b["n"]
+    g = sc["grid"]
+    half, cell = g["half"], g["cell"]
+    nX = 1 + int(np.ceil(2 * half / cell))
+    total = nX ** 3
+    grid = {"gridParams": np.array([-half, -half, -half, cell, 1.0 / cell, g["grab"]], np.float32),
+            "gridDims": np.array([nX, nX, nX, total], np.int32),
+            "center": np.zeros(3 * n, np.float32), "R": np.zeros(n, np.float32),
+            "ownerStore": np.zeros(n, np.int32), "ownerSlot": np.zeros(n, np.int32),
+            "bodyCell": np.full(n, -1, np.int32), "cellCount": np.zeros(total, np.int32),
+            "chunkSum": np.zeros((total + 511) // 512 + 1, np.int32),
+            "offsets": np.zeros(total + 1, np.int32), "contents": np.full(n, -1, np.int32),
+            "candCountSeg": np.zeros(n, np.int32), "candBaseSeg": np.zeros(n + 1, np.int32)}
+    vp = np.array([g["radius"]], np.float32)
+    orc.fil_publish(n, b["coord"], b["segLength"], n, grid["center"], grid["R"], grid["ownerStore"],
+                    grid["ownerSlot"], vp, None)
+    orc.body_cell(n, grid["center"], grid["gridParams"], grid["gridDims"], n, grid["bodyCell"])
+    orc.grid_zero(total, grid["cellCount"])
+    orc.grid_histogram(grid["bodyCell"], n, grid["cellCount"])
+    orc.grid_scan_local(total, grid["cellCount"], grid["offsets"], grid["chunkSum"])
+    orc.grid_scan_chunks(total, grid["chunkSum"])
+    orc.grid_scan_add(total, grid["offsets"], n, grid["cellCount"], grid["chunkSum"])
+    orc.grid_scatter(grid["bodyCell"], n, grid["offsets"], grid["contents"], n, grid["cellCount"])
+    return grid
+
+
+def oracle_formation(orc, sc, step, use_grid=True):
+    """CrosslinkerBundleHarness.formationCpu (CrosslinkerBundleHarness.java:451-507) on host
+    arrays: counts, candidates, gates, admission, free list, ranks, allocate, orientation."""
+    f, xl = sc["fil"], sc["xl"]
+    b = f["body"]
+    n, C, K = b["n"], sc["C"], sc["reqCap"]
+    xl["formCounts"][1] = step
+    orc.count_active_links(C, xl["linkState"], xl["linkFilA"], xl["linkFilB"], n, xl["activeLinkCount"])
+    if use_grid:
+        g = oracle_formation_grid(orc, sc)
+        orc.xl_grid_form_count(n, b["coord"], b["segLength"], sc["filID"], g["gridParams"], g["gridDims"],
+                               g["offsets"], g["contents"], g["candCountSeg"], xl["formParams"])
+        orc.xl_grid_form_scan(n, g["candCountSeg"], g["candBaseSeg"], K, xl["reqFilA"], xl["reqFilB"],
+                              xl["formCounts"])
+        orc.xl_grid_form_emit(n, b["coord"], b["segLength"], sc["filID"], g["gridParams"], g["gridDims"],
+                              g["offsets"], g["contents"], g["candBaseSeg"], g["candCountSeg"], K, xl["reqFilA"],
+                              xl["reqFilB"], xl["formParams"])
+    else:
+        orc.xl_fil_fil_candidates(n, b["coord"], b["segLength"], sc["filID"], K, xl["reqFilA"], xl["reqFilB"],
+                                  xl["formParams"], xl["formCounts"])
+    orc.xl_form_gates(n, b["uVec"], b["end1"], b["end2"], b["segLength"], K, xl["reqFilA"], xl["reqFilB"],
+                      xl["reqLoc1"], xl["reqLoc2"], xl["reqOrient"], xl["gatePass"], xl["formParams"],
+                      xl["formCounts"])
+    orc.xl_form_admit_reduce(K, xl["reqFilA"], xl["reqFilB"], xl["gatePass"], n, xl["minCand"])
+    orc.xl_form_admit(K, xl["reqFilA"], xl["reqFilB"], xl["reqLoc1"], xl["reqLoc2"], xl["gatePass"], xl["minCand"],
+                      xl["activeLinkCount"], C, xl["linkState"], xl["linkFilA"], xl["linkFilB"], xl["loc1"],
+                      xl["loc2"], xl["acceptFlag"], xl["formParams"])
+    orc.xl_free_flags(C, xl["linkState"], xl["freeCount"])
+    orc.csr_scan(C, xl["freeCount"], xl["freeOffsets"])
+    orc.xl_free_scatter(C, xl["linkState"], xl["freeOffsets"], xl["freeList"])
+    orc.csr_scan(K, xl["acceptFlag"], xl["rankOffsets"])
+    orc.xl_allocate(K, xl["reqFilA"], xl["reqFilB"], xl["reqLoc1"], xl["reqLoc2"], xl["rankOffsets"],
+                    xl["freeList"], xl["freeOffsets"], C, xl["linkFilA"], xl["linkFilB"], xl["loc1"], xl["loc2"],
+                    xl["linkState"], xl["strainHist"], xl["strainPlace"])
+    orc.xl_place_orient(K, xl["reqOrient"], xl["rankOffsets"], xl["freeList"], xl["freeOffsets"], C,
+                        xl["linkOrientSame"], xl["torqueMagHist"], xl["torqueMagPlace"])
+    return sc
