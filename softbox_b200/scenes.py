@@ -95,6 +95,17 @@ def store_drag(b, i, g):
         b["bRotDiff"][k * n + i] = F32(KT / g[3 + k])
 
 
+def store_drag_slots(b, idx, g):
+    """store_drag for every slot in `idx` (one drag tuple)."""
+    n = b["n"]
+    idx = np.asarray(idx)
+    for k in range(3):
+        b["bTransGam"][k * n + idx] = F32(g[k])
+        b["bRotGam"][k * n + idx] = F32(g[3 + k])
+        b["bTransDiff"][k * n + idx] = F32(KT / g[k])
+        b["bRotDiff"][k * n + idx] = F32(KT / g[3 + k])
+
+
 def set_vec(arr, n, i, x, y, z):
     arr[i] = F32(x)
     arr[n + i] = F32(y)
@@ -142,13 +153,19 @@ def drag_run_filament(f, aeta):
     """DragTensorSystem.run(FilamentStore) (DragTensorSystem.java:71-97), viscosity `aeta`."""
     b = f["body"]
     halfmono = ACTIN_MONO_RADIUS
-    for i in range(b["n"]):
-        length = (int(f["monomerCount"][i]) + 1) * ACTIN_MONO_RADIUS
-        b["segLength"][i] = F32(length)
-        at_end = f["end1NbrSlot"][i] == -1 or f["end2NbrSlot"][i] == -1
-        min_len = STD_SEG_LENGTH * halfmono if at_end else 30 * halfmono
-        as_if = length if length >= min_len else min_len
-        store_drag(b, i, rod_drag_si(as_if, ACTIN_RADIUS, aeta))
+    mono = f["monomerCount"].astype(np.int64)
+    at_end = (f["end1NbrSlot"] == -1) | (f["end2NbrSlot"] == -1)
+    for m in np.unique(mono):
+        length = (int(m) + 1) * ACTIN_MONO_RADIUS
+        sel_m = mono == m
+        b["segLength"][sel_m] = F32(length)
+        for end in (False, True):
+            sel = np.flatnonzero(sel_m & (at_end == end))
+            if sel.size == 0:
+                continue
+            min_len = STD_SEG_LENGTH * halfmono if end else 30 * halfmono
+            as_if = length if length >= min_len else min_len
+            store_drag_slots(b, sel, rod_drag_si(as_if, ACTIN_RADIUS, aeta))
 
 
 def rescale_viscosity(b, r):
@@ -287,6 +304,7 @@ class DenseConfig:
     xl_off: tuple = (1.0, 0.0, 2.0)  # k_off = c + a*exp(b*strain): 1/s
     xl_torsion_spring: float = 1.0e-19
     xl_unbind: bool = True
+    fast_links: bool = False         # seeded KD-tree placement (large scale-sweep networks)
     seed: int = 0x0CDE5
     seed_bb: int = 0x5C2F11
     seed_fil: int = 0xF11A
@@ -359,6 +377,49 @@ def _place_dimer_along(b, mA, mB, e1, d, p, cfg):
     _place_arm(b, mB, rc, (dx, dy, dz), (px, py, pz), e2, -1, cfg)
 
 
+def _place_dimers(b, e1, d, p, cfg):
+    """_place_dimer_along for every dimer at once (dimer k: motors 2k, 2k+1), the same double
+    expressions evaluated elementwise. e1, d, p: (3, nDimers) float64."""
+    n = b["n"]
+    nd = e1.shape[1]
+    dm = np.sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2])
+    dx, dy, dz = d[0] / dm, d[1] / dm, d[2] / dm
+    pm = np.sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2])
+    px, py, pz = p[0] / pm, p[1] / pm, p[2] / pm
+    rl = ROD_LEN
+    rc = (e1[0] + 0.5 * rl * dx, e1[1] + 0.5 * rl * dy, e1[2] + 0.5 * rl * dz)
+    e2 = (e1[0] + rl * dx, e1[1] + rl * dy, e1[2] + rl * dz)
+    ll, hl = LEVER_LEN, HEAD_LEN
+    nx, ny, nz = dy * pz - dz * py, dz * px - dx * pz, dx * py - dy * px
+
+    def put(arr, slots, x, y, z):
+        arr[slots] = np.asarray(x).astype(F32)
+        arr[n + slots] = np.asarray(y).astype(F32)
+        arr[2 * n + slots] = np.asarray(z).astype(F32)
+
+    for splay, m in ((+1, 2 * np.arange(nd)), (-1, 2 * np.arange(nd) + 1)):
+        rod, lever, head = 3 * m, 3 * m + 1, 3 * m + 2
+        put(b["coord"], rod, *rc)
+        put(b["uVec"], rod, dx, dy, dz)
+        put(b["yVec"], rod, px, py, pz)
+        lux = COS80 * dx + splay * SIN80 * px
+        luy = COS80 * dy + splay * SIN80 * py
+        luz = COS80 * dz + splay * SIN80 * pz
+        put(b["coord"], lever, e2[0] + 0.5 * ll * lux, e2[1] + 0.5 * ll * luy, e2[2] + 0.5 * ll * luz)
+        put(b["uVec"], lever, lux, luy, luz)
+        put(b["yVec"], lever, nx, ny, nz)
+        le2 = (e2[0] + ll * lux, e2[1] + ll * luy, e2[2] + ll * luz)
+        put(b["coord"], head, le2[0] + 0.5 * hl * lux, le2[1] + 0.5 * hl * luy, le2[2] + 0.5 * hl * luz)
+        put(b["uVec"], head, lux, luy, luz)
+        put(b["yVec"], head, nx, ny, nz)
+        b["brownTransScale"][rod] = F32(cfg.brown_trans)
+        b["brownRotScale"][rod] = F32(cfg.brown_rot)
+        b["brownTransScale"][lever] = 0
+        b["brownRotScale"][lever] = 0
+        b["brownTransScale"][head] = F32(cfg.brown_trans)
+        b["brownRotScale"][head] = F32(cfg.brown_rot)
+
+
 def _pack_cell(x, y, z):
     return ((x & 0x1FFFFF) << 42) | ((y & 0x1FFFFF) << 21) | (z & 0x1FFFFF)
 
@@ -381,30 +442,33 @@ def dense_contractile(cfg: DenseConfig = C1):
     # ---- filaments: free multi-segment chains ----
     f = filament_store(n_seg)
     fb = f["body"]
+    # per filament: the reference's four draws, in order; per segment: the same double
+    # expressions evaluated elementwise
+    fil = np.empty((n_fil, 6))
     for p in range(n_fil):
         cx = (rng.next_double() - 0.5) * (side - 2 * margin)
         cy = (rng.next_double() - 0.5) * (side - 2 * margin)
         cz = (rng.next_double() - 0.5) * (box_z - 0.1)
         th = rng.next_double() * math.pi * 2
-        ux, uy, uz = math.cos(th), math.sin(th), 0.0
-        yx, yy, yz = -uy, ux, 0.0
-        g0 = p * S
-        for s in range(S):
-            g = g0 + s
-            off = (s - 0.5 * (S - 1)) * L
-            f["monomerCount"][g] = cfg.monomer_ct
-            set_vec(fb["uVec"], n_seg, g, ux, uy, uz)
-            set_vec(fb["yVec"], n_seg, g, yx, yy, yz)
-            set_vec(fb["coord"], n_seg, g, cx + off * ux, cy + off * uy, cz + off * uz)
-            fb["brownTransScale"][g] = F32(BTRANS_COEFF)
-            end = (s == 0 or s == S - 1)
-            fb["brownRotScale"][g] = F32(BROT_COEFF if end else 0.0)
-            if s < S - 1:
-                f["end2NbrSlot"][g] = g + 1
-                f["end2NbrSide"][g] = 0
-            if s > 0:
-                f["end1NbrSlot"][g] = g - 1
-                f["end1NbrSide"][g] = 1
+        fil[p] = (cx, cy, cz, math.cos(th), math.sin(th), 0.0)
+    off = (np.arange(S) - 0.5 * (S - 1)) * L
+    cx, cy, cz, ux, uy, uz = (np.repeat(fil[:, k], S) for k in range(6))
+    offs = np.tile(off, n_fil)
+    f["monomerCount"][:] = cfg.monomer_ct
+    fb["uVec"][:] = np.concatenate([ux, uy, uz]).astype(F32)
+    fb["yVec"][:] = np.concatenate([-uy, ux, np.zeros(n_seg)]).astype(F32)
+    fb["coord"][:] = np.concatenate([cx + offs * ux, cy + offs * uy, cz + offs * uz]).astype(F32)
+    fb["brownTransScale"][:] = F32(BTRANS_COEFF)
+    sidx = np.tile(np.arange(S), n_fil)
+    ends = (sidx == 0) | (sidx == S - 1)
+    fb["brownRotScale"][:] = np.where(ends, F32(BROT_COEFF), F32(0.0)).astype(F32)
+    g = np.arange(n_seg)
+    inner2 = sidx < S - 1
+    f["end2NbrSlot"][inner2] = g[inner2] + 1
+    f["end2NbrSide"][inner2] = 0
+    inner1 = sidx > 0
+    f["end1NbrSlot"][inner1] = g[inner1] - 1
+    f["end1NbrSide"][inner1] = 1
     drag_run_filament(f, cfg.aeta)
     if cfg.fil_aeta != cfg.aeta:
         rescale_viscosity(fb, cfg.fil_aeta / cfg.aeta)
@@ -427,6 +491,7 @@ def dense_contractile(cfg: DenseConfig = C1):
     bbb = mini["backbone"]
     reach = np.zeros(n_mot, F32)
     d = 0
+    dimer_rows = []
     for mfi in range(n_mini):
         bx = (rng.next_double() - 0.5) * (side - 2 * margin)
         by = (rng.next_double() - 0.5) * (side - 2 * margin)
@@ -444,18 +509,21 @@ def dense_contractile(cfg: DenseConfig = C1):
             for j in range(cfg.dimers_per_end):
                 mag = cfg.backbone_len / 2.0 - (j + 0.5) / cfg.dimers_per_end * cfg.head_zone
                 ax = sgn * mag
-                e1 = (bx + ax * ux, by + ax * uy, bz + ax * uz)
                 phi = (j + 0.5) / cfg.dimers_per_end * math.pi
-                px = math.cos(phi) * yx + math.sin(phi) * (uy * yz - uz * yy)
-                py = math.cos(phi) * yy + math.sin(phi) * (uz * yx - ux * yz)
-                pz = math.cos(phi) * yz + math.sin(phi) * (ux * yy - uy * yx)
-                mA, mB = 2 * d, 2 * d + 1
-                _place_dimer_along(mb, mA, mB, e1, (sgn * ux, sgn * uy, sgn * uz), (px, py, pz), cfg)
-                dim["motorA"][d], dim["motorB"][d], dim["parallel"][d] = mA, mB, 1
-                mini["headBackboneSlot"][d], mini["motorA"][d] = mfi, mA
-                mini["attachAxial"][d] = F32(ax)
-                reach[mA] = reach[mB] = F32(cfg.myo_col_tol)
+                dimer_rows.append((bx + ax * ux, by + ax * uy, bz + ax * uz, sgn * ux, sgn * uy, sgn * uz,
+                                   math.cos(phi) * yx + math.sin(phi) * (uy * yz - uz * yy),
+                                   math.cos(phi) * yy + math.sin(phi) * (uz * yx - ux * yz),
+                                   math.cos(phi) * yz + math.sin(phi) * (ux * yy - uy * yx), ax, mfi))
                 d += 1
+    if n_dimers:
+        rows = np.array(dimer_rows)
+        _place_dimers(mb, rows[:, 0:3].T, rows[:, 3:6].T, rows[:, 6:9].T, cfg)
+        dd = np.arange(n_dimers)
+        dim["motorA"][:], dim["motorB"][:], dim["parallel"][:] = 2 * dd, 2 * dd + 1, 1
+        mini["headBackboneSlot"][:] = rows[:, 10].astype(I32)
+        mini["motorA"][:] = 2 * dd
+        mini["attachAxial"][:] = rows[:, 9].astype(F32)
+        reach[:] = F32(cfg.myo_col_tol)
     # DragTensorSystem.run(MotorStore) (DragTensorSystem.java:105-122)
     gr = rod_drag_si(ROD_LEN, ROD_R, cfg.aeta)
     gl = rod_drag_si(LEVER_LEN, LEVER_R, cfg.aeta)
@@ -463,17 +531,15 @@ def dense_contractile(cfg: DenseConfig = C1):
     mb["segLength"][0::3] = F32(ROD_LEN)
     mb["segLength"][1::3] = F32(LEVER_LEN)
     mb["segLength"][2::3] = F32(HEAD_LEN)
-    for m in range(n_mot):
-        store_drag(mb, 3 * m, gr)
-        store_drag(mb, 3 * m + 1, gl)
-        store_drag(mb, 3 * m + 2, gh)
+    store_drag_slots(mb, np.arange(n_mot) * 3, gr)
+    store_drag_slots(mb, np.arange(n_mot) * 3 + 1, gl)
+    store_drag_slots(mb, np.arange(n_mot) * 3 + 2, gh)
     # MiniFilamentStore.initBackboneDrag (MiniFilamentStore.java:294-307)
     gbb = rod_drag_si(cfg.backbone_len, BACKBONE_R, cfg.aeta)
-    for bbi in range(n_mini):
-        bbb["segLength"][bbi] = F32(cfg.backbone_len)
-        store_drag(bbb, bbi, gbb)
-        mini["bbInvDragY"][bbi] = F32(1.0 / gbb[1])
-        mini["bbInvDragY"][n_mini + bbi] = F32(1.0 / gbb[4])
+    bbb["segLength"][:] = F32(cfg.backbone_len)
+    store_drag_slots(bbb, np.arange(n_mini), gbb)
+    mini["bbInvDragY"][:n_mini] = F32(1.0 / gbb[1])
+    mini["bbInvDragY"][n_mini:] = F32(1.0 / gbb[4])
 
     # MotorStore set-up (MotorStore.java:190-263), DenseContractileHarness.java:210-215
     mot.update({
@@ -523,7 +589,7 @@ def dense_contractile(cfg: DenseConfig = C1):
     }
 
     # ---- crosslinkers pre-placed between nearby segments of distinct filaments ----
-    xl = _build_crosslinkers(f, n_seg, S, cfg, rng)
+    xl = _build_crosslinkers_fast(f, n_seg, S, cfg) if cfg.fast_links else _build_crosslinkers(f, n_seg, S, cfg, rng)
 
     check_int = max(1, int(round(1.0e-4 / dt)))
     scene = {
@@ -606,6 +672,63 @@ def _build_crosslinkers(f, n_seg, segs_per_fil, cfg, rng):
     xl["torsionParams"] = np.array([cfg.xl_torsion_spring, 1.0], F32)
     xl["counts"][2] = cfg.seed
     return xl
+
+
+def _build_crosslinkers_fast(f, n_seg, segs_per_fil, cfg):
+    """The composition of buildCrosslinkers for large networks: each link joins a random
+    segment to the nearest segment of another filament within the grab distance, found with
+    a KD-tree; draws from a seeded numpy generator (not the harness's java.util.Random
+    sequence), so the network differs from the exact builder's but has its statistics."""
+    from scipy.spatial import cKDTree
+    n_links = cfg.n_links
+    proto = _build_crosslinkers(f, n_seg, segs_per_fil, replace(cfg, n_links=0), None)
+    xl = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in proto.items()}
+    for k, shape, fill, dt in (("linkFilA", n_links, -1, I32), ("linkFilB", n_links, -1, I32),
+                               ("linkState", n_links, -1, I32), ("linkOrientSame", n_links, 0, I32),
+                               ("loc1", n_links, 0, F32), ("loc2", n_links, 0, F32),
+                               ("xlinkData", n_links * XL_STRIDE, 0, F32), ("strainHist", n_links * STRAIN_WIN, 0, F32),
+                               ("torqueMagHist", n_links * TORQUE_WIN, 0, F32), ("strainPlace", n_links, 0, I32),
+                               ("torqueMagPlace", n_links, 0, I32), ("segIdxA", n_links, 0, I32),
+                               ("segIdxB", n_links, 0, I32)):
+        xl[k] = np.full(shape, fill, dt)
+    xl["nLinks"] = n_links
+    xl["counts"][0] = n_links
+    fb = f["body"]
+    pts = np.stack([fb["coord"][:n_seg], fb["coord"][n_seg:2 * n_seg], fb["coord"][2 * n_seg:]], 1).astype(np.float64)
+    fil = np.arange(n_seg) // segs_per_fil
+    tree = cKDTree(pts)
+    rng = np.random.default_rng(cfg.seed)
+    placed = 0
+    while placed < n_links:
+        draws = rng.integers(0, n_seg, size=2 * (n_links - placed) + 64)
+        dist, idx = tree.query(pts[draws], k=24, distance_upper_bound=cfg.xl_grab)
+        ok = (idx < n_seg)
+        ok &= fil[np.minimum(idx, n_seg - 1)] != fil[draws][:, None]
+        has = ok.any(1)
+        first = np.argmax(ok, 1)
+        for r in np.flatnonzero(has):
+            if placed == n_links:
+                break
+            a, b = int(draws[r]), int(idx[r, first[r]])
+            xl["linkFilA"][placed], xl["linkFilB"][placed] = a, b
+            xl["loc1"][placed] = F32(0.5 * float(fb["segLength"][a]))
+            xl["loc2"][placed] = F32(0.5 * float(fb["segLength"][b]))
+            xl["linkState"][placed] = 0
+            xl["linkOrientSame"][placed] = 1
+            placed += 1
+    xl["placed"] = placed
+    return xl
+
+
+def dense_scaled(n_rods, **kw):
+    """The benchmark network's composition at `n_rods` actin rods and the same density
+    (the scale sweep: slab side scaled by sqrt(n_rods / 20,000)), crosslinkers placed by
+    the KD-tree builder."""
+    c = C1
+    scale = n_rods / c.n_seg
+    return replace(c, n_fil=int(n_rods) // c.segs_per_fil, n_mini=max(1, int(round(c.n_mini * scale))),
+                   n_links=max(1, int(round(c.n_links * scale))), side=c.side * math.sqrt(scale), fast_links=True,
+                   **kw)
 
 
 # ---------------------------------------------------------------- crosslinker formation scene
