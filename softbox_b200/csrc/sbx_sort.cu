@@ -73,15 +73,28 @@ __global__ void __launch_bounds__(256) k_scan_local(const int* rowCount, int nRo
     if (threadIdx.x == 0) chunkSum[blockIdx.x] = total;
 }
 
-// SpatialGrid.gridScanChunks (SpatialGrid.java:188-200) as a one-block scan with carry
+// SpatialGrid.gridScanChunks (SpatialGrid.java:188-200) as a one-block scan with carry,
+// eight consecutive tile sums per thread per pass
 __global__ void __launch_bounds__(1024) k_scan_chunks(int* chunkSum, int numChunks) {
+    constexpr int PER = 8;
     int carry = 0;
-    for (int t0 = 0; t0 < numChunks; t0 += 1024) {
-        int idx = t0 + threadIdx.x;
-        int v = idx < numChunks ? chunkSum[idx] : 0;
+    for (int t0 = 0; t0 < numChunks; t0 += 1024 * PER) {
+        int base = t0 + threadIdx.x * PER;
+        int v[PER];
+        int sum = 0;
+#pragma unroll
+        for (int j = 0; j < PER; j++) {
+            v[j] = base + j < numChunks ? chunkSum[base + j] : 0;
+            sum += v[j];
+        }
         int total;
-        int ex = block_exclusive_scan<1024>(v, &total);
-        if (idx < numChunks) chunkSum[idx] = carry + ex;
+        int ex = block_exclusive_scan<1024>(sum, &total);
+        int run = carry + ex;
+#pragma unroll
+        for (int j = 0; j < PER; j++) {
+            if (base + j < numChunks) chunkSum[base + j] = run;
+            run += v[j];
+        }
         carry += total;
     }
     if (threadIdx.x == 0) chunkSum[numChunks] = carry;

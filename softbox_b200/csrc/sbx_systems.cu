@@ -471,27 +471,52 @@ extern "C" sbx_status sbx_fusion_integ_derive_confined(sbx_ctx* ctx, int32_t n, 
 }
 
 // ============================================================================ chain
-__device__ __forceinline__ void chain_slot(int n, int i, const float* coord, const float* uVec, const float* segLength,
-                                           const int* e2s, const int* e2d, const int* e1s, const int* e1d,
-                                           const float* bTG, const float* bRG, const ChainParams& cp, double f[3],
-                                           double t[3]) {
-    RodGeom r = load_rod(n, i, coord, uVec, segLength, bTG, bRG);
-    f[0] = f[1] = f[2] = 0.0;
-    t[0] = t[1] = t[2] = 0.0;
-    int s2 = e2s[i];
-    if (s2 >= 0) chain_side(cp, i, 0, s2, e2d[i], r, load_rod(n, s2, coord, uVec, segLength, bTG, bRG), f, t);
-    int s1 = e1s[i];
-    if (s1 >= 0) chain_side(cp, i, 1, s1, e1d[i], r, load_rod(n, s1, coord, uVec, segLength, bTG, bRG), f, t);
-}
+// ChainBendingForceSystem.chainForces (ChainBendingForceSystem.java:105-331), one thread per
+// rod. Each joint's costly scalars (chain_joint) are computed once by its lower-slot rod and
+// shared through shared memory with the partner when both rods are in the block and the
+// partner's neighbour entries point back consistently; otherwise the rod computes the joint
+// from its own side, which gives the same bits.
+constexpr int CHAIN_THREADS = 256;
 
-__global__ void k_chain(int n, const float* coord, const float* uVec, const float* segLength, const int* e2s,
-                        const int* e2d, const int* e1s, const int* e1d, const float* bTG, const float* bRG, float* F,
-                        float* T, const float* chainParams) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__global__ void __launch_bounds__(CHAIN_THREADS) k_chain(int n, const float* coord, const float* uVec,
+                                                         const float* segLength, const int* e2s, const int* e2d,
+                                                         const int* e1s, const int* e1d, const float* bTG,
+                                                         const float* bRG, float* F, float* T,
+                                                         const float* chainParams) {
+    __shared__ ChainJoint js[2 * CHAIN_THREADS];
+    const int tid = threadIdx.x, lo = blockIdx.x * blockDim.x;
+    const int hi = min(lo + (int)blockDim.x, n);
+    const int i = lo + tid;
     ChainParams cp = chain_params(chainParams);
-    double f[3], t[3];
-    chain_slot(n, i, coord, uVec, segLength, e2s, e2d, e1s, e1d, bTG, bRG, cp, f, t);
+    RodGeom r, nb2, nb1;
+    int s2 = -1, d2 = 0, s1 = -1, d1 = 0;
+    if (i < n) {
+        r = load_rod(n, i, coord, uVec, segLength, bTG, bRG);
+        s2 = e2s[i]; d2 = e2d[i]; s1 = e1s[i]; d1 = e1d[i];
+        if (s2 >= 0) {
+            nb2 = load_rod(n, s2, coord, uVec, segLength, bTG, bRG);
+            if (s2 > i) js[2 * tid] = chain_joint(cp, i, 0, s2, d2, r, nb2);
+        }
+        if (s1 >= 0) {
+            nb1 = load_rod(n, s1, coord, uVec, segLength, bTG, bRG);
+            if (s1 > i) js[2 * tid + 1] = chain_joint(cp, i, 1, s1, d1, r, nb1);
+        }
+    }
+    __syncthreads();
+    if (i >= n) return;
+    // the joint seen from side `side` of rod i: its own slot, the partner's slot, or recomputed
+    auto joint = [&](int side, int slot, int nside, const RodGeom& nb) -> ChainJoint {
+        if (slot > i) return js[2 * tid + side];
+        if (slot >= lo && slot < hi && (nside == 0 || nside == 1)) {
+            int ps = 1 - nside;                                  // the partner's side facing rod i
+            int back = ps == 0 ? e2s[slot] : e1s[slot], backSide = ps == 0 ? e2d[slot] : e1d[slot];
+            if (back == i && backSide == 1 - side) return js[2 * (slot - lo) + ps];
+        }
+        return chain_joint(cp, i, side, slot, nside, r, nb);
+    };
+    double f[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
+    if (s2 >= 0) chain_apply(cp, i, 0, s2, d2, r, nb2, joint(0, s2, d2, nb2), f, t);
+    if (s1 >= 0) chain_apply(cp, i, 1, s1, d1, r, nb1, joint(1, s1, d1, nb1), f, t);
     for (int k = 0; k < 3; k++) {
         F[k * n + i] = (float)(F[k * n + i] + f[k]);
         T[k * n + i] = (float)(T[k * n + i] + t[k]);
@@ -505,7 +530,7 @@ extern "C" sbx_status sbx_chain_forces(sbx_ctx* ctx, int32_t n, const float* coo
     SBX_REQUIRE(ctx && n >= 0 && (n == 0 || (coord && uVec && segLength && e2s && e2d && e1s && e1d && bTG && bRG &&
                                              F && T && chainParams)));
     if (n == 0) return SBX_OK;
-    SBX_LAUNCH(ctx, k_chain, blocks(n), 256, n, coord, uVec, segLength, e2s, e2d, e1s, e1d, bTG, bRG, F, T,
+    SBX_LAUNCH(ctx, k_chain, blocks(n, CHAIN_THREADS), CHAIN_THREADS, n, coord, uVec, segLength, e2s, e2d, e1s, e1d, bTG, bRG, F, T,
                chainParams);
     return check_launch(ctx, "sbx_chain_forces");
 }
@@ -1034,15 +1059,24 @@ extern "C" sbx_status sbx_xlink_unbind(sbx_ctx* ctx, int32_t nSeg, const float* 
 }
 
 // ============================================================================ myosin structure
+// MotorJointSystem.joints (MotorJointSystem.java:72-197): one thread per motor evaluates its
+// two joints once and accumulates them into its rod, lever and head in the reference order.
 __global__ void k_joints(int nB, const float* coord, const float* uVec, const float* segLength, const float* bTG,
                          const float* bRG, float* F, float* T, const int* nuc, const float* jp) {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nB) return;
-    double f[3], t[3];
-    joints_one(s, nB, coord, uVec, segLength, bTG, bRG, nuc[s / 3], jp, f, t);
-    for (int k = 0; k < 3; k++) {
-        F[k * nB + s] = (float)(F[k * nB + s] + f[k]);
-        T[k * nB + s] = (float)(T[k * nB + s] + t[k]);
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nB / 3) return;
+    int st = nuc[m];
+    MotorJoint J2 = motor_joint(m, 0, nB, coord, uVec, segLength, bTG, bRG, jp);
+    MotorJoint J1 = motor_joint(m, 1, nB, coord, uVec, segLength, bTG, bRG, jp);
+    for (int role = 0; role < 3; role++) {
+        int s = 3 * m + role;
+        double f[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
+        if (role == 0 || role == 1) motor_joint_apply(J2, 0, role == 1, st, s, nB, uVec, segLength, jp, f, t);
+        if (role == 1 || role == 2) motor_joint_apply(J1, 1, role == 2, st, s, nB, uVec, segLength, jp, f, t);
+        for (int k = 0; k < 3; k++) {
+            F[k * nB + s] = (float)(F[k * nB + s] + f[k]);
+            T[k * nB + s] = (float)(T[k * nB + s] + t[k]);
+        }
     }
 }
 
@@ -1052,7 +1086,7 @@ extern "C" sbx_status sbx_motor_joints(sbx_ctx* ctx, int32_t nB, const float* co
     SBX_REQUIRE(ctx && nB >= 0 && nB % 3 == 0 && (nB == 0 || (coord && uVec && segLength && bTG && bRG && F && T &&
                                                               nuc && jp)));
     if (nB == 0) return SBX_OK;
-    SBX_LAUNCH(ctx, k_joints, blocks(nB), 256, nB, coord, uVec, segLength, bTG, bRG, F, T, nuc, jp);
+    SBX_LAUNCH(ctx, k_joints, blocks(nB / 3, 128), 128, nB, coord, uVec, segLength, bTG, bRG, F, T, nuc, jp);
     return check_launch(ctx, "sbx_motor_joints");
 }
 
