@@ -350,9 +350,10 @@ extern "C" sbx_status sbx_dense_plan_create(sbx_ctx* ctx, const sbx_dense_scene*
 }
 
 extern "C" sbx_status sbx_dense_plan_run(sbx_dense_plan* p, int32_t t0, int32_t nsteps, int32_t mode) {
-    if (!p || nsteps < 0 || mode < 0 || mode > 2) return SBX_EINVAL;
+    if (!p || nsteps < 0 || mode < 0 || mode > 3) return SBX_EINVAL;
     sbx_ctx* ctx = p->ctx;
     if (nsteps == 0) return SBX_OK;
+    if (mode == 3) mode = (p->fused_ok && p->scene.fil.body.n <= SBX_DENSE_AUTO_MAX_FUSED_RODS) ? 2 : 1;
     if (mode == 2) {
         if (!p->fused_ok) return fail(ctx, SBX_ESTATE, "fused path unavailable: " + p->fused_why);
         // the kernel leaves its histograms zeroed and its barrier words consistent at the

@@ -29,7 +29,7 @@ class DenseNetwork:
         if st != 0:
             raise SbxError(st, "sbx_dense_plan_create: " + self.ctx.last_error())
 
-    MODES = {"unfused": 0, "graph": 1, "fused": 2}
+    MODES = {"unfused": 0, "graph": 1, "fused": 2, "auto": 3}
 
     @property
     def kernels_per_step(self):
@@ -45,11 +45,13 @@ class DenseNetwork:
         return LIB.sbx_dense_plan_fused_grid(self.plan)
 
     def run(self, t0, nsteps, mode=None):
-        """Advance steps t0..t0+nsteps-1. mode: "fused" (default when available: one
-        persistent cooperative launch for all steps), "graph" (one CUDA-graph replay per
-        step) or "unfused" (the per-system call sequence). All give the same bits."""
+        """Advance steps t0..t0+nsteps-1. mode: "auto" (default: the fused kernel for
+        networks up to SBX_DENSE_AUTO_MAX_FUSED_RODS rods when available, else the graph
+        path), "fused" (one persistent cooperative launch for all steps), "graph" (one
+        CUDA-graph replay per step) or "unfused" (the per-system call sequence). All give
+        the same bits."""
         if mode is None:
-            mode = "fused" if self.fused_available else "graph"
+            mode = "auto"
         st = LIB.sbx_dense_plan_run(self.plan, int(t0), int(nsteps), self.MODES[mode])
         if st != 0:
             raise SbxError(st, "sbx_dense_plan_run: " + self.ctx.last_error())

@@ -37,7 +37,7 @@ def host(x):
 
 
 # ----------------------------------------------------------------------------- whole step
-@pytest.mark.parametrize("mode", ["unfused", "graph", "fused"])
+@pytest.mark.parametrize("mode", ["unfused", "graph", "fused", "auto"])
 def test_dense_steps_bitwise(orc_dm, warm_scene, mode):
     from softbox_b200.engine import DenseNetwork
     ref = copy.deepcopy(warm_scene)
