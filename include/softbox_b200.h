@@ -343,6 +343,107 @@ sbx_status sbx_xlink_place_orient(sbx_ctx* ctx, int32_t K, const int32_t* reqOri
                                   const int32_t* freeList, const int32_t* freeOffsets, int32_t C,
                                   int32_t* linkOrientSame, float* torqueMagHist, int32_t* torqueMagPlace);
 
+/* ---------------------------------------------------------------- actin turnover
+ * Planar filament slot arrays of capacity C (FilamentStore: coord/uVec/yVec [3*C], filState
+ * FREE -1 / ACTIVE 0, end1/end2 neighbour slot and side). growCounts/depolyCounts carry
+ * [1] step, [2] seed, [3] fires; severCounts/agingCounts carry [1] fires. Split and birth
+ * requests use the crosslinker allocator's scan ranks: freeFlags/freeScatter on filState are
+ * sbx_xlink_free_flags/_free_scatter (FilamentBirthSystem.java:41-58), ranks by sbx_csr_scan.
+ * GrowthSystem.grow (GrowthSystem.java:73-104): barbed-tip growth, wang-hash salt "GROW";
+ * growParams [P, halfmono, maxMon] */
+sbx_status sbx_growth_grow(sbx_ctx* ctx, int32_t C, const int32_t* seedNode, int32_t* monomerCount, float* coord,
+                           const float* uVec, int32_t* grewFlag, const float* growParams, const int32_t* growCounts);
+/* GrowthSystem.markSplits (:106-136): split requests at splitThresh monomers, request index =
+ * slot, request planar stride reqCap >= C; splitParams [halfmono, splitThresh, childMon] */
+sbx_status sbx_growth_mark_splits(sbx_ctx* ctx, int32_t C, const int32_t* seedNode, const int32_t* monomerCount,
+                                  const float* coord, const float* uVec, const float* yVec, int32_t* acceptFlag,
+                                  float* reqCoord, float* reqUVec, float* reqYVec, int32_t reqCap,
+                                  const float* splitParams, const int32_t* growCounts);
+/* GrowthSystem.splitWire (:148-190): parent shrink and the 3-slot chain rewire per formed split */
+sbx_status sbx_growth_split_wire(sbx_ctx* ctx, int32_t K, int32_t C, const int32_t* rankOffsets,
+                                 const int32_t* freeList, const int32_t* freeOffsets, int32_t* monomerCount,
+                                 float* coord, const float* uVec, int32_t* end1NbrSlot, int32_t* end1NbrSide,
+                                 int32_t* end2NbrSlot, int32_t* end2NbrSide, int32_t* seedNode,
+                                 const float* splitParams);
+/* GrowthSystem.recomputeDrag (:199-228): segLength and slender-rod drag from monomerCount;
+ * dragParams [halfmono, aeta, radius, kT, aPar, aOrth, aTurn, stdSeg, minMon] */
+sbx_status sbx_growth_recompute_drag(sbx_ctx* ctx, int32_t C, const int32_t* monomerCount, float* segLength,
+                                     const int32_t* end1NbrSlot, const int32_t* end2NbrSlot, float* bTransGam,
+                                     float* bRotGam, float* bTransDiff, float* bRotDiff, const float* dragParams,
+                                     const int32_t* growCounts);
+/* DepolySystem.depoly (DepolySystem.java:70-101): pointed-tip loss at fixed rate, death below
+ * the floor; depolyParams [P, halfmono, floor], salt "DEPO" */
+sbx_status sbx_depoly(sbx_ctx* ctx, int32_t C, const int32_t* filState, int32_t* monomerCount, float* coord,
+                      const float* uVec, const int32_t* end1NbrSlot, int32_t* returnedMon, int32_t* deathFlag,
+                      const float* depolyParams, const int32_t* depolyCounts);
+/* DepolySystem.depolyProxy (:115-145): rate = rateParams[0]*(1-fADP) + rateParams[1]*fADP */
+sbx_status sbx_depoly_proxy(sbx_ctx* ctx, int32_t C, const int32_t* filState, int32_t* monomerCount, float* coord,
+                            const float* uVec, const int32_t* end1NbrSlot, const float* nucFrac,
+                            int32_t* returnedMon, int32_t* deathFlag, const float* depolyParams,
+                            const float* depolyRateParams, const int32_t* depolyCounts);
+/* DepolySystem.applyDeath (:158-188): free each dying slot and break its chain links */
+sbx_status sbx_depoly_apply_death(sbx_ctx* ctx, int32_t C, int32_t* filState, int32_t* monomerCount,
+                                  int32_t* seedNode, int32_t* end1NbrSlot, int32_t* end1NbrSide,
+                                  int32_t* end2NbrSlot, int32_t* end2NbrSide, float* brownTransScale,
+                                  float* brownRotScale, const int32_t* deathFlag);
+/* SeveringSystem.cofilinAccumulate (SeveringSystem.java:37-49); cofilinParams [p_cof, ratio] */
+sbx_status sbx_sever_cofilin_accumulate(sbx_ctx* ctx, int32_t C, const int32_t* filState, const float* nucFrac,
+                                        float* cofFrac, const float* cofilinParams, const int32_t* severCounts);
+/* SeveringSystem.cofilinDissolve (:58-74): death flags where cofFrac > ratio */
+sbx_status sbx_sever_cofilin_dissolve(sbx_ctx* ctx, int32_t C, const int32_t* filState, const int32_t* monomerCount,
+                                      const float* cofFrac, int32_t* severDeathFlag, int32_t* severReturnedMon,
+                                      const float* cofilinParams, const int32_t* severCounts);
+/* SeveringSystem.nucleateFreshCofilin (:88-98): cofFrac = 0 in each claimed slot */
+sbx_status sbx_sever_nucleate_fresh_cofilin(sbx_ctx* ctx, int32_t K, int32_t C, const int32_t* rankOffsets,
+                                            const int32_t* freeList, const int32_t* freeOffsets, float* cofFrac);
+/* FilamentBirthSystem.allocate (FilamentBirthSystem.java:64-87): request pose into the claimed
+ * slot, birthParams [brownTransScale, brownRotScale], state ACTIVE */
+sbx_status sbx_birth_allocate(sbx_ctx* ctx, int32_t K, int32_t C, int32_t reqCap, const float* reqCoord,
+                              const float* reqUVec, const float* reqYVec, const int32_t* rankOffsets,
+                              const int32_t* freeList, const int32_t* freeOffsets, float* coord, float* uVec,
+                              float* yVec, float* brownTransScale, float* brownRotScale, int32_t* filState,
+                              const float* birthParams);
+/* AgingSystem.age (AgingSystem.java:40-57): ATP -> ADP-Pi -> ADP; agingParams [pH, pD] */
+sbx_status sbx_aging_age(sbx_ctx* ctx, int32_t C, const int32_t* filState, float* nucFrac,
+                         const float* agingParams, const int32_t* agingCounts);
+/* AgingSystem.growthAtp (:65-77): one fresh ATP monomer mixed into each grown tip */
+sbx_status sbx_aging_growth_atp(sbx_ctx* ctx, int32_t C, const int32_t* grewFlag, const int32_t* monomerCount,
+                                float* nucFrac);
+/* AgingSystem.splitInheritNuc (:88-102): a split child takes its parent's fractions */
+sbx_status sbx_aging_split_inherit_nuc(sbx_ctx* ctx, int32_t K, int32_t C, const int32_t* rankOffsets,
+                                       const int32_t* freeList, const int32_t* freeOffsets, float* nucFrac);
+/* AgingSystem.nucleateFreshAtp (:114-125): a newborn slot is all ATP */
+sbx_status sbx_aging_nucleate_fresh_atp(sbx_ctx* ctx, int32_t K, int32_t C, const int32_t* rankOffsets,
+                                        const int32_t* freeList, const int32_t* freeOffsets, float* nucFrac);
+/* ActinPool (ActinPool.java:27-63), held in device memory so that a turnover cadence needs
+ * no host round trip: the [actin] scalar (uM), the uM per monomer of the chamber volume
+ * ((1e5^3 * 1e6) / (boxVolume_um3 * 6.022e23)) and the exact integer ledger. */
+typedef struct sbx_actin_pool {
+    double conc;
+    double uMPerMonomer;
+    int64_t totalTaken;
+    int64_t totalReturned;
+} sbx_actin_pool;
+/* ActinPool.put (:49-52) of offsets[n] monomers, the total of a sbx_csr_scan (depoly and
+ * death returns: DepolyStore.returnPoolForDepoly, DepolyStore.java:88-93) */
+sbx_status sbx_actin_pool_put_total(sbx_ctx* ctx, sbx_actin_pool* pool, const int32_t* offsets, int32_t n);
+/* GrowthStore.depletePoolForGrows (GrowthStore.java:94-99): ActinPool.take (:42-46) of
+ * offsets[n] monomers when it is positive, the pool floored at 0 */
+sbx_status sbx_actin_pool_take_total(sbx_ctx* ctx, sbx_actin_pool* pool, const int32_t* offsets, int32_t n);
+/* The per-step prologue of the turnover block (FullSystemDemoHarness.java:648-651) on the
+ * device: GrowthStore/DepolyStore.setCounts (step, seed, fires), AgingStore/SeverStore
+ * .setFires, and GrowthStore.refreshRate (GrowthStore.java:84-88): growParams[0] =
+ * (float)(onRate * conc * biochemDeltaT), 0 when fires == 0. NULL arrays are skipped. */
+sbx_status sbx_turnover_begin(sbx_ctx* ctx, int32_t step, int32_t seed, int32_t fires, double onRate,
+                              double biochemDeltaT, const sbx_actin_pool* pool, float* growParams,
+                              int32_t* growCounts, int32_t* depolyCounts, int32_t* agingCounts,
+                              int32_t* severCounts);
+/* FilIDSystem.init (FilIDSystem.java:38-47): ptr = end2 neighbour (self at a chain end, -s-2 when FREE) */
+sbx_status sbx_filid_init(sbx_ctx* ctx, int32_t n, const int32_t* filState, const int32_t* end2NbrSlot,
+                          int32_t* ptr);
+/* FilIDSystem.jump (:52-58): one pointer-doubling round, ptrOut = ptrIn[ptrIn] (ptrIn != ptrOut) */
+sbx_status sbx_filid_jump(sbx_ctx* ctx, int32_t n, const int32_t* ptrIn, int32_t* ptrOut, const int32_t* filState);
+
 /* ---------------------------------------------------------------- myosin structure
  * MotorJointSystem.joints (MotorJointSystem.java:72-197) */
 sbx_status sbx_motor_joints(sbx_ctx* ctx, int32_t nB, const float* coord, const float* uVec,

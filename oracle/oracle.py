@@ -50,6 +50,24 @@ _SIGS = {
     "orc_xl_form_gates": "ippppipppppppp", "orc_xl_form_admit_reduce": "ipppip",
     "orc_xl_form_admit": "ipppppppippppppp", "orc_xl_free_flags": "ipp", "orc_xl_free_scatter": "ippp",
     "orc_xl_allocate": "ipppppppippppppp", "orc_xl_place_orient": "ippppippp",
+    "orc_growth_grow": "ippppppp",
+    "orc_growth_mark_splits": "ipppppppppipp",
+    "orc_growth_split_wire": "iipppppppppppp",
+    "orc_growth_recompute_drag": "ipppppppppp",
+    "orc_depoly": "ippppppppp",
+    "orc_depoly_proxy": "ippppppppppp",
+    "orc_apply_death": "ipppppppppp",
+    "orc_cofilin_accumulate": "ippppp",
+    "orc_cofilin_dissolve": "ippppppp",
+    "orc_nucleate_fresh_cofilin": "iipppp",
+    "orc_birth_allocate": "iiippppppppppppp",
+    "orc_aging_age": "ipppp",
+    "orc_aging_growth_atp": "ippp",
+    "orc_aging_split_inherit_nuc": "iipppp",
+    "orc_aging_nucleate_fresh_atp": "iipppp",
+    "orc_filid_init": "ippp",
+    "orc_filid_jump": "ippp",
+    "orc_pool_put_total": "ppi", "orc_pool_take_total": "ppi", "orc_turnover_begin": "iiiddpppppp",
 }
 _CT = {"i": C.c_int32, "I": C.c_uint64, "d": C.c_double, "f": C.c_float, "p": C.c_void_p, "s": C.c_void_p}
 _RET = {"orc_max_threads": C.c_int, "orc_accurate_acos": C.c_double, "orc_angle_from_sin_cos": C.c_double,

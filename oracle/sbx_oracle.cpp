@@ -2265,3 +2265,359 @@ EXPORT void orc_xl_place_orient(i32 K, const i32* reqOrient, const i32* rankOffs
         for (int j = 0; j < TORQUE_WIN; j++) torqueMagHist[b + j] = 0.f;
     }
 }
+
+// ============================================================================
+// Actin turnover: GrowthSystem.java:73-229, DepolySystem.java:70-189,
+// SeveringSystem.java:37-99, FilamentBirthSystem.java:41-88, AgingSystem.java:40-125,
+// FilIDSystem.java:38-59. Per-slot decisions are integer/wang-hash; poses float/double as
+// the Java source. `C` = the filament slot capacity; counts[1] = step, [2] = seed, [3] = fires.
+// ============================================================================
+namespace {
+const int FIL_FREE = -1, FIL_ACTIVE = 0;   // FilamentStore.java:112-113
+inline float turnover_unit(int s, i32 step, i32 seed, uint32_t salt) {
+    return sbxm::unit_from_hash(sbxm::wang_hash(sbxm::rng_base(s, step, seed) ^ salt));
+}
+}  // namespace
+
+// GrowthSystem.grow (:73-104)
+EXPORT void orc_growth_grow(i32 C, const i32* seedNode, i32* monomerCount, float* coord, const float* uVec,
+                            i32* grewFlag, const float* growParams, const i32* growCounts) {
+    i32 fires = growCounts[3], step = growCounts[1], seed = growCounts[2];
+    float P = growParams[0], halfmono = growParams[1];
+    int maxMon = jf2i(growParams[2]);
+    for (int s = 0; s < C; s++) {
+        grewFlag[s] = 0;
+        if (fires == 0) continue;
+        if (seedNode[s] < 0) continue;
+        if (monomerCount[s] >= maxMon) continue;
+        float u = turnover_unit(s, step, seed, 0x47524F57u);
+        if (u >= P) continue;
+        monomerCount[s] = monomerCount[s] + 1;
+        float ux = uVec[s], uy = uVec[C + s], uz = uVec[2 * C + s];
+        coord[s] = coord[s] - 0.5f * halfmono * ux;
+        coord[C + s] = coord[C + s] - 0.5f * halfmono * uy;
+        coord[2 * C + s] = coord[2 * C + s] - 0.5f * halfmono * uz;
+        grewFlag[s] = 1;
+    }
+}
+
+// GrowthSystem.markSplits (:113-136); RC = request planar stride
+EXPORT void orc_growth_mark_splits(i32 C, const i32* seedNode, const i32* monomerCount, const float* coord,
+                                   const float* uVec, const float* yVec, i32* acceptFlag, float* reqCoord,
+                                   float* reqUVec, float* reqYVec, i32 RC, const float* splitParams,
+                                   const i32* growCounts) {
+    i32 fires = growCounts[3];
+    double halfmono = splitParams[0];
+    int splitThresh = jf2i(splitParams[1]), childMon = jf2i(splitParams[2]);
+    for (int s = 0; s < C; s++) {
+        acceptFlag[s] = 0;
+        if (fires == 0) continue;
+        if (seedNode[s] < 0) continue;
+        int M = monomerCount[s];
+        if (M < splitThresh) continue;
+        int parentNewMon = M - childMon;
+        double Lold = (M + 1) * halfmono, Lpar = (parentNewMon + 1) * halfmono, Lchild = (childMon + 1) * halfmono;
+        double ux = uVec[s], uy = uVec[C + s], uz = uVec[2 * C + s];
+        double shift = 0.5 * Lold - Lpar - 0.5 * Lchild + halfmono;
+        reqCoord[s] = (float)(coord[s] + shift * ux);
+        reqCoord[RC + s] = (float)(coord[C + s] + shift * uy);
+        reqCoord[2 * RC + s] = (float)(coord[2 * C + s] + shift * uz);
+        reqUVec[s] = (float)ux; reqUVec[RC + s] = (float)uy; reqUVec[2 * RC + s] = (float)uz;
+        reqYVec[s] = yVec[s]; reqYVec[RC + s] = yVec[C + s]; reqYVec[2 * RC + s] = yVec[2 * C + s];
+        acceptFlag[s] = 1;
+    }
+}
+
+// GrowthSystem.splitWire (:147-190); K requests (request index == parent slot)
+EXPORT void orc_growth_split_wire(i32 K, i32 C, const i32* rankOffsets, const i32* freeList, const i32* freeOffsets,
+                                  i32* monomerCount, float* coord, const float* uVec, i32* e1s, i32* e1d, i32* e2s,
+                                  i32* e2d, i32* seedNode, const float* splitParams) {
+    int nFree = freeOffsets[C];
+    double halfmono = splitParams[0];
+    int childMon = jf2i(splitParams[2]);
+    for (int r = 0; r < K; r++) {
+        int rank = rankOffsets[r];
+        if (!(rankOffsets[r + 1] > rank)) continue;
+        if (rank >= nFree) continue;
+        int Gs = r, Cs = freeList[rank];
+        int M = monomerCount[Gs];
+        int parentNewMon = M - childMon;
+        int Mold = e1s[Gs], MoldSide = e1d[Gs];
+        double Lold = (M + 1) * halfmono, Lpar = (parentNewMon + 1) * halfmono;
+        double ux = uVec[Gs], uy = uVec[C + Gs], uz = uVec[2 * C + Gs];
+        double shift = 0.5 * Lold - 0.5 * Lpar;
+        coord[Gs] = (float)(coord[Gs] + shift * ux);
+        coord[C + Gs] = (float)(coord[C + Gs] + shift * uy);
+        coord[2 * C + Gs] = (float)(coord[2 * C + Gs] + shift * uz);
+        monomerCount[Gs] = parentNewMon;
+        monomerCount[Cs] = childMon;
+        seedNode[Cs] = -1;
+        e1s[Gs] = Cs; e1d[Gs] = 1;
+        e2s[Cs] = Gs; e2d[Cs] = 0;
+        e1s[Cs] = Mold;
+        e1d[Cs] = Mold >= 0 ? MoldSide : -1;
+        if (Mold >= 0) {
+            if (MoldSide == 0) e1s[Mold] = Cs;
+            else e2s[Mold] = Cs;
+        }
+    }
+}
+
+// GrowthSystem.recomputeDrag (:200-228); dragParams [halfmono, aeta, radius, kT, aPar, aOrth, aTurn, stdSeg, minMon]
+EXPORT void orc_growth_recompute_drag(i32 C, const i32* monomerCount, float* segLength, const i32* e1s,
+                                      const i32* e2s, float* bTG, float* bRG, float* bTD, float* bRD,
+                                      const float* dragParams, const i32* growCounts) {
+    i32 fires = growCounts[3];
+    double halfmono = dragParams[0], aeta = dragParams[1], radius = dragParams[2], kT = dragParams[3];
+    double aPar = dragParams[4], aOrth = dragParams[5], aTurn = dragParams[6];
+    int stdSeg = jf2i(dragParams[7]), minMon = jf2i(dragParams[8]);
+    PAR for (int i = 0; i < C; i++) {
+        if (fires == 0) continue;
+        int mc = monomerCount[i];
+        double length = (mc + 1) * halfmono;
+        segLength[i] = (float)length;
+        bool atEnd = (e1s[i] < 0) || (e2s[i] < 0);
+        double minLength = (atEnd ? stdSeg : minMon) * halfmono;
+        double asIf = length < minLength ? minLength : length;
+        double LM = 1.0e-6 * asIf, RM = radius * 1.0e-6;
+        double logT = JLOG(LM / (2.0 * RM));
+        double bTGx = (2.0 * PI_D * aeta * LM) / (logT + aPar);
+        double bTGy = (4.0 * PI_D * aeta * LM) / (logT + aOrth);
+        double bRGx = 4.0 * PI_D * aeta * RM * RM * LM;
+        double bRGy = (PI_D * aeta * (LM * LM * LM)) / (3.0 * (logT + aTurn));
+        int iy = C + i, iz = 2 * C + i;
+        bTG[i] = (float)bTGx; bTG[iy] = (float)bTGy; bTG[iz] = (float)bTGy;
+        bRG[i] = (float)bRGx; bRG[iy] = (float)bRGy; bRG[iz] = (float)bRGy;
+        bTD[i] = (float)(kT / bTGx); bTD[iy] = (float)(kT / bTGy); bTD[iz] = (float)(kT / bTGy);
+        bRD[i] = (float)(kT / bRGx); bRD[iy] = (float)(kT / bRGy); bRD[iz] = (float)(kT / bRGy);
+    }
+}
+
+// DepolySystem.depoly (:70-101) and depolyProxy (:113-145); rate = NULL for the fixed-rate form
+static void depoly_impl(i32 C, const i32* filState, i32* monomerCount, float* coord, const float* uVec,
+                        const i32* e1s, const float* nucFrac, i32* returnedMon, i32* deathFlag,
+                        const float* depolyParams, const float* rateParams, const i32* depolyCounts) {
+    i32 fires = depolyCounts[3], step = depolyCounts[1], seed = depolyCounts[2];
+    float halfmono = depolyParams[1];
+    int floorM = jf2i(depolyParams[2]);
+    for (int s = 0; s < C; s++) {
+        returnedMon[s] = 0;
+        deathFlag[s] = 0;
+        if (fires == 0) continue;
+        if (filState[s] < 0) continue;
+        if (e1s[s] >= 0) continue;
+        int M = monomerCount[s];
+        float P;
+        if (rateParams) {
+            float adp = nucFrac[2 * C + s];
+            P = rateParams[0] * (1.0f - adp) + rateParams[1] * adp;
+        } else {
+            P = depolyParams[0];
+        }
+        if (M >= floorM) {
+            float u = turnover_unit(s, step, seed, 0x4445504Fu);
+            if (u >= P) continue;
+            monomerCount[s] = M - 1;
+            float ux = uVec[s], uy = uVec[C + s], uz = uVec[2 * C + s];
+            coord[s] = coord[s] + 0.5f * halfmono * ux;
+            coord[C + s] = coord[C + s] + 0.5f * halfmono * uy;
+            coord[2 * C + s] = coord[2 * C + s] + 0.5f * halfmono * uz;
+            returnedMon[s] = 1;
+        } else {
+            deathFlag[s] = 1;
+            returnedMon[s] = M;
+        }
+    }
+}
+EXPORT void orc_depoly(i32 C, const i32* filState, i32* monomerCount, float* coord, const float* uVec, const i32* e1s,
+                       i32* returnedMon, i32* deathFlag, const float* depolyParams, const i32* depolyCounts) {
+    depoly_impl(C, filState, monomerCount, coord, uVec, e1s, nullptr, returnedMon, deathFlag, depolyParams, nullptr,
+                depolyCounts);
+}
+EXPORT void orc_depoly_proxy(i32 C, const i32* filState, i32* monomerCount, float* coord, const float* uVec,
+                             const i32* e1s, const float* nucFrac, i32* returnedMon, i32* deathFlag,
+                             const float* depolyParams, const float* rateParams, const i32* depolyCounts) {
+    depoly_impl(C, filState, monomerCount, coord, uVec, e1s, nucFrac, returnedMon, deathFlag, depolyParams, rateParams,
+                depolyCounts);
+}
+
+// DepolySystem.applyDeath (:155-188), serial
+EXPORT void orc_apply_death(i32 C, i32* filState, i32* monomerCount, i32* seedNode, i32* e1s, i32* e1d, i32* e2s,
+                            i32* e2d, float* bTS, float* bRS, const i32* deathFlag) {
+    for (int s = 0; s < C; s++) {
+        if (deathFlag[s] == 0) continue;
+        filState[s] = FIL_FREE;
+        bTS[s] = 0.f;
+        bRS[s] = 0.f;
+        monomerCount[s] = 0;
+        int n2 = e2s[s], n2side = e2d[s];
+        if (n2 >= 0) {
+            if (n2side == 0) { e1s[n2] = -1; e1d[n2] = -1; }
+            else { e2s[n2] = -1; e2d[n2] = -1; }
+            e2s[s] = -1; e2d[s] = -1;
+        }
+        int n1 = e1s[s], n1side = e1d[s];
+        if (n1 >= 0) {
+            if (n1side == 0) { e1s[n1] = -1; e1d[n1] = -1; }
+            else { e2s[n1] = -1; e2d[n1] = -1; }
+            e1s[s] = -1; e1d[s] = -1;
+        }
+        if (seedNode[s] >= 0) seedNode[s] = -1;
+    }
+}
+
+// SeveringSystem.cofilinAccumulate (:37-49), cofilinDissolve (:58-74), nucleateFreshCofilin (:87-98)
+EXPORT void orc_cofilin_accumulate(i32 C, const i32* filState, const float* nucFrac, float* cofFrac,
+                                   const float* cofilinParams, const i32* severCounts) {
+    i32 fires = severCounts[1];
+    float pCof = cofilinParams[0];
+    for (int s = 0; s < C; s++) {
+        if (fires == 0) continue;
+        if (filState[s] < 0) continue;
+        float fADP = nucFrac[2 * C + s], fCof = cofFrac[s];
+        cofFrac[s] = fCof + (fADP - fCof) * pCof;
+    }
+}
+EXPORT void orc_cofilin_dissolve(i32 C, const i32* filState, const i32* monomerCount, const float* cofFrac,
+                                 i32* severDeathFlag, i32* severReturnedMon, const float* cofilinParams,
+                                 const i32* severCounts) {
+    i32 fires = severCounts[1];
+    float ratio = cofilinParams[1];
+    for (int s = 0; s < C; s++) {
+        severDeathFlag[s] = 0;
+        severReturnedMon[s] = 0;
+        if (fires == 0) continue;
+        if (filState[s] < 0) continue;
+        if (cofFrac[s] > ratio) { severDeathFlag[s] = 1; severReturnedMon[s] = monomerCount[s]; }
+    }
+}
+// the accepted-rank -> slot pattern of the allocator companions (rank < nFree)
+static inline int alloc_slot(int r, const i32* rankOffsets, const i32* freeList, int nFree) {
+    int rank = rankOffsets[r];
+    if (!(rankOffsets[r + 1] > rank) || rank >= nFree) return -1;
+    return freeList[rank];
+}
+EXPORT void orc_nucleate_fresh_cofilin(i32 K, i32 C, const i32* rankOffsets, const i32* freeList,
+                                       const i32* freeOffsets, float* cofFrac) {
+    int nFree = freeOffsets[C];
+    for (int r = 0; r < K; r++) {
+        int slot = alloc_slot(r, rankOffsets, freeList, nFree);
+        if (slot >= 0) cofFrac[slot] = 0.f;
+    }
+}
+
+// FilamentBirthSystem.allocate (:61-87); freeFlags/freeScatter = orc_xl_free_flags/_scatter on filState
+EXPORT void orc_birth_allocate(i32 K, i32 C, i32 RC, const float* reqCoord, const float* reqUVec, const float* reqYVec,
+                               const i32* rankOffsets, const i32* freeList, const i32* freeOffsets, float* coord,
+                               float* uVec, float* yVec, float* bTS, float* bRS, i32* filState,
+                               const float* birthParams) {
+    int nFree = freeOffsets[C];
+    float bt = birthParams[0], br = birthParams[1];
+    for (int r = 0; r < K; r++) {
+        int slot = alloc_slot(r, rankOffsets, freeList, nFree);
+        if (slot < 0) continue;
+        for (int k = 0; k < 3; k++) {
+            coord[k * C + slot] = reqCoord[k * RC + r];
+            uVec[k * C + slot] = reqUVec[k * RC + r];
+            yVec[k * C + slot] = reqYVec[k * RC + r];
+        }
+        bTS[slot] = bt;
+        bRS[slot] = br;
+        filState[slot] = FIL_ACTIVE;
+    }
+}
+
+// AgingSystem.age (:40-57), growthAtp (:65-77), splitInheritNuc (:88-102), nucleateFreshAtp (:114-125)
+EXPORT void orc_aging_age(i32 C, const i32* filState, float* nucFrac, const float* agingParams,
+                          const i32* agingCounts) {
+    i32 fires = agingCounts[1];
+    float pH = agingParams[0], pD = agingParams[1];
+    for (int s = 0; s < C; s++) {
+        if (fires == 0) continue;
+        if (filState[s] < 0) continue;
+        float fATP = nucFrac[s], fADPPi = nucFrac[C + s];
+        float nATP = fATP * (1.0f - pH);
+        float nADPPi = fADPPi * (1.0f - pD) + fATP * pH;
+        float nADP = 1.0f - nATP - nADPPi;
+        nucFrac[s] = nATP; nucFrac[C + s] = nADPPi; nucFrac[2 * C + s] = nADP;
+    }
+}
+EXPORT void orc_aging_growth_atp(i32 C, const i32* grewFlag, const i32* monomerCount, float* nucFrac) {
+    for (int s = 0; s < C; s++) {
+        if (grewFlag[s] == 0) continue;
+        int M = monomerCount[s];
+        if (M <= 0) continue;
+        float w = (float)(M - 1) / (float)M;
+        float inv = 1.0f / (float)M;
+        nucFrac[s] = nucFrac[s] * w + inv;
+        nucFrac[C + s] = nucFrac[C + s] * w;
+        nucFrac[2 * C + s] = nucFrac[2 * C + s] * w;
+    }
+}
+EXPORT void orc_aging_split_inherit_nuc(i32 K, i32 C, const i32* rankOffsets, const i32* freeList,
+                                        const i32* freeOffsets, float* nucFrac) {
+    int nFree = freeOffsets[C];
+    for (int r = 0; r < K; r++) {
+        int Cs = alloc_slot(r, rankOffsets, freeList, nFree);
+        if (Cs < 0) continue;
+        int Gs = r;
+        nucFrac[Cs] = nucFrac[Gs]; nucFrac[C + Cs] = nucFrac[C + Gs]; nucFrac[2 * C + Cs] = nucFrac[2 * C + Gs];
+    }
+}
+EXPORT void orc_aging_nucleate_fresh_atp(i32 K, i32 C, const i32* rankOffsets, const i32* freeList,
+                                         const i32* freeOffsets, float* nucFrac) {
+    int nFree = freeOffsets[C];
+    for (int r = 0; r < K; r++) {
+        int slot = alloc_slot(r, rankOffsets, freeList, nFree);
+        if (slot < 0) continue;
+        nucFrac[slot] = 1.0f; nucFrac[C + slot] = 0.f; nucFrac[2 * C + slot] = 0.f;
+    }
+}
+
+// FilIDSystem.init (:38-47) and one pointer-doubling round, jump (:51-58)
+EXPORT void orc_filid_init(i32 n, const i32* filState, const i32* e2s, i32* ptr) {
+    for (int seg = 0; seg < n; seg++) {
+        if (filState[seg] < 0) { ptr[seg] = -seg - 2; continue; }
+        int nx = e2s[seg];
+        ptr[seg] = (nx >= 0 && nx != seg && filState[nx] >= 0) ? nx : seg;
+    }
+}
+EXPORT void orc_filid_jump(i32 n, const i32* ptrIn, i32* ptrOut, const i32* filState) {
+    for (int seg = 0; seg < n; seg++) {
+        if (filState[seg] < 0) { ptrOut[seg] = ptrIn[seg]; continue; }
+        ptrOut[seg] = ptrIn[ptrIn[seg]];
+    }
+}
+
+// ActinPool (ActinPool.java:27-63) as the 32-byte record {conc, uMPerMonomer, totalTaken,
+// totalReturned}; put (:49-52) / take (:42-46) of a scan total; GrowthStore.depletePoolForGrows
+// (GrowthStore.java:94-99) takes only a positive count.
+struct OrcPool { double conc; double uM; int64_t taken; int64_t returned; };
+EXPORT void orc_pool_put_total(void* poolp, const i32* offsets, i32 n) {
+    OrcPool* p = (OrcPool*)poolp;
+    int m = offsets[n];
+    p->conc += m * p->uM;
+    p->returned += m;
+}
+EXPORT void orc_pool_take_total(void* poolp, const i32* offsets, i32 n) {
+    OrcPool* p = (OrcPool*)poolp;
+    int m = offsets[n];
+    if (m <= 0) return;
+    p->conc -= m * p->uM;
+    if (p->conc < 0.0) p->conc = 0.0;
+    p->taken += m;
+}
+// the host prologue of the turnover block (FullSystemDemoHarness.java:648-651): setCounts,
+// setFires and GrowthStore.refreshRate (GrowthStore.java:84-88)
+EXPORT void orc_turnover_begin(i32 step, i32 seed, i32 fires, double onRate, double bdt, const void* poolp,
+                               float* growParams, i32* gc, i32* dc, i32* ac, i32* sc) {
+    const OrcPool* p = (const OrcPool*)poolp;
+    if (gc) { gc[1] = step; gc[2] = seed; gc[3] = fires; }
+    if (dc) { dc[1] = step; dc[2] = seed; dc[3] = fires; }
+    if (ac) ac[1] = fires;
+    if (sc) sc[1] = fires;
+    if (growParams) {
+        double P = fires ? onRate * p->conc * bdt : 0.0;
+        growParams[0] = (float)P;
+    }
+}

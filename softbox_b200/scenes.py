@@ -803,3 +803,74 @@ def xlink_bundle(n_fil=200, box=(0.7, 0.7, 0.3), dt=1.0e-4, seed=7, pos_sigma=0.
     g = max(2.0, max_c * 4.0 + cell + 0.5)
     grid = {"half": g, "cell": cell, "grab": XL_GRAB_DIST, "radius": ACTIN_RADIUS}
     return {"fil": f, "xl": xl, "filID": np.arange(n, dtype=I32), "grid": grid, "reqCap": req_cap, "C": C}
+
+
+# ---------------------------------------------------------------- turnover scene
+def turnover_chains(n_chains=200, cap=2048, seg_range=(1, 8), seed=5, cfg=None, tip_mono=(30, 64),
+                    body_mono=(2, 40), cofilin_high=0.0):
+    """Formin-pinned actin chains for the turnover path, in the harness's chain convention
+    (FullSystemDemoHarness.placeRandomChain, :580-606): segment 0 of chain k is the barbed
+    tip (seedNode = k, end2 free), segment i's end1 glues to segment i+1's end2, the last
+    segment is the pointed tip (end1 free). Chains take random slots of a store of capacity
+    `cap`; the other slots are FREE (state -1, zero Brownian scale, monomerCount 0).
+
+    Random, seeded: chain lengths in seg_range, tip monomer counts in tip_mono (64 = at the
+    split threshold), other segments in body_mono (below actinSeed = 3 they die at their
+    first cadence as a pointed tip), nucleotide compositions summing to 1, cofilin fractions
+    up to f_ADP (raised by `cofilin_high` on a tenth of the segments, so that dissolves fire)."""
+    from .turnover import TurnoverConfig, turnover_arrays
+    cfg = cfg or TurnoverConfig()
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(seg_range[0], seg_range[1] + 1, n_chains)
+    n_used = int(lens.sum())
+    if n_used > cap:
+        raise ValueError(f"{n_used} segments do not fit capacity {cap}")
+    f = filament_store(cap)
+    b = f["body"]
+    slots = rng.permutation(cap)[:n_used].astype(I32)
+    seedNode = np.full(cap, -1, I32)
+    mono = np.zeros(cap, I32)
+    f["filState"][:] = -1
+    pos = 0
+    for k in range(n_chains):
+        sl = slots[pos:pos + lens[k]]
+        pos += lens[k]
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        p = np.cross(d, [0.0, 0.0, 1.0] if abs(d[2]) < 0.9 else [1.0, 0.0, 0.0])
+        p /= np.linalg.norm(p)
+        e = rng.uniform(-2.0, 2.0, 3)
+        for i, s in enumerate(sl):
+            m = int(rng.integers(tip_mono[0], tip_mono[1] + 1)) if i == 0 else int(
+                rng.integers(body_mono[0], body_mono[1] + 1))
+            mono[s] = m
+            L = (m + 1) * ACTIN_MONO_RADIUS
+            c = e + 0.5 * L * d
+            set_vec(b["coord"], cap, s, *c)
+            set_vec(b["uVec"], cap, s, *d)
+            set_vec(b["yVec"], cap, s, *p)
+            e = e + L * d
+            f["filState"][s] = 0
+            b["brownTransScale"][s] = F32(BTRANS_COEFF)
+            b["brownRotScale"][s] = F32(BROT_COEFF if i in (0, lens[k] - 1) else 0.0)
+            if i == 0:
+                seedNode[s] = k
+            if i > 0:
+                f["end2NbrSlot"][s], f["end2NbrSide"][s] = sl[i - 1], 0
+            if i < lens[k] - 1:
+                f["end1NbrSlot"][s], f["end1NbrSide"][s] = sl[i + 1], 1
+    f["monomerCount"][:] = mono
+    free = f["filState"] < 0
+    drag_run_filament(f, 0.1)
+    b["segLength"][free] = F32(0)
+    derive_host(b)
+    a = rng.uniform(0.0, 1.0, cap).astype(F32)
+    bb = (rng.uniform(0.0, 1.0, cap).astype(F32) * (F32(1) - a)).astype(F32)
+    nuc = np.concatenate([a, bb, (F32(1) - a - bb).astype(F32)]).astype(F32)
+    adp = nuc[2 * cap:]
+    cof = (rng.uniform(0.0, 1.0, cap).astype(F32) * adp).astype(F32)
+    if cofilin_high > 0:
+        hi = rng.random(cap) < 0.1
+        cof[hi] = np.minimum(F32(1), cof[hi] + F32(cofilin_high)).astype(F32)
+    t = turnover_arrays(cap, cfg, seedNode=seedNode, nucFrac=nuc, cofFrac=cof)
+    return {"fil": f, "t": t, "cfg": cfg, "C": cap, "n_chains": n_chains}

@@ -378,6 +378,143 @@ class FormationGrid:                         # FormationGrid.java:28-109
                                        self.candCountSeg, reqFilA, reqFilB, formParams)
 
 
+def _alloc_ck(allocCounts, rankOffsets, freeOffsets, K):
+    """(C, K) of an allocator-companion call: allocCounts [0]=C [1]=K when given (host ints),
+    else C from freeOffsets (C+1 entries) and K from rankOffsets (reqCap+1 entries)."""
+    if allocCounts is not None:
+        return int(allocCounts[0]), int(allocCounts[1])
+    return freeOffsets.numel() - 1, (rankOffsets.numel() - 1 if K is None else K)
+
+
+class GrowthSystem:                          # GrowthSystem.java:73-228
+    @staticmethod
+    def grow(seedNode, monomerCount, coord, uVec, grewFlag, growParams, growCounts):
+        _ctx()("sbx_growth_grow", seedNode.numel(), seedNode, monomerCount, coord, uVec, grewFlag, growParams,
+               growCounts)
+
+    @staticmethod
+    def markSplits(seedNode, monomerCount, coord, uVec, yVec, acceptFlag, reqCoord, reqUVec, reqYVec, splitParams,
+                   growCounts):
+        _ctx()("sbx_growth_mark_splits", seedNode.numel(), seedNode, monomerCount, coord, uVec, yVec, acceptFlag,
+               reqCoord, reqUVec, reqYVec, _n3(reqCoord), splitParams, growCounts)
+
+    @staticmethod
+    def splitWire(rankOffsets, freeList, freeOffsets, monomerCount, coord, uVec, end1NbrSlot, end1NbrSide,
+                  end2NbrSlot, end2NbrSide, seedNode, splitParams, allocCounts=None, K=None):
+        C, K = _alloc_ck(allocCounts, rankOffsets, freeOffsets, K)
+        _ctx()("sbx_growth_split_wire", K, C, rankOffsets, freeList, freeOffsets, monomerCount, coord, uVec,
+               end1NbrSlot, end1NbrSide, end2NbrSlot, end2NbrSide, seedNode, splitParams)
+
+    @staticmethod
+    def recomputeDrag(monomerCount, segLength, end1NbrSlot, end2NbrSlot, bTransGam, bRotGam, bTransDiff, bRotDiff,
+                      dragParams, growCounts):
+        _ctx()("sbx_growth_recompute_drag", monomerCount.numel(), monomerCount, segLength, end1NbrSlot, end2NbrSlot,
+               bTransGam, bRotGam, bTransDiff, bRotDiff, dragParams, growCounts)
+
+
+class DepolySystem:                          # DepolySystem.java:70-188
+    @staticmethod
+    def depoly(filState, monomerCount, coord, uVec, end1NbrSlot, returnedMon, deathFlag, depolyParams, depolyCounts):
+        _ctx()("sbx_depoly", filState.numel(), filState, monomerCount, coord, uVec, end1NbrSlot, returnedMon,
+               deathFlag, depolyParams, depolyCounts)
+
+    @staticmethod
+    def depolyProxy(filState, monomerCount, coord, uVec, end1NbrSlot, nucFrac, returnedMon, deathFlag, depolyParams,
+                    depolyRateParams, depolyCounts):
+        _ctx()("sbx_depoly_proxy", filState.numel(), filState, monomerCount, coord, uVec, end1NbrSlot, nucFrac,
+               returnedMon, deathFlag, depolyParams, depolyRateParams, depolyCounts)
+
+    @staticmethod
+    def applyDeath(filState, monomerCount, seedNode, end1NbrSlot, end1NbrSide, end2NbrSlot, end2NbrSide,
+                   brownTransScale, brownRotScale, deathFlag, depolyCounts=None):
+        _ctx()("sbx_depoly_apply_death", filState.numel(), filState, monomerCount, seedNode, end1NbrSlot,
+               end1NbrSide, end2NbrSlot, end2NbrSide, brownTransScale, brownRotScale, deathFlag)
+
+
+class SeveringSystem:                        # SeveringSystem.java:37-98
+    @staticmethod
+    def cofilinAccumulate(filState, nucFrac, cofFrac, cofilinParams, severCounts):
+        _ctx()("sbx_sever_cofilin_accumulate", filState.numel(), filState, nucFrac, cofFrac, cofilinParams,
+               severCounts)
+
+    @staticmethod
+    def cofilinDissolve(filState, monomerCount, cofFrac, severDeathFlag, severReturnedMon, cofilinParams,
+                        severCounts):
+        _ctx()("sbx_sever_cofilin_dissolve", filState.numel(), filState, monomerCount, cofFrac, severDeathFlag,
+               severReturnedMon, cofilinParams, severCounts)
+
+    @staticmethod
+    def nucleateFreshCofilin(rankOffsets, freeList, freeOffsets, cofFrac, allocCounts=None, K=None):
+        C, K = _alloc_ck(allocCounts, rankOffsets, freeOffsets, K)
+        _ctx()("sbx_sever_nucleate_fresh_cofilin", K, C, rankOffsets, freeList, freeOffsets, cofFrac)
+
+
+class FilamentBirthSystem:                   # FilamentBirthSystem.java:41-87
+    @staticmethod
+    def freeFlags(filState, freeCount, allocCounts=None):
+        _ctx()("sbx_xlink_free_flags", freeCount.numel(), filState, freeCount)
+
+    @staticmethod
+    def freeScatter(filState, freeOffsets, freeList, allocCounts=None):
+        _ctx()("sbx_xlink_free_scatter", freeList.numel(), filState, freeOffsets, freeList)
+
+    @staticmethod
+    def allocate(reqCoord, reqUVec, reqYVec, rankOffsets, freeList, freeOffsets, coord, uVec, yVec, brownTransScale,
+                 brownRotScale, filState, birthParams, allocCounts=None, K=None):
+        C, K = _alloc_ck(allocCounts, rankOffsets, freeOffsets, K)
+        _ctx()("sbx_birth_allocate", K, C, _n3(reqCoord), reqCoord, reqUVec, reqYVec, rankOffsets, freeList,
+               freeOffsets, coord, uVec, yVec, brownTransScale, brownRotScale, filState, birthParams)
+
+
+class AgingSystem:                           # AgingSystem.java:40-125
+    @staticmethod
+    def age(filState, nucFrac, agingParams, agingCounts):
+        _ctx()("sbx_aging_age", filState.numel(), filState, nucFrac, agingParams, agingCounts)
+
+    @staticmethod
+    def growthAtp(grewFlag, monomerCount, nucFrac):
+        _ctx()("sbx_aging_growth_atp", grewFlag.numel(), grewFlag, monomerCount, nucFrac)
+
+    @staticmethod
+    def splitInheritNuc(rankOffsets, freeList, freeOffsets, nucFrac, allocCounts=None, K=None):
+        C, K = _alloc_ck(allocCounts, rankOffsets, freeOffsets, K)
+        _ctx()("sbx_aging_split_inherit_nuc", K, C, rankOffsets, freeList, freeOffsets, nucFrac)
+
+    @staticmethod
+    def nucleateFreshAtp(rankOffsets, freeList, freeOffsets, nucFrac, allocCounts=None, K=None):
+        C, K = _alloc_ck(allocCounts, rankOffsets, freeOffsets, K)
+        _ctx()("sbx_aging_nucleate_fresh_atp", K, C, rankOffsets, freeList, freeOffsets, nucFrac)
+
+
+class FilIDSystem:                           # FilIDSystem.java:30-58
+    @staticmethod
+    def rounds(n):
+        """ceil(log2 n), rounded up to even so the answer lands back in the first buffer."""
+        k = 1 if n <= 1 else (n - 1).bit_length()
+        return k if k % 2 == 0 else k + 1
+
+    @staticmethod
+    def init(filState, end2NbrSlot, ptr, counts=None):
+        n = ptr.numel() if counts is None else int(counts[0])
+        _ctx()("sbx_filid_init", n, filState, end2NbrSlot, ptr)
+
+    @staticmethod
+    def jump(ptrIn, ptrOut, filState, counts=None):
+        n = ptrIn.numel() if counts is None else int(counts[0])
+        _ctx()("sbx_filid_jump", n, ptrIn, ptrOut, filState)
+
+    @staticmethod
+    def compute(filState, end2NbrSlot, ptrA, ptrB):
+        """init + rounds(n) jumps ping-ponging A -> B -> A; the result is in ptrA: each active
+        segment's chain terminal (its filament id), FREE slots -s-2."""
+        n = ptrA.numel()
+        FilIDSystem.init(filState, end2NbrSlot, ptrA)
+        for r in range(FilIDSystem.rounds(n)):
+            src, dst = (ptrA, ptrB) if r % 2 == 0 else (ptrB, ptrA)
+            FilIDSystem.jump(src, dst, filState)
+        return ptrA
+
+
 class MotorJointSystem:                      # MotorJointSystem.java:72
     @staticmethod
     def joints(coord, uVec, segLength, bTransGam, bRotGam, forceSum, torqueSum, nucleotideState, jointParams,

@@ -127,3 +127,154 @@ def oracle_formation(orc, sc, step, use_grid=True):
     orc.xl_place_orient(K, xl["reqOrient"], xl["rankOffsets"], xl["freeList"], xl["freeOffsets"], C,
                         xl["linkOrientSame"], xl["torqueMagHist"], xl["torqueMagPlace"])
     return sc
+
+
+def oracle_turnover_allocate(orc, sc, accept, req_coord, req_u, req_y, rank_offsets, K=None):
+    """FullSystemDemoHarness.allocCpu (:950-957) on host arrays."""
+    f, t, C = sc["fil"], sc["t"], sc["C"]
+    b = f["body"]
+    K = C if K is None else K
+    orc.xl_free_flags(C, f["filState"], t["freeCount"])
+    orc.csr_scan(C, t["freeCount"], t["freeOffsets"])
+    orc.xl_free_scatter(C, f["filState"], t["freeOffsets"], t["freeList"])
+    orc.csr_scan(K, accept, rank_offsets)
+    orc.birth_allocate(K, C, req_coord.size // 3, req_coord, req_u, req_y, rank_offsets, t["freeList"],
+                       t["freeOffsets"], b["coord"], b["uVec"], b["yVec"], b["brownTransScale"], b["brownRotScale"],
+                       f["filState"], t["birthParams"])
+
+
+def oracle_turnover_cadence(orc, sc, step):
+    """The turnover block of FullSystemDemoHarness.cpuStep (:648-683) on host arrays; returns
+    False off-cadence (every kernel of the block is then a no-op)."""
+    cfg = sc["cfg"]
+    if not cfg.fires_at(step):
+        return False
+    from softbox_b200.turnover import BIOCHEM_DT
+    f, t, C = sc["fil"], sc["t"], sc["C"]
+    b = f["body"]
+    orc.turnover_begin(step, cfg.seed, 1, float(cfg.on_rate), float(BIOCHEM_DT), t["pool"], t["growParams"],
+                       t["growCounts"], t["depolyCounts"], t["agingCounts"], t["severCounts"])
+
+    def death(flag):
+        orc.apply_death(C, f["filState"], f["monomerCount"], t["seedNode"], f["end1NbrSlot"], f["end1NbrSide"],
+                        f["end2NbrSlot"], f["end2NbrSide"], b["brownTransScale"], b["brownRotScale"], flag)
+
+    orc.aging_age(C, f["filState"], t["nucFrac"], t["agingParams"], t["agingCounts"])
+    orc.depoly_proxy(C, f["filState"], f["monomerCount"], b["coord"], b["uVec"], f["end1NbrSlot"], t["nucFrac"],
+                     t["returnedMon"], t["deathFlag"], t["depolyParams"], t["depolyRateParams"], t["depolyCounts"])
+    orc.csr_scan(C, t["returnedMon"], t["returnedOffsets"])
+    death(t["deathFlag"])
+    orc.pool_put_total(t["pool"], t["returnedOffsets"], C)
+    for _ in range(max(1, cfg.polyboost)):
+        orc.growth_grow(C, t["seedNode"], f["monomerCount"], b["coord"], b["uVec"], t["grewFlag"], t["growParams"],
+                        t["growCounts"])
+        orc.csr_scan(C, t["grewFlag"], t["grewOffsets"])
+        orc.aging_growth_atp(C, t["grewFlag"], f["monomerCount"], t["nucFrac"])
+        orc.pool_take_total(t["pool"], t["grewOffsets"], C)
+    orc.cofilin_accumulate(C, f["filState"], t["nucFrac"], t["cofFrac"], t["cofilinParams"], t["severCounts"])
+    orc.cofilin_dissolve(C, f["filState"], f["monomerCount"], t["cofFrac"], t["severDeathFlag"],
+                         t["severReturnedMon"], t["cofilinParams"], t["severCounts"])
+    orc.csr_scan(C, t["severReturnedMon"], t["severReturnedOffsets"])
+    death(t["severDeathFlag"])
+    orc.pool_put_total(t["pool"], t["severReturnedOffsets"], C)
+    orc.growth_mark_splits(C, t["seedNode"], f["monomerCount"], b["coord"], b["uVec"], b["yVec"], t["acceptFlag"],
+                           t["reqCoord"], t["reqUVec"], t["reqYVec"], C, t["splitParams"], t["growCounts"])
+    oracle_turnover_allocate(orc, sc, t["acceptFlag"], t["reqCoord"], t["reqUVec"], t["reqYVec"], t["rankOffsets"])
+    orc.growth_split_wire(C, C, t["rankOffsets"], t["freeList"], t["freeOffsets"], f["monomerCount"], b["coord"],
+                          b["uVec"], f["end1NbrSlot"], f["end1NbrSide"], f["end2NbrSlot"], f["end2NbrSide"],
+                          t["seedNode"], t["splitParams"])
+    orc.aging_split_inherit_nuc(C, C, t["rankOffsets"], t["freeList"], t["freeOffsets"], t["nucFrac"])
+    orc.nucleate_fresh_cofilin(C, C, t["rankOffsets"], t["freeList"], t["freeOffsets"], t["cofFrac"])
+    orc.growth_recompute_drag(C, f["monomerCount"], b["segLength"], f["end1NbrSlot"], f["end2NbrSlot"],
+                              b["bTransGam"], b["bRotGam"], b["bTransDiff"], b["bRotDiff"], t["dragParams"],
+                              t["growCounts"])
+    return True
+
+
+def oracle_filament_ids(orc, sc):
+    """FilIDSystem init + rounds(C) ping-pong jumps; the ids end in t['filID']."""
+    from softbox_b200.systems import FilIDSystem
+    f, t, C = sc["fil"], sc["t"], sc["C"]
+    orc.filid_init(C, f["filState"], f["end2NbrSlot"], t["filID"])
+    for r in range(FilIDSystem.rounds(C)):
+        src, dst = (t["filID"], t["filIDTmp"]) if r % 2 == 0 else (t["filIDTmp"], t["filID"])
+        orc.filid_jump(C, src, dst, f["filState"])
+    return t["filID"]
+
+
+def chain_walk_ids(sc):
+    """Filament ids by walking end2 links to the chain terminal (the host chain walk that
+    FilIDSystem replaces): an independent check of the pointer doubling."""
+    f = sc["fil"]
+    st, e2 = f["filState"], f["end2NbrSlot"]
+    out = np.empty(st.size, np.int32)
+    for s in range(st.size):
+        if st[s] < 0:
+            out[s] = -s - 2
+            continue
+        cur, seen = s, 0
+        while True:
+            nx = e2[cur]
+            if nx < 0 or nx == cur or st[nx] < 0:
+                break
+            cur = nx
+            seen += 1
+            assert seen <= st.size, "cycle in the end2 links"
+        out[s] = cur
+    return out
+
+
+def turnover_store(C, cfg, seed_conc=None):
+    """A turnover scene of capacity C with every slot FREE (the harnesses' small stores)."""
+    from softbox_b200 import scenes
+    from softbox_b200.turnover import pool_array, turnover_arrays
+    f = scenes.filament_store(C)
+    f["filState"][:] = -1
+    t = turnover_arrays(C, cfg)
+    if seed_conc is not None:
+        t["pool"][:] = pool_array(seed_conc, cfg.box_vol_um3)
+    return {"fil": f, "t": t, "cfg": cfg, "C": C}
+
+
+def set_segment(sc, s, mono, x=0.0, u=(-1.0, 0.0, 0.0), seed_node=-1):
+    """Slot s ACTIVE with `mono` monomers at (x, 0, 0) along u, y = +y; drag from the length."""
+    from softbox_b200 import scenes
+    f, C = sc["fil"], sc["C"]
+    b = f["body"]
+    f["filState"][s] = 0
+    f["monomerCount"][s] = mono
+    scenes.set_vec(b["coord"], C, s, x, 0.0, 0.0)
+    scenes.set_vec(b["uVec"], C, s, *u)
+    scenes.set_vec(b["yVec"], C, s, 0.0, 1.0, 0.0)
+    b["brownTransScale"][s] = np.float32(1.0)
+    sc["t"]["seedNode"][s] = seed_node
+    b["segLength"][s] = np.float32((mono + 1) * scenes.ACTIN_MONO_RADIUS)
+
+
+def link(sc, a, a_end, b, b_end):
+    """Glue end a_end (1 or 2) of slot a to end b_end of slot b, both directions."""
+    f = sc["fil"]
+    f[f"end{a_end}NbrSlot"][a], f[f"end{a_end}NbrSide"][a] = b, b_end - 1
+    f[f"end{b_end}NbrSlot"][b], f[f"end{b_end}NbrSide"][b] = a, a_end - 1
+
+
+def oracle_growth_cadence(orc, sc, step):
+    """The growth-only cadence of GrowthHarness (grow -> grew scan -> markSplits -> split
+    allocation -> splitWire -> recomputeDrag) on host arrays."""
+    from softbox_b200.turnover import BIOCHEM_DT
+    f, t, C, cfg = sc["fil"], sc["t"], sc["C"], sc["cfg"]
+    b = f["body"]
+    orc.turnover_begin(step, cfg.seed, 1, float(cfg.on_rate), float(BIOCHEM_DT), t["pool"], t["growParams"],
+                       t["growCounts"], t["depolyCounts"], t["agingCounts"], t["severCounts"])
+    orc.growth_grow(C, t["seedNode"], f["monomerCount"], b["coord"], b["uVec"], t["grewFlag"], t["growParams"],
+                    t["growCounts"])
+    orc.csr_scan(C, t["grewFlag"], t["grewOffsets"])
+    orc.growth_mark_splits(C, t["seedNode"], f["monomerCount"], b["coord"], b["uVec"], b["yVec"], t["acceptFlag"],
+                           t["reqCoord"], t["reqUVec"], t["reqYVec"], C, t["splitParams"], t["growCounts"])
+    oracle_turnover_allocate(orc, sc, t["acceptFlag"], t["reqCoord"], t["reqUVec"], t["reqYVec"], t["rankOffsets"])
+    orc.growth_split_wire(C, C, t["rankOffsets"], t["freeList"], t["freeOffsets"], f["monomerCount"], b["coord"],
+                          b["uVec"], f["end1NbrSlot"], f["end1NbrSide"], f["end2NbrSlot"], f["end2NbrSide"],
+                          t["seedNode"], t["splitParams"])
+    orc.growth_recompute_drag(C, f["monomerCount"], b["segLength"], f["end1NbrSlot"], f["end2NbrSlot"],
+                              b["bTransGam"], b["bRotGam"], b["bTransDiff"], b["bRotDiff"], t["dragParams"],
+                              t["growCounts"])
