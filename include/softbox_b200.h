@@ -438,6 +438,29 @@ sbx_status sbx_turnover_begin(sbx_ctx* ctx, int32_t step, int32_t seed, int32_t 
                               double biochemDeltaT, const sbx_actin_pool* pool, float* growParams,
                               int32_t* growCounts, int32_t* depolyCounts, int32_t* agingCounts,
                               int32_t* severCounts);
+/* Network turnover (no reference counterpart: the reference's full demo leaves links and
+ * heads attached to a dead slot): after applyDeath, every ACTIVE crosslink with an end on a
+ * FREE segment becomes FREE and every head bound to a FREE segment unbinds. */
+sbx_status sbx_turnover_release_dead(sbx_ctx* ctx, const int32_t* filState, int32_t nLinks, const int32_t* linkFilA,
+                                     const int32_t* linkFilB, int32_t* linkState, int32_t nMotors, int32_t* boundSeg);
+/* Birth holding the polymer mass constant (no reference counterpart; the request layout is
+ * FilamentStore's): K = (totalReturned - totalTaken) / birthBox[3] seeds are requested,
+ * request r < K at a wang-hash uniform position in the box of half-widths birthBox[0..2]
+ * with a uniform in-plane axis (salts "BIR1".."BIR4"); acceptFlag[r] = r < K over reqCap. */
+sbx_status sbx_birth_emit_constant_actin(sbx_ctx* ctx, int32_t reqCap, const sbx_actin_pool* pool,
+                                         const float* birthBox, int32_t step, int32_t seed, int32_t* acceptFlag,
+                                         float* reqCoord, float* reqUVec, float* reqYVec);
+/* NodeNucleationSystem.initNewborn (NodeNucleationSystem.java:228-244): monomerCount =
+ * seedParams[0], segLength = seedParams[1] in each claimed slot */
+sbx_status sbx_birth_init_newborn(sbx_ctx* ctx, int32_t K, int32_t C, const int32_t* rankOffsets,
+                                  const int32_t* freeList, const int32_t* freeOffsets, int32_t* monomerCount,
+                                  float* segLength, const float* seedParams);
+/* NodeNucleationSystem.tagSeeds (:95-106): seedNode[slot] = request index (a growing tip) */
+sbx_status sbx_birth_tag_seeds(sbx_ctx* ctx, int32_t K, int32_t C, const int32_t* rankOffsets,
+                               const int32_t* freeList, const int32_t* freeOffsets, int32_t* seedNode);
+/* pool.take(min(rankOffsets[K], freeOffsets[C]) * monomersPerBirth) (FullSystemDemoHarness.java:689-691) */
+sbx_status sbx_actin_pool_take_births(sbx_ctx* ctx, sbx_actin_pool* pool, const int32_t* rankOffsets, int32_t K,
+                                      const int32_t* freeOffsets, int32_t C, int32_t monomersPerBirth);
 /* FilIDSystem.init (FilIDSystem.java:38-47): ptr = end2 neighbour (self at a chain end, -s-2 when FREE) */
 sbx_status sbx_filid_init(sbx_ctx* ctx, int32_t n, const int32_t* filState, const int32_t* end2NbrSlot,
                           int32_t* ptr);

@@ -2621,3 +2621,65 @@ EXPORT void orc_turnover_begin(i32 step, i32 seed, i32 fires, double onRate, dou
         growParams[0] = (float)P;
     }
 }
+
+// network turnover companions (same rules as the library's entry points of these names)
+EXPORT void orc_turnover_release_dead(const i32* filState, i32 nLinks, const i32* linkFilA, const i32* linkFilB,
+                                      i32* linkState, i32 nMotors, i32* boundSeg) {
+    for (int i = 0; i < nLinks; i++) {
+        if (linkState[i] < 0) continue;
+        int a = linkFilA[i], b = linkFilB[i];
+        if ((a >= 0 && filState[a] < 0) || (b >= 0 && filState[b] < 0)) linkState[i] = -1;
+    }
+    for (int m = 0; m < nMotors; m++) {
+        int sg = boundSeg[m];
+        if (sg >= 0 && filState[sg] < 0) boundSeg[m] = -1;
+    }
+}
+EXPORT void orc_birth_emit_constant_actin(i32 reqCap, const void* poolp, const float* bp, i32 step, i32 seed,
+                                          i32* accept, float* reqCoord, float* reqUVec, float* reqYVec) {
+    const OrcPool* p = (const OrcPool*)poolp;
+    long long deficit = p->returned - p->taken;
+    int seedMon = jf2i(bp[3]);
+    long long K = (deficit > 0 && seedMon > 0) ? deficit / seedMon : 0;
+    for (int r = 0; r < reqCap; r++) {
+        if (r >= K) { accept[r] = 0; continue; }
+        accept[r] = 1;
+        float ux = turnover_unit(r, step, seed, 0x42495231u), uy = turnover_unit(r, step, seed, 0x42495232u);
+        float uz = turnover_unit(r, step, seed, 0x42495233u), ua = turnover_unit(r, step, seed, 0x42495234u);
+        reqCoord[r] = (float)((2.0 * ux - 1.0) * bp[0]);
+        reqCoord[reqCap + r] = (float)((2.0 * uy - 1.0) * bp[1]);
+        reqCoord[2 * reqCap + r] = (float)((2.0 * uz - 1.0) * bp[2]);
+        double th = 2.0 * PI_D * ua, c = JCOS(th), sn = JSIN(th);
+        reqUVec[r] = (float)c; reqUVec[reqCap + r] = (float)sn; reqUVec[2 * reqCap + r] = 0.f;
+        reqYVec[r] = (float)(-sn); reqYVec[reqCap + r] = (float)c; reqYVec[2 * reqCap + r] = 0.f;
+    }
+}
+// NodeNucleationSystem.initNewborn (NodeNucleationSystem.java:228-244), tagSeeds (:95-106)
+EXPORT void orc_birth_init_newborn(i32 K, i32 C, const i32* rankOffsets, const i32* freeList, const i32* freeOffsets,
+                                   i32* monomerCount, float* segLength, const float* seedParams) {
+    int nFree = freeOffsets[C];
+    for (int r = 0; r < K; r++) {
+        int slot = alloc_slot(r, rankOffsets, freeList, nFree);
+        if (slot < 0) continue;
+        monomerCount[slot] = jf2i(seedParams[0]);
+        segLength[slot] = seedParams[1];
+    }
+}
+EXPORT void orc_birth_tag_seeds(i32 K, i32 C, const i32* rankOffsets, const i32* freeList, const i32* freeOffsets,
+                                i32* seedNode) {
+    int nFree = freeOffsets[C];
+    for (int r = 0; r < K; r++) {
+        int slot = alloc_slot(r, rankOffsets, freeList, nFree);
+        if (slot >= 0) seedNode[slot] = r;
+    }
+}
+EXPORT void orc_pool_take_births(void* poolp, const i32* rankOffsets, i32 K, const i32* freeOffsets, i32 C,
+                                 i32 seedMon) {
+    OrcPool* p = (OrcPool*)poolp;
+    int nb = std::min(rankOffsets[K], freeOffsets[C]);
+    if (nb <= 0) return;
+    int m = nb * seedMon;
+    p->conc -= m * p->uM;
+    if (p->conc < 0.0) p->conc = 0.0;
+    p->taken += m;
+}

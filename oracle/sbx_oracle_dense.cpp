@@ -129,7 +129,7 @@ EXPORT void orc_dense_step(const sbx_dense_scene* sc, i32 t) {
     // ---- (i) binding ----
     orc_mot_publish_head(nM, b.coord, b.uVec, b.segLength, mot.head, mot.uVec, mot.rodUVec);
     orc_fil_publish(nSeg, fb.coord, fb.segLength, g.cap, g.center, g.boundingRadius, g.ownerStore,
-                    g.ownerSlot, g.viewParams, nullptr);
+                    g.ownerSlot, g.viewParams, f.filState);
     orc_mot_publish(nM, mot.head, mot.reach, g.cap, g.center, g.boundingRadius, g.ownerStore, g.ownerSlot,
                     mot.publishParams[0]);
     orc_body_cell(g.cap, g.center, g.gridParams, g.gridDims, g.gridCounts[1], g.bodyCell);

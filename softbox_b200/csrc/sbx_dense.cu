@@ -60,7 +60,7 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
     // (i) binding
     CHK(sbx_motor_publish_head(ctx, nM, b.coord, b.uVec, b.segLength, mot.head, mot.uVec, mot.rodUVec));
     CHK(sbx_filament_publish(ctx, nSeg, fb.coord, fb.segLength, g.cap, g.center, g.boundingRadius, g.ownerStore,
-                             g.ownerSlot, g.viewParams, nullptr));
+                             g.ownerSlot, g.viewParams, f.filState));
     CHK(sbx_motor_publish(ctx, nM, mot.head, mot.reach, g.cap, g.center, g.boundingRadius, g.ownerStore, g.ownerSlot,
                           mot.publishParams));
     CHK(sbx_grid_body_cell(ctx, g.cap, g.center, g.gridParams, g.gridDims, g.gridCounts, g.bodyCell));
@@ -219,6 +219,12 @@ bool fused_prepare(sbx_dense_plan* p) {
     int per = fused_max_blocks_per_sm();
     if (!coop || per <= 0) return why("cooperative launch unavailable");
     p->fused_grid = sms * per;
+    // the fused kernel publishes every filament slot as live: no FREE slot may exist
+    if (sc.fil.filState) {
+        auto fs = d2h(sc.fil.filState, a.nSeg, st);
+        for (int i = 0; i < a.nSeg; i++)
+            if (fs[i] < 0) return why("FREE filament slots (turnover) need the per-system or graph path");
+    }
     // chain topology: filaments must be contiguous slot ranges. A rod group is a run of
     // whole filaments (a multiple of 4 segments, <= FUSED_MAX_ROD); the smallest group
     // size whose groups fit one wave of CTAs, else the largest valid one.

@@ -290,6 +290,64 @@ __global__ void k_filid_jump(int n, const int* ptrIn, int* ptrOut, const int* fi
     ptrOut[seg] = filState[seg] < 0 ? ptrIn[seg] : ptrIn[ptrIn[seg]];
 }
 
+// links and bound heads on FREE segments let go (the network-turnover rule of this library)
+__global__ void k_release_dead(const int* filState, int nLinks, const int* linkFilA, const int* linkFilB,
+                               int* linkState, int nMotors, int* boundSeg) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nLinks && linkState[i] >= 0) {
+        int a = linkFilA[i], b = linkFilB[i];
+        if ((a >= 0 && filState[a] < 0) || (b >= 0 && filState[b] < 0)) linkState[i] = -1;
+    }
+    if (i < nMotors) {
+        int sg = boundSeg[i];
+        if (sg >= 0 && filState[sg] < 0) boundSeg[i] = -1;
+    }
+}
+
+// birth requests that restore the polymer mass: deficit = returned - taken (ledger since the
+// pool was made) in whole seeds; request r < K gets a uniform position in the box and a
+// uniform in-plane axis. bp: [0..2] box half-widths, [3] monomers per seed
+__global__ void k_birth_emit(int reqCap, const sbx_actin_pool* pool, const float* bp, int step, int seed,
+                             int* accept, float* reqCoord, float* reqUVec, float* reqYVec) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= reqCap) return;
+    long long deficit = pool->totalReturned - pool->totalTaken;
+    int seedMon = (int)bp[3];
+    long long K = (deficit > 0 && seedMon > 0) ? deficit / seedMon : 0;
+    if (r >= K) { accept[r] = 0; return; }
+    accept[r] = 1;
+    float ux = unit_salted(r, step, seed, 0x42495231u), uy = unit_salted(r, step, seed, 0x42495232u);
+    float uz = unit_salted(r, step, seed, 0x42495233u), ua = unit_salted(r, step, seed, 0x42495234u);
+    reqCoord[r] = (float)((2.0 * ux - 1.0) * bp[0]);
+    reqCoord[reqCap + r] = (float)((2.0 * uy - 1.0) * bp[1]);
+    reqCoord[2 * reqCap + r] = (float)((2.0 * uz - 1.0) * bp[2]);
+    double th = 2.0 * PI_D * ua, c = sbxm::cos(th), sn = sbxm::sin(th);
+    reqUVec[r] = (float)c; reqUVec[reqCap + r] = (float)sn; reqUVec[2 * reqCap + r] = 0.f;
+    reqYVec[r] = (float)(-sn); reqYVec[reqCap + r] = (float)c; reqYVec[2 * reqCap + r] = 0.f;
+}
+
+// NodeNucleationSystem.initNewborn (NodeNucleationSystem.java:228-244) and tagSeeds (:95-106)
+__global__ void k_newborn(int K, int C, const int* rankOffsets, const int* freeList, const int* freeOffsets,
+                          int* monomerCount, float* segLength, int* seedNode, const float* sp) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= K) return;
+    int slot = formed_slot(r, rankOffsets, freeList, freeOffsets[C]);
+    if (slot < 0) return;
+    if (monomerCount) { monomerCount[slot] = (int)sp[0]; segLength[slot] = sp[1]; }
+    if (seedNode) seedNode[slot] = r;
+}
+
+// the births' monomers leave the pool: min(accepted, nFree) seeds (FullSystemDemoHarness.java:689-691)
+__global__ void k_pool_births(sbx_actin_pool* pool, const int* rankOffsets, int K, const int* freeOffsets, int C,
+                              int seedMon) {
+    int nb = min(rankOffsets[K], freeOffsets[C]);
+    if (nb <= 0) return;
+    int m = nb * seedMon;
+    double c = pool->conc - m * pool->uMPerMonomer;
+    pool->conc = c < 0.0 ? 0.0 : c;
+    pool->totalTaken += m;
+}
+
 // ActinPool.put (ActinPool.java:49-52) / take (:42-46) of a scan total, one thread
 __global__ void k_pool(sbx_actin_pool* pool, const int* offsets, int n, int take) {
     int m = offsets[n];
@@ -525,4 +583,54 @@ extern "C" sbx_status sbx_turnover_begin(sbx_ctx* ctx, int32_t step, int32_t see
     SBX_LAUNCH(ctx, k_turnover_begin, 1, 1, step, seed, fires, onRate, biochemDeltaT, pool, growParams, growCounts,
                depolyCounts, agingCounts, severCounts);
     SBX_DONE("sbx_turnover_begin");
+}
+
+extern "C" sbx_status sbx_turnover_release_dead(sbx_ctx* ctx, const int32_t* filState, int32_t nLinks,
+                                                const int32_t* linkFilA, const int32_t* linkFilB, int32_t* linkState,
+                                                int32_t nMotors, int32_t* boundSeg) {
+    SBX_REQUIRE(ctx && filState && nLinks >= 0 && nMotors >= 0 && (nLinks == 0 || (linkFilA && linkFilB && linkState)) &&
+                (nMotors == 0 || boundSeg));
+    int n = nLinks > nMotors ? nLinks : nMotors;
+    if (n == 0) return SBX_OK;
+    SBX_LAUNCH(ctx, k_release_dead, blocks(n), 256, filState, nLinks, linkFilA, linkFilB, linkState, nMotors, boundSeg);
+    SBX_DONE("sbx_turnover_release_dead");
+}
+
+extern "C" sbx_status sbx_birth_emit_constant_actin(sbx_ctx* ctx, int32_t reqCap, const sbx_actin_pool* pool,
+                                                    const float* birthBox, int32_t step, int32_t seed,
+                                                    int32_t* acceptFlag, float* reqCoord, float* reqUVec,
+                                                    float* reqYVec) {
+    SBX_REQUIRE(ctx && reqCap >= 0 && (reqCap == 0 || (pool && birthBox && acceptFlag && reqCoord && reqUVec && reqYVec)));
+    if (reqCap == 0) return SBX_OK;
+    SBX_LAUNCH(ctx, k_birth_emit, blocks(reqCap), 256, reqCap, pool, birthBox, step, seed, acceptFlag, reqCoord,
+               reqUVec, reqYVec);
+    SBX_DONE("sbx_birth_emit_constant_actin");
+}
+
+extern "C" sbx_status sbx_birth_init_newborn(sbx_ctx* ctx, int32_t K, int32_t C, const int32_t* rankOffsets,
+                                             const int32_t* freeList, const int32_t* freeOffsets,
+                                             int32_t* monomerCount, float* segLength, const float* seedParams) {
+    SBX_REQUIRE(ctx && K >= 0 && C >= 0 && rankOffsets && freeOffsets &&
+                (K == 0 || (freeList && monomerCount && segLength && seedParams)));
+    if (K == 0) return SBX_OK;
+    SBX_LAUNCH(ctx, k_newborn, blocks(K), 256, K, C, rankOffsets, freeList, freeOffsets, monomerCount, segLength,
+               nullptr, seedParams);
+    SBX_DONE("sbx_birth_init_newborn");
+}
+
+extern "C" sbx_status sbx_birth_tag_seeds(sbx_ctx* ctx, int32_t K, int32_t C, const int32_t* rankOffsets,
+                                          const int32_t* freeList, const int32_t* freeOffsets, int32_t* seedNode) {
+    SBX_REQUIRE(ctx && K >= 0 && C >= 0 && rankOffsets && freeOffsets && (K == 0 || (freeList && seedNode)));
+    if (K == 0) return SBX_OK;
+    SBX_LAUNCH(ctx, k_newborn, blocks(K), 256, K, C, rankOffsets, freeList, freeOffsets, nullptr, nullptr, seedNode,
+               nullptr);
+    SBX_DONE("sbx_birth_tag_seeds");
+}
+
+extern "C" sbx_status sbx_actin_pool_take_births(sbx_ctx* ctx, sbx_actin_pool* pool, const int32_t* rankOffsets,
+                                                 int32_t K, const int32_t* freeOffsets, int32_t C,
+                                                 int32_t monomersPerBirth) {
+    SBX_REQUIRE(ctx && pool && rankOffsets && freeOffsets && K >= 0 && C >= 0 && monomersPerBirth >= 0);
+    SBX_LAUNCH(ctx, k_pool_births, 1, 1, pool, rankOffsets, K, freeOffsets, C, monomersPerBirth);
+    SBX_DONE("sbx_actin_pool_take_births");
 }

@@ -19,7 +19,7 @@ class DenseNetwork:
     def __init__(self, host_scene, ctx=None, fp64_coords=False, device="cuda"):
         self.ctx = ctx or default_context()
         self.host = host_scene
-        self.dev = D.to_device({k: v for k, v in host_scene.items() if k != "cfg"}, device)
+        self.dev = D.to_device({k: v for k, v in host_scene.items() if k not in ("cfg", "tcfg")}, device)
         if fp64_coords:
             for path in (("fil", "body"), ("mot", "body"), ("mini", "backbone")):
                 D.add_coord64(self.dev[path[0]][path[1]])
@@ -75,6 +75,10 @@ class DenseNetwork:
             x = x[field]
         return D.to_host(x)
 
+    def pull_all(self):
+        """Every device array of the network, copied to host (UNDER_DEMAND for all stores)."""
+        return D.to_host(self.dev)
+
     def close(self):
         if self.plan:
             LIB.sbx_dense_plan_destroy(self.plan)
@@ -85,6 +89,37 @@ class DenseNetwork:
             self.close()
         except Exception:
             pass
+
+
+class TurnoverNetwork(DenseNetwork):
+    """A dense network with actin turnover (scenes.dense_turnover): at every biochem cadence
+    the turnover block (growth, depolymerisation, death, severing, splits), the release of
+    links and heads on dead slots, and constant-actin births run before that step's
+    mechanics, all on the library's stream with no host synchronisation. The mechanics run
+    on the graph or per-system path: the fused kernel assumes a static chain topology."""
+
+    def __init__(self, host_scene, ctx=None, fp64_coords=False, device="cuda"):
+        from .turnover import Turnover
+        super().__init__(host_scene, ctx=ctx, fp64_coords=fp64_coords, device=device)
+        d = self.dev
+        self.tcfg = host_scene["tcfg"]
+        xl = d["xl"]
+        self.turnover = Turnover(d["fil"], d["turnover"], self.tcfg,
+                                 links=(xl["linkFilA"], xl["linkFilB"], xl["linkState"]),
+                                 boundSeg=d["mot"]["boundSeg"])
+
+    def run(self, t0, nsteps, mode="graph"):
+        if mode not in ("graph", "unfused"):
+            raise ValueError("turnover runs on the graph or per-system path")
+        t, end = int(t0), int(t0) + int(nsteps)
+        ci = self.tcfg.check_int
+        while t < end:
+            if self.tcfg.fires_at(t):
+                self.turnover.cadence(t)
+                self.turnover.births(t)
+            nxt = min(end, (t // ci + 1) * ci)
+            super().run(t, nxt - t, mode)
+            t = nxt
 
 
 class FreeRods:

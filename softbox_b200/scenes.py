@@ -874,3 +874,49 @@ def turnover_chains(n_chains=200, cap=2048, seg_range=(1, 8), seed=5, cfg=None, 
         cof[hi] = np.minimum(F32(1), cof[hi] + F32(cofilin_high)).astype(F32)
     t = turnover_arrays(cap, cfg, seedNode=seedNode, nucFrac=nuc, cofFrac=cof)
     return {"fil": f, "t": t, "cfg": cfg, "C": cap, "n_chains": n_chains}
+
+
+def dense_turnover(cfg=None, growth_rate=10.0, sever_rate=0.01, cof_ratio=0.5, birth_cap=None, seed_mon=None,
+                   seed=0x7A11):
+    """The dense network with actin turnover on (the scale sweep's turnover workload):
+
+    * growth at every filament's barbed terminal (the end2-free segment, tagged as a
+      growing tip in seedNode) at `growth_rate` subunits/s: GrowthSystem's probability
+      k_on [actin] biochemDeltaT with the initial [actin] = growth_rate / k_on;
+    * severing at `sever_rate` per rod per second through the reference's cofilin rule: an
+      aged network (f_ADP = 1) whose cofilin fractions are spread so that -ln(1 - f_cof) is
+      uniform on [0, -ln(1 - ratio)), with p_cof chosen so that a rod takes 1/sever_rate
+      seconds from f_cof = 0 to the ratio: each rod dissolves once per 1/sever_rate s;
+    * pointed-end depolymerisation at the ADP off-rate (depolyProxy);
+    * constant-actin births: when depolymerisation and dissolves have returned more
+      monomers than growth took, newborn one-rod filaments of `seed_mon` monomers (default:
+      the network's rod size) appear at uniform positions in the slab, in dead slots.
+
+    Turnover semantics of a free-filament network are not the reference's (its growth is
+    node-bonded and it has no random birth), so this workload is specified here."""
+    from .turnover import (BIOCHEM_DT, K_ATP_ON2_WITH_FORMIN, TurnoverConfig, birth_arrays, turnover_arrays)
+    cfg = cfg or C1
+    sc = dense_contractile(cfg)
+    f = sc["fil"]
+    n = f["body"]["n"]
+    tcfg = TurnoverConfig(dt=cfg.dt, cof_ratio=cof_ratio, pool0_um=growth_rate / K_ATP_ON2_WITH_FORMIN,
+                          box_vol_um3=cfg.side * cfg.side * cfg.box_z, aeta=cfg.fil_aeta, born_trans=cfg.brown_trans,
+                          born_rot=BROT_COEFF)
+    seedNode = np.full(n, -1, I32)
+    tips = np.flatnonzero(f["end2NbrSlot"] < 0)
+    seedNode[tips] = np.arange(tips.size, dtype=I32)
+    nuc = np.zeros(3 * n, F32)
+    nuc[2 * n:] = 1.0
+    rng = np.random.default_rng(seed)
+    x_star = -math.log(1.0 - cof_ratio)
+    x0 = rng.uniform(0.0, x_star, n)
+    cof = (1.0 - np.exp(-x0)).astype(F32)
+    t = turnover_arrays(n, tcfg, seedNode=seedNode, nucFrac=nuc, cofFrac=cof)
+    cadences = (1.0 / sever_rate) / BIOCHEM_DT
+    t["cofilinParams"][0] = F32(-math.expm1(-x_star / cadences))
+    seed_mon = cfg.monomer_ct if seed_mon is None else seed_mon
+    birth_cap = birth_cap or max(64, n // 50)
+    birth_arrays(t, birth_cap, (0.5 * cfg.side, 0.5 * cfg.side, 0.5 * cfg.box_z), seed_mon)
+    sc["turnover"] = t
+    sc["tcfg"] = tcfg
+    return sc

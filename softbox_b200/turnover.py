@@ -147,14 +147,35 @@ def turnover_arrays(C, cfg, seedNode=None, nucFrac=None, cofFrac=None):
     return t
 
 
+def birth_arrays(t, req_cap, box_half, seed_mon):
+    """Adds the constant-actin birth requests to turnover arrays `t`: request buffers of
+    capacity req_cap, the birth box [hx, hy, hz, monomers per newborn] and the newborn's
+    [monomerCount, segLength] (NodeNucleationStore.seedParams)."""
+    t["birthAccept"] = np.zeros(req_cap, I32)
+    t["birthRankOffsets"] = np.zeros(req_cap + 1, I32)
+    for k in ("birthReqCoord", "birthReqUVec", "birthReqYVec"):
+        t[k] = np.zeros(3 * req_cap, F32)
+    t["birthBox"] = np.array([box_half[0], box_half[1], box_half[2], seed_mon], F32)
+    t["seedParams"] = np.array([seed_mon, (seed_mon + 1) * scenes.ACTIN_MONO_RADIUS], F32)
+    return t
+
+
 class Turnover:
     """Device turnover over a device filament store `fil` (dict of torch tensors as made by
     device.to_device from scenes.filament_store) and device turnover arrays `t` (from
-    turnover_arrays). All calls launch on the library's default context."""
+    turnover_arrays). All calls launch on the library's default context.
 
-    def __init__(self, fil, t, cfg):
+    In a network (`links` = (linkFilA, linkFilB, linkState) of a crosslinker store,
+    `boundSeg` of a motor store), every death is followed by sbx_turnover_release_dead, so
+    no link or head stays on a FREE slot, and one that a split or birth reuses later in the
+    same cadence starts unattached."""
+
+    def __init__(self, fil, t, cfg, links=None, boundSeg=None):
         self.f, self.t, self.cfg = fil, t, cfg
         self.C = int(fil["filState"].numel())
+        self.links, self.boundSeg = links, boundSeg
+        # monomers per newborn, read once here so that a cadence never reads device memory
+        self.seed_mon = int(np.asarray(t["birthBox"].cpu())[3]) if "birthBox" in t else 0
 
     def begin(self, step):
         from .systems import _ctx
@@ -169,10 +190,14 @@ class Turnover:
         _ctx()("sbx_csr_scan", self.C, counts, offsets)
 
     def _death(self, flag):
-        from .systems import DepolySystem
+        from .systems import DepolySystem, _ctx
         f, b, t = self.f, self.f["body"], self.t
         DepolySystem.applyDeath(f["filState"], f["monomerCount"], t["seedNode"], f["end1NbrSlot"], f["end1NbrSide"],
                                 f["end2NbrSlot"], f["end2NbrSide"], b["brownTransScale"], b["brownRotScale"], flag)
+        if self.links is not None or self.boundSeg is not None:
+            la, lb, ls = self.links if self.links is not None else (None, None, None)
+            _ctx()("sbx_turnover_release_dead", f["filState"], 0 if ls is None else ls.numel(), la, lb, ls,
+                   0 if self.boundSeg is None else self.boundSeg.numel(), self.boundSeg)
 
     def allocate(self, acceptFlag, reqCoord, reqUVec, reqYVec, rankOffsets, K=None):
         """FullSystemDemoHarness.allocCpu (:950-957): free list over filState, dense ranks of the
@@ -226,6 +251,29 @@ class Turnover:
         S.nucleateFreshCofilin(t["rankOffsets"], t["freeList"], t["freeOffsets"], t["cofFrac"], allocCounts=(C, C))
         G.recomputeDrag(f["monomerCount"], b["segLength"], f["end1NbrSlot"], f["end2NbrSlot"], b["bTransGam"],
                         b["bRotGam"], b["bTransDiff"], b["bRotDiff"], t["dragParams"], t["growCounts"])
+        return True
+
+    def births(self, step):
+        """Constant-actin births after the turnover block (in the place of the node nucleation
+        of FullSystemDemoHarness.cpuStep, :685-692): requests for the polymer deficit, the
+        allocator, initNewborn, tagSeeds (a newborn is a growing tip), fresh ATP and cofilin,
+        and the pool debit of the formed births."""
+        from .systems import AgingSystem as A, SeveringSystem as S, _ctx
+        if not self.cfg.fires_at(step) or "birthBox" not in self.t:
+            return False
+        f, t, C = self.f, self.t, self.C
+        K = t["birthAccept"].numel()
+        _ctx()("sbx_birth_emit_constant_actin", K, t["pool"], t["birthBox"], step, self.cfg.seed, t["birthAccept"],
+               t["birthReqCoord"], t["birthReqUVec"], t["birthReqYVec"])
+        self.allocate(t["birthAccept"], t["birthReqCoord"], t["birthReqUVec"], t["birthReqYVec"],
+                      t["birthRankOffsets"], K=K)
+        ro, fl, fo = t["birthRankOffsets"], t["freeList"], t["freeOffsets"]
+        _ctx()("sbx_birth_init_newborn", K, C, ro, fl, fo, f["monomerCount"], f["body"]["segLength"],
+               t["seedParams"])
+        _ctx()("sbx_birth_tag_seeds", K, C, ro, fl, fo, t["seedNode"])
+        A.nucleateFreshAtp(ro, fl, fo, t["nucFrac"], allocCounts=(C, K))
+        S.nucleateFreshCofilin(ro, fl, fo, t["cofFrac"], allocCounts=(C, K))
+        _ctx()("sbx_actin_pool_take_births", t["pool"], ro, K, fo, C, self.seed_mon)
         return True
 
     def filament_ids(self):

@@ -158,6 +158,9 @@ def oracle_turnover_cadence(orc, sc, step):
     def death(flag):
         orc.apply_death(C, f["filState"], f["monomerCount"], t["seedNode"], f["end1NbrSlot"], f["end1NbrSide"],
                         f["end2NbrSlot"], f["end2NbrSide"], b["brownTransScale"], b["brownRotScale"], flag)
+        if sc.get("release") is not None:
+            la, lb, ls, bs = sc["release"]
+            orc.turnover_release_dead(f["filState"], ls.size, la, lb, ls, bs.size, bs)
 
     orc.aging_age(C, f["filState"], t["nucFrac"], t["agingParams"], t["agingCounts"])
     orc.depoly_proxy(C, f["filState"], f["monomerCount"], b["coord"], b["uVec"], f["end1NbrSlot"], t["nucFrac"],
@@ -278,3 +281,46 @@ def oracle_growth_cadence(orc, sc, step):
     orc.growth_recompute_drag(C, f["monomerCount"], b["segLength"], f["end1NbrSlot"], f["end2NbrSlot"],
                               b["bTransGam"], b["bRotGam"], b["bTransDiff"], b["bRotDiff"], t["dragParams"],
                               t["growCounts"])
+
+
+def oracle_births(orc, sc, step):
+    """Turnover.births on host arrays."""
+    cfg = sc["cfg"]
+    t, f, C = sc["t"], sc["fil"], sc["C"]
+    if not cfg.fires_at(step) or "birthBox" not in t:
+        return False
+    K = t["birthAccept"].size
+    orc.birth_emit_constant_actin(K, t["pool"], t["birthBox"], step, cfg.seed, t["birthAccept"], t["birthReqCoord"],
+                                  t["birthReqUVec"], t["birthReqYVec"])
+    oracle_turnover_allocate(orc, sc, t["birthAccept"], t["birthReqCoord"], t["birthReqUVec"], t["birthReqYVec"],
+                             t["birthRankOffsets"], K=K)
+    ro, fl, fo = t["birthRankOffsets"], t["freeList"], t["freeOffsets"]
+    orc.birth_init_newborn(K, C, ro, fl, fo, f["monomerCount"], f["body"]["segLength"], t["seedParams"])
+    orc.birth_tag_seeds(K, C, ro, fl, fo, t["seedNode"])
+    orc.aging_nucleate_fresh_atp(K, C, ro, fl, fo, t["nucFrac"])
+    orc.nucleate_fresh_cofilin(K, C, ro, fl, fo, t["cofFrac"])
+    orc.pool_take_births(t["pool"], ro, K, fo, C, int(t["birthBox"][3]))
+    return True
+
+
+def turnover_view(sc):
+    """The turnover arrays of a dense turnover scene as the cadence helpers take them."""
+    xl, mot = sc["xl"], sc["mot"]
+    return {"fil": sc["fil"], "t": sc["turnover"], "C": sc["fil"]["body"]["n"], "cfg": sc["tcfg"],
+            "release": (xl["linkFilA"], xl["linkFilB"], xl["linkState"], mot["boundSeg"])}
+
+
+def oracle_turnover_network_run(orc, sc, t0, nsteps):
+    """TurnoverNetwork.run on host arrays: the turnover cadence and births at each biochem
+    cadence, then the dense steps up to the next one."""
+    view = turnover_view(sc)
+    cfg = sc["tcfg"]
+    t, end, ci = t0, t0 + nsteps, cfg.check_int
+    while t < end:
+        if cfg.fires_at(t):
+            oracle_turnover_cadence(orc, view, t)
+            oracle_births(orc, view, t)
+        nxt = min(end, (t // ci + 1) * ci)
+        oracle_dense_run(orc, sc, t, nxt - t)
+        t = nxt
+    return sc
