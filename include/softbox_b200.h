@@ -618,7 +618,57 @@ sbx_status sbx_dense_plan_phase_times(sbx_dense_plan* plan, int64_t* dev_times);
  * arrivals that never come, so its bounded wait runs out and the run reports
  * SBX_ETIMEOUT. 0 restores normal operation. */
 sbx_status sbx_dense_plan_test_barrier_extra(sbx_dense_plan* plan, int32_t extra);
+/* Waits for the device and frees the plan; safe after the plan's context was destroyed. */
 sbx_status sbx_dense_plan_destroy(sbx_dense_plan* plan);
+
+/* ---------------------------------------------------------------- batched networks
+ * Many independent dense networks packed into one sbx_dense_scene: network k owns a
+ * contiguous index range of every store (cross-store indices offset accordingly) and its
+ * own grid cells. The step runs one launch per phase for all networks; the draws are keyed
+ * by each item's local index and its network's seed, the grid and walls are the
+ * network's own, so each network's result equals its run alone, bit for bit.
+ * Key arrays hold (network, local index) int32 pairs per item. */
+typedef struct sbx_batch {
+    int32_t nNet;
+    int32_t *segKey, *motKey, *bbKey, *linkKey;
+    int32_t *seeds;                       /* nNet x 3: SEED (motors, links), SEED_BB, filament counts[2] */
+    float *gridParams;                    /* nNet x 6: each network's gridParams */
+    int32_t *gridDims;                    /* nNet x 4: nX, nY, nZ, first global cell */
+    float *boxParams;                     /* nNet x 8: each network's boxParams */
+} sbx_batch;
+/* the batched forms of the step's network-dependent kernels (same arithmetic as the
+ * single-network entry points; perKey = 3 for motor bodies, keyed by their motor) */
+sbx_status sbx_brownian_force_batched(sbx_ctx* ctx, int32_t n, int32_t perKey, float* rF, float* rT, const float* bTG,
+                                      const float* bRG, const float* tSc, const float* rSc, const float* params,
+                                      const int32_t* counts, const int32_t* key, const int32_t* seeds,
+                                      int32_t seedCol);
+sbx_status sbx_nucleotide_release_batched(sbx_ctx* ctx, int32_t nM, int32_t* boundSeg, const float* fdf,
+                                          const float* fm, int32_t* cooldown, int32_t* stats, int32_t* capStats,
+                                          const float* kp, const int32_t* counts, const int32_t* motKey,
+                                          const int32_t* seeds);
+sbx_status sbx_nucleotide_cycle_batched(sbx_ctx* ctx, int32_t nM, int32_t* state, const int32_t* boundSeg,
+                                        const float* hist, const float* np, const int32_t* counts,
+                                        const int32_t* motKey, const int32_t* seeds);
+sbx_status sbx_xlink_unbind_batched(sbx_ctx* ctx, int32_t nSeg, const float* fU, const float* fE1, int32_t nLinks,
+                                    const int32_t* A, const int32_t* B, const float* loc1, const float* loc2,
+                                    int32_t* state, float* hist, int32_t* place, const float* op,
+                                    const int32_t* counts, const int32_t* linkKey, const int32_t* seeds);
+sbx_status sbx_grid_body_cell_batched(sbx_ctx* ctx, int32_t cap, const float* center, const int32_t* counts,
+                                      int32_t* bodyCell, int32_t nSeg, const int32_t* segKey, const int32_t* motKey,
+                                      const float* gpTab, const int32_t* gdTab);
+sbx_status sbx_binding_grid_reachable_batched(sbx_ctx* ctx, const float* head, const float* uVec,
+                                              const float* rodUVec, int32_t nSeg, const float* e1, const float* e2,
+                                              const int32_t* offsets, const int32_t* contents,
+                                              const int32_t* ownerStore, const int32_t* ownerSlot, int32_t* reachSeg,
+                                              int32_t* reachCount, const float* kp, int32_t nM,
+                                              const int32_t* motKey, const float* gpTab, const int32_t* gdTab);
+sbx_status sbx_confine_batched(sbx_ctx* ctx, int32_t n, const float* coord, const float* uVec,
+                               const float* segLength, const float* bTG, float* F, float* T, const float* boxTab,
+                               const int32_t* counts, const int32_t* key);
+/* A plan over a packed scene (graph and per-system paths; the fused kernel is for one
+ * network). `batch` is copied; its arrays must stay alive. */
+sbx_status sbx_dense_plan_create_batched(sbx_ctx* ctx, const sbx_dense_scene* scene, const sbx_batch* batch,
+                                         sbx_dense_plan** out);
 
 /* Free rods (DiffusionHarness cpuStepFdt order: brownian -> integrate -> derive).
  * Runs nsteps steps (t0..) in one persistent launch that keeps each rod in registers.

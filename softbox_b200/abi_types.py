@@ -89,3 +89,8 @@ def fill(struct, arrays, prefix=""):
             ctype = {f32p: C.c_float, f64p: C.c_double, i32p: C.c_int32}[ftype]
             setattr(struct, name, _ptr(arrays.get(key), ctype))
     return struct
+
+
+class BatchDesc(C.Structure):           # packed networks (sbx_batch)
+    _fields_ = [("nNet", C.c_int32)] + [(k, i32p) for k in ("segKey", "motKey", "bbKey", "linkKey", "seeds")] + [
+        ("gridParams", f32p), ("gridDims", i32p), ("boxParams", f32p)]

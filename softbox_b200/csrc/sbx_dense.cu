@@ -42,7 +42,8 @@ __global__ void k_step_advance(int* d_step) { *d_step += 1; }
     } while (0)
 
 // the reference step order over the per-system entry points
-sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_step, int t) {
+sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_step, int t,
+                          const sbx_batch* bt = nullptr) {
     const sbx_filament_store& f = sc->fil;
     const sbx_motor_store& mot = sc->mot;
     const sbx_dimer_store& dim = sc->dim;
@@ -63,25 +64,52 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
                              g.ownerSlot, g.viewParams, f.filState));
     CHK(sbx_motor_publish(ctx, nM, mot.head, mot.reach, g.cap, g.center, g.boundingRadius, g.ownerStore, g.ownerSlot,
                           mot.publishParams));
-    CHK(sbx_grid_body_cell(ctx, g.cap, g.center, g.gridParams, g.gridDims, g.gridCounts, g.bodyCell));
+    if (bt)
+        CHK(sbx_grid_body_cell_batched(ctx, g.cap, g.center, g.gridCounts, g.bodyCell, nSeg, bt->segKey, bt->motKey,
+                                       bt->gridParams, bt->gridDims));
+    else
+        CHK(sbx_grid_body_cell(ctx, g.cap, g.center, g.gridParams, g.gridDims, g.gridCounts, g.bodyCell));
     CHK(sbx_grid_build(ctx, g.cap, g.bodyCell, g.gridCounts, g.totalCells, g.cellCount, g.chunkSum,
                        g.gridCellOffsets, g.gridCellContents, g.cap));
-    CHK(sbx_binding_grid_reachable(ctx, mot.head, mot.uVec, mot.rodUVec, nSeg, fb.end1, fb.end2, g.gridParams,
-                                   g.gridDims, g.gridCellOffsets, g.gridCellContents, g.ownerStore, g.ownerSlot,
-                                   g.reachSeg, g.reachCount, mot.kinParams, nM));
-    CHK(sbx_nucleotide_release(ctx, nM, mot.boundSeg, mot.forceDotFil, mot.forceMag, mot.cooldown, mot.stats,
-                               mot.capStats, mot.kinParams, mot.counts));
+    if (bt) {
+        CHK(sbx_binding_grid_reachable_batched(ctx, mot.head, mot.uVec, mot.rodUVec, nSeg, fb.end1, fb.end2,
+                                               g.gridCellOffsets, g.gridCellContents, g.ownerStore, g.ownerSlot,
+                                               g.reachSeg, g.reachCount, mot.kinParams, nM, bt->motKey,
+                                               bt->gridParams, bt->gridDims));
+        CHK(sbx_nucleotide_release_batched(ctx, nM, mot.boundSeg, mot.forceDotFil, mot.forceMag, mot.cooldown,
+                                           mot.stats, mot.capStats, mot.kinParams, mot.counts, bt->motKey,
+                                           bt->seeds));
+    } else {
+        CHK(sbx_binding_grid_reachable(ctx, mot.head, mot.uVec, mot.rodUVec, nSeg, fb.end1, fb.end2, g.gridParams,
+                                       g.gridDims, g.gridCellOffsets, g.gridCellContents, g.ownerStore, g.ownerSlot,
+                                       g.reachSeg, g.reachCount, mot.kinParams, nM));
+        CHK(sbx_nucleotide_release(ctx, nM, mot.boundSeg, mot.forceDotFil, mot.forceMag, mot.cooldown, mot.stats,
+                                   mot.capStats, mot.kinParams, mot.counts));
+    }
     CHK(sbx_binding_bind_nearest(ctx, mot.head, mot.uVec, mot.rodUVec, nSeg, fb.end1, fb.end2, g.reachSeg,
                                  g.reachCount, mot.boundSeg, mot.bindArc, mot.kinParams, nM));
-    CHK(sbx_nucleotide_cycle(ctx, nM, mot.nucleotideState, mot.boundSeg, mot.forceDotHist, mot.nucParams,
-                             mot.counts));
+    if (bt)
+        CHK(sbx_nucleotide_cycle_batched(ctx, nM, mot.nucleotideState, mot.boundSeg, mot.forceDotHist, mot.nucParams,
+                                         mot.counts, bt->motKey, bt->seeds));
+    else
+        CHK(sbx_nucleotide_cycle(ctx, nM, mot.nucleotideState, mot.boundSeg, mot.forceDotHist, mot.nucParams,
+                                 mot.counts));
     // (ii) minifilament structure
     CHK(sbx_zero_accumulators(ctx, nB, b.forceSum, b.torqueSum));
     CHK(sbx_zero_accumulators(ctx, nBb, bb.forceSum, bb.torqueSum));
-    CHK(sbx_brownian_force(ctx, nB, b.randForce, b.randTorque, b.bTransGam, b.bRotGam, b.brownTransScale,
-                           b.brownRotScale, mot.bodyParams, mot.counts));
-    CHK(sbx_brownian_force(ctx, nBb, bb.randForce, bb.randTorque, bb.bTransGam, bb.bRotGam, bb.brownTransScale,
-                           bb.brownRotScale, mini.bbBodyParams, mini.bbCounts));
+    if (bt) {
+        CHK(sbx_brownian_force_batched(ctx, nB, 3, b.randForce, b.randTorque, b.bTransGam, b.bRotGam,
+                                       b.brownTransScale, b.brownRotScale, mot.bodyParams, mot.counts, bt->motKey,
+                                       bt->seeds, 0));
+        CHK(sbx_brownian_force_batched(ctx, nBb, 1, bb.randForce, bb.randTorque, bb.bTransGam, bb.bRotGam,
+                                       bb.brownTransScale, bb.brownRotScale, mini.bbBodyParams, mini.bbCounts,
+                                       bt->bbKey, bt->seeds, 1));
+    } else {
+        CHK(sbx_brownian_force(ctx, nB, b.randForce, b.randTorque, b.bTransGam, b.bRotGam, b.brownTransScale,
+                               b.brownRotScale, mot.bodyParams, mot.counts));
+        CHK(sbx_brownian_force(ctx, nBb, bb.randForce, bb.randTorque, bb.bTransGam, bb.bRotGam, bb.brownTransScale,
+                               bb.brownRotScale, mini.bbBodyParams, mini.bbCounts));
+    }
     CHK(sbx_motor_joints(ctx, nB, b.coord, b.uVec, b.segLength, b.bTransGam, b.bRotGam, b.forceSum, b.torqueSum,
                          mot.nucleotideState, mot.jointParams));
     CHK(sbx_dimer_couple(ctx, nB, b.coord, b.uVec, b.segLength, b.bTransGam, b.bRotGam, b.forceSum, b.torqueSum, nD,
@@ -99,8 +127,12 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
     CHK(sbx_xbridge_apply_head_force(ctx, nB, sc->bondData, b.forceSum, b.torqueSum));
     CHK(sbx_integrate(ctx, nB, b.coord, b.coord64, b.uVec, b.yVec, b.forceSum, b.torqueSum, b.randForce, b.randTorque,
                       b.bTransGam, b.bRotGam, mot.bodyParams));
-    CHK(sbx_confine(ctx, nBb, bb.coord, bb.uVec, bb.segLength, bb.bTransGam, bb.forceSum, bb.torqueSum,
-                    sc->boxParams, mini.bbCounts));
+    if (bt)
+        CHK(sbx_confine_batched(ctx, nBb, bb.coord, bb.uVec, bb.segLength, bb.bTransGam, bb.forceSum, bb.torqueSum,
+                                bt->boxParams, mini.bbCounts, bt->bbKey));
+    else
+        CHK(sbx_confine(ctx, nBb, bb.coord, bb.uVec, bb.segLength, bb.bTransGam, bb.forceSum, bb.torqueSum,
+                        sc->boxParams, mini.bbCounts));
     CHK(sbx_integrate(ctx, nBb, bb.coord, bb.coord64, bb.uVec, bb.yVec, bb.forceSum, bb.torqueSum, bb.randForce,
                       bb.randTorque, bb.bTransGam, bb.bRotGam, mini.bbBodyParams));
     CHK(sbx_derive(ctx, nB, b.coord, b.uVec, b.yVec, b.zVec, b.end1, b.end2, b.segLength));
@@ -109,12 +141,21 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
                                        mot.forceDotHist, mot.forceDotPlace));
     // (iii)-(v) filaments
     CHK(sbx_zero_accumulators(ctx, nSeg, fb.forceSum, fb.torqueSum));
-    CHK(sbx_brownian_force(ctx, nSeg, fb.randForce, fb.randTorque, fb.bTransGam, fb.bRotGam, fb.brownTransScale,
-                           fb.brownRotScale, f.params, f.counts));
+    if (bt)
+        CHK(sbx_brownian_force_batched(ctx, nSeg, 1, fb.randForce, fb.randTorque, fb.bTransGam, fb.bRotGam,
+                                       fb.brownTransScale, fb.brownRotScale, f.params, f.counts, bt->segKey,
+                                       bt->seeds, 2));
+    else
+        CHK(sbx_brownian_force(ctx, nSeg, fb.randForce, fb.randTorque, fb.bTransGam, fb.bRotGam, fb.brownTransScale,
+                               fb.brownRotScale, f.params, f.counts));
     CHK(sbx_chain_forces(ctx, nSeg, fb.coord, fb.uVec, fb.segLength, f.end2NbrSlot, f.end2NbrSide, f.end1NbrSlot,
                          f.end1NbrSide, fb.bTransGam, fb.bRotGam, fb.forceSum, fb.torqueSum, f.chainParams));
     if (xlOn) {
-        if (sc->xlUnbind)
+        if (sc->xlUnbind && bt)
+            CHK(sbx_xlink_unbind_batched(ctx, nSeg, fb.uVec, fb.end1, xl.nLinks, xl.linkFilA, xl.linkFilB, xl.loc1,
+                                         xl.loc2, xl.linkState, xl.strainHist, xl.strainPlace, xl.offParams,
+                                         xl.counts, bt->linkKey, bt->seeds));
+        else if (sc->xlUnbind)
             CHK(sbx_xlink_unbind(ctx, nSeg, fb.uVec, fb.end1, xl.nLinks, xl.linkFilA, xl.linkFilB, xl.loc1, xl.loc2,
                                  xl.linkState, xl.strainHist, xl.strainPlace, xl.offParams, xl.counts));
         CHK(sbx_xlink_count_active(ctx, xl.nLinks, xl.linkState, xl.linkFilA, xl.linkFilB, nSeg,
@@ -134,8 +175,12 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
     CHK(sbx_csr_build(ctx, mot.boundSeg, nM, nSeg, sc->segMotorCount, sc->segMotorOffsets, sc->segMotorMyo));
     CHK(sbx_xbridge_seg_gather(ctx, nSeg, sc->segMotorOffsets, sc->segMotorMyo, sc->bondData, fb.forceSum,
                                fb.torqueSum));
-    CHK(sbx_confine(ctx, nSeg, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.forceSum, fb.torqueSum,
-                    sc->boxParams, f.counts));
+    if (bt)
+        CHK(sbx_confine_batched(ctx, nSeg, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.forceSum, fb.torqueSum,
+                                bt->boxParams, f.counts, bt->segKey));
+    else
+        CHK(sbx_confine(ctx, nSeg, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.forceSum, fb.torqueSum,
+                        sc->boxParams, f.counts));
     CHK(sbx_integrate(ctx, nSeg, fb.coord, fb.coord64, fb.uVec, fb.yVec, fb.forceSum, fb.torqueSum, fb.randForce,
                       fb.randTorque, fb.bTransGam, fb.bRotGam, f.params));
     CHK(sbx_derive(ctx, nSeg, fb.coord, fb.uVec, fb.yVec, fb.zVec, fb.end1, fb.end2, fb.segLength));
@@ -168,6 +213,9 @@ struct sbx_dense_plan {
     FusedArgs fa{};
     int fused_grid = 0;
     std::vector<void*> allocs;
+    // packed networks (graph and per-system paths only)
+    bool batched = false;
+    sbx_batch batch{};
 };
 
 namespace {
@@ -312,13 +360,17 @@ extern "C" sbx_status sbx_dense_step_unfused(sbx_ctx* ctx, const sbx_dense_scene
     return dense_sequence(ctx, sc, nullptr, t);
 }
 
-extern "C" sbx_status sbx_dense_plan_create(sbx_ctx* ctx, const sbx_dense_scene* sc, sbx_dense_plan** out) {
+static sbx_status plan_create(sbx_ctx* ctx, const sbx_dense_scene* sc, const sbx_batch* bt, sbx_dense_plan** out) {
     if (!ctx || !sc || !out) return SBX_EINVAL;
     *out = nullptr;
     CHK(ensure_scratch(ctx, dense_scratch_bytes(sc)));
     sbx_dense_plan* p = new sbx_dense_plan();
     p->ctx = ctx;
     p->scene = *sc;
+    if (bt) {
+        p->batched = true;
+        p->batch = *bt;
+    }
     if (cudaMalloc(&p->d_step, sizeof(int)) != cudaSuccess) {
         delete p;
         return fail(ctx, SBX_ENOMEM, "sbx_dense_plan_create: step word");
@@ -331,7 +383,7 @@ extern "C" sbx_status sbx_dense_plan_create(sbx_ctx* ctx, const sbx_dense_scene*
         delete p;
         return fail(ctx, SBX_ECUDA, "sbx_dense_plan_create: begin capture");
     }
-    sbx_status st = dense_sequence(ctx, &p->scene, p->d_step, 0);
+    sbx_status st = dense_sequence(ctx, &p->scene, p->d_step, 0, p->batched ? &p->batch : nullptr);
     if (st == SBX_OK) SBX_LAUNCH(ctx, k_step_advance, 1, 1, p->d_step);
     cudaError_t ce = cudaStreamEndCapture(ctx->stream, &p->graph);
     if (st != SBX_OK || ce != cudaSuccess) {
@@ -349,10 +401,27 @@ extern "C" sbx_status sbx_dense_plan_create(sbx_ctx* ctx, const sbx_dense_scene*
         delete p;
         return fail(ctx, SBX_ECUDA, "sbx_dense_plan_create: instantiate");
     }
-    p->fused_ok = fused_prepare(p);
+    if (p->batched) {
+        p->fused_ok = false;
+        p->fused_why = "packed networks run on the graph or per-system path";
+    } else {
+        p->fused_ok = fused_prepare(p);
+    }
     cudaGetLastError();
     *out = p;
     return SBX_OK;
+}
+
+extern "C" sbx_status sbx_dense_plan_create(sbx_ctx* ctx, const sbx_dense_scene* sc, sbx_dense_plan** out) {
+    return plan_create(ctx, sc, nullptr, out);
+}
+
+extern "C" sbx_status sbx_dense_plan_create_batched(sbx_ctx* ctx, const sbx_dense_scene* sc, const sbx_batch* batch,
+                                                    sbx_dense_plan** out) {
+    if (!batch || batch->nNet < 1 || !batch->segKey || !batch->motKey || !batch->bbKey || !batch->seeds ||
+        !batch->gridParams || !batch->gridDims || !batch->boxParams || (sc && sc->xl.nLinks > 0 && !batch->linkKey))
+        return ctx ? fail(ctx, SBX_EINVAL, "sbx_dense_plan_create_batched: incomplete batch") : SBX_EINVAL;
+    return plan_create(ctx, sc, batch, out);
 }
 
 extern "C" sbx_status sbx_dense_plan_run(sbx_dense_plan* p, int32_t t0, int32_t nsteps, int32_t mode) {
@@ -386,7 +455,8 @@ extern "C" sbx_status sbx_dense_plan_run(sbx_dense_plan* p, int32_t t0, int32_t 
         }
         return check_launch(ctx, "sbx_dense_plan_run");
     }
-    for (int k = 0; k < nsteps; k++) CHK(dense_sequence(ctx, &p->scene, nullptr, t0 + k));
+    for (int k = 0; k < nsteps; k++)
+        CHK(dense_sequence(ctx, &p->scene, nullptr, t0 + k, p->batched ? &p->batch : nullptr));
     return SBX_OK;
 }
 
@@ -427,7 +497,9 @@ extern "C" sbx_status sbx_dense_plan_test_barrier_extra(sbx_dense_plan* p, int32
 
 extern "C" sbx_status sbx_dense_plan_destroy(sbx_dense_plan* p) {
     if (!p) return SBX_EINVAL;
-    cudaStreamSynchronize(p->ctx->stream);
+    // the plan may outlive its context (language runtimes finalise objects in any order at
+    // exit), so it touches no context state here: a device-wide wait before the frees
+    cudaDeviceSynchronize();
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
     if (p->d_step) cudaFree(p->d_step);
