@@ -665,6 +665,37 @@ sbx_status sbx_binding_grid_reachable_batched(sbx_ctx* ctx, const float* head, c
 sbx_status sbx_confine_batched(sbx_ctx* ctx, int32_t n, const float* coord, const float* uVec,
                                const float* segLength, const float* bTG, float* F, float* T, const float* boxTab,
                                const int32_t* counts, const int32_t* key);
+/* ---------------------------------------------------------------- observables
+ * Per network k of a single or packed scene (segBase/linkBase/motBase: nNet+1 device
+ * offsets of the network's index ranges). Deterministic FP64 reductions: one block per
+ * network, thread t sums items t, t+256, ... in index order, then a fixed tree.
+ * RMS extent of the ACTIVE filament rods about their mean (FullSystemDemoHarness.filRms,
+ * FullSystemDemoHarness.java:1047-1055): out[2k] = R_rms (um), out[2k+1] = rods counted.
+ * coord64 (FP64 centres) is used when given; filState may be NULL (all ACTIVE). */
+sbx_status sbx_obs_extent(sbx_ctx* ctx, int32_t nNet, const int32_t* segBase, int32_t nSeg, const float* coord,
+                          const double* coord64, const int32_t* filState, double* out);
+/* Mean in-plane network stress: out[k] = -(1/(2V_k)) sum (r_x F_x + r_y F_y) over ACTIVE
+ * crosslinks (r = attachment A - attachment B, F = the payload force on A) and bound heads
+ * (r = head tip - attachment point, F = the payload force on the head), r in m, V in um^3
+ * (volume[k]), Pa; positive = tension. linkBase or motBase may be NULL to leave a term out. */
+sbx_status sbx_obs_stress(sbx_ctx* ctx, int32_t nNet, int32_t nSeg, const float* coord, const float* uVec,
+                          const float* end1, const float* segLength, const int32_t* linkBase, const int32_t* linkFilA,
+                          const int32_t* linkFilB, const int32_t* linkState, const float* loc1, const float* loc2,
+                          const float* xlinkData, int32_t nMotors, const int32_t* motBase, const float* motCoord,
+                          const float* motUVec, const int32_t* boundSeg, const float* bindArc,
+                          const float* bondData, double headLen, const float* volume, double* out);
+/* Largest cluster: components over ACTIVE segments and backbones joined by chain links,
+ * ACTIVE crosslinks and bound heads (segment -- its head's backbone, motorBackbone[m]).
+ * `rounds` hook-and-compress rounds (each skipped once the previous one changed nothing);
+ * flags[rounds] scratch, flags[rounds-1] != 0 afterwards means not converged. label
+ * receives each node's component id (its smallest node id; -1 for FREE segments), size the
+ * component sizes in segments; out[2k] = largest component (segments), out[2k+1] = ACTIVE
+ * segments of network k. */
+sbx_status sbx_obs_clusters(sbx_ctx* ctx, int32_t nNet, const int32_t* segBase, int32_t nSeg, const int32_t* filState,
+                            const int32_t* end2NbrSlot, int32_t nLinks, const int32_t* linkFilA,
+                            const int32_t* linkFilB, const int32_t* linkState, int32_t nMotors,
+                            const int32_t* boundSeg, const int32_t* motorBackbone, int32_t nBackbones,
+                            int32_t rounds, int32_t* label, int32_t* size, int32_t* flags, int32_t* out);
 /* A plan over a packed scene (graph and per-system paths; the fused kernel is for one
  * network). `batch` is copied; its arrays must stay alive. */
 sbx_status sbx_dense_plan_create_batched(sbx_ctx* ctx, const sbx_dense_scene* scene, const sbx_batch* batch,

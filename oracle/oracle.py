@@ -70,6 +70,8 @@ _SIGS = {
     "orc_pool_put_total": "ppi", "orc_pool_take_total": "ppi", "orc_turnover_begin": "iiiddpppppp",
     "orc_turnover_release_dead": "pipppip", "orc_birth_emit_constant_actin": "ippiipppp",
     "orc_birth_init_newborn": "iipppppp", "orc_birth_tag_seeds": "iipppp", "orc_pool_take_births": "ppipii",
+    "orc_obs_extent": "ipipppp", "orc_obs_stress": "iipppppppppppippppppdpp",
+    "orc_obs_clusters": "ipippipppippippp",
 }
 _CT = {"i": C.c_int32, "I": C.c_uint64, "d": C.c_double, "f": C.c_float, "p": C.c_void_p, "s": C.c_void_p}
 _RET = {"orc_max_threads": C.c_int, "orc_accurate_acos": C.c_double, "orc_angle_from_sin_cos": C.c_double,

@@ -2683,3 +2683,133 @@ EXPORT void orc_pool_take_births(void* poolp, const i32* rankOffsets, i32 K, con
     if (p->conc < 0.0) p->conc = 0.0;
     p->taken += m;
 }
+
+// ============================================================================
+// Observables (the library's sbx_obs_* entry points): the same FP64 summation order —
+// 256 strided partial sums per network, then the fixed tree — and union-find clusters.
+// ============================================================================
+namespace {
+const int OBS_T = 256;
+void obs_tree(double* p) {
+    for (int s = OBS_T / 2; s > 0; s >>= 1)
+        for (int t = 0; t < s; t++) p[t] += p[t + s];
+}
+inline double obs_c(const float* c, const double* c64, int n, int i, int k) {
+    return c64 ? c64[(int64_t)k * n + i] : (double)c[(int64_t)k * n + i];
+}
+}  // namespace
+
+EXPORT void orc_obs_extent(i32 nNet, const i32* segBase, i32 n, const float* coord, const double* coord64,
+                           const i32* filState, double* out) {
+    for (int net = 0; net < nNet; net++) {
+        int b0 = segBase[net], b1 = segBase[net + 1];
+        double pc[OBS_T], px[OBS_T], py[OBS_T], pz[OBS_T];
+        for (int t = 0; t < OBS_T; t++) {
+            double cnt = 0, sx = 0, sy = 0, sz = 0;
+            for (int i = b0 + t; i < b1; i += OBS_T) {
+                if (filState && filState[i] < 0) continue;
+                cnt += 1.0;
+                sx += obs_c(coord, coord64, n, i, 0);
+                sy += obs_c(coord, coord64, n, i, 1);
+                sz += obs_c(coord, coord64, n, i, 2);
+            }
+            pc[t] = cnt; px[t] = sx; py[t] = sy; pz[t] = sz;
+        }
+        obs_tree(pc); obs_tree(px); obs_tree(py); obs_tree(pz);
+        double c = pc[0];
+        double mx = c > 0 ? px[0] / c : 0.0, my = c > 0 ? py[0] / c : 0.0, mz = c > 0 ? pz[0] / c : 0.0;
+        double p2[OBS_T];
+        for (int t = 0; t < OBS_T; t++) {
+            double s2 = 0;
+            for (int i = b0 + t; i < b1; i += OBS_T) {
+                if (filState && filState[i] < 0) continue;
+                double dx = obs_c(coord, coord64, n, i, 0) - mx;
+                double dy = obs_c(coord, coord64, n, i, 1) - my;
+                double dz = obs_c(coord, coord64, n, i, 2) - mz;
+                s2 += dx * dx + dy * dy + dz * dz;
+            }
+            p2[t] = s2;
+        }
+        obs_tree(p2);
+        out[2 * net] = c > 0 ? std::sqrt(p2[0] / c) : 0.0;
+        out[2 * net + 1] = c;
+    }
+}
+
+EXPORT void orc_obs_stress(i32 nNet, i32 nSeg, const float* fC, const float* fU, const float* fE1, const float* fLen,
+                           const i32* linkBase, const i32* linkA, const i32* linkB, const i32* linkState,
+                           const float* loc1, const float* loc2, const float* xd, i32 nMotors, const i32* motBase,
+                           const float* mC, const float* mU, const i32* boundSeg, const float* bindArc,
+                           const float* bd, double headLen, const float* volume, double* out) {
+    int nB = 3 * nMotors;
+    for (int net = 0; net < nNet; net++) {
+        double p[OBS_T];
+        for (int t = 0; t < OBS_T; t++) {
+            double w = 0;
+            if (linkBase)
+                for (int k = linkBase[net] + t; k < linkBase[net + 1]; k += OBS_T) {
+                    if (linkState[k] < 0) continue;
+                    int a = linkA[k], b = linkB[k];
+                    if (a < 0 || b < 0) continue;
+                    double l1 = loc1[k], l2 = loc2[k];
+                    double rx = (fE1[a] + l1 * fU[a]) - (fE1[b] + l2 * fU[b]);
+                    double ry = (fE1[nSeg + a] + l1 * fU[nSeg + a]) - (fE1[nSeg + b] + l2 * fU[nSeg + b]);
+                    w += 1.0e-6 * rx * xd[12 * (int64_t)k] + 1.0e-6 * ry * xd[12 * (int64_t)k + 1];
+                }
+            if (motBase)
+                for (int m = motBase[net] + t; m < motBase[net + 1]; m += OBS_T) {
+                    int s = boundSeg[m];
+                    if (s < 0) continue;
+                    int h = 3 * m + 2;
+                    double hx = mC[h] + 0.5 * headLen * mU[h], hy = mC[nB + h] + 0.5 * headLen * mU[nB + h];
+                    double off = (double)bindArc[m] - 0.5 * fLen[s];
+                    double ax = fC[s] + off * fU[s], ay = fC[nSeg + s] + off * fU[nSeg + s];
+                    w += 1.0e-6 * (hx - ax) * bd[13 * (int64_t)m] + 1.0e-6 * (hy - ay) * bd[13 * (int64_t)m + 1];
+                }
+            p[t] = w;
+        }
+        obs_tree(p);
+        out[net] = -p[0] / (2.0 * volume[net] * 1.0e-18);
+    }
+}
+
+namespace {
+int uf_find(std::vector<int>& par, int x) {
+    while (par[x] != x) { par[x] = par[par[x]]; x = par[x]; }
+    return x;
+}
+void uf_union(std::vector<int>& par, int a, int b) {
+    int ra = uf_find(par, a), rb = uf_find(par, b);
+    if (ra == rb) return;
+    if (ra < rb) par[rb] = ra; else par[ra] = rb;
+}
+}  // namespace
+
+EXPORT void orc_obs_clusters(i32 nNet, const i32* segBase, i32 nSeg, const i32* filState, const i32* e2, i32 nLinks,
+                             const i32* linkA, const i32* linkB, const i32* linkState, i32 nMotors,
+                             const i32* boundSeg, const i32* motorBackbone, i32 nBackbones, i32* label, i32* size,
+                             i32* out) {
+    int nNode = nSeg + nBackbones;
+    std::vector<int> par(nNode);
+    for (int i = 0; i < nNode; i++) par[i] = i;
+    auto live = [&](int x) { return x >= 0 && (x >= nSeg || !filState || filState[x] >= 0); };
+    for (int s = 0; s < nSeg; s++)
+        if (live(s) && e2[s] >= 0 && live(e2[s])) uf_union(par, s, e2[s]);
+    for (int k = 0; k < nLinks; k++)
+        if (linkState[k] >= 0 && live(linkA[k]) && live(linkB[k])) uf_union(par, linkA[k], linkB[k]);
+    for (int m = 0; m < nMotors; m++)
+        if (boundSeg[m] >= 0 && motorBackbone[m] >= 0 && live(boundSeg[m]))
+            uf_union(par, boundSeg[m], nSeg + motorBackbone[m]);
+    for (int i = 0; i < nNode; i++) { label[i] = live(i) ? uf_find(par, i) : -1; size[i] = 0; }
+    for (int s = 0; s < nSeg; s++) if (label[s] >= 0) size[label[s]]++;
+    for (int net = 0; net < nNet; net++) {
+        int best = 0, cnt = 0;
+        for (int s = segBase[net]; s < segBase[net + 1]; s++) {
+            if (label[s] < 0) continue;
+            cnt++;
+            best = std::max(best, size[label[s]]);
+        }
+        out[2 * net] = best;
+        out[2 * net + 1] = cnt;
+    }
+}

@@ -324,3 +324,34 @@ def oracle_turnover_network_run(orc, sc, t0, nsteps):
         oracle_dense_run(orc, sc, t, nxt - t)
         t = nxt
     return sc
+
+
+def oracle_observables(orc, sc, seg_base=None, link_base=None, mot_base=None, volume=None, rounds=None):
+    """The sbx_obs_* restatements on a host dense scene: (extent[nNet,2], stress[nNet],
+    clusters[nNet,2], label)."""
+    from softbox_b200.observables import HEAD_LEN, motor_backbones
+    f, xl, mot = sc["fil"], sc["xl"], sc["mot"]
+    fb = f["body"]
+    nS, nM, nL, nBb = fb["n"], mot["nMotors"], xl["nLinks"], sc["mini"]["nBackbones"]
+    seg = np.asarray(seg_base if seg_base is not None else [0, nS], np.int32)
+    lnk = np.asarray(link_base if link_base is not None else [0, nL], np.int32)
+    mtb = np.asarray(mot_base if mot_base is not None else [0, nM], np.int32)
+    nNet = seg.size - 1
+    if volume is None:
+        b = sc["boxParams"]
+        volume = [b[1] * b[2] * b[3]]
+    vol = np.asarray(volume, np.float32)
+    ext = np.zeros(2 * nNet)
+    orc.obs_extent(nNet, seg, nS, fb["coord"], fb.get("coord64"), f["filState"], ext)
+    st = np.zeros(nNet)
+    orc.obs_stress(nNet, nS, fb["coord"], fb["uVec"], fb["end1"], fb["segLength"], lnk, xl["linkFilA"],
+                   xl["linkFilB"], xl["linkState"], xl["loc1"], xl["loc2"], xl["xlinkData"], nM, mtb,
+                   mot["body"]["coord"], mot["body"]["uVec"], mot["boundSeg"], mot["bindArc"], sc["bondData"],
+                   HEAD_LEN, vol, st)
+    mb = motor_backbones(sc["dim"], sc["mini"], nM)
+    label = np.zeros(nS + nBb, np.int32)
+    size = np.zeros(nS + nBb, np.int32)
+    cl = np.zeros(2 * nNet, np.int32)
+    orc.obs_clusters(nNet, seg, nS, f["filState"], f["end2NbrSlot"], nL, xl["linkFilA"], xl["linkFilB"],
+                     xl["linkState"], nM, mot["boundSeg"], mb, nBb, label, size, cl)
+    return ext.reshape(-1, 2), st, cl.reshape(-1, 2), label
