@@ -284,6 +284,8 @@ class DenseConfig:
     head_zone: float = 0.05
     n_links: int = 4000
     side: float = 20.0
+    aspect: float = 1.0              # slab x:y aspect at the same area (side_x = side*sqrt(aspect))
+    cell_scale: float = 1.0          # grid cell / the completeness minimum (>= 1; a tuning knob)
     box_z: float = 0.5
     dt: float = 1.0e-5
     aeta: float = 0.1               # Constants.aeta: motors, backbones, and the filament base drag
@@ -429,13 +431,14 @@ def dense_contractile(cfg: DenseConfig = C1):
     composition `cfg`. Returns a dict-of-stores scene (host numpy arrays)."""
     rng = JavaRandom(cfg.seed)
     side, box_z, dt = cfg.side, cfg.box_z, cfg.dt
+    side_x, side_y = (side, side) if cfg.aspect == 1.0 else (side * math.sqrt(cfg.aspect),
+                                                              side / math.sqrt(cfg.aspect))
     n_fil, S = cfg.n_fil, cfg.segs_per_fil
     n_seg = n_fil * S
     n_mini = cfg.n_mini
     n_dimers = n_mini * 2 * cfg.dimers_per_end
     n_mot = 2 * n_dimers
     L = (cfg.monomer_ct + 1) * ACTIN_MONO_RADIUS
-    half = 0.5 * side
     hz = 0.5 * box_z
     margin = 0.5 * (S * L)
 
@@ -446,8 +449,8 @@ def dense_contractile(cfg: DenseConfig = C1):
     # expressions evaluated elementwise
     fil = np.empty((n_fil, 6))
     for p in range(n_fil):
-        cx = (rng.next_double() - 0.5) * (side - 2 * margin)
-        cy = (rng.next_double() - 0.5) * (side - 2 * margin)
+        cx = (rng.next_double() - 0.5) * (side_x - 2 * margin)
+        cy = (rng.next_double() - 0.5) * (side_y - 2 * margin)
         cz = (rng.next_double() - 0.5) * (box_z - 0.1)
         th = rng.next_double() * math.pi * 2
         fil[p] = (cx, cy, cz, math.cos(th), math.sin(th), 0.0)
@@ -493,8 +496,8 @@ def dense_contractile(cfg: DenseConfig = C1):
     d = 0
     dimer_rows = []
     for mfi in range(n_mini):
-        bx = (rng.next_double() - 0.5) * (side - 2 * margin)
-        by = (rng.next_double() - 0.5) * (side - 2 * margin)
+        bx = (rng.next_double() - 0.5) * (side_x - 2 * margin)
+        by = (rng.next_double() - 0.5) * (side_y - 2 * margin)
         bz = (rng.next_double() - 0.5) * (box_z - 0.1)
         th = rng.next_double() * math.pi * 2
         ux, uy, uz = math.cos(th), math.sin(th), 0.0
@@ -567,8 +570,10 @@ def dense_contractile(cfg: DenseConfig = C1):
     seg_bound_r = 0.5 * L + ACTIN_RADIUS
     cutoff = cfg.myo_col_tol + 0.5 * ROD_LEN
     cell = 2.0 * seg_bound_r + cutoff
-    gx = half + 1.0
-    gy = gx
+    if cfg.cell_scale != 1.0:
+        cell *= max(1.0, cfg.cell_scale)
+    gx = 0.5 * side_x + 1.0
+    gy = 0.5 * side_y + 1.0
     gz = hz + 0.3
     nX = 1 + int(math.ceil(2 * gx / cell))
     nY = 1 + int(math.ceil(2 * gy / cell))
@@ -596,7 +601,7 @@ def dense_contractile(cfg: DenseConfig = C1):
         "cfg": cfg, "fil": f, "mot": mot, "dim": dim, "mini": mini, "xl": xl, "grid": grid,
         "bondData": np.zeros(n_mot * XB_STRIDE, F32),
         "xbParams": np.array([cfg.myo_spring, 90.0, cfg.j1_fmt, dt, HEAD_LEN, 0.0], F32),
-        "boxParams": np.array([1.0e-4, side, side, box_z, ACTIN_RADIUS, 0.5, check_int, dt], F32),
+        "boxParams": np.array([1.0e-4, side_x, side_y, box_z, ACTIN_RADIUS, 0.5, check_int, dt], F32),
         "segMotorCount": np.zeros(n_seg, I32), "segMotorOffsets": np.zeros(n_seg + 1, I32),
         "segMotorMyo": np.zeros(n_mot, I32),
         "seed": cfg.seed, "seedBb": cfg.seed_bb, "xlinkOn": 1, "xlUnbind": 1 if cfg.xl_unbind else 0,
@@ -900,7 +905,8 @@ def dense_turnover(cfg=None, growth_rate=10.0, sever_rate=0.01, cof_ratio=0.5, b
     f = sc["fil"]
     n = f["body"]["n"]
     tcfg = TurnoverConfig(dt=cfg.dt, cof_ratio=cof_ratio, pool0_um=growth_rate / K_ATP_ON2_WITH_FORMIN,
-                          box_vol_um3=cfg.side * cfg.side * cfg.box_z, aeta=cfg.fil_aeta, born_trans=cfg.brown_trans,
+                          box_vol_um3=float(sc["boxParams"][1]) * float(sc["boxParams"][2]) * cfg.box_z,
+                          aeta=cfg.fil_aeta, born_trans=cfg.brown_trans,
                           born_rot=BROT_COEFF)
     seedNode = np.full(n, -1, I32)
     tips = np.flatnonzero(f["end2NbrSlot"] < 0)
@@ -916,7 +922,8 @@ def dense_turnover(cfg=None, growth_rate=10.0, sever_rate=0.01, cof_ratio=0.5, b
     t["cofilinParams"][0] = F32(-math.expm1(-x_star / cadences))
     seed_mon = cfg.monomer_ct if seed_mon is None else seed_mon
     birth_cap = birth_cap or max(64, n // 50)
-    birth_arrays(t, birth_cap, (0.5 * cfg.side, 0.5 * cfg.side, 0.5 * cfg.box_z), seed_mon)
+    bp = sc["boxParams"]
+    birth_arrays(t, birth_cap, (0.5 * float(bp[1]), 0.5 * float(bp[2]), 0.5 * cfg.box_z), seed_mon)
     sc["turnover"] = t
     sc["tcfg"] = tcfg
     return sc
