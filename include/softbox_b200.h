@@ -696,6 +696,34 @@ sbx_status sbx_obs_clusters(sbx_ctx* ctx, int32_t nNet, const int32_t* segBase, 
                             const int32_t* linkFilB, const int32_t* linkState, int32_t nMotors,
                             const int32_t* boundSeg, const int32_t* motorBackbone, int32_t nBackbones,
                             int32_t rounds, int32_t* label, int32_t* size, int32_t* flags, int32_t* out);
+/* ---------------------------------------------------------------- surrogate (MLP ensemble)
+ * C[M x N] = A[M x K] . B[N x K]^T on the tensor cores (tcgen05, BF16 operands, FP32
+ * accumulation), K <= 256, for nz independent problems (ensemble members) at the given
+ * element strides. A and B are row-major BF16 (uint16 bit patterns). Epilogue per element:
+ * v = acc (+ bias[n]); outF = v (FP32, optional); a = act ? GELU(v) : v (act 1 = exact GELU);
+ * out = bf16(a) row-major (optional) and outT = bf16(a) transposed, N x M with leading
+ * dimension ldt (optional). errFlag (optional device int) gets bit 0 when an MMA completion
+ * wait ran out. */
+sbx_status sbx_mlp_gemm_bf16(sbx_ctx* ctx, int32_t nz, int32_t M, int32_t N, int32_t K, const void* A, int32_t lda,
+                             int64_t strideA, const void* B, int32_t ldb, int64_t strideB, const float* bias,
+                             int64_t strideBias, int32_t act, void* out, int32_t ldo, int64_t strideOut, void* outT,
+                             int32_t ldt, int64_t strideOutT, float* outF, int32_t ldf, int64_t strideOutF,
+                             int32_t* errFlag);
+/* g = dA * GELU'(Z) (Z NULL: g = dA) as BF16, row-major M x N and transposed N x M */
+sbx_status sbx_mlp_gelu_backward(sbx_ctx* ctx, int32_t nz, int32_t M, int32_t N, const float* dA, const float* Z,
+                                 int64_t strideMN, void* g, void* gT, int64_t strideG, int64_t strideGT);
+/* out[n] = sum over rows of a BF16 M x N matrix, rows in order (bias gradients) */
+sbx_status sbx_mlp_colsum_bf16(sbx_ctx* ctx, int32_t nz, int32_t M, int32_t N, const void* in, int64_t strideIn,
+                               float* out, int64_t strideOut);
+/* mean-squared-error gradient over the first nOut of Np columns (0 on the padding); loss
+ * (optional, nz floats) accumulates the mean squared error */
+sbx_status sbx_mlp_mse_grad(sbx_ctx* ctx, int32_t nz, int32_t M, int32_t Np, int32_t nOut, const float* y,
+                            int64_t strideY, const float* t, int64_t strideT, float* g, int64_t strideG, float* loss);
+/* Adam step (bias-corrected with stepNumber) on FP32 master weights N x K; refreshes the
+ * BF16 copy (N x K) and, when given, its transpose (K x N) */
+sbx_status sbx_mlp_adam(sbx_ctx* ctx, int32_t nz, int32_t N, int32_t K, float* w, const float* gw, float* m, float* v,
+                        int64_t stride, float lr, float beta1, float beta2, float eps, int32_t stepNumber,
+                        void* wBf16, void* wBf16T, int64_t strideB, int64_t strideBT);
 /* A plan over a packed scene (graph and per-system paths; the fused kernel is for one
  * network). `batch` is copied; its arrays must stay alive. */
 sbx_status sbx_dense_plan_create_batched(sbx_ctx* ctx, const sbx_dense_scene* scene, const sbx_batch* batch,
