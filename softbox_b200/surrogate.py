@@ -1,0 +1,216 @@
+"""Surrogate of the parameter sweep: an ensemble of MLPs trained and evaluated on the
+device by the library's tensor-core kernels (sbx_mlp_*), with the plain simulation as the
+fallback wherever the ensemble disagrees.
+
+    ens = MLPEnsemble()                             # 5 nets, 6 -> 256 x4 (GELU) -> 3, BF16
+    ens.fit(X, Y, epochs=...)                        # Adam, lr 1e-3, batch 256
+    mean, std = ens.predict(X_new)                   # per output, de-normalised
+    rerun = fallback_mask(mean, std, 0.10)           # points for the plain simulator
+
+Every GEMM of the forward and backward passes (C = A B^T with BF16 operands and FP32
+accumulation in tensor memory) is sbx_mlp_gemm_bf16 with all ensemble members in one
+launch (blockIdx.z); the epilogues write the BF16 activations, their transposes (the
+operands of the weight-gradient GEMMs) and the FP32 pre-activations. The GELU backward,
+bias gradients, loss gradient and Adam (FP32 master weights, BF16 copies and transposes)
+are the library's elementwise kernels. Torch provides the device buffers and the batch
+gathers only.
+
+Shapes are padded for the tensor cores: the 6 inputs to 16 columns and the 3 outputs to
+16 rows of the last weight matrix; the padding stays exactly zero (zero inputs and zero
+output gradients give it zero gradients).
+"""
+import numpy as np
+
+KPAD_IN = 16
+NPAD_OUT = 16
+
+
+class MLPEnsemble:
+    def __init__(self, n_nets=5, dims=(6, 256, 256, 256, 256, 3), batch=256, seed=0, lr=1e-3, device="cuda"):
+        import torch
+        self.torch = torch
+        self.nz, self.dims, self.B, self.lr = n_nets, tuple(dims), batch, lr
+        self.L = len(dims) - 1
+        self.nin, self.nout = dims[0], dims[-1]
+        self.Kp = [KPAD_IN] + [dims[l] for l in range(1, self.L)]
+        self.Np = [dims[l + 1] for l in range(self.L - 1)] + [NPAD_OUT]
+        self.dev = device
+        self.step_no = 0
+        rng = np.random.default_rng(seed)
+        f32 = dict(dtype=torch.float32, device=device)
+        i16 = dict(dtype=torch.int16, device=device)
+        self.W, self.Wb, self.WbT, self.b = [], [], [], []
+        self.mW, self.vW, self.mb, self.vb, self.dW, self.db = [], [], [], [], [], []
+        for l in range(self.L):
+            fin, fout = dims[l], dims[l + 1]
+            w = np.zeros((n_nets, self.Np[l], self.Kp[l]), np.float32)
+            w[:, :fout, :fin] = rng.uniform(-1, 1, (n_nets, fout, fin)) * np.sqrt(3.0 / fin)
+            bb = np.zeros((n_nets, self.Np[l]), np.float32)
+            self.W.append(torch.from_numpy(w).to(device))
+            self.b.append(torch.from_numpy(bb).to(device))
+            self.Wb.append(torch.zeros((n_nets, self.Np[l], self.Kp[l]), **i16))
+            self.WbT.append(torch.zeros((n_nets, self.Kp[l], self.Np[l]), **i16))
+            for lst in (self.mW, self.vW, self.dW):
+                lst.append(torch.zeros((n_nets, self.Np[l], self.Kp[l]), **f32))
+            for lst in (self.mb, self.vb, self.db):
+                lst.append(torch.zeros((n_nets, self.Np[l]), **f32))
+        self._refresh_bf16()
+        self._alloc(batch)
+        self.x_mean = self.x_std = self.y_mean = self.y_std = None
+        self.err = torch.zeros(1, dtype=torch.int32, device=device)
+        self.graph = None
+
+    # ---------------------------------------------------------------- buffers
+    def _alloc(self, M):
+        t = self.torch
+        f32 = dict(dtype=t.float32, device=self.dev)
+        i16 = dict(dtype=t.int16, device=self.dev)
+        nz = self.nz
+        self.M = M
+        self.X0 = t.zeros((nz, M, KPAD_IN), **i16)
+        self.X0T = t.zeros((nz, KPAD_IN, M), **i16)
+        self.T = t.zeros((nz, M, self.nout), **f32)
+        self.Z = [t.zeros((nz, M, self.Np[l]), **f32) for l in range(self.L)]
+        self.A = [t.zeros((nz, M, self.Np[l]), **i16) for l in range(self.L)]
+        self.AT = [t.zeros((nz, self.Np[l], M), **i16) for l in range(self.L)]
+        self.G = [t.zeros((nz, M, self.Np[l]), **i16) for l in range(self.L)]
+        self.GT = [t.zeros((nz, self.Np[l], M), **i16) for l in range(self.L)]
+        self.dA = [t.zeros((nz, M, self.Kp[l]), **f32) for l in range(self.L)]     # dL / d(input of layer l)
+        self.gout = t.zeros((nz, M, NPAD_OUT), **f32)
+        self.loss = t.zeros(nz, **f32)
+
+    def _ctx(self):
+        from .runtime import default_context
+        return default_context()
+
+    def _refresh_bf16(self):
+        """BF16 copies (and transposes) of the FP32 master weights (at initialisation)."""
+        t = self.torch
+        for l in range(self.L):
+            wb = self.W[l].to(t.bfloat16)
+            self.Wb[l].copy_(wb.view(t.int16))
+            self.WbT[l].copy_(wb.transpose(1, 2).contiguous().view(t.int16))
+
+    # ---------------------------------------------------------------- passes
+    def _gemm(self, M, N, K, A, lda, sA, B, ldb, sB, bias=None, act=0, out=None, outT=None, outF=None, ldt=None):
+        ctx = self._ctx()
+        ctx("sbx_mlp_gemm_bf16", self.nz, M, N, K, A, lda, sA, B, ldb, sB, bias, 0 if bias is None else bias.shape[-1],
+            act, out, N, 0 if out is None else out[0].numel(), outT, ldt or M, 0 if outT is None else outT[0].numel(),
+            outF, N, 0 if outF is None else outF[0].numel(), self.err)
+
+    def forward(self, M=None, keep_t=True):
+        """Forward pass over the staged inputs X0 (M rows)."""
+        M = M or self.M
+        prev, lda = self.X0, KPAD_IN
+        for l in range(self.L):
+            last = l == self.L - 1
+            self._gemm(M, self.Np[l], self.Kp[l], prev, lda, prev[0].numel(), self.Wb[l], self.Kp[l],
+                       self.Wb[l][0].numel(), bias=self.b[l], act=0 if last else 1, out=None if last else self.A[l],
+                       outT=self.AT[l] if (keep_t and not last) else None, outF=self.Z[l])
+            prev, lda = self.A[l], self.Np[l]
+        return self.Z[-1]
+
+    def backward(self):
+        ctx = self._ctx()
+        M, nz = self.M, self.nz
+        self.loss.zero_()
+        ctx("sbx_mlp_mse_grad", nz, M, NPAD_OUT, self.nout, self.Z[-1], self.Z[-1][0].numel(), self.T,
+            self.T[0].numel(), self.gout, self.gout[0].numel(), self.loss)
+        ctx("sbx_mlp_gelu_backward", nz, M, NPAD_OUT, self.gout, None, self.gout[0].numel(), self.G[-1], self.GT[-1],
+            self.G[-1][0].numel(), self.GT[-1][0].numel())
+        for l in range(self.L - 1, -1, -1):
+            N, K = self.Np[l], self.Kp[l]
+            ctx("sbx_mlp_colsum_bf16", nz, M, N, self.G[l], self.G[l][0].numel(), self.db[l], N)
+            # dW_l = G_l^T . A_{l-1}: C[N x K] = GT[N x M] . (A_{l-1}^T)[K x M]^T
+            AprevT = self.X0T if l == 0 else self.AT[l - 1]
+            self._gemm(N, K, M, self.GT[l], M, self.GT[l][0].numel(), AprevT, M, AprevT[0].numel(),
+                       outF=self.dW[l])
+            if l > 0:
+                # dA_{l-1} = G_l . W_l: C[M x K] = G[M x N] . (W_l^T)[K x N]^T
+                self._gemm(M, K, N, self.G[l], N, self.G[l][0].numel(), self.WbT[l], N, self.WbT[l][0].numel(),
+                           outF=self.dA[l])
+                ctx("sbx_mlp_gelu_backward", nz, M, K, self.dA[l], self.Z[l - 1], self.Z[l - 1][0].numel(),
+                    self.G[l - 1], self.GT[l - 1], self.G[l - 1][0].numel(), self.GT[l - 1][0].numel())
+
+    def adam(self):
+        ctx = self._ctx()
+        self.step_no += 1
+        for l in range(self.L):
+            N, K = self.Np[l], self.Kp[l]
+            ctx("sbx_mlp_adam", self.nz, N, K, self.W[l], self.dW[l], self.mW[l], self.vW[l], N * K, self.lr, 0.9,
+                0.999, 1e-8, self.step_no, self.Wb[l], self.WbT[l], N * K, N * K)
+            ctx("sbx_mlp_adam", self.nz, N, 1, self.b[l], self.db[l], self.mb[l], self.vb[l], N, self.lr, 0.9, 0.999,
+                1e-8, self.step_no, None, None, 0, 0)
+
+    # ---------------------------------------------------------------- data
+    def _stage_inputs(self, x):
+        """x: [nz, M, nin] float tensor (normalised) -> X0 and X0T (BF16, padded to 16)."""
+        t = self.torch
+        nz, M = x.shape[0], x.shape[1]
+        xp = t.zeros((nz, M, KPAD_IN), dtype=t.bfloat16, device=self.dev)
+        xp[:, :, :self.nin] = x.to(t.bfloat16)
+        self.X0[:, :M].copy_(xp.view(t.int16))
+        self.X0T[:, :, :M].copy_(xp.transpose(1, 2).contiguous().view(t.int16))
+
+    def set_normalisation(self, X, Y):
+        X = np.asarray(X, np.float64)
+        Y = np.asarray(Y, np.float64)
+        self.x_mean, self.x_std = X.mean(0), X.std(0) + 1e-8
+        self.y_mean, self.y_std = Y.mean(0), Y.std(0) + 1e-8
+
+    def train_step(self, xb, tb):
+        """One Adam step per member on its own batch: xb [nz, B, nin], tb [nz, B, nout]
+        (normalised, device). Returns nothing; the losses stay in self.loss."""
+        self._stage_inputs(xb)
+        self.T.copy_(tb)
+        self.forward()
+        self.backward()
+        self.adam()
+
+    def fit(self, X, Y, epochs=100, seed=0, log=None):
+        """Trains every member on (X, Y) with its own shuffling; returns the loss history."""
+        t = self.torch
+        if self.x_mean is None:
+            self.set_normalisation(X, Y)
+        Xn = t.tensor((np.asarray(X) - self.x_mean) / self.x_std, dtype=t.float32, device=self.dev)
+        Yn = t.tensor((np.asarray(Y) - self.y_mean) / self.y_std, dtype=t.float32, device=self.dev)
+        n = Xn.shape[0]
+        g = t.Generator(device="cpu").manual_seed(seed)
+        hist = []
+        steps = max(1, n // self.B)
+        for ep in range(epochs):
+            perms = t.stack([t.randperm(n, generator=g) for _ in range(self.nz)]).to(self.dev)
+            for s in range(steps):
+                idx = perms[:, s * self.B:(s + 1) * self.B]
+                if idx.shape[1] < self.B:
+                    break
+                self.train_step(Xn[idx], Yn[idx])
+            hist.append(float(self.loss.mean().item()))
+            if log:
+                log(ep, hist[-1])
+        return hist
+
+    def predict(self, X, chunk=65536):
+        """Ensemble mean and standard deviation of the de-normalised outputs for X [P, nin]."""
+        t = self.torch
+        Xn = t.tensor((np.asarray(X) - self.x_mean) / self.x_std, dtype=t.float32, device=self.dev)
+        P = Xn.shape[0]
+        outs = []
+        saved = self.M
+        for c0 in range(0, P, chunk):
+            xc = Xn[c0:c0 + chunk]
+            m = xc.shape[0]
+            if m > self.M:
+                self._alloc(m)
+            self._stage_inputs(xc.unsqueeze(0).expand(self.nz, m, self.nin))
+            y = self.forward(M=m, keep_t=False)[:, :m, :self.nout].clone()
+            outs.append(y)
+        if self.M != saved:
+            self._alloc(saved)
+        y = t.cat(outs, dim=1).cpu().numpy().astype(np.float64) * self.y_std + self.y_mean
+        return y.mean(axis=0), y.std(axis=0), y
+
+
+def fallback_mask(mean, std, threshold=0.10):
+    """Points where any output's ensemble std exceeds `threshold` of its |mean|."""
+    return (std > threshold * np.abs(mean)).any(axis=1)
