@@ -1,0 +1,151 @@
+"""The surrogate sweep end to end: training data from packed batched runs, the MLP
+ensemble trained on the GPU, fresh points predicted with the plain batched simulator as
+the fallback where the ensemble disagrees, and the throughput against the plain per-run
+GPU sweep.
+
+    python -m softbox_b200.sweep_surrogate [--train 1024] [--heldout 512] [--fresh 100000]
+                                           [--steps 2000] [--rods 2000 80000] [--epochs 200]
+
+Points per second are whole-sweep figures for runs of `steps` steps:
+* plain per-run: each point's network advanced alone by the single-network plan (the
+  fused kernel where available), timed on a sample of the points and scaled to the sweep;
+* plain batched: packed batches of up to 256 points (the timed training-data batches);
+* surrogate: ensemble inference for every fresh point plus, for the points whose ensemble
+  standard deviation exceeds the threshold on any output, a plain batched rerun charged at
+  the measured batched cost per point (on the held-out points a fallback point takes its
+  plain result, which gives the error of the whole rule).
+Relative error on an output: mean |prediction - plain run| / mean |plain run| over the
+held-out points.
+"""
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import ensemble
+
+OUTPUTS = ("contraction_rate", "largest_fraction", "stress_pa")
+
+
+def _targets(r):
+    return np.stack([r[k] for k in OUTPUTS], axis=1)
+
+
+def generate(points, steps, sample_every, batch=256):
+    """Plain batched runs of `points` in packs of `batch`; returns targets and GPU seconds."""
+    ys, gpu_s, build_s = [], 0.0, 0.0
+    for b0 in range(0, len(points), batch):
+        r = ensemble.run_ensemble(points[b0:b0 + batch], steps, sample_every)
+        ys.append(_targets(r))
+        gpu_s += r["gpu_ms"] * 1e-3
+        build_s += r["build_s"]
+    return np.concatenate(ys), gpu_s, build_s
+
+
+def per_run_seconds(points, steps, sample=8):
+    """Mean GPU seconds of one point's run alone (single-network plan, auto path)."""
+    import torch
+    from .engine import DenseNetwork
+    from . import scenes
+    secs = []
+    for p in points[:sample]:
+        net = DenseNetwork(scenes.dense_contractile(ensemble.point_config(p)), fp64_coords=True)
+        net.run(0, 3)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(True), torch.cuda.Event(True)
+        s.record()
+        net.run(3, steps)
+        e.record()
+        torch.cuda.synchronize()
+        secs.append(s.elapsed_time(e) * 1e-3)
+        net.close()
+    return float(np.mean(secs)), secs
+
+
+def rel_error(pred, true):
+    return (np.abs(pred - true).mean(axis=0) / np.maximum(np.abs(true).mean(axis=0), 1e-30)).tolist()
+
+
+def main():
+    import torch
+    from .surrogate import MLPEnsemble, fallback_mask
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train", type=int, default=1024)
+    ap.add_argument("--heldout", type=int, default=512)
+    ap.add_argument("--fresh", type=int, default=100000)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--sample-every", type=int, default=250)
+    ap.add_argument("--rods", type=int, nargs=2, default=list(ensemble.RODS_RANGE))
+    ap.add_argument("--epochs", type=int, default=200)
+    ap.add_argument("--threshold", type=float, default=0.10)
+    ap.add_argument("--floor", type=float, default=0.0,
+                    help="also report the rule with |mean| floored at this fraction of each output's training spread")
+    ap.add_argument("--per-run-sample", type=int, default=8)
+    ap.add_argument("--seed", type=int, default=11)
+    a = ap.parse_args()
+    rr = tuple(a.rods)
+    pts_train = ensemble.sample_points(a.train, a.seed, rr)
+    pts_held = ensemble.sample_points(a.heldout, a.seed + 1, rr)
+    pts_fresh = ensemble.sample_points(a.fresh, a.seed + 2, rr)
+
+    y_train, gen_gpu_s, gen_build_s = generate(pts_train, a.steps, a.sample_every)
+    y_held, held_gpu_s, _ = generate(pts_held, a.steps, a.sample_every)
+    batched_s_per_point = (gen_gpu_s + held_gpu_s) / (a.train + a.heldout)
+
+    x_train = ensemble.features(pts_train, rr)
+    x_held = ensemble.features(pts_held, rr)
+    ens = MLPEnsemble(n_nets=5, seed=a.seed)
+    t0 = time.perf_counter()
+    hist = ens.fit(x_train, y_train, epochs=a.epochs)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+
+    mean_h, std_h, _ = ens.predict(x_held)
+    fb_h = fallback_mask(mean_h, std_h, a.threshold)
+    blended = np.where(fb_h[:, None], y_held, mean_h)          # fallback points take the plain result
+    err_surrogate = rel_error(mean_h, y_held)
+    err_with_fallback = rel_error(blended, y_held)
+    err_mean_predictor = rel_error(np.broadcast_to(y_train.mean(axis=0), y_held.shape), y_held)
+
+    x_fresh = ensemble.features(pts_fresh, rr)
+    ens.predict(x_fresh[:1024])                                 # warm-up of the inference buffers
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    mean_f, std_f, _ = ens.predict(x_fresh)
+    torch.cuda.synchronize()
+    infer_s = time.perf_counter() - t0
+    fb_f = fallback_mask(mean_f, std_f, a.threshold)
+    n_fb = int(fb_f.sum())
+    surrogate_s = infer_s + n_fb * batched_s_per_point
+
+    floored = {}
+    if a.floor > 0:
+        scale = a.floor * y_train.std(axis=0)
+        fbh2 = (std_h > a.threshold * np.maximum(np.abs(mean_h), scale)).any(axis=1)
+        fbf2 = (std_f > a.threshold * np.maximum(np.abs(mean_f), scale)).any(axis=1)
+        s2 = infer_s + int(fbf2.sum()) * batched_s_per_point
+        floored = {"floor": a.floor, "fallback_fraction": float(fbf2.mean()),
+                   "heldout_fallback_fraction": float(fbh2.mean()),
+                   "heldout_rel_error_with_fallback": rel_error(np.where(fbh2[:, None], y_held, mean_h), y_held),
+                   "surrogate_sweep_points_per_s": a.fresh / s2}
+    run_s, run_samples = per_run_seconds(pts_fresh, a.steps, a.per_run_sample)
+    out = {"steps_per_run": a.steps, "rods_range": rr, "train_points": a.train, "heldout_points": a.heldout,
+           "fresh_points": a.fresh, "outputs": OUTPUTS,
+           "plain_per_run_points_per_s": 1.0 / run_s, "per_run_sample_s": run_samples,
+           "plain_batched_points_per_s": 1.0 / batched_s_per_point,
+           "surrogate_inference_points_per_s": a.fresh / infer_s,
+           "fallback_fraction": n_fb / a.fresh, "threshold": a.threshold,
+           "surrogate_sweep_points_per_s": a.fresh / surrogate_s,
+           "gain_vs_plain_per_run": (a.fresh / surrogate_s) * run_s,
+           "gain_vs_plain_batched": (a.fresh / surrogate_s) * batched_s_per_point,
+           "heldout_rel_error_surrogate": err_surrogate, "heldout_rel_error_with_fallback": err_with_fallback,
+           "heldout_rel_error_mean_predictor": err_mean_predictor, "heldout_fallback_fraction": float(fb_h.mean()),
+           "floored_rule": floored,
+           "train_loss_first_last": [hist[0], hist[-1]], "train_s": train_s, "epochs": a.epochs,
+           "data_gpu_s": gen_gpu_s + held_gpu_s, "data_build_s": gen_build_s}
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()
