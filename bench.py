@@ -248,6 +248,9 @@ def run_ours(args):
                "sample": f"{args.cpu_steps} full steps of the workload on 1 host core ({dt:.1f} s), C++ "
                          f"restatement of the Java System classes' single-threaded -cpu runner"}
     clocks = clk.summary()
+    sweep = None
+    if ws == 1 and args.sweep_points > 0:
+        sweep = sweep_measure(args.sweep_points, args.sweep_steps)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "rod-steps/s", "n_gpus": ws, "steps": args.steps,
                 "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -264,11 +267,41 @@ def run_ours(args):
                 "e2e": {"value": e2e, "unit": "rod-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": args.steps,
                 "clocks": clocks,
-                "step_ms_median": float(np.median(step_ms)), "step_ms_p90": float(np.percentile(step_ms, 90))}
+                "step_ms_median": float(np.median(step_ms)), "step_ms_p90": float(np.percentile(step_ms, 90)),
+                "sweep": sweep}
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def sweep_measure(n_points, steps, run_steps=50000):
+    """The sweep side of the metric on this box: one packed batch of sampled sweep points
+    advanced `steps` steps (CUDA events), extrapolated to sweep runs of `run_steps` steps,
+    and the surrogate ensemble's inference rate (5 x 6-256x4-3 MLPs, tensor-core GEMMs) on
+    100,000 points. The surrogate's error and fallback fraction come from the full pipeline
+    (python -m softbox_b200.sweep_surrogate; profiles/surrogate_sweep.md)."""
+    import torch
+    from softbox_b200 import ensemble
+    from softbox_b200.surrogate import MLPEnsemble
+    pts = ensemble.sample_points(n_points, seed=1)
+    r = ensemble.run_ensemble(pts, steps, sample_every=steps)
+    ens = MLPEnsemble(n_nets=5, seed=0)
+    x = ensemble.features(ensemble.sample_points(100000, seed=2))
+    ens.set_normalisation(x, np.zeros((1, 3)))
+    ens.predict(x[:1024])
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(True), torch.cuda.Event(True)
+    s.record()
+    ens.predict(x)
+    e.record()
+    torch.cuda.synchronize()
+    infer_s = s.elapsed_time(e) / 1e3
+    return {"points": n_points, "rods": r["rods"], "bodies": r["bodies"], "steps_timed": steps,
+            "ms_per_packed_step": r["ms_per_step"], "rod_steps_per_s": r["rods"] / (r["ms_per_step"] / 1e3),
+            "batched_points_per_s_at_run_steps": n_points / (r["ms_per_step"] / 1e3 * run_steps),
+            "run_steps": run_steps, "surrogate_inference_points_per_s": 100000 / infer_s,
+            "surrogate_error_source": "profiles/surrogate_sweep.md"}
 
 
 def main():
@@ -279,6 +312,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=600)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--sweep-points", type=int, default=32, help="packed sweep points timed beside the step (0: off)")
+    ap.add_argument("--sweep-steps", type=int, default=200)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

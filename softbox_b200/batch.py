@@ -18,6 +18,7 @@ import numpy as np
 
 from . import abi_types as T
 from . import device as D
+from .device import DeviceFill
 
 I32, F32 = np.int32, np.float32
 
@@ -136,15 +137,16 @@ def pack_networks(scenes_):
 
     cap = NS + NM
     chunk = 512
-    grid = {"cap": cap, "totalCells": NC, "center": np.zeros(3 * cap, F32), "boundingRadius": np.zeros(cap, F32),
-            "ownerStore": np.full(cap, -1, I32), "ownerSlot": np.full(cap, -1, I32),
-            "gridParams": S[0]["grid"]["gridParams"].copy(),
+    # per-step scratch lives on the device only
+    grid = {"cap": cap, "totalCells": NC, "center": DeviceFill(3 * cap, 0, F32),
+            "boundingRadius": DeviceFill(cap, 0, F32), "ownerStore": DeviceFill(cap, -1, I32),
+            "ownerSlot": DeviceFill(cap, -1, I32), "gridParams": S[0]["grid"]["gridParams"].copy(),
             "viewParams": _same([s["grid"]["viewParams"] for s in S], "grid.viewParams"),
             "gridDims": np.array([0, 0, 0, NC], I32), "gridCounts": np.array([0, cap, 0, 0], I32),
-            "bodyCell": np.full(cap, -1, I32), "cellCount": np.zeros(NC, I32),
-            "chunkSum": np.zeros((NC + chunk - 1) // chunk + 1, I32), "gridCellOffsets": np.zeros(NC + 1, I32),
-            "gridCellContents": np.full(cap, -1, I32),
-            "reachSeg": np.full(NM * 256, -1, I32), "reachCount": np.zeros(NM, I32)}
+            "bodyCell": DeviceFill(cap, -1, I32), "cellCount": DeviceFill(NC, 0, I32),
+            "chunkSum": DeviceFill((NC + chunk - 1) // chunk + 1, 0, I32),
+            "gridCellOffsets": DeviceFill(NC + 1, 0, I32), "gridCellContents": DeviceFill(cap, -1, I32),
+            "reachSeg": DeviceFill(NM * 256, -1, I32), "reachCount": DeviceFill(NM, 0, I32)}
 
     xon = {int(s["xlinkOn"]) for s in S}
     xun = {int(s["xlUnbind"]) for s in S}

@@ -10,12 +10,23 @@ import numpy as np
 from . import abi_types as T
 
 
+class DeviceFill:
+    """A scratch array that exists only on the device: to_device creates it filled with
+    `value` (no host copy, no transfer)."""
+
+    def __init__(self, n, value, dtype):
+        self.n, self.value, self.dtype = int(n), value, np.dtype(dtype)
+
+
 def to_device(obj, device="cuda"):
     import torch
     if isinstance(obj, dict):
         return {k: to_device(v, device) for k, v in obj.items()}
     if isinstance(obj, np.ndarray):
         return torch.from_numpy(np.ascontiguousarray(obj)).to(device)
+    if isinstance(obj, DeviceFill):
+        tdt = {np.dtype(np.int32): torch.int32, np.dtype(np.float32): torch.float32}[obj.dtype]
+        return torch.full((obj.n,), obj.value, dtype=tdt, device=device)
     return obj
 
 

@@ -86,7 +86,12 @@ def point_config(p, cell_scale=1.0):
 
 def build_batch(points, cell_scale=1.0):
     from .batch import pack_networks
-    nets = [scenes.dense_contractile(point_config(p, cell_scale)) for p in points]
+    nets = []
+    for p in points:
+        sc = scenes.dense_contractile(point_config(p, cell_scale))
+        for k in ("reachSeg", "center", "gridCellContents", "bodyCell", "cellCount", "gridCellOffsets"):
+            sc["grid"].pop(k, None)                 # per-step scratch: the packed scene makes its own
+        nets.append(sc)
     return pack_networks(nets)
 
 
