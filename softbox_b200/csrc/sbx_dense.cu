@@ -94,9 +94,18 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
     else
         CHK(sbx_nucleotide_cycle(ctx, nM, mot.nucleotideState, mot.boundSeg, mot.forceDotHist, mot.nucParams,
                                  mot.counts));
-    // (ii) minifilament structure
-    CHK(sbx_zero_accumulators(ctx, nB, b.forceSum, b.torqueSum));
-    CHK(sbx_zero_accumulators(ctx, nBb, bb.forceSum, bb.torqueSum));
+    // (ii) minifilament structure. A single network zeroes and draws in one pass per store
+    // (MechanicsFusion.forceBuild, the same values as the zero + Brownian pair)
+    if (!bt) {
+        CHK(sbx_fusion_force_build(ctx, nB, b.forceSum, b.torqueSum, b.randForce, b.randTorque, b.bTransGam,
+                                   b.bRotGam, b.brownTransScale, b.brownRotScale, mot.bodyParams, mot.counts));
+        CHK(sbx_fusion_force_build(ctx, nBb, bb.forceSum, bb.torqueSum, bb.randForce, bb.randTorque, bb.bTransGam,
+                                   bb.bRotGam, bb.brownTransScale, bb.brownRotScale, mini.bbBodyParams,
+                                   mini.bbCounts));
+    } else {
+        CHK(sbx_zero_accumulators(ctx, nB, b.forceSum, b.torqueSum));
+        CHK(sbx_zero_accumulators(ctx, nBb, bb.forceSum, bb.torqueSum));
+    }
     if (bt) {
         CHK(sbx_brownian_force_batched(ctx, nB, 3, b.randForce, b.randTorque, b.bTransGam, b.bRotGam,
                                        b.brownTransScale, b.brownRotScale, mot.bodyParams, mot.counts, bt->motKey,
@@ -104,11 +113,6 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
         CHK(sbx_brownian_force_batched(ctx, nBb, 1, bb.randForce, bb.randTorque, bb.bTransGam, bb.bRotGam,
                                        bb.brownTransScale, bb.brownRotScale, mini.bbBodyParams, mini.bbCounts,
                                        bt->bbKey, bt->seeds, 1));
-    } else {
-        CHK(sbx_brownian_force(ctx, nB, b.randForce, b.randTorque, b.bTransGam, b.bRotGam, b.brownTransScale,
-                               b.brownRotScale, mot.bodyParams, mot.counts));
-        CHK(sbx_brownian_force(ctx, nBb, bb.randForce, bb.randTorque, bb.bTransGam, bb.bRotGam, bb.brownTransScale,
-                               bb.brownRotScale, mini.bbBodyParams, mini.bbCounts));
     }
     CHK(sbx_motor_joints(ctx, nB, b.coord, b.uVec, b.segLength, b.bTransGam, b.bRotGam, b.forceSum, b.torqueSum,
                          mot.nucleotideState, mot.jointParams));
@@ -125,29 +129,38 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
                                 fb.bRotGam, fb.segLength, mot.boundSeg, mot.bindArc, mot.nucleotideState, sc->bondData,
                                 sc->xbParams));
     CHK(sbx_xbridge_apply_head_force(ctx, nB, sc->bondData, b.forceSum, b.torqueSum));
-    CHK(sbx_integrate(ctx, nB, b.coord, b.coord64, b.uVec, b.yVec, b.forceSum, b.torqueSum, b.randForce, b.randTorque,
-                      b.bTransGam, b.bRotGam, mot.bodyParams));
-    if (bt)
+    if (bt) {
+        CHK(sbx_integrate(ctx, nB, b.coord, b.coord64, b.uVec, b.yVec, b.forceSum, b.torqueSum, b.randForce,
+                          b.randTorque, b.bTransGam, b.bRotGam, mot.bodyParams));
         CHK(sbx_confine_batched(ctx, nBb, bb.coord, bb.uVec, bb.segLength, bb.bTransGam, bb.forceSum, bb.torqueSum,
                                 bt->boxParams, mini.bbCounts, bt->bbKey));
-    else
-        CHK(sbx_confine(ctx, nBb, bb.coord, bb.uVec, bb.segLength, bb.bTransGam, bb.forceSum, bb.torqueSum,
-                        sc->boxParams, mini.bbCounts));
-    CHK(sbx_integrate(ctx, nBb, bb.coord, bb.coord64, bb.uVec, bb.yVec, bb.forceSum, bb.torqueSum, bb.randForce,
-                      bb.randTorque, bb.bTransGam, bb.bRotGam, mini.bbBodyParams));
-    CHK(sbx_derive(ctx, nB, b.coord, b.uVec, b.yVec, b.zVec, b.end1, b.end2, b.segLength));
-    CHK(sbx_derive(ctx, nBb, bb.coord, bb.uVec, bb.yVec, bb.zVec, bb.end1, bb.end2, bb.segLength));
+        CHK(sbx_integrate(ctx, nBb, bb.coord, bb.coord64, bb.uVec, bb.yVec, bb.forceSum, bb.torqueSum, bb.randForce,
+                          bb.randTorque, bb.bTransGam, bb.bRotGam, mini.bbBodyParams));
+        CHK(sbx_derive(ctx, nB, b.coord, b.uVec, b.yVec, b.zVec, b.end1, b.end2, b.segLength));
+        CHK(sbx_derive(ctx, nBb, bb.coord, bb.uVec, bb.yVec, bb.zVec, bb.end1, bb.end2, bb.segLength));
+    } else {
+        // MechanicsFusion.integDerive / integDeriveConfined: confine, integrate and derive in one
+        // pass per store, in that order (the same values as the separate kernels)
+        CHK(sbx_fusion_integ_derive(ctx, nB, b.coord, b.coord64, b.uVec, b.yVec, b.zVec, b.segLength, b.end1,
+                                    b.end2, b.forceSum, b.torqueSum, b.randForce, b.randTorque, b.bTransGam,
+                                    b.bRotGam, mot.bodyParams));
+        CHK(sbx_fusion_integ_derive_confined(ctx, nBb, bb.coord, bb.coord64, bb.uVec, bb.yVec, bb.zVec, bb.segLength,
+                                             bb.end1, bb.end2, bb.forceSum, bb.torqueSum, bb.randForce,
+                                             bb.randTorque, bb.bTransGam, bb.bRotGam, sc->boxParams,
+                                             mini.bbCounts));
+    }
     CHK(sbx_xbridge_register_force_dot(ctx, nM, sc->bondData, mot.boundSeg, mot.forceDotFil, mot.forceMag,
                                        mot.forceDotHist, mot.forceDotPlace));
     // (iii)-(v) filaments
-    CHK(sbx_zero_accumulators(ctx, nSeg, fb.forceSum, fb.torqueSum));
-    if (bt)
+    if (bt) {
+        CHK(sbx_zero_accumulators(ctx, nSeg, fb.forceSum, fb.torqueSum));
         CHK(sbx_brownian_force_batched(ctx, nSeg, 1, fb.randForce, fb.randTorque, fb.bTransGam, fb.bRotGam,
                                        fb.brownTransScale, fb.brownRotScale, f.params, f.counts, bt->segKey,
                                        bt->seeds, 2));
-    else
-        CHK(sbx_brownian_force(ctx, nSeg, fb.randForce, fb.randTorque, fb.bTransGam, fb.bRotGam, fb.brownTransScale,
-                               fb.brownRotScale, f.params, f.counts));
+    } else {
+        CHK(sbx_fusion_force_build(ctx, nSeg, fb.forceSum, fb.torqueSum, fb.randForce, fb.randTorque, fb.bTransGam,
+                                   fb.bRotGam, fb.brownTransScale, fb.brownRotScale, f.params, f.counts));
+    }
     CHK(sbx_chain_forces(ctx, nSeg, fb.coord, fb.uVec, fb.segLength, f.end2NbrSlot, f.end2NbrSide, f.end1NbrSlot,
                          f.end1NbrSide, fb.bTransGam, fb.bRotGam, fb.forceSum, fb.torqueSum, f.chainParams));
     if (xlOn) {
@@ -175,15 +188,17 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
     CHK(sbx_csr_build(ctx, mot.boundSeg, nM, nSeg, sc->segMotorCount, sc->segMotorOffsets, sc->segMotorMyo));
     CHK(sbx_xbridge_seg_gather(ctx, nSeg, sc->segMotorOffsets, sc->segMotorMyo, sc->bondData, fb.forceSum,
                                fb.torqueSum));
-    if (bt)
+    if (bt) {
         CHK(sbx_confine_batched(ctx, nSeg, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.forceSum, fb.torqueSum,
                                 bt->boxParams, f.counts, bt->segKey));
-    else
-        CHK(sbx_confine(ctx, nSeg, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.forceSum, fb.torqueSum,
-                        sc->boxParams, f.counts));
-    CHK(sbx_integrate(ctx, nSeg, fb.coord, fb.coord64, fb.uVec, fb.yVec, fb.forceSum, fb.torqueSum, fb.randForce,
-                      fb.randTorque, fb.bTransGam, fb.bRotGam, f.params));
-    CHK(sbx_derive(ctx, nSeg, fb.coord, fb.uVec, fb.yVec, fb.zVec, fb.end1, fb.end2, fb.segLength));
+        CHK(sbx_integrate(ctx, nSeg, fb.coord, fb.coord64, fb.uVec, fb.yVec, fb.forceSum, fb.torqueSum, fb.randForce,
+                          fb.randTorque, fb.bTransGam, fb.bRotGam, f.params));
+        CHK(sbx_derive(ctx, nSeg, fb.coord, fb.uVec, fb.yVec, fb.zVec, fb.end1, fb.end2, fb.segLength));
+    } else {
+        CHK(sbx_fusion_integ_derive_confined(ctx, nSeg, fb.coord, fb.coord64, fb.uVec, fb.yVec, fb.zVec, fb.segLength,
+                                             fb.end1, fb.end2, fb.forceSum, fb.torqueSum, fb.randForce,
+                                             fb.randTorque, fb.bTransGam, fb.bRotGam, sc->boxParams, f.counts));
+    }
     return SBX_OK;
 }
 

@@ -214,3 +214,34 @@ class MLPEnsemble:
 def fallback_mask(mean, std, threshold=0.10):
     """Points where any output's ensemble std exceeds `threshold` of its |mean|."""
     return (std > threshold * np.abs(mean)).any(axis=1)
+
+
+def main():
+    """Times ensemble inference: python -m softbox_b200.surrogate [--points 100000] [--repeat 5]"""
+    import argparse
+    import json
+    import torch
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--points", type=int, default=100000)
+    ap.add_argument("--repeat", type=int, default=5)
+    a = ap.parse_args()
+    rng = np.random.default_rng(0)
+    x = rng.uniform(size=(a.points, 6))
+    ens = MLPEnsemble()
+    ens.set_normalisation(x, np.zeros((1, 3)))
+    ens.predict(x[:1024])
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(True), torch.cuda.Event(True)
+    s.record()
+    for _ in range(a.repeat):
+        ens.predict(x)
+    e.record()
+    torch.cuda.synchronize()
+    sec = s.elapsed_time(e) / 1e3 / a.repeat
+    flops = 2.0 * a.points * ens.nz * sum(ens.Np[l] * ens.Kp[l] for l in range(ens.L))
+    print(json.dumps({"points": a.points, "nets": ens.nz, "s_per_predict": sec, "points_per_s": a.points / sec,
+                      "gemm_tflops_incl_host": flops / sec / 1e12}), flush=True)
+
+
+if __name__ == "__main__":
+    main()
