@@ -23,6 +23,8 @@ constexpr int NT = 256;              // max columns of a C tile (the MMA's N)
 constexpr int KMAX = 256;            // max contraction length
 constexpr int GEMM_THREADS = 128;
 constexpr long long WAIT_NS = 1000000000LL;
+constexpr int STG_LD = 17;                           // padded row of the epilogue staging (floats)
+constexpr int STG_BYTES = 4 * 2 * 32 * STG_LD * 4;   // 4 warps x (values, activations) x 32 rows
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
@@ -62,40 +64,55 @@ struct GemmArgs {
 };
 
 // rows [r0, r0 + rows) x [0, Kp) of a row-major BF16 matrix into the core-matrix layout;
-// rows past `rowsValid` and columns past K are zero
+// rows past `rowsValid` and columns past K are zero. Aligned 16-byte pieces go by cp.async
+// (every thread keeps all its copies in flight), the rest by plain loads; the caller waits
+// with cp_async_wait_all() before the block barrier.
 __device__ void stage(char* dst, const __nv_bfloat16* src, int ld, int r0, int rows, int rowsValid, int K, int Kp,
                       bool vec) {
     int kg = Kp >> 3;
     for (int u = threadIdx.x; u < rows * kg; u += GEMM_THREADS) {
         int r = u / kg, c = u - r * kg;
-        uint4 v = make_uint4(0, 0, 0, 0);
         int gr = r0 + r, k0 = c * 8;
+        char* d = dst + ((r >> 3) * kg + c) * 128 + (r & 7) * 16;
+        if (gr < rowsValid && vec && k0 + 8 <= K) {
+            const __nv_bfloat16* p = src + (long long)gr * ld + k0;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(d)), "l"(p));
+            continue;
+        }
+        uint4 v = make_uint4(0, 0, 0, 0);
         if (gr < rowsValid) {
             const __nv_bfloat16* p = src + (long long)gr * ld + k0;
-            if (vec && k0 + 8 <= K) {
-                v = *reinterpret_cast<const uint4*>(p);
-            } else {
-                unsigned short h[8];
-                for (int j = 0; j < 8; j++) h[j] = (k0 + j < K) ? __bfloat16_as_ushort(p[j]) : (unsigned short)0;
-                v = make_uint4(h[0] | (unsigned)h[1] << 16, h[2] | (unsigned)h[3] << 16, h[4] | (unsigned)h[5] << 16,
-                               h[6] | (unsigned)h[7] << 16);
-            }
+            unsigned short h[8];
+            for (int j = 0; j < 8; j++) h[j] = (k0 + j < K) ? __bfloat16_as_ushort(p[j]) : (unsigned short)0;
+            v = make_uint4(h[0] | (unsigned)h[1] << 16, h[2] | (unsigned)h[3] << 16, h[4] | (unsigned)h[5] << 16,
+                           h[6] | (unsigned)h[7] << 16);
         }
-        *reinterpret_cast<uint4*>(dst + ((r >> 3) * kg + c) * 128 + (r & 7) * 16) = v;
+        *reinterpret_cast<uint4*>(d) = v;
     }
 }
 
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+// One CTA keeps its B tile (up to 256 x 256 BF16) in shared memory and loops over M tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ...: per tile it stages A, issues the MMA chain into
+// TMEM, waits for the tile's commit (mbarrier phase = tile iteration parity) and runs the
+// epilogue, then syncs before the next tile's MMAs overwrite the accumulators.
 __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm(GemmArgs g) {
     extern __shared__ __align__(1024) char smem[];
     const int z = blockIdx.z;
-    const int m0 = blockIdx.x * MT, n0 = blockIdx.y * NT;
+    const int n0 = blockIdx.y * NT;
     const int nCols = min(NT, g.N - n0);
     const int Np = (nCols + 15) & ~15;             // MMA N: a multiple of 16 for M = 128
     const int Kp = (g.K + 15) & ~15;
+    const int tilesM = (g.M + MT - 1) / MT;
     char* sA = smem;
     char* sB = smem + MT * Kp * 2;
     unsigned long long* mbar = reinterpret_cast<unsigned long long*>(sB + NT * Kp * 2);
     unsigned* tmemSlot = reinterpret_cast<unsigned*>(mbar + 1);
+    float* stage_base = reinterpret_cast<float*>(reinterpret_cast<char*>(mbar) + 16);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned ncolsAlloc = 32;
     while ((int)ncolsAlloc < Np) ncolsAlloc <<= 1;
@@ -111,83 +128,108 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm(GemmArgs g) {
     const __nv_bfloat16* B = g.B + z * g.sB;
     bool vecA = (g.lda % 8 == 0) && (((uintptr_t)A & 15) == 0);
     bool vecB = (g.ldb % 8 == 0) && (((uintptr_t)B & 15) == 0);
-    stage(sA, A, g.lda, m0, MT, g.M, g.K, Kp, vecA);
     stage(sB, B, g.ldb, n0, Np, g.N, g.K, Kp, vecB);
-    asm volatile("fence.proxy.async.shared::cta;");
-    asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    const unsigned tmem = *tmemSlot;
+    const float* bias = g.bias ? g.bias + z * g.sBias : nullptr;
+    __nv_bfloat16* out = g.out ? g.out + z * g.sOut : nullptr;
+    __nv_bfloat16* outT = g.outT ? g.outT + z * g.sOutT : nullptr;
+    float* outF = g.outF ? g.outF + z * g.sOutF : nullptr;
+    // per-warp staging of a 32-row x 16-column chunk, so that the row-major outputs are
+    // written by lanes spanning columns (two rows of 16 per store instruction)
+    float* stV = stage_base + warp * (2 * 32 * STG_LD);
+    float* stA = stV + 32 * STG_LD;
+    bool ok = true;
+    unsigned tmem = 0;
 
-    if (threadIdx.x == 0) {
-        const unsigned idesc = idesc_bf16(MT, Np);
-        const unsigned aBase = smem_u32(sA), bBase = smem_u32(sB);
-        const unsigned sbo = (unsigned)(Kp >> 3) * 128u;
-        for (int kk = 0; kk < Kp / 16; kk++) {
-            unsigned long long ad = kmajor_desc(aBase + kk * 256u, 128u, sbo);
-            unsigned long long bd = kmajor_desc(bBase + kk * 256u, 128u, sbo);
-            unsigned acc = kk > 0 ? 1u : 0u;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-                "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+    int iter = 0;
+    for (int tile = blockIdx.x; tile < tilesM && ok; tile += gridDim.x, iter++) {
+        const int m0 = tile * MT;
+        stage(sA, A, g.lda, m0, MT, g.M, g.K, Kp, vecA);
+        cp_async_wait_all();
+        asm volatile("fence.proxy.async.shared::cta;");
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        tmem = *tmemSlot;
+        if (threadIdx.x == 0) {
+            const unsigned idesc = idesc_bf16(MT, Np);
+            const unsigned aBase = smem_u32(sA), bBase = smem_u32(sB);
+            const unsigned sbo = (unsigned)(Kp >> 3) * 128u;
+            for (int kk = 0; kk < Kp / 16; kk++) {
+                unsigned long long ad = kmajor_desc(aBase + kk * 256u, 128u, sbo);
+                unsigned long long bd = kmajor_desc(bBase + kk * 256u, 128u, sbo);
+                unsigned acc = kk > 0 ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                smem_u32(mbar)));
         }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-            smem_u32(mbar)));
-    }
-    // bounded wait for the MMAs
-    bool ok = false;
-    {
-        long long t0 = gtimer();
-        for (;;) {
-            unsigned done;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
-                "selp.u32 %0, 1, 0, p;\n\t}"
-                : "=r"(done)
-                : "r"(smem_u32(mbar)));
-            if (done) { ok = true; break; }
-            if (gtimer() - t0 > WAIT_NS) break;
+        // bounded wait for this tile's MMAs: phase `iter` of the barrier
+        {
+            const unsigned parity = (unsigned)(iter & 1);
+            bool done_ok = false;
+            long long t0 = gtimer();
+            for (;;) {
+                unsigned done;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                    "selp.u32 %0, 1, 0, p;\n\t}"
+                    : "=r"(done)
+                    : "r"(smem_u32(mbar)), "r"(parity));
+                if (done) { done_ok = true; break; }
+                if (gtimer() - t0 > WAIT_NS) break;
+            }
+            ok = __syncthreads_and(done_ok ? 1 : 0) != 0;   // one verdict for the whole CTA
         }
-    }
-    if (!ok && threadIdx.x == 0 && g.err) atomicOr(g.err, 1);
-    asm volatile("tcgen05.fence::after_thread_sync;");
-
-    if (ok) {
-        const int row = m0 + warp * 32 + lane;
-        const float* bias = g.bias ? g.bias + z * g.sBias : nullptr;
-        __nv_bfloat16* out = g.out ? g.out + z * g.sOut : nullptr;
-        __nv_bfloat16* outT = g.outT ? g.outT + z * g.sOutT : nullptr;
-        float* outF = g.outF ? g.outF + z * g.sOutF : nullptr;
-        for (int c0 = 0; c0 < Np; c0 += 16) {
-            unsigned r[16];
-            unsigned taddr = tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
-                "[%16];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                  "=r"(r[15])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;");
-            if (row < g.M) {
+        if (!ok && threadIdx.x == 0 && g.err) atomicOr(g.err, 1);
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (ok) {
+            const int row = m0 + warp * 32 + lane;
+            for (int c0 = 0; c0 < Np; c0 += 16) {
+                unsigned r[16];
+                unsigned taddr = tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0;
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                    "[%16];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                      "=r"(r[15])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;");
                 for (int j = 0; j < 16; j++) {
                     int n = n0 + c0 + j;
-                    if (n >= g.N) break;
                     float v = __uint_as_float(r[j]);
-                    if (bias) v += bias[n];
-                    if (outF) outF[(long long)row * g.ldf + n] = v;
+                    if (bias && n < g.N) v += bias[n];
                     float a = g.act ? gelu(v) : v;
-                    __nv_bfloat16 h = __float2bfloat16_rn(a);
-                    if (out) out[(long long)row * g.ldo + n] = h;
-                    if (outT) outT[(long long)n * g.ldt + row] = h;
+                    stV[lane * STG_LD + j] = v;
+                    stA[lane * STG_LD + j] = a;
+                    if (outT && row < g.M && n < g.N) outT[(long long)n * g.ldt + row] = __float2bfloat16_rn(a);
                 }
+                __syncwarp();
+                if (out || outF) {
+                    const int col = lane & 15, n = n0 + c0 + col;
+                    for (int rr = lane >> 4; rr < 32; rr += 2) {
+                        const int orow = m0 + warp * 32 + rr;
+                        if (orow < g.M && n < g.N) {
+                            if (outF) outF[(long long)orow * g.ldf + n] = stV[rr * STG_LD + col];
+                            if (out) out[(long long)orow * g.ldo + n] = __float2bfloat16_rn(stA[rr * STG_LD + col]);
+                        }
+                    }
+                }
+                __syncwarp();
             }
         }
+        // every warp is done with sA and the accumulators before the next tile
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
     }
-    asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncolsAlloc));
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        tmem = *tmemSlot;
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncolsAlloc));
+    }
 }
 
 // dZ = dA * GELU'(Z) (or dA when Z is NULL) -> BF16 row-major and transposed; M x N, per z
@@ -274,15 +316,27 @@ extern "C" sbx_status sbx_mlp_gemm_bf16(sbx_ctx* ctx, int32_t nz, int32_t M, int
     if (M == 0) return SBX_OK;
     static bool attr = false;
     const int Kp = (K + 15) & ~15;
-    size_t smem = (size_t)(MT + NT) * Kp * 2 + 16 + 16;
+    size_t smem = (size_t)(MT + NT) * Kp * 2 + 16 + STG_BYTES;
     if (!attr) {
-        cudaFuncSetAttribute(k_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (MT + NT) * KMAX * 2 + 64);
+        cudaFuncSetAttribute(k_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (MT + NT) * KMAX * 2 + 16 + STG_BYTES);
         attr = true;
     }
     GemmArgs g{M, N, K, (const __nv_bfloat16*)A, lda, strideA, (const __nv_bfloat16*)B, ldb, strideB, bias,
                strideBias, act, (__nv_bfloat16*)out, ldo, strideOut, (__nv_bfloat16*)outT, ldt, strideOutT, outF, ldf,
                strideOutF, errFlag};
-    dim3 grid((M + MT - 1) / MT, (N + NT - 1) / NT, nz);
+    // one wave of CTAs (1 per SM, shared memory bound), each looping over its M tiles with
+    // its B tile resident
+    int sms = 148;
+    {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    const int tilesM = (M + MT - 1) / MT, tilesN = (N + NT - 1) / NT;
+    int gx = sms / (tilesN * nz);                  // a single wave: no SM runs two of them
+    gx = gx < 1 ? 1 : (gx > tilesM ? tilesM : gx);
+    dim3 grid(gx, tilesN, nz);
     SBX_LAUNCH_SMEM(ctx, k_gemm, grid, GEMM_THREADS, smem, g);
     return check_launch(ctx, "sbx_mlp_gemm_bf16");
 }

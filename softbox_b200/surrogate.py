@@ -99,14 +99,16 @@ class MLPEnsemble:
             outF, N, 0 if outF is None else outF[0].numel(), self.err)
 
     def forward(self, M=None, keep_t=True):
-        """Forward pass over the staged inputs X0 (M rows)."""
+        """Forward pass over the staged inputs X0 (M rows); keep_t=False (inference) writes
+        only the activations and the last layer's output."""
         M = M or self.M
         prev, lda = self.X0, KPAD_IN
         for l in range(self.L):
             last = l == self.L - 1
             self._gemm(M, self.Np[l], self.Kp[l], prev, lda, prev[0].numel(), self.Wb[l], self.Kp[l],
                        self.Wb[l][0].numel(), bias=self.b[l], act=0 if last else 1, out=None if last else self.A[l],
-                       outT=self.AT[l] if (keep_t and not last) else None, outF=self.Z[l])
+                       outT=self.AT[l] if (keep_t and not last) else None,
+                       outF=self.Z[l] if (keep_t or last) else None)
             prev, lda = self.A[l], self.Np[l]
         return self.Z[-1]
 

@@ -49,11 +49,9 @@ def test_batched_equals_each_network_alone(mode):
 
 
 def test_batched_launches_per_step_do_not_grow_with_networks():
-    from softbox_b200.engine import DenseNetwork
     nets = _nets()
-    one = DenseNetwork(nets[0])
-    packed, info = batch.pack_networks(nets)
-    ens = batch.BatchedNetworks(packed, info)
+    one = batch.BatchedNetworks(*batch.pack_networks(nets[:1]))
+    ens = batch.BatchedNetworks(*batch.pack_networks(nets))
     assert ens.kernels_per_step == one.kernels_per_step
     one.close()
     ens.close()
