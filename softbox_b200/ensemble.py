@@ -195,3 +195,36 @@ def main():
 
 if __name__ == "__main__":
     main()
+
+
+def run_sharded(points, steps, sample_every, runner=None, **kw):
+    """A sweep over all ranks of the default process group: rank r runs points r, r + N,
+    ... (one packed batch per rank), then the per-point outputs are gathered once and put
+    back in the points' order. Without a process group it is `runner` on all points."""
+    runner = runner or run_ensemble
+    try:
+        import torch.distributed as dist
+        ws = dist.get_world_size() if dist.is_available() and dist.is_initialized() else 1
+        rank = dist.get_rank() if ws > 1 else 0
+    except Exception:
+        ws, rank = 1, 0
+    if ws == 1:
+        return runner(points, steps, sample_every, **kw)
+    mine = list(range(rank, len(points), ws))
+    r = runner([points[i] for i in mine], steps, sample_every, **kw) if mine else None
+    part = {"index": mine}
+    if r is not None:
+        for k in ("contraction_rate", "largest_fraction", "stress_pa"):
+            part[k] = np.asarray(r[k]).tolist()
+        part["gpu_ms"] = float(r.get("gpu_ms", 0.0))
+    parts = [None] * ws
+    dist.all_gather_object(parts, part)
+    out = {k: np.zeros(len(points)) for k in ("contraction_rate", "largest_fraction", "stress_pa")}
+    gpu_ms = 0.0
+    for p in parts:
+        for j, i in enumerate(p["index"]):
+            for k in out:
+                out[k][i] = p[k][j]
+        gpu_ms = max(gpu_ms, p.get("gpu_ms", 0.0))
+    out["gpu_ms_max_over_ranks"] = gpu_ms
+    return out
