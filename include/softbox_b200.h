@@ -586,8 +586,9 @@ typedef struct sbx_dense_plan sbx_dense_plan;
  * the DenseContractileHarness.cpuStep order. */
 sbx_status sbx_dense_plan_create(sbx_ctx* ctx, const sbx_dense_scene* scene, sbx_dense_plan** out);
 /* Advances steps t0, t0+1, ..., t0+nsteps-1 (the step index feeds every RNG key and
- * the containment cadence). mode 0: the per-system call sequence; 1: one CUDA-graph
- * replay per step of that sequence; 2: the fused persistent kernel (all nsteps in one
+ * the containment cadence). mode 0: the call sequence of the per-system entry points
+ * (zero + draws and confine + integrate + derive as the MechanicsFusion passes, which give
+ * the same values); 1: one CUDA-graph replay per step of that sequence; 2: the fused persistent kernel (all nsteps in one
  * cooperative launch; available when the scene has the harness layout, see
  * sbx_dense_plan_fused_available). All three give the same bits. mode 3 (auto): the fused
  * kernel up to SBX_DENSE_AUTO_MAX_FUSED_RODS rods when available, the graph path above it,

@@ -318,13 +318,15 @@ __device__ __forceinline__ void store3(float* a, int n, int i, const float v[3])
 }
 
 // integrate one slot in place; writes coord (and coord64 when given), uVec, yVec
-__device__ __forceinline__ void integrate_slot(int n, int i, float* coord, double* coord64, float* uVec, float* yVec,
-                                               const float* F, const float* T, const float* rF, const float* rT,
-                                               const float* bTG, const float* bRG, float dt, Pose& q) {
+// integration of slot i with its force and torque sums already in registers
+__device__ __forceinline__ void integrate_slot_ft(int n, int i, float* coord, double* coord64, float* uVec,
+                                                  float* yVec, const float f[3], const float t[3], const float* rF,
+                                                  const float* rT, const float* bTG, const float* bRG, float dt,
+                                                  Pose& q) {
     Pose p;
     load3(coord, n, i, p.c); load3(uVec, n, i, p.u); load3(yVec, n, i, p.y);
-    float f[3], t[3], rf[3], rt[3], gT[3], gR[3], dc[3];
-    load3(F, n, i, f); load3(T, n, i, t); load3(rF, n, i, rf); load3(rT, n, i, rt);
+    float rf[3], rt[3], gT[3], gR[3], dc[3];
+    load3(rF, n, i, rf); load3(rT, n, i, rt);
     load3(bTG, n, i, gT); load3(bRG, n, i, gR);
     integrate_pose(p, f, t, rf, rt, gT, gR, dt, q, dc);
     if (coord64) {
@@ -335,6 +337,14 @@ __device__ __forceinline__ void integrate_slot(int n, int i, float* coord, doubl
         }
     }
     store3(coord, n, i, q.c); store3(uVec, n, i, q.u); store3(yVec, n, i, q.y);
+}
+
+__device__ __forceinline__ void integrate_slot(int n, int i, float* coord, double* coord64, float* uVec, float* yVec,
+                                               const float* F, const float* T, const float* rF, const float* rT,
+                                               const float* bTG, const float* bRG, float dt, Pose& q) {
+    float f[3], t[3];
+    load3(F, n, i, f); load3(T, n, i, t);
+    integrate_slot_ft(n, i, coord, coord64, uVec, yVec, f, t, rF, rT, bTG, bRG, dt, q);
 }
 
 __global__ void k_integrate(int n, float* coord, double* coord64, float* uVec, float* yVec, const float* F,
@@ -469,6 +479,7 @@ extern "C" sbx_status sbx_fusion_integ_derive_confined(sbx_ctx* ctx, int32_t n, 
                F, T, rF, rT, bTG, bRG, boxParams, counts);
     return check_launch(ctx, "sbx_fusion_integ_derive_confined");
 }
+
 
 // ============================================================================ chain
 // ChainBendingForceSystem.chainForces (ChainBendingForceSystem.java:105-331), one thread per
