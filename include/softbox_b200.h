@@ -461,6 +461,66 @@ sbx_status sbx_birth_tag_seeds(sbx_ctx* ctx, int32_t K, int32_t C, const int32_t
 /* pool.take(min(rankOffsets[K], freeOffsets[C]) * monomersPerBirth) (FullSystemDemoHarness.java:689-691) */
 sbx_status sbx_actin_pool_take_births(sbx_ctx* ctx, sbx_actin_pool* pool, const int32_t* rankOffsets, int32_t K,
                                       const int32_t* freeOffsets, int32_t C, int32_t monomersPerBirth);
+/* Turnover of packed networks (each network's filament slots a contiguous range): the
+ * kernels above with the network looked up per slot or request — draws keyed by the local
+ * index and the network's seed, rates from the network's table row, one pool per network —
+ * and a segmented allocator (a network's slice of the global free list and request ranks
+ * found at its base index). Each network gets exactly its run alone. Kernels without
+ * rates, draws or allocation (apply_death, release_dead, mark_splits, recompute_drag,
+ * growth_atp, filid_*, the scans) run unchanged over the packed arrays. */
+typedef struct sbx_turnover_batch {
+    int32_t nNet;
+    const int32_t* slotKey;               /* (network, local slot) per filament slot */
+    const int32_t* slotBase;              /* nNet + 1 slot offsets */
+    const int32_t* seeds;                 /* nNet turnover RNG seeds */
+    float* growParams;                    /* nNet x 3; [0] written by sbx_tb_begin */
+    const float* depolyParams;            /* nNet x 3 */
+    const float* depolyRateParams;        /* nNet x 2 */
+    const float* agingParams;             /* nNet x 2 */
+    const float* cofilinParams;           /* nNet x 2 */
+    const float* birthBox;                /* nNet x 4 (half-widths, monomers per newborn) */
+    const double* onRate;                 /* nNet growth on-rates (per uM per s) */
+    sbx_actin_pool* pools;                /* nNet */
+    const int32_t* birthNet;              /* network of each birth request */
+    const int32_t* birthBase;             /* nNet + 1 birth-request offsets */
+} sbx_turnover_batch;
+sbx_status sbx_tb_begin(sbx_ctx* ctx, const sbx_turnover_batch* tb, int32_t fires, double biochemDeltaT);
+sbx_status sbx_tb_grow(sbx_ctx* ctx, const sbx_turnover_batch* tb, int32_t C, const int32_t* seedNode,
+                       int32_t* monomerCount, float* coord, const float* uVec, int32_t* grewFlag,
+                       const int32_t* growCounts);
+sbx_status sbx_tb_depoly_proxy(sbx_ctx* ctx, const sbx_turnover_batch* tb, int32_t C, const int32_t* filState,
+                               int32_t* monomerCount, float* coord, const float* uVec, const int32_t* end1NbrSlot,
+                               const float* nucFrac, int32_t* returnedMon, int32_t* deathFlag,
+                               const int32_t* depolyCounts);
+sbx_status sbx_tb_age(sbx_ctx* ctx, const sbx_turnover_batch* tb, int32_t C, const int32_t* filState, float* nucFrac,
+                      const int32_t* agingCounts);
+/* dissolve 0: cofilinAccumulate, 1: cofilinDissolve */
+sbx_status sbx_tb_cofilin(sbx_ctx* ctx, const sbx_turnover_batch* tb, int32_t C, int32_t dissolve,
+                          const int32_t* filState, const float* nucFrac, float* cofFrac, const int32_t* monomerCount,
+                          int32_t* severDeathFlag, int32_t* severReturnedMon, const int32_t* severCounts);
+/* per network: put (take 0) or take (1) its slice total of a slot scan */
+sbx_status sbx_tb_pool(sbx_ctx* ctx, const sbx_turnover_batch* tb, const int32_t* offsets, int32_t take);
+sbx_status sbx_tb_split_wire(sbx_ctx* ctx, const sbx_turnover_batch* tb, int32_t C, const int32_t* rankOffsets,
+                             const int32_t* freeList, const int32_t* freeOffsets, int32_t* monomerCount, float* coord,
+                             const float* uVec, int32_t* end1NbrSlot, int32_t* end1NbrSide, int32_t* end2NbrSlot,
+                             int32_t* end2NbrSide, int32_t* seedNode, const float* splitParams);
+/* space 0: requests are slots (splits), 1: birth requests; what 0 fresh cofilin, 1 fresh
+ * ATP, 2 split inherit (space 0) */
+sbx_status sbx_tb_formed_init(sbx_ctx* ctx, const sbx_turnover_batch* tb, int32_t space, int32_t K, int32_t C,
+                              const int32_t* rankOffsets, const int32_t* freeList, const int32_t* freeOffsets,
+                              float* a, int32_t what);
+sbx_status sbx_tb_birth_allocate(sbx_ctx* ctx, const sbx_turnover_batch* tb, int32_t space, int32_t K, int32_t C,
+                                 int32_t reqCap, const float* reqCoord, const float* reqUVec, const float* reqYVec,
+                                 const int32_t* rankOffsets, const int32_t* freeList, const int32_t* freeOffsets,
+                                 float* coord, float* uVec, float* yVec, float* brownTransScale, float* brownRotScale,
+                                 int32_t* filState, const float* birthParams);
+sbx_status sbx_tb_birth_emit(sbx_ctx* ctx, const sbx_turnover_batch* tb, int32_t R, int32_t step, int32_t* acceptFlag,
+                             float* reqCoord, float* reqUVec, float* reqYVec);
+sbx_status sbx_tb_newborn(sbx_ctx* ctx, const sbx_turnover_batch* tb, int32_t R, const int32_t* rankOffsets,
+                          const int32_t* freeList, const int32_t* freeOffsets, int32_t* monomerCount, float* segLength,
+                          int32_t* seedNode, const float* seedParams);
+sbx_status sbx_tb_pool_births(sbx_ctx* ctx, const sbx_turnover_batch* tb, const int32_t* rankOffsets,
+                              const int32_t* freeOffsets, int32_t monomersPerBirth);
 /* FilIDSystem.init (FilIDSystem.java:38-47): ptr = end2 neighbour (self at a chain end, -s-2 when FREE) */
 sbx_status sbx_filid_init(sbx_ctx* ctx, int32_t n, const int32_t* filState, const int32_t* end2NbrSlot,
                           int32_t* ptr);

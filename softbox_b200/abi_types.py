@@ -94,3 +94,10 @@ def fill(struct, arrays, prefix=""):
 class BatchDesc(C.Structure):           # packed networks (sbx_batch)
     _fields_ = [("nNet", C.c_int32)] + [(k, i32p) for k in ("segKey", "motKey", "bbKey", "linkKey", "seeds")] + [
         ("gridParams", f32p), ("gridDims", i32p), ("boxParams", f32p)]
+
+
+class TurnoverBatchDesc(C.Structure):   # packed-network turnover tables (sbx_turnover_batch)
+    _fields_ = [("nNet", C.c_int32), ("slotKey", i32p), ("slotBase", i32p), ("seeds", i32p), ("growParams", f32p),
+                ("depolyParams", f32p), ("depolyRateParams", f32p), ("agingParams", f32p),
+                ("cofilinParams", f32p), ("birthBox", f32p), ("onRate", f64p), ("pools", f64p),
+                ("birthNet", i32p), ("birthBase", i32p)]

@@ -170,7 +170,57 @@ def pack_networks(scenes_):
     info = {"nNet": len(S), "seg": sB, "mot": mB, "bb": bbB, "dim": dB, "link": _bases(nL), "cells": cB,
             "nS": nS, "nM": nM, "nBb": nBb, "nD": nD, "nL": nL}
     packed["batch"] = batch
+    if all("turnover" in s for s in S):
+        _pack_turnover(S, packed, info)
     return packed, info
+
+
+def _pack_turnover(S, packed, info):
+    """The networks' turnover arrays packed like their filament stores, plus the per-network
+    tables of sbx_turnover_batch (rates, seeds, pools, birth request ranges)."""
+    T_ = [s["turnover"] for s in S]
+    cfgs = [s["tcfg"] for s in S]
+    if len({c.check_int for c in cfgs}) != 1 or len({c.polyboost for c in cfgs}) != 1:
+        raise ValueError("the biochem cadence and growth rounds must be shared")
+    nS = info["nS"]
+    sB = info["seg"]
+    R = [t["birthAccept"].size for t in T_]
+    rB = _bases(R)
+    NS, NR = int(sB[-1]), int(rB[-1])
+    t = {}
+    for k in ("seedNode", "cofFrac", "grewFlag", "returnedMon", "deathFlag", "severDeathFlag", "severReturnedMon",
+              "acceptFlag", "freeCount", "freeList", "filID", "filIDTmp"):
+        t[k] = np.concatenate([x[k] for x in T_])
+    t["nucFrac"] = _planar([x["nucFrac"] for x in T_], nS, 3)
+    for k in ("reqCoord", "reqUVec", "reqYVec"):
+        t[k] = _planar([x[k] for x in T_], nS, 3)
+    for k in ("grewOffsets", "returnedOffsets", "severReturnedOffsets", "freeOffsets", "rankOffsets"):
+        t[k] = np.zeros(NS + 1, I32)
+    for k in ("splitParams", "dragParams", "birthParams", "seedParams"):
+        t[k] = _same([x[k] for x in T_], "turnover." + k)
+    seed_mon = _same([x["birthBox"][3:4] for x in T_], "turnover.birthBox[3]")
+    t["growCounts"] = np.array([NS, 0, 0, 0], I32)
+    t["depolyCounts"] = np.array([NS, 0, 0, 0], I32)
+    t["agingCounts"] = np.array([NS, 0], I32)
+    t["severCounts"] = np.array([NS, 0], I32)
+    t["birthAccept"] = np.zeros(NR, I32)
+    t["birthRankOffsets"] = np.zeros(NR + 1, I32)
+    for k in ("birthReqCoord", "birthReqUVec", "birthReqYVec"):
+        t[k] = np.zeros(3 * NR, F32)
+    # per-network tables
+    t["tbSeeds"] = np.array([c.seed for c in cfgs], I32)
+    for k, w in (("growParams", 3), ("depolyParams", 3), ("depolyRateParams", 2), ("agingParams", 2),
+                 ("cofilinParams", 2), ("birthBox", 4)):
+        t["tb_" + k] = np.concatenate([x[k].reshape(-1)[:w] for x in T_]).astype(F32)
+    t["tbOnRate"] = np.array([c.on_rate for c in cfgs], np.float64)
+    t["tbPools"] = np.concatenate([x["pool"] for x in T_]).astype(np.float64)
+    t["tbSlotBase"] = sB.astype(I32)
+    t["tbBirthNet"] = np.concatenate([np.full(r, k, I32) for k, r in enumerate(R)])
+    t["tbBirthBase"] = rB.astype(I32)
+    packed["turnover"] = t
+    packed["tcfg"] = cfgs[0]
+    info["birth"] = rB
+    info["seed_mon"] = int(seed_mon[0])
 
 
 def _unplanar(a, base, n, total, width):
@@ -222,7 +272,13 @@ def unpack_network(packed, info, k):
     x["strainHist"] = xl["strainHist"][10 * l0:10 * (l0 + nl)]
     x["torqueMagHist"] = xl["torqueMagHist"][5 * l0:5 * (l0 + nl)]
     x["activeLinkCount"] = xl["activeLinkCount"][s0:s0 + n]
-    return {"fil": fil, "mot": mot, "mini": mini, "xl": x, "bondData": packed["bondData"][13 * m0:13 * (m0 + nm)]}
+    out = {"fil": fil, "mot": mot, "mini": mini, "xl": x, "bondData": packed["bondData"][13 * m0:13 * (m0 + nm)]}
+    if "turnover" in packed:
+        t = packed["turnover"]
+        out["turnover"] = {"seedNode": t["seedNode"][s0:s0 + n], "cofFrac": t["cofFrac"][s0:s0 + n],
+                           "nucFrac": _unplanar(t["nucFrac"], s0, n, NS, 3),
+                           "pool": t["tbPools"][4 * k:4 * k + 4]}
+    return out
 
 
 def batch_desc(b):
@@ -281,3 +337,31 @@ class BatchedNetworks:
             self.close()
         except Exception:
             pass
+
+
+class BatchedTurnoverNetworks(BatchedNetworks):
+    """Packed dense networks with actin turnover (each packed from scenes.dense_turnover):
+    at each biochem cadence the batched turnover block and births run for every network,
+    then the packed mechanics up to the next cadence; each network's arrays equal those of
+    its engine.TurnoverNetwork run alone."""
+
+    def __init__(self, packed, info, ctx=None, fp64_coords=False, device="cuda"):
+        from .turnover import BatchedTurnover
+        super().__init__(packed, info, ctx=ctx, fp64_coords=fp64_coords, device=device)
+        d = self.dev
+        self.tcfg = packed["tcfg"]
+        xl = d["xl"]
+        self.turnover = BatchedTurnover(d["fil"], d["turnover"], self.tcfg, info,
+                                        links=(xl["linkFilA"], xl["linkFilB"], xl["linkState"]),
+                                        boundSeg=d["mot"]["boundSeg"], segKey=d["batch"]["segKey"])
+
+    def run(self, t0, nsteps, mode="graph"):
+        t, end = int(t0), int(t0) + int(nsteps)
+        ci = self.tcfg.check_int
+        while t < end:
+            if self.tcfg.fires_at(t):
+                self.turnover.cadence(t)
+                self.turnover.births(t)
+            nxt = min(end, (t // ci + 1) * ci)
+            super().run(t, nxt - t, mode)
+            t = nxt

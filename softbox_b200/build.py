@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libsoftbox_b200.so")
-SOURCES = ["sbx_systems.cu", "sbx_sort.cu", "sbx_dense.cu", "sbx_free.cu", "sbx_fused.cu", "sbx_noalloc.cu", "sbx_form.cu", "sbx_turnover.cu", "sbx_batch.cu", "sbx_obs.cu", "sbx_mlp.cu"]
+SOURCES = ["sbx_systems.cu", "sbx_sort.cu", "sbx_dense.cu", "sbx_free.cu", "sbx_fused.cu", "sbx_noalloc.cu", "sbx_form.cu", "sbx_turnover.cu", "sbx_batch.cu", "sbx_obs.cu", "sbx_mlp.cu", "sbx_turnover_batch.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FP_FLAGS = ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
 

@@ -6,8 +6,10 @@
 
 Sweep distribution (per point, seeded): actin rods log-uniform in [2,000, 80,000]; myosin
 minifilaments per actin rod U(0.005, 0.05); crosslinkers per actin rod U(0, 0.5);
-filament chain length U{5..20} rods of 0.1 um; turnover rate U(0, 0.02)/s (a sweep input
-only: packed runs advance the mechanics, turnover of packed networks is not built); slab aspect
+filament chain length U{5..20} rods of 0.1 um; turnover rate U(0, 0.02)/s (with
+`turnover=True` each network runs scenes.dense_turnover's turnover with that rate as its
+severing rate, its own turnover seed and actin pool; otherwise the rate is a surrogate
+input only and the runs advance the mechanics); slab aspect
 x:y log-uniform in [1/2, 2] at the benchmark density (20 x 20 um per 20,000 rods, depth
 0.5 um). Every network has its own seeds. The network's other parameters are the
 benchmark's (scenes.C1).
@@ -84,11 +86,15 @@ def point_config(p, cell_scale=1.0):
                    seed_fil=seeds[2])
 
 
-def build_batch(points, cell_scale=1.0):
+def build_batch(points, cell_scale=1.0, turnover=False):
     from .batch import pack_networks
     nets = []
     for p in points:
-        sc = scenes.dense_contractile(point_config(p, cell_scale))
+        cfg = point_config(p, cell_scale)
+        if turnover:
+            sc = scenes.dense_turnover(cfg, sever_rate=p.turnover, turnover_seed=p.seed ^ 0x0F0501)
+        else:
+            sc = scenes.dense_contractile(cfg)
         for k in ("reachSeg", "center", "gridCellContents", "bodyCell", "cellCount", "gridCellOffsets"):
             sc["grid"].pop(k, None)                 # per-step scratch: the packed scene makes its own
         nets.append(sc)
@@ -122,16 +128,16 @@ def autotune_cell(points, candidates=(1.0, 1.25, 1.5, 2.0), steps=20, fp64_coord
     return best, timings
 
 
-def run_ensemble(points, steps, sample_every, cell_scale=1.0, fp64_coords=True, t0=0):
+def run_ensemble(points, steps, sample_every, cell_scale=1.0, fp64_coords=True, t0=0, turnover=False):
     """Advances every point's network `steps` steps in one packed batch and returns the
-    observables per point plus timing."""
+    observables per point plus timing (`turnover`: with each point's actin turnover)."""
     import torch
-    from .batch import BatchedNetworks
+    from .batch import BatchedNetworks, BatchedTurnoverNetworks
     from .observables import Observables, contraction_rate
     tb = time.perf_counter()
-    packed, info = build_batch(points, cell_scale)
+    packed, info = build_batch(points, cell_scale, turnover)
     build_s = time.perf_counter() - tb
-    ens = BatchedNetworks(packed, info, fp64_coords=fp64_coords)
+    ens = (BatchedTurnoverNetworks if turnover else BatchedNetworks)(packed, info, fp64_coords=fp64_coords)
     obs = Observables(ens)
     dt = float(packed["fil"]["params"][0])
     times, rms, stress = [], [], []
@@ -176,17 +182,19 @@ def main():
     ap.add_argument("--run-steps", type=int, default=50000, help="steps of one sweep run (for points/s)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--turnover", action="store_true", help="run each point's actin turnover")
     a = ap.parse_args()
     pts = sample_points(a.points, a.seed)
     cell, tune = 1.0, None
     if a.autotune:
         cell, tune = autotune_cell(pts)
-    r = run_ensemble(pts, a.steps, a.sample_every, cell_scale=cell)
+    r = run_ensemble(pts, a.steps, a.sample_every, cell_scale=cell, turnover=a.turnover)
     sec_per_run = r["ms_per_step"] * 1e-3 * a.run_steps
     print(json.dumps({"points": a.points, "rods": r["rods"], "bodies": r["bodies"], "steps_timed": a.steps,
                       "ms_per_step": r["ms_per_step"], "rod_steps_per_s": r["rods"] / (r["ms_per_step"] * 1e-3),
                       "body_steps_per_s": r["bodies"] / (r["ms_per_step"] * 1e-3), "run_steps": a.run_steps,
                       "sweep_points_per_s": a.points / sec_per_run, "cell_scale": cell, "autotune_ms": tune,
+                      "turnover": a.turnover,
                       "build_s": r["build_s"],
                       "contraction_rate_mean": float(np.mean(r["contraction_rate"])),
                       "largest_fraction_mean": float(np.mean(r["largest_fraction"])),

@@ -882,7 +882,7 @@ def turnover_chains(n_chains=200, cap=2048, seg_range=(1, 8), seed=5, cfg=None, 
 
 
 def dense_turnover(cfg=None, growth_rate=10.0, sever_rate=0.01, cof_ratio=0.5, birth_cap=None, seed_mon=None,
-                   seed=0x7A11):
+                   seed=0x7A11, turnover_seed=None):
     """The dense network with actin turnover on (the scale sweep's turnover workload):
 
     * growth at every filament's barbed terminal (the end2-free segment, tagged as a
@@ -904,7 +904,8 @@ def dense_turnover(cfg=None, growth_rate=10.0, sever_rate=0.01, cof_ratio=0.5, b
     sc = dense_contractile(cfg)
     f = sc["fil"]
     n = f["body"]["n"]
-    tcfg = TurnoverConfig(dt=cfg.dt, cof_ratio=cof_ratio, pool0_um=growth_rate / K_ATP_ON2_WITH_FORMIN,
+    kw = {} if turnover_seed is None else {"seed": int(turnover_seed)}
+    tcfg = TurnoverConfig(dt=cfg.dt, cof_ratio=cof_ratio, pool0_um=growth_rate / K_ATP_ON2_WITH_FORMIN, **kw,
                           box_vol_um3=float(sc["boxParams"][1]) * float(sc["boxParams"][2]) * cfg.box_z,
                           aeta=cfg.fil_aeta, born_trans=cfg.brown_trans,
                           born_rot=BROT_COEFF)
@@ -918,8 +919,11 @@ def dense_turnover(cfg=None, growth_rate=10.0, sever_rate=0.01, cof_ratio=0.5, b
     x0 = rng.uniform(0.0, x_star, n)
     cof = (1.0 - np.exp(-x0)).astype(F32)
     t = turnover_arrays(n, tcfg, seedNode=seedNode, nucFrac=nuc, cofFrac=cof)
-    cadences = (1.0 / sever_rate) / BIOCHEM_DT
-    t["cofilinParams"][0] = F32(-math.expm1(-x_star / cadences))
+    if sever_rate > 0:
+        cadences = (1.0 / sever_rate) / BIOCHEM_DT
+        t["cofilinParams"][0] = F32(-math.expm1(-x_star / cadences))
+    else:                                   # no severing: cofilin stays where it is
+        t["cofilinParams"][0] = F32(0.0)
     seed_mon = cfg.monomer_ct if seed_mon is None else seed_mon
     birth_cap = birth_cap or max(64, n // 50)
     bp = sc["boxParams"]

@@ -32,25 +32,31 @@ def _targets(r):
     return np.stack([r[k] for k in OUTPUTS], axis=1)
 
 
-def generate(points, steps, sample_every, batch=256):
+def generate(points, steps, sample_every, batch=256, turnover=False):
     """Plain batched runs of `points` in packs of `batch`; returns targets and GPU seconds."""
     ys, gpu_s, build_s = [], 0.0, 0.0
     for b0 in range(0, len(points), batch):
-        r = ensemble.run_ensemble(points[b0:b0 + batch], steps, sample_every)
+        r = ensemble.run_ensemble(points[b0:b0 + batch], steps, sample_every, turnover=turnover)
         ys.append(_targets(r))
         gpu_s += r["gpu_ms"] * 1e-3
         build_s += r["build_s"]
     return np.concatenate(ys), gpu_s, build_s
 
 
-def per_run_seconds(points, steps, sample=8):
-    """Mean GPU seconds of one point's run alone (single-network plan, auto path)."""
+def per_run_seconds(points, steps, sample=8, turnover=False):
+    """Mean GPU seconds of one point's run alone (single-network plan: the auto path, or
+    the graph path with turnover)."""
     import torch
-    from .engine import DenseNetwork
+    from .engine import DenseNetwork, TurnoverNetwork
     from . import scenes
     secs = []
     for p in points[:sample]:
-        net = DenseNetwork(scenes.dense_contractile(ensemble.point_config(p)), fp64_coords=True)
+        cfg = ensemble.point_config(p)
+        if turnover:
+            net = TurnoverNetwork(scenes.dense_turnover(cfg, sever_rate=p.turnover, turnover_seed=p.seed ^ 0x0F0501),
+                                  fp64_coords=True)
+        else:
+            net = DenseNetwork(scenes.dense_contractile(cfg), fp64_coords=True)
         net.run(0, 3)
         torch.cuda.synchronize()
         s, e = torch.cuda.Event(True), torch.cuda.Event(True)
@@ -83,14 +89,15 @@ def main():
                     help="also report the rule with |mean| floored at this fraction of each output's training spread")
     ap.add_argument("--per-run-sample", type=int, default=8)
     ap.add_argument("--seed", type=int, default=11)
+    ap.add_argument("--turnover", action="store_true", help="every run with its point's actin turnover")
     a = ap.parse_args()
     rr = tuple(a.rods)
     pts_train = ensemble.sample_points(a.train, a.seed, rr)
     pts_held = ensemble.sample_points(a.heldout, a.seed + 1, rr)
     pts_fresh = ensemble.sample_points(a.fresh, a.seed + 2, rr)
 
-    y_train, gen_gpu_s, gen_build_s = generate(pts_train, a.steps, a.sample_every)
-    y_held, held_gpu_s, _ = generate(pts_held, a.steps, a.sample_every)
+    y_train, gen_gpu_s, gen_build_s = generate(pts_train, a.steps, a.sample_every, turnover=a.turnover)
+    y_held, held_gpu_s, _ = generate(pts_held, a.steps, a.sample_every, turnover=a.turnover)
     batched_s_per_point = (gen_gpu_s + held_gpu_s) / (a.train + a.heldout)
 
     x_train = ensemble.features(pts_train, rr)
@@ -129,8 +136,8 @@ def main():
                    "heldout_fallback_fraction": float(fbh2.mean()),
                    "heldout_rel_error_with_fallback": rel_error(np.where(fbh2[:, None], y_held, mean_h), y_held),
                    "surrogate_sweep_points_per_s": a.fresh / s2}
-    run_s, run_samples = per_run_seconds(pts_fresh, a.steps, a.per_run_sample)
-    out = {"steps_per_run": a.steps, "rods_range": rr, "train_points": a.train, "heldout_points": a.heldout,
+    run_s, run_samples = per_run_seconds(pts_fresh, a.steps, a.per_run_sample, a.turnover)
+    out = {"steps_per_run": a.steps, "turnover": a.turnover, "rods_range": rr, "train_points": a.train, "heldout_points": a.heldout,
            "fresh_points": a.fresh, "outputs": OUTPUTS,
            "plain_per_run_points_per_s": 1.0 / run_s, "per_run_sample_s": run_samples,
            "plain_batched_points_per_s": 1.0 / batched_s_per_point,

@@ -284,3 +284,114 @@ class Turnover:
     def pool(self):
         """(conc, uMPerMonomer, totalTaken, totalReturned), read back (synchronises)."""
         return pool_fields(self.t["pool"].cpu().numpy())
+
+
+class BatchedTurnover:
+    """The turnover block and births of packed networks (batch.pack_networks of
+    scenes.dense_turnover scenes): the same sequence as Turnover.cadence / births, with the
+    sbx_tb_* kernels where a rate, a draw, a pool or the allocator is involved and the
+    single-network kernels elsewhere."""
+
+    def __init__(self, fil, t, cfg, info, links, boundSeg, segKey):
+        from . import abi_types as T
+        self.f, self.t, self.cfg, self.info = fil, t, cfg, info
+        self.C = int(fil["filState"].numel())
+        self.R = int(t["birthAccept"].numel())
+        self.links, self.boundSeg = links, boundSeg
+        self.seed_mon = int(info["seed_mon"])
+        d = T.TurnoverBatchDesc()
+        T.fill(d, {"slotKey": segKey, "slotBase": t["tbSlotBase"], "seeds": t["tbSeeds"],
+                   "growParams": t["tb_growParams"], "depolyParams": t["tb_depolyParams"],
+                   "depolyRateParams": t["tb_depolyRateParams"], "agingParams": t["tb_agingParams"],
+                   "cofilinParams": t["tb_cofilinParams"], "birthBox": t["tb_birthBox"], "onRate": t["tbOnRate"],
+                   "pools": t["tbPools"], "birthNet": t["tbBirthNet"], "birthBase": t["tbBirthBase"]})
+        d.nNet = int(info["nNet"])
+        self.desc = d
+
+    def _ctx(self):
+        from .systems import _ctx
+        return _ctx()
+
+    def _scan(self, n, counts, offsets):
+        self._ctx()("sbx_csr_scan", n, counts, offsets)
+
+    def _death(self, flag):
+        f, b, t = self.f, self.f["body"], self.t
+        ctx = self._ctx()
+        ctx("sbx_depoly_apply_death", self.C, f["filState"], f["monomerCount"], t["seedNode"], f["end1NbrSlot"],
+            f["end1NbrSide"], f["end2NbrSlot"], f["end2NbrSide"], b["brownTransScale"], b["brownRotScale"], flag)
+        la, lb, ls = self.links
+        ctx("sbx_turnover_release_dead", f["filState"], ls.numel(), la, lb, ls, self.boundSeg.numel(), self.boundSeg)
+
+    def _free_list(self):
+        f, t = self.f, self.t
+        ctx = self._ctx()
+        ctx("sbx_xlink_free_flags", self.C, f["filState"], t["freeCount"])
+        self._scan(self.C, t["freeCount"], t["freeOffsets"])
+        ctx("sbx_xlink_free_scatter", self.C, f["filState"], t["freeOffsets"], t["freeList"])
+
+    def cadence(self, step):
+        import ctypes as C
+        if not self.cfg.fires_at(step):
+            return False
+        f, b, t, n = self.f, self.f["body"], self.t, self.C
+        ctx = self._ctx()
+        tb = C.byref(self.desc)
+        ctx("sbx_turnover_begin", step, 0, 1, 0.0, float(BIOCHEM_DT), None, None, t["growCounts"], t["depolyCounts"],
+            t["agingCounts"], t["severCounts"])
+        ctx("sbx_tb_begin", tb, 1, float(BIOCHEM_DT))
+        ctx("sbx_tb_age", tb, n, f["filState"], t["nucFrac"], t["agingCounts"])
+        ctx("sbx_tb_depoly_proxy", tb, n, f["filState"], f["monomerCount"], b["coord"], b["uVec"], f["end1NbrSlot"],
+            t["nucFrac"], t["returnedMon"], t["deathFlag"], t["depolyCounts"])
+        self._scan(n, t["returnedMon"], t["returnedOffsets"])
+        self._death(t["deathFlag"])
+        ctx("sbx_tb_pool", tb, t["returnedOffsets"], 0)
+        for _ in range(max(1, self.cfg.polyboost)):
+            ctx("sbx_tb_grow", tb, n, t["seedNode"], f["monomerCount"], b["coord"], b["uVec"], t["grewFlag"],
+                t["growCounts"])
+            self._scan(n, t["grewFlag"], t["grewOffsets"])
+            ctx("sbx_aging_growth_atp", n, t["grewFlag"], f["monomerCount"], t["nucFrac"])
+            ctx("sbx_tb_pool", tb, t["grewOffsets"], 1)
+        ctx("sbx_tb_cofilin", tb, n, 0, f["filState"], t["nucFrac"], t["cofFrac"], None, None, None, t["severCounts"])
+        ctx("sbx_tb_cofilin", tb, n, 1, f["filState"], None, t["cofFrac"], f["monomerCount"], t["severDeathFlag"],
+            t["severReturnedMon"], t["severCounts"])
+        self._scan(n, t["severReturnedMon"], t["severReturnedOffsets"])
+        self._death(t["severDeathFlag"])
+        ctx("sbx_tb_pool", tb, t["severReturnedOffsets"], 0)
+        ctx("sbx_growth_mark_splits", n, t["seedNode"], f["monomerCount"], b["coord"], b["uVec"], b["yVec"],
+            t["acceptFlag"], t["reqCoord"], t["reqUVec"], t["reqYVec"], n, t["splitParams"], t["growCounts"])
+        self._free_list()
+        self._scan(n, t["acceptFlag"], t["rankOffsets"])
+        ctx("sbx_tb_birth_allocate", tb, 0, n, n, n, t["reqCoord"], t["reqUVec"], t["reqYVec"], t["rankOffsets"],
+            t["freeList"], t["freeOffsets"], b["coord"], b["uVec"], b["yVec"], b["brownTransScale"],
+            b["brownRotScale"], f["filState"], t["birthParams"])
+        ctx("sbx_tb_split_wire", tb, n, t["rankOffsets"], t["freeList"], t["freeOffsets"], f["monomerCount"],
+            b["coord"], b["uVec"], f["end1NbrSlot"], f["end1NbrSide"], f["end2NbrSlot"], f["end2NbrSide"],
+            t["seedNode"], t["splitParams"])
+        ctx("sbx_tb_formed_init", tb, 0, n, n, t["rankOffsets"], t["freeList"], t["freeOffsets"], t["nucFrac"], 2)
+        ctx("sbx_tb_formed_init", tb, 0, n, n, t["rankOffsets"], t["freeList"], t["freeOffsets"], t["cofFrac"], 0)
+        ctx("sbx_growth_recompute_drag", n, f["monomerCount"], b["segLength"], f["end1NbrSlot"], f["end2NbrSlot"],
+            b["bTransGam"], b["bRotGam"], b["bTransDiff"], b["bRotDiff"], t["dragParams"], t["growCounts"])
+        return True
+
+    def births(self, step):
+        import ctypes as C
+        if not self.cfg.fires_at(step):
+            return False
+        f, b, t, n, R = self.f, self.f["body"], self.t, self.C, self.R
+        ctx = self._ctx()
+        tb = C.byref(self.desc)
+        ctx("sbx_tb_birth_emit", tb, R, step, t["birthAccept"], t["birthReqCoord"], t["birthReqUVec"],
+            t["birthReqYVec"])
+        self._free_list()
+        self._scan(R, t["birthAccept"], t["birthRankOffsets"])
+        ro = t["birthRankOffsets"]
+        ctx("sbx_tb_birth_allocate", tb, 1, R, n, R, t["birthReqCoord"], t["birthReqUVec"], t["birthReqYVec"], ro,
+            t["freeList"], t["freeOffsets"], b["coord"], b["uVec"], b["yVec"], b["brownTransScale"],
+            b["brownRotScale"], f["filState"], t["birthParams"])
+        ctx("sbx_tb_newborn", tb, R, ro, t["freeList"], t["freeOffsets"], f["monomerCount"], b["segLength"],
+            t["seedNode"], t["seedParams"])
+        ctx("sbx_tb_formed_init", tb, 1, R, n, ro, t["freeList"], t["freeOffsets"], t["nucFrac"], 1)
+        ctx("sbx_tb_formed_init", tb, 1, R, n, ro, t["freeList"], t["freeOffsets"], t["cofFrac"], 0)
+        ctx("sbx_tb_pool_births", tb, ro, t["freeOffsets"], self.seed_mon)
+        return True
