@@ -146,6 +146,20 @@ sbx_status sbx_chain_forces(sbx_ctx* ctx, int32_t n, const float* coord, const f
                             const float* segLength, const int32_t* end2NbrSlot, const int32_t* end2NbrSide,
                             const int32_t* end1NbrSlot, const int32_t* end1NbrSide, const float* bTransGam,
                             const float* bRotGam, float* forceSum, float* torqueSum, const float* chainParams);
+/* chainForces followed, in the same pass, by the filament-side gathers of the step in the
+ * reference's order: CrosslinkerSystem.segGatherA, segGatherB (CrosslinkerSystem.java:129-173)
+ * and CrossBridgeSystem.segGather (CrossBridgeSystem.java:302-320), each reading the
+ * row-ordered payload of sbx_csr_build_payload (xlinkData offsets 0 / 6 guarded by linkState;
+ * bondData offset 6). The accumulators get the bits of sbx_chain_forces followed by the three
+ * separate gathers. A null offsets pointer skips that gather. */
+sbx_status sbx_fusion_chain_gathers(sbx_ctx* ctx, int32_t n, const float* coord, const float* uVec,
+                                    const float* segLength, const int32_t* end2NbrSlot,
+                                    const int32_t* end2NbrSide, const int32_t* end1NbrSlot,
+                                    const int32_t* end1NbrSide, const float* bTransGam, const float* bRotGam,
+                                    float* forceSum, float* torqueSum, const float* chainParams,
+                                    const int32_t* segOffsetsA, const float* rowPayloadA,
+                                    const int32_t* segOffsetsB, const float* rowPayloadB,
+                                    const int32_t* segMotorOffsets, const float* rowPayloadM);
 
 /* ---------------------------------------------------------------- body view publishing
  * FilamentStore.publishToBodyView (FilamentStore.java:275-328); filState may be NULL (8-arg form) */
@@ -245,6 +259,14 @@ sbx_status sbx_csr_build(sbx_ctx* ctx, const int32_t* keys, int32_t nItems, int3
  * capture begins. */
 #define SBX_CSR_NOALLOC_MAX_ITEMS (1 << 20)
 #define SBX_CSR_NOALLOC_MAX_ROWS (1 << 22)
+/* sbx_csr_build that also copies each item's 6-float payload (payload[item * payloadStride +
+ * payloadOffset + 0..5]; zeros where guard != NULL and guard[item] < 0) into rowPayload in
+ * list order: row r's items are rowPayload[6 k .. 6 k + 5] for k in [rowOffsets[r],
+ * rowOffsets[r+1]). rowPayload: 6 * nItems floats, 8-byte aligned. */
+sbx_status sbx_csr_build_payload(sbx_ctx* ctx, const int32_t* keys, int32_t nItems, int32_t nRows,
+                                 int32_t* rowCount, int32_t* rowOffsets, int32_t* rowList,
+                                 const float* payload, int32_t payloadStride, int32_t payloadOffset,
+                                 const int32_t* guard, float* rowPayload);
 sbx_status sbx_csr_build_noalloc(sbx_ctx* ctx, const int32_t* keys, int32_t nItems, int32_t nRows,
                                  int32_t* rowCount, int32_t* rowOffsets, int32_t* rowList);
 /* CrossBridgeSystem.segGather (CrossBridgeSystem.java:302-320) */

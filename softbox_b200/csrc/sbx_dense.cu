@@ -42,6 +42,25 @@ __global__ void k_step_advance(int* d_step) { *d_step += 1; }
     } while (0)
 
 // the reference step order over the per-system entry points
+// Context scratch of one dense step: the counting sorts' temporaries first, then the
+// row-ordered payload copies of the three filament-side CSRs (crosslinker A and B sides,
+// motors; 6 floats per item).
+size_t dense_sort_bytes(const sbx_dense_scene* sc) {
+    auto rows = [](int n) { return (size_t)(n + SCAN_CHUNK - 1) / SCAN_CHUNK + 1; };
+    size_t nSeg = sc->fil.body.n;
+    size_t need = (size_t)std::max(sc->grid.cap, 1);
+    need = std::max(need, rows(sc->mini.backbone.n) + (size_t)std::max(sc->mini.nDimers, 1));
+    need = std::max(need, rows((int)nSeg) + (size_t)std::max(sc->mot.nMotors, 1));
+    need = std::max(need, rows((int)nSeg) + (size_t)std::max(sc->xl.nLinks, 1));
+    return sizeof(int) * need;
+}
+
+size_t dense_row_payload_offset(const sbx_dense_scene* sc) { return (dense_sort_bytes(sc) + 255) & ~(size_t)255; }
+
+float* dense_row_payload(sbx_ctx* ctx, const sbx_dense_scene* sc) {
+    return reinterpret_cast<float*>(static_cast<char*>(ctx->scratch) + dense_row_payload_offset(sc));
+}
+
 sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_step, int t,
                           const sbx_batch* bt = nullptr) {
     const sbx_filament_store& f = sc->fil;
@@ -161,8 +180,13 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
         CHK(sbx_fusion_force_build(ctx, nSeg, fb.forceSum, fb.torqueSum, fb.randForce, fb.randTorque, fb.bTransGam,
                                    fb.bRotGam, fb.brownTransScale, fb.brownRotScale, f.params, f.counts));
     }
-    CHK(sbx_chain_forces(ctx, nSeg, fb.coord, fb.uVec, fb.segLength, f.end2NbrSlot, f.end2NbrSide, f.end1NbrSlot,
-                         f.end1NbrSide, fb.bTransGam, fb.bRotGam, fb.forceSum, fb.torqueSum, f.chainParams));
+    // The crosslinker kernels and the three CSR builds read no filament accumulator, so they run
+    // before the chain forces; chain and the three gathers then share one pass
+    // (sbx_fusion_chain_gathers), each gather reading its row-ordered payload copy made by the
+    // CSR build. The accumulators get the bits of chain, segGatherA, segGatherB, segGather.
+    float* payA = dense_row_payload(ctx, sc);
+    float* payB = payA + 6 * (size_t)std::max(xl.nLinks, 0);
+    float* payM = payB + 6 * (size_t)std::max(xl.nLinks, 0);
     if (xlOn) {
         if (sc->xlUnbind && bt)
             CHK(sbx_xlink_unbind_batched(ctx, nSeg, fb.uVec, fb.end1, xl.nLinks, xl.linkFilA, xl.linkFilB, xl.loc1,
@@ -178,16 +202,17 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
         CHK(sbx_xlink_torsion(ctx, nSeg, fb.uVec, xl.nLinks, xl.linkFilA, xl.linkFilB, xl.linkState,
                               xl.linkOrientSame, xl.torqueMagHist, xl.torqueMagPlace, xl.xlinkData,
                               xl.torsionParams));
-        CHK(sbx_csr_build(ctx, xl.linkFilA, xl.nLinks, nSeg, xl.segCountA, xl.segOffsetsA, xl.segIdxA));
-        CHK(sbx_xlink_seg_gather(ctx, 0, nSeg, xl.segOffsetsA, xl.segIdxA, xl.xlinkData, xl.linkState, fb.forceSum,
-                                 fb.torqueSum));
-        CHK(sbx_csr_build(ctx, xl.linkFilB, xl.nLinks, nSeg, xl.segCountB, xl.segOffsetsB, xl.segIdxB));
-        CHK(sbx_xlink_seg_gather(ctx, 1, nSeg, xl.segOffsetsB, xl.segIdxB, xl.xlinkData, xl.linkState, fb.forceSum,
-                                 fb.torqueSum));
+        CHK(sbx_csr_build_payload(ctx, xl.linkFilA, xl.nLinks, nSeg, xl.segCountA, xl.segOffsetsA, xl.segIdxA,
+                                  xl.xlinkData, XL_STRIDE, 0, xl.linkState, payA));
+        CHK(sbx_csr_build_payload(ctx, xl.linkFilB, xl.nLinks, nSeg, xl.segCountB, xl.segOffsetsB, xl.segIdxB,
+                                  xl.xlinkData, XL_STRIDE, 6, xl.linkState, payB));
     }
-    CHK(sbx_csr_build(ctx, mot.boundSeg, nM, nSeg, sc->segMotorCount, sc->segMotorOffsets, sc->segMotorMyo));
-    CHK(sbx_xbridge_seg_gather(ctx, nSeg, sc->segMotorOffsets, sc->segMotorMyo, sc->bondData, fb.forceSum,
-                               fb.torqueSum));
+    CHK(sbx_csr_build_payload(ctx, mot.boundSeg, nM, nSeg, sc->segMotorCount, sc->segMotorOffsets, sc->segMotorMyo,
+                              sc->bondData, XB_STRIDE, 6, nullptr, payM));
+    CHK(sbx_fusion_chain_gathers(ctx, nSeg, fb.coord, fb.uVec, fb.segLength, f.end2NbrSlot, f.end2NbrSide,
+                                 f.end1NbrSlot, f.end1NbrSide, fb.bTransGam, fb.bRotGam, fb.forceSum, fb.torqueSum,
+                                 f.chainParams, xlOn ? xl.segOffsetsA : nullptr, payA,
+                                 xlOn ? xl.segOffsetsB : nullptr, payB, sc->segMotorOffsets, payM));
     if (bt) {
         CHK(sbx_confine_batched(ctx, nSeg, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.forceSum, fb.torqueSum,
                                 bt->boxParams, f.counts, bt->segKey));
@@ -203,13 +228,8 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
 }
 
 size_t dense_scratch_bytes(const sbx_dense_scene* sc) {
-    auto rows = [](int n) { return (size_t)(n + SCAN_CHUNK - 1) / SCAN_CHUNK + 1; };
-    size_t nSeg = sc->fil.body.n;
-    size_t need = (size_t)std::max(sc->grid.cap, 1);
-    need = std::max(need, rows(sc->mini.backbone.n) + (size_t)std::max(sc->mini.nDimers, 1));
-    need = std::max(need, rows((int)nSeg) + (size_t)std::max(sc->mot.nMotors, 1));
-    need = std::max(need, rows((int)nSeg) + (size_t)std::max(sc->xl.nLinks, 1));
-    return sizeof(int) * need;
+    return dense_row_payload_offset(sc) +
+           sizeof(float) * 6 * (2 * (size_t)std::max(sc->xl.nLinks, 0) + (size_t)std::max(sc->mot.nMotors, 0));
 }
 
 }  // namespace
@@ -231,7 +251,33 @@ struct sbx_dense_plan {
     // packed networks (graph and per-system paths only)
     bool batched = false;
     sbx_batch batch{};
+    // the step's scratch (sort temporaries, row-ordered payloads), owned by the plan: the
+    // captured graph holds its address, so it must not move when another plan on the same
+    // context needs a larger context scratch
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
 };
+
+namespace {
+
+// Points the context's scratch at the plan's for the duration of a scope (the graph capture
+// and the per-system path); the plan's buffer covers every request of the step, so nothing
+// inside reallocates it.
+struct PlanScratch {
+    sbx_ctx* ctx;
+    void* saved;
+    size_t savedBytes;
+    PlanScratch(sbx_dense_plan* p) : ctx(p->ctx), saved(p->ctx->scratch), savedBytes(p->ctx->scratch_bytes) {
+        ctx->scratch = p->scratch;
+        ctx->scratch_bytes = p->scratch_bytes;
+    }
+    ~PlanScratch() {
+        ctx->scratch = saved;
+        ctx->scratch_bytes = savedBytes;
+    }
+};
+
+}  // namespace
 
 namespace {
 
@@ -378,7 +424,6 @@ extern "C" sbx_status sbx_dense_step_unfused(sbx_ctx* ctx, const sbx_dense_scene
 static sbx_status plan_create(sbx_ctx* ctx, const sbx_dense_scene* sc, const sbx_batch* bt, sbx_dense_plan** out) {
     if (!ctx || !sc || !out) return SBX_EINVAL;
     *out = nullptr;
-    CHK(ensure_scratch(ctx, dense_scratch_bytes(sc)));
     sbx_dense_plan* p = new sbx_dense_plan();
     p->ctx = ctx;
     p->scene = *sc;
@@ -386,7 +431,13 @@ static sbx_status plan_create(sbx_ctx* ctx, const sbx_dense_scene* sc, const sbx
         p->batched = true;
         p->batch = *bt;
     }
+    p->scratch_bytes = dense_scratch_bytes(sc);
+    if (cudaMalloc(&p->scratch, p->scratch_bytes) != cudaSuccess) {
+        delete p;
+        return fail(ctx, SBX_ENOMEM, "sbx_dense_plan_create: step scratch");
+    }
     if (cudaMalloc(&p->d_step, sizeof(int)) != cudaSuccess) {
+        cudaFree(p->scratch);
         delete p;
         return fail(ctx, SBX_ENOMEM, "sbx_dense_plan_create: step word");
     }
@@ -398,12 +449,17 @@ static sbx_status plan_create(sbx_ctx* ctx, const sbx_dense_scene* sc, const sbx
         delete p;
         return fail(ctx, SBX_ECUDA, "sbx_dense_plan_create: begin capture");
     }
-    sbx_status st = dense_sequence(ctx, &p->scene, p->d_step, 0, p->batched ? &p->batch : nullptr);
+    sbx_status st;
+    {
+        PlanScratch use(p);
+        st = dense_sequence(ctx, &p->scene, p->d_step, 0, p->batched ? &p->batch : nullptr);
+    }
     if (st == SBX_OK) SBX_LAUNCH(ctx, k_step_advance, 1, 1, p->d_step);
     cudaError_t ce = cudaStreamEndCapture(ctx->stream, &p->graph);
     if (st != SBX_OK || ce != cudaSuccess) {
         if (p->graph) cudaGraphDestroy(p->graph);
         cudaFree(p->d_step);
+        cudaFree(p->scratch);
         delete p;
         cudaGetLastError();
         return st != SBX_OK ? st : fail(ctx, SBX_ECUDA, std::string("end capture: ") + cudaGetErrorString(ce));
@@ -413,6 +469,7 @@ static sbx_status plan_create(sbx_ctx* ctx, const sbx_dense_scene* sc, const sbx
     if (cudaGraphInstantiate(&p->exec, p->graph, 0) != cudaSuccess) {
         cudaGraphDestroy(p->graph);
         cudaFree(p->d_step);
+        cudaFree(p->scratch);
         delete p;
         return fail(ctx, SBX_ECUDA, "sbx_dense_plan_create: instantiate");
     }
@@ -470,6 +527,7 @@ extern "C" sbx_status sbx_dense_plan_run(sbx_dense_plan* p, int32_t t0, int32_t 
         }
         return check_launch(ctx, "sbx_dense_plan_run");
     }
+    PlanScratch use(p);
     for (int k = 0; k < nsteps; k++)
         CHK(dense_sequence(ctx, &p->scene, nullptr, t0 + k, p->batched ? &p->batch : nullptr));
     return SBX_OK;
@@ -518,6 +576,7 @@ extern "C" sbx_status sbx_dense_plan_destroy(sbx_dense_plan* p) {
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
     if (p->d_step) cudaFree(p->d_step);
+    if (p->scratch) cudaFree(p->scratch);
     for (void* q : p->allocs) cudaFree(q);
     delete p;
     return SBX_OK;

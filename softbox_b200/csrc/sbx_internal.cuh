@@ -58,6 +58,12 @@ struct CountingSort {
     int* rowList;         // listCap
     int listCap;
     int* tmp;             // unordered scatter buffer, >= nBound ints
+    // optional: the items' 6-float payloads copied in list order (rowPayload[6 pos + j] =
+    // payload[item * pStride + pOff + j], zeros where guard[item] < 0)
+    const float* payload = nullptr;
+    int pStride = 0, pOff = 0;
+    const int* guard = nullptr;
+    float* rowPayload = nullptr;
 };
 
 sbx_status counting_sort(sbx_ctx* ctx, const CountingSort& cs, const char* what);

@@ -129,7 +129,8 @@ __global__ void k_cs_scatter(const int* keys, const int* nDev, int useDevN, int 
 }
 
 __global__ void k_cs_rank(const int* keys, const int* nDev, int useDevN, int nBound, const int* offsets,
-                          const int* tmp, int* rowList, int listCap) {
+                          const int* tmp, int* rowList, int listCap, const float* payload, int pStride, int pOff,
+                          const int* guard, float* rowPayload) {
     int n = item_count(nDev, useDevN, nBound);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int c = keys[i];
@@ -138,7 +139,20 @@ __global__ void k_cs_rank(const int* keys, const int* nDev, int useDevN, int nBo
         int rank = 0;
         for (int j = start; j < end; j++) rank += tmp[j] < i;
         int pos = start + rank;
-        if (pos < listCap) rowList[pos] = i;
+        if (pos >= listCap) continue;
+        rowList[pos] = i;
+        if (rowPayload) {
+            // 6 floats at pos: a row's items end up contiguous, so a gather reads them in order
+            float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            if (!guard || guard[i] >= 0) {
+                const float* q = payload + (int64_t)i * pStride + pOff;
+                for (int j = 0; j < 6; j++) v[j] = q[j];
+            }
+            float2* o = reinterpret_cast<float2*>(rowPayload + 6 * (int64_t)pos);
+            o[0] = make_float2(v[0], v[1]);
+            o[1] = make_float2(v[2], v[3]);
+            o[2] = make_float2(v[4], v[5]);
+        }
     }
 }
 
@@ -189,7 +203,7 @@ sbx_status counting_sort(sbx_ctx* ctx, const CountingSort& cs, const char* what)
         SBX_LAUNCH(ctx, k_cs_scatter, itemBlocks, 256, cs.keys, cs.nDev, cs.useDevN, cs.nBound, cs.rowOffsets,
                    cs.rowCount, cs.tmp);
         SBX_LAUNCH(ctx, k_cs_rank, itemBlocks, 256, cs.keys, cs.nDev, cs.useDevN, cs.nBound, cs.rowOffsets, cs.tmp,
-                   cs.rowList, cs.listCap);
+                   cs.rowList, cs.listCap, cs.payload, cs.pStride, cs.pOff, cs.guard, cs.rowPayload);
     }
     return check_launch(ctx, what);
 }

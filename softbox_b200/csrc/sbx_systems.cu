@@ -486,52 +486,131 @@ extern "C" sbx_status sbx_fusion_integ_derive_confined(sbx_ctx* ctx, int32_t n, 
 // rod. Each joint's costly scalars (chain_joint) are computed once by its lower-slot rod and
 // shared through shared memory with the partner when both rods are in the block and the
 // partner's neighbour entries point back consistently; otherwise the rod computes the joint
-// from its own side, which gives the same bits.
+// from its own side, which gives the same bits. The rod geometry is loaded where each part
+// needs it (the joint, then the apply step re-reads the few values it uses) so that no full
+// geometry set stays live across the barrier: fewer registers, more resident warps to hide
+// the FP64 and load latencies.
+//
+// With GATHER the same pass then adds the filament-side CSR gathers of the step, in the
+// reference's order: CrosslinkerSystem.segGatherA (:129-150), segGatherB (:153-173) and
+// CrossBridgeSystem.segGather (:302-320). Each reads a row-ordered payload (sbx_csr_build_payload:
+// row s's items at rows [offsets[s], offsets[s+1]) of 6 floats), sums the row in FP64 in list
+// order and adds it to the float accumulators; a guarded-out item holds zeros, which leave the
+// sum's bits unchanged (the sum starts at +0.0 and so is never -0.0). The accumulators are read
+// and written once for chain and gathers, and the gathers' loads overlap the joint arithmetic.
 constexpr int CHAIN_THREADS = 256;
 
-__global__ void __launch_bounds__(CHAIN_THREADS) k_chain(int n, const float* coord, const float* uVec,
-                                                         const float* segLength, const int* e2s, const int* e2d,
-                                                         const int* e1s, const int* e1d, const float* bTG,
-                                                         const float* bRG, float* F, float* T,
-                                                         const float* chainParams) {
+struct RowGathers {
+    const int* offA; const float* payA;
+    const int* offB; const float* payB;
+    const int* offM; const float* payM;
+};
+
+struct RowSum {
+    int k0, k1;
+    float2 q[3];
+};
+
+SBX_DEV void row_begin(RowSum& r, int s, const int* off) {
+    r.k0 = r.k1 = 0;
+    if (off) { r.k0 = off[s]; r.k1 = off[s + 1]; }
+}
+
+SBX_DEV void row_first(RowSum& r, const float* pay) {
+    if (r.k0 < r.k1) {
+        const float2* q = reinterpret_cast<const float2*>(pay + 6 * (int64_t)r.k0);
+        r.q[0] = q[0]; r.q[1] = q[1]; r.q[2] = q[2];
+    }
+}
+
+SBX_DEV void row_finish(const RowSum& r, const float* pay, float Fv[3], float Tv[3]) {
+    double f[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
+    if (r.k0 < r.k1) {
+        f[0] += r.q[0].x; f[1] += r.q[0].y; f[2] += r.q[1].x;
+        t[0] += r.q[1].y; t[1] += r.q[2].x; t[2] += r.q[2].y;
+        for (int k = r.k0 + 1; k < r.k1; k++) {
+            const float* q = pay + 6 * (int64_t)k;
+            f[0] += q[0]; f[1] += q[1]; f[2] += q[2];
+            t[0] += q[3]; t[1] += q[4]; t[2] += q[5];
+        }
+    }
+    for (int k = 0; k < 3; k++) {
+        Fv[k] = (float)(Fv[k] + f[k]);
+        Tv[k] = (float)(Tv[k] + t[k]);
+    }
+}
+
+template <bool GATHER>
+__global__ void __launch_bounds__(CHAIN_THREADS, 3) k_chain(int n, const float* coord, const float* uVec,
+                                                            const float* segLength, const int* e2s, const int* e2d,
+                                                            const int* e1s, const int* e1d, const float* bTG,
+                                                            const float* bRG, float* F, float* T,
+                                                            const float* chainParams, RowGathers g) {
     __shared__ ChainJoint js[2 * CHAIN_THREADS];
     const int tid = threadIdx.x, lo = blockIdx.x * blockDim.x;
     const int hi = min(lo + (int)blockDim.x, n);
     const int i = lo + tid;
-    ChainParams cp = chain_params(chainParams);
-    RodGeom r, nb2, nb1;
     int s2 = -1, d2 = 0, s1 = -1, d1 = 0;
     if (i < n) {
-        r = load_rod(n, i, coord, uVec, segLength, bTG, bRG);
         s2 = e2s[i]; d2 = e2d[i]; s1 = e1s[i]; d1 = e1d[i];
-        if (s2 >= 0) {
-            nb2 = load_rod(n, s2, coord, uVec, segLength, bTG, bRG);
-            if (s2 > i) js[2 * tid] = chain_joint(cp, i, 0, s2, d2, r, nb2);
+        if (s2 > i) {
+            ChainParams cp = chain_params(chainParams);
+            js[2 * tid] = chain_joint(cp, i, 0, s2, d2, load_rod(n, i, coord, uVec, segLength, bTG, bRG),
+                                      load_rod(n, s2, coord, uVec, segLength, bTG, bRG));
         }
-        if (s1 >= 0) {
-            nb1 = load_rod(n, s1, coord, uVec, segLength, bTG, bRG);
-            if (s1 > i) js[2 * tid + 1] = chain_joint(cp, i, 1, s1, d1, r, nb1);
+        if (s1 > i) {
+            ChainParams cp = chain_params(chainParams);
+            js[2 * tid + 1] = chain_joint(cp, i, 1, s1, d1, load_rod(n, i, coord, uVec, segLength, bTG, bRG),
+                                          load_rod(n, s1, coord, uVec, segLength, bTG, bRG));
         }
     }
     __syncthreads();
     if (i >= n) return;
-    // the joint seen from side `side` of rod i: its own slot, the partner's slot, or recomputed
-    auto joint = [&](int side, int slot, int nside, const RodGeom& nb) -> ChainJoint {
-        if (slot > i) return js[2 * tid + side];
-        if (slot >= lo && slot < hi && (nside == 0 || nside == 1)) {
+    float Fv[3], Tv[3];
+    for (int k = 0; k < 3; k++) { Fv[k] = F[k * n + i]; Tv[k] = T[k * n + i]; }
+    RowSum ra, rb, rm;
+    if (GATHER) {
+        row_begin(ra, i, g.offA);
+        row_begin(rb, i, g.offB);
+        row_begin(rm, i, g.offM);
+    }
+    double f[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
+    // side `side` of rod i: the joint from its own slot, the partner's slot, or recomputed
+    for (int side = 0; side < 2; side++) {
+        int slot = side == 0 ? s2 : s1, nside = side == 0 ? d2 : d1;
+        if (slot < 0) continue;
+        ChainParams cp = chain_params(chainParams);
+        RodGeom r = load_rod(n, i, coord, uVec, segLength, bTG, bRG);
+        RodGeom nb = load_rod(n, slot, coord, uVec, segLength, bTG, bRG);
+        ChainJoint J;
+        bool have = false;
+        if (slot > i) {
+            J = js[2 * tid + side];
+            have = true;
+        } else if (slot >= lo && slot < hi && (nside == 0 || nside == 1)) {
             int ps = 1 - nside;                                  // the partner's side facing rod i
             int back = ps == 0 ? e2s[slot] : e1s[slot], backSide = ps == 0 ? e2d[slot] : e1d[slot];
-            if (back == i && backSide == 1 - side) return js[2 * (slot - lo) + ps];
+            if (back == i && backSide == 1 - side) {
+                J = js[2 * (slot - lo) + ps];
+                have = true;
+            }
         }
-        return chain_joint(cp, i, side, slot, nside, r, nb);
-    };
-    double f[3] = {0.0, 0.0, 0.0}, t[3] = {0.0, 0.0, 0.0};
-    if (s2 >= 0) chain_apply(cp, i, 0, s2, d2, r, nb2, joint(0, s2, d2, nb2), f, t);
-    if (s1 >= 0) chain_apply(cp, i, 1, s1, d1, r, nb1, joint(1, s1, d1, nb1), f, t);
-    for (int k = 0; k < 3; k++) {
-        F[k * n + i] = (float)(F[k * n + i] + f[k]);
-        T[k * n + i] = (float)(T[k * n + i] + t[k]);
+        if (!have) J = chain_joint(cp, i, side, slot, nside, r, nb);
+        chain_apply(cp, i, side, slot, nside, r, nb, J, f, t);
     }
+    for (int k = 0; k < 3; k++) {
+        Fv[k] = (float)(Fv[k] + f[k]);
+        Tv[k] = (float)(Tv[k] + t[k]);
+    }
+    if (GATHER) {
+        row_first(ra, g.payA);
+        row_first(rb, g.payB);
+        row_first(rm, g.payM);
+        if (g.offA) row_finish(ra, g.payA, Fv, Tv);
+        if (g.offB) row_finish(rb, g.payB, Fv, Tv);
+        if (g.offM) row_finish(rm, g.payM, Fv, Tv);
+    }
+    for (int k = 0; k < 3; k++) { F[k * n + i] = Fv[k]; T[k * n + i] = Tv[k]; }
 }
 
 extern "C" sbx_status sbx_chain_forces(sbx_ctx* ctx, int32_t n, const float* coord, const float* uVec,
@@ -541,9 +620,30 @@ extern "C" sbx_status sbx_chain_forces(sbx_ctx* ctx, int32_t n, const float* coo
     SBX_REQUIRE(ctx && n >= 0 && (n == 0 || (coord && uVec && segLength && e2s && e2d && e1s && e1d && bTG && bRG &&
                                              F && T && chainParams)));
     if (n == 0) return SBX_OK;
-    SBX_LAUNCH(ctx, k_chain, blocks(n, CHAIN_THREADS), CHAIN_THREADS, n, coord, uVec, segLength, e2s, e2d, e1s, e1d, bTG, bRG, F, T,
-               chainParams);
+    SBX_LAUNCH(ctx, k_chain<false>, blocks(n, CHAIN_THREADS), CHAIN_THREADS, n, coord, uVec, segLength, e2s, e2d,
+               e1s, e1d, bTG, bRG, F, T, chainParams, RowGathers{});
     return check_launch(ctx, "sbx_chain_forces");
+}
+
+static bool aligned8(const void* p) { return ((uintptr_t)p & 7u) == 0; }
+
+extern "C" sbx_status sbx_fusion_chain_gathers(sbx_ctx* ctx, int32_t n, const float* coord, const float* uVec,
+                                               const float* segLength, const int32_t* e2s, const int32_t* e2d,
+                                               const int32_t* e1s, const int32_t* e1d, const float* bTG,
+                                               const float* bRG, float* F, float* T, const float* chainParams,
+                                               const int32_t* segOffsetsA, const float* rowPayloadA,
+                                               const int32_t* segOffsetsB, const float* rowPayloadB,
+                                               const int32_t* segMotorOffsets, const float* rowPayloadM) {
+    SBX_REQUIRE(ctx && n >= 0 && (n == 0 || (coord && uVec && segLength && e2s && e2d && e1s && e1d && bTG && bRG &&
+                                             F && T && chainParams)) &&
+                (!segOffsetsA || (rowPayloadA && aligned8(rowPayloadA))) &&
+                (!segOffsetsB || (rowPayloadB && aligned8(rowPayloadB))) &&
+                (!segMotorOffsets || (rowPayloadM && aligned8(rowPayloadM))));
+    if (n == 0) return SBX_OK;
+    RowGathers g{segOffsetsA, rowPayloadA, segOffsetsB, rowPayloadB, segMotorOffsets, rowPayloadM};
+    SBX_LAUNCH(ctx, k_chain<true>, blocks(n, CHAIN_THREADS), CHAIN_THREADS, n, coord, uVec, segLength, e2s, e2d,
+               e1s, e1d, bTG, bRG, F, T, chainParams, g);
+    return check_launch(ctx, "sbx_fusion_chain_gathers");
 }
 
 // ============================================================================ publishing
@@ -915,6 +1015,26 @@ extern "C" sbx_status sbx_csr_build(sbx_ctx* ctx, const int32_t* keys, int32_t n
     int* s = (int*)ctx->scratch;
     CountingSort cs{keys, nullptr, 0, nItems, nRows, rowCount, s, rowOffsets, rowList, nItems, s + chunks};
     return counting_sort(ctx, cs, "sbx_csr_build");
+}
+
+extern "C" sbx_status sbx_csr_build_payload(sbx_ctx* ctx, const int32_t* keys, int32_t nItems, int32_t nRows,
+                                            int32_t* rowCount, int32_t* rowOffsets, int32_t* rowList,
+                                            const float* payload, int32_t payloadStride, int32_t payloadOffset,
+                                            const int32_t* guard, float* rowPayload) {
+    SBX_REQUIRE(ctx && nItems >= 0 && nRows > 0 && rowCount && rowOffsets && payloadStride >= 6 &&
+                payloadOffset >= 0 && payloadOffset + 6 <= payloadStride &&
+                (nItems == 0 || (keys && rowList && payload && rowPayload && aligned8(rowPayload))));
+    size_t chunks = (size_t)(nRows + SCAN_CHUNK - 1) / SCAN_CHUNK + 1;
+    sbx_status st = ensure_scratch(ctx, sizeof(int) * (chunks + (size_t)std::max(nItems, 1)));
+    if (st) return st;
+    int* s = (int*)ctx->scratch;
+    CountingSort cs{keys, nullptr, 0, nItems, nRows, rowCount, s, rowOffsets, rowList, nItems, s + chunks};
+    cs.payload = payload;
+    cs.pStride = payloadStride;
+    cs.pOff = payloadOffset;
+    cs.guard = guard;
+    cs.rowPayload = rowPayload;
+    return counting_sort(ctx, cs, "sbx_csr_build_payload");
 }
 
 __global__ void k_csr_gather(int nRows, const int* offsets, const int* list, const float* payload, int stride, int off,
