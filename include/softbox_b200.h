@@ -211,6 +211,20 @@ sbx_status sbx_binding_grid_reachable(sbx_ctx* ctx, const float* head, const flo
                                       const int32_t* ownerStore, const int32_t* ownerSlot,
                                       int32_t* motorReachSeg, int32_t* motorReachCount,
                                       const float* kinParams, int32_t nM);
+/* gridReachable over cell-ordered segment endpoints: sbx_grid_cell_endpoints writes, for every
+ * grid entry idx < gridCellOffsets[totalCells], cellEnd1[4 idx..] = (end1 xyz, slot as int
+ * bits; -1 for a non-filament entry) and cellEnd2[4 idx..] = (end2 xyz, 0) (cap float4 each,
+ * 16-byte aligned); sbx_fusion_grid_reachable then walks them with the reach lists and
+ * counts of sbx_binding_grid_reachable. */
+sbx_status sbx_grid_cell_endpoints(sbx_ctx* ctx, int32_t cap, int32_t totalCells,
+                                   const int32_t* gridCellOffsets, const int32_t* gridCellContents,
+                                   const int32_t* ownerStore, const int32_t* ownerSlot, int32_t nSeg,
+                                   const float* segEnd1, const float* segEnd2, float* cellEnd1, float* cellEnd2);
+sbx_status sbx_fusion_grid_reachable(sbx_ctx* ctx, const float* head, const float* uVec, const float* rodUVec,
+                                     const float* gridParams, const int32_t* gridDims,
+                                     const int32_t* gridCellOffsets, const float* cellEnd1,
+                                     const float* cellEnd2, int32_t* motorReachSeg, int32_t* motorReachCount,
+                                     const float* kinParams, int32_t nM);
 /* BindingDetectionSystem.bruteReachable (BindingDetectionSystem.java:260-283) */
 sbx_status sbx_binding_brute_reachable(sbx_ctx* ctx, const float* head, const float* uVec,
                                        const float* rodUVec, int32_t nSeg, const float* segEnd1,
@@ -745,6 +759,11 @@ sbx_status sbx_binding_grid_reachable_batched(sbx_ctx* ctx, const float* head, c
                                               const int32_t* ownerStore, const int32_t* ownerSlot, int32_t* reachSeg,
                                               int32_t* reachCount, const float* kp, int32_t nM,
                                               const int32_t* motKey, const float* gpTab, const int32_t* gdTab);
+sbx_status sbx_fusion_grid_reachable_batched(sbx_ctx* ctx, const float* head, const float* uVec,
+                                             const float* rodUVec, const int32_t* offsets, const float* cellEnd1,
+                                             const float* cellEnd2, int32_t* reachSeg, int32_t* reachCount,
+                                             const float* kp, int32_t nM, const int32_t* motKey,
+                                             const float* gpTab, const int32_t* gdTab);
 sbx_status sbx_confine_batched(sbx_ctx* ctx, int32_t n, const float* coord, const float* uVec,
                                const float* segLength, const float* bTG, float* F, float* T, const float* boxTab,
                                const int32_t* counts, const int32_t* key);

@@ -110,6 +110,18 @@ __global__ void k_grid_reachable_b(int nM, const float* head, const float* uVec,
                                     contents, ownerStore, ownerSlot, reachSeg + (int64_t)m * MAX_CAND, kp[7], kp[8]);
 }
 
+__global__ void k_grid_reachable_cells_b(int nM, const float* head, const float* uVec, const float* rodUVec,
+                                         const int* offsets, const float4* cellE1, const float4* cellE2,
+                                         int* reachSeg, int* reachCount, const float* kp, const int* motKey,
+                                         const float* gpTab, const int* gdTab) {
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nM) return;
+    int net = motKey[2 * m];
+    const int* gd = gdTab + 4 * net;
+    reachCount[m] = grid_reach_walk_cells(m, nM, head, uVec, rodUVec, gpTab + 6 * net, gd, offsets + gd[3], cellE1,
+                                          cellE2, reachSeg + (int64_t)m * MAX_CAND, kp[7], kp[8]);
+}
+
 __global__ void k_confine_b(int n, const float* coord, const float* uVec, const float* segLength, const float* bTG,
                             float* F, float* T, const float* bpTab, const int* counts, const int* key) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -118,8 +130,10 @@ __global__ void k_confine_b(int n, const float* coord, const float* uVec, const 
     if (!bx.active) return;
     float c[3], u[3], f[3], t[3];
     ld3(coord, n, i, c); ld3(uVec, n, i, u); ld3(F, n, i, f); ld3(T, n, i, t);
-    confine_one(bx, c, u, segLength[i], bTG[i], f, t);
-    st3(F, n, i, f); st3(T, n, i, t);
+    if (confine_one(bx, c, u, segLength[i], bTG[i], f, t)) {
+        st3(F, n, i, f);
+        st3(T, n, i, t);
+    }
 }
 
 }  // namespace
@@ -199,6 +213,21 @@ extern "C" sbx_status sbx_binding_grid_reachable_batched(sbx_ctx* ctx, const flo
     SBX_LAUNCH(ctx, k_grid_reachable_b, blocks(nM, 128), 128, nM, head, uVec, rodUVec, nSeg, e1, e2, offsets,
                contents, ownerStore, ownerSlot, reachSeg, reachCount, kp, motKey, gpTab, gdTab);
     SBX_DONE("sbx_binding_grid_reachable_batched");
+}
+
+extern "C" sbx_status sbx_fusion_grid_reachable_batched(sbx_ctx* ctx, const float* head, const float* uVec,
+                                                        const float* rodUVec, const int32_t* gridCellOffsets,
+                                                        const float* cellEnd1, const float* cellEnd2,
+                                                        int32_t* reachSeg, int32_t* reachCount, const float* kp,
+                                                        int32_t nM, const int32_t* motKey, const float* gpTab,
+                                                        const int32_t* gdTab) {
+    SBX_REQUIRE(ctx && nM >= 0 && (nM == 0 || (head && uVec && rodUVec && gridCellOffsets && cellEnd1 && cellEnd2 &&
+                                               reachSeg && reachCount && kp && motKey && gpTab && gdTab)));
+    if (nM == 0) return SBX_OK;
+    SBX_LAUNCH(ctx, k_grid_reachable_cells_b, blocks(nM, 128), 128, nM, head, uVec, rodUVec, gridCellOffsets,
+               reinterpret_cast<const float4*>(cellEnd1), reinterpret_cast<const float4*>(cellEnd2), reachSeg,
+               reachCount, kp, motKey, gpTab, gdTab);
+    SBX_DONE("sbx_fusion_grid_reachable_batched");
 }
 
 extern "C" sbx_status sbx_confine_batched(sbx_ctx* ctx, int32_t n, const float* coord, const float* uVec,

@@ -44,21 +44,39 @@ __global__ void k_step_advance(int* d_step) { *d_step += 1; }
 // the reference step order over the per-system entry points
 // Context scratch of one dense step: the counting sorts' temporaries first, then the
 // row-ordered payload copies of the three filament-side CSRs (crosslinker A and B sides,
-// motors; 6 floats per item).
+// motors; 6 floats per item), then the reach walk's cell-ordered endpoints.
 size_t dense_sort_bytes(const sbx_dense_scene* sc) {
     auto rows = [](int n) { return (size_t)(n + SCAN_CHUNK - 1) / SCAN_CHUNK + 1; };
-    size_t nSeg = sc->fil.body.n;
-    size_t need = (size_t)std::max(sc->grid.cap, 1);
-    need = std::max(need, rows(sc->mini.backbone.n) + (size_t)std::max(sc->mini.nDimers, 1));
-    need = std::max(need, rows((int)nSeg) + (size_t)std::max(sc->mot.nMotors, 1));
-    need = std::max(need, rows((int)nSeg) + (size_t)std::max(sc->xl.nLinks, 1));
-    return sizeof(int) * need;
+    auto csr = [&](int nRows, int nItems) {           // sbx_csr_build's layout: ints, then tile sums
+        return ((sizeof(int) * (rows(nRows) + (size_t)std::max(nItems, 1)) + 7) & ~(size_t)7) +
+               sizeof(int) * scan_tile_words(nRows);
+    };
+    int nSeg = sc->fil.body.n;
+    size_t need = ((sizeof(int) * (size_t)std::max(sc->grid.cap, 1) + 7) & ~(size_t)7) +
+                  sizeof(int) * scan_tile_words(sc->grid.totalCells);
+    need = std::max(need, csr(sc->mini.backbone.n, sc->mini.nDimers));
+    need = std::max(need, csr(nSeg, sc->mot.nMotors));
+    need = std::max(need, csr(nSeg, sc->xl.nLinks));
+    return need;
 }
 
 size_t dense_row_payload_offset(const sbx_dense_scene* sc) { return (dense_sort_bytes(sc) + 255) & ~(size_t)255; }
 
+size_t dense_row_payload_bytes(const sbx_dense_scene* sc) {
+    return sizeof(float) * 6 * (2 * (size_t)std::max(sc->xl.nLinks, 0) + (size_t)std::max(sc->mot.nMotors, 0));
+}
+
+// then the cell-ordered endpoints of the reach walk (two float4 per grid entry)
+size_t dense_cell_endpoints_offset(const sbx_dense_scene* sc) {
+    return (dense_row_payload_offset(sc) + dense_row_payload_bytes(sc) + 255) & ~(size_t)255;
+}
+
 float* dense_row_payload(sbx_ctx* ctx, const sbx_dense_scene* sc) {
     return reinterpret_cast<float*>(static_cast<char*>(ctx->scratch) + dense_row_payload_offset(sc));
+}
+
+float* dense_cell_endpoints(sbx_ctx* ctx, const sbx_dense_scene* sc) {
+    return reinterpret_cast<float*>(static_cast<char*>(ctx->scratch) + dense_cell_endpoints_offset(sc));
 }
 
 sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_step, int t,
@@ -90,18 +108,22 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
         CHK(sbx_grid_body_cell(ctx, g.cap, g.center, g.gridParams, g.gridDims, g.gridCounts, g.bodyCell));
     CHK(sbx_grid_build(ctx, g.cap, g.bodyCell, g.gridCounts, g.totalCells, g.cellCount, g.chunkSum,
                        g.gridCellOffsets, g.gridCellContents, g.cap));
+    // the reach walk reads the segment endpoints in cell order (one float4 pair per grid entry)
+    float* cellE1 = dense_cell_endpoints(ctx, sc);
+    float* cellE2 = cellE1 + 4 * (size_t)std::max(g.cap, 0);
+    CHK(sbx_grid_cell_endpoints(ctx, g.cap, g.totalCells, g.gridCellOffsets, g.gridCellContents, g.ownerStore,
+                                g.ownerSlot, nSeg, fb.end1, fb.end2, cellE1, cellE2));
     if (bt) {
-        CHK(sbx_binding_grid_reachable_batched(ctx, mot.head, mot.uVec, mot.rodUVec, nSeg, fb.end1, fb.end2,
-                                               g.gridCellOffsets, g.gridCellContents, g.ownerStore, g.ownerSlot,
-                                               g.reachSeg, g.reachCount, mot.kinParams, nM, bt->motKey,
-                                               bt->gridParams, bt->gridDims));
+        CHK(sbx_fusion_grid_reachable_batched(ctx, mot.head, mot.uVec, mot.rodUVec, g.gridCellOffsets, cellE1,
+                                              cellE2, g.reachSeg, g.reachCount, mot.kinParams, nM, bt->motKey,
+                                              bt->gridParams, bt->gridDims));
         CHK(sbx_nucleotide_release_batched(ctx, nM, mot.boundSeg, mot.forceDotFil, mot.forceMag, mot.cooldown,
                                            mot.stats, mot.capStats, mot.kinParams, mot.counts, bt->motKey,
                                            bt->seeds));
     } else {
-        CHK(sbx_binding_grid_reachable(ctx, mot.head, mot.uVec, mot.rodUVec, nSeg, fb.end1, fb.end2, g.gridParams,
-                                       g.gridDims, g.gridCellOffsets, g.gridCellContents, g.ownerStore, g.ownerSlot,
-                                       g.reachSeg, g.reachCount, mot.kinParams, nM));
+        CHK(sbx_fusion_grid_reachable(ctx, mot.head, mot.uVec, mot.rodUVec, g.gridParams, g.gridDims,
+                                      g.gridCellOffsets, cellE1, cellE2, g.reachSeg, g.reachCount, mot.kinParams,
+                                      nM));
         CHK(sbx_nucleotide_release(ctx, nM, mot.boundSeg, mot.forceDotFil, mot.forceMag, mot.cooldown, mot.stats,
                                    mot.capStats, mot.kinParams, mot.counts));
     }
@@ -228,8 +250,7 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
 }
 
 size_t dense_scratch_bytes(const sbx_dense_scene* sc) {
-    return dense_row_payload_offset(sc) +
-           sizeof(float) * 6 * (2 * (size_t)std::max(sc->xl.nLinks, 0) + (size_t)std::max(sc->mot.nMotors, 0));
+    return dense_cell_endpoints_offset(sc) + 2 * sizeof(float4) * (size_t)std::max(sc->grid.cap, 0);
 }
 
 }  // namespace

@@ -64,7 +64,12 @@ struct CountingSort {
     int pStride = 0, pOff = 0;
     const int* guard = nullptr;
     float* rowPayload = nullptr;
+    // the scan's per-tile sums: scan_tile_words(nRows) ints
+    int* tileSum = nullptr;
 };
+
+// tiles of the counting sort's scan (8 scan chunks each)
+static inline size_t scan_tile_words(int nRows) { return (size_t)(nRows + 8 * SCAN_CHUNK - 1) / (8 * SCAN_CHUNK); }
 
 sbx_status counting_sort(sbx_ctx* ctx, const CountingSort& cs, const char* what);
 

@@ -35,7 +35,11 @@ constexpr int NOALLOC_CHUNK_INTS =
     ((SBX_CSR_NOALLOC_MAX_ROWS / SCAN_CHUNK + 1) + 63) / 64 * 64;
 constexpr int MAX_DEVICES = 64;
 
-static __device__ __align__(256) int g_csr_scratch[NOALLOC_CHUNK_INTS + SBX_CSR_NOALLOC_MAX_ITEMS];
+// scan tile sums: scan_tile_words(MAX_ROWS) ints, rounded up to 256 bytes
+constexpr int NOALLOC_TILE_INTS = (SBX_CSR_NOALLOC_MAX_ROWS / (8 * SCAN_CHUNK) + 1 + 63) / 64 * 64;
+
+static __device__ __align__(256) int g_csr_scratch[NOALLOC_CHUNK_INTS + NOALLOC_TILE_INTS +
+                                                   SBX_CSR_NOALLOC_MAX_ITEMS];
 
 std::mutex g_setup_mutex;
 int* g_scratch_addr[MAX_DEVICES] = {};
@@ -78,6 +82,7 @@ extern "C" sbx_status sbx_csr_build_noalloc(sbx_ctx* ctx, const int32_t* keys, i
     sbx_status st = scratch_for_device(ctx, &s);
     if (st) return st;
     CountingSort cs{keys, nullptr, 0, nItems, nRows, rowCount, s, rowOffsets, rowList, nItems,
-                    s + NOALLOC_CHUNK_INTS};
+                    s + NOALLOC_CHUNK_INTS + NOALLOC_TILE_INTS};
+    cs.tileSum = s + NOALLOC_CHUNK_INTS;
     return counting_sort(ctx, cs, "sbx_csr_build_noalloc");
 }

@@ -182,7 +182,8 @@ SBX_DEV BoxParams box_params(const float* bp, int32_t step) {
 }
 
 // ContainmentSystem.java:407-457: += into F/T only on penetration
-SBX_DEV void confine_one(const BoxParams& bx, const float c[3], const float u[3], float segLength, float bTGx,
+// Returns whether an endpoint touched a wall (F and T are unchanged otherwise).
+SBX_DEV bool confine_one(const BoxParams& bx, const float c[3], const float u[3], float segLength, float bTGx,
                          float F[3], float T[3]) {
     double cx = c[0], cy = c[1], cz = c[2];
     double ux = u[0], uy = u[1], uz = u[2];
@@ -223,6 +224,7 @@ SBX_DEV void confine_one(const BoxParams& bx, const float c[3], const float u[3]
         T[1] = (float)((double)T[1] + ty);
         T[2] = (float)((double)T[2] + tz);
     }
+    return touched;
 }
 
 // ---------------------------------------------------------------- angles
@@ -578,6 +580,44 @@ SBX_DEV int grid_reach_walk(int m, int nM, const float* head, const float* uVec,
                     }
                 }
             }
+    return out;
+}
+
+// grid_reach_walk over cell-ordered endpoints: cellE1[idx] / cellE2[idx] hold the segment
+// endpoints of grid entry idx (the slot in cellE1[idx].w as int bits, -1 for an entry that is
+// not a filament segment). The three x-neighbour cells of a (y, z) row are consecutive cell
+// ids, so their entries are one contiguous range [offsets[x0 + row], offsets[x1 + 1 + row]),
+// walked in the same order as cell by cell: the reach list is the same.
+SBX_DEV int grid_reach_walk_cells(int m, int nM, const float* head, const float* uVec, const float* rodUVec,
+                                  const float* gp, const int* gd, const int* offsets, const float4* cellE1,
+                                  const float4* cellE2, int* outSlice, float myoColTol, float alignTol) {
+    float mx = head[m], my = head[nM + m], mz = head[2 * nM + m];
+    float mux = uVec[m], muy = uVec[nM + m], muz = uVec[2 * nM + m];
+    float rux = rodUVec[m], ruy = rodUVec[nM + m], ruz = rodUVec[2 * nM + m];
+    int nX = gd[0], nY = gd[1], nZ = gd[2], nXY = nX * nY;
+    int cx = cell_coord(mx, gp[0], gp[4], nX);
+    int cy = cell_coord(my, gp[1], gp[4], nY);
+    int cz = cell_coord(mz, gp[2], gp[4], nZ);
+    int x0 = max(cx - 1, 0), x1 = min(cx + 1, nX - 1);
+    int y0 = max(cy - 1, 0), y1 = min(cy + 1, nY - 1);
+    int z0 = max(cz - 1, 0), z1 = min(cz + 1, nZ - 1);
+    int out = 0;
+    for (int zz = z0; zz <= z1; zz++)
+        for (int yy = y0; yy <= y1; yy++) {
+            int row = yy * nX + zz * nXY;
+            int start = offsets[x0 + row], end = offsets[x1 + 1 + row];
+            for (int idx = start; idx < end; idx++) {
+                float4 a = cellE1[idx], b = cellE2[idx];
+                int s = __float_as_int(a.w);
+                if (s < 0) continue;
+                float d = reach_test_dist_sq(mx, my, mz, mux, muy, muz, rux, ruy, ruz, a.x, a.y, a.z, b.x, b.y, b.z,
+                                             myoColTol, alignTol);
+                if (d >= 0.f) {
+                    if (out < MAX_CAND) outSlice[out] = s;
+                    out++;
+                }
+            }
+        }
     return out;
 }
 

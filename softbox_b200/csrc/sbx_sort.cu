@@ -100,20 +100,74 @@ __global__ void __launch_bounds__(1024) k_scan_chunks(int* chunkSum, int numChun
     if (threadIdx.x == 0) chunkSum[numChunks] = carry;
 }
 
-// SpatialGrid.gridScanAdd (SpatialGrid.java:204-227)
-__global__ void __launch_bounds__(256) k_scan_add(int* offsets, int nRows, const int* chunkSum, int numChunks,
-                                                  int* rowCount, int listCap) {
-    int b = chunkSum[blockIdx.x];
-    int base = blockIdx.x * SCAN_CHUNK;
-    for (int k = threadIdx.x; k < SCAN_CHUNK; k += blockDim.x) {
-        int c = base + k;
-        if (c < nRows) {
-            offsets[c] += b;
-            rowCount[c] = 0;
+// The counting sort's exclusive scan (SpatialGrid.gridScanLocal / gridScanChunks / gridScanAdd,
+// SpatialGrid.java:166-227, with the same outputs) as reduce-then-scan over tiles of
+// SCAN_TILE_ROWS = 8 scan chunks: k_tile_reduce writes each tile's sum; k_tile_scan adds the
+// sums of the preceding tiles itself (a strided block reduction, no single-block pass and no
+// inter-block wait), scans its tile through shared memory and writes offsets, the chunk
+// prefixes chunkSum[c] (chunkSum[numChunks] = the total), offsets[nRows] = min(total, listCap),
+// and resets the counts to zero (the scatter cursor).
+constexpr int SCAN_TILE_ROWS = 8 * SCAN_CHUNK;
+constexpr int TILE_PER_THREAD = SCAN_TILE_ROWS / 256;
+
+__device__ __forceinline__ int tile_slot(int r) { return r + (r >> 5); }     // padded: no bank conflicts
+
+__global__ void __launch_bounds__(256) k_tile_reduce(const int* rowCount, int nRows, int* tileSum) {
+    const int base = blockIdx.x * SCAN_TILE_ROWS;
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < TILE_PER_THREAD; k++) {
+        int r = base + threadIdx.x + 256 * k;
+        if (r < nRows) s += rowCount[r];
+    }
+    int total;
+    block_exclusive_scan<256>(s, &total);
+    if (threadIdx.x == 0) tileSum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(256) k_tile_scan(int* rowCount, int nRows, int* offsets, int* chunkSum, int numChunks,
+                                                   const int* tileSum, int listCap) {
+    __shared__ int sv[SCAN_TILE_ROWS + SCAN_TILE_ROWS / 32];
+    const int tile = blockIdx.x, base = tile * SCAN_TILE_ROWS;
+    int p = 0;
+    for (int k = threadIdx.x; k < tile; k += 256) p += tileSum[k];
+    int prefix;
+    block_exclusive_scan<256>(p, &prefix);
+#pragma unroll
+    for (int k = 0; k < TILE_PER_THREAD; k++) {
+        int r = threadIdx.x + 256 * k, g = base + r;
+        sv[tile_slot(r)] = g < nRows ? rowCount[g] : 0;
+    }
+    __syncthreads();
+    int v[TILE_PER_THREAD], s = 0;
+#pragma unroll
+    for (int k = 0; k < TILE_PER_THREAD; k++) {
+        v[k] = sv[tile_slot(TILE_PER_THREAD * threadIdx.x + k)];
+        s += v[k];
+    }
+    int tot;
+    int run = block_exclusive_scan<256>(s, &tot);
+#pragma unroll
+    for (int k = 0; k < TILE_PER_THREAD; k++) {
+        sv[tile_slot(TILE_PER_THREAD * threadIdx.x + k)] = run;
+        run += v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < TILE_PER_THREAD; k++) {
+        int r = threadIdx.x + 256 * k, g = base + r;
+        if (g < nRows) {
+            offsets[g] = prefix + sv[tile_slot(r)];
+            rowCount[g] = 0;
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        int total = chunkSum[numChunks];
+    if (threadIdx.x < SCAN_TILE_ROWS / SCAN_CHUNK) {
+        int c = tile * (SCAN_TILE_ROWS / SCAN_CHUNK) + threadIdx.x;
+        if (c < numChunks) chunkSum[c] = prefix + sv[tile_slot(threadIdx.x * SCAN_CHUNK)];
+    }
+    if (tile == gridDim.x - 1 && threadIdx.x == 0) {
+        int total = prefix + tot;
+        chunkSum[numChunks] = total;
         offsets[nRows] = total < listCap ? total : listCap;
     }
 }
@@ -188,6 +242,7 @@ sbx_status exclusive_scan(sbx_ctx* ctx, int* in, int n, int* out, bool zeroIn, i
 }
 
 sbx_status counting_sort(sbx_ctx* ctx, const CountingSort& cs, const char* what) {
+    if (!cs.tileSum) return fail(ctx, SBX_EINVAL, std::string(what) + ": no tile-sum scratch");
     int numChunks = (cs.nRows + SCAN_CHUNK - 1) / SCAN_CHUNK;
     int itemBlocks = blocks(cs.nBound);
     if (itemBlocks > 148 * 16) itemBlocks = 148 * 16;
@@ -195,10 +250,10 @@ sbx_status counting_sort(sbx_ctx* ctx, const CountingSort& cs, const char* what)
         return fail(ctx, SBX_ECUDA, std::string(what) + ": memset");
     if (cs.nBound > 0)
         SBX_LAUNCH(ctx, k_cs_hist, itemBlocks, 256, cs.keys, cs.nDev, cs.useDevN, cs.nBound, cs.rowCount);
-    SBX_LAUNCH(ctx, k_scan_local, numChunks, 256, cs.rowCount, cs.nRows, cs.rowOffsets, cs.chunkSum);
-    SBX_LAUNCH(ctx, k_scan_chunks, 1, 1024, cs.chunkSum, numChunks);
-    SBX_LAUNCH(ctx, k_scan_add, numChunks, 256, cs.rowOffsets, cs.nRows, cs.chunkSum, numChunks, cs.rowCount,
-               cs.listCap);
+    int numTiles = (int)scan_tile_words(cs.nRows);
+    SBX_LAUNCH(ctx, k_tile_reduce, numTiles, 256, cs.rowCount, cs.nRows, cs.tileSum);
+    SBX_LAUNCH(ctx, k_tile_scan, numTiles, 256, cs.rowCount, cs.nRows, cs.rowOffsets, cs.chunkSum, numChunks,
+               cs.tileSum, cs.listCap);
     if (cs.nBound > 0) {
         SBX_LAUNCH(ctx, k_cs_scatter, itemBlocks, 256, cs.keys, cs.nDev, cs.useDevN, cs.nBound, cs.rowOffsets,
                    cs.rowCount, cs.tmp);

@@ -86,6 +86,8 @@ sbx_status check_launch(sbx_ctx* ctx, const char* what) {
     return SBX_OK;
 }
 
+static size_t align8(size_t b) { return (b + 7) & ~(size_t)7; }
+
 sbx_status ensure_scratch(sbx_ctx* ctx, size_t bytes) {
     if (bytes <= ctx->scratch_bytes) return SBX_OK;
     cudaStreamSynchronize(ctx->stream);
@@ -374,8 +376,10 @@ __global__ void k_confine(int n, const float* coord, const float* uVec, const fl
     if (!bx.active) return;
     float c[3], u[3], f[3], t[3];
     load3(coord, n, i, c); load3(uVec, n, i, u); load3(F, n, i, f); load3(T, n, i, t);
-    confine_one(bx, c, u, segLength[i], bTG[i], f, t);
-    store3(F, n, i, f); store3(T, n, i, t);
+    if (confine_one(bx, c, u, segLength[i], bTG[i], f, t)) {
+        store3(F, n, i, f);
+        store3(T, n, i, t);
+    }
 }
 
 // MechanicsFusion.forceBuild / integDerive / integDeriveConfined (MechanicsFusion.java:52-338)
@@ -393,7 +397,7 @@ __global__ void k_force_build(int n, float* F, float* T, float* rF, float* rT, c
 }
 
 template <bool CONFINED>
-__global__ void k_integ_derive(int n, float* coord, double* coord64, float* uVec, float* yVec, float* zVec,
+__global__ void __launch_bounds__(256, 4) k_integ_derive(int n, float* coord, double* coord64, float* uVec, float* yVec, float* zVec,
                                const float* segLength, float* end1, float* end2, float* F, float* T, const float* rF,
                                const float* rT, const float* bTG, const float* bRG, const float* params,
                                const int* counts) {
@@ -406,8 +410,10 @@ __global__ void k_integ_derive(int n, float* coord, double* coord64, float* uVec
         if (bx.active) {
             float c[3], u[3], f[3], t[3];
             load3(coord, n, i, c); load3(uVec, n, i, u); load3(F, n, i, f); load3(T, n, i, t);
-            confine_one(bx, c, u, segLength[i], bTG[i], f, t);
-            store3(F, n, i, f); store3(T, n, i, t);
+            if (confine_one(bx, c, u, segLength[i], bTG[i], f, t)) {     // most rods touch no wall
+                store3(F, n, i, f);
+                store3(T, n, i, t);
+            }
         }
     } else {
         dt = params[0];
@@ -743,10 +749,12 @@ extern "C" sbx_status sbx_grid_build(sbx_ctx* ctx, int32_t cap, const int32_t* b
     SBX_REQUIRE(ctx && cap >= 0 && totalCells > 0 && bodyCell && counts && cellCount && chunkSum && offsets &&
                 contents);
     if (contentsCap < cap) return fail(ctx, SBX_EINVAL, "sbx_grid_build: contentsCap < cap");
-    sbx_status st = ensure_scratch(ctx, sizeof(int) * (size_t)std::max(cap, 1));
+    size_t tmpBytes = align8(sizeof(int) * (size_t)std::max(cap, 1));
+    sbx_status st = ensure_scratch(ctx, tmpBytes + sizeof(int) * scan_tile_words(totalCells));
     if (st) return st;
     CountingSort cs{bodyCell, counts, 1, cap, totalCells, cellCount, chunkSum, offsets, contents, contentsCap,
                     (int*)ctx->scratch};
+    cs.tileSum = reinterpret_cast<int*>(static_cast<char*>(ctx->scratch) + tmpBytes);
     return counting_sort(ctx, cs, "sbx_grid_build");
 }
 
@@ -857,6 +865,64 @@ extern "C" sbx_status sbx_binding_grid_reachable(sbx_ctx* ctx, const float* head
     SBX_LAUNCH(ctx, k_grid_reachable, blocks(nM, 128), 128, nM, head, uVec, rodUVec, nSeg, e1, e2, gp, gd, offsets,
                contents, ownerStore, ownerSlot, reachSeg, reachCount, kp);
     return check_launch(ctx, "sbx_binding_grid_reachable");
+}
+
+// The endpoints of every grid entry in cell order (for grid_reach_walk_cells): one pass over
+// the contents after the grid build, entries past offsets[C] untouched.
+__global__ void k_cell_endpoints(int C, const int* offsets, const int* contents, const int* ownerStore,
+                                 const int* ownerSlot, int nSeg, const float* e1, const float* e2, float4* cellE1,
+                                 float4* cellE2) {
+    int total = offsets[C];
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+        int j = contents[idx];
+        float4 a = make_float4(0.f, 0.f, 0.f, __int_as_float(-1)), b = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (ownerStore[j] == STORE_FILAMENT) {
+            int s = ownerSlot[j];
+            a = make_float4(e1[s], e1[nSeg + s], e1[2 * nSeg + s], __int_as_float(s));
+            b = make_float4(e2[s], e2[nSeg + s], e2[2 * nSeg + s], 0.f);
+        }
+        cellE1[idx] = a;
+        cellE2[idx] = b;
+    }
+}
+
+extern "C" sbx_status sbx_grid_cell_endpoints(sbx_ctx* ctx, int32_t cap, int32_t totalCells,
+                                              const int32_t* gridCellOffsets, const int32_t* gridCellContents,
+                                              const int32_t* ownerStore, const int32_t* ownerSlot, int32_t nSeg,
+                                              const float* e1, const float* e2, float* cellEnd1, float* cellEnd2) {
+    SBX_REQUIRE(ctx && cap >= 0 && totalCells > 0 && nSeg >= 0 && gridCellOffsets &&
+                (cap == 0 || (gridCellContents && ownerStore && ownerSlot && cellEnd1 && cellEnd2 &&
+                              ((uintptr_t)cellEnd1 & 15u) == 0 && ((uintptr_t)cellEnd2 & 15u) == 0)) &&
+                (nSeg == 0 || (e1 && e2)));
+    if (cap == 0) return SBX_OK;
+    int nb = blocks(cap);
+    if (nb > 148 * 16) nb = 148 * 16;
+    SBX_LAUNCH(ctx, k_cell_endpoints, nb, 256, totalCells, gridCellOffsets, gridCellContents, ownerStore, ownerSlot,
+               nSeg, e1, e2, reinterpret_cast<float4*>(cellEnd1), reinterpret_cast<float4*>(cellEnd2));
+    return check_launch(ctx, "sbx_grid_cell_endpoints");
+}
+
+__global__ void k_grid_reachable_cells(int nM, const float* head, const float* uVec, const float* rodUVec,
+                                       const float* gp, const int* gd, const int* offsets, const float4* cellE1,
+                                       const float4* cellE2, int* reachSeg, int* reachCount, const float* kp) {
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nM) return;
+    reachCount[m] = grid_reach_walk_cells(m, nM, head, uVec, rodUVec, gp, gd, offsets, cellE1, cellE2,
+                                          reachSeg + (int64_t)m * MAX_CAND, kp[7], kp[8]);
+}
+
+extern "C" sbx_status sbx_fusion_grid_reachable(sbx_ctx* ctx, const float* head, const float* uVec,
+                                                const float* rodUVec, const float* gp, const int32_t* gd,
+                                                const int32_t* gridCellOffsets, const float* cellEnd1,
+                                                const float* cellEnd2, int32_t* reachSeg, int32_t* reachCount,
+                                                const float* kp, int32_t nM) {
+    SBX_REQUIRE(ctx && nM >= 0 && (nM == 0 || (head && uVec && rodUVec && gp && gd && gridCellOffsets && cellEnd1 &&
+                                               cellEnd2 && reachSeg && reachCount && kp)));
+    if (nM == 0) return SBX_OK;
+    SBX_LAUNCH(ctx, k_grid_reachable_cells, blocks(nM, 128), 128, nM, head, uVec, rodUVec, gp, gd, gridCellOffsets,
+               reinterpret_cast<const float4*>(cellEnd1), reinterpret_cast<const float4*>(cellEnd2), reachSeg,
+               reachCount, kp);
+    return check_launch(ctx, "sbx_fusion_grid_reachable");
 }
 
 __global__ void k_brute_reachable(int nM, const float* head, const float* uVec, const float* rodUVec, int nSeg,
@@ -1010,10 +1076,12 @@ extern "C" sbx_status sbx_csr_build(sbx_ctx* ctx, const int32_t* keys, int32_t n
                                     int32_t* rowCount, int32_t* rowOffsets, int32_t* rowList) {
     SBX_REQUIRE(ctx && nItems >= 0 && nRows > 0 && rowCount && rowOffsets && (nItems == 0 || (keys && rowList)));
     size_t chunks = (size_t)(nRows + SCAN_CHUNK - 1) / SCAN_CHUNK + 1;
-    sbx_status st = ensure_scratch(ctx, sizeof(int) * (chunks + (size_t)std::max(nItems, 1)));
+    size_t intBytes = align8(sizeof(int) * (chunks + (size_t)std::max(nItems, 1)));
+    sbx_status st = ensure_scratch(ctx, intBytes + sizeof(int) * scan_tile_words(nRows));
     if (st) return st;
     int* s = (int*)ctx->scratch;
     CountingSort cs{keys, nullptr, 0, nItems, nRows, rowCount, s, rowOffsets, rowList, nItems, s + chunks};
+    cs.tileSum = reinterpret_cast<int*>(static_cast<char*>(ctx->scratch) + intBytes);
     return counting_sort(ctx, cs, "sbx_csr_build");
 }
 
@@ -1025,10 +1093,12 @@ extern "C" sbx_status sbx_csr_build_payload(sbx_ctx* ctx, const int32_t* keys, i
                 payloadOffset >= 0 && payloadOffset + 6 <= payloadStride &&
                 (nItems == 0 || (keys && rowList && payload && rowPayload && aligned8(rowPayload))));
     size_t chunks = (size_t)(nRows + SCAN_CHUNK - 1) / SCAN_CHUNK + 1;
-    sbx_status st = ensure_scratch(ctx, sizeof(int) * (chunks + (size_t)std::max(nItems, 1)));
+    size_t intBytes = align8(sizeof(int) * (chunks + (size_t)std::max(nItems, 1)));
+    sbx_status st = ensure_scratch(ctx, intBytes + sizeof(int) * scan_tile_words(nRows));
     if (st) return st;
     int* s = (int*)ctx->scratch;
     CountingSort cs{keys, nullptr, 0, nItems, nRows, rowCount, s, rowOffsets, rowList, nItems, s + chunks};
+    cs.tileSum = reinterpret_cast<int*>(static_cast<char*>(ctx->scratch) + intBytes);
     cs.payload = payload;
     cs.pStride = payloadStride;
     cs.pOff = payloadOffset;

@@ -213,9 +213,45 @@ class MLPEnsemble:
         return y.mean(axis=0), y.std(axis=0), y
 
 
-def fallback_mask(mean, std, threshold=0.10):
-    """Points where any output's ensemble std exceeds `threshold` of its |mean|."""
-    return (std > threshold * np.abs(mean)).any(axis=1)
+def fallback_mask(mean, std, threshold=0.10, outputs=None, scale=None):
+    """Points where an output's ensemble std exceeds `threshold` of its |mean| (any of the
+    `outputs` columns, default all); with `scale` (one value per output) |mean| is floored at
+    it, so outputs whose mean sits near zero do not fall back on their absolute noise alone."""
+    ref = np.abs(mean)
+    if scale is not None:
+        ref = np.maximum(ref, np.asarray(scale)[None, :])
+    over = std > threshold * ref
+    if outputs is not None:
+        over = over[:, list(outputs)]
+    return over.any(axis=1)
+
+
+def select_rule(mean_v, std_v, y_v, mean_f, std_f, spread, infer_s, rerun_s_per_point, per_run_s, target_col=0,
+                max_err=0.05, thresholds=(0.05, 0.1, 0.2, 0.3, 0.5), floors=(0.0, 0.25, 0.5, 1.0),
+                output_sets=((0, 1, 2), (0,))):
+    """Picks the fallback rule (outputs checked, threshold, floor as a fraction of each output's
+    training spread) with the highest sweep rate whose relative error on column `target_col`
+    over the validation points (mean_v, std_v against plain runs y_v; fallback points take their
+    plain result) stays within max_err. The sweep rate of a rule is len(mean_f) fresh points
+    over inference time plus a plain rerun for each fresh fallback point; gain = rate x the
+    plain per-run seconds. Returns (best rule or None, every rule's row)."""
+    rows = []
+    for outs in output_sets:
+        for th in thresholds:
+            for fl in floors:
+                sc = fl * spread if fl > 0 else None
+                fb_v = fallback_mask(mean_v, std_v, th, outs, sc)
+                blend = np.where(fb_v[:, None], y_v, mean_v)
+                err = np.abs(blend - y_v).mean(axis=0) / np.maximum(np.abs(y_v).mean(axis=0), 1e-30)
+                fb_f = fallback_mask(mean_f, std_f, th, outs, sc)
+                rate = len(mean_f) / (infer_s + int(fb_f.sum()) * rerun_s_per_point)
+                rows.append({"outputs": list(outs), "threshold": th, "floor": fl,
+                             "validation_fallback": float(fb_v.mean()), "validation_rel_error": err.tolist(),
+                             "fresh_fallback": float(fb_f.mean()), "points_per_s": rate,
+                             "gain_vs_plain_per_run": rate * per_run_s})
+    ok = [r for r in rows if r["validation_rel_error"][target_col] <= max_err]
+    best = max(ok, key=lambda r: r["points_per_s"]) if ok else None
+    return best, rows
 
 
 def main():

@@ -16,6 +16,11 @@ Points per second are whole-sweep figures for runs of `steps` steps:
   plain result, which gives the error of the whole rule).
 Relative error on an output: mean |prediction - plain run| / mean |plain run| over the
 held-out points.
+
+Rule selection: the fallback rule (outputs checked: all three or the contraction rate alone;
+threshold on std / |mean|; |mean| floored at a fraction of each output's training spread) is
+chosen on the first half of the held-out runs as the fastest sweep whose contraction-rate
+error there stays within --max-err, and its error is reported on the second half.
 """
 import argparse
 import json
@@ -90,6 +95,7 @@ def main():
     ap.add_argument("--per-run-sample", type=int, default=8)
     ap.add_argument("--seed", type=int, default=11)
     ap.add_argument("--turnover", action="store_true", help="every run with its point's actin turnover")
+    ap.add_argument("--max-err", type=float, default=0.05, help="contraction-rate error bound of the selected rule")
     a = ap.parse_args()
     rr = tuple(a.rods)
     pts_train = ensemble.sample_points(a.train, a.seed, rr)
@@ -137,6 +143,19 @@ def main():
                    "heldout_rel_error_with_fallback": rel_error(np.where(fbh2[:, None], y_held, mean_h), y_held),
                    "surrogate_sweep_points_per_s": a.fresh / s2}
     run_s, run_samples = per_run_seconds(pts_fresh, a.steps, a.per_run_sample, a.turnover)
+    # rule selection on one half of the held-out runs, its error reported on the other half
+    from .surrogate import fallback_mask as fbm, select_rule
+    half = a.heldout // 2
+    spread = y_train.std(axis=0)
+    best, rules = select_rule(mean_h[:half], std_h[:half], y_held[:half], mean_f, std_f, spread, infer_s,
+                              batched_s_per_point, run_s, target_col=0, max_err=a.max_err)
+    selected = None
+    if best is not None:
+        sc = best["floor"] * spread if best["floor"] > 0 else None
+        fb_t = fbm(mean_h[half:], std_h[half:], best["threshold"], best["outputs"], sc)
+        blend_t = np.where(fb_t[:, None], y_held[half:], mean_h[half:])
+        selected = dict(best, test_points=int(a.heldout - half), test_fallback=float(fb_t.mean()),
+                        test_rel_error=rel_error(blend_t, y_held[half:]))
     out = {"steps_per_run": a.steps, "turnover": a.turnover, "rods_range": rr, "train_points": a.train, "heldout_points": a.heldout,
            "fresh_points": a.fresh, "outputs": OUTPUTS,
            "plain_per_run_points_per_s": 1.0 / run_s, "per_run_sample_s": run_samples,
@@ -149,6 +168,7 @@ def main():
            "heldout_rel_error_surrogate": err_surrogate, "heldout_rel_error_with_fallback": err_with_fallback,
            "heldout_rel_error_mean_predictor": err_mean_predictor, "heldout_fallback_fraction": float(fb_h.mean()),
            "floored_rule": floored,
+           "selected_rule": selected, "max_err_contraction_rate": a.max_err, "rules": rules,
            "train_loss_first_last": [hist[0], hist[-1]], "train_s": train_s, "epochs": a.epochs,
            "data_gpu_s": gen_gpu_s + held_gpu_s, "data_build_s": gen_build_s}
     print(json.dumps(out), flush=True)

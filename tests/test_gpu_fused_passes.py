@@ -1,4 +1,4 @@
-"""The fused filament pass of the dense step against the separate reference calls, bit for bit:
+"""The fused passes of the dense step against the separate reference calls, bit for bit:
 
 * sbx_csr_build_payload: offsets and lists equal the serial CSR build, and each row's
   payload copy equals the listed items' payload (zeros where the guard is negative);
@@ -6,7 +6,10 @@
   chainForces followed by segGatherA, segGatherB and the cross-bridge segGather
   (ChainBendingForceSystem.java:105-331, CrosslinkerSystem.java:129-173,
   CrossBridgeSystem.java:302-320), with -0.0 accumulators and with the crosslinker
-  gathers skipped.
+  gathers skipped;
+* sbx_grid_cell_endpoints + sbx_fusion_grid_reachable (the reach walk over cell-ordered
+  endpoints): reach lists and counts equal the oracle's gridReachable
+  (BindingDetectionSystem.java:143-228).
 """
 import copy
 
@@ -117,3 +120,32 @@ def test_chain_gathers_equal_chain_then_gathers(orc_dm, warm, xl_on, neg_zero):
     assert_same(fb["forceSum"], D.to_host(dfb["forceSum"]), "forceSum")
     assert_same(fb["torqueSum"], D.to_host(dfb["torqueSum"]), "torqueSum")
     assert (xl["linkState"] < 0).any() and (xl["linkState"] >= 0).any()
+
+
+def test_cell_endpoint_walk_equals_grid_reachable(orc_dm, warm):
+    sc = copy.deepcopy(warm)
+    m, g, fb = sc["mot"], sc["grid"], sc["fil"]["body"]
+    nM, nSeg, cap = m["nMotors"], fb["n"], int(g["cap"])
+    d = D.to_device({"m": m, "g": g, "e1": fb["end1"], "e2": fb["end2"]})
+    dm, dg = d["m"], d["g"]
+    orc_dm.grid_reachable(nM, m["head"], m["uVec"], m["rodUVec"], nSeg, fb["end1"], fb["end2"], g["gridParams"],
+                          g["gridDims"], g["gridCellOffsets"], g["gridCellContents"], g["ownerStore"],
+                          g["ownerSlot"], g["reachSeg"], g["reachCount"], m["kinParams"])
+    ce1 = torch.zeros(4 * cap, dtype=torch.float32, device="cuda")
+    ce2 = torch.zeros(4 * cap, dtype=torch.float32, device="cuda")
+    dg["reachSeg"].fill_(-7)
+    dg["reachCount"].fill_(-7)
+    c = _ctx()
+    c("sbx_grid_cell_endpoints", cap, int(g["totalCells"]), dg["gridCellOffsets"], dg["gridCellContents"],
+      dg["ownerStore"], dg["ownerSlot"], nSeg, d["e1"], d["e2"], ce1, ce2)
+    c("sbx_fusion_grid_reachable", dm["head"], dm["uVec"], dm["rodUVec"], dg["gridParams"], dg["gridDims"],
+      dg["gridCellOffsets"], ce1, ce2, dg["reachSeg"], dg["reachCount"], dm["kinParams"], nM)
+    torch.cuda.synchronize()
+    hc = D.to_host(dg["reachCount"])
+    assert_same(g["reachCount"], hc, "reachCount")
+    hs = D.to_host(dg["reachSeg"]).reshape(nM, -1)
+    want = g["reachSeg"].reshape(nM, -1)
+    for i in range(nM):
+        k = min(int(hc[i]), want.shape[1])
+        assert_same(want[i, :k], hs[i, :k], f"reachSeg row {i}")
+    assert hc.sum() > 0
