@@ -169,8 +169,10 @@ class MLPEnsemble:
         self.backward()
         self.adam()
 
-    def fit(self, X, Y, epochs=100, seed=0, log=None):
-        """Trains every member on (X, Y) with its own shuffling; returns the loss history."""
+    def fit(self, X, Y, epochs=100, seed=0, log=None, bootstrap=False):
+        """Trains every member on (X, Y) with its own shuffling (with `bootstrap`, each member
+        on its own resample of the points drawn with replacement, so the members' spread
+        reflects what the data leaves open); returns the loss history."""
         t = self.torch
         if self.x_mean is None:
             self.set_normalisation(X, Y)
@@ -178,10 +180,11 @@ class MLPEnsemble:
         Yn = t.tensor((np.asarray(Y) - self.y_mean) / self.y_std, dtype=t.float32, device=self.dev)
         n = Xn.shape[0]
         g = t.Generator(device="cpu").manual_seed(seed)
+        samples = [t.randint(0, n, (n,), generator=g) if bootstrap else t.arange(n) for _ in range(self.nz)]
         hist = []
         steps = max(1, n // self.B)
         for ep in range(epochs):
-            perms = t.stack([t.randperm(n, generator=g) for _ in range(self.nz)]).to(self.dev)
+            perms = t.stack([smp[t.randperm(n, generator=g)] for smp in samples]).to(self.dev)
             for s in range(steps):
                 idx = perms[:, s * self.B:(s + 1) * self.B]
                 if idx.shape[1] < self.B:

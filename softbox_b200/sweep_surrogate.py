@@ -96,14 +96,30 @@ def main():
     ap.add_argument("--seed", type=int, default=11)
     ap.add_argument("--turnover", action="store_true", help="every run with its point's actin turnover")
     ap.add_argument("--max-err", type=float, default=0.05, help="contraction-rate error bound of the selected rule")
+    ap.add_argument("--save-data", default="", help="write the plain runs' targets and timings to this .npz")
+    ap.add_argument("--load-data", default="", help="reuse the plain runs of a --save-data file (same settings)")
+    ap.add_argument("--train-grid", action="store_true",
+                    help="also train ensembles for 25/50/100/200 epochs, with and without bootstrap resampling, "
+                         "and select training and rule together on the validation half")
     a = ap.parse_args()
     rr = tuple(a.rods)
     pts_train = ensemble.sample_points(a.train, a.seed, rr)
     pts_held = ensemble.sample_points(a.heldout, a.seed + 1, rr)
     pts_fresh = ensemble.sample_points(a.fresh, a.seed + 2, rr)
 
-    y_train, gen_gpu_s, gen_build_s = generate(pts_train, a.steps, a.sample_every, turnover=a.turnover)
-    y_held, held_gpu_s, _ = generate(pts_held, a.steps, a.sample_every, turnover=a.turnover)
+    sig = np.array([a.train, a.heldout, a.steps, a.sample_every, a.seed, rr[0], rr[1], int(a.turnover)], np.int64)
+    if a.load_data:
+        z = np.load(a.load_data)
+        if not np.array_equal(z["sig"], sig):
+            raise SystemExit(f"{a.load_data} was generated with other sweep settings")
+        y_train, y_held = z["y_train"], z["y_held"]
+        gen_gpu_s, held_gpu_s, gen_build_s = float(z["gen_gpu_s"]), float(z["held_gpu_s"]), float(z["gen_build_s"])
+    else:
+        y_train, gen_gpu_s, gen_build_s = generate(pts_train, a.steps, a.sample_every, turnover=a.turnover)
+        y_held, held_gpu_s, _ = generate(pts_held, a.steps, a.sample_every, turnover=a.turnover)
+        if a.save_data:
+            np.savez(a.save_data, sig=sig, y_train=y_train, y_held=y_held, gen_gpu_s=gen_gpu_s,
+                     held_gpu_s=held_gpu_s, gen_build_s=gen_build_s)
     batched_s_per_point = (gen_gpu_s + held_gpu_s) / (a.train + a.heldout)
 
     x_train = ensemble.features(pts_train, rr)
@@ -156,7 +172,30 @@ def main():
         blend_t = np.where(fb_t[:, None], y_held[half:], mean_h[half:])
         selected = dict(best, test_points=int(a.heldout - half), test_fallback=float(fb_t.mean()),
                         test_rel_error=rel_error(blend_t, y_held[half:]))
-    out = {"steps_per_run": a.steps, "turnover": a.turnover, "rods_range": rr, "train_points": a.train, "heldout_points": a.heldout,
+    grid, chosen = [], None
+    if a.train_grid:
+        for boot in (False, True):
+            for ep in (25, 50, 100, 200):
+                e2 = MLPEnsemble(n_nets=5, seed=a.seed)
+                e2.fit(x_train, y_train, epochs=ep, bootstrap=boot)
+                mh, sh, _ = e2.predict(x_held)
+                mf, sf, _ = e2.predict(x_fresh)
+                b2, _ = select_rule(mh[:half], sh[:half], y_held[:half], mf, sf, spread, infer_s,
+                                    batched_s_per_point, run_s, target_col=0, max_err=a.max_err)
+                row = {"epochs": ep, "bootstrap": boot, "validation_rel_error_surrogate": rel_error(mh[:half],
+                                                                                                y_held[:half]),
+                       "best_rule": b2}
+                if b2 is not None:
+                    sc = b2["floor"] * spread if b2["floor"] > 0 else None
+                    fb_t = fbm(mh[half:], sh[half:], b2["threshold"], b2["outputs"], sc)
+                    row["test_fallback"] = float(fb_t.mean())
+                    row["test_rel_error"] = rel_error(np.where(fb_t[:, None], y_held[half:], mh[half:]),
+                                                      y_held[half:])
+                    row["test_rel_error_surrogate"] = rel_error(mh[half:], y_held[half:])
+                grid.append(row)
+        ok = [r for r in grid if r["best_rule"] is not None]
+        chosen = max(ok, key=lambda r: r["best_rule"]["points_per_s"]) if ok else None
+    out = {"steps_per_run": a.steps, "turnover": a.turnover, "train_grid": grid, "selected_training": chosen, "rods_range": rr, "train_points": a.train, "heldout_points": a.heldout,
            "fresh_points": a.fresh, "outputs": OUTPUTS,
            "plain_per_run_points_per_s": 1.0 / run_s, "per_run_sample_s": run_samples,
            "plain_batched_points_per_s": 1.0 / batched_s_per_point,
