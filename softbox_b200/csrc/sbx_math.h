@@ -127,6 +127,17 @@ SBX_HD double cos(double x) {
 #endif
 }
 
+// sin(x) and cos(x) together: one reduction and one evaluation of each polynomial, each
+// result selected exactly as sin() and cos() above select it (the same bits)
+SBX_HD void sincos(double x, double* sOut, double* cOut) {
+    int q; double r = reduce_pio2(x, &q);
+    double sp = sin_poly(r), cp = cos_poly(r);
+    double vs = (q & 1) ? cp : sp;
+    double vc = (q & 1) ? sp : cp;
+    *sOut = (q & 2) ? -vs : vs;
+    *cOut = ((q + 1) & 2) ? -vc : vc;
+}
+
 // natural log of a positive double (x <= 0 -> -inf / NaN like libm)
 SBX_HD double log(double x) {
     if (!(x > 0.0)) return (x == 0.0) ? bitsd(0xfff0000000000000ULL) : bitsd(0x7ff8000000000000ULL);

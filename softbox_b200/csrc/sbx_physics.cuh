@@ -30,18 +30,22 @@ SBX_DEV float fsqrt(float x) { return __fsqrt_rn(x); }
 // Box-Muller of BrownianForceSystem.java:88-104; g = {gfx,gfy,gfz,gtx,gty,gtz}
 SBX_DEV void box_muller6(float u1, float u2, float u3, float u4, float u5, float u6, float g[6]) {
     const float TWO_PI_F = 2.0f * 3.14159265f;
+    double sn, cs;
     float r1 = fsqrt(-2.0f * (float)sbxm::log((double)u1));
     float th1 = TWO_PI_F * u2;
-    g[0] = r1 * (float)sbxm::cos((double)th1);
-    g[3] = r1 * (float)sbxm::sin((double)th1);
+    sbxm::sincos((double)th1, &sn, &cs);
+    g[0] = r1 * (float)cs;
+    g[3] = r1 * (float)sn;
     float r2 = fsqrt(-2.0f * (float)sbxm::log((double)u3));
     float th2 = TWO_PI_F * u4;
-    g[1] = r2 * (float)sbxm::cos((double)th2);
-    g[4] = r2 * (float)sbxm::sin((double)th2);
+    sbxm::sincos((double)th2, &sn, &cs);
+    g[1] = r2 * (float)cs;
+    g[4] = r2 * (float)sn;
     float r3 = fsqrt(-2.0f * (float)sbxm::log((double)u5));
     float th3 = TWO_PI_F * u6;
-    g[2] = r3 * (float)sbxm::cos((double)th3);
-    g[5] = r3 * (float)sbxm::sin((double)th3);
+    sbxm::sincos((double)th3, &sn, &cs);
+    g[2] = r3 * (float)cs;
+    g[5] = r3 * (float)sn;
 }
 
 // BrownianForceSystem.java:74-86: keyed (slot, step, seed)
@@ -248,20 +252,22 @@ SBX_DEV double accurate_acos(double x) {
         p = p * sqrt(1.0 - ax);
         y = (x < 0.0) ? (3.141592653589793 - p) : p;
     }
-    double s = sbxm::sin(y);
-    if (s > 1.0e-12 || s < -1.0e-12) y = y + (sbxm::cos(y) - x) / s;
-    s = sbxm::sin(y);
-    if (s > 1.0e-12 || s < -1.0e-12) y = y + (sbxm::cos(y) - x) / s;
+    double s, c;
+    sbxm::sincos(y, &s, &c);
+    if (s > 1.0e-12 || s < -1.0e-12) y = y + (c - x) / s;
+    sbxm::sincos(y, &s, &c);
+    if (s > 1.0e-12 || s < -1.0e-12) y = y + (c - x) / s;
     return y;
 }
 
 SBX_DEV double accurate_asin(double s) {                    // ChainBendingForceSystem.java:76-84
     double s2 = s * s;
     double y = s * (1.0 + s2 * (0.16666666666666666 + s2 * (0.075 + s2 * 0.044642857142857)));
-    double cy = sbxm::cos(y);
-    if (cy > 1.0e-12) y = y + (s - sbxm::sin(y)) / cy;
-    cy = sbxm::cos(y);
-    if (cy > 1.0e-12) y = y + (s - sbxm::sin(y)) / cy;
+    double sy, cy;
+    sbxm::sincos(y, &sy, &cy);
+    if (cy > 1.0e-12) y = y + (s - sy) / cy;
+    sbxm::sincos(y, &sy, &cy);
+    if (cy > 1.0e-12) y = y + (s - sy) / cy;
     return y;
 }
 
