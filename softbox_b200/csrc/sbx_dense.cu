@@ -79,8 +79,58 @@ float* dense_cell_endpoints(sbx_ctx* ctx, const sbx_dense_scene* sc) {
     return reinterpret_cast<float*>(static_cast<char*>(ctx->scratch) + dense_cell_endpoints_offset(sc));
 }
 
+// A second stream for the filament-side work of a step (owned by a plan): the fork and join
+// events and that stream's own sort scratch, so that its CSR builds and the minifilament
+// CSR build on the main stream never share temporaries.
+struct SideStream {
+    cudaStream_t stream;
+    cudaEvent_t fork, join;
+    void* scratch;
+    size_t scratchBytes;
+};
+
+// Moves the context's launches (and its sort scratch) to the side stream for a scope, after
+// the side stream waits for the work already on the main stream; at scope end the side
+// stream records the join event and the context is restored.
+struct SideScope {
+    sbx_ctx* ctx;
+    const SideStream* side;
+    cudaStream_t savedStream = nullptr;
+    void* savedScratch = nullptr;
+    size_t savedBytes = 0;
+    sbx_status status = SBX_OK;
+    SideScope(sbx_ctx* c, const SideStream* s) : ctx(c), side(s) {
+        if (!side) return;
+        if (cudaEventRecord(side->fork, ctx->stream) != cudaSuccess ||
+            cudaStreamWaitEvent(side->stream, side->fork, 0) != cudaSuccess) {
+            status = fail(ctx, SBX_ECUDA, "dense step: side-stream fork");
+            side = nullptr;
+            return;
+        }
+        savedStream = ctx->stream;
+        savedScratch = ctx->scratch;
+        savedBytes = ctx->scratch_bytes;
+        ctx->stream = side->stream;
+        ctx->scratch = side->scratch;
+        ctx->scratch_bytes = side->scratchBytes;
+    }
+    ~SideScope() {
+        if (!side) return;
+        cudaEventRecord(side->join, side->stream);
+        ctx->stream = savedStream;
+        ctx->scratch = savedScratch;
+        ctx->scratch_bytes = savedBytes;
+    }
+};
+
+sbx_status side_join(sbx_ctx* ctx, const SideStream* side) {
+    if (cudaStreamWaitEvent(ctx->stream, side->join, 0) != cudaSuccess)
+        return fail(ctx, SBX_ECUDA, "dense step: side-stream join");
+    return SBX_OK;
+}
+
 sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_step, int t,
-                          const sbx_batch* bt = nullptr) {
+                          const sbx_batch* bt = nullptr, const SideStream* side = nullptr) {
     const sbx_filament_store& f = sc->fil;
     const sbx_motor_store& mot = sc->mot;
     const sbx_dimer_store& dim = sc->dim;
@@ -135,6 +185,52 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
     else
         CHK(sbx_nucleotide_cycle(ctx, nM, mot.nucleotideState, mot.boundSeg, mot.forceDotHist, mot.nucParams,
                                  mot.counts));
+    // (iii)-(v) filaments, the part that needs nothing from the minifilament structure below:
+    // draws, crosslinker kernels and the crosslinker CSR builds. With a side stream it runs
+    // concurrently with (ii); the streams join before the motor CSR, which reads the
+    // cross-bridge payload. The row-ordered payload copies live in the main scratch.
+    float* payA = dense_row_payload(ctx, sc);
+    float* payB = payA + 6 * (size_t)std::max(xl.nLinks, 0);
+    float* payM = payB + 6 * (size_t)std::max(xl.nLinks, 0);
+    {
+        SideScope onSide(ctx, side);
+        if (side) CHK(onSide.status);
+        if (bt) {
+            CHK(sbx_zero_accumulators(ctx, nSeg, fb.forceSum, fb.torqueSum));
+            CHK(sbx_brownian_force_batched(ctx, nSeg, 1, fb.randForce, fb.randTorque, fb.bTransGam, fb.bRotGam,
+                                           fb.brownTransScale, fb.brownRotScale, f.params, f.counts, bt->segKey,
+                                           bt->seeds, 2));
+        } else {
+            CHK(sbx_fusion_force_build(ctx, nSeg, fb.forceSum, fb.torqueSum, fb.randForce, fb.randTorque,
+                                       fb.bTransGam, fb.bRotGam, fb.brownTransScale, fb.brownRotScale, f.params,
+                                       f.counts));
+        }
+        // The crosslinker kernels and the CSR builds read no filament accumulator, so they run
+        // before the chain forces; chain and the three gathers then share one pass
+        // (sbx_fusion_chain_gathers), each gather reading its row-ordered payload copy made by
+        // the CSR build. The accumulators get the bits of chain, segGatherA, segGatherB, segGather.
+        if (xlOn) {
+            if (sc->xlUnbind && bt)
+                CHK(sbx_xlink_unbind_batched(ctx, nSeg, fb.uVec, fb.end1, xl.nLinks, xl.linkFilA, xl.linkFilB,
+                                             xl.loc1, xl.loc2, xl.linkState, xl.strainHist, xl.strainPlace,
+                                             xl.offParams, xl.counts, bt->linkKey, bt->seeds));
+            else if (sc->xlUnbind)
+                CHK(sbx_xlink_unbind(ctx, nSeg, fb.uVec, fb.end1, xl.nLinks, xl.linkFilA, xl.linkFilB, xl.loc1,
+                                     xl.loc2, xl.linkState, xl.strainHist, xl.strainPlace, xl.offParams,
+                                     xl.counts));
+            CHK(sbx_xlink_count_active(ctx, xl.nLinks, xl.linkState, xl.linkFilA, xl.linkFilB, nSeg,
+                                       xl.activeLinkCount));
+            CHK(sbx_xlink_forces(ctx, nSeg, fb.coord, fb.uVec, fb.end1, fb.bTransGam, xl.nLinks, xl.linkFilA,
+                                 xl.linkFilB, xl.loc1, xl.loc2, xl.activeLinkCount, xl.xlinkData, xl.xlParams));
+            CHK(sbx_xlink_torsion(ctx, nSeg, fb.uVec, xl.nLinks, xl.linkFilA, xl.linkFilB, xl.linkState,
+                                  xl.linkOrientSame, xl.torqueMagHist, xl.torqueMagPlace, xl.xlinkData,
+                                  xl.torsionParams));
+            CHK(sbx_csr_build_payload(ctx, xl.linkFilA, xl.nLinks, nSeg, xl.segCountA, xl.segOffsetsA,
+                                      xl.segIdxA, xl.xlinkData, XL_STRIDE, 0, xl.linkState, payA));
+            CHK(sbx_csr_build_payload(ctx, xl.linkFilB, xl.nLinks, nSeg, xl.segCountB, xl.segOffsetsB,
+                                      xl.segIdxB, xl.xlinkData, XL_STRIDE, 6, xl.linkState, payB));
+        }
+    }
     // (ii) minifilament structure. A single network zeroes and draws in one pass per store
     // (MechanicsFusion.forceBuild, the same values as the zero + Brownian pair)
     if (!bt) {
@@ -192,43 +288,7 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
     }
     CHK(sbx_xbridge_register_force_dot(ctx, nM, sc->bondData, mot.boundSeg, mot.forceDotFil, mot.forceMag,
                                        mot.forceDotHist, mot.forceDotPlace));
-    // (iii)-(v) filaments
-    if (bt) {
-        CHK(sbx_zero_accumulators(ctx, nSeg, fb.forceSum, fb.torqueSum));
-        CHK(sbx_brownian_force_batched(ctx, nSeg, 1, fb.randForce, fb.randTorque, fb.bTransGam, fb.bRotGam,
-                                       fb.brownTransScale, fb.brownRotScale, f.params, f.counts, bt->segKey,
-                                       bt->seeds, 2));
-    } else {
-        CHK(sbx_fusion_force_build(ctx, nSeg, fb.forceSum, fb.torqueSum, fb.randForce, fb.randTorque, fb.bTransGam,
-                                   fb.bRotGam, fb.brownTransScale, fb.brownRotScale, f.params, f.counts));
-    }
-    // The crosslinker kernels and the three CSR builds read no filament accumulator, so they run
-    // before the chain forces; chain and the three gathers then share one pass
-    // (sbx_fusion_chain_gathers), each gather reading its row-ordered payload copy made by the
-    // CSR build. The accumulators get the bits of chain, segGatherA, segGatherB, segGather.
-    float* payA = dense_row_payload(ctx, sc);
-    float* payB = payA + 6 * (size_t)std::max(xl.nLinks, 0);
-    float* payM = payB + 6 * (size_t)std::max(xl.nLinks, 0);
-    if (xlOn) {
-        if (sc->xlUnbind && bt)
-            CHK(sbx_xlink_unbind_batched(ctx, nSeg, fb.uVec, fb.end1, xl.nLinks, xl.linkFilA, xl.linkFilB, xl.loc1,
-                                         xl.loc2, xl.linkState, xl.strainHist, xl.strainPlace, xl.offParams,
-                                         xl.counts, bt->linkKey, bt->seeds));
-        else if (sc->xlUnbind)
-            CHK(sbx_xlink_unbind(ctx, nSeg, fb.uVec, fb.end1, xl.nLinks, xl.linkFilA, xl.linkFilB, xl.loc1, xl.loc2,
-                                 xl.linkState, xl.strainHist, xl.strainPlace, xl.offParams, xl.counts));
-        CHK(sbx_xlink_count_active(ctx, xl.nLinks, xl.linkState, xl.linkFilA, xl.linkFilB, nSeg,
-                                   xl.activeLinkCount));
-        CHK(sbx_xlink_forces(ctx, nSeg, fb.coord, fb.uVec, fb.end1, fb.bTransGam, xl.nLinks, xl.linkFilA,
-                             xl.linkFilB, xl.loc1, xl.loc2, xl.activeLinkCount, xl.xlinkData, xl.xlParams));
-        CHK(sbx_xlink_torsion(ctx, nSeg, fb.uVec, xl.nLinks, xl.linkFilA, xl.linkFilB, xl.linkState,
-                              xl.linkOrientSame, xl.torqueMagHist, xl.torqueMagPlace, xl.xlinkData,
-                              xl.torsionParams));
-        CHK(sbx_csr_build_payload(ctx, xl.linkFilA, xl.nLinks, nSeg, xl.segCountA, xl.segOffsetsA, xl.segIdxA,
-                                  xl.xlinkData, XL_STRIDE, 0, xl.linkState, payA));
-        CHK(sbx_csr_build_payload(ctx, xl.linkFilB, xl.nLinks, nSeg, xl.segCountB, xl.segOffsetsB, xl.segIdxB,
-                                  xl.xlinkData, XL_STRIDE, 6, xl.linkState, payB));
-    }
+    if (side) CHK(side_join(ctx, side));
     CHK(sbx_csr_build_payload(ctx, mot.boundSeg, nM, nSeg, sc->segMotorCount, sc->segMotorOffsets, sc->segMotorMyo,
                               sc->bondData, XB_STRIDE, 6, nullptr, payM));
     CHK(sbx_fusion_chain_gathers(ctx, nSeg, fb.coord, fb.uVec, fb.segLength, f.end2NbrSlot, f.end2NbrSide,
@@ -277,6 +337,9 @@ struct sbx_dense_plan {
     // context needs a larger context scratch
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
+    // the side stream of the step's filament-side work, with its own sort scratch
+    SideStream side{};
+    bool sideOk = false;
 };
 
 namespace {
@@ -297,6 +360,14 @@ struct PlanScratch {
         ctx->scratch_bytes = savedBytes;
     }
 };
+
+void release_side(sbx_dense_plan* p) {
+    if (p->side.scratch) cudaFree(p->side.scratch);
+    if (p->side.join) cudaEventDestroy(p->side.join);
+    if (p->side.fork) cudaEventDestroy(p->side.fork);
+    if (p->side.stream) cudaStreamDestroy(p->side.stream);
+    p->side = SideStream{};
+}
 
 }  // namespace
 
@@ -462,6 +533,19 @@ static sbx_status plan_create(sbx_ctx* ctx, const sbx_dense_scene* sc, const sbx
         delete p;
         return fail(ctx, SBX_ENOMEM, "sbx_dense_plan_create: step word");
     }
+    p->side.scratchBytes = dense_sort_bytes(sc);
+    p->sideOk = cudaStreamCreateWithFlags(&p->side.stream, cudaStreamNonBlocking) == cudaSuccess &&
+                cudaEventCreateWithFlags(&p->side.fork, cudaEventDisableTiming) == cudaSuccess &&
+                cudaEventCreateWithFlags(&p->side.join, cudaEventDisableTiming) == cudaSuccess &&
+                cudaMalloc(&p->side.scratch, p->side.scratchBytes) == cudaSuccess;
+    if (!p->sideOk) {
+        release_side(p);
+        cudaFree(p->d_step);
+        cudaFree(p->scratch);
+        delete p;
+        cudaGetLastError();
+        return fail(ctx, SBX_ENOMEM, "sbx_dense_plan_create: side stream");
+    }
     // capture one step into a graph
     cudaStreamSynchronize(ctx->stream);
     int64_t l0 = ctx->launches;
@@ -473,7 +557,7 @@ static sbx_status plan_create(sbx_ctx* ctx, const sbx_dense_scene* sc, const sbx
     sbx_status st;
     {
         PlanScratch use(p);
-        st = dense_sequence(ctx, &p->scene, p->d_step, 0, p->batched ? &p->batch : nullptr);
+        st = dense_sequence(ctx, &p->scene, p->d_step, 0, p->batched ? &p->batch : nullptr, &p->side);
     }
     if (st == SBX_OK) SBX_LAUNCH(ctx, k_step_advance, 1, 1, p->d_step);
     cudaError_t ce = cudaStreamEndCapture(ctx->stream, &p->graph);
@@ -481,6 +565,7 @@ static sbx_status plan_create(sbx_ctx* ctx, const sbx_dense_scene* sc, const sbx
         if (p->graph) cudaGraphDestroy(p->graph);
         cudaFree(p->d_step);
         cudaFree(p->scratch);
+        release_side(p);
         delete p;
         cudaGetLastError();
         return st != SBX_OK ? st : fail(ctx, SBX_ECUDA, std::string("end capture: ") + cudaGetErrorString(ce));
@@ -491,6 +576,7 @@ static sbx_status plan_create(sbx_ctx* ctx, const sbx_dense_scene* sc, const sbx
         cudaGraphDestroy(p->graph);
         cudaFree(p->d_step);
         cudaFree(p->scratch);
+        release_side(p);
         delete p;
         return fail(ctx, SBX_ECUDA, "sbx_dense_plan_create: instantiate");
     }
@@ -550,7 +636,7 @@ extern "C" sbx_status sbx_dense_plan_run(sbx_dense_plan* p, int32_t t0, int32_t 
     }
     PlanScratch use(p);
     for (int k = 0; k < nsteps; k++)
-        CHK(dense_sequence(ctx, &p->scene, nullptr, t0 + k, p->batched ? &p->batch : nullptr));
+        CHK(dense_sequence(ctx, &p->scene, nullptr, t0 + k, p->batched ? &p->batch : nullptr, &p->side));
     return SBX_OK;
 }
 
@@ -598,6 +684,7 @@ extern "C" sbx_status sbx_dense_plan_destroy(sbx_dense_plan* p) {
     if (p->graph) cudaGraphDestroy(p->graph);
     if (p->d_step) cudaFree(p->d_step);
     if (p->scratch) cudaFree(p->scratch);
+    release_side(p);
     for (void* q : p->allocs) cudaFree(q);
     delete p;
     return SBX_OK;
