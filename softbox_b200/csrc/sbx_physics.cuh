@@ -607,23 +607,47 @@ SBX_DEV int grid_reach_walk_cells(int m, int nM, const float* head, const float*
     int x0 = max(cx - 1, 0), x1 = min(cx + 1, nX - 1);
     int y0 = max(cy - 1, 0), y1 = min(cy + 1, nY - 1);
     int z0 = max(cz - 1, 0), z1 = min(cz + 1, nZ - 1);
+    // the (up to) nine row ranges as one sequence k = 0..total-1 (row order, then index
+    // order), taken four entries at a time so that their loads are in flight together
+    int rs[9], pre[10];
+    pre[0] = 0;
+#pragma unroll
+    for (int r = 0; r < 9; r++) {
+        int zz = z0 + r / 3, yy = y0 + r % 3;
+        bool ok = zz <= z1 && yy <= y1;
+        int row = yy * nX + zz * nXY;
+        rs[r] = ok ? offsets[x0 + row] : 0;
+        pre[r + 1] = pre[r] + (ok ? offsets[x1 + 1 + row] - rs[r] : 0);
+    }
+    const int total = pre[9];
     int out = 0;
-    for (int zz = z0; zz <= z1; zz++)
-        for (int yy = y0; yy <= y1; yy++) {
-            int row = yy * nX + zz * nXY;
-            int start = offsets[x0 + row], end = offsets[x1 + 1 + row];
-            for (int idx = start; idx < end; idx++) {
-                float4 a = cellE1[idx], b = cellE2[idx];
-                int s = __float_as_int(a.w);
-                if (s < 0) continue;
-                float d = reach_test_dist_sq(mx, my, mz, mux, muy, muz, rux, ruy, ruz, a.x, a.y, a.z, b.x, b.y, b.z,
-                                             myoColTol, alignTol);
-                if (d >= 0.f) {
-                    if (out < MAX_CAND) outSlice[out] = s;
-                    out++;
-                }
+    for (int k0 = 0; k0 < total; k0 += 4) {
+        float4 a[4], b[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            int k = k0 + q;
+            if (k < total) {
+                int idx = rs[0] + k;
+#pragma unroll
+                for (int r = 1; r < 9; r++)
+                    if (k >= pre[r]) idx = rs[r] + (k - pre[r]);
+                a[q] = cellE1[idx];
+                b[q] = cellE2[idx];
             }
         }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (k0 + q >= total) break;
+            int s = __float_as_int(a[q].w);
+            if (s < 0) continue;
+            float d = reach_test_dist_sq(mx, my, mz, mux, muy, muz, rux, ruy, ruz, a[q].x, a[q].y, a[q].z, b[q].x,
+                                         b[q].y, b[q].z, myoColTol, alignTol);
+            if (d >= 0.f) {
+                if (out < MAX_CAND) outSlice[out] = s;
+                out++;
+            }
+        }
+    }
     return out;
 }
 
