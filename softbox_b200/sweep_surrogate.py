@@ -97,6 +97,8 @@ def main():
     ap.add_argument("--turnover", action="store_true", help="every run with its point's actin turnover")
     ap.add_argument("--max-err", type=float, default=0.05, help="contraction-rate error bound of the selected rule")
     ap.add_argument("--save-data", default="", help="write the plain runs' targets and timings to this .npz")
+    ap.add_argument("--retime-batched", type=int, default=0,
+                    help="time the packed rerun cost on a fresh batch of this many training points")
     ap.add_argument("--load-data", default="", help="reuse the plain runs of a --save-data file (same settings)")
     ap.add_argument("--train-grid", action="store_true",
                     help="also train ensembles for 25/50/100/200 epochs, with and without bootstrap resampling, "
@@ -121,6 +123,10 @@ def main():
             np.savez(a.save_data, sig=sig, y_train=y_train, y_held=y_held, gen_gpu_s=gen_gpu_s,
                      held_gpu_s=held_gpu_s, gen_build_s=gen_build_s)
     batched_s_per_point = (gen_gpu_s + held_gpu_s) / (a.train + a.heldout)
+    if a.retime_batched > 0:                 # the rerun cost from a fresh packed batch of this build
+        _, rt_gpu_s, _ = generate(pts_train[:a.retime_batched], a.steps, a.sample_every, batch=a.retime_batched,
+                                  turnover=a.turnover)
+        batched_s_per_point = rt_gpu_s / a.retime_batched
 
     x_train = ensemble.features(pts_train, rr)
     x_held = ensemble.features(pts_held, rr)
@@ -195,7 +201,8 @@ def main():
                 grid.append(row)
         ok = [r for r in grid if r["best_rule"] is not None]
         chosen = max(ok, key=lambda r: r["best_rule"]["points_per_s"]) if ok else None
-    out = {"steps_per_run": a.steps, "turnover": a.turnover, "train_grid": grid, "selected_training": chosen, "rods_range": rr, "train_points": a.train, "heldout_points": a.heldout,
+    out = {"steps_per_run": a.steps, "turnover": a.turnover, "train_grid": grid, "selected_training": chosen,
+           "batched_s_per_point": batched_s_per_point, "batched_retimed_on": a.retime_batched, "rods_range": rr, "train_points": a.train, "heldout_points": a.heldout,
            "fresh_points": a.fresh, "outputs": OUTPUTS,
            "plain_per_run_points_per_s": 1.0 / run_s, "per_run_sample_s": run_samples,
            "plain_batched_points_per_s": 1.0 / batched_s_per_point,
