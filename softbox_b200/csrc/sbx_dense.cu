@@ -84,7 +84,8 @@ float* dense_cell_endpoints(sbx_ctx* ctx, const sbx_dense_scene* sc) {
 // CSR build on the main stream never share temporaries.
 struct SideStream {
     cudaStream_t stream;
-    cudaEvent_t fork, join;
+    cudaEvent_t fork, join;      // filament-side head of the step
+    cudaEvent_t fork2, join2;    // motor-side tail of the step
     void* scratch;
     size_t scratchBytes;
 };
@@ -95,14 +96,17 @@ struct SideStream {
 struct SideScope {
     sbx_ctx* ctx;
     const SideStream* side;
+    cudaEvent_t join = nullptr;
     cudaStream_t savedStream = nullptr;
     void* savedScratch = nullptr;
     size_t savedBytes = 0;
     sbx_status status = SBX_OK;
-    SideScope(sbx_ctx* c, const SideStream* s) : ctx(c), side(s) {
+    SideScope(sbx_ctx* c, const SideStream* s, bool tail = false) : ctx(c), side(s) {
         if (!side) return;
-        if (cudaEventRecord(side->fork, ctx->stream) != cudaSuccess ||
-            cudaStreamWaitEvent(side->stream, side->fork, 0) != cudaSuccess) {
+        cudaEvent_t fork = tail ? side->fork2 : side->fork;
+        join = tail ? side->join2 : side->join;
+        if (cudaEventRecord(fork, ctx->stream) != cudaSuccess ||
+            cudaStreamWaitEvent(side->stream, fork, 0) != cudaSuccess) {
             status = fail(ctx, SBX_ECUDA, "dense step: side-stream fork");
             side = nullptr;
             return;
@@ -116,15 +120,15 @@ struct SideScope {
     }
     ~SideScope() {
         if (!side) return;
-        cudaEventRecord(side->join, side->stream);
+        cudaEventRecord(join, side->stream);
         ctx->stream = savedStream;
         ctx->scratch = savedScratch;
         ctx->scratch_bytes = savedBytes;
     }
 };
 
-sbx_status side_join(sbx_ctx* ctx, const SideStream* side) {
-    if (cudaStreamWaitEvent(ctx->stream, side->join, 0) != cudaSuccess)
+sbx_status side_join(sbx_ctx* ctx, const SideStream* side, bool tail = false) {
+    if (cudaStreamWaitEvent(ctx->stream, tail ? side->join2 : side->join, 0) != cudaSuccess)
         return fail(ctx, SBX_ECUDA, "dense step: side-stream join");
     return SBX_OK;
 }
@@ -265,30 +269,37 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
     CHK(sbx_xbridge_bond_forces(ctx, nB, b.coord, b.uVec, b.yVec, b.bRotGam, nSeg, fb.coord, fb.uVec, fb.yVec,
                                 fb.bRotGam, fb.segLength, mot.boundSeg, mot.bindArc, mot.nucleotideState, sc->bondData,
                                 sc->xbParams));
-    CHK(sbx_xbridge_apply_head_force(ctx, nB, sc->bondData, b.forceSum, b.torqueSum));
-    if (bt) {
-        CHK(sbx_integrate(ctx, nB, b.coord, b.coord64, b.uVec, b.yVec, b.forceSum, b.torqueSum, b.randForce,
-                          b.randTorque, b.bTransGam, b.bRotGam, mot.bodyParams));
-        CHK(sbx_confine_batched(ctx, nBb, bb.coord, bb.uVec, bb.segLength, bb.bTransGam, bb.forceSum, bb.torqueSum,
-                                bt->boxParams, mini.bbCounts, bt->bbKey));
-        CHK(sbx_integrate(ctx, nBb, bb.coord, bb.coord64, bb.uVec, bb.yVec, bb.forceSum, bb.torqueSum, bb.randForce,
-                          bb.randTorque, bb.bTransGam, bb.bRotGam, mini.bbBodyParams));
-        CHK(sbx_derive(ctx, nB, b.coord, b.uVec, b.yVec, b.zVec, b.end1, b.end2, b.segLength));
-        CHK(sbx_derive(ctx, nBb, bb.coord, bb.uVec, bb.yVec, bb.zVec, bb.end1, bb.end2, bb.segLength));
-    } else {
-        // MechanicsFusion.integDerive / integDeriveConfined: confine, integrate and derive in one
-        // pass per store, in that order (the same values as the separate kernels)
-        CHK(sbx_fusion_integ_derive(ctx, nB, b.coord, b.coord64, b.uVec, b.yVec, b.zVec, b.segLength, b.end1,
-                                    b.end2, b.forceSum, b.torqueSum, b.randForce, b.randTorque, b.bTransGam,
-                                    b.bRotGam, mot.bodyParams));
-        CHK(sbx_fusion_integ_derive_confined(ctx, nBb, bb.coord, bb.coord64, bb.uVec, bb.yVec, bb.zVec, bb.segLength,
-                                             bb.end1, bb.end2, bb.forceSum, bb.torqueSum, bb.randForce,
-                                             bb.randTorque, bb.bTransGam, bb.bRotGam, sc->boxParams,
-                                             mini.bbCounts));
-    }
-    CHK(sbx_xbridge_register_force_dot(ctx, nM, sc->bondData, mot.boundSeg, mot.forceDotFil, mot.forceMag,
-                                       mot.forceDotHist, mot.forceDotPlace));
+    // the motor-side tail (head forces, motor and backbone integration, force-dot registry)
+    // reads no filament state and the filament tail below reads none of it: with a side stream
+    // they run concurrently, joined at the end of the step
     if (side) CHK(side_join(ctx, side));
+    {
+        SideScope onSide(ctx, side, true);
+        if (side) CHK(onSide.status);
+        CHK(sbx_xbridge_apply_head_force(ctx, nB, sc->bondData, b.forceSum, b.torqueSum));
+        if (bt) {
+            CHK(sbx_integrate(ctx, nB, b.coord, b.coord64, b.uVec, b.yVec, b.forceSum, b.torqueSum, b.randForce,
+                              b.randTorque, b.bTransGam, b.bRotGam, mot.bodyParams));
+            CHK(sbx_confine_batched(ctx, nBb, bb.coord, bb.uVec, bb.segLength, bb.bTransGam, bb.forceSum,
+                                    bb.torqueSum, bt->boxParams, mini.bbCounts, bt->bbKey));
+            CHK(sbx_integrate(ctx, nBb, bb.coord, bb.coord64, bb.uVec, bb.yVec, bb.forceSum, bb.torqueSum,
+                              bb.randForce, bb.randTorque, bb.bTransGam, bb.bRotGam, mini.bbBodyParams));
+            CHK(sbx_derive(ctx, nB, b.coord, b.uVec, b.yVec, b.zVec, b.end1, b.end2, b.segLength));
+            CHK(sbx_derive(ctx, nBb, bb.coord, bb.uVec, bb.yVec, bb.zVec, bb.end1, bb.end2, bb.segLength));
+        } else {
+            // MechanicsFusion.integDerive / integDeriveConfined: confine, integrate and derive in
+            // one pass per store, in that order (the same values as the separate kernels)
+            CHK(sbx_fusion_integ_derive(ctx, nB, b.coord, b.coord64, b.uVec, b.yVec, b.zVec, b.segLength, b.end1,
+                                        b.end2, b.forceSum, b.torqueSum, b.randForce, b.randTorque, b.bTransGam,
+                                        b.bRotGam, mot.bodyParams));
+            CHK(sbx_fusion_integ_derive_confined(ctx, nBb, bb.coord, bb.coord64, bb.uVec, bb.yVec, bb.zVec,
+                                                 bb.segLength, bb.end1, bb.end2, bb.forceSum, bb.torqueSum,
+                                                 bb.randForce, bb.randTorque, bb.bTransGam, bb.bRotGam,
+                                                 sc->boxParams, mini.bbCounts));
+        }
+        CHK(sbx_xbridge_register_force_dot(ctx, nM, sc->bondData, mot.boundSeg, mot.forceDotFil, mot.forceMag,
+                                           mot.forceDotHist, mot.forceDotPlace));
+    }
     CHK(sbx_csr_build_payload(ctx, mot.boundSeg, nM, nSeg, sc->segMotorCount, sc->segMotorOffsets, sc->segMotorMyo,
                               sc->bondData, XB_STRIDE, 6, nullptr, payM));
     CHK(sbx_fusion_chain_gathers(ctx, nSeg, fb.coord, fb.uVec, fb.segLength, f.end2NbrSlot, f.end2NbrSide,
@@ -306,6 +317,7 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
                                              fb.end1, fb.end2, fb.forceSum, fb.torqueSum, fb.randForce,
                                              fb.randTorque, fb.bTransGam, fb.bRotGam, sc->boxParams, f.counts));
     }
+    if (side) CHK(side_join(ctx, side, true));
     return SBX_OK;
 }
 
@@ -364,6 +376,8 @@ struct PlanScratch {
 void release_side(sbx_dense_plan* p) {
     if (p->side.scratch) cudaFree(p->side.scratch);
     if (p->side.join) cudaEventDestroy(p->side.join);
+    if (p->side.join2) cudaEventDestroy(p->side.join2);
+    if (p->side.fork2) cudaEventDestroy(p->side.fork2);
     if (p->side.fork) cudaEventDestroy(p->side.fork);
     if (p->side.stream) cudaStreamDestroy(p->side.stream);
     p->side = SideStream{};
@@ -537,6 +551,8 @@ static sbx_status plan_create(sbx_ctx* ctx, const sbx_dense_scene* sc, const sbx
     p->sideOk = cudaStreamCreateWithFlags(&p->side.stream, cudaStreamNonBlocking) == cudaSuccess &&
                 cudaEventCreateWithFlags(&p->side.fork, cudaEventDisableTiming) == cudaSuccess &&
                 cudaEventCreateWithFlags(&p->side.join, cudaEventDisableTiming) == cudaSuccess &&
+                cudaEventCreateWithFlags(&p->side.fork2, cudaEventDisableTiming) == cudaSuccess &&
+                cudaEventCreateWithFlags(&p->side.join2, cudaEventDisableTiming) == cudaSuccess &&
                 cudaMalloc(&p->side.scratch, p->side.scratchBytes) == cudaSuccess;
     if (!p->sideOk) {
         release_side(p);
