@@ -688,9 +688,10 @@ sbx_status sbx_dense_plan_create(sbx_ctx* ctx, const sbx_dense_scene* scene, sbx
  * cooperative launch; available when the scene has the harness layout, see
  * sbx_dense_plan_fused_available). All three give the same bits. mode 3 (auto): the fused
  * kernel up to SBX_DENSE_AUTO_MAX_FUSED_RODS rods when available, the graph path above it,
- * where the per-system kernels' occupancy beats the persistent kernel's (measured: fused
- * 0.20 ms vs graph 0.30 ms per step at 1e5 rods, 1.01 vs 0.57 ms at 5e5). */
-#define SBX_DENSE_AUTO_MAX_FUSED_RODS 262144
+ * where the per-system kernels' occupancy beats the persistent kernel's (measured, fused vs
+ * graph ms per step: 0.070 / 0.157 at 2e4 rods, 0.092 / 0.177 at 4e4, 0.298 / 0.181 at 5e4,
+ * 0.202 / 0.198 at 1e5, 1.01 / 0.44 at 5e5). */
+#define SBX_DENSE_AUTO_MAX_FUSED_RODS 40960
 sbx_status sbx_dense_plan_run(sbx_dense_plan* plan, int32_t t0, int32_t nsteps, int32_t mode);
 /* Runs one step as the unfused per-system call sequence (reference granularity). */
 sbx_status sbx_dense_step_unfused(sbx_ctx* ctx, const sbx_dense_scene* scene, int32_t t);
