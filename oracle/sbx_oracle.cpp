@@ -1975,9 +1975,16 @@ EXPORT double orc_m_log(double x) { return sbxm::log(x); }
 EXPORT double orc_m_exp(double x) { return sbxm::exp(x); }
 EXPORT double orc_m_sin(double x) { return sbxm::sin(x); }
 EXPORT double orc_m_cos(double x) { return sbxm::cos(x); }
+// which: 0 log, 1 exp, 2 sin, 3 cos, 4 / 5 the sine / cosine of sbxm::sincos
 EXPORT void orc_m_eval(int which, int n, const double* x, double* y) {
     PAR for (int i = 0; i < n; i++) {
         double v = x[i];
+        if (which >= 4) {
+            double sn, cs;
+            sbxm::sincos(v, &sn, &cs);
+            y[i] = which == 4 ? sn : cs;
+            continue;
+        }
         y[i] = which == 0 ? sbxm::log(v) : which == 1 ? sbxm::exp(v) : which == 2 ? sbxm::sin(v) : sbxm::cos(v);
     }
 }

@@ -51,3 +51,13 @@ def test_boxmuller_float_results_match_libm(orc):
         b = fn(x).astype(np.float32)
         diffs += int((a != b).sum())
     assert diffs <= 3
+
+
+def test_sincos_equals_sin_and_cos_bitwise(orc):
+    """sincos (one argument reduction for both results, as the Box-Muller draws and the
+    acos/asin Newton steps use it) gives the bits of sin and cos evaluated separately."""
+    rng = np.random.default_rng(4)
+    x = np.concatenate([rng.uniform(0, 2 * np.pi, 100000), rng.uniform(-8, 8, 50000),
+                        rng.uniform(-2.0 ** 20, 2.0 ** 20, 50000), [0.0, -0.0, np.pi / 4, -np.pi / 2]])
+    assert np.array_equal(_eval(orc, 4, x).view(np.uint64), _eval(orc, 2, x).view(np.uint64))
+    assert np.array_equal(_eval(orc, 5, x).view(np.uint64), _eval(orc, 3, x).view(np.uint64))
