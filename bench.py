@@ -289,7 +289,7 @@ def sweep_measure(n_points, steps, run_steps=50000):
     ens = MLPEnsemble(n_nets=5, seed=0)
     x = ensemble.features(ensemble.sample_points(100000, seed=2))
     ens.set_normalisation(x, np.zeros((1, 3)))
-    ens.predict(x[:1024])
+    ens.predict(x)                                  # warm-up: the inference buffers exist after it
     torch.cuda.synchronize()
     s, e = torch.cuda.Event(True), torch.cuda.Event(True)
     s.record()
