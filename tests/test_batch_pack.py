@@ -38,3 +38,27 @@ def test_pack_tables():
     s1 = int(info["seg"][1])
     e2 = packed["fil"]["end2NbrSlot"][s1:s1 + 10]
     assert (e2[e2 >= 0] >= s1).all()
+
+
+def test_sweep_batch_with_turnover_packs_per_network_tables():
+    """ensemble.build_batch(turnover=True): every point's network carries its own turnover
+    seed, severing rate (its point's turnover rate), actin pool and birth request range, and
+    each network unpacks to the arrays it was built with."""
+    from softbox_b200 import ensemble
+    pts = ensemble.sample_points(3, seed=4, rods_range=(2000, 3000))
+    packed, info = ensemble.build_batch(pts, turnover=True)
+    t = packed["turnover"]
+    assert info["nNet"] == 3 and t["tbSeeds"].size == 3 and len(set(t["tbSeeds"].tolist())) == 3
+    assert t["tbSlotBase"].tolist() == [int(v) for v in info["seg"]]
+    assert t["tbBirthBase"][0] == 0 and np.all(np.diff(t["tbBirthBase"]) > 0)
+    assert t["tbPools"].reshape(3, 4)[:, 0].min() > 0                     # initial [actin] per network
+    for k, p in enumerate(pts):
+        want = scenes.dense_turnover(ensemble.point_config(p), sever_rate=p.turnover,
+                                     turnover_seed=p.seed ^ 0x0F0501)
+        got = batch.unpack_network(packed, info, k)
+        assert np.array_equal(got["turnover"]["seedNode"], want["turnover"]["seedNode"])
+        assert np.array_equal(got["turnover"]["cofFrac"].view(np.uint32),
+                              want["turnover"]["cofFrac"].view(np.uint32))
+        assert np.array_equal(got["fil"]["body"]["coord"].view(np.uint32),
+                              want["fil"]["body"]["coord"].view(np.uint32))
+        assert np.float32(t["tb_cofilinParams"].reshape(3, 2)[k, 0]) == want["turnover"]["cofilinParams"][0]
