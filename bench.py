@@ -9,10 +9,14 @@ scene builder with these counts); no dataset.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+Both arms first advance the network WARM_STEPS steps untimed, to the state where binding
+has built up (about 700 bound heads; a fresh scene has about 120 in its first 25 steps),
+then take W untimed warm-up steps and time K steps.
 Our arm: each step is one launch of the fused persistent kernel; timed with CUDA events
 on the library's stream, one step at a time, with L2 flushed (a 256 MiB write) between
 timed steps. The reference arm times the reference's CPU path: the C++ restatement of
-the Java System classes (oracle/), on all host threads, on the same workload.
+the Java System classes (oracle/), on all host threads, on the same workload, for at
+least REF_MIN_STEPS timed steps.
 Multi-GPU: one process per GPU (torchrun), each advancing its own independent network
 (replicas; the single network does not shard), value = all ranks' rod-steps / max time.
 """
@@ -37,6 +41,26 @@ WORKLOAD = ("dense contractile network: 2000 filaments x 10 rods of 0.1 um (2000
 
 
 from softbox_b200.roofline import peaks, step_bytes  # noqa: E402
+
+WARM_STEPS = 3000      # untimed steps before the warm-up: bound heads have built up
+REF_MIN_STEPS = 200    # the reference arm times at least this many steps
+# DRAM bytes (read + write) of one launch of the fused kernel advancing one step of this
+# workload (FP64 centres, warmed state, L2 flushed before the launch), from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum, one kernel, one launch)
+FUSED_STEP_DRAM_BYTES = None
+
+
+def workload_config(sc_host, warmup):
+    """The `config` object of the bench line: identical in both arms."""
+    return {"workload": WORKLOAD, "rods": int(sc_host["fil"]["body"]["n"]), "heads": int(sc_host["mot"]["nMotors"]),
+            "crosslinks": int(sc_host["xl"]["nLinks"]), "warm_steps": WARM_STEPS + warmup,
+            "l2": "inputs (18 MB) below L2 size: L2 flushed between timed steps (256 MiB write) in the GPU arm"}
+
+
+def bound_state(sc_or_dev):
+    """Bound heads and active crosslinks of a host scene (numpy) or device scene (torch)."""
+    bs, ls = sc_or_dev["mot"]["boundSeg"], sc_or_dev["xl"]["linkState"]
+    return {"bound_heads": int((bs >= 0).sum()), "active_links": int((ls >= 0).sum())}
 
 
 def dist_env():
@@ -102,40 +126,60 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------- CPU arm
-def cpu_oracle_rate(sc_host, steps, threads):
-    """rod-steps/s of the oracle (C++ restatement of the reference's Java System classes)."""
+def _oracle(threads):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import copy
     import oracle
-    from softbox_b200 import device as D
     orc = oracle.get(devmath=False)
     orc.set_threads(threads)
-    sc = copy.deepcopy(sc_host)
+    return orc
+
+
+def cpu_oracle_rate(sc, t0, steps, threads, warmup=0):
+    """rod-steps/s of the oracle (C++ restatement of the reference's Java System classes)
+    advancing the host scene `sc` (FP64 centres attached) in place from step t0: `warmup`
+    untimed steps, then `steps` timed ones. Returns (rate, seconds, next step)."""
+    from softbox_b200 import device as D
+    orc = _oracle(threads)
+    desc = D.dense_desc(sc)
+    if warmup:
+        orc.dense_run(desc, t0, warmup)
+    t0 += warmup
+    s0 = time.perf_counter()
+    orc.dense_run(desc, t0, steps)
+    dt = time.perf_counter() - s0
+    return sc["fil"]["body"]["n"] * steps / dt, dt, t0 + steps
+
+
+def host_scene_fp64():
+    """The benchmark scene on the host with FP64 centres attached."""
+    from softbox_b200 import device as D, scenes
+    sc = scenes.dense_contractile(scenes.C1)
     for s_, b_ in (("fil", "body"), ("mot", "body"), ("mini", "backbone")):
         D.add_coord64(sc[s_][b_])
-    desc = D.dense_desc(sc)
-    orc.dense_run(desc, 0, 2)                      # warm
-    t0 = time.perf_counter()
-    orc.dense_run(desc, 2, steps)
-    dt = time.perf_counter() - t0
-    return sc["fil"]["body"]["n"] * steps / dt, dt
+    return sc
 
 
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    from softbox_b200 import scenes
-    sc = scenes.dense_contractile(scenes.C1)
+    from softbox_b200 import device as D
+    sc = host_scene_fp64()
     threads = os.cpu_count() or 1
-    rate, dt = cpu_oracle_rate(sc, max(1, args.warmup + args.steps), threads)
-    line = {"metric": METRIC, "value": rate, "unit": "rod-steps/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * sc["fil"]["body"]["n"] / rate, "higher_is_better": True,
+    steps = max(args.steps, REF_MIN_STEPS)
+    warmup = max(3, args.warmup)
+    _oracle(threads).dense_run(D.dense_desc(sc), 0, WARM_STEPS)      # to the warmed state, untimed
+    rate, dt, _ = cpu_oracle_rate(sc, WARM_STEPS, steps, threads, warmup=warmup)
+    line = {"metric": METRIC, "value": rate, "unit": "rod-steps/s", "n_gpus": args.gpus, "steps": steps,
+            "warmup": warmup, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 forces, f64 centres", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "parallelism": "host threads"}, "impl": "reference",
+            "config": workload_config(sc, warmup), "impl": "reference",
+            "arm": {"path": "C++ restatement of the Java System classes (oracle/, libm), OpenMP over slots",
+                    "parallelism": f"{threads} host threads", "state_at_end": bound_state(sc)},
             "cpu_baseline": {"value": rate, "unit": "rod-steps/s", "cores": threads, "kind": "port",
-                             "sample": f"{args.warmup + args.steps} full steps of the workload, "
-                                       f"{dt:.1f} s, C++ restatement of the Java System classes (no JVM on the box)"},
+                             "sample": f"{steps} full steps of the workload after {WARM_STEPS + warmup} untimed "
+                                       f"steps, {dt:.1f} s, C++ restatement of the Java System classes "
+                                       f"(no JVM on the box)"},
             "e2e": {"value": rate, "unit": "rod-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -166,7 +210,10 @@ def run_ours(args):
     def one_step(t):
         net.run(t, 1, mode="fused")
 
-    t = 0
+    # advance to the warmed state (one persistent launch), untimed
+    net.run(0, WARM_STEPS, mode="fused")
+    net.status()
+    t = WARM_STEPS
     with torch.cuda.stream(stream):
         for _ in range(max(3, args.warmup)):
             flush.zero_()
@@ -190,6 +237,7 @@ def run_ours(args):
                 t += 1
         torch.cuda.synchronize()
     net.status()
+    state = bound_state(net.dev)
     step_ms = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
     total_ms = float(step_ms.sum())
     if pg:
@@ -233,19 +281,20 @@ def run_ours(args):
     hbm, how = peaks()
     bytes_step = step_bytes(sc_host, fp64=True)
     achieved = bytes_step / (float(np.mean(step_ms)) / 1e3) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "fused_step_traffic.json")
-    if os.path.exists(tp):
-        try:
-            traffic = json.load(open(tp)).get("dram_bytes_per_launch")
-        except Exception:
-            traffic = None
+    traffic = FUSED_STEP_DRAM_BYTES
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        rate, dt = cpu_oracle_rate(sc_host, args.cpu_steps, 1)
+        # the same warmed state: the device arrays (bit-identical to the oracle's run)
+        import copy
+        sc_cpu = copy.deepcopy(sc_host)
+        got = net.pull_all()
+        for k in sc_cpu:
+            if k in got:
+                sc_cpu[k] = got[k]
+        rate, dt, _ = cpu_oracle_rate(sc_cpu, t, args.cpu_steps, 1)
         cpu = {"value": rate, "unit": "rod-steps/s", "cores": 1, "kind": "port",
-               "sample": f"{args.cpu_steps} full steps of the workload on 1 host core ({dt:.1f} s), C++ "
+               "sample": f"{args.cpu_steps} full steps of the warmed workload on 1 host core ({dt:.1f} s), C++ "
                          f"restatement of the Java System classes' single-threaded -cpu runner"}
     clocks = clk.summary()
     sweep = None
@@ -255,11 +304,9 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": "rod-steps/s", "n_gpus": ws, "steps": args.steps,
                 "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32 forces, f64 centres", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "rods": nrods, "heads": sc_host["mot"]["nMotors"],
-                           "crosslinks": sc_host["xl"]["nLinks"], "parallelism": f"replicas x{ws}",
-                           "l2": "flushed between timed steps (256 MiB write)",
-                           "path": "fused persistent cooperative kernel, 1 launch per step",
-                           "grid_ctas": net.fused_grid},
+                "config": workload_config(sc_host, max(3, args.warmup)),
+                "arm": {"path": "fused persistent cooperative kernel, 1 launch per step",
+                        "parallelism": f"replicas x{ws}", "grid_ctas": net.fused_grid, "state_at_timing": state},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                              "frac": achieved / hbm, "traffic": traffic, "peak_source": how,
                              "kernel": "k_dense_fused", "algorithmic_bytes_per_launch": bytes_step},
@@ -280,7 +327,7 @@ def sweep_measure(n_points, steps, run_steps=50000):
     advanced `steps` steps (CUDA events), extrapolated to sweep runs of `run_steps` steps,
     and the surrogate ensemble's inference rate (5 x 6-256x4-3 MLPs, tensor-core GEMMs) on
     100,000 points. The surrogate's error and fallback fraction come from the full pipeline
-    (python -m softbox_b200.sweep_surrogate; profiles/surrogate_sweep.md)."""
+    (python -m softbox_b200.sweep_surrogate)."""
     import torch
     from softbox_b200 import ensemble
     from softbox_b200.surrogate import MLPEnsemble
@@ -301,7 +348,7 @@ def sweep_measure(n_points, steps, run_steps=50000):
             "ms_per_packed_step": r["ms_per_step"], "rod_steps_per_s": r["rods"] / (r["ms_per_step"] / 1e3),
             "batched_points_per_s_at_run_steps": n_points / (r["ms_per_step"] / 1e3 * run_steps),
             "run_steps": run_steps, "surrogate_inference_points_per_s": 100000 / infer_s,
-            "surrogate_error_source": "profiles/surrogate_sweep.md"}
+            "surrogate_error_source": "python -m softbox_b200.sweep_surrogate (not measured in this run)"}
 
 
 def main():

@@ -5,8 +5,8 @@
  * method of the reference's System classes (package softbox/, notaboxllc/SoftBox). The
  * Java side keeps its signatures and its planar SoA store layouts
  * ([x0..xN-1 | y0..yN-1 | z0..zN-1], FilamentStore.java:10-22) and calls these
- * functions through the Foreign Function & Memory API; INTEGRATION.md shows the
- * binding. Conventions:
+ * functions through the Foreign Function & Memory API (a MethodHandle downcall per entry
+ * point, with MemorySegment addresses for the device pointers). Conventions:
  *   - every array argument is a DEVICE pointer owned by the caller (the store);
  *     entry points allocate nothing except where a comment says "scratch";
  *   - an argument `n`, `cap`, ... carries the length the Java code reads with
@@ -39,7 +39,7 @@ typedef int32_t sbx_status;
 #define SBX_ENONFINITE -6   /* a supplied-noise / state array holds NaN or Inf */
 #define SBX_ESTATE     -7   /* call out of order (e.g. plan not built) */
 
-/* reference constants (SpatialGrid.java:113-115, CrossBridgeSystem.java:36, ...) */
+/* reference constants (SpatialGrid.java:46-48, CrossBridgeSystem.java:36, ...) */
 #define SBX_MAX_CAND        256
 #define SBX_GRID_SCAN_CHUNK 512
 #define SBX_XB_STRIDE        13
@@ -60,9 +60,14 @@ sbx_status sbx_ctx_destroy(sbx_ctx* ctx);
 const char* sbx_ctx_last_error(sbx_ctx* ctx);
 sbx_status sbx_ctx_set_stream(sbx_ctx* ctx, void* stream);
 void* sbx_ctx_stream(sbx_ctx* ctx);
+/* Waits for the context's stream. Also reports (SBX_EINVAL, then cleared) an input that a
+ * kernel since the last sync found outside its documented range and skipped: a CSR key at
+ * or past its row count (sbx_csr_build*, sbx_grid_build). */
 sbx_status sbx_ctx_sync(sbx_ctx* ctx);
 /* number of kernels this context has launched (for launch accounting) */
 int64_t sbx_ctx_launch_count(sbx_ctx* ctx);
+/* bytes of device scratch the context holds (grows on demand, never shrinks; -1 for NULL) */
+int64_t sbx_ctx_scratch_bytes(sbx_ctx* ctx);
 
 /* DataTransferMode analogues: FIRST_EXECUTION / EVERY_EXECUTION uploads and
  * UNDER_DEMAND pulls are plain async copies on the context stream. */
@@ -82,13 +87,13 @@ sbx_status sbx_drag_run_filament(sbx_ctx* ctx, int32_t n, const int32_t* monomer
 /* DragTensorSystem.run(MotorStore) (DragTensorSystem.java:105-122) */
 sbx_status sbx_drag_run_motor(sbx_ctx* ctx, int32_t nMotors, double aeta, float* segLength,
                               float* bTransGam, float* bRotGam, float* bTransDiff, float* bRotDiff);
-/* MiniFilamentStore.initBackboneDrag (MiniFilamentStore.java:294-307); backbone length is a parameter */
+/* MiniFilamentStore.initBackboneDrag (MiniFilamentStore.java:121-134); backbone length is a parameter */
 sbx_status sbx_drag_run_backbone(sbx_ctx* ctx, int32_t nBb, double bbLenUm, double aeta, float* segLength,
                                  float* bTransGam, float* bRotGam, float* bTransDiff, float* bRotDiff,
                                  float* bbInvDragY);
 
 /* ---------------------------------------------------------------- Brownian forcing
- * BrownianForceSystem.brownianForce (BrownianForceSystem.java:183-245): Wang-hash keyed
+ * BrownianForceSystem.brownianForce (BrownianForceSystem.java:44-106): Wang-hash keyed
  * (slot, counts[1]=step, counts[2]=seed), three Box-Muller pairs. params[1]=sqrt(2kT/dt). */
 sbx_status sbx_brownian_force(sbx_ctx* ctx, int32_t n, float* randForce, float* randTorque,
                               const float* bTransGam, const float* bRotGam, const float* brownTransScale,
@@ -109,17 +114,17 @@ sbx_status sbx_brownian_force_supplied(sbx_ctx* ctx, int32_t n, float* randForce
 sbx_status sbx_zero_accumulators(sbx_ctx* ctx, int32_t n, float* forceSum, float* torqueSum);
 
 /* ---------------------------------------------------------------- integration
- * RigidRodLangevinIntegrationSystem.integrate (RigidRodLangevinIntegrationSystem.java:279-358).
+ * RigidRodLangevinIntegrationSystem.integrate (RigidRodLangevinIntegrationSystem.java:33-112).
  * coord64 may be NULL; when given, centres accumulate in FP64 and coord receives the
  * rounded projection (the per-step increment is the reference's FP32 dt*v). */
 sbx_status sbx_integrate(sbx_ctx* ctx, int32_t n, float* coord, double* coord64, float* uVec, float* yVec,
                          const float* forceSum, const float* torqueSum, const float* randForce,
                          const float* randTorque, const float* bTransGam, const float* bRotGam,
                          const float* params);
-/* DerivedGeometrySystem.derive (DerivedGeometrySystem.java:386-432) */
+/* DerivedGeometrySystem.derive (DerivedGeometrySystem.java:27-73) */
 sbx_status sbx_derive(sbx_ctx* ctx, int32_t n, const float* coord, const float* uVec, float* yVec,
                       float* zVec, float* end1, float* end2, const float* segLength);
-/* ContainmentSystem.confine (ContainmentSystem.java:390-458); boxParams[0..6] */
+/* ContainmentSystem.confine (ContainmentSystem.java:58-126); boxParams[0..6] */
 sbx_status sbx_confine(sbx_ctx* ctx, int32_t n, const float* coord, const float* uVec,
                        const float* segLength, const float* bTransGam, float* forceSum, float* torqueSum,
                        const float* boxParams, const int32_t* counts);
@@ -176,11 +181,11 @@ sbx_status sbx_motor_publish(sbx_ctx* ctx, int32_t nMotors, const float* head, c
                              int32_t* ownerSlot, const int32_t* publishParams);
 
 /* ---------------------------------------------------------------- spatial grid
- * SpatialGrid.bodyCell (SpatialGrid.java:118-142); counts[1] = S */
+ * SpatialGrid.bodyCell (SpatialGrid.java:51-75); counts[1] = S */
 sbx_status sbx_grid_body_cell(sbx_ctx* ctx, int32_t cap, const float* center, const float* gridParams,
                               const int32_t* gridDims, const int32_t* counts, int32_t* bodyCell);
 /* The counting sort that replaces gridZero+gridHistogram+gridScanLocal/Chunks/Add+gridScatter
- * (SpatialGrid.java:145-249) and the chunked gridChunk* variant (SpatialGrid.java:304-398):
+ * (SpatialGrid.java:78-182) and the chunked gridChunk* variant (SpatialGrid.java:237-331):
  * atomic cell histogram, block scan over GRID_SCAN_CHUNK tiles (chunkSum holds the tile
  * sums, as in the reference), scatter, then an in-cell ascending sort so that the
  * within-cell order is body-index order. Outputs equal the serial reference bit for bit:
@@ -191,13 +196,13 @@ sbx_status sbx_grid_body_cell(sbx_ctx* ctx, int32_t cap, const float* center, co
 sbx_status sbx_grid_build(sbx_ctx* ctx, int32_t cap, const int32_t* bodyCell, const int32_t* counts,
                           int32_t totalCells, int32_t* cellCount, int32_t* chunkSum,
                           int32_t* gridCellOffsets, int32_t* gridCellContents, int32_t contentsCap);
-/* SpatialGrid.broadPhase (SpatialGrid.java:407-473); candPartner is cap*SBX_MAX_CAND */
+/* SpatialGrid.broadPhase (SpatialGrid.java:340-406); candPartner is cap*SBX_MAX_CAND */
 sbx_status sbx_grid_broad_phase(sbx_ctx* ctx, int32_t cap, const float* center, const float* boundingRadius,
                                 const int32_t* bodyCell, const int32_t* gridCellOffsets,
                                 const int32_t* gridCellContents, const int32_t* gridDims,
                                 const float* gridParams, const int32_t* counts, int32_t* candPartner,
                                 int32_t* candCount);
-/* SpatialGrid.bruteForce (SpatialGrid.java:480-512) */
+/* SpatialGrid.bruteForce (SpatialGrid.java:413-445) */
 sbx_status sbx_grid_brute_force(sbx_ctx* ctx, int32_t cap, const float* center, const float* boundingRadius,
                                 const float* gridParams, const int32_t* counts, int32_t* brutePartner,
                                 int32_t* bruteCount);
@@ -259,7 +264,10 @@ sbx_status sbx_xbridge_register_force_dot(sbx_ctx* ctx, int32_t nM, const float*
 /* The CSR-inverse that replaces csrHistogram/csrScan/csrScatter and csrChunk*
  * (CrossBridgeSystem.java:190-298): rows = key values, items in ascending index per row.
  * Outputs equal the serial reference: rowOffsets[0..nRows], rowList, rowCount (= row
- * lengths, as the serial csrScatter leaves it). Uses context scratch for the scan. */
+ * lengths, as the serial csrScatter leaves it). Uses context scratch for the scan.
+ * Keys: -1 (or any negative value) = unbound item, skipped as in the reference; 0..nRows-1
+ * = its row. A key >= nRows (where the reference's Java would throw) is skipped too and
+ * reported by the next sbx_ctx_sync as SBX_EINVAL; the outputs then hold the valid items. */
 sbx_status sbx_csr_build(sbx_ctx* ctx, const int32_t* keys, int32_t nItems, int32_t nRows,
                          int32_t* rowCount, int32_t* rowOffsets, int32_t* rowList);
 /* No counterpart in the reference. Same outputs as sbx_csr_build, but it allocates no
@@ -270,9 +278,11 @@ sbx_status sbx_csr_build(sbx_ctx* ctx, const int32_t* keys, int32_t nItems, int3
  * Nothing needs to start at zero. The scratch is shared by every context on a device:
  * calls that overlap in time on one device (different streams) race; calls on one stream
  * are safe. The first call on each device sets the scratch up; make it before any stream
- * capture begins. */
+ * capture begins. Keys as for sbx_csr_build. */
 #define SBX_CSR_NOALLOC_MAX_ITEMS (1 << 20)
 #define SBX_CSR_NOALLOC_MAX_ROWS (1 << 22)
+sbx_status sbx_csr_build_noalloc(sbx_ctx* ctx, const int32_t* keys, int32_t nItems, int32_t nRows,
+                                 int32_t* rowCount, int32_t* rowOffsets, int32_t* rowList);
 /* sbx_csr_build that also copies each item's 6-float payload (payload[item * payloadStride +
  * payloadOffset + 0..5]; zeros where guard != NULL and guard[item] < 0) into rowPayload in
  * list order: row r's items are rowPayload[6 k .. 6 k + 5] for k in [rowOffsets[r],
@@ -281,8 +291,6 @@ sbx_status sbx_csr_build_payload(sbx_ctx* ctx, const int32_t* keys, int32_t nIte
                                  int32_t* rowCount, int32_t* rowOffsets, int32_t* rowList,
                                  const float* payload, int32_t payloadStride, int32_t payloadOffset,
                                  const int32_t* guard, float* rowPayload);
-sbx_status sbx_csr_build_noalloc(sbx_ctx* ctx, const int32_t* keys, int32_t nItems, int32_t nRows,
-                                 int32_t* rowCount, int32_t* rowOffsets, int32_t* rowList);
 /* CrossBridgeSystem.segGather (CrossBridgeSystem.java:302-320) */
 sbx_status sbx_xbridge_seg_gather(sbx_ctx* ctx, int32_t nSeg, const int32_t* segMotorOffsets,
                                   const int32_t* segMotorMyo, const float* bondData, float* filForceSum,
@@ -319,7 +327,7 @@ sbx_status sbx_xlink_unbind(sbx_ctx* ctx, int32_t nSeg, const float* filUVec, co
                             int32_t* strainPlace, const float* offParams, const int32_t* counts);
 
 /* ---------------------------------------------------------------- crosslinker formation + allocator
- * CrosslinkerSystem formation (CrosslinkerSystem.java:417-752) and the scan-rank free-list
+ * CrosslinkerSystem formation (CrosslinkerSystem.java:405-756) and the scan-rank free-list
  * allocator (:297-345). formParams: [0] maxXLinkBondAngle (rad) [1] crossLinkGrabDist^2
  * [2] minSepBetweenXLinks [3] maxXLinksOnSeg [4] P_form [5] loc jitter half-range
  * [6] crossLinkGrabDist; formCounts: [0] nCand (written) [1] step [2] seed [3] xLinkMode
@@ -468,7 +476,7 @@ sbx_status sbx_actin_pool_put_total(sbx_ctx* ctx, sbx_actin_pool* pool, const in
 sbx_status sbx_actin_pool_take_total(sbx_ctx* ctx, sbx_actin_pool* pool, const int32_t* offsets, int32_t n);
 /* The per-step prologue of the turnover block (FullSystemDemoHarness.java:648-651) on the
  * device: GrowthStore/DepolyStore.setCounts (step, seed, fires), AgingStore/SeverStore
- * .setFires, and GrowthStore.refreshRate (GrowthStore.java:84-88): growParams[0] =
+ * .setFires, and GrowthStore.refreshRate (GrowthStore.java:81-91): growParams[0] =
  * (float)(onRate * conc * biochemDeltaT), 0 when fires == 0. NULL arrays are skipped. */
 sbx_status sbx_turnover_begin(sbx_ctx* ctx, int32_t step, int32_t seed, int32_t fires, double onRate,
                               double biochemDeltaT, const sbx_actin_pool* pool, float* growParams,
@@ -622,13 +630,13 @@ typedef struct sbx_motor_store {          /* MotorStore.java:32-161 */
     int32_t *publishParams;               /* [0]=base body-view slot */
 } sbx_motor_store;
 
-typedef struct sbx_dimer_store {          /* DimerStore.java:211-252 */
+typedef struct sbx_dimer_store {          /* DimerStore.java:26-67 */
     int32_t nDimers;
     int32_t *motorA, *motorB, *parallel;
     float *dimerParams;
 } sbx_dimer_store;
 
-typedef struct sbx_minifilament_store {   /* MiniFilamentStore.java:201-308 */
+typedef struct sbx_minifilament_store {   /* MiniFilamentStore.java:28-135 */
     sbx_rigid_body backbone;
     int32_t nBackbones, nDimers;
     float *bbBodyParams;
@@ -646,7 +654,7 @@ typedef struct sbx_crosslinker_store {    /* CrosslinkerStore.java:31-179 */
     int32_t *strainPlace, *torqueMagPlace;
     float *xlParams, *offParams, *torsionParams;
     int32_t *counts;                      /* [0]=nLinks [1]=step [2]=seed [3]=nSeg */
-    /* two-pass gather CSRs (DenseContractileHarness.java:82-83) */
+    /* two-pass gather CSRs (DenseContractileHarness.java:101-102) */
     int32_t *segCountA, *segOffsetsA, *segIdxA, *segCountB, *segOffsetsB, *segIdxB;
 } sbx_crosslinker_store;
 
@@ -716,6 +724,40 @@ sbx_status sbx_dense_plan_phase_times(sbx_dense_plan* plan, int64_t* dev_times);
  * arrivals that never come, so its bounded wait runs out and the run reports
  * SBX_ETIMEOUT. 0 restores normal operation. */
 sbx_status sbx_dense_plan_test_barrier_extra(sbx_dense_plan* plan, int32_t extra);
+/* Supplied-noise mode of the dense step: both the library and a CPU implementation of the
+ * step consume the same Gaussian array. Each step t in [t0, t0 + nsteps) takes its six
+ * Gaussians per body from planar device arrays fil[t - t0][6][nRods],
+ * mot[t - t0][6][3 nMotors] and bb[t - t0][6][nBackbones] (gfx gfy gfz gtx gty gtz, the
+ * order of the Box-Muller outputs of BrownianForceSystem.brownianForce,
+ * BrownianForceSystem.java:78-92) instead of the Wang-hash draws; the amplitudes, the rest
+ * of the step and every other RNG stream (release, nucleotide cycle, Bell unbind) are
+ * unchanged. NULL switches the mode off. The arrays must stay alive while the mode is on;
+ * they are checked for NaN/Inf here (SBX_ENONFINITE, mode left unchanged). A run whose steps
+ * leave [t0, t0 + nsteps) returns SBX_EINVAL. Not available for packed plans. All paths
+ * (per-system, graph, fused) honour it and give the same bits. */
+typedef struct sbx_dense_noise {
+    const float *fil, *mot, *bb;
+    int32_t t0, nsteps;
+} sbx_dense_noise;
+sbx_status sbx_dense_plan_set_noise(sbx_dense_plan* plan, const sbx_dense_noise* noise);
+/* Counters of the fused kernel's capacity fallbacks since the plan was created (or since
+ * the last call with reset != 0), for tests that must show the fallback paths ran:
+ * out[0] grid cells with more than the fixed row slots (overflow list walked),
+ * out[1] segments with more link ends than the fixed slots, out[2] segments with more bound
+ * motors than the fixed slots, out[3] link payload entries read from global memory past
+ * the rod CTA's staging capacity, out[4] motor reactions read from global memory past the
+ * staged ones, out[5] motor rows longer than the sorted-slot capacity (repeated-minimum
+ * walk), out[6] reach lists longer than SBX_MAX_CAND, out[7] reserved; `out` holds
+ * SBX_FUSED_STATS values. */
+#define SBX_FUSED_STATS 8
+sbx_status sbx_dense_plan_fused_stats(sbx_dense_plan* plan, int64_t* out, int32_t reset);
+/* Test hook: lowers the fused kernel's capacities (link payload entries a rod CTA stages,
+ * motor reactions staged per segment, motor slots sorted per segment, fixed row slots per
+ * segment row, fixed slots per grid cell) to exercise the fallback paths on ordinary
+ * scenes; each value is clamped to [0, the compiled capacity], a negative value restores
+ * the compiled capacity. Takes effect at the next run; the results are the same bits. */
+sbx_status sbx_dense_plan_test_caps(sbx_dense_plan* plan, int32_t entCap, int32_t motorCap, int32_t motorIds,
+                                    int32_t rowSlots, int32_t cellSlots);
 /* Waits for the device and frees the plan; safe after the plan's context was destroyed. */
 sbx_status sbx_dense_plan_destroy(sbx_dense_plan* plan);
 

@@ -43,7 +43,7 @@ _SIGS = {
     "orc_compute_fil_link_ct": "ipppip", "orc_joints": "ippppppppp", "orc_dimer_couple": "ipppppppippppp",
     "orc_mini_tether": "ipppppppipppippppp", "orc_backbone_gather": "ippppp",
     "orc_mini_brute_gather": "iipppp", "orc_torsional_restore": "ipppdd", "orc_dense_step": "si",
-    "orc_dense_run": "sii", "orc_fdt_run": "sii", "orc_chain_run": "sii",
+    "orc_dense_run": "sii", "orc_dense_run_supplied": "siippp", "orc_fdt_run": "sii", "orc_chain_run": "sii",
     "orc_m_log": "d", "orc_m_exp": "d", "orc_m_sin": "d", "orc_m_cos": "d", "orc_m_eval": "iipp",
     "orc_xl_fil_fil_candidates": "ipppipppp", "orc_xl_grid_form_count": "ippppppppp",
     "orc_xl_grid_form_scan": "ippippp", "orc_xl_grid_form_emit": "ipppppppppippp",

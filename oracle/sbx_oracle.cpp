@@ -56,20 +56,20 @@ const double ACTIN_RADIUS = 0.007 / 2.0;
 const int STD_SEG_LENGTH = 32;
 const double A_PARALLEL = -0.20, A_ORTHOG = 0.84, A_TURNING = -0.662;
 
-// MotorStore.java:45-46, MiniFilamentStore.java:207
+// MotorStore.java:45-46, MiniFilamentStore.java:34
 const double ROD_LEN = 0.080, LEVER_LEN = 0.008, HEAD_LEN = 0.020;
 const double ROD_R = 0.003, LEVER_R = 0.002, HEAD_R = 0.010;
 const double BACKBONE_R = 0.005;
 
 const int STORE_FILAMENT = 0, STORE_MOTOR = 1, STORE_NONE = -1;
-const int MAX_CAND = 256;          // SpatialGrid.java:115
-const int GRID_SCAN_CHUNK = 512;   // SpatialGrid.java:113
+const int MAX_CAND = 256;          // SpatialGrid.java:48
+const int GRID_SCAN_CHUNK = 512;   // SpatialGrid.java:46
 const int NUC_NONE = 0, NUC_ATP = 1, NUC_ADPPI = 2, NUC_ADP = 3;   // MotorStore.java:117
 const int FREE_BINDABLE = -1, FREE_COOLDOWN = -2;                   // MotorStore.java:111-112
 const int XB_STRIDE = 13;          // CrossBridgeSystem.java:36
 const int XL_STRIDE = 12;          // CrosslinkerStore.java:33
 const int STRAIN_WIN = 10, TORQUE_WIN = 5;   // CrosslinkerStore.java:64,118
-const int MINI_STRIDE = 6;         // MiniFilamentStore.java:224
+const int MINI_STRIDE = 6;         // MiniFilamentStore.java:51
 const int LINK_FREE = -1, LINK_ACTIVE = 0;   // CrosslinkerStore.java:58-59
 
 // Java (int) cast of a float / double
@@ -166,7 +166,7 @@ double wall_push(double d, double halfDim) {
     return push;
 }
 
-// Box-Muller from six uniforms: BrownianForceSystem.java:86-104
+// Box-Muller from six uniforms: BrownianForceSystem.java:78-92
 inline void box_muller6(float u1, float u2, float u3, float u4, float u5, float u6, float g[6]) {
     const float TWO_PI_F = 2.0f * 3.14159265f;
     float r1 = jsqrtf(-2.0f * (float)JLOG((double)u1));
@@ -183,7 +183,7 @@ inline void box_muller6(float u1, float u2, float u3, float u4, float u5, float 
     g[5] = r3 * (float)JSIN((double)th3);
 }
 
-// Wang-hash keyed draws of BrownianForceSystem.java:74-86 -> g = {gfx,gfy,gfz,gtx,gty,gtz}
+// Wang-hash keyed draws of BrownianForceSystem.java:63-92 -> g = {gfx,gfy,gfz,gtx,gty,gtz}
 inline void gauss6_wang(i32 i, i32 step, i32 seed, float g[6]) {
     uint32_t base = sbxm::rng_base(i, step, seed);
     uint32_t h1 = sbxm::wang_hash(base);
@@ -242,7 +242,7 @@ EXPORT double orc_angle_from_sin_cos(double s2, double c) { return angle_from_si
 EXPORT double orc_kT() { return KT; }
 
 // ============================================================================
-// DragTensorSystem.java:33-122, MiniFilamentStore.java:294-307
+// DragTensorSystem.java:33-122, MiniFilamentStore.java:121-134
 // ============================================================================
 EXPORT void orc_rod_drag_si(double lengthUm, double radiusUm, double aeta, double* g) {
     double LM = 1.0e-6 * lengthUm;
@@ -322,7 +322,7 @@ EXPORT void orc_backbone_drag(int nBb, double bbLen, double aeta, float* segLeng
 }
 
 // ============================================================================
-// BrownianForceSystem.java:183-245 (wang), plus the Philox and supplied-noise modes
+// BrownianForceSystem.java:44-106 (wang), plus the Philox and supplied-noise modes
 // ============================================================================
 static inline void brownian_store(int N, int i, const float g[6], float* rF, float* rT,
                                   const float* bTG, const float* bRG, const float* tSc,
@@ -396,7 +396,7 @@ EXPORT void orc_zero_accumulators(int N, float* F, float* T) {
 }
 
 // ============================================================================
-// RigidRodLangevinIntegrationSystem.java:279-358 and DerivedGeometrySystem.java:386-432
+// RigidRodLangevinIntegrationSystem.java:33-112 and DerivedGeometrySystem.java:27-73
 // coord64 (optional, may be null): FP64 accumulation of the centre; the FP32 coord
 // is then the rounded projection. The per-step increment dt*v is the reference's.
 // ============================================================================
@@ -493,7 +493,7 @@ EXPORT void orc_derive(int N, const float* coord, const float* uVec, float* yVec
 }
 
 // ============================================================================
-// ContainmentSystem.java:390-458
+// ContainmentSystem.java:58-126
 // boxParams: [0]=tau [1..3]=box dims [4]=R inset [5]=coeff [6]=checkInt
 // ============================================================================
 static inline void confine_one(int N, int i, const float* coord, const float* uVec, const float* segLength,
@@ -808,7 +808,7 @@ EXPORT void orc_mot_publish(int nM, const float* head, const float* reach, int c
 }
 
 // ============================================================================
-// SpatialGrid.java:118-445
+// SpatialGrid.java:51-445
 // gridParams: [0..2]=min [3]=cell [4]=invCell [5]=cutoff; gridDims: [0..2]=nX,nY,nZ [3]=cells
 // ============================================================================
 EXPORT void orc_body_cell(int cap, const float* center, const float* gridParams, const i32* gridDims,
@@ -1990,7 +1990,7 @@ EXPORT void orc_m_eval(int which, int n, const double* x, double* y) {
 }
 
 // ============================================================================
-// Crosslinker formation (CrosslinkerSystem.java:417-752) and the scan-rank free-list
+// Crosslinker formation (CrosslinkerSystem.java:405-756) and the scan-rank free-list
 // allocator (CrosslinkerSystem.java:297-345); FormationGrid.java:28-109 builds its grid
 // with the SpatialGrid functions above.
 // formParams: [0] maxXLinkBondAngle (rad) [1] crossLinkGrabDist^2 [2] minSepBetweenXLinks
@@ -1998,9 +1998,9 @@ EXPORT void orc_m_eval(int which, int n, const double* x, double* y) {
 // formCounts: [0] nCand [1] step [2] seed [3] xLinkMode (0 both, 1 parallel, -1 antiparallel)
 // ============================================================================
 namespace {
-const int FORM_MAXC = 256;   // CrosslinkerSystem.java:472
+const int FORM_MAXC = 256;   // CrosslinkerSystem.java:457
 
-// the coarse capsule bound of filFilCandidates / gridFormCount (CrosslinkerSystem.java:444-448)
+// the coarse capsule bound of filFilCandidates / gridFormCount (CrosslinkerSystem.java:414-420)
 inline bool form_pair_ok(i32 nSeg, const float* coord, const float* segLength, const i32* filID, int i, int j,
                          double cix, double ciy, double ciz, double hi, double grab) {
     if (filID[j] == filID[i]) return false;
@@ -2024,7 +2024,7 @@ inline void form_cell_range(double cix, double ciy, double ciz, const float* gp,
 }
 }  // namespace
 
-// CrosslinkerSystem.filFilCandidates (CrosslinkerSystem.java:431-452): all distinct
+// CrosslinkerSystem.filFilCandidates (CrosslinkerSystem.java:405-427): all distinct
 // cross-filament pairs i<j within the coarse bound, lexicographic, capped at reqCap
 EXPORT void orc_xl_fil_fil_candidates(i32 nSeg, const float* coord, const float* segLength, const i32* filID,
                                       i32 reqCap, i32* reqFilA, i32* reqFilB, const float* formParams,
@@ -2043,7 +2043,7 @@ EXPORT void orc_xl_fil_fil_candidates(i32 nSeg, const float* coord, const float*
     for (int k = c; k < reqCap; k++) { reqFilA[k] = -1; reqFilB[k] = -1; }
 }
 
-// CrosslinkerSystem.gridFormCount (CrosslinkerSystem.java:474-516)
+// CrosslinkerSystem.gridFormCount (CrosslinkerSystem.java:461-512)
 EXPORT void orc_xl_grid_form_count(i32 nSeg, const float* coord, const float* segLength, const i32* filID,
                                    const float* gridParams, const i32* gridDims, const i32* offsets,
                                    const i32* contents, i32* candCountSeg, const float* formParams) {
@@ -2071,7 +2071,7 @@ EXPORT void orc_xl_grid_form_count(i32 nSeg, const float* coord, const float* se
     }
 }
 
-// CrosslinkerSystem.gridFormScan (CrosslinkerSystem.java:520-532)
+// CrosslinkerSystem.gridFormScan (CrosslinkerSystem.java:516-528)
 EXPORT void orc_xl_grid_form_scan(i32 nSeg, const i32* candCountSeg, i32* candBaseSeg, i32 reqCap, i32* reqFilA,
                                   i32* reqFilB, i32* formCounts) {
     int acc = 0;
@@ -2082,7 +2082,7 @@ EXPORT void orc_xl_grid_form_scan(i32 nSeg, const i32* candCountSeg, i32* candBa
     for (int k = total; k < reqCap; k++) { reqFilA[k] = -1; reqFilB[k] = -1; }
 }
 
-// CrosslinkerSystem.gridFormEmit (CrosslinkerSystem.java:538-595): partners ascending in
+// CrosslinkerSystem.gridFormEmit (CrosslinkerSystem.java:535-602): partners ascending in
 // each segment's owned region; a full region keeps the smallest FORM_MAXC
 EXPORT void orc_xl_grid_form_emit(i32 nSeg, const float* coord, const float* segLength, const i32* filID,
                                   const float* gridParams, const i32* gridDims, const i32* offsets,
@@ -2125,7 +2125,7 @@ EXPORT void orc_xl_grid_form_emit(i32 nSeg, const float* coord, const float* seg
     }
 }
 
-// CrosslinkerSystem.formGates (CrosslinkerSystem.java:600-665)
+// CrosslinkerSystem.formGates (CrosslinkerSystem.java:607-675)
 EXPORT void orc_xl_form_gates(i32 nSeg, const float* fU, const float* fE1, const float* fE2, const float* segLength,
                               i32 reqCap, const i32* reqFilA, const i32* reqFilB, float* reqLoc1, float* reqLoc2,
                               i32* reqOrient, i32* gatePass, const float* formParams, const i32* formCounts) {
@@ -2186,7 +2186,7 @@ EXPORT void orc_xl_form_gates(i32 nSeg, const float* fU, const float* fE1, const
     }
 }
 
-// CrosslinkerSystem.formAdmitReduce (CrosslinkerSystem.java:670-682)
+// CrosslinkerSystem.formAdmitReduce (CrosslinkerSystem.java:680-691)
 EXPORT void orc_xl_form_admit_reduce(i32 reqCap, const i32* reqFilA, const i32* reqFilB, const i32* gatePass,
                                      i32 nSeg, i32* minCand) {
     for (int s = 0; s < nSeg; s++) minCand[s] = reqCap;
@@ -2198,7 +2198,7 @@ EXPORT void orc_xl_form_admit_reduce(i32 reqCap, const i32* reqFilA, const i32* 
     }
 }
 
-// CrosslinkerSystem.formAdmit (CrosslinkerSystem.java:713-735)
+// CrosslinkerSystem.formAdmit (CrosslinkerSystem.java:713-738)
 EXPORT void orc_xl_form_admit(i32 reqCap, const i32* reqFilA, const i32* reqFilB, const float* reqLoc1,
                               const float* reqLoc2, const i32* gatePass, const i32* minCand,
                               const i32* activeLinkCount, i32 nLinks, const i32* linkState, const i32* linkFilA,
@@ -2615,7 +2615,7 @@ EXPORT void orc_pool_take_total(void* poolp, const i32* offsets, i32 n) {
     p->taken += m;
 }
 // the host prologue of the turnover block (FullSystemDemoHarness.java:648-651): setCounts,
-// setFires and GrowthStore.refreshRate (GrowthStore.java:84-88)
+// setFires and GrowthStore.refreshRate (GrowthStore.java:81-91)
 EXPORT void orc_turnover_begin(i32 step, i32 seed, i32 fires, double onRate, double bdt, const void* poolp,
                                float* growParams, i32* gc, i32* dc, i32* ac, i32* sc) {
     const OrcPool* p = (const OrcPool*)poolp;

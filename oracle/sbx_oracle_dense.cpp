@@ -2,7 +2,7 @@
 // reference harnesses, driven over host arrays described by the public scene structs.
 //   orc_dense_step : DenseContractileHarness.cpuStep (DenseContractileHarness.java:350-429)
 //   orc_fdt_step   : DiffusionHarness.cpuStepFdt     (DiffusionHarness.java:161-169)
-//   orc_chain_step : DiffusionHarness.cpuStepChain   (DiffusionHarness.java:184-195)
+//   orc_chain_step : DiffusionHarness.cpuStepChain   (DiffusionHarness.java:185-196)
 // The grid and CSR builds use the serial reference forms (gridHistogram/gridScatter,
 // csrHistogram/csrScan/csrScatter); the chunked forms the harness wires produce the
 // same arrays (the reference's own parallel==serial gate, tested separately).
@@ -109,7 +109,21 @@ static void csr_build_serial(const i32* keys, i32 nItems, i32 nRows, i32* cnt, i
     orc_csr_scatter(keys, nItems, off, cnt, list);
 }
 
-EXPORT void orc_dense_step(const sbx_dense_scene* sc, i32 t) {
+EXPORT void orc_brownian_force_supplied(int N, float* rF, float* rT, const float* bTG, const float* bRG,
+                                        const float* tSc, const float* rSc, const float* params,
+                                        const float* noise);
+
+// Supplied-noise mode of the step: the step's six Gaussians per body come from planar
+// arrays [6][n] (filament rods, motor sub-bodies, backbones) instead of the Wang-hash
+// Box-Muller draws of BrownianForceSystem.brownianForce (BrownianForceSystem.java:44-106);
+// the rest of the step is unchanged.
+struct DenseNoise {
+    const float* fil;
+    const float* mot;
+    const float* bb;
+};
+
+static void dense_step(const sbx_dense_scene* sc, i32 t, const DenseNoise* nz) {
     const sbx_filament_store& f = sc->fil;
     const sbx_motor_store& mot = sc->mot;
     const sbx_dimer_store& dim = sc->dim;
@@ -146,10 +160,17 @@ EXPORT void orc_dense_step(const sbx_dense_scene* sc, i32 t) {
     // ---- (ii) minifilament structure ----
     orc_zero_accumulators(nB, b.forceSum, b.torqueSum);
     orc_zero_accumulators(nBb, bb.forceSum, bb.torqueSum);
-    orc_brownian_force(nB, b.randForce, b.randTorque, b.bTransGam, b.bRotGam, b.brownTransScale,
-                       b.brownRotScale, mot.bodyParams, mot.counts);
-    orc_brownian_force(nBb, bb.randForce, bb.randTorque, bb.bTransGam, bb.bRotGam, bb.brownTransScale,
-                       bb.brownRotScale, mini.bbBodyParams, mini.bbCounts);
+    if (nz) {
+        orc_brownian_force_supplied(nB, b.randForce, b.randTorque, b.bTransGam, b.bRotGam, b.brownTransScale,
+                                    b.brownRotScale, mot.bodyParams, nz->mot);
+        orc_brownian_force_supplied(nBb, bb.randForce, bb.randTorque, bb.bTransGam, bb.bRotGam,
+                                    bb.brownTransScale, bb.brownRotScale, mini.bbBodyParams, nz->bb);
+    } else {
+        orc_brownian_force(nB, b.randForce, b.randTorque, b.bTransGam, b.bRotGam, b.brownTransScale,
+                           b.brownRotScale, mot.bodyParams, mot.counts);
+        orc_brownian_force(nBb, bb.randForce, bb.randTorque, bb.bTransGam, bb.bRotGam, bb.brownTransScale,
+                           bb.brownRotScale, mini.bbBodyParams, mini.bbCounts);
+    }
     orc_joints(nB, b.coord, b.uVec, b.segLength, b.bTransGam, b.bRotGam, b.forceSum, b.torqueSum,
                mot.nucleotideState, mot.jointParams);
     orc_dimer_couple(nB, b.coord, b.uVec, b.segLength, b.bTransGam, b.bRotGam, b.forceSum, b.torqueSum, nD,
@@ -176,8 +197,12 @@ EXPORT void orc_dense_step(const sbx_dense_scene* sc, i32 t) {
 
     // ---- (iii)-(v) filaments ----
     orc_zero_accumulators(nSeg, fb.forceSum, fb.torqueSum);
-    orc_brownian_force(nSeg, fb.randForce, fb.randTorque, fb.bTransGam, fb.bRotGam, fb.brownTransScale,
-                       fb.brownRotScale, f.params, f.counts);
+    if (nz)
+        orc_brownian_force_supplied(nSeg, fb.randForce, fb.randTorque, fb.bTransGam, fb.bRotGam,
+                                    fb.brownTransScale, fb.brownRotScale, f.params, nz->fil);
+    else
+        orc_brownian_force(nSeg, fb.randForce, fb.randTorque, fb.bTransGam, fb.bRotGam, fb.brownTransScale,
+                           fb.brownRotScale, f.params, f.counts);
     orc_chain_forces(nSeg, fb.coord, fb.uVec, fb.segLength, f.end2NbrSlot, f.end2NbrSide, f.end1NbrSlot,
                      f.end1NbrSide, fb.bTransGam, fb.bRotGam, fb.forceSum, fb.torqueSum, f.chainParams);
     if (sc->xlinkOn && xl.nLinks > 0) {
@@ -204,8 +229,22 @@ EXPORT void orc_dense_step(const sbx_dense_scene* sc, i32 t) {
     orc_derive(nSeg, fb.coord, fb.uVec, fb.yVec, fb.zVec, fb.end1, fb.end2, fb.segLength);
 }
 
+EXPORT void orc_dense_step(const sbx_dense_scene* sc, i32 t) { dense_step(sc, t, nullptr); }
+
 EXPORT void orc_dense_run(const sbx_dense_scene* sc, i32 t0, i32 nsteps) {
-    for (i32 k = 0; k < nsteps; k++) orc_dense_step(sc, t0 + k);
+    for (i32 k = 0; k < nsteps; k++) dense_step(sc, t0 + k, nullptr);
+}
+
+// Steps t0..t0+nsteps-1 in supplied-noise mode: step t0+k reads noiseFil[k][6][nRods],
+// noiseMot[k][6][3 nMotors] and noiseBb[k][6][nBackbones].
+EXPORT void orc_dense_run_supplied(const sbx_dense_scene* sc, i32 t0, i32 nsteps, const float* noiseFil,
+                                   const float* noiseMot, const float* noiseBb) {
+    const int64_t nf = 6 * (int64_t)sc->fil.body.n, nm = 6 * (int64_t)sc->mot.body.n,
+                  nb = 6 * (int64_t)sc->mini.backbone.n;
+    for (i32 k = 0; k < nsteps; k++) {
+        DenseNoise nz{noiseFil + k * nf, noiseMot + k * nm, noiseBb + k * nb};
+        dense_step(sc, t0 + k, &nz);
+    }
 }
 
 // DiffusionHarness.cpuStepFdt: brownian -> integrate -> derive, with counts[1] = step

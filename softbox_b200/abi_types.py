@@ -33,12 +33,12 @@ class MotorStoreDesc(C.Structure):      # MotorStore.java:32-161
         ("counts", i32p), ("publishParams", i32p)]
 
 
-class DimerStoreDesc(C.Structure):      # DimerStore.java:211-252
+class DimerStoreDesc(C.Structure):      # DimerStore.java:26-67
     _fields_ = [("nDimers", C.c_int32), ("motorA", i32p), ("motorB", i32p), ("parallel", i32p),
                 ("dimerParams", f32p)]
 
 
-class MiniStoreDesc(C.Structure):       # MiniFilamentStore.java:201-308
+class MiniStoreDesc(C.Structure):       # MiniFilamentStore.java:28-135
     _fields_ = [("backbone", RigidBody), ("nBackbones", C.c_int32), ("nDimers", C.c_int32),
                 ("bbBodyParams", f32p), ("bbCounts", i32p), ("headBackboneSlot", i32p), ("motorA", i32p),
                 ("attachAxial", f32p), ("miniData", f32p), ("bbInvDragY", f32p), ("miniParams", f32p),
@@ -101,3 +101,7 @@ class TurnoverBatchDesc(C.Structure):   # packed-network turnover tables (sbx_tu
                 ("depolyParams", f32p), ("depolyRateParams", f32p), ("agingParams", f32p),
                 ("cofilinParams", f32p), ("birthBox", f32p), ("onRate", f64p), ("pools", f64p),
                 ("birthNet", i32p), ("birthBase", i32p)]
+
+
+class DenseNoiseDesc(C.Structure):      # supplied Gaussians of the dense step (sbx_dense_noise)
+    _fields_ = [("fil", f32p), ("mot", f32p), ("bb", f32p), ("t0", C.c_int32), ("nsteps", C.c_int32)]

@@ -33,6 +33,46 @@ __global__ void k_dense_set_counts(const int* d_step, int t_host, int* motCounts
 }
 
 __global__ void k_step_set(int* d_step, int t) { *d_step = t; }
+
+// MechanicsFusion.forceBuild (zero + BrownianForceSystem.brownianForce) in supplied-noise
+// mode: the step's six Gaussians of slot i are noise[counts[1] - t0][k][i]. A step outside
+// the supplied range (the host rejects such runs before launching) draws zeros and sets *err.
+__global__ void k_force_build_supplied(int n, float* F, float* T, float* rF, float* rT, const float* bTG,
+                                       const float* bRG, const float* tSc, const float* rSc, const float* params,
+                                       const int* counts, const float* noise, int t0, int nsteps, int* err) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int k = 0; k < 3; k++) { F[k * n + i] = 0.f; T[k * n + i] = 0.f; }
+    int s = counts[1] - t0;
+    bool in = s >= 0 && s < nsteps;
+    if (!in && i == 0) atomicOr(err, 1);
+    const float* q = noise + (int64_t)(in ? s : 0) * 6 * n + i;
+    float g[6];
+    for (int k = 0; k < 6; k++) g[k] = in ? q[(int64_t)k * n] : 0.f;
+    float gT[3] = {bTG[i], bTG[n + i], bTG[2 * n + i]};
+    float gR[3] = {bRG[i], bRG[n + i], bRG[2 * n + i]};
+    float rf[3], rt[3];
+    brownian_amplitudes(g, tSc[i], rSc[i], params[1], gT, gR, rf, rt);
+    for (int k = 0; k < 3; k++) { rF[k * n + i] = rf[k]; rT[k * n + i] = rt[k]; }
+}
+
+// the noise of one store for the step's force build (null: the Wang-hash draws)
+struct StoreNoise {
+    const float* noise;
+    int t0, nsteps;
+    int* err;
+};
+
+sbx_status force_build(sbx_ctx* ctx, int n, float* F, float* T, float* rF, float* rT, const float* bTG,
+                       const float* bRG, const float* tSc, const float* rSc, const float* params,
+                       const int* counts, const StoreNoise& nz) {
+    if (!nz.noise)
+        return sbx_fusion_force_build(ctx, n, F, T, rF, rT, bTG, bRG, tSc, rSc, params, counts);
+    if (n == 0) return SBX_OK;
+    SBX_LAUNCH(ctx, k_force_build_supplied, blocks(n), 256, n, F, T, rF, rT, bTG, bRG, tSc, rSc, params, counts,
+               nz.noise, nz.t0, nz.nsteps, nz.err);
+    return check_launch(ctx, "dense step: supplied-noise force build");
+}
 __global__ void k_step_advance(int* d_step) { *d_step += 1; }
 
 #define CHK(x)                      \
@@ -133,8 +173,16 @@ sbx_status side_join(sbx_ctx* ctx, const SideStream* side, bool tail = false) {
     return SBX_OK;
 }
 
+// the supplied noise of a plan (sbx_dense_plan_set_noise) as the step sees it
+struct StepNoise {
+    sbx_dense_noise nz;
+    int* err;
+    StoreNoise store(const float* p) const { return StoreNoise{p, nz.t0, nz.nsteps, err}; }
+};
+
 sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_step, int t,
-                          const sbx_batch* bt = nullptr, const SideStream* side = nullptr) {
+                          const sbx_batch* bt = nullptr, const SideStream* side = nullptr,
+                          const StepNoise* noise = nullptr) {
     const sbx_filament_store& f = sc->fil;
     const sbx_motor_store& mot = sc->mot;
     const sbx_dimer_store& dim = sc->dim;
@@ -205,9 +253,9 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
                                            fb.brownTransScale, fb.brownRotScale, f.params, f.counts, bt->segKey,
                                            bt->seeds, 2));
         } else {
-            CHK(sbx_fusion_force_build(ctx, nSeg, fb.forceSum, fb.torqueSum, fb.randForce, fb.randTorque,
-                                       fb.bTransGam, fb.bRotGam, fb.brownTransScale, fb.brownRotScale, f.params,
-                                       f.counts));
+            CHK(force_build(ctx, nSeg, fb.forceSum, fb.torqueSum, fb.randForce, fb.randTorque, fb.bTransGam,
+                            fb.bRotGam, fb.brownTransScale, fb.brownRotScale, f.params, f.counts,
+                            noise ? noise->store(noise->nz.fil) : StoreNoise{}));
         }
         // The crosslinker kernels and the CSR builds read no filament accumulator, so they run
         // before the chain forces; chain and the three gathers then share one pass
@@ -238,11 +286,12 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
     // (ii) minifilament structure. A single network zeroes and draws in one pass per store
     // (MechanicsFusion.forceBuild, the same values as the zero + Brownian pair)
     if (!bt) {
-        CHK(sbx_fusion_force_build(ctx, nB, b.forceSum, b.torqueSum, b.randForce, b.randTorque, b.bTransGam,
-                                   b.bRotGam, b.brownTransScale, b.brownRotScale, mot.bodyParams, mot.counts));
-        CHK(sbx_fusion_force_build(ctx, nBb, bb.forceSum, bb.torqueSum, bb.randForce, bb.randTorque, bb.bTransGam,
-                                   bb.bRotGam, bb.brownTransScale, bb.brownRotScale, mini.bbBodyParams,
-                                   mini.bbCounts));
+        CHK(force_build(ctx, nB, b.forceSum, b.torqueSum, b.randForce, b.randTorque, b.bTransGam, b.bRotGam,
+                        b.brownTransScale, b.brownRotScale, mot.bodyParams, mot.counts,
+                        noise ? noise->store(noise->nz.mot) : StoreNoise{}));
+        CHK(force_build(ctx, nBb, bb.forceSum, bb.torqueSum, bb.randForce, bb.randTorque, bb.bTransGam,
+                        bb.bRotGam, bb.brownTransScale, bb.brownRotScale, mini.bbBodyParams, mini.bbCounts,
+                        noise ? noise->store(noise->nz.bb) : StoreNoise{}));
     } else {
         CHK(sbx_zero_accumulators(ctx, nB, b.forceSum, b.torqueSum));
         CHK(sbx_zero_accumulators(ctx, nBb, bb.forceSum, bb.torqueSum));
@@ -352,6 +401,12 @@ struct sbx_dense_plan {
     // the side stream of the step's filament-side work, with its own sort scratch
     SideStream side{};
     bool sideOk = false;
+    // supplied-noise mode (sbx_dense_plan_set_noise)
+    bool noiseOn = false;
+    sbx_dense_noise noise{};
+    int* noiseErr = nullptr;        // device word: a step outside the supplied range ran
+    // capacity-fallback counters of the fused path (SBX_FUSED_STATS, device)
+    unsigned long long* stats = nullptr;
 };
 
 namespace {
@@ -514,6 +569,12 @@ bool fused_prepare(sbx_dense_plan* p) {
     a.bar = (unsigned long long*)alloc(32);
     a.err = (int*)alloc(16);
     a.d_step = p->d_step;
+    a.stats = p->stats;
+    a.entCap = FUSED_ENT_CAP;
+    a.mCap = FUSED_MCAP;
+    a.mIds = FUSED_MIDS;
+    a.cellUse = FUSED_CELL_SLOTS;
+    a.rowUse = FUSED_ROW_SLOTS;
     for (void* q : p->allocs)
         if (!q) return why("scratch allocation failed");
     return true;
@@ -525,6 +586,46 @@ extern "C" sbx_status sbx_dense_step_unfused(sbx_ctx* ctx, const sbx_dense_scene
     if (!ctx || !sc) return SBX_EINVAL;
     CHK(ensure_scratch(ctx, dense_scratch_bytes(sc)));
     return dense_sequence(ctx, sc, nullptr, t);
+}
+
+// Captures one step (the sequence, then the step-counter advance) into the plan's graph,
+// replacing a previous capture; the supplied noise, when on, is part of the capture.
+static sbx_status capture_step(sbx_dense_plan* p) {
+    sbx_ctx* ctx = p->ctx;
+    cudaStreamSynchronize(ctx->stream);
+    int64_t l0 = ctx->launches;
+    if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return fail(ctx, SBX_ECUDA, "dense plan: begin capture");
+    sbx_status st;
+    StepNoise sn{p->noise, p->noiseErr};
+    {
+        PlanScratch use(p);
+        st = dense_sequence(ctx, &p->scene, p->d_step, 0, p->batched ? &p->batch : nullptr, &p->side,
+                            p->noiseOn ? &sn : nullptr);
+    }
+    if (st == SBX_OK) SBX_LAUNCH(ctx, k_step_advance, 1, 1, p->d_step);
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+    if (st != SBX_OK || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        ctx->launches = l0;
+        cudaGetLastError();
+        return st != SBX_OK ? st : fail(ctx, SBX_ECUDA, std::string("end capture: ") + cudaGetErrorString(ce));
+    }
+    cudaGraphExec_t ex = nullptr;
+    if (cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) {
+        cudaGraphDestroy(g);
+        ctx->launches = l0;
+        cudaGetLastError();
+        return fail(ctx, SBX_ECUDA, "dense plan: graph instantiate");
+    }
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    p->graph = g;
+    p->exec = ex;
+    p->kernels_per_step = (int)(ctx->launches - l0);
+    ctx->launches = l0;
+    return SBX_OK;
 }
 
 static sbx_status plan_create(sbx_ctx* ctx, const sbx_dense_scene* sc, const sbx_batch* bt, sbx_dense_plan** out) {
@@ -562,39 +663,25 @@ static sbx_status plan_create(sbx_ctx* ctx, const sbx_dense_scene* sc, const sbx
         cudaGetLastError();
         return fail(ctx, SBX_ENOMEM, "sbx_dense_plan_create: side stream");
     }
-    // capture one step into a graph
-    cudaStreamSynchronize(ctx->stream);
-    int64_t l0 = ctx->launches;
-    if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
-        cudaFree(p->d_step);
-        delete p;
-        return fail(ctx, SBX_ECUDA, "sbx_dense_plan_create: begin capture");
-    }
-    sbx_status st;
-    {
-        PlanScratch use(p);
-        st = dense_sequence(ctx, &p->scene, p->d_step, 0, p->batched ? &p->batch : nullptr, &p->side);
-    }
-    if (st == SBX_OK) SBX_LAUNCH(ctx, k_step_advance, 1, 1, p->d_step);
-    cudaError_t ce = cudaStreamEndCapture(ctx->stream, &p->graph);
-    if (st != SBX_OK || ce != cudaSuccess) {
-        if (p->graph) cudaGraphDestroy(p->graph);
+    if (cudaMalloc(&p->stats, sizeof(unsigned long long) * SBX_FUSED_STATS) != cudaSuccess ||
+        cudaMemsetAsync(p->stats, 0, sizeof(unsigned long long) * SBX_FUSED_STATS, ctx->stream) != cudaSuccess) {
+        if (p->stats) cudaFree(p->stats);
         cudaFree(p->d_step);
         cudaFree(p->scratch);
         release_side(p);
         delete p;
         cudaGetLastError();
-        return st != SBX_OK ? st : fail(ctx, SBX_ECUDA, std::string("end capture: ") + cudaGetErrorString(ce));
+        return fail(ctx, SBX_ENOMEM, "sbx_dense_plan_create: counters");
     }
-    p->kernels_per_step = (int)(ctx->launches - l0);
-    ctx->launches = l0;
-    if (cudaGraphInstantiate(&p->exec, p->graph, 0) != cudaSuccess) {
-        cudaGraphDestroy(p->graph);
+    // capture one step into a graph
+    sbx_status st = capture_step(p);
+    if (st != SBX_OK) {
+        cudaFree(p->stats);
         cudaFree(p->d_step);
         cudaFree(p->scratch);
         release_side(p);
         delete p;
-        return fail(ctx, SBX_ECUDA, "sbx_dense_plan_create: instantiate");
+        return st;
     }
     if (p->batched) {
         p->fused_ok = false;
@@ -623,6 +710,8 @@ extern "C" sbx_status sbx_dense_plan_run(sbx_dense_plan* p, int32_t t0, int32_t 
     if (!p || nsteps < 0 || mode < 0 || mode > 3) return SBX_EINVAL;
     sbx_ctx* ctx = p->ctx;
     if (nsteps == 0) return SBX_OK;
+    if (p->noiseOn && ((int64_t)t0 < p->noise.t0 || (int64_t)t0 + nsteps > (int64_t)p->noise.t0 + p->noise.nsteps))
+        return fail(ctx, SBX_EINVAL, "sbx_dense_plan_run: steps outside the supplied-noise range");
     if (mode == 3) mode = (p->fused_ok && p->scene.fil.body.n <= SBX_DENSE_AUTO_MAX_FUSED_RODS) ? 2 : 1;
     if (mode == 2) {
         if (!p->fused_ok) return fail(ctx, SBX_ESTATE, "fused path unavailable: " + p->fused_why);
@@ -651,8 +740,10 @@ extern "C" sbx_status sbx_dense_plan_run(sbx_dense_plan* p, int32_t t0, int32_t 
         return check_launch(ctx, "sbx_dense_plan_run");
     }
     PlanScratch use(p);
+    StepNoise sn{p->noise, p->noiseErr};
     for (int k = 0; k < nsteps; k++)
-        CHK(dense_sequence(ctx, &p->scene, nullptr, t0 + k, p->batched ? &p->batch : nullptr, &p->side));
+        CHK(dense_sequence(ctx, &p->scene, nullptr, t0 + k, p->batched ? &p->batch : nullptr, &p->side,
+                           p->noiseOn ? &sn : nullptr));
     return SBX_OK;
 }
 
@@ -661,6 +752,15 @@ extern "C" int32_t sbx_dense_plan_kernels_per_step(sbx_dense_plan* p) { return p
 extern "C" sbx_status sbx_dense_plan_status(sbx_dense_plan* p, int32_t* flags) {
     if (!p || !flags) return SBX_EINVAL;
     *flags = 0;
+    if (p->noiseErr) {
+        int ne = 0;
+        cudaMemcpyAsync(&ne, p->noiseErr, sizeof(int), cudaMemcpyDeviceToHost, p->ctx->stream);
+        CHK(sbx_ctx_sync(p->ctx));
+        if (ne) {
+            cudaMemsetAsync(p->noiseErr, 0, sizeof(int), p->ctx->stream);
+            return fail(p->ctx, SBX_EINVAL, "dense step: a step ran outside the supplied-noise range");
+        }
+    }
     if (!p->fused_ok) return SBX_OK;
     int h = 0;
     cudaMemcpyAsync(&h, p->fa.err, sizeof(int), cudaMemcpyDeviceToHost, p->ctx->stream);
@@ -691,6 +791,70 @@ extern "C" sbx_status sbx_dense_plan_test_barrier_extra(sbx_dense_plan* p, int32
     return SBX_OK;
 }
 
+extern "C" sbx_status sbx_dense_plan_set_noise(sbx_dense_plan* p, const sbx_dense_noise* nz) {
+    if (!p) return SBX_EINVAL;
+    sbx_ctx* ctx = p->ctx;
+    if (p->batched) return fail(ctx, SBX_EINVAL, "sbx_dense_plan_set_noise: not available for packed plans");
+    const sbx_dense_scene& sc = p->scene;
+    if (nz) {
+        const int64_t nf = sc.fil.body.n, nm = sc.mot.body.n, nb = sc.mini.backbone.n;
+        if (nz->nsteps < 1 || (nf > 0 && !nz->fil) || (nm > 0 && !nz->mot) || (nb > 0 && !nz->bb))
+            return fail(ctx, SBX_EINVAL, "sbx_dense_plan_set_noise: missing array or empty range");
+        const float* arr[3] = {nz->fil, nz->mot, nz->bb};
+        const int64_t len[3] = {nf, nm, nb};
+        for (int k = 0; k < 3; k++) {
+            if (len[k] == 0) continue;
+            bool bad = false;
+            CHK(any_nonfinite(ctx, arr[k], 6 * len[k] * nz->nsteps, &bad));
+            if (bad) return fail(ctx, SBX_ENONFINITE, "sbx_dense_plan_set_noise: noise holds NaN/Inf");
+        }
+        if (!p->noiseErr) {
+            if (cudaMalloc(&p->noiseErr, sizeof(int)) != cudaSuccess)
+                return fail(ctx, SBX_ENOMEM, "sbx_dense_plan_set_noise: flag");
+            cudaMemsetAsync(p->noiseErr, 0, sizeof(int), ctx->stream);
+        }
+    }
+    bool wasOn = p->noiseOn;
+    sbx_dense_noise was = p->noise;
+    p->noiseOn = nz != nullptr;
+    p->noise = nz ? *nz : sbx_dense_noise{};
+    sbx_status st = capture_step(p);
+    if (st != SBX_OK) {
+        p->noiseOn = wasOn;
+        p->noise = was;
+        return st;
+    }
+    FusedArgs& a = p->fa;
+    a.nzFil = p->noiseOn ? p->noise.fil : nullptr;
+    a.nzMot = p->noiseOn ? p->noise.mot : nullptr;
+    a.nzBb = p->noiseOn ? p->noise.bb : nullptr;
+    a.nzT0 = p->noise.t0;
+    a.nzN = p->noise.nsteps;
+    return SBX_OK;
+}
+
+extern "C" sbx_status sbx_dense_plan_fused_stats(sbx_dense_plan* p, int64_t* out, int32_t reset) {
+    if (!p || !out) return SBX_EINVAL;
+    unsigned long long h[SBX_FUSED_STATS];
+    cudaMemcpyAsync(h, p->stats, sizeof(h), cudaMemcpyDeviceToHost, p->ctx->stream);
+    if (reset) cudaMemsetAsync(p->stats, 0, sizeof(h), p->ctx->stream);
+    CHK(sbx_ctx_sync(p->ctx));
+    for (int k = 0; k < SBX_FUSED_STATS; k++) out[k] = (int64_t)h[k];
+    return SBX_OK;
+}
+
+extern "C" sbx_status sbx_dense_plan_test_caps(sbx_dense_plan* p, int32_t entCap, int32_t motorCap, int32_t motorIds,
+                                               int32_t rowSlots, int32_t cellSlots) {
+    if (!p) return SBX_EINVAL;
+    auto clampCap = [](int v, int cap) { return v < 0 ? cap : (v > cap ? cap : v); };
+    p->fa.entCap = clampCap(entCap, FUSED_ENT_CAP);
+    p->fa.mCap = clampCap(motorCap, FUSED_MCAP);
+    p->fa.mIds = clampCap(motorIds, FUSED_MIDS);
+    p->fa.rowUse = clampCap(rowSlots, FUSED_ROW_SLOTS);
+    p->fa.cellUse = clampCap(cellSlots, FUSED_CELL_SLOTS);
+    return SBX_OK;
+}
+
 extern "C" sbx_status sbx_dense_plan_destroy(sbx_dense_plan* p) {
     if (!p) return SBX_EINVAL;
     // the plan may outlive its context (language runtimes finalise objects in any order at
@@ -700,6 +864,8 @@ extern "C" sbx_status sbx_dense_plan_destroy(sbx_dense_plan* p) {
     if (p->graph) cudaGraphDestroy(p->graph);
     if (p->d_step) cudaFree(p->d_step);
     if (p->scratch) cudaFree(p->scratch);
+    if (p->noiseErr) cudaFree(p->noiseErr);
+    if (p->stats) cudaFree(p->stats);
     release_side(p);
     for (void* q : p->allocs) cudaFree(q);
     delete p;

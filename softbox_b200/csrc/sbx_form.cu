@@ -1,6 +1,6 @@
 // sbx_form.cu — crosslinker formation and the scan-rank free-list allocator of the C ABI.
 //
-// CrosslinkerSystem formation (CrosslinkerSystem.java:417-752): candidate segment pairs
+// CrosslinkerSystem formation (CrosslinkerSystem.java:405-756): candidate segment pairs
 // (all-pairs or over a dedicated formation grid, FormationGrid.java), per-candidate
 // gates, one-new-link-per-segment admission against start-of-step state, then the
 // allocator (:297-345): free list of FREE slots in index order, dense ranks of the
@@ -20,10 +20,10 @@ using namespace sbx;
 
 namespace {
 
-constexpr int FORM_MAXC = 256;          // CrosslinkerSystem.java:472
+constexpr int FORM_MAXC = 256;          // CrosslinkerSystem.java:457
 constexpr int LINK_ACTIVE_STATE = 0;    // CrosslinkerStore.java:57
 
-// the coarse capsule bound of filFilCandidates / gridFormCount (CrosslinkerSystem.java:444-448)
+// the coarse capsule bound of filFilCandidates / gridFormCount (CrosslinkerSystem.java:414-420)
 __device__ __forceinline__ bool form_pair_ok(int nSeg, const float* coord, const float* segLength, const int* filID,
                                              int fi, int j, double cix, double ciy, double ciz, double hi,
                                              double grab) {
@@ -90,7 +90,7 @@ __device__ __forceinline__ void form_cells(double cix, double ciy, double ciz, c
     }
 }
 
-// CrosslinkerSystem.gridFormCount (CrosslinkerSystem.java:474-516)
+// CrosslinkerSystem.gridFormCount (CrosslinkerSystem.java:461-512)
 __global__ void k_grid_form_count(int nSeg, const float* coord, const float* segLength, const int* filID,
                                   const float* gp, const int* gd, const int* offsets, const int* contents,
                                   int* candCountSeg, const float* fp) {
@@ -116,7 +116,7 @@ __global__ void k_grid_form_count(int nSeg, const float* coord, const float* seg
     candCountSeg[i] = cnt < FORM_MAXC ? cnt : FORM_MAXC;
 }
 
-// CrosslinkerSystem.gridFormEmit (CrosslinkerSystem.java:538-595): partners ascending in
+// CrosslinkerSystem.gridFormEmit (CrosslinkerSystem.java:535-602): partners ascending in
 // the segment's owned region; a full region keeps the smallest FORM_MAXC
 __global__ void k_grid_form_emit(int nSeg, const float* coord, const float* segLength, const int* filID,
                                  const float* gp, const int* gd, const int* offsets, const int* contents,
@@ -160,7 +160,7 @@ __global__ void k_grid_form_emit(int nSeg, const float* coord, const float* segL
 }
 
 // ---------------------------------------------------------------- gates
-// CrosslinkerSystem.formGates (CrosslinkerSystem.java:600-665)
+// CrosslinkerSystem.formGates (CrosslinkerSystem.java:607-675)
 __global__ void k_form_gates(int nSeg, const float* fU, const float* fE1, const float* fE2, const float* segLength,
                              int reqCap, const int* reqFilA, const int* reqFilB, float* reqLoc1, float* reqLoc2,
                              int* reqOrient, int* gatePass, const float* fp, const int* fc) {
@@ -227,7 +227,7 @@ __global__ void k_fill(int* a, int n, int v) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = v;
 }
 
-// CrosslinkerSystem.formAdmitReduce (CrosslinkerSystem.java:670-682): an integer minimum,
+// CrosslinkerSystem.formAdmitReduce (CrosslinkerSystem.java:680-691): an integer minimum,
 // whatever the order of the updates
 __global__ void k_admit_reduce(int reqCap, const int* reqFilA, const int* reqFilB, const int* gatePass, int* minCand) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -236,7 +236,7 @@ __global__ void k_admit_reduce(int reqCap, const int* reqFilA, const int* reqFil
     atomicMin(&minCand[reqFilB[c]], c);
 }
 
-// CrosslinkerSystem.formAdmit (CrosslinkerSystem.java:713-735): the spacing test is an OR
+// CrosslinkerSystem.formAdmit (CrosslinkerSystem.java:713-738): the spacing test is an OR
 // over the existing ACTIVE links, so it may stop at the first violation
 __global__ void k_admit(int reqCap, const int* reqFilA, const int* reqFilB, const float* reqLoc1, const float* reqLoc2,
                         const int* gatePass, const int* minCand, const int* activeLinkCount, int nLinks,
@@ -274,7 +274,7 @@ __global__ void k_free_scatter(int C, const int* linkState, const int* freeOffse
     if (s < C && linkState[s] < 0) freeList[freeOffsets[s]] = s;
 }
 
-// CrosslinkerSystem.allocate (CrosslinkerSystem.java:322-341)
+// CrosslinkerSystem.allocate (CrosslinkerSystem.java:323-345)
 __global__ void k_allocate(int K, const int* reqFilA, const int* reqFilB, const float* reqLoc1, const float* reqLoc2,
                            const int* rankOffsets, const int* freeList, const int* freeOffsets, int C, int* linkFilA,
                            int* linkFilB, float* loc1, float* loc2, int* linkState, float* strainHist,
@@ -294,7 +294,7 @@ __global__ void k_allocate(int K, const int* reqFilA, const int* reqFilB, const 
     linkState[slot] = LINK_ACTIVE_STATE;
 }
 
-// CrosslinkerSystem.placeOrient (CrosslinkerSystem.java:740-752)
+// CrosslinkerSystem.placeOrient (CrosslinkerSystem.java:742-756)
 __global__ void k_place_orient(int K, const int* reqOrient, const int* rankOffsets, const int* freeList,
                                const int* freeOffsets, int C, int* linkOrientSame, float* torqueMagHist,
                                int* torqueMagPlace) {

@@ -40,8 +40,7 @@ using namespace sbx;
 
 namespace {
 
-constexpr long long SPIN_LIMIT = 1LL << 24;    // x ~64 ns sleeps: about one second (bulk-copy waits)
-constexpr unsigned long long WAIT_NS = 1000000000ULL;   // barrier waits give up after one second
+constexpr unsigned long long WAIT_NS = 1000000000ULL;   // barrier and bulk-copy waits give up after one second
 constexpr int ERR_BARRIER = 1, ERR_REACH_OVERFLOW = 2, ERR_TMA = 4, ERR_LIST = 8;
 
 // shared memory of one CTA, reused by the phases
@@ -99,13 +98,13 @@ __device__ bool counter_sync(unsigned long long* ctr, unsigned long long& target
         bool ok = true;
         while (ld_acquire(ctr) < target) {
             if ((++it & 63u) == 0) {
-                if (vload(err) & ERR_BARRIER) { ok = false; break; }
+                if (vload(err) & (ERR_BARRIER | ERR_TMA)) { ok = false; break; }
                 unsigned long long now = gtimer();
                 if (t0 == 0) t0 = now;
                 else if (now - t0 > WAIT_NS) { atomicOr(err, ERR_BARRIER); ok = false; break; }
             }
         }
-        s_ok = ok && (vload(err) & ERR_BARRIER) == 0;
+        s_ok = ok && (vload(err) & (ERR_BARRIER | ERR_TMA)) == 0;
     }
     __syncthreads();
     return s_ok;
@@ -121,11 +120,21 @@ __device__ __forceinline__ unsigned long long counter_base(const unsigned long l
 __device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
 __device__ __forceinline__ int gthreads() { return gridDim.x * blockDim.x; }
 
-// BrownianForceSystem.brownianForces for one slot (BrownianForceSystem.java:183-245)
-__device__ __forceinline__ void brownian_slot(const sbx_rigid_body& b, int s, int t, int seed, float mag) {
+// BrownianForceSystem.brownianForce for one slot (BrownianForceSystem.java:44-106); in
+// supplied-noise mode the six Gaussians come from noise[t - t0][6][n] (a step outside the
+// supplied range, which the host rejects before the launch, draws zeros)
+__device__ __forceinline__ void brownian_slot(const FusedArgs& a, const sbx_rigid_body& b, int s, int t, int seed,
+                                              float mag, const float* noise) {
     const int n = b.n;
     float g[6];
-    gauss6_wang(s, t, seed, g);
+    if (noise) {
+        int k = t - a.nzT0;
+        bool in = k >= 0 && k < a.nzN;
+        const float* q = noise + (int64_t)(in ? k : 0) * 6 * n + s;
+        for (int j = 0; j < 6; j++) g[j] = in ? q[(int64_t)j * n] : 0.f;
+    } else {
+        gauss6_wang(s, t, seed, g);
+    }
     float gT[3] = {b.bTransGam[s], b.bTransGam[n + s], b.bTransGam[2 * n + s]};
     float gR[3] = {b.bRotGam[s], b.bRotGam[n + s], b.bRotGam[2 * n + s]};
     float rf[3], rt[3];
@@ -149,24 +158,35 @@ __device__ __forceinline__ int list_rank(const FusedArgs& a, int head, const int
     return r;
 }
 
-// Appends `item` to row r: the histogram's old count is its arrival index; the first S
-// arrivals take the row's fixed slots, later ones join the row's overflow list.
-__device__ __forceinline__ void row_insert(int* cnt, int* slot, int S, int* head, int* next, int r, int item) {
+// Appends `item` to row r: the histogram's old count is its arrival index; the first `use`
+// (<= S, the slot stride) arrivals take the row's fixed slots, later ones join the row's
+// overflow list (returns 1).
+__device__ __forceinline__ int row_insert(int* cnt, int* slot, int S, int use, int* head, int* next, int r,
+                                          int item) {
     int j = atomicAdd(&cnt[r], 1);
-    if (j < S) slot[(size_t)r * S + j] = item;
-    else next[item] = atomicExch(&head[r], item);
+    if (j < use) {
+        slot[(size_t)r * S + j] = item;
+        return 0;
+    }
+    next[item] = atomicExch(&head[r], item);
+    return 1;
+}
+
+// adds a thread's count of a capacity fallback to the plan's counters
+__device__ __forceinline__ void stat_add(const FusedArgs& a, int which, int v) {
+    if (v) atomicAdd(&a.stats[which], (unsigned long long)v);
 }
 
 // rank of `item` in row r: the row's members with a smaller index (slots, then the list)
 template <int S>
-__device__ __forceinline__ int row_rank(const FusedArgs& a, const int* cnt, const int* slot, const int* head,
-                                        const int* next, int r, int item, int bound) {
+__device__ __forceinline__ int row_rank(const FusedArgs& a, const int* cnt, const int* slot, int use,
+                                        const int* head, const int* next, int r, int item, int bound) {
     int n = cnt[r];
     int rank = 0;
 #pragma unroll
     for (int j = 0; j < S; j++)
-        if (j < n) rank += slot[(size_t)r * S + j] < item;
-    if (n > S) rank += list_rank(a, head[r], next, item, bound);
+        if (j < n && j < use) rank += slot[(size_t)r * S + j] < item;
+    if (n > use) rank += list_rank(a, head[r], next, item, bound);
     return rank;
 }
 
@@ -182,6 +202,7 @@ __device__ void phase_publish_bin(const FusedArgs& a, int t) {
     const int nX = a.nX, nY = a.nY, nZ = a.nZ;
     const int nLk = a.xlOn ? a.nL : 0;
     const int total = cap + nLk + nSeg;
+    int overCell = 0, overLink = 0;
     for (int i = gtid(); i < total; i += gthreads()) {
         if (i >= cap + nLk) {
             // the motor lists and counts of the previous step were last read by its rod phase
@@ -201,7 +222,7 @@ __device__ void phase_publish_bin(const FusedArgs& a, int t) {
                            cell_coord(c[2], gp[2], gp[4], nZ) * (nX * nY);
                 g.bodyCell[i] = cell;
                 atomicAdd(&a.cntSeg[cell], 1);
-                row_insert(a.cntCell, a.cellSlot, FUSED_CELL_SLOTS, a.cellHead, a.cellNext, cell, i);
+                overCell += row_insert(a.cntCell, a.cellSlot, FUSED_CELL_SLOTS, a.cellUse, a.cellHead, a.cellNext, cell, i);
             } else {
                 g.bodyCell[i] = -1;
             }
@@ -224,7 +245,7 @@ __device__ void phase_publish_bin(const FusedArgs& a, int t) {
                 int cell = cell_coord(hd[0], gp[0], gp[4], nX) + cell_coord(hd[1], gp[1], gp[4], nY) * nX +
                            cell_coord(hd[2], gp[2], gp[4], nZ) * (nX * nY);
                 g.bodyCell[b] = cell;
-                row_insert(a.cntCell, a.cellSlot, FUSED_CELL_SLOTS, a.cellHead, a.cellNext, cell, b);
+                overCell += row_insert(a.cntCell, a.cellSlot, FUSED_CELL_SLOTS, a.cellUse, a.cellHead, a.cellNext, cell, b);
             } else {
                 g.bodyCell[b] = -1;
             }
@@ -233,10 +254,12 @@ __device__ void phase_publish_bin(const FusedArgs& a, int t) {
         } else {
             int k = i - cap;
             int la = xl.linkFilA[k], lb = xl.linkFilB[k];
-            if (la >= 0) row_insert(a.cntA, a.slotA, FUSED_ROW_SLOTS, a.headA, a.nextA, la, k);
-            if (lb >= 0) row_insert(a.cntB, a.slotB, FUSED_ROW_SLOTS, a.headB, a.nextB, lb, k);
+            if (la >= 0) overLink += row_insert(a.cntA, a.slotA, FUSED_ROW_SLOTS, a.rowUse, a.headA, a.nextA, la, k);
+            if (lb >= 0) overLink += row_insert(a.cntB, a.slotB, FUSED_ROW_SLOTS, a.rowUse, a.headB, a.nextB, lb, k);
         }
     }
+    stat_add(a, ST_CELL_LIST, overCell);
+    stat_add(a, ST_LINK_LIST, overLink);
 }
 
 // CrosslinkerSystem.unbind (Bell law over the strain window, CrosslinkerSystem.java:
@@ -274,8 +297,8 @@ __device__ void motor_brownian(const FusedArgs& a, int t, int firstWarp) {
     if (w < firstWarp) return;
     const int nB = a.nB, n = nB + a.nBb;
     for (int j = (w - firstWarp) * 32 + (threadIdx.x & 31); j < n; j += (nw - firstWarp) * 32) {
-        if (j < nB) brownian_slot(sc.mot.body, j, t, sc.seed, sc.mot.bodyParams[1]);
-        else brownian_slot(sc.mini.backbone, j - nB, t, sc.seedBb, sc.mini.bbBodyParams[1]);
+        if (j < nB) brownian_slot(a, sc.mot.body, j, t, sc.seed, sc.mot.bodyParams[1], a.nzMot);
+        else brownian_slot(a, sc.mini.backbone, j - nB, t, sc.seedBb, sc.mini.bbBodyParams[1], a.nzBb);
     }
 }
 
@@ -377,7 +400,7 @@ __device__ void phase_place(const FusedArgs& a) {
         if (i < a.cap) {
             int c = g.bodyCell[i];
             if (c < 0) continue;
-            int rank = row_rank<FUSED_CELL_SLOTS>(a, a.cntCell, a.cellSlot, a.cellHead, a.cellNext, c, i, a.cap);
+            int rank = row_rank<FUSED_CELL_SLOTS>(a, a.cntCell, a.cellSlot, a.cellUse, a.cellHead, a.cellNext, c, i, a.cap);
             g.gridCellContents[g.gridCellOffsets[c] + rank] = i;
             // segment endpoints in cell order for the reach walk: within a cell the segments
             // (slots below nSeg) precede the motor heads, so a segment's rank among the
@@ -392,10 +415,10 @@ __device__ void phase_place(const FusedArgs& a) {
             int la = xl.linkFilA[k], lb = xl.linkFilB[k];
             if (la >= 0)
                 xl.segIdxA[xl.segOffsetsA[la] +
-                           row_rank<FUSED_ROW_SLOTS>(a, a.cntA, a.slotA, a.headA, a.nextA, la, k, a.nL)] = k;
+                           row_rank<FUSED_ROW_SLOTS>(a, a.cntA, a.slotA, a.rowUse, a.headA, a.nextA, la, k, a.nL)] = k;
             if (lb >= 0)
                 xl.segIdxB[xl.segOffsetsB[lb] +
-                           row_rank<FUSED_ROW_SLOTS>(a, a.cntB, a.slotB, a.headB, a.nextB, lb, k, a.nL)] = k;
+                           row_rank<FUSED_ROW_SLOTS>(a, a.cntB, a.slotB, a.rowUse, a.headB, a.nextB, lb, k, a.nL)] = k;
         }
     }
 }
@@ -508,7 +531,10 @@ __device__ void mini_unit(const FusedArgs& a, MiniSmem& ms, int u, int t) {
             float arc;
             int rc = reach_walk_bind(a, mx, my, mz, mux, muy, muz, rux, ruy, ruz, slice, kp[7], kp[8], &best, &arc);
             sc.grid.reachCount[m] = rc;
-            if (rc > MAX_CAND) atomicOr(a.err, ERR_REACH_OVERFLOW);
+            if (rc > MAX_CAND) {
+                atomicOr(a.err, ERR_REACH_OVERFLOW);
+                stat_add(a, ST_REACH_OVER, 1);
+            }
             if (bs == FREE_BINDABLE && best >= 0) {
                 bs = best;
                 mot.bindArc[m] = arc;
@@ -517,7 +543,7 @@ __device__ void mini_unit(const FusedArgs& a, MiniSmem& ms, int u, int t) {
             mot.capStats[m] = cs;
             mot.nucleotideState[m] = cycle_one(m, mot.nucleotideState[m], bs >= 0, mot.forceDotHist + 10 * m,
                                                mot.nucParams, t, sc.seed);
-            if (bs >= 0) row_insert(a.cntM, a.slotM, FUSED_ROW_SLOTS, a.headM, a.nextM, bs, m);
+            if (bs >= 0) stat_add(a, ST_MOTOR_LIST, row_insert(a.cntM, a.slotM, FUSED_ROW_SLOTS, a.rowUse, a.headM, a.nextM, bs, m));
         }
     } else if (tid < 96) {
         // warps 1-2: motor joints (local motor k/2, joint k&1), then a lever (warp 1) or a tether (warp 2)
@@ -686,7 +712,7 @@ __device__ void phase_motors_links(const FusedArgs& a, FusedSmem& sm, int t) {
                                         load_rod(n, s1, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.bRotGam));
                 }
             }
-            brownian_slot(fb, i, t, a.filSeed, fs.params[1]);
+            brownian_slot(a, fb, i, t, a.filSeed, fs.params[1], a.nzFil);
         }
     }
     // the reference's activeLinkCount array holds this step's counts
@@ -705,7 +731,7 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 
 // FP64 row sum of CSR c for local rod l, from the fetched entries (global past the cap);
 // the arithmetic of csr_gather_row
-__device__ __forceinline__ void gather_staged(const RodSmem& rs, int c, int l, int eBase, const int* list,
+__device__ __forceinline__ void gather_staged(const RodSmem& rs, int c, int l, int eBase, int entCap, const int* list,
                                               const float* payload, int stride, int poff, const int* guard,
                                               double f[3], double t[3]) {
     f[0] = f[1] = f[2] = 0.0;
@@ -714,7 +740,7 @@ __device__ __forceinline__ void gather_staged(const RodSmem& rs, int c, int l, i
     for (int k = rs.off[c][l]; k < rs.off[c][l + 1]; k++) {
         int e = eBase + (k - k0);
         const float* p;
-        if (e < FUSED_ENT_CAP) {
+        if (e < entCap) {
             if (!rs.entOk[e]) continue;
             p = rs.ent[e];
         } else {
@@ -727,7 +753,27 @@ __device__ __forceinline__ void gather_staged(const RodSmem& rs, int c, int l, i
     }
 }
 
-__device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t* mbar, unsigned& phase) {
+// Bounded wait of the calling thread on the bulk-copy barrier's phase `phase` (one second by
+// %globaltimer); returns whether the phase completed.
+__device__ __forceinline__ bool bulk_wait(uint64_t* mbar, unsigned phase) {
+    unsigned mb = (unsigned)__cvta_generic_to_shared(mbar);
+    unsigned done = 0, it = 0;
+    unsigned long long t0 = 0;
+    while (!done) {
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(done) : "r"(mb), "r"(phase) : "memory");
+        if (!done && (++it & 15u) == 0) {
+            unsigned long long now = gtimer();
+            if (t0 == 0) t0 = now;
+            else if (now - t0 > WAIT_NS) break;
+        }
+    }
+    return done != 0;
+}
+
+// One rod group; returns false when its bulk copies did not complete in time (ERR_TMA set;
+// the CTA then leaves the launch).
+__device__ bool rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t* mbar, unsigned& phase) {
     const sbx_dense_scene& sc = a.sc;
     const sbx_filament_store& f = sc.fil;
     const sbx_rigid_body& fb = f.body;
@@ -769,22 +815,22 @@ __device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
         s1 = f.end1NbrSlot[i]; n1 = f.end1NbrSide[i];
     }
     if (tma) {
-        // bounded wait on the transaction barrier
-        unsigned mb = (unsigned)__cvta_generic_to_shared(mbar);
-        long long it = 0;
-        unsigned done = 0;
-        while (!done) {
-            asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-                         : "=r"(done) : "r"(mb), "r"(phase) : "memory");
-            if (!done && ++it > SPIN_LIMIT) {
+        // bounded wait on the transaction barrier, one verdict per CTA: the phase completed
+        // if any thread saw it complete. Otherwise the copies may still be landing in the
+        // staging buffer, so nothing else is written there: the CTA flags the failure,
+        // gives its copies one more bounded wait and leaves the launch (the other CTAs see
+        // the flag at their next grid barrier and return too).
+        bool ok = __syncthreads_or(bulk_wait(mbar, phase)) != 0;
+        if (!ok) {
+            if (tid == 0) {
                 atomicOr(a.err, ERR_TMA);
-                break;
+                bulk_wait(mbar, phase);
             }
+            __syncthreads();
+            return false;
         }
         phase ^= 1u;
-        if (!done) tma = false;
-    }
-    if (!tma) {
+    } else {
         for (int k = 0; k < 10; k++)
             for (int j = tid; j < cnt; j += blockDim.x) sc_[k][j] = src[k][j];
     }
@@ -809,7 +855,8 @@ __device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
     // the link CSR payloads of the group's rows (link A, link B), one entry per thread
     const int eA = a.xlOn ? rs.off[0][cnt] - rs.off[0][0] : 0;
     const int eB = a.xlOn ? rs.off[1][cnt] - rs.off[1][0] : 0;
-    const int eLim = min(eA + eB, FUSED_ENT_CAP);
+    const int eLim = min(eA + eB, a.entCap);
+    if (tid == 0) stat_add(a, ST_ENT_GLOBAL, eA + eB - eLim);
     const int first = tid;
     for (int e = first; e < eLim; e += blockDim.x) {
         const float* p;
@@ -836,7 +883,7 @@ __device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
         const int nm = a.cntM[r];
         int got = 0;
         auto put = [&](int m) {
-            if (got < FUSED_MIDS) {
+            if (got < a.mIds) {
                 int q = got;
                 while (q > 0 && ids[q - 1] > m) { ids[q] = ids[q - 1]; q--; }
                 ids[q] = m;
@@ -845,11 +892,12 @@ __device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
         };
         int sl[FUSED_ROW_SLOTS];
 #pragma unroll
-        for (int j = 0; j < FUSED_ROW_SLOTS; j++) sl[j] = j < nm ? a.slotM[(size_t)r * FUSED_ROW_SLOTS + j] : 0;
+        for (int j = 0; j < FUSED_ROW_SLOTS; j++)
+            sl[j] = (j < nm && j < a.rowUse) ? a.slotM[(size_t)r * FUSED_ROW_SLOTS + j] : 0;
 #pragma unroll
         for (int j = 0; j < FUSED_ROW_SLOTS; j++)
-            if (j < nm) put(sl[j]);
-        if (nm > FUSED_ROW_SLOTS) {
+            if (j < nm && j < a.rowUse) put(sl[j]);
+        if (nm > a.rowUse) {
             int it = 0;
             for (int m = a.headM[r]; m >= 0; m = a.nextM[m]) {
                 put(m);
@@ -857,8 +905,10 @@ __device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
             }
         }
         rs.mCnt[l] = got == nm ? nm : 0;
-        int np = nm < FUSED_MCAP ? nm : FUSED_MCAP;
-        if (got != nm) np = 0;
+        // reactions staged only for rows whose sorted slots are complete (nm <= mIds)
+        int np = nm < a.mCap ? nm : a.mCap;
+        if (got != nm || nm > a.mIds) np = 0;
+        if (got == nm) stat_add(a, nm > a.mIds ? ST_MIDS_WALK : ST_MPAY_GLOBAL, nm > a.mIds ? 1 : nm - np);
         for (int q = 0; q < np; q++) {
             const float* p = sc.bondData + (int64_t)ids[q] * XB_STRIDE + 6;
             for (int k = 0; k < 6; k++) rs.mPay[l][q][k] = p[k];
@@ -879,18 +929,18 @@ __device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
         for (int k = 0; k < 3; k++) { F[k] = (float)(0.0f + fd[k]); T[k] = (float)(0.0f + td[k]); }
         double gf[3], gt[3];
         if (a.xlOn) {
-            gather_staged(rs, 0, tid, 0, xl.segIdxA, xl.xlinkData, XL_STRIDE, 0, xl.linkState, gf, gt);
+            gather_staged(rs, 0, tid, 0, a.entCap, xl.segIdxA, xl.xlinkData, XL_STRIDE, 0, xl.linkState, gf, gt);
             for (int k = 0; k < 3; k++) { F[k] = (float)(F[k] + gf[k]); T[k] = (float)(T[k] + gt[k]); }
-            gather_staged(rs, 1, tid, eA, xl.segIdxB, xl.xlinkData, XL_STRIDE, 6, xl.linkState, gf, gt);
+            gather_staged(rs, 1, tid, eA, a.entCap, xl.segIdxB, xl.xlinkData, XL_STRIDE, 6, xl.linkState, gf, gt);
             for (int k = 0; k < 3; k++) { F[k] = (float)(F[k] + gf[k]); T[k] = (float)(T[k] + gt[k]); }
         }
         // CrossBridgeSystem.segGather: FP64 sums of the bound motors' reactions, ascending slot
         gf[0] = gf[1] = gf[2] = 0.0;
         gt[0] = gt[1] = gt[2] = 0.0;
         int nm = rs.mCnt[tid];
-        if (nm <= FUSED_MIDS) {
+        if (nm <= a.mIds) {
             for (int q = 0; q < nm; q++) {
-                const float* p = q < FUSED_MCAP ? rs.mPay[tid][q]
+                const float* p = q < a.mCap ? rs.mPay[tid][q]
                                                 : sc.bondData + (int64_t)rs.mIds[tid][q] * XB_STRIDE + 6;
                 gf[0] += p[0]; gf[1] += p[1]; gf[2] += p[2];
                 gt[0] += p[3]; gt[1] += p[4]; gt[2] += p[5];
@@ -901,6 +951,7 @@ __device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
             for (int q = 0; q < nm; q++) {
                 int next = 0x7fffffff, it = 0;
                 for (int j = 0; j < FUSED_ROW_SLOTS; j++) {
+                    if (j >= nm || j >= a.rowUse) break;
                     int m = a.slotM[(size_t)i * FUSED_ROW_SLOTS + j];
                     if (m > last && m < next) next = m;
                 }
@@ -923,6 +974,7 @@ __device__ void rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
         if (bx.active) confine_one(bx, c, uu, sc_[6][tid], sc_[7][tid], F, T);
         integrate_derive_store(fb, i, F, T, f.params[0]);
     }
+    return true;
 }
 
 // The motor CSR of the reference's cpuStep (CrossBridgeSystem.csrHistogram/csrScan/
@@ -944,20 +996,22 @@ __device__ void motor_csr(const FusedArgs& a, int h, int nH, unsigned long long&
     for (int m = h * blockDim.x + threadIdx.x; m < a.nM; m += nH * blockDim.x) {
         int bs = sc.mot.boundSeg[m];
         if (bs < 0) continue;
-        int pos = sc.segMotorOffsets[bs] + row_rank<FUSED_ROW_SLOTS>(a, a.cntM, a.slotM, a.headM, a.nextM, bs, m, a.nM);
+        int pos = sc.segMotorOffsets[bs] + row_rank<FUSED_ROW_SLOTS>(a, a.cntM, a.slotM, a.rowUse, a.headM, a.nextM, bs, m, a.nM);
         if (pos < a.nM) sc.segMotorMyo[pos] = m;
     }
 }
 
-__device__ void phase_rods(const FusedArgs& a, FusedSmem& sm, int t, uint64_t* mbar, unsigned& phase,
+__device__ bool phase_rods(const FusedArgs& a, FusedSmem& sm, int t, uint64_t* mbar, unsigned& phase,
                            unsigned long long& hTarget) {
-    for (int u = blockIdx.x; u < a.nRodUnits; u += gridDim.x) rod_unit(a, sm.rod, u, t, mbar, phase);
+    for (int u = blockIdx.x; u < a.nRodUnits; u += gridDim.x)
+        if (!rod_unit(a, sm.rod, u, t, mbar, phase)) return false;
     if ((int)blockIdx.x >= a.kHelp0) motor_csr(a, blockIdx.x - a.kHelp0, gridDim.x - a.kHelp0, hTarget);
     // reset the histograms and lists of this step's grid and link CSRs for the next step
     for (int i = gtid(); i < a.C; i += gthreads()) { a.cntCell[i] = 0; a.cntSeg[i] = 0; a.cellHead[i] = -1; }
     for (int i = gtid(); i < a.nSeg; i += gthreads()) {
         a.cntAct[i] = 0; a.cntA[i] = 0; a.cntB[i] = 0; a.headA[i] = -1; a.headB[i] = -1;
     }
+    return true;
 }
 
 __global__ void __launch_bounds__(FUSED_THREADS, 4) k_dense_fused(FusedArgs a, int t0, int nsteps) {
@@ -1031,7 +1085,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_dense_fused(FusedArgs a, i
         if (!counter_sync(a.bar, gTarget, nGrid, a.err)) return;
         stamp(s);
         // K: rods; helpers build the motor CSR and reset the step's histograms and lists
-        phase_rods(a, sm, t, &mbar, phase, hTarget);
+        if (!phase_rods(a, sm, t, &mbar, phase, hTarget)) return;
         if (!counter_sync(a.bar, gTarget, nGrid, a.err)) return;
         stamp(s);
     }

@@ -42,7 +42,17 @@ struct FusedArgs {
     int* d_step;
     int barrierExtra;        // test hook: arrivals the barrier waits for beyond gridDim.x
     long long* phaseTimes;   // optional: %globaltimer after each phase barrier, [nsteps][FUSED_PHASES]
+    // supplied-noise mode (sbx_dense_plan_set_noise): planar [nzN][6][n] per store, or null
+    const float *nzFil, *nzMot, *nzBb;
+    int nzT0, nzN;
+    unsigned long long* stats;   // capacity-fallback counters (SBX_FUSED_STATS)
+    int entCap, mCap, mIds;      // staging capacities in use (<= the compiled ones; lowered by a test hook)
+    int cellUse, rowUse;         // fixed row slots in use per cell / per segment row (<= the compiled ones)
 };
+
+// counters of sbx_dense_plan_fused_stats
+enum FusedStat { ST_CELL_LIST = 0, ST_LINK_LIST, ST_MOTOR_LIST, ST_ENT_GLOBAL, ST_MPAY_GLOBAL, ST_MIDS_WALK,
+                 ST_REACH_OVER };
 
 constexpr int FUSED_PHASES = SBX_FUSED_PHASES;
 

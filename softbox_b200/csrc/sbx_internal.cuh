@@ -15,6 +15,10 @@ struct sbx_ctx {
     void* scratch = nullptr;          // grow-only device scratch for scans / unordered scatters
     size_t scratch_bytes = 0;
     int* host_flag = nullptr;         // pinned word for device -> host status flags
+    // mapped pinned word that kernels set when an input breaks a documented range (a CSR key
+    // >= its row count); sbx_ctx_sync reports and clears it. err_dev is its device address.
+    int* err_host = nullptr;
+    int* err_dev = nullptr;
 };
 
 sbx_status fail(sbx_ctx* ctx, sbx_status code, const std::string& msg);
@@ -39,7 +43,8 @@ static inline int blocks(int64_t n, int bs = 256) {
     } while (0)
 
 // ---------------------------------------------------------------- counting sort
-// Stable counting sort of items [0, n) by key (keys < 0 are skipped) into row CSR form:
+// Stable counting sort of items [0, n) by key (keys < 0 are skipped; keys >= nRows are
+// skipped and set *errFlag) into row CSR form:
 // rowCount (atomic histogram, left equal to the row lengths), rowOffsets[0..nRows]
 // (exclusive scan over SCAN_CHUNK tiles with the tile sums in chunkSum, terminator
 // clamped to listCap), rowList (items in ascending index within each row).
@@ -66,6 +71,8 @@ struct CountingSort {
     float* rowPayload = nullptr;
     // the scan's per-tile sums: scan_tile_words(nRows) ints
     int* tileSum = nullptr;
+    // set to 1 when a key is >= nRows (the item is skipped); may be null
+    int* errFlag = nullptr;
 };
 
 // tiles of the counting sort's scan (8 scan chunks each)

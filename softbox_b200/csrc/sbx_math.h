@@ -1,7 +1,7 @@
 // sbx_math.h — scalar arithmetic shared by the CUDA kernels and by host code.
 //
 // Why this file exists: the reference evaluates Math.log / Math.sin / Math.cos /
-// Math.exp in double and rounds the result to float (BrownianForceSystem.java:88-104,
+// Math.exp in double and rounds the result to float (BrownianForceSystem.java:78-92,
 // ChainBendingForceSystem.java:48-84, NucleotideCycleSystem.java:116). To make the
 // device and a CPU checker produce the SAME bits, both sides must evaluate the SAME
 // double-precision function. This header supplies one portable implementation of

@@ -27,7 +27,7 @@ constexpr double PI_D = 3.141592653589793;
 SBX_DEV float fsqrt(float x) { return __fsqrt_rn(x); }
 
 // ---------------------------------------------------------------- Gaussian draws
-// Box-Muller of BrownianForceSystem.java:88-104; g = {gfx,gfy,gfz,gtx,gty,gtz}
+// Box-Muller of BrownianForceSystem.java:78-92; g = {gfx,gfy,gfz,gtx,gty,gtz}
 SBX_DEV void box_muller6(float u1, float u2, float u3, float u4, float u5, float u6, float g[6]) {
     const float TWO_PI_F = 2.0f * 3.14159265f;
     double sn, cs;
@@ -48,7 +48,7 @@ SBX_DEV void box_muller6(float u1, float u2, float u3, float u4, float u5, float
     g[5] = r3 * (float)sn;
 }
 
-// BrownianForceSystem.java:74-86: keyed (slot, step, seed)
+// BrownianForceSystem.java:63-76: keyed (slot, step, seed)
 SBX_DEV void gauss6_wang(int32_t i, int32_t step, int32_t seed, float g[6]) {
     uint32_t base = sbxm::rng_base(i, step, seed);
     float u1 = fmaxf(1.0e-7f, sbxm::unit_from_hash(sbxm::wang_hash(base)));
@@ -75,7 +75,7 @@ SBX_DEV void gauss6_philox(int32_t i, int32_t step, uint64_t seed, float g[6]) {
     box_muller6(u1, u2, u3, u4, u5, u6, g);
 }
 
-// BrownianForceSystem.java:103-112: randF = ((tS*mag)*sqrt(gamma))*g
+// BrownianForceSystem.java:94-104: randF = ((tS*mag)*sqrt(gamma))*g
 SBX_DEV void brownian_amplitudes(const float g[6], float tS, float rS, float mag, const float gT[3],
                                  const float gR[3], float rf[3], float rt[3]) {
     for (int k = 0; k < 3; k++) rf[k] = tS * mag * fsqrt(gT[k]) * g[k];
@@ -87,7 +87,7 @@ struct Pose {
     float c[3], u[3], y[3];
 };
 
-// RigidRodLangevinIntegrationSystem.java:299-356 (and MechanicsFusion.java:134-176).
+// RigidRodLangevinIntegrationSystem.java:53-110 (and MechanicsFusion.java:134-176).
 // Returns the new pose; `dc` receives the FP32 increments dt*v for FP64 accumulation.
 SBX_DEV void integrate_pose(const Pose& p, const float F[3], const float T[3], const float rF[3],
                             const float rT[3], const float gT[3], const float gR[3], float dt, Pose& q,
@@ -136,7 +136,7 @@ SBX_DEV void integrate_pose(const Pose& p, const float F[3], const float T[3], c
     q.y[0] = nyX * nyInv; q.y[1] = nyY * nyInv; q.y[2] = nyZ * nyInv;
 }
 
-// DerivedGeometrySystem.java:402-430: z = unit(u x y), y' = z x u, ends = c -/+ (L/2) u
+// DerivedGeometrySystem.java:43-71: z = unit(u x y), y' = z x u, ends = c -/+ (L/2) u
 SBX_DEV void derive_pose(const float c[3], const float u[3], float y[3], float z[3], float e1[3], float e2[3],
                          float segLength) {
     float ux = u[0], uyc = u[1], uzc = u[2];
@@ -159,7 +159,7 @@ SBX_DEV void derive_pose(const float c[3], const float u[3], float y[3], float z
 }
 
 // ---------------------------------------------------------------- containment
-SBX_DEV double wall_push(double d, double halfDim) {       // ContainmentSystem.java:462-468
+SBX_DEV double wall_push(double d, double halfDim) {       // ContainmentSystem.java:130-136
     double s = (d > 0.0) ? 1.0 : ((d < 0.0) ? -1.0 : 0.0);
     double push = s * halfDim - d;
     double ps = (push > 0.0) ? 1.0 : ((push < 0.0) ? -1.0 : 0.0);
@@ -172,7 +172,7 @@ struct BoxParams {
     bool active;        // cadence gate of this step
 };
 
-// ContainmentSystem.java:398-404 for step `step`
+// ContainmentSystem.java:64-72 for step `step`
 SBX_DEV BoxParams box_params(const float* bp, int32_t step) {
     BoxParams b;
     int32_t checkInt = (int32_t)bp[6];
@@ -185,7 +185,7 @@ SBX_DEV BoxParams box_params(const float* bp, int32_t step) {
     return b;
 }
 
-// ContainmentSystem.java:407-457: += into F/T only on penetration
+// ContainmentSystem.java:75-125: += into F/T only on penetration
 // Returns whether an endpoint touched a wall (F and T are unchanged otherwise).
 SBX_DEV bool confine_one(const BoxParams& bx, const float c[3], const float u[3], float segLength, float bTGx,
                          float F[3], float T[3]) {
@@ -468,7 +468,7 @@ SBX_DEV float bind_arc(float mx, float my, float mz, float e1x, float e1y, float
     return numer / fsqrt(denom);
 }
 
-// SpatialGrid.java:134-140 / BindingDetectionSystem.java:167-172: clamp-binned cell coordinate
+// SpatialGrid.java:67-73 / BindingDetectionSystem.java:167-172: clamp-binned cell coordinate
 SBX_DEV int cell_coord(float x, float xMin, float invCell, int nX) {
     int ix = (int)((x - xMin) * invCell);
     if (ix < 0) ix = 0;

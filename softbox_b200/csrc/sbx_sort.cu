@@ -1,7 +1,7 @@
 // sbx_sort.cu — the stable counting sort behind the spatial grid and every CSR-inverse.
 //
 // Replaces SpatialGrid.gridHistogram/gridScanLocal/gridScanChunks/gridScanAdd/
-// gridScatter (SpatialGrid.java:154-249) and CrossBridgeSystem.csrHistogram/csrScan/
+// gridScatter (SpatialGrid.java:87-182) and CrossBridgeSystem.csrHistogram/csrScan/
 // csrScatter (CrossBridgeSystem.java:190-217), plus their chunk-matrix variants, with:
 //   1. atomic histogram of the keys (integer atomics: the counts are order-free);
 //   2. exclusive scan in SCAN_CHUNK = 512 tiles: per-tile block scan, one-block scan of
@@ -23,11 +23,21 @@ __device__ __forceinline__ int item_count(const int* nDev, int useDevN, int nBou
     return n < nBound ? n : nBound;
 }
 
-__global__ void k_cs_hist(const int* keys, const int* nDev, int useDevN, int nBound, int* rowCount) {
+// a key names a row: keys < 0 are unbound items (skipped, as the reference does); a key at
+// or past the row count would index past the row arrays, so the item is skipped and the
+// caller's error word is set
+__device__ __forceinline__ bool key_ok(int c, int nRows, int* errFlag) {
+    if (c < nRows) return c >= 0;
+    if (errFlag) *(volatile int*)errFlag = 1;
+    return false;
+}
+
+__global__ void k_cs_hist(const int* keys, const int* nDev, int useDevN, int nBound, int nRows, int* rowCount,
+                          int* errFlag) {
     int n = item_count(nDev, useDevN, nBound);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int c = keys[i];
-        if (c >= 0) atomicAdd(&rowCount[c], 1);
+        if (key_ok(c, nRows, errFlag)) atomicAdd(&rowCount[c], 1);
     }
 }
 
@@ -60,7 +70,7 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
     return warp_prefix + x - v;
 }
 
-// SpatialGrid.gridScanLocal (SpatialGrid.java:166-184), one block per 512-row tile
+// SpatialGrid.gridScanLocal (SpatialGrid.java:99-117), one block per 512-row tile
 __global__ void __launch_bounds__(256) k_scan_local(const int* rowCount, int nRows, int* offsets, int* chunkSum) {
     int base = blockIdx.x * SCAN_CHUNK;
     int i0 = base + 2 * threadIdx.x, i1 = i0 + 1;
@@ -73,7 +83,7 @@ __global__ void __launch_bounds__(256) k_scan_local(const int* rowCount, int nRo
     if (threadIdx.x == 0) chunkSum[blockIdx.x] = total;
 }
 
-// SpatialGrid.gridScanChunks (SpatialGrid.java:188-200) as a one-block scan with carry,
+// SpatialGrid.gridScanChunks (SpatialGrid.java:121-133) as a one-block scan with carry,
 // eight consecutive tile sums per thread per pass
 __global__ void __launch_bounds__(1024) k_scan_chunks(int* chunkSum, int numChunks) {
     constexpr int PER = 8;
@@ -101,7 +111,7 @@ __global__ void __launch_bounds__(1024) k_scan_chunks(int* chunkSum, int numChun
 }
 
 // The counting sort's exclusive scan (SpatialGrid.gridScanLocal / gridScanChunks / gridScanAdd,
-// SpatialGrid.java:166-227, with the same outputs) as reduce-then-scan over tiles of
+// SpatialGrid.java:99-160, with the same outputs) as reduce-then-scan over tiles of
 // SCAN_TILE_ROWS = 8 scan chunks: k_tile_reduce writes each tile's sum; k_tile_scan adds the
 // sums of the preceding tiles itself (a strided block reduction, no single-block pass and no
 // inter-block wait), scans its tile through shared memory and writes offsets, the chunk
@@ -172,23 +182,23 @@ __global__ void __launch_bounds__(256) k_tile_scan(int* rowCount, int nRows, int
     }
 }
 
-__global__ void k_cs_scatter(const int* keys, const int* nDev, int useDevN, int nBound, const int* offsets,
-                             int* rowCount, int* tmp) {
+__global__ void k_cs_scatter(const int* keys, const int* nDev, int useDevN, int nBound, int nRows,
+                             const int* offsets, int* rowCount, int* tmp) {
     int n = item_count(nDev, useDevN, nBound);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int c = keys[i];
-        if (c < 0) continue;
+        if (c < 0 || c >= nRows) continue;
         tmp[offsets[c] + atomicAdd(&rowCount[c], 1)] = i;
     }
 }
 
-__global__ void k_cs_rank(const int* keys, const int* nDev, int useDevN, int nBound, const int* offsets,
+__global__ void k_cs_rank(const int* keys, const int* nDev, int useDevN, int nBound, int nRows, const int* offsets,
                           const int* tmp, int* rowList, int listCap, const float* payload, int pStride, int pOff,
                           const int* guard, float* rowPayload) {
     int n = item_count(nDev, useDevN, nBound);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int c = keys[i];
-        if (c < 0) continue;
+        if (c < 0 || c >= nRows) continue;
         int start = offsets[c], end = offsets[c + 1];
         int rank = 0;
         for (int j = start; j < end; j++) rank += tmp[j] < i;
@@ -249,16 +259,17 @@ sbx_status counting_sort(sbx_ctx* ctx, const CountingSort& cs, const char* what)
     if (cudaMemsetAsync(cs.rowCount, 0, sizeof(int) * (size_t)cs.nRows, ctx->stream) != cudaSuccess)
         return fail(ctx, SBX_ECUDA, std::string(what) + ": memset");
     if (cs.nBound > 0)
-        SBX_LAUNCH(ctx, k_cs_hist, itemBlocks, 256, cs.keys, cs.nDev, cs.useDevN, cs.nBound, cs.rowCount);
+        SBX_LAUNCH(ctx, k_cs_hist, itemBlocks, 256, cs.keys, cs.nDev, cs.useDevN, cs.nBound, cs.nRows, cs.rowCount,
+                   cs.errFlag ? cs.errFlag : ctx->err_dev);
     int numTiles = (int)scan_tile_words(cs.nRows);
     SBX_LAUNCH(ctx, k_tile_reduce, numTiles, 256, cs.rowCount, cs.nRows, cs.tileSum);
     SBX_LAUNCH(ctx, k_tile_scan, numTiles, 256, cs.rowCount, cs.nRows, cs.rowOffsets, cs.chunkSum, numChunks,
                cs.tileSum, cs.listCap);
     if (cs.nBound > 0) {
-        SBX_LAUNCH(ctx, k_cs_scatter, itemBlocks, 256, cs.keys, cs.nDev, cs.useDevN, cs.nBound, cs.rowOffsets,
-                   cs.rowCount, cs.tmp);
-        SBX_LAUNCH(ctx, k_cs_rank, itemBlocks, 256, cs.keys, cs.nDev, cs.useDevN, cs.nBound, cs.rowOffsets, cs.tmp,
-                   cs.rowList, cs.listCap, cs.payload, cs.pStride, cs.pOff, cs.guard, cs.rowPayload);
+        SBX_LAUNCH(ctx, k_cs_scatter, itemBlocks, 256, cs.keys, cs.nDev, cs.useDevN, cs.nBound, cs.nRows,
+                   cs.rowOffsets, cs.rowCount, cs.tmp);
+        SBX_LAUNCH(ctx, k_cs_rank, itemBlocks, 256, cs.keys, cs.nDev, cs.useDevN, cs.nBound, cs.nRows, cs.rowOffsets,
+                   cs.tmp, cs.rowList, cs.listCap, cs.payload, cs.pStride, cs.pOff, cs.guard, cs.rowPayload);
     }
     return check_launch(ctx, what);
 }

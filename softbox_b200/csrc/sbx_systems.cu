@@ -3,7 +3,7 @@
 // One entry point per public static method of the reference's System classes; each
 // launches sm_100a kernels on the context stream. Per-slot systems are one thread per
 // slot (the reference's @Parallel loop index). The reference's atomic-free chunked
-// counting sorts (SpatialGrid.java:304-398, CrossBridgeSystem.java:232-298) and its
+// counting sorts (SpatialGrid.java:237-331, CrossBridgeSystem.java:232-298) and its
 // single-thread scans are replaced by an atomic histogram, a two-level parallel scan
 // and a rank pass that restores the stable (ascending index) order, so the CSR arrays
 // come out bit-identical to the reference's serial build.
@@ -36,6 +36,17 @@ extern "C" sbx_status sbx_ctx_create(int device, void* stream, sbx_ctx** out) {
         }
         ctx->own_stream = true;
     }
+    // the input-range error word: mapped pinned host memory, so that a kernel can set it
+    // and sbx_ctx_sync can read it without a copy
+    if (cudaHostAlloc(&ctx->err_host, sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess ||
+        cudaHostGetDevicePointer(&ctx->err_dev, ctx->err_host, 0) != cudaSuccess) {
+        if (ctx->err_host) cudaFreeHost(ctx->err_host);
+        if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        cudaGetLastError();
+        return SBX_ENOMEM;
+    }
+    *ctx->err_host = 0;
     *out = ctx;
     return SBX_OK;
 }
@@ -46,6 +57,7 @@ extern "C" sbx_status sbx_ctx_destroy(sbx_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->host_flag) cudaFreeHost(ctx->host_flag);
+    if (ctx->err_host) cudaFreeHost(ctx->err_host);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SBX_OK;
@@ -70,10 +82,16 @@ extern "C" sbx_status sbx_ctx_sync(sbx_ctx* ctx) {
     if (!ctx) return SBX_EINVAL;
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return fail(ctx, SBX_ECUDA, std::string("sync: ") + cudaGetErrorString(e));
+    if (ctx->err_host && *(volatile int*)ctx->err_host) {
+        *(volatile int*)ctx->err_host = 0;
+        return fail(ctx, SBX_EINVAL, "a CSR key was >= its row count (the item was skipped)");
+    }
     return SBX_OK;
 }
 
 extern "C" int64_t sbx_ctx_launch_count(sbx_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+extern "C" int64_t sbx_ctx_scratch_bytes(sbx_ctx* ctx) { return ctx ? (int64_t)ctx->scratch_bytes : -1; }
 
 sbx_status fail(sbx_ctx* ctx, sbx_status code, const std::string& msg) {
     if (ctx) ctx->err = msg;

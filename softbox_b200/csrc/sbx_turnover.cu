@@ -348,7 +348,7 @@ __global__ void k_pool_births(sbx_actin_pool* pool, const int* rankOffsets, int 
     pool->totalTaken += m;
 }
 
-// ActinPool.put (ActinPool.java:49-52) / take (:42-46) of a scan total, one thread
+// ActinPool.put (ActinPool.java:53-56) / take (:42-46) of a scan total, one thread
 __global__ void k_pool(sbx_actin_pool* pool, const int* offsets, int n, int take) {
     int m = offsets[n];
     if (take) {

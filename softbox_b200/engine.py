@@ -67,6 +67,47 @@ class DenseNetwork:
     def step_unfused(self, t):
         self.ctx("sbx_dense_step_unfused", self.desc, int(t))
 
+    def set_noise(self, fil, mot, bb, t0):
+        """Supplied-noise mode: steps t0 .. t0 + len(fil) - 1 take their Gaussians from the
+        device arrays fil [nsteps][6][nRods], mot [nsteps][6][3 nMotors] and
+        bb [nsteps][6][nBackbones] (float32, contiguous) instead of the Wang-hash draws.
+        None switches the mode off. The arrays are kept alive by the network while in use."""
+        from .abi_types import DenseNoiseDesc, _ptr
+        if fil is None:
+            self._noise = None
+            st = LIB.sbx_dense_plan_set_noise(self.plan, None)
+        else:
+            nsteps = int(fil.shape[0])
+            for x in (mot, bb):
+                if int(x.shape[0]) != nsteps:
+                    raise ValueError("noise arrays cover different step counts")
+            d = DenseNoiseDesc()
+            d.fil, d.mot, d.bb = _ptr(fil, C.c_float), _ptr(mot, C.c_float), _ptr(bb, C.c_float)
+            d.t0, d.nsteps = int(t0), nsteps
+            self._noise = (fil, mot, bb, d)
+            st = LIB.sbx_dense_plan_set_noise(self.plan, C.byref(d))
+        if st != 0:
+            raise SbxError(st, "sbx_dense_plan_set_noise: " + self.ctx.last_error())
+
+    def fused_stats(self, reset=False):
+        """The fused kernel's capacity-fallback counters (SBX_FUSED_STATS): cell overflow
+        lists, link-end lists, motor lists, link payloads read past staging, motor reactions
+        read past staging, motor rows walked by repeated minimum, reach lists past MAX_CAND."""
+        out = (C.c_int64 * 8)()
+        st = LIB.sbx_dense_plan_fused_stats(self.plan, out, 1 if reset else 0)
+        if st != 0:
+            raise SbxError(st, "sbx_dense_plan_fused_stats: " + self.ctx.last_error())
+        keys = ("cell_list", "link_list", "motor_list", "link_payload_global", "motor_payload_global",
+                "motor_row_walk", "reach_over_cap")
+        return {k: int(out[i]) for i, k in enumerate(keys)}
+
+    def test_caps(self, ent=-1, motor=-1, motor_ids=-1, row_slots=-1, cell_slots=-1):
+        """Test hook: lowers the fused kernel's capacities (negative restores)."""
+        st = LIB.sbx_dense_plan_test_caps(self.plan, int(ent), int(motor), int(motor_ids), int(row_slots),
+                                          int(cell_slots))
+        if st != 0:
+            raise SbxError(st, "sbx_dense_plan_test_caps")
+
     def pull(self, store, field=None, sub=None):
         x = self.dev[store]
         if sub is not None:

@@ -1,6 +1,6 @@
 """Timing helpers for the fused dense step.
 
-    python -m softbox_b200.profiling phases [--steps 200]   # per-phase times inside the fused step
+    python -m softbox_b200.profiling phases [--steps 200] [--warm 3000] [--fp64]   # per-phase times
     python -m softbox_b200.profiling onestep                 # two one-step fused launches (for ncu -s 1 -c 1)
 
 `phases` switches on the plan's %globaltimer stamps (sbx_dense_plan_phase_times): the
@@ -22,17 +22,18 @@ PHASES = ["A publish, bin, histograms + lists, crosslinker unbind",   # K(prev) 
           "K rods (+ motor CSR helpers, resets)"]
 
 
-def phase_times(steps=200, fp64_coords=False, cfg=None):
+def phase_times(steps=200, fp64_coords=False, cfg=None, warm=20):
+    """Median per-phase times (us) of `steps` fused steps after `warm` untimed ones."""
     import torch
     net = DenseNetwork(scenes.dense_contractile(cfg or scenes.C1), fp64_coords=fp64_coords)
-    net.run(0, 20)
+    net.run(0, warm, mode="fused")
     torch.cuda.synchronize()
     nph = len(PHASES)
     times = torch.zeros(steps * nph, dtype=torch.int64, device="cuda")
     LIB.sbx_dense_plan_phase_times(net.plan, C.c_void_p(times.data_ptr()))
     s, e = torch.cuda.Event(True), torch.cuda.Event(True)
     s.record()
-    net.run(20, steps)
+    net.run(warm, steps, mode="fused")
     e.record()
     torch.cuda.synchronize()
     net.status()
@@ -61,9 +62,10 @@ def main():
     ap.add_argument("what", choices=["phases", "onestep"])
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--fp64", action="store_true")
+    ap.add_argument("--warm", type=int, default=3000)
     a = ap.parse_args()
     if a.what == "phases":
-        for k, v in phase_times(a.steps, a.fp64).items():
+        for k, v in phase_times(a.steps, a.fp64, warm=a.warm).items():
             print(f"{k:48s} {v:9.2f} {'ms' if k.startswith('ms') else 'us'}")
     else:
         print("status", one_step_launches())

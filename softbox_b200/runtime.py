@@ -113,6 +113,9 @@ class Context:
     def launches(self):
         return LIB.sbx_ctx_launch_count(self.h)
 
+    def scratch_bytes(self):
+        return LIB.sbx_ctx_scratch_bytes(self.h)
+
     def sync(self):
         self("sbx_ctx_sync")
 

@@ -35,7 +35,7 @@ A_PARALLEL, A_ORTHOG, A_TURNING = -0.20, 0.84, -0.662
 BTRANS_COEFF, BROT_COEFF = 1.0, 0.5
 PERSISTENCE_LENGTH = 15.0
 EI = KT * (PERSISTENCE_LENGTH * 1.0e-6)
-# MotorStore.java:45-46, MiniFilamentStore.java:207-211, DimerStore.java:225-228
+# MotorStore.java:45-46, MiniFilamentStore.java:34-38, DimerStore.java:40-43
 ROD_LEN, LEVER_LEN, HEAD_LEN = 0.080, 0.008, 0.020
 ROD_R, LEVER_R, HEAD_R = 0.003, 0.002, 0.010
 BACKBONE_R = 0.005
@@ -537,7 +537,7 @@ def dense_contractile(cfg: DenseConfig = C1):
     store_drag_slots(mb, np.arange(n_mot) * 3, gr)
     store_drag_slots(mb, np.arange(n_mot) * 3 + 1, gl)
     store_drag_slots(mb, np.arange(n_mot) * 3 + 2, gh)
-    # MiniFilamentStore.initBackboneDrag (MiniFilamentStore.java:294-307)
+    # MiniFilamentStore.initBackboneDrag (MiniFilamentStore.java:121-134)
     gbb = rod_drag_si(cfg.backbone_len, BACKBONE_R, cfg.aeta)
     bbb["segLength"][:] = F32(cfg.backbone_len)
     store_drag_slots(bbb, np.arange(n_mini), gbb)

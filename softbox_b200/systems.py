@@ -35,7 +35,7 @@ class DragTensorSystem:                      # DragTensorSystem.java
                bTransDiff, bRotDiff, bbInvDragY)
 
 
-class BrownianForceSystem:                   # BrownianForceSystem.java:183
+class BrownianForceSystem:                   # BrownianForceSystem.java:44
     @staticmethod
     def brownianForce(randForce, randTorque, bTransGam, bRotGam, brownTransScale, brownRotScale, params, counts):
         _ctx()("sbx_brownian_force", _n3(randForce), randForce, randTorque, bTransGam, bRotGam, brownTransScale,
@@ -54,7 +54,7 @@ class BrownianForceSystem:                   # BrownianForceSystem.java:183
                brownTransScale, brownRotScale, params, noise)
 
 
-class RigidRodLangevinIntegrationSystem:     # RigidRodLangevinIntegrationSystem.java:279
+class RigidRodLangevinIntegrationSystem:     # RigidRodLangevinIntegrationSystem.java:33
     @staticmethod
     def integrate(coord, uVec, yVec, forceSum, torqueSum, randForce, randTorque, bTransGam, bRotGam, params,
                   counts=None, coord64=None):
@@ -62,13 +62,13 @@ class RigidRodLangevinIntegrationSystem:     # RigidRodLangevinIntegrationSystem
                bTransGam, bRotGam, params)
 
 
-class DerivedGeometrySystem:                 # DerivedGeometrySystem.java:386
+class DerivedGeometrySystem:                 # DerivedGeometrySystem.java:27
     @staticmethod
     def derive(coord, uVec, yVec, zVec, end1, end2, segLength, counts=None):
         _ctx()("sbx_derive", _n3(coord), coord, uVec, yVec, zVec, end1, end2, segLength)
 
 
-class ContainmentSystem:                     # ContainmentSystem.java:390
+class ContainmentSystem:                     # ContainmentSystem.java:58
     @staticmethod
     def confine(coord, uVec, segLength, bTransGam, forceSum, torqueSum, boxParams, counts):
         _ctx()("sbx_confine", _n3(coord), coord, uVec, segLength, bTransGam, forceSum, torqueSum, boxParams, counts)
@@ -264,7 +264,7 @@ class CrosslinkerSystem:                     # CrosslinkerSystem.java
         _ctx()("sbx_xlink_unbind", _n3(filCoord), filUVec, filEnd1, linkFilA.numel(), linkFilA, linkFilB, loc1, loc2,
                linkState, strainHist, strainPlace, offParams, counts)
 
-    # ---- formation (CrosslinkerSystem.java:417-752) and the free-list allocator (:297-345)
+    # ---- formation (CrosslinkerSystem.java:405-756) and the free-list allocator (:297-345)
     FORM_MAXC = 256
 
     @staticmethod

@@ -79,7 +79,7 @@ class TurnoverConfig:
 
     @property
     def check_int(self):
-        """biochemCheckInt = max(1, round(biochemDeltaT / dt)) (GrowthStore.java:51)."""
+        """biochemCheckInt = max(1, round(biochemDeltaT / dt)) (GrowthStore.java:47)."""
         return max(1, int(math.floor(BIOCHEM_DT / self.dt + 0.5)))
 
     def fires_at(self, step):

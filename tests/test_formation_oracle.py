@@ -1,7 +1,7 @@
 """Crosslinker formation in the oracle: the reference's own relational gates.
 
 FORMATION == BRUTE (the grid candidate query equals the all-pairs enumeration,
-CrosslinkerSystem.java:417-452 vs :474-595), the allocator's slot stability (an ACTIVE
+CrosslinkerSystem.java:405-427 vs :474-595), the allocator's slot stability (an ACTIVE
 slot is never overwritten; CrosslinkerHarness.java:799-836), one new link per segment
 per step, and saturation/spacing of the admitted links.
 """

@@ -57,6 +57,27 @@ def test_dense_steps_bitwise(orc_dm, warm_scene, mode):
     assert len(names) > 80
 
 
+@pytest.mark.parametrize("mode", ["unfused", "graph", "fused"])
+def test_dense_supplied_noise_bitwise(orc, warm_scene, mode):
+    """Supplied-noise mode of the dense step (every path) against the libm oracle fed the
+    same Gaussian array: the same bits."""
+    from softbox_b200.engine import DenseNetwork
+    ref = copy.deepcopy(warm_scene)
+    net = DenseNetwork(copy.deepcopy(warm_scene))
+    rng = np.random.default_rng(21)
+    nsteps = 40
+    nf = rng.standard_normal((nsteps, 6, ref["fil"]["body"]["n"]), dtype=np.float32)
+    nm = rng.standard_normal((nsteps, 6, ref["mot"]["body"]["n"]), dtype=np.float32)
+    nb = rng.standard_normal((nsteps, 6, ref["mini"]["backbone"]["n"]), dtype=np.float32)
+    net.set_noise(dev(nf), dev(nm), dev(nb), 300)
+    net.run(300, nsteps, mode=mode)
+    assert net.status() == 0
+    torch.cuda.synchronize()
+    orc.dense_run_supplied(D.dense_desc(ref), 300, nsteps, nf, nm, nb)
+    names = compare_scenes({k: v for k, v in ref.items() if k != "cfg"}, host(net.dev))
+    assert len(names) > 80
+
+
 @pytest.mark.parametrize("mode", ["graph", "fused"])
 def test_dense_fp64_coords(orc_dm, warm_scene, mode):
     from softbox_b200.engine import DenseNetwork
@@ -258,6 +279,39 @@ def test_csr_build_matches_serial_and_chunked(orc_dm, warm_scene, which):
     d = dev({"k": keys, "c": np.zeros(rows, np.int32), "o": np.zeros(rows + 1, np.int32),
              "l": np.full(max(n, 1), -1, np.int32)})
     CrossBridgeSystem.csrBuild(d["k"], rows, d["c"], d["o"], d["l"])
+    h = host(d)
+    assert_same(off, h["o"], "offsets")
+    assert_same(lst, h["l"], "list")
+    assert_same(cnt, h["c"], "rowCount")
+
+
+@pytest.mark.parametrize("entry", ["sbx_csr_build", "sbx_csr_build_payload"])
+def test_csr_build_out_of_range_key_is_skipped_and_reported(orc_dm, warm_scene, entry):
+    """A key >= the row count (the reference's Java would throw) touches no row: the item
+    is skipped, the next sync reports SBX_EINVAL once, and offsets/list/counts equal the
+    oracle's build of the same keys with that item unbound."""
+    from softbox_b200.runtime import default_context
+    sc = _s(warm_scene)
+    rows = sc["fil"]["body"]["n"]
+    keys = sc["mot"]["boundSeg"].copy()
+    keys[3] = rows
+    keys[-1] = rows + 1000
+    n = keys.size
+    fixed = np.where(keys >= rows, -1, keys).astype(np.int32)
+    cnt, off, lst = np.zeros(rows, np.int32), np.zeros(rows + 1, np.int32), np.full(n, -1, np.int32)
+    orc_dm.csr_histogram(fixed, n, rows, cnt)
+    orc_dm.csr_scan(rows, cnt, off)
+    orc_dm.csr_scatter(fixed, n, off, cnt, lst)
+    d = dev({"k": keys, "c": np.zeros(rows, np.int32), "o": np.zeros(rows + 1, np.int32),
+             "l": np.full(n, -1, np.int32), "p": np.ones(13 * n, np.float32), "rp": np.zeros(6 * n, np.float32)})
+    ctx = default_context()
+    ctx.sync()
+    args = [d["k"], n, rows, d["c"], d["o"], d["l"]]
+    if entry == "sbx_csr_build_payload":
+        args += [d["p"], 13, 6, None, d["rp"]]
+    assert ctx.raw(entry, *args) == 0
+    assert ctx.raw("sbx_ctx_sync") == -1
+    assert ctx.raw("sbx_ctx_sync") == 0
     h = host(d)
     assert_same(off, h["o"], "offsets")
     assert_same(lst, h["l"], "list")

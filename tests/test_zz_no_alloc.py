@@ -36,7 +36,7 @@ def _build(ctx, name, keys, rows):
     return cnt.cpu().numpy(), off.cpu().numpy(), lst.cpu().numpy()
 
 
-@pytest.mark.parametrize("n,rows", [(6400, 20000), (200_000, 4096), (MAX_ITEMS, 1 << 16)])
+@pytest.mark.parametrize("n,rows", [(6400, 20000), (200_000, 4096), (MAX_ITEMS, 1 << 16), (MAX_ITEMS, MAX_ROWS)])
 def test_noalloc_matches_csr_build_twice(n, rows):
     ref_ctx, ctx = Context(0), Context(0)
     try:
@@ -62,12 +62,17 @@ def test_noalloc_takes_no_device_memory():
         off = torch.zeros(10_001, dtype=torch.int32, device="cuda")
         lst = torch.zeros(keys.size, dtype=torch.int32, device="cuda")
         torch.cuda.synchronize()
+        scratch0 = ctx.scratch_bytes()
         free0, _ = torch.cuda.mem_get_info()
         for _ in range(3):
             ctx("sbx_csr_build_noalloc", d_keys.data_ptr(), keys.size, 10_000, cnt.data_ptr(), off.data_ptr(),
                 lst.data_ptr())
         ctx.sync()
         free1, _ = torch.cuda.mem_get_info()
+        # the context's own scratch did not grow (the direct check) ...
+        assert ctx.scratch_bytes() == scratch0
+        # ... and the device's free memory did not move (a secondary check: another process
+        # on the same GPU could move it)
         assert free1 == free0
     finally:
         ctx.close()
@@ -88,5 +93,37 @@ def test_noalloc_rejects_sizes_beyond_the_static_scratch():
         got = _build(ctx, "sbx_csr_build_noalloc", keys, 64)
         for w, g in zip(want, got):
             assert np.array_equal(w, g)
+    finally:
+        ctx.close()
+
+
+def test_noalloc_out_of_range_key_is_skipped_and_reported():
+    """A key at or past the row count indexes no row: the item is skipped (the static
+    scratch is not written past its rows), the next sync reports SBX_EINVAL, and the
+    outputs equal the build of the same keys with that item unbound."""
+    ctx = Context(0)
+    try:
+        rows = 4096
+        keys = _keys(11, 100_000, rows)
+        bad = keys.copy()
+        bad[777] = rows          # one past the last row
+        bad[5000] = rows + 12345
+        d_keys = torch.from_numpy(bad).cuda()
+        cnt = torch.zeros(rows, dtype=torch.int32, device="cuda")
+        off = torch.zeros(rows + 1, dtype=torch.int32, device="cuda")
+        lst = torch.full((bad.size,), -1, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        assert ctx.raw("sbx_csr_build_noalloc", d_keys.data_ptr(), bad.size, rows, cnt.data_ptr(), off.data_ptr(),
+                       lst.data_ptr()) == 0
+        assert ctx.raw("sbx_ctx_sync") == SBX_EINVAL
+        assert "row count" in ctx.last_error()
+        assert ctx.raw("sbx_ctx_sync") == 0          # reported once
+        fixed = bad.copy()
+        fixed[bad >= rows] = -1
+        want = _build(ctx, "sbx_csr_build", fixed, rows)
+        assert np.array_equal(want[0], cnt.cpu().numpy())
+        assert np.array_equal(want[1], off.cpu().numpy())
+        n_valid = int(want[1][-1])
+        assert np.array_equal(want[2][:n_valid], lst.cpu().numpy()[:n_valid])
     finally:
         ctx.close()
