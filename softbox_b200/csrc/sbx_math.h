@@ -11,8 +11,10 @@
 //     the Elementary Functions", 1980): x = k*(pi/2) + r with pi/2 split into three
 //     doubles, and x = k*ln2 + r with ln2 split into two doubles. The split constants
 //     are derived by gen_math_constants.py (decimal arithmetic, 60 digits).
-//   * Taylor polynomials on the reduced range (coefficients are 1/n! and 1/(2k+1)),
-//     evaluated by Horner's rule.
+//   * minimax polynomials on the reduced range, evaluated by Horner's rule; their
+//     coefficients come from the Remez exchange algorithm (gen_math_polys.py, 60-digit
+//     arithmetic), which reaches double accuracy with 6 to 11 terms where the
+//     truncated Taylor series of the same functions needs 10 to 14.
 //   * log(m) = 2*atanh(f/(2+f)), f = m - 1, m in [sqrt(1/2), sqrt(2)).
 //
 // Accuracy (checked in tests/test_math.py against libm and, on the GPU, against
@@ -42,6 +44,42 @@ namespace sbxm {
 #define SBXM_INV_LN2   0x1.71547652b82fep+0
 #define SBXM_SQRT2     0x1.6a09e667f3bcdp+0
 
+// ---- minimax coefficients (gen_math_polys.py) ----
+// SBXM_SIN: weighted minimax error 2^-58.0
+#define SBXM_SIN0 -0x1.5555555555549p-3
+#define SBXM_SIN1 0x1.111111110f87ap-7
+#define SBXM_SIN2 -0x1.a01a019c1198fp-13
+#define SBXM_SIN3 0x1.71de3577b6439p-19
+#define SBXM_SIN4 -0x1.ae5e663a4e7efp-26
+#define SBXM_SIN5 0x1.5d9300e9b8b15p-33
+// SBXM_COS: weighted minimax error 2^-64.2
+#define SBXM_COS0 0x1.555555555554cp-5
+#define SBXM_COS1 -0x1.6c16c16c1517ep-10
+#define SBXM_COS2 0x1.a01a019cb1bd6p-16
+#define SBXM_COS3 -0x1.27e4f809f068ep-22
+#define SBXM_COS4 0x1.1ee9ebe90849ap-29
+#define SBXM_COS5 -0x1.8fae9c63fbf36p-37
+// SBXM_LOG: weighted minimax error 2^-59.5
+#define SBXM_LOG0 0x1.5555555555592p-2
+#define SBXM_LOG1 0x1.999999997fd37p-3
+#define SBXM_LOG2 0x1.24924941f8cffp-3
+#define SBXM_LOG3 0x1.c71c5202b41b2p-4
+#define SBXM_LOG4 0x1.7466405ba762dp-4
+#define SBXM_LOG5 0x1.39a1933c05c0fp-4
+#define SBXM_LOG6 0x1.2f070557504cdp-4
+// SBXM_EXP: weighted minimax error 2^-59.3
+#define SBXM_EXP0 0x1.0000000000000p-1
+#define SBXM_EXP1 0x1.5555555555557p-3
+#define SBXM_EXP2 0x1.5555555555558p-5
+#define SBXM_EXP3 0x1.11111111100d8p-7
+#define SBXM_EXP4 0x1.6c16c16c151f7p-10
+#define SBXM_EXP5 0x1.a01a01abe9f2ap-13
+#define SBXM_EXP6 0x1.a01a01acfce36p-16
+#define SBXM_EXP7 0x1.71de022b7114ap-19
+#define SBXM_EXP8 0x1.27e4ccc8e655ep-22
+#define SBXM_EXP9 0x1.af4df62e8c93ep-26
+#define SBXM_EXP10 0x1.1f8b54dcb8058p-29
+
 SBX_HD uint64_t dbits(double x) { uint64_t u; memcpy(&u, &x, 8); return u; }
 SBX_HD double bitsd(uint64_t u) { double x; memcpy(&x, &u, 8); return x; }
 
@@ -51,35 +89,27 @@ SBX_HD int nearest_int(double x) {
     return (int)t;
 }
 
-// sin and cos of a reduced argument |r| <= ~pi/4 (Taylor, Horner in r^2)
+// sin and cos of a reduced argument |r| <= ~pi/4 (minimax in r^2, Horner)
 SBX_HD double sin_poly(double r) {
     double r2 = r * r;
-    double p = 1.0 / 51090942171709440000.0;      //  1/21!
-    p = p * r2 - 1.0 / 121645100408832000.0;      // -1/19!
-    p = p * r2 + 1.0 / 355687428096000.0;         //  1/17!
-    p = p * r2 - 1.0 / 1307674368000.0;           // -1/15!
-    p = p * r2 + 1.0 / 6227020800.0;              //  1/13!
-    p = p * r2 - 1.0 / 39916800.0;                // -1/11!
-    p = p * r2 + 1.0 / 362880.0;                  //  1/9!
-    p = p * r2 - 1.0 / 5040.0;                    // -1/7!
-    p = p * r2 + 1.0 / 120.0;                     //  1/5!
-    p = p * r2 - 1.0 / 6.0;                       // -1/3!
+    double p = SBXM_SIN5;
+    p = p * r2 + SBXM_SIN4;
+    p = p * r2 + SBXM_SIN3;
+    p = p * r2 + SBXM_SIN2;
+    p = p * r2 + SBXM_SIN1;
+    p = p * r2 + SBXM_SIN0;                       // ~ -1/3!
     return r + r * (r2 * p);
 }
 
 SBX_HD double cos_poly(double r) {
     double r2 = r * r;
-    double p = -1.0 / 1124000727777607680000.0;   // -1/22!
-    p = p * r2 + 1.0 / 2432902008176640000.0;     //  1/20!
-    p = p * r2 - 1.0 / 6402373705728000.0;        // -1/18!
-    p = p * r2 + 1.0 / 20922789888000.0;          //  1/16!
-    p = p * r2 - 1.0 / 87178291200.0;             // -1/14!
-    p = p * r2 + 1.0 / 479001600.0;               //  1/12!
-    p = p * r2 - 1.0 / 3628800.0;                 // -1/10!
-    p = p * r2 + 1.0 / 40320.0;                   //  1/8!
-    p = p * r2 - 1.0 / 720.0;                     // -1/6!
-    p = p * r2 + 1.0 / 24.0;                      //  1/4!
-    p = p * r2 - 0.5;                             // -1/2!
+    double p = SBXM_COS5;
+    p = p * r2 + SBXM_COS4;
+    p = p * r2 + SBXM_COS3;
+    p = p * r2 + SBXM_COS2;
+    p = p * r2 + SBXM_COS1;
+    p = p * r2 + SBXM_COS0;                       // ~ 1/4!
+    p = p * r2 - 0.5;
     return 1.0 + r2 * p;
 }
 
@@ -154,17 +184,13 @@ SBX_HD double log(double x) {
     double f = m - 1.0;
     double s = f / (2.0 + f);
     double s2 = s * s;
-    double q = 1.0 / 23.0;
-    q = q * s2 + 1.0 / 21.0;
-    q = q * s2 + 1.0 / 19.0;
-    q = q * s2 + 1.0 / 17.0;
-    q = q * s2 + 1.0 / 15.0;
-    q = q * s2 + 1.0 / 13.0;
-    q = q * s2 + 1.0 / 11.0;
-    q = q * s2 + 1.0 / 9.0;
-    q = q * s2 + 1.0 / 7.0;
-    q = q * s2 + 1.0 / 5.0;
-    q = q * s2 + 1.0 / 3.0;
+    double q = SBXM_LOG6;
+    q = q * s2 + SBXM_LOG5;
+    q = q * s2 + SBXM_LOG4;
+    q = q * s2 + SBXM_LOG3;
+    q = q * s2 + SBXM_LOG2;
+    q = q * s2 + SBXM_LOG1;
+    q = q * s2 + SBXM_LOG0;                       // ~ 1/3
     double two_s = 2.0 * s;
     double ed = (double)e;
     double lo = ed * SBXM_LN2_LO + two_s * (s2 * q);
@@ -180,20 +206,17 @@ SBX_HD double exp(double x) {
     double kd = (double)k;
     double r = x - kd * SBXM_LN2_HI;
     r = r - kd * SBXM_LN2_LO;
-    double p = 1.0 / 1307674368000.0;               // 1/15!
-    p = p * r + 1.0 / 87178291200.0;                // 1/14!
-    p = p * r + 1.0 / 6227020800.0;                 // 1/13!
-    p = p * r + 1.0 / 479001600.0;                  // 1/12!
-    p = p * r + 1.0 / 39916800.0;                   // 1/11!
-    p = p * r + 1.0 / 3628800.0;                    // 1/10!
-    p = p * r + 1.0 / 362880.0;                     // 1/9!
-    p = p * r + 1.0 / 40320.0;                      // 1/8!
-    p = p * r + 1.0 / 5040.0;                       // 1/7!
-    p = p * r + 1.0 / 720.0;                        // 1/6!
-    p = p * r + 1.0 / 120.0;                        // 1/5!
-    p = p * r + 1.0 / 24.0;                         // 1/4!
-    p = p * r + 1.0 / 6.0;                          // 1/3!
-    p = p * r + 0.5;                                // 1/2!
+    double p = SBXM_EXP10;
+    p = p * r + SBXM_EXP9;
+    p = p * r + SBXM_EXP8;
+    p = p * r + SBXM_EXP7;
+    p = p * r + SBXM_EXP6;
+    p = p * r + SBXM_EXP5;
+    p = p * r + SBXM_EXP4;
+    p = p * r + SBXM_EXP3;
+    p = p * r + SBXM_EXP2;
+    p = p * r + SBXM_EXP1;
+    p = p * r + SBXM_EXP0;                        // ~ 1/2
     double er = 1.0 + (r + r * (r * p));
     // scale by 2^k in two halves so that k down to -1074 stays representable
     int k1 = k / 2, k2 = k - k1;

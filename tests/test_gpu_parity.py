@@ -550,7 +550,7 @@ def test_drag_kernels_match_oracle(orc_dm):
 def test_thermostat_equipartition():
     """ThermostatDiag Cut 3 (ThermostatDiag.java:41-58): a single rod held to +z by the
     fracMove torsional restore sits at the discrete AR(1) equipartition
-    <theta^2> = 4 kT dt / (gamma c (2 - c)), within 3 %."""
+    <theta^2> = 4 kT dt / (gamma c (2 - c)), within 2 % (measured 0.992)."""
     from softbox_b200 import systems as S
     reps, dt, coeff = 2000, 1.0e-5, 0.4
     nB = 3 * reps
@@ -592,7 +592,7 @@ def test_thermostat_equipartition():
     meas = s2 / nsamp
     bRGy = float(b["bRotGam"][nB + 0])
     pred = 4.0 * scenes.KT * dt / (bRGy * coeff * (2.0 - coeff))
-    assert abs(meas / pred - 1.0) < 0.03, (meas, pred)
+    assert abs(meas / pred - 1.0) < 0.02, (meas, pred)
 
 
 def test_fused_equals_graph_on_full_network():
