@@ -594,6 +594,16 @@ sbx_status sbx_mini_backbone_gather(sbx_ctx* ctx, int32_t nBb, const int32_t* bb
                                     const int32_t* bbDimerList, const float* miniData, float* bbForceSum,
                                     float* bbTorqueSum);
 
+/* DeflectionSupport.seedAccumulators (DeflectionSupport.java:24-33): forceSum = counts[3] *
+ * extForce, torqueSum = 0 (the deflection benchmark's constant load, switched by counts[3]). */
+sbx_status sbx_deflection_seed_accumulators(sbx_ctx* ctx, int32_t n, float* forceSum, float* torqueSum,
+                                            const float* extForce, const int32_t* counts);
+/* DeflectionSupport.pinEndpoints (DeflectionSupport.java:40-58): after integration, pin p moves
+ * segment pinSeg[p] so its end pinEnd[p] (1 = end1, 2 = end2) lands on pinAnchor[3p..3p+2]. */
+sbx_status sbx_deflection_pin_endpoints(sbx_ctx* ctx, int32_t n, float* coord, const float* uVec,
+                                        const float* segLength, int32_t nPins, const int32_t* pinSeg,
+                                        const int32_t* pinEnd, const float* pinAnchor);
+
 /* ThermostatDiag.torsionalRestore (ThermostatDiag.java:127-145): diagnostic restore of
  * every motor rod's uVec toward +z, used by the equipartition check. */
 sbx_status sbx_thermostat_torsional_restore(sbx_ctx* ctx, int32_t nMotors, const float* uVec,

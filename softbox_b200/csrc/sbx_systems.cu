@@ -1389,3 +1389,53 @@ extern "C" sbx_status sbx_thermostat_torsional_restore(sbx_ctx* ctx, int32_t nMo
     SBX_LAUNCH(ctx, k_torsional_restore, blocks(nMotors), 256, nMotors, uVec, bRG, T, coeff, dt);
     return check_launch(ctx, "sbx_thermostat_torsional_restore");
 }
+
+// ============================================================================ deflection support
+// DeflectionSupport.seedAccumulators (DeflectionSupport.java:24-33): forceSum = load * extForce
+// with load = (float)counts[3], torqueSum = 0
+__global__ void k_seed_accumulators(int n, float* F, float* T, const float* ext, const int* counts) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float load = (float)counts[3];
+    for (int k = 0; k < 3; k++) {
+        F[k * n + i] = load * ext[k * n + i];
+        T[k * n + i] = 0.f;
+    }
+}
+
+extern "C" sbx_status sbx_deflection_seed_accumulators(sbx_ctx* ctx, int32_t n, float* forceSum, float* torqueSum,
+                                                       const float* extForce, const int32_t* counts) {
+    SBX_REQUIRE(ctx && n >= 0 && (n == 0 || (forceSum && torqueSum && extForce && counts)));
+    if (n == 0) return SBX_OK;
+    SBX_LAUNCH(ctx, k_seed_accumulators, blocks(n), 256, n, forceSum, torqueSum, extForce, counts);
+    return check_launch(ctx, "sbx_deflection_seed_accumulators");
+}
+
+// DeflectionSupport.pinEndpoints (DeflectionSupport.java:40-58): pin p translates segment
+// pinSeg[p] so that its end pinEnd[p] (1 = end1, else end2) sits on pinAnchor[3p..3p+2]
+__global__ void k_pin_endpoints(int n, float* coord, const float* uVec, const float* segLength, int P,
+                                const int* pinSeg, const int* pinEnd, const float* anchor) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    int s = pinSeg[p];
+    if (s < 0 || s >= n) return;
+    float c[3] = {coord[s], coord[n + s], coord[2 * n + s]};
+    float u[3] = {uVec[s], uVec[n + s], uVec[2 * n + s]};
+    float half = 0.5f * segLength[s];
+    float sgn = pinEnd[p] == 1 ? -1.f : 1.f;
+    for (int k = 0; k < 3; k++) {
+        float e = sgn < 0.f ? c[k] - half * u[k] : c[k] + half * u[k];
+        float d = anchor[3 * p + k] - e;
+        coord[k * n + s] = c[k] + d;
+    }
+}
+
+extern "C" sbx_status sbx_deflection_pin_endpoints(sbx_ctx* ctx, int32_t n, float* coord, const float* uVec,
+                                                   const float* segLength, int32_t nPins, const int32_t* pinSeg,
+                                                   const int32_t* pinEnd, const float* pinAnchor) {
+    SBX_REQUIRE(ctx && n >= 0 && nPins >= 0 && (nPins == 0 || (coord && uVec && segLength && pinSeg && pinEnd &&
+                                                               pinAnchor)));
+    if (nPins == 0) return SBX_OK;
+    SBX_LAUNCH(ctx, k_pin_endpoints, blocks(nPins), 256, n, coord, uVec, segLength, nPins, pinSeg, pinEnd, pinAnchor);
+    return check_launch(ctx, "sbx_deflection_pin_endpoints");
+}

@@ -545,6 +545,17 @@ class MiniFilamentSystem:                    # MiniFilamentSystem.java
                bbForceSum, bbTorqueSum)
 
 
+class DeflectionSupport:                     # DeflectionSupport.java:24-58
+    @staticmethod
+    def seedAccumulators(forceSum, torqueSum, extForce, counts):
+        _ctx()("sbx_deflection_seed_accumulators", _n3(forceSum), forceSum, torqueSum, extForce, counts)
+
+    @staticmethod
+    def pinEndpoints(coord, uVec, segLength, pinSeg, pinEnd, pinAnchor, counts=None):
+        _ctx()("sbx_deflection_pin_endpoints", _n3(coord), coord, uVec, segLength, pinSeg.numel(), pinSeg, pinEnd,
+               pinAnchor)
+
+
 class ThermostatDiag:                        # ThermostatDiag.java:127
     @staticmethod
     def torsionalRestore(uVec, bRotGam, torqueSum, nMotors, coeff, dt):

@@ -86,3 +86,30 @@ def test_fused_reach_list_past_cap_reports_overflow(orc_dm):
         assert_same(ref[s][f], got[s][f], f"{s}.{f}")
     assert_same(ref["fil"]["body"]["coord"], got["fil"]["body"]["coord"], "fil.coord")
     assert net.fused_stats()["reach_over_cap"] > 0
+
+
+def test_deflection_support_matches_oracle(orc_dm):
+    """DeflectionSupport.seedAccumulators / pinEndpoints (the deflection benchmark's load and
+    pins) on the GPU equal the oracle bit for bit, load on and off."""
+    from softbox_b200 import device as D, scenes
+    from softbox_b200.systems import DeflectionSupport
+    rng = np.random.default_rng(5)
+    n, P = 257, 9
+    host = {"F": rng.standard_normal(3 * n).astype(np.float32), "T": rng.standard_normal(3 * n).astype(np.float32),
+            "ext": rng.standard_normal(3 * n).astype(np.float32) * 1e-12, "c": np.array([n, 3, 0, 1], np.int32),
+            "coord": rng.standard_normal(3 * n).astype(np.float32), "seg": rng.uniform(0.05, 0.2, n).astype(np.float32),
+            "pinSeg": rng.choice(n, P, replace=False).astype(np.int32), "pinEnd": rng.integers(1, 3, P).astype(np.int32),
+            "anchor": rng.standard_normal(3 * P).astype(np.float32)}
+    u = rng.standard_normal((3, n))
+    host["u"] = (u / np.linalg.norm(u, axis=0)).reshape(-1).astype(np.float32)
+    for load in (1, 0):
+        host["c"][3] = load
+        ref = copy.deepcopy(host)
+        d = D.to_device(host)
+        DeflectionSupport.seedAccumulators(d["F"], d["T"], d["ext"], d["c"])
+        DeflectionSupport.pinEndpoints(d["coord"], d["u"], d["seg"], d["pinSeg"], d["pinEnd"], d["anchor"])
+        orc_dm.seed_accumulators(n, ref["F"], ref["T"], ref["ext"], ref["c"])
+        orc_dm.pin_endpoints(n, ref["coord"], ref["u"], ref["seg"], P, ref["pinSeg"], ref["pinEnd"], ref["anchor"])
+        h = D.to_host(d)
+        for k in ("F", "T", "coord"):
+            assert_same(ref[k], h[k], k)
