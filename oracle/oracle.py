@@ -1,8 +1,10 @@
 """ctypes wrapper of the CPU oracle (test infrastructure only).
 
-Loads oracle/_build/liboracle.so (libm transcendentals, the reference's platform math)
-or liboracle_dm.so (the portable double functions the CUDA kernels evaluate). Only the
-tests, the smoke check and bench.py's CPU-baseline leg use this module.
+Loads oracle/_build/liboracle.so (libm transcendentals, the reference's platform math),
+liboracle_dm.so (the portable double functions the CUDA kernels evaluate) or
+liboracle_f64.so (liboracle_dm.so with every float evaluated as double: its array
+arguments are float64 where the others take float32). Only the tests, the smoke check and
+bench.py's CPU-baseline leg use this module.
 """
 import ctypes as C
 import os
@@ -87,13 +89,14 @@ class Oracle:
     """One loaded oracle library. Array arguments may be numpy arrays (passed by
     pointer), None (NULL) or ctypes structures (passed by reference)."""
 
-    def __init__(self, devmath=False):
-        name = "liboracle_dm.so" if devmath else "liboracle.so"
+    def __init__(self, devmath=False, fp64=False):
+        name = "liboracle_f64.so" if fp64 else ("liboracle_dm.so" if devmath else "liboracle.so")
         path = os.path.join(_BUILD, name)
         if not os.path.exists(path):
             build()
         self.lib = C.CDLL(path)
-        self.devmath = devmath
+        self.devmath = devmath or fp64
+        self.fp64 = fp64
         for fn, sig in _SIGS.items():
             f = getattr(self.lib, fn)
             f.argtypes = [_CT[c] for c in sig]
@@ -127,7 +130,20 @@ class Oracle:
 _cache = {}
 
 
-def get(devmath=False):
-    if devmath not in _cache:
-        _cache[devmath] = Oracle(devmath)
-    return _cache[devmath]
+def get(devmath=False, fp64=False):
+    key = (devmath, fp64)
+    if key not in _cache:
+        _cache[key] = Oracle(devmath, fp64)
+    return _cache[key]
+
+
+def to_fp64(obj):
+    """A copy of a (nested) host scene for the FP64 build: float32 arrays become float64,
+    the separate FP64 centres are dropped (the centres themselves are double there)."""
+    if isinstance(obj, dict):
+        return {k: to_fp64(v) for k, v in obj.items() if k != "coord64"}
+    if isinstance(obj, np.ndarray) and obj.dtype == np.float32:
+        return obj.astype(np.float64)
+    if isinstance(obj, np.ndarray):
+        return obj.copy()
+    return obj

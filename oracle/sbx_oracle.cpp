@@ -192,11 +192,11 @@ inline void gauss6_wang(i32 i, i32 step, i32 seed, float g[6]) {
     uint32_t h4 = sbxm::wang_hash(base ^ 0xc2b2ae35u);
     uint32_t h5 = sbxm::wang_hash(base ^ 0x517cc1b7u);
     uint32_t h6 = sbxm::wang_hash(base ^ 0x1f0a7ed5u);
-    float u1 = std::max(1.0e-7f, sbxm::unit_from_hash(h1));
+    float u1 = std::max((float)1.0e-7f, sbxm::unit_from_hash(h1));
     float u2 = sbxm::unit_from_hash(h2);
-    float u3 = std::max(1.0e-7f, sbxm::unit_from_hash(h3));
+    float u3 = std::max((float)1.0e-7f, sbxm::unit_from_hash(h3));
     float u4 = sbxm::unit_from_hash(h4);
-    float u5 = std::max(1.0e-7f, sbxm::unit_from_hash(h5));
+    float u5 = std::max((float)1.0e-7f, sbxm::unit_from_hash(h5));
     float u6 = sbxm::unit_from_hash(h6);
     box_muller6(u1, u2, u3, u4, u5, u6, g);
 }
@@ -207,11 +207,11 @@ inline void gauss6_philox(i32 i, i32 step, uint64_t seed, float g[6]) {
     uint32_t c1[4] = {(uint32_t)i, (uint32_t)step, 1u, 0x53425830u};
     sbxm::philox4x32_10(c0, (uint32_t)seed, (uint32_t)(seed >> 32));
     sbxm::philox4x32_10(c1, (uint32_t)seed, (uint32_t)(seed >> 32));
-    float u1 = std::max(1.0e-7f, sbxm::unit_from_hash(c0[0]));
+    float u1 = std::max((float)1.0e-7f, sbxm::unit_from_hash(c0[0]));
     float u2 = sbxm::unit_from_hash(c0[1]);
-    float u3 = std::max(1.0e-7f, sbxm::unit_from_hash(c0[2]));
+    float u3 = std::max((float)1.0e-7f, sbxm::unit_from_hash(c0[2]));
     float u4 = sbxm::unit_from_hash(c0[3]);
-    float u5 = std::max(1.0e-7f, sbxm::unit_from_hash(c1[0]));
+    float u5 = std::max((float)1.0e-7f, sbxm::unit_from_hash(c1[0]));
     float u6 = sbxm::unit_from_hash(c1[1]);
     box_muller6(u1, u2, u3, u4, u5, u6, g);
 }
