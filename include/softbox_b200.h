@@ -728,7 +728,7 @@ int32_t sbx_dense_plan_fused_grid(sbx_dense_plan* plan);
 /* Phase timing of the fused path: when dev_times (device int64 array of
  * nsteps*SBX_FUSED_PHASES) is set, each run writes the %globaltimer value (ns) after every
  * phase barrier of every step; NULL switches it off. */
-#define SBX_FUSED_PHASES 6
+#define SBX_FUSED_PHASES 7
 sbx_status sbx_dense_plan_phase_times(sbx_dense_plan* plan, int64_t* dev_times);
 /* Test hook for failure detection: the fused kernel's grid barrier waits for `extra`
  * arrivals that never come, so its bounded wait runs out and the run reports

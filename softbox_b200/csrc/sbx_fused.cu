@@ -1,6 +1,6 @@
 // sbx_fused.cu — the dense contractile step as ONE persistent cooperative kernel.
 //
-// A launch advances nsteps steps. Within a step, six phases are separated by a grid-wide
+// A launch advances nsteps steps. Within a step, seven phases are separated by a grid-wide
 // barrier (bounded spin: a barrier that does not complete within the limit raises
 // error bit 0 and every CTA returns, so a fault cannot hang the device):
 //
@@ -14,12 +14,13 @@
 //      Brownian forces of the motor sub-bodies and backbones
 //   E  stable placement by list rank -> gridCellContents, segIdxA, segIdxB and the
 //      segment endpoints in cell order (float4) for the reach walk
-//   F  one CTA per minifilament: binding of its 32 heads (reach walk fused with the
-//      nearest-segment choice; bound heads join their segment's motor list) alongside
-//      every position-only myosin term, then the ordered sums, the cross-bridge bonds
-//      and integrate + derive of its 96 sub-bodies and backbone, all force sums in
-//      shared memory; other CTAs compute crosslinker forces + torsion and the filament
-//      Brownian draws
+//   B0 binding of every head, one warp per head: release, the reach walk fused with the
+//      nearest-segment choice (lanes test 32 candidates at a time, appended in order),
+//      nucleotide cycle; bound heads join their segment's motor list
+//   F  one CTA per minifilament: every position-only myosin term, then the ordered sums,
+//      the cross-bridge bonds and integrate + derive of its 96 sub-bodies and backbone,
+//      all force sums in shared memory; other CTAs compute crosslinker forces + torsion,
+//      the chain joints and the filament Brownian draws
 //   K  one CTA per group of whole filaments, poses staged in shared memory with TMA
 //      bulk copies: chain forces (each joint once), crosslinker A/B gathers, motor
 //      gather from the segment's motor list in ascending slot order (FP64 sums),
@@ -426,79 +427,154 @@ __device__ void phase_place(const FusedArgs& a) {
 // ---------------------------------------------------------------- F: minifilaments + links
 // BindingDetectionSystem.gridReachable (BindingDetectionSystem.java:161-227) over the
 // segment-only cell-ordered endpoints, fused with bindNearest's selection
-// (BindingDetectionSystem.java:366-388): the same 27 cells in the same order, the same
-// predicate, and the first nearest among the first MAX_CAND candidates. The nine row
-// ranges (three consecutive x-cells each) are loaded before the walk starts.
-__device__ int reach_walk_bind(const FusedArgs& a, float mx, float my, float mz, float mux, float muy, float muz,
-                               float rux, float ruy, float ruz, int* out, float tol, float align, int* bestSeg,
-                               float* bestArc) {
+// (BindingDetectionSystem.java:366-388): the same 27 cells in the same order (nine rows of
+// three consecutive x-cells), the same predicate, and the first nearest among the first
+// MAX_CAND candidates; one warp walks one head (every lane calls it with the same head):
+// lanes 0..8 read the nine stencil row ranges, then the entries are tested 32 at a
+// time, lane k taking entry k0 + k. Passing entries are appended in entry order (ballot, and
+// the popcount of the lower lanes' passes), so the list is the serial walk's list; the
+// nearest of the first MAX_CAND (strict <, the first in list order wins) is the serial
+// choice: a chunk's minimum with ties to its lowest lane replaces the running best only when
+// strictly smaller. Returns the reach count; best and arc are the same on every lane.
+__device__ int warp_reach_bind(const FusedArgs& a, int lane, float mx, float my, float mz, float mux, float muy,
+                               float muz, float rux, float ruy, float ruz, int* out, float tol, float align,
+                               int* bestSeg, float* bestArc) {
     const float* gp = a.sc.grid.gridParams;
     const int* off = a.segCellOff;
-    int nX = a.nX, nY = a.nY, nZ = a.nZ, nXY = nX * nY;
-    int cx = cell_coord(mx, gp[0], gp[4], nX), cy = cell_coord(my, gp[1], gp[4], nY),
-        cz = cell_coord(mz, gp[2], gp[4], nZ);
-    int x0 = max(cx - 1, 0), x1 = min(cx + 1, nX - 1);
-    int rs[9], re[9];
+    const int nX = a.nX, nY = a.nY, nZ = a.nZ, nXY = nX * nY;
+    const int cx = cell_coord(mx, gp[0], gp[4], nX), cy = cell_coord(my, gp[1], gp[4], nY),
+              cz = cell_coord(mz, gp[2], gp[4], nZ);
+    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, nX - 1);
+    int rs = 0, len = 0;
+    if (lane < 9) {
+        int zz = cz - 1 + lane / 3, yy = cy - 1 + lane % 3;
+        if (zz >= 0 && zz < nZ && yy >= 0 && yy < nY) {
+            int c0 = x0 + yy * nX + zz * nXY;
+            rs = off[c0];
+            len = off[c0 + (x1 - x0) + 1] - rs;
+        }
+    }
+    int inc = len;
+#pragma unroll
+    for (int o = 1; o < 16; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, inc, 8);
+    // every lane holds the nine (start of row in the sequence, start of row in memory) pairs
+    int preR[9], rsR[9];
 #pragma unroll
     for (int r = 0; r < 9; r++) {
-        int zz = cz - 1 + r / 3, yy = cy - 1 + r % 3;
-        bool ok = zz >= 0 && zz < nZ && yy >= 0 && yy < nY;
-        int c0 = x0 + yy * nX + zz * nXY;
-        rs[r] = ok ? off[c0] : 0;
-        re[r] = ok ? off[c0 + (x1 - x0) + 1] : 0;
+        preR[r] = __shfl_sync(0xffffffffu, inc - len, r);
+        rsR[r] = __shfl_sync(0xffffffffu, rs, r);
     }
-    // the nine ranges as one sequence k = 0..total-1 (row order, then index order), taken
-    // four items at a time so that their loads are in flight together
-    int pre[10];
-    pre[0] = 0;
-#pragma unroll
-    for (int r = 0; r < 9; r++) pre[r + 1] = pre[r] + (re[r] - rs[r]);
-    const int total = pre[9];
+    const unsigned lower = (1u << lane) - 1u;
     int cnt = 0, best = -1;
     float bestD = 1.0e30f, arc = 0.f;
-    for (int k0 = 0; k0 < total; k0 += 4) {
-        float4 e1[4], e2[4];
+    for (int k0 = 0; k0 < total; k0 += 32) {
+        const int k = k0 + lane;
+        bool pass = false;
+        float d = 0.f;
+        float4 e1 = make_float4(0.f, 0.f, 0.f, 0.f), e2 = e1;
+        if (k < total) {
+            int idx = rsR[0] + k;
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            int k = k0 + q;
-            if (k < total) {
-                int idx = rs[0] + k;
-#pragma unroll
-                for (int r = 1; r < 9; r++)
-                    if (k >= pre[r]) idx = rs[r] + (k - pre[r]);
-                e1[q] = a.segE1[idx];
-                e2[q] = a.segE2[idx];
-            }
+            for (int r = 1; r < 9; r++)
+                if (k >= preR[r]) idx = rsR[r] + (k - preR[r]);
+            e1 = a.segE1[idx];
+            e2 = a.segE2[idx];
+            d = reach_test_dist_sq(mx, my, mz, mux, muy, muz, rux, ruy, ruz, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z, tol,
+                                   align);
+            pass = d >= 0.f;
         }
+        const unsigned mask = __ballot_sync(0xffffffffu, pass);
+        const int pos = cnt + __popc(mask & lower);
+        const int sg = __float_as_int(e1.w);
+        const bool elig = pass && pos < MAX_CAND;
+        if (elig) out[pos] = sg;
+        float v = elig ? d : 3.0e38f;
+        int who = lane;
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            if (k0 + q >= total) break;
-            float d = reach_test_dist_sq(mx, my, mz, mux, muy, muz, rux, ruy, ruz, e1[q].x, e1[q].y, e1[q].z, e2[q].x,
-                                         e2[q].y, e2[q].z, tol, align);
-            if (d >= 0.f) {
-                if (cnt < MAX_CAND) {
-                    int sg = __float_as_int(e1[q].w);
-                    out[cnt] = sg;
-                    if (d < bestD) {
-                        bestD = d;
-                        best = sg;
-                        arc = bind_arc(mx, my, mz, e1[q].x, e1[q].y, e1[q].z, e2[q].x, e2[q].y, e2[q].z);
-                    }
-                }
-                cnt++;
-            }
+        for (int o = 16; o > 0; o >>= 1) {
+            float ov = __shfl_xor_sync(0xffffffffu, v, o);
+            int ow = __shfl_xor_sync(0xffffffffu, who, o);
+            if (ov < v || (ov == v && ow < who)) { v = ov; who = ow; }
         }
+        if (v < bestD) {
+            float myArc = 0.f;
+            if (lane == who) myArc = bind_arc(mx, my, mz, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z);
+            bestD = v;
+            best = __shfl_sync(0xffffffffu, sg, who);
+            arc = __shfl_sync(0xffffffffu, myArc, who);
+        }
+        cnt += __popc(mask);
     }
     *bestSeg = best;
     *bestArc = arc;
     return cnt;
 }
 
-// One minifilament per CTA. Stage 1: warp 0 runs binding for the heads while warps 1-3
-// evaluate every position-only term of the myosin mechanics (motor joints, dimer coupling
-// variants and lever torsion, tethers), none of which depends on this step's binding.
-// Stage 2: each sub-body accumulates its terms in the order of the reference's System
-// sequence (joints, coupling, tether; the head's bond after its joint). Stage 3: integrate.
+// BindingDetectionSystem / NucleotideCycleSystem for every head, one warp per head: the
+// catch-slip release (NucleotideCycleSystem.java:77-134), the reach walk fused with
+// bindNearest's choice (BindingDetectionSystem.java:161-227, :366-388), the nucleotide cycle
+// (NucleotideCycleSystem.java:33-69) and the bound head's entry in its segment's motor row.
+// Warp w takes heads w, w + W, w + 2W, ... (W warps in the grid) in rounds of 32: lane j
+// releases and cycles the round's head j, all lanes walk each head in turn.
+__device__ void phase_bind(const FusedArgs& a, int t) {
+    const sbx_dense_scene& sc = a.sc;
+    const sbx_motor_store& mot = sc.mot;
+    const float* kp = mot.kinParams;
+    const int lane = threadIdx.x & 31, gw = gtid() >> 5, nw = gthreads() >> 5;
+    const int nM = a.nM;
+    int listed = 0;
+    for (int base = gw; base < nM; base += 32 * nw) {
+        const int myM = base + lane * nw;
+        const bool mine = myM < nM;
+        int bs = 0, cd = 0, sb = 0, sr = 0, cs = 0;
+        if (mine) {
+            bs = mot.boundSeg[myM]; cd = mot.cooldown[myM]; sb = mot.stats[2 * myM]; sr = mot.stats[2 * myM + 1];
+            cs = mot.capStats[myM];
+            release_one(myM, bs, cd, sb, sr, cs, mot.forceDotFil[myM], mot.forceMag[myM], kp, t, sc.seed);
+        }
+        for (int j = 0; j < 32; j++) {
+            const int m = base + j * nw;
+            if (m >= nM) break;
+            float mx = mot.head[m], my = mot.head[nM + m], mz = mot.head[2 * nM + m];
+            float mux = mot.uVec[m], muy = mot.uVec[nM + m], muz = mot.uVec[2 * nM + m];
+            float rux = mot.rodUVec[m], ruy = mot.rodUVec[nM + m], ruz = mot.rodUVec[2 * nM + m];
+            int best;
+            float arc;
+            int rc = warp_reach_bind(a, lane, mx, my, mz, mux, muy, muz, rux, ruy, ruz,
+                                     sc.grid.reachSeg + (int64_t)m * MAX_CAND, kp[7], kp[8], &best, &arc);
+            if (lane == 0) {
+                sc.grid.reachCount[m] = rc;
+                if (rc > MAX_CAND) {
+                    atomicOr(a.err, ERR_REACH_OVERFLOW);
+                    stat_add(a, ST_REACH_OVER, 1);
+                }
+            }
+            if (lane == j && bs == FREE_BINDABLE && best >= 0) {
+                bs = best;
+                mot.bindArc[m] = arc;
+            }
+        }
+        if (mine) {
+            mot.boundSeg[myM] = bs; mot.cooldown[myM] = cd; mot.stats[2 * myM] = sb; mot.stats[2 * myM + 1] = sr;
+            mot.capStats[myM] = cs;
+            mot.nucleotideState[myM] = cycle_one(myM, mot.nucleotideState[myM], bs >= 0, mot.forceDotHist + 10 * myM,
+                                                 mot.nucParams, t, sc.seed);
+            if (bs >= 0) listed += row_insert(a.cntM, a.slotM, FUSED_ROW_SLOTS, a.rowUse, a.headM, a.nextM, bs, myM);
+        }
+    }
+    stat_add(a, ST_MOTOR_LIST, listed);
+}
+
+// One minifilament per CTA (its heads' binding ran in the previous phase). Stage 1: the four
+// warps evaluate every position-only term of the myosin mechanics (warps 0-1: the motor
+// joints; warp 2: lever torsion and tethers; warp 3: the dimer coupling variants), none of
+// which depends on this step's binding. Stage 2: each sub-body accumulates its terms in the
+// order of the reference's System sequence (joints, coupling, tether; the head's bond after
+// its joint). Stage 3: integrate.
 __device__ void mini_unit(const FusedArgs& a, MiniSmem& ms, int u, int t) {
     const sbx_dense_scene& sc = a.sc;
     const sbx_motor_store& mot = sc.mot;
@@ -516,45 +592,19 @@ __device__ void mini_unit(const FusedArgs& a, MiniSmem& ms, int u, int t) {
     const float* kp = mot.kinParams;
 
     // ---- stage 1
-    if (tid < 32) {
-        if (tid < mpm) {
-            // BindingDetectionSystem / NucleotideCycleSystem for this head
-            int m = m0 + tid;
-            float mx = mot.head[m], my = mot.head[nM + m], mz = mot.head[2 * nM + m];
-            float mux = mot.uVec[m], muy = mot.uVec[nM + m], muz = mot.uVec[2 * nM + m];
-            float rux = mot.rodUVec[m], ruy = mot.rodUVec[nM + m], ruz = mot.rodUVec[2 * nM + m];
-            int* slice = sc.grid.reachSeg + (int64_t)m * MAX_CAND;
-            int bs = mot.boundSeg[m], cd = mot.cooldown[m], sb = mot.stats[2 * m], sr = mot.stats[2 * m + 1],
-                cs = mot.capStats[m];
-            release_one(m, bs, cd, sb, sr, cs, mot.forceDotFil[m], mot.forceMag[m], kp, t, sc.seed);
-            int best;
-            float arc;
-            int rc = reach_walk_bind(a, mx, my, mz, mux, muy, muz, rux, ruy, ruz, slice, kp[7], kp[8], &best, &arc);
-            sc.grid.reachCount[m] = rc;
-            if (rc > MAX_CAND) {
-                atomicOr(a.err, ERR_REACH_OVERFLOW);
-                stat_add(a, ST_REACH_OVER, 1);
-            }
-            if (bs == FREE_BINDABLE && best >= 0) {
-                bs = best;
-                mot.bindArc[m] = arc;
-            }
-            mot.boundSeg[m] = bs; mot.cooldown[m] = cd; mot.stats[2 * m] = sb; mot.stats[2 * m + 1] = sr;
-            mot.capStats[m] = cs;
-            mot.nucleotideState[m] = cycle_one(m, mot.nucleotideState[m], bs >= 0, mot.forceDotHist + 10 * m,
-                                               mot.nucParams, t, sc.seed);
-            if (bs >= 0) stat_add(a, ST_MOTOR_LIST, row_insert(a.cntM, a.slotM, FUSED_ROW_SLOTS, a.rowUse, a.headM, a.nextM, bs, m));
-        }
-    } else if (tid < 96) {
-        // warps 1-2: motor joints (local motor k/2, joint k&1), then a lever (warp 1) or a tether (warp 2)
-        int k = tid - 32;
+    if (tid < 64) {
+        // warps 0-1: the motor joints (local motor k/2, joint k&1)
+        const int k = tid;
         if (k < 2 * mpm)
             ms.mj[k] = motor_joint(m0 + (k >> 1), k & 1, nB, mb.coord, mb.uVec, mb.segLength, mb.bTransGam,
                                    mb.bRotGam, mot.jointParams);
-        int dl = k & 31;
+    } else if (tid < 96) {
+        // warp 2: lever torsion (lanes 0-15) and tethers (lanes 16-31) of the dimers
+        const int k = tid - 64;
+        const int dl = k & 15;
         if (dl < dpm) {
             int d = d0 + dl;
-            if (k < 32) {
+            if (k < 16) {
                 ms.lt[dl] = couple_lever(nB, mb.uVec, mb.bRotGam, 2 * d, 2 * d + 1, sc.dim.dimerParams);
             } else {
                 TetherTerm T = tether_terms(nB, mb.coord, mb.uVec, mb.segLength, mb.bTransGam, mb.bRotGam, nBb,
@@ -1080,7 +1130,11 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_dense_fused(FusedArgs a, i
         phase_place(a);
         if (!counter_sync(a.bar, gTarget, nGrid, a.err)) return;
         stamp(s);
-        // F: minifilaments (binding + myosin mechanics), crosslinker forces, filament Brownian
+        // B0: binding of every head (one warp per head)
+        phase_bind(a, t);
+        if (!counter_sync(a.bar, gTarget, nGrid, a.err)) return;
+        stamp(s);
+        // F: minifilament mechanics, crosslinker forces, chain joints, filament Brownian
         phase_motors_links(a, sm, t);
         if (!counter_sync(a.bar, gTarget, nGrid, a.err)) return;
         stamp(s);
