@@ -46,8 +46,9 @@ WARM_STEPS = 3000      # untimed steps before the warm-up: bound heads have buil
 REF_MIN_STEPS = 200    # the reference arm times at least this many steps
 # DRAM bytes (read + write) of one launch of the fused kernel advancing one step of this
 # workload (FP64 centres, warmed state, L2 flushed before the launch), from one ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum, one kernel, one launch)
-FUSED_STEP_DRAM_BYTES = None
+# (dram__bytes_read.sum + dram__bytes_write.sum, mean of three launches; the command is
+# in profiles/k_dense_fused_benchmark_network.md)
+FUSED_STEP_DRAM_BYTES = 11_140_000
 
 
 def workload_config(sc_host, warmup):
