@@ -30,6 +30,7 @@
 // Every slot is computed by the same device functions as the per-system kernels, in the
 // reference's accumulation order, so the result is bit-identical to
 // DenseContractileHarness.cpuStep (DenseContractileHarness.java:350-429).
+#define SBX_SHARE_CALLS 1
 #include <cuda_runtime.h>
 
 #include "../../include/softbox_b200.h"
@@ -121,26 +122,27 @@ __device__ __forceinline__ unsigned long long counter_base(const unsigned long l
 __device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
 __device__ __forceinline__ int gthreads() { return gridDim.x * blockDim.x; }
 
-// BrownianForceSystem.brownianForce for one slot (BrownianForceSystem.java:44-106); in
-// supplied-noise mode the six Gaussians come from noise[t - t0][6][n] (a step outside the
-// supplied range, which the host rejects before the launch, draws zeros)
-__device__ __forceinline__ void brownian_slot(const FusedArgs& a, const sbx_rigid_body& b, int s, int t, int seed,
-                                              float mag, const float* noise) {
+// BrownianForceSystem.brownianForce (BrownianForceSystem.java:44-106), component j (0..2) of
+// one slot: the slot's j-th Box-Muller pair gives its random force and torque components j
+// (randF = ((tS * mag) * sqrt(gamma)) * g, :94-104). In supplied-noise mode the Gaussians come
+// from noise[t - t0][6][n] (a step outside the supplied range, which the host rejects before
+// the launch, draws zeros).
+__device__ __forceinline__ void brownian_component(const FusedArgs& a, const sbx_rigid_body& b, int s, int j, int t,
+                                                   int seed, float mag, const float* noise) {
     const int n = b.n;
-    float g[6];
+    float gf, gt;
     if (noise) {
         int k = t - a.nzT0;
         bool in = k >= 0 && k < a.nzN;
         const float* q = noise + (int64_t)(in ? k : 0) * 6 * n + s;
-        for (int j = 0; j < 6; j++) g[j] = in ? q[(int64_t)j * n] : 0.f;
+        gf = in ? q[(int64_t)j * n] : 0.f;
+        gt = in ? q[(int64_t)(3 + j) * n] : 0.f;
     } else {
-        gauss6_wang(s, t, seed, g);
+        gauss_pair_wang(s, t, seed, j, &gf, &gt);
     }
-    float gT[3] = {b.bTransGam[s], b.bTransGam[n + s], b.bTransGam[2 * n + s]};
-    float gR[3] = {b.bRotGam[s], b.bRotGam[n + s], b.bRotGam[2 * n + s]};
-    float rf[3], rt[3];
-    brownian_amplitudes(g, b.brownTransScale[s], b.brownRotScale[s], mag, gT, gR, rf, rt);
-    for (int k = 0; k < 3; k++) { b.randForce[k * n + s] = rf[k]; b.randTorque[k * n + s] = rt[k]; }
+    const float tS = b.brownTransScale[s], rS = b.brownRotScale[s];
+    b.randForce[j * n + s] = tS * mag * fsqrt(b.bTransGam[j * n + s]) * gf;
+    b.randTorque[j * n + s] = rS * mag * fsqrt(b.bRotGam[j * n + s]) * gt;
 }
 
 // ---------------------------------------------------------------- rows: slots + overflow lists
@@ -290,16 +292,17 @@ __device__ void link_unbind(const FusedArgs& a, int t, int firstWarp) {
 }
 
 // BrownianForceSystem for the motor sub-bodies, then the backbones, on the warps from
-// `firstWarp` on (all warps when there are none)
+// `firstWarp` on (all warps when there are none): one thread per (component, slot)
 __device__ void motor_brownian(const FusedArgs& a, int t, int firstWarp) {
     const sbx_dense_scene& sc = a.sc;
     int w = gtid() >> 5, nw = gthreads() >> 5;
     if (firstWarp >= nw) firstWarp = 0;
     if (w < firstWarp) return;
     const int nB = a.nB, n = nB + a.nBb;
-    for (int j = (w - firstWarp) * 32 + (threadIdx.x & 31); j < n; j += (nw - firstWarp) * 32) {
-        if (j < nB) brownian_slot(a, sc.mot.body, j, t, sc.seed, sc.mot.bodyParams[1], a.nzMot);
-        else brownian_slot(a, sc.mini.backbone, j - nB, t, sc.seedBb, sc.mini.bbBodyParams[1], a.nzBb);
+    for (int q = (w - firstWarp) * 32 + (threadIdx.x & 31); q < 3 * n; q += (nw - firstWarp) * 32) {
+        const int c = q / n, j = q - c * n;
+        if (j < nB) brownian_component(a, sc.mot.body, j, c, t, sc.seed, sc.mot.bodyParams[1], a.nzMot);
+        else brownian_component(a, sc.mini.backbone, j - nB, c, t, sc.seedBb, sc.mini.bbBodyParams[1], a.nzBb);
     }
 }
 
@@ -739,7 +742,8 @@ __device__ void phase_motors_links(const FusedArgs& a, FusedSmem& sm, int t) {
     }
     // on the CTAs without a unit (all CTAs when there are none): the chain joints of the
     // filaments (ChainBendingForceSystem's costly part, from this step's start poses; each
-    // joint once, by its lower-slot rod) and the filament Brownian forcing
+    // joint once, by its lower-slot rod: item 2 i + side) and the filament Brownian forcing
+    // (one item per component and rod)
     const sbx_filament_store& fs = a.sc.fil;
     const sbx_rigid_body& fb = fs.body;
     int helpers = (int)gridDim.x - units, h0 = units;
@@ -747,22 +751,21 @@ __device__ void phase_motors_links(const FusedArgs& a, FusedSmem& sm, int t) {
     if ((int)blockIdx.x >= h0) {
         ChainJoint* J = reinterpret_cast<ChainJoint*>(a.joints);
         const int n = a.nSeg;
-        ChainParams cp = chain_params(fs.chainParams);
-        for (int i = ((int)blockIdx.x - h0) * blockDim.x + threadIdx.x; i < n; i += helpers * blockDim.x) {
-            if (a.jointShare) {
-                int s2 = fs.end2NbrSlot[i], s1 = fs.end1NbrSlot[i];
-                if (s2 > i || s1 > i) {
-                    RodGeom me = load_rod(n, i, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.bRotGam);
-                    if (s2 > i)
-                        J[2 * i] = chain_joint(cp, i, 0, s2, fs.end2NbrSide[i], me,
-                                               load_rod(n, s2, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.bRotGam));
-                    if (s1 > i)
-                        J[2 * i + 1] =
-                            chain_joint(cp, i, 1, s1, fs.end1NbrSide[i], me,
-                                        load_rod(n, s1, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.bRotGam));
+        const int nJ = a.jointShare ? 2 * n : 0, total = nJ + 3 * n;
+        for (int q = ((int)blockIdx.x - h0) * blockDim.x + threadIdx.x; q < total; q += helpers * blockDim.x) {
+            if (q < nJ) {
+                const int i = q >> 1, side = q & 1;
+                const int nb = side == 0 ? fs.end2NbrSlot[i] : fs.end1NbrSlot[i];
+                if (nb > i) {
+                    ChainParams cp = chain_params(fs.chainParams);
+                    J[q] = chain_joint(cp, i, side, nb, side == 0 ? fs.end2NbrSide[i] : fs.end1NbrSide[i],
+                                       load_rod(n, i, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.bRotGam),
+                                       load_rod(n, nb, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.bRotGam));
                 }
+            } else {
+                const int r = q - nJ, c = r / n, i = r - c * n;
+                brownian_component(a, fb, i, c, t, a.filSeed, fs.params[1], a.nzFil);
             }
-            brownian_slot(a, fb, i, t, a.filSeed, fs.params[1], a.nzFil);
         }
     }
     // the reference's activeLinkCount array holds this step's counts
@@ -1064,7 +1067,7 @@ __device__ bool phase_rods(const FusedArgs& a, FusedSmem& sm, int t, uint64_t* m
     return true;
 }
 
-__global__ void __launch_bounds__(FUSED_THREADS, 4) k_dense_fused(FusedArgs a, int t0, int nsteps) {
+__global__ void __launch_bounds__(FUSED_THREADS, 4) k_dense_fused(const __grid_constant__ FusedArgs a, int t0, int nsteps) {
     __shared__ __align__(8) uint64_t mbar;
     extern __shared__ __align__(16) unsigned char fused_dsm[];
     FusedSmem& sm = *reinterpret_cast<FusedSmem*>(fused_dsm);

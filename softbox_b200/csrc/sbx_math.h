@@ -31,6 +31,15 @@
 #else
 #define SBX_HD static inline
 #endif
+// The transcendentals themselves: inlined at every call site by default; a translation
+// unit that defines SBX_SHARE_CALLS before including this header gets one out-of-line
+// copy of each instead (a kernel with many call sites then runs the same instructions
+// from every one of them and keeps them in the instruction cache)
+#if defined(__CUDACC__) && defined(SBX_SHARE_CALLS)
+#define SBX_HD_CALL static __host__ __device__ __noinline__
+#else
+#define SBX_HD_CALL SBX_HD
+#endif
 
 namespace sbxm {
 
@@ -124,7 +133,7 @@ SBX_HD double reduce_pio2(double x, int* quadrant) {
     return r;
 }
 
-SBX_HD double sin(double x) {
+SBX_HD_CALL double sin(double x) {
     int q; double r = reduce_pio2(x, &q);
 #ifdef __CUDA_ARCH__
     // both polynomials and a select: lanes in different quadrants do not diverge
@@ -141,7 +150,7 @@ SBX_HD double sin(double x) {
 #endif
 }
 
-SBX_HD double cos(double x) {
+SBX_HD_CALL double cos(double x) {
     int q; double r = reduce_pio2(x, &q);
 #ifdef __CUDA_ARCH__
     double sp = sin_poly(r), cp = cos_poly(r);
@@ -159,7 +168,7 @@ SBX_HD double cos(double x) {
 
 // sin(x) and cos(x) together: one reduction and one evaluation of each polynomial, each
 // result selected exactly as sin() and cos() above select it (the same bits)
-SBX_HD void sincos(double x, double* sOut, double* cOut) {
+SBX_HD_CALL void sincos(double x, double* sOut, double* cOut) {
     int q; double r = reduce_pio2(x, &q);
     double sp = sin_poly(r), cp = cos_poly(r);
     double vs = (q & 1) ? cp : sp;
@@ -169,7 +178,7 @@ SBX_HD void sincos(double x, double* sOut, double* cOut) {
 }
 
 // natural log of a positive double (x <= 0 -> -inf / NaN like libm)
-SBX_HD double log(double x) {
+SBX_HD_CALL double log(double x) {
     if (!(x > 0.0)) return (x == 0.0) ? bitsd(0xfff0000000000000ULL) : bitsd(0x7ff8000000000000ULL);
     uint64_t u = dbits(x);
     int e = (int)((u >> 52) & 0x7ff);
@@ -198,7 +207,7 @@ SBX_HD double log(double x) {
 }
 
 // e^x
-SBX_HD double exp(double x) {
+SBX_HD_CALL double exp(double x) {
     if (x != x) return x;
     if (x > 709.782712893384) return bitsd(0x7ff0000000000000ULL);
     if (x < -745.1332191019412) return 0.0;

@@ -12,6 +12,12 @@
 #include "../../include/softbox_b200.h"
 
 #define SBX_DEV __device__ __forceinline__
+// functions with many call sites in one kernel (SBX_SHARE_CALLS: one out-of-line copy)
+#if defined(SBX_SHARE_CALLS)
+#define SBX_DEV_CALL static __device__ __noinline__
+#else
+#define SBX_DEV_CALL SBX_DEV
+#endif
 
 namespace sbx {
 
@@ -58,6 +64,23 @@ SBX_DEV void gauss6_wang(int32_t i, int32_t step, int32_t seed, float g[6]) {
     float u5 = fmaxf(1.0e-7f, sbxm::unit_from_hash(sbxm::wang_hash(base ^ 0x517cc1b7u)));
     float u6 = sbxm::unit_from_hash(sbxm::wang_hash(base ^ 0x1f0a7ed5u));
     box_muller6(u1, u2, u3, u4, u5, u6, g);
+}
+
+// Pair j (0..2) of gauss6_wang alone: g[j] and g[3 + j] by the same operations (the three
+// pairs of a slot are independent, so three threads can draw one slot)
+SBX_DEV void gauss_pair_wang(int32_t i, int32_t step, int32_t seed, int j, float* gc, float* gs) {
+    const uint32_t base = sbxm::rng_base(i, step, seed);
+    const uint32_t ka = j == 0 ? 0u : (j == 1 ? 0x85ebca6bu : 0x517cc1b7u);
+    const uint32_t kb = j == 0 ? 0x9e3779b9u : (j == 1 ? 0xc2b2ae35u : 0x1f0a7ed5u);
+    float ua = fmaxf(1.0e-7f, sbxm::unit_from_hash(sbxm::wang_hash(base ^ ka)));
+    float ub = sbxm::unit_from_hash(sbxm::wang_hash(base ^ kb));
+    const float TWO_PI_F = 2.0f * 3.14159265f;
+    double sn, cs;
+    float r = fsqrt(-2.0f * (float)sbxm::log((double)ua));
+    float th = TWO_PI_F * ub;
+    sbxm::sincos((double)th, &sn, &cs);
+    *gc = r * (float)cs;
+    *gs = r * (float)sn;
 }
 
 // Counter-based Philox4x32-10 keyed (seed64, step, slot); same uniform/Box-Muller map
@@ -233,7 +256,7 @@ SBX_DEV bool confine_one(const BoxParams& bx, const float c[3], const float u[3]
 
 // ---------------------------------------------------------------- angles
 // ChainBendingForceSystem.java:48-72 (same polynomial + two Newton steps in every System)
-SBX_DEV double accurate_acos(double x) {
+SBX_DEV_CALL double accurate_acos(double x) {
     if (x > 1.0) x = 1.0;
     if (x < -1.0) x = -1.0;
     double y;
@@ -260,7 +283,7 @@ SBX_DEV double accurate_acos(double x) {
     return y;
 }
 
-SBX_DEV double accurate_asin(double s) {                    // ChainBendingForceSystem.java:76-84
+SBX_DEV_CALL double accurate_asin(double s) {                    // ChainBendingForceSystem.java:76-84
     double s2 = s * s;
     double y = s * (1.0 + s2 * (0.16666666666666666 + s2 * (0.075 + s2 * 0.044642857142857)));
     double sy, cy;
