@@ -566,6 +566,7 @@ bool fused_prepare(sbx_dense_plan* p) {
     a.headM = (int*)alloc(4 * nS); a.nextM = (int*)alloc(4 * (size_t)a.nM);
     a.segE1 = (float4*)alloc(16 * nS); a.segE2 = (float4*)alloc(16 * nS);
     a.joints = alloc(2 * nS * FUSED_JOINT_BYTES);
+    a.terms = alloc((2 * (size_t)a.nM + 4 * (size_t)a.nD) * FUSED_TERM_BYTES);
     a.bar = (unsigned long long*)alloc(32);
     a.err = (int*)alloc(16);
     a.d_step = p->d_step;

@@ -57,12 +57,25 @@ struct RodSmem {
 };
 struct MiniSmem {
     float sF[3 * FUSED_MAX_SUB], sT[3 * FUSED_MAX_SUB];
-    MotorJoint mj[4 * FUSED_MAX_DPM];            // [local motor][joint 2, joint 1]
-    CoupleTerm ct[2 * FUSED_MAX_DPM];            // [local dimer][end variant]
-    LeverTerm lt[FUSED_MAX_DPM];
-    TetherTerm tt[FUSED_MAX_DPM];
 };
 static_assert(sizeof(ChainJoint) <= FUSED_JOINT_BYTES, "joint slot size");
+static_assert(sizeof(MotorJoint) <= FUSED_TERM_BYTES && sizeof(CoupleTerm) <= FUSED_TERM_BYTES &&
+                  sizeof(LeverTerm) <= FUSED_TERM_BYTES && sizeof(TetherTerm) <= FUSED_TERM_BYTES,
+              "myosin term slot size");
+
+// slots of the step's myosin terms (FusedArgs::terms)
+__device__ __forceinline__ MotorJoint& term_joint(const FusedArgs& a, int m, int which) {
+    return *reinterpret_cast<MotorJoint*>((char*)a.terms + ((size_t)which * a.nM + m) * FUSED_TERM_BYTES);
+}
+__device__ __forceinline__ CoupleTerm& term_couple(const FusedArgs& a, int d, int variant) {
+    return *reinterpret_cast<CoupleTerm*>((char*)a.terms + (2 * (size_t)a.nM + 2 * d + variant) * FUSED_TERM_BYTES);
+}
+__device__ __forceinline__ LeverTerm& term_lever(const FusedArgs& a, int d) {
+    return *reinterpret_cast<LeverTerm*>((char*)a.terms + (2 * (size_t)a.nM + 2 * (size_t)a.nD + d) * FUSED_TERM_BYTES);
+}
+__device__ __forceinline__ TetherTerm& term_tether(const FusedArgs& a, int d) {
+    return *reinterpret_cast<TetherTerm*>((char*)a.terms + (2 * (size_t)a.nM + 3 * (size_t)a.nD + d) * FUSED_TERM_BYTES);
+}
 
 union FusedSmem {
     RodSmem rod;
@@ -303,6 +316,48 @@ __device__ void motor_brownian(const FusedArgs& a, int t, int firstWarp) {
         const int c = q / n, j = q - c * n;
         if (j < nB) brownian_component(a, sc.mot.body, j, c, t, sc.seed, sc.mot.bodyParams[1], a.nzMot);
         else brownian_component(a, sc.mini.backbone, j - nB, c, t, sc.seedBb, sc.mini.bbBodyParams[1], a.nzBb);
+    }
+}
+
+// The position-only terms of the myosin mechanics, none of which depends on this step's
+// binding or forces (MotorJointSystem.java:72-123 joint geometry, DimerCouplingSystem.java:
+// 99-182 end variants and lever torsion, MiniFilamentSystem tethers with their backbone
+// reaction rows), one item per term on the warps from `firstWarp` on (all warps when
+// there are none); the minifilament phase accumulates them in the reference's order.
+__device__ void myosin_terms(const FusedArgs& a, int firstWarp) {
+    const sbx_dense_scene& sc = a.sc;
+    const sbx_motor_store& mot = sc.mot;
+    const sbx_rigid_body& mb = mot.body;
+    const sbx_minifilament_store& mini = sc.mini;
+    const sbx_rigid_body& bb = mini.backbone;
+    int w = gtid() >> 5, nw = gthreads() >> 5;
+    if (firstWarp >= nw) firstWarp = 0;
+    if (w < firstWarp) return;
+    const int nM = a.nM, nD = a.nD, nB = a.nB;
+    const int total = 2 * nM + 4 * nD;
+    for (int k = (w - firstWarp) * 32 + (threadIdx.x & 31); k < total; k += (nw - firstWarp) * 32) {
+        if (k < 2 * nM) {
+            const int which = k >= nM, m = k - which * nM;
+            term_joint(a, m, which) = motor_joint(m, which, nB, mb.coord, mb.uVec, mb.segLength, mb.bTransGam,
+                                                  mb.bRotGam, mot.jointParams);
+        } else if (k < 2 * nM + 2 * nD) {
+            const int q = k - 2 * nM, d = q >> 1;
+            term_couple(a, d, q & 1) = couple_variant(nB, mb.coord, mb.uVec, mb.segLength, mb.bTransGam, mb.bRotGam,
+                                                      2 * d, 2 * d + 1, sc.dim.parallel[d] != 0, sc.dim.dimerParams,
+                                                      q & 1);
+        } else if (k < 2 * nM + 3 * nD) {
+            const int d = k - 2 * nM - 2 * nD;
+            term_lever(a, d) = couple_lever(nB, mb.uVec, mb.bRotGam, 2 * d, 2 * d + 1, sc.dim.dimerParams);
+        } else {
+            const int d = k - 2 * nM - 3 * nD, u = d / a.dpm;
+            TetherTerm T = tether_terms(nB, mb.coord, mb.uVec, mb.segLength, mb.bTransGam, mb.bRotGam, a.nBb, bb.coord,
+                                        bb.uVec, mini.bbInvDragY, u, 2 * d, mini.attachAxial[d], mini.miniParams);
+            term_tether(a, d) = T;
+            float* o = mini.miniData + (int64_t)MINI_STRIDE * d;
+            for (int j = 0; j < 6; j++) o[j] = T.row[j];
+            // backbone CSR of the reference (rows = backbones, items = dimers in index order)
+            mini.bbDimerList[d] = d;
+        }
     }
 }
 
@@ -572,12 +627,10 @@ __device__ void phase_bind(const FusedArgs& a, int t) {
     stat_add(a, ST_MOTOR_LIST, listed);
 }
 
-// One minifilament per CTA (its heads' binding ran in the previous phase). Stage 1: the four
-// warps evaluate every position-only term of the myosin mechanics (warps 0-1: the motor
-// joints; warp 2: lever torsion and tethers; warp 3: the dimer coupling variants), none of
-// which depends on this step's binding. Stage 2: each sub-body accumulates its terms in the
-// order of the reference's System sequence (joints, coupling, tether; the head's bond after
-// its joint). Stage 3: integrate.
+// One minifilament per CTA (its heads' binding and its position-only terms ran in earlier
+// phases). Stage 2: each sub-body accumulates its terms in the order of the reference's
+// System sequence (joints, coupling, tether; the head's bond after its joint). Stage 3:
+// integrate.
 __device__ void mini_unit(const FusedArgs& a, MiniSmem& ms, int u, int t) {
     const sbx_dense_scene& sc = a.sc;
     const sbx_motor_store& mot = sc.mot;
@@ -585,51 +638,14 @@ __device__ void mini_unit(const FusedArgs& a, MiniSmem& ms, int u, int t) {
     const sbx_minifilament_store& mini = sc.mini;
     const sbx_rigid_body& bb = mini.backbone;
     const sbx_rigid_body& fb = sc.fil.body;
-    const int nB = a.nB, nM = a.nM, nSeg = a.nSeg, nBb = a.nBb;
+    const int nB = a.nB, nSeg = a.nSeg, nBb = a.nBb;
     const int dpm = a.dpm, mpm = 2 * dpm, spm = 6 * dpm;
     const int m0 = u * mpm, s0 = u * spm, d0 = u * dpm;
     const int tid = threadIdx.x;
     float* sF = ms.sF;
     float* sT = ms.sT;
     LocalAcc acc{sF, sT, s0, spm};
-    const float* kp = mot.kinParams;
 
-    // ---- stage 1
-    if (tid < 64) {
-        // warps 0-1: the motor joints (local motor k/2, joint k&1)
-        const int k = tid;
-        if (k < 2 * mpm)
-            ms.mj[k] = motor_joint(m0 + (k >> 1), k & 1, nB, mb.coord, mb.uVec, mb.segLength, mb.bTransGam,
-                                   mb.bRotGam, mot.jointParams);
-    } else if (tid < 96) {
-        // warp 2: lever torsion (lanes 0-15) and tethers (lanes 16-31) of the dimers
-        const int k = tid - 64;
-        const int dl = k & 15;
-        if (dl < dpm) {
-            int d = d0 + dl;
-            if (k < 16) {
-                ms.lt[dl] = couple_lever(nB, mb.uVec, mb.bRotGam, 2 * d, 2 * d + 1, sc.dim.dimerParams);
-            } else {
-                TetherTerm T = tether_terms(nB, mb.coord, mb.uVec, mb.segLength, mb.bTransGam, mb.bRotGam, nBb,
-                                            bb.coord, bb.uVec, mini.bbInvDragY, u, 2 * d, mini.attachAxial[d],
-                                            mini.miniParams);
-                ms.tt[dl] = T;
-                float* o = mini.miniData + (int64_t)MINI_STRIDE * d;
-                for (int j = 0; j < 6; j++) o[j] = T.row[j];
-                // backbone CSR of the reference (rows = backbones, items = dimers in index order)
-                mini.bbDimerList[d] = d;
-            }
-        }
-    } else {
-        // warp 3: the two end variants of each dimer's rod-rod coupling
-        int q = tid - 96;
-        if (q < 2 * dpm) {
-            int d = d0 + (q >> 1);
-            ms.ct[q] = couple_variant(nB, mb.coord, mb.uVec, mb.segLength, mb.bTransGam, mb.bRotGam, 2 * d,
-                                      2 * d + 1, sc.dim.parallel[d] != 0, sc.dim.dimerParams, q & 1);
-        }
-    }
-    __syncthreads();
     // ---- stage 2
     if (tid < 32) {
         if (tid < mpm) {
@@ -641,7 +657,7 @@ __device__ void mini_unit(const FusedArgs& a, MiniSmem& ms, int u, int t) {
             for (int k = 0; k < XB_STRIDE; k++) sc.bondData[m * XB_STRIDE + k] = out[k];
             int hl = 3 * tid + 2;
             double f[3] = {0.0, 0.0, 0.0}, tq[3] = {0.0, 0.0, 0.0};
-            motor_joint_apply(ms.mj[2 * tid + 1], 1, true, mot.nucleotideState[m], s0 + hl, nB, mb.uVec,
+            motor_joint_apply(term_joint(a, m, 1), 1, true, mot.nucleotideState[m], s0 + hl, nB, mb.uVec,
                               mb.segLength, mot.jointParams, f, tq);
             for (int k = 0; k < 3; k++) {
                 float F = (float)(0.0 + f[k]), T = (float)(0.0 + tq[k]);
@@ -658,10 +674,12 @@ __device__ void mini_unit(const FusedArgs& a, MiniSmem& ms, int u, int t) {
             int nuc = mot.nucleotideState[m];
             double f[3] = {0.0, 0.0, 0.0}, tq[3] = {0.0, 0.0, 0.0};
             if (role == 0) {
-                motor_joint_apply(ms.mj[2 * ml], 0, false, nuc, s, nB, mb.uVec, mb.segLength, mot.jointParams, f, tq);
+                motor_joint_apply(term_joint(a, m, 0), 0, false, nuc, s, nB, mb.uVec, mb.segLength, mot.jointParams, f,
+                                  tq);
             } else {
-                motor_joint_apply(ms.mj[2 * ml], 0, true, nuc, s, nB, mb.uVec, mb.segLength, mot.jointParams, f, tq);
-                motor_joint_apply(ms.mj[2 * ml + 1], 1, false, nuc, s, nB, mb.uVec, mb.segLength, mot.jointParams, f,
+                motor_joint_apply(term_joint(a, m, 0), 0, true, nuc, s, nB, mb.uVec, mb.segLength, mot.jointParams, f,
+                                  tq);
+                motor_joint_apply(term_joint(a, m, 1), 1, false, nuc, s, nB, mb.uVec, mb.segLength, mot.jointParams, f,
                                   tq);
             }
             for (int k = 0; k < 3; k++) {
@@ -671,12 +689,12 @@ __device__ void mini_unit(const FusedArgs& a, MiniSmem& ms, int u, int t) {
             int dl = ml >> 1, d = d0 + dl;
             bool isA = (ml & 1) == 0;            // motorA = 2d, motorB = 2d + 1
             if (role == 0) {
-                couple_apply_rod(acc, s, isA, ms.ct[2 * dl]);
-                couple_apply_rod(acc, s, isA, ms.ct[2 * dl + 1]);
-                if (isA) tether_apply(acc, s, ms.tt[dl]);
+                couple_apply_rod(acc, s, isA, term_couple(a, d, 0));
+                couple_apply_rod(acc, s, isA, term_couple(a, d, 1));
+                if (isA) tether_apply(acc, s, term_tether(a, d));
             } else {
                 bool bothBound = mot.boundSeg[2 * d] >= 0 && mot.boundSeg[2 * d + 1] >= 0;
-                if (sc.dim.parallel[d] != 0 && !bothBound) couple_apply_lever(acc, s, isA, ms.lt[dl]);
+                if (sc.dim.parallel[d] != 0 && !bothBound) couple_apply_lever(acc, s, isA, term_lever(a, d));
             }
         } else if (w == 2 * mpm) {
             // the backbone: gather its dimers' reactions, confine, integrate, derive
@@ -1123,6 +1141,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_dense_fused(const __grid_c
         // B, C: scans of the cell, segment-per-cell and link-key histograms (+ motor Brownian)
         tile_sums(first, narr1, a.tileSum, gw, nw);
         if (a.xlOn) link_unbind(a, t, nTiles1);
+        myosin_terms(a, nTiles1 + (a.xlOn ? (a.nL + 31) / 32 : 0));
         if (!counter_sync(a.bar, gTarget, nGrid, a.err)) return;
         stamp(s);
         tile_scan(first, narr1, a.tileSum, out1, copy1, clamp1, sc.grid.chunkSum, gw, nw);

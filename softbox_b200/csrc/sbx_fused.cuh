@@ -12,6 +12,7 @@ constexpr int FUSED_MCAP = 4;         // motor reactions per segment a rod CTA s
 constexpr int FUSED_MIDS = 16;        // motor slots per segment a rod CTA sorts (more: repeated-minimum walk)
 constexpr int FUSED_CELL_SLOTS = 4;   // fixed slots per grid cell
 constexpr int FUSED_JOINT_BYTES = 64; // one chain joint (ChainJoint, padded)
+constexpr int FUSED_TERM_BYTES = 80;  // one position-only myosin term (MotorJoint, CoupleTerm, LeverTerm, TetherTerm)
 constexpr int FUSED_ROW_SLOTS = 4;    // fixed slots per segment (link A ends, link B ends, motors)
 constexpr int FUSED_MIN_HELPERS = 16; // CTAs kept free of rod units in the rod phase
 
@@ -29,6 +30,10 @@ struct FusedArgs {
     int *cntCell, *cntSeg, *cntAct, *cntA, *cntB, *cntM;   // cntSeg: segments per cell
     int* segCellOff;         // segment-only exclusive prefix over cells (C + 1)
     void* joints;            // chain joints at (owner rod, owner side): 2 * nSeg slots of FUSED_JOINT_BYTES
+    // the position-only myosin terms of the step, 2 nM + 4 nD slots of FUSED_TERM_BYTES:
+    // motor joints [which][motor], coupling end variants [dimer][variant], lever torsion
+    // [dimer], tethers [dimer]
+    void* terms;
     int* tileSum;            // tile sums of the step's scans (cells, segments, link A, link B)
     int* mTileSum;           // tile sums of the motor CSR scan
     // rows of the step's inverse maps (cells -> bodies, segments -> link A/B ends,
