@@ -763,7 +763,7 @@ sbx_status sbx_dense_plan_set_noise(sbx_dense_plan* plan, const sbx_dense_noise*
 sbx_status sbx_dense_plan_fused_stats(sbx_dense_plan* plan, int64_t* out, int32_t reset);
 /* Test hook: lowers the fused kernel's capacities (link payload entries a rod CTA stages,
  * motor reactions staged per segment, motor slots sorted per segment, fixed row slots per
- * segment row, fixed slots per grid cell) to exercise the fallback paths on ordinary
+ * segment row (link rows and motor rows alike), fixed slots per grid cell) to exercise the fallback paths on ordinary
  * scenes; each value is clamped to [0, the compiled capacity], a negative value restores
  * the compiled capacity. Takes effect at the next run; the results are the same bits. */
 sbx_status sbx_dense_plan_test_caps(sbx_dense_plan* plan, int32_t entCap, int32_t motorCap, int32_t motorIds,

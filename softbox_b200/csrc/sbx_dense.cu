@@ -558,7 +558,7 @@ bool fused_prepare(sbx_dense_plan* p) {
     a.mTileSum = (int*)alloc(4 * (size_t)(a.tilesS + 1));
     a.cellSlot = (int*)alloc(4 * (size_t)a.C * FUSED_CELL_SLOTS);
     a.slotA = (int*)alloc(4 * nS * FUSED_ROW_SLOTS); a.slotB = (int*)alloc(4 * nS * FUSED_ROW_SLOTS);
-    a.slotM = (int*)alloc(4 * nS * FUSED_ROW_SLOTS);
+    a.slotM = (int*)alloc(4 * nS * FUSED_MOTOR_SLOTS);
     a.cellHead = (int*)alloc(4 * (size_t)a.C); a.cellNext = (int*)alloc(4 * (size_t)a.cap);
     size_t nLk = (size_t)std::max(a.nL, 1);
     a.headA = (int*)alloc(4 * nS); a.nextA = (int*)alloc(4 * nLk);
@@ -576,6 +576,7 @@ bool fused_prepare(sbx_dense_plan* p) {
     a.mIds = FUSED_MIDS;
     a.cellUse = FUSED_CELL_SLOTS;
     a.rowUse = FUSED_ROW_SLOTS;
+    a.mRowUse = FUSED_MOTOR_SLOTS;
     for (void* q : p->allocs)
         if (!q) return why("scratch allocation failed");
     return true;
@@ -852,6 +853,7 @@ extern "C" sbx_status sbx_dense_plan_test_caps(sbx_dense_plan* p, int32_t entCap
     p->fa.mCap = clampCap(motorCap, FUSED_MCAP);
     p->fa.mIds = clampCap(motorIds, FUSED_MIDS);
     p->fa.rowUse = clampCap(rowSlots, FUSED_ROW_SLOTS);
+    p->fa.mRowUse = clampCap(rowSlots, FUSED_MOTOR_SLOTS);
     p->fa.cellUse = clampCap(cellSlots, FUSED_CELL_SLOTS);
     return SBX_OK;
 }

@@ -52,6 +52,8 @@ struct RodSmem {
     float ent[FUSED_ENT_CAP][6];                  // the group's link CSR payloads, in CSR order
     int entOk[FUSED_ENT_CAP];                     // guard passed (active link)
     int mCnt[FUSED_MAX_ROD];                      // motors bound to each rod
+    int mLen[FUSED_MAX_ROD];                      // each rod's motor row length (histogram)
+    int mRaw[FUSED_MAX_ROD][FUSED_MOTOR_SLOTS];   // a short row's slots in arrival order
     int mIds[FUSED_MAX_ROD][FUSED_MIDS];          // their slots, ascending (the first FUSED_MIDS)
     float mPay[FUSED_MAX_ROD][FUSED_MCAP][6];     // the first FUSED_MCAP bond reactions
 };
@@ -621,7 +623,7 @@ __device__ void phase_bind(const FusedArgs& a, int t) {
             mot.capStats[myM] = cs;
             mot.nucleotideState[myM] = cycle_one(myM, mot.nucleotideState[myM], bs >= 0, mot.forceDotHist + 10 * myM,
                                                  mot.nucParams, t, sc.seed);
-            if (bs >= 0) listed += row_insert(a.cntM, a.slotM, FUSED_ROW_SLOTS, a.rowUse, a.headM, a.nextM, bs, myM);
+            if (bs >= 0) listed += row_insert(a.cntM, a.slotM, FUSED_MOTOR_SLOTS, a.mRowUse, a.headM, a.nextM, bs, myM);
         }
     }
     stat_add(a, ST_MOTOR_LIST, listed);
@@ -760,8 +762,9 @@ __device__ void phase_motors_links(const FusedArgs& a, FusedSmem& sm, int t) {
     }
     // on the CTAs without a unit (all CTAs when there are none): the chain joints of the
     // filaments (ChainBendingForceSystem's costly part, from this step's start poses; each
-    // joint once, by its lower-slot rod: item 2 i + side) and the filament Brownian forcing
-    // (one item per component and rod)
+    // joint once, by its lower-slot rod: item i computes rod i's first joint with a
+    // higher-slot neighbour, then its second one if it has two) and the filament Brownian
+    // forcing (one item per component and rod)
     const sbx_filament_store& fs = a.sc.fil;
     const sbx_rigid_body& fb = fs.body;
     int helpers = (int)gridDim.x - units, h0 = units;
@@ -769,16 +772,23 @@ __device__ void phase_motors_links(const FusedArgs& a, FusedSmem& sm, int t) {
     if ((int)blockIdx.x >= h0) {
         ChainJoint* J = reinterpret_cast<ChainJoint*>(a.joints);
         const int n = a.nSeg;
-        const int nJ = a.jointShare ? 2 * n : 0, total = nJ + 3 * n;
+        const int nJ = a.jointShare ? n : 0, total = nJ + 3 * n;
         for (int q = ((int)blockIdx.x - h0) * blockDim.x + threadIdx.x; q < total; q += helpers * blockDim.x) {
             if (q < nJ) {
-                const int i = q >> 1, side = q & 1;
-                const int nb = side == 0 ? fs.end2NbrSlot[i] : fs.end1NbrSlot[i];
-                if (nb > i) {
+                const int i = q;
+                const int s2 = fs.end2NbrSlot[i], s1 = fs.end1NbrSlot[i];
+                const int d2 = fs.end2NbrSide[i], d1 = fs.end1NbrSide[i];
+                if (s2 > i || s1 > i) {
                     ChainParams cp = chain_params(fs.chainParams);
-                    J[q] = chain_joint(cp, i, side, nb, side == 0 ? fs.end2NbrSide[i] : fs.end1NbrSide[i],
-                                       load_rod(n, i, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.bRotGam),
-                                       load_rod(n, nb, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.bRotGam));
+                    const RodGeom me = load_rod(n, i, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.bRotGam);
+                    const int side = s2 > i ? 0 : 1, nb = side == 0 ? s2 : s1;
+                    J[2 * i + side] = chain_joint(cp, i, side, nb, side == 0 ? d2 : d1, me,
+                                                  load_rod(n, nb, fb.coord, fb.uVec, fb.segLength, fb.bTransGam,
+                                                           fb.bRotGam));
+                    if (side == 0 && s1 > i)
+                        J[2 * i + 1] = chain_joint(cp, i, 1, s1, d1, me,
+                                                   load_rod(n, s1, fb.coord, fb.uVec, fb.segLength, fb.bTransGam,
+                                                            fb.bRotGam));
                 }
             } else {
                 const int r = q - nJ, c = r / n, i = r - c * n;
@@ -879,6 +889,8 @@ __device__ bool rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
             rs.off[c][r] = offSrc[c][g0 + r];
         }
     }
+    // the group's motor row lengths
+    for (int l = tid; l < cnt; l += blockDim.x) rs.mLen[l] = a.cntM[g0 + l];
     int i = g0 + tid;
     int s2 = -1, n2 = 0, s1 = -1, n1 = 0;
     if (tid < cnt) {
@@ -946,12 +958,26 @@ __device__ bool rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
         for (int k = 0; k < 6; k++) rs.ent[e][k] = ok ? v[k] : 0.f;
         rs.entOk[e] = ok;
     }
-    // each rod's bound motors (its row's slots and overflow list), sorted ascending = the
-    // motor CSR row order
+    // each rod's bound motors in ascending slot order (the motor CSR row order). A row held
+    // in its fixed slots (the common case): one thread per (row, slot) reads the slot, then,
+    // after the block barrier, puts it at its rank among the row's slots and stages its bond
+    // reaction. A longer row: one thread walks the row's slots and overflow list.
+    auto shortRow = [&](int nm) { return nm <= a.mRowUse && nm <= a.mIds; };
+    const int pairs = cnt * FUSED_MOTOR_SLOTS;
+    for (int k = tid; k < pairs; k += blockDim.x) {
+        const int l = k / FUSED_MOTOR_SLOTS, j = k - l * FUSED_MOTOR_SLOTS;
+        const int nm = rs.mLen[l];
+        if (j < nm && shortRow(nm)) rs.mRaw[l][j] = a.slotM[(size_t)(g0 + l) * FUSED_MOTOR_SLOTS + j];
+    }
     for (int l = first; l < cnt; l += blockDim.x) {
         int* ids = rs.mIds[l];
         const int r = g0 + l;
-        const int nm = a.cntM[r];
+        const int nm = rs.mLen[l];
+        if (shortRow(nm)) {
+            rs.mCnt[l] = nm;
+            stat_add(a, ST_MPAY_GLOBAL, nm - min(nm, a.mCap));
+            continue;
+        }
         int got = 0;
         auto put = [&](int m) {
             if (got < a.mIds) {
@@ -961,14 +987,14 @@ __device__ bool rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
             }
             got++;
         };
-        int sl[FUSED_ROW_SLOTS];
+        int sl[FUSED_MOTOR_SLOTS];
 #pragma unroll
-        for (int j = 0; j < FUSED_ROW_SLOTS; j++)
-            sl[j] = (j < nm && j < a.rowUse) ? a.slotM[(size_t)r * FUSED_ROW_SLOTS + j] : 0;
+        for (int j = 0; j < FUSED_MOTOR_SLOTS; j++)
+            sl[j] = (j < nm && j < a.mRowUse) ? a.slotM[(size_t)r * FUSED_MOTOR_SLOTS + j] : 0;
 #pragma unroll
-        for (int j = 0; j < FUSED_ROW_SLOTS; j++)
-            if (j < nm && j < a.rowUse) put(sl[j]);
-        if (nm > a.rowUse) {
+        for (int j = 0; j < FUSED_MOTOR_SLOTS; j++)
+            if (j < nm && j < a.mRowUse) put(sl[j]);
+        if (nm > a.mRowUse) {
             int it = 0;
             for (int m = a.headM[r]; m >= 0; m = a.nextM[m]) {
                 put(m);
@@ -983,6 +1009,22 @@ __device__ bool rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
         for (int q = 0; q < np; q++) {
             const float* p = sc.bondData + (int64_t)ids[q] * XB_STRIDE + 6;
             for (int k = 0; k < 6; k++) rs.mPay[l][q][k] = p[k];
+        }
+    }
+    __syncthreads();
+    for (int k = tid; k < pairs; k += blockDim.x) {
+        const int l = k / FUSED_MOTOR_SLOTS, j = k - l * FUSED_MOTOR_SLOTS;
+        const int nm = rs.mLen[l];
+        if (j >= nm || !shortRow(nm)) continue;
+        const int m = rs.mRaw[l][j];
+        int rank = 0;
+        for (int q = 0; q < nm; q++) rank += rs.mRaw[l][q] < m;
+        rs.mIds[l][rank] = m;
+        if (rank < a.mCap) {
+            const float* p = sc.bondData + (int64_t)m * XB_STRIDE + 6;
+            float v[6];
+            for (int c = 0; c < 6; c++) v[c] = p[c];
+            for (int c = 0; c < 6; c++) rs.mPay[l][rank][c] = v[c];
         }
     }
     __syncthreads();
@@ -1021,9 +1063,9 @@ __device__ bool rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
             int last = -1;
             for (int q = 0; q < nm; q++) {
                 int next = 0x7fffffff, it = 0;
-                for (int j = 0; j < FUSED_ROW_SLOTS; j++) {
-                    if (j >= nm || j >= a.rowUse) break;
-                    int m = a.slotM[(size_t)i * FUSED_ROW_SLOTS + j];
+                for (int j = 0; j < FUSED_MOTOR_SLOTS; j++) {
+                    if (j >= nm || j >= a.mRowUse) break;
+                    int m = a.slotM[(size_t)i * FUSED_MOTOR_SLOTS + j];
                     if (m > last && m < next) next = m;
                 }
                 for (int m = a.headM[i]; m >= 0 && it <= a.nM; m = a.nextM[m], it++)
@@ -1067,7 +1109,8 @@ __device__ void motor_csr(const FusedArgs& a, int h, int nH, unsigned long long&
     for (int m = h * blockDim.x + threadIdx.x; m < a.nM; m += nH * blockDim.x) {
         int bs = sc.mot.boundSeg[m];
         if (bs < 0) continue;
-        int pos = sc.segMotorOffsets[bs] + row_rank<FUSED_ROW_SLOTS>(a, a.cntM, a.slotM, a.rowUse, a.headM, a.nextM, bs, m, a.nM);
+        int pos = sc.segMotorOffsets[bs] +
+                  row_rank<FUSED_MOTOR_SLOTS>(a, a.cntM, a.slotM, a.mRowUse, a.headM, a.nextM, bs, m, a.nM);
         if (pos < a.nM) sc.segMotorMyo[pos] = m;
     }
 }

@@ -8,12 +8,13 @@ constexpr int FUSED_MAX_SUB = 120;    // sub-bodies per minifilament CTA (6 per 
 constexpr int FUSED_MAX_ROD = 64;     // segments per rod CTA (whole filaments)
 constexpr int FUSED_MAX_DPM = 16;     // dimers per minifilament (32 heads: one warp)
 constexpr int FUSED_ENT_CAP = 256;    // CSR payload entries a rod CTA stages in shared memory
-constexpr int FUSED_MCAP = 4;         // motor reactions per segment a rod CTA stages in shared memory
+constexpr int FUSED_MCAP = 16;        // motor reactions per segment a rod CTA stages in shared memory
 constexpr int FUSED_MIDS = 16;        // motor slots per segment a rod CTA sorts (more: repeated-minimum walk)
 constexpr int FUSED_CELL_SLOTS = 4;   // fixed slots per grid cell
 constexpr int FUSED_JOINT_BYTES = 64; // one chain joint (ChainJoint, padded)
 constexpr int FUSED_TERM_BYTES = 80;  // one position-only myosin term (MotorJoint, CoupleTerm, LeverTerm, TetherTerm)
-constexpr int FUSED_ROW_SLOTS = 4;    // fixed slots per segment (link A ends, link B ends, motors)
+constexpr int FUSED_ROW_SLOTS = 4;    // fixed slots per segment row of link A ends, of link B ends
+constexpr int FUSED_MOTOR_SLOTS = 16; // fixed slots per segment row of bound motors
 constexpr int FUSED_MIN_HELPERS = 16; // CTAs kept free of rod units in the rod phase
 
 struct FusedArgs {
@@ -52,7 +53,7 @@ struct FusedArgs {
     int nzT0, nzN;
     unsigned long long* stats;   // capacity-fallback counters (SBX_FUSED_STATS)
     int entCap, mCap, mIds;      // staging capacities in use (<= the compiled ones; lowered by a test hook)
-    int cellUse, rowUse;         // fixed row slots in use per cell / per segment row (<= the compiled ones)
+    int cellUse, rowUse, mRowUse;   // fixed row slots in use per cell / per link row / per motor row (<= the compiled ones)
 };
 
 // counters of sbx_dense_plan_fused_stats
