@@ -579,6 +579,9 @@ bool fused_prepare(sbx_dense_plan* p) {
     a.mRowUse = FUSED_MOTOR_SLOTS;
     for (void* q : p->allocs)
         if (!q) return why("scratch allocation failed");
+    // the error word and barrier counters are read by the plan status before any fused run
+    cudaMemsetAsync(a.err, 0, 16, st);
+    cudaMemsetAsync(a.bar, 0, 32, st);
     return true;
 }
 

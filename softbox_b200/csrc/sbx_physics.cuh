@@ -348,15 +348,17 @@ struct ChainJoint {
     int tvOK;
 };
 
-SBX_DEV ChainJoint chain_joint(const ChainParams& cp, int i, int side, int slot, int nside, const RodGeom& r,
-                               const RodGeom& nb) {
-    const double RAD2DEG = 180.0 / PI_D;
-    const double DEG2RAD = PI_D / 180.0;
-    ChainJoint J;
+// The joint's strain geometry: strain vector, its length and unit vector, and the two rods'
+// (clamped) direction cosines to it (ChainBendingForceSystem.java:165-190 / :250-276).
+struct JointGeom {
+    double strainDist, luX, luY, luZ, cosB1, cosB2;
+};
+
+SBX_DEV JointGeom chain_joint_geom(const ChainParams& cp, int i, int side, int slot, int nside, const RodGeom& r,
+                                   const RodGeom& nb) {
+    JointGeom G;
     double halfLen_um = 0.5 * r.len;
-    double lSqSelf = 1.0e-12 * r.len * r.len;
     double nHalfLen_um = 0.5 * nb.len;
-    double lSqN = 1.0e-12 * nb.len * nb.len;
     double ex, ey, ez, selfLpx, selfLpy, selfLpz;
     if (side == 0) {
         ex = r.cx + halfLen_um * r.ux; ey = r.cy + halfLen_um * r.uy; ez = r.cz + halfLen_um * r.uz;
@@ -377,46 +379,67 @@ SBX_DEV ChainJoint chain_joint(const ChainParams& cp, int i, int side, int slot,
     double lpx = owner ? selfLpx : nlpx, lpy = owner ? selfLpy : nlpy, lpz = owner ? selfLpz : nlpz;
     double pex = owner ? tipx : ex, pey = owner ? tipy : ey, pez = owner ? tipz : ez;
     double dx = pex - lpx, dy = pey - lpy, dz = pez - lpz;
-    double strainDist = sqrt(dx * dx + dy * dy + dz * dz);
-    double invStrain = (strainDist > 0.0) ? (1.0 / strainDist) : 0.0;
-    double luX = dx * invStrain, luY = dy * invStrain, luZ = dz * invStrain;
-
-    double cosB1 = r.ux * luX + r.uy * luY + r.uz * luZ;
+    G.strainDist = sqrt(dx * dx + dy * dy + dz * dz);
+    double invStrain = (G.strainDist > 0.0) ? (1.0 / G.strainDist) : 0.0;
+    G.luX = dx * invStrain; G.luY = dy * invStrain; G.luZ = dz * invStrain;
+    double cosB1 = r.ux * G.luX + r.uy * G.luY + r.uz * G.luZ;
     if (cosB1 > 1.0) cosB1 = 1.0;
     if (cosB1 < -1.0) cosB1 = -1.0;
-    double cosA1 = sbxm::sin(accurate_acos(cosB1));
-    double cosA1_2 = cosA1 * cosA1;
-    double moveC1 = cosB1 * cosB1 / r.bTGx + cosA1_2 / r.bTGy + lSqSelf * cosA1_2 / (4.0 * r.bRGy);
-    double cosB2 = nb.ux * luX + nb.uy * luY + nb.uz * luZ;
+    double cosB2 = nb.ux * G.luX + nb.uy * G.luY + nb.uz * G.luZ;
     if (cosB2 > 1.0) cosB2 = 1.0;
     if (cosB2 < -1.0) cosB2 = -1.0;
-    double cosA2 = sbxm::sin(accurate_acos(cosB2));
-    double cosA2_2 = cosA2 * cosA2;
-    double moveC2 = cosB2 * cosB2 / nb.bTGx + cosA2_2 / nb.bTGy + lSqN * cosA2_2 / (4.0 * nb.bRGy);
-    double denom = cp.dt * (moveC1 + moveC2);
-    J.forceMag = (denom > 0.0) ? (cp.fracMove * 1.0e-6 * strainDist / denom) : 0.0;
-    J.luX = luX; J.luY = luY; J.luZ = luZ;
+    G.cosB1 = cosB1;
+    G.cosB2 = cosB2;
+    return G;
+}
 
+// One rod's mobility term along the strain (the moveC of :191-200 / :277-286)
+SBX_DEV double chain_move_c(double cosB, const RodGeom& r) {
+    double lSq = 1.0e-12 * r.len * r.len;
+    double cosA = sbxm::sin(accurate_acos(cosB));
+    double cosA_2 = cosA * cosA;
+    return cosB * cosB / r.bTGx + cosA_2 / r.bTGy + lSq * cosA_2 / (4.0 * r.bRGy);
+}
+
+SBX_DEV double chain_force_mag(const ChainParams& cp, double strainDist, double moveC1, double moveC2) {
+    double denom = cp.dt * (moveC1 + moveC2);
+    return (denom > 0.0) ? (cp.fracMove * 1.0e-6 * strainDist / denom) : 0.0;
+}
+
+// The joint's torsion (:203-233 / :289-319): tvOK, 1/|tv| and the torsion magnitude
+SBX_DEV void chain_torsion(const ChainParams& cp, int side, int nside, const RodGeom& r, const RodGeom& nb, int* tvOK,
+                           double* invMag, double* torsionMag) {
+    const double RAD2DEG = 180.0 / PI_D;
+    const double DEG2RAD = PI_D / 180.0;
     double nxE = (nside == 0) ? nb.ux : -nb.ux, nyE = (nside == 0) ? nb.uy : -nb.uy, nzE = (nside == 0) ? nb.uz : -nb.uz;
     double mux = (side == 0) ? r.ux : -r.ux, muy = (side == 0) ? r.uy : -r.uy, muz = (side == 0) ? r.uz : -r.uz;
     double tvx = muy * nzE - muz * nyE, tvy = muz * nxE - mux * nzE, tvz = mux * nyE - muy * nxE;
     double tvMag2 = tvx * tvx + tvy * tvy + tvz * tvz;
-    J.tvOK = tvMag2 > 1.0e-30;
-    J.invMag = 0.0;
-    J.torsionMag = 0.0;
-    if (J.tvOK) {
-        J.invMag = 1.0 / sqrt(tvMag2);
+    *tvOK = tvMag2 > 1.0e-30;
+    *invMag = 0.0;
+    *torsionMag = 0.0;
+    if (*tvOK) {
+        *invMag = 1.0 / sqrt(tvMag2);
         double dotV = mux * nxE + muy * nyE + muz * nzE;
         if (dotV > 1.0) dotV = 1.0;
         if (dotV < -1.0) dotV = -1.0;
         double angTween = angle_from_sin_cos(tvMag2, dotV) * RAD2DEG;
         if (cp.springActive > 0.5) {
-            J.torsionMag = cp.fracMoveTorq * cp.spring * angTween;
+            *torsionMag = cp.fracMoveTorq * cp.spring * angTween;
         } else {
             double invBRG = 1.0 / r.bRGy + 1.0 / nb.bRGy;
-            J.torsionMag = cp.fracMoveTorq * DEG2RAD * angTween / (invBRG * cp.dt);
+            *torsionMag = cp.fracMoveTorq * DEG2RAD * angTween / (invBRG * cp.dt);
         }
     }
+}
+
+SBX_DEV ChainJoint chain_joint(const ChainParams& cp, int i, int side, int slot, int nside, const RodGeom& r,
+                               const RodGeom& nb) {
+    JointGeom G = chain_joint_geom(cp, i, side, slot, nside, r, nb);
+    ChainJoint J;
+    J.forceMag = chain_force_mag(cp, G.strainDist, chain_move_c(G.cosB1, r), chain_move_c(G.cosB2, nb));
+    J.luX = G.luX; J.luY = G.luY; J.luZ = G.luZ;
+    chain_torsion(cp, side, nside, r, nb, &J.tvOK, &J.invMag, &J.torsionMag);
     return J;
 }
 
