@@ -14,6 +14,7 @@
 #include "sbx_fused.cuh"
 #include "sbx_internal.cuh"
 #include "sbx_physics.cuh"
+#include "sbx_trace.h"
 
 #include <vector>
 
@@ -194,10 +195,13 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
     const sbx_rigid_body& fb = f.body;
     const int nSeg = fb.n, nM = mot.nMotors, nB = b.n, nBb = bb.n, nD = dim.nDimers;
     const bool xlOn = sc->xlinkOn && xl.nLinks > 0;
+    SBX_TRACE("sbx.dense.step");
+    TracePhases tr;
 
     SBX_LAUNCH(ctx, k_dense_set_counts, 1, 1, d_step, t, mot.counts, nM, nSeg, sc->seed, mini.bbCounts, nBb,
                sc->seedBb, f.counts, xlOn ? xl.counts : nullptr);
     // (i) binding
+    tr.next("sbx.dense.binding");
     CHK(sbx_motor_publish_head(ctx, nM, b.coord, b.uVec, b.segLength, mot.head, mot.uVec, mot.rodUVec));
     CHK(sbx_filament_publish(ctx, nSeg, fb.coord, fb.segLength, g.cap, g.center, g.boundingRadius, g.ownerStore,
                              g.ownerSlot, g.viewParams, f.filState));
@@ -238,6 +242,7 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
         CHK(sbx_nucleotide_cycle(ctx, nM, mot.nucleotideState, mot.boundSeg, mot.forceDotHist, mot.nucParams,
                                  mot.counts));
     // (iii)-(v) filaments, the part that needs nothing from the minifilament structure below:
+    tr.next("sbx.dense.filament_forces");
     // draws, crosslinker kernels and the crosslinker CSR builds. With a side stream it runs
     // concurrently with (ii); the streams join before the motor CSR, which reads the
     // cross-bridge payload. The row-ordered payload copies live in the main scratch.
@@ -284,6 +289,7 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
         }
     }
     // (ii) minifilament structure. A single network zeroes and draws in one pass per store
+    tr.next("sbx.dense.myosin");
     // (MechanicsFusion.forceBuild, the same values as the zero + Brownian pair)
     if (!bt) {
         CHK(force_build(ctx, nB, b.forceSum, b.torqueSum, b.randForce, b.randTorque, b.bTransGam, b.bRotGam,
@@ -318,6 +324,7 @@ sbx_status dense_sequence(sbx_ctx* ctx, const sbx_dense_scene* sc, const int* d_
     CHK(sbx_xbridge_bond_forces(ctx, nB, b.coord, b.uVec, b.yVec, b.bRotGam, nSeg, fb.coord, fb.uVec, fb.yVec,
                                 fb.bRotGam, fb.segLength, mot.boundSeg, mot.bindArc, mot.nucleotideState, sc->bondData,
                                 sc->xbParams));
+    tr.next("sbx.dense.integrate");
     // the motor-side tail (head forces, motor and backbone integration, force-dot registry)
     // reads no filament state and the filament tail below reads none of it: with a side stream
     // they run concurrently, joined at the end of the step
@@ -596,6 +603,7 @@ extern "C" sbx_status sbx_dense_step_unfused(sbx_ctx* ctx, const sbx_dense_scene
 // Captures one step (the sequence, then the step-counter advance) into the plan's graph,
 // replacing a previous capture; the supplied noise, when on, is part of the capture.
 static sbx_status capture_step(sbx_dense_plan* p) {
+    SBX_TRACE("sbx.dense.capture");
     sbx_ctx* ctx = p->ctx;
     cudaStreamSynchronize(ctx->stream);
     int64_t l0 = ctx->launches;
@@ -733,9 +741,11 @@ extern "C" sbx_status sbx_dense_plan_run(sbx_dense_plan* p, int32_t t0, int32_t 
             cudaMemsetAsync(a.err, 0, 16, ctx->stream);
             p->fused_dirty = false;
         }
+        SBX_TRACE("sbx.dense.fused_launch");
         return fused_launch(ctx, p->fa, p->fused_grid, t0, nsteps);
     }
     if (mode == 1) {
+        SBX_TRACE("sbx.dense.graph_replay");
         SBX_LAUNCH(ctx, k_step_set, 1, 1, p->d_step, t0);
         for (int k = 0; k < nsteps; k++) {
             if (cudaGraphLaunch(p->exec, ctx->stream) != cudaSuccess)
@@ -744,6 +754,7 @@ extern "C" sbx_status sbx_dense_plan_run(sbx_dense_plan* p, int32_t t0, int32_t 
         }
         return check_launch(ctx, "sbx_dense_plan_run");
     }
+    SBX_TRACE("sbx.dense.unfused");
     PlanScratch use(p);
     StepNoise sn{p->noise, p->noiseErr};
     for (int k = 0; k < nsteps; k++)

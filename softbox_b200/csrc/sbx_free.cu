@@ -10,6 +10,7 @@
 #include "../../include/softbox_b200.h"
 #include "sbx_internal.cuh"
 #include "sbx_physics.cuh"
+#include "sbx_trace.h"
 
 using namespace sbx;
 
@@ -64,6 +65,7 @@ __global__ void __launch_bounds__(128) k_free_rods(int n, float* coord, double* 
 
 extern "C" sbx_status sbx_free_rods_run(sbx_ctx* ctx, sbx_filament_store* fil, int32_t t0, int32_t nsteps,
                                         int32_t noise_mode, uint64_t philox_seed, const float* noise) {
+    SBX_TRACE("sbx.free.run");
     if (!ctx || !fil || nsteps < 0 || noise_mode < 0 || noise_mode > 2) return SBX_EINVAL;
     const sbx_rigid_body& b = fil->body;
     int n = b.n;
