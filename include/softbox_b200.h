@@ -68,6 +68,15 @@ sbx_status sbx_ctx_sync(sbx_ctx* ctx);
 int64_t sbx_ctx_launch_count(sbx_ctx* ctx);
 /* bytes of device scratch the context holds (grows on demand, never shrinks; -1 for NULL) */
 int64_t sbx_ctx_scratch_bytes(sbx_ctx* ctx);
+/* 1 in the index-checking debug build (libsoftbox_b200_check.so, compiled with -DSBX_CHECK),
+ * 0 in the normal build. */
+int32_t sbx_check_build(void);
+/* Index checks of the debug build: the number of data-dependent indices the kernels found
+ * outside the array they index (and skipped) since the last reset, the first one's site
+ * (1 chain neighbour, 2 bound segment, 3 link end, 4 CSR list entry, 5 grid cell, 6 motor
+ * slot, 7 reach-walk entry, 8 CSR position; 0 when none) and its value; reset != 0 clears
+ * them. Synchronous (reads device counters). The normal build reports zeros. */
+sbx_status sbx_check_report(int64_t* count, int32_t* site, int64_t* index, int32_t reset);
 
 /* DataTransferMode analogues: FIRST_EXECUTION / EVERY_EXECUTION uploads and
  * UNDER_DEMAND pulls are plain async copies on the context stream. */

@@ -5,7 +5,11 @@ IEEE division and square root, no flush-to-zero. With them every float/double
 operation in the kernels is one IEEE round-to-nearest step, which is what lets the
 kernels reproduce the reference's (and the CPU oracle's) bits.
 
-    python -m softbox_b200.build [--force] [--verbose-ptxas]
+    python -m softbox_b200.build [--force] [--verbose-ptxas] [--check]
+
+--check builds the index-checking debug library (libsoftbox_b200_check.so, -DSBX_CHECK): its
+kernels test every data-dependent index against the array it indexes, count and skip bad
+ones (sbx_check_report). Select it at load time with SBX_LIB=check.
 """
 import os
 import shutil
@@ -17,6 +21,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libsoftbox_b200.so")
+LIB_CHECK = os.path.join(OUT_DIR, "libsoftbox_b200_check.so")
 SOURCES = ["sbx_systems.cu", "sbx_sort.cu", "sbx_dense.cu", "sbx_free.cu", "sbx_fused.cu", "sbx_noalloc.cu", "sbx_form.cu", "sbx_turnover.cu", "sbx_batch.cu", "sbx_obs.cu", "sbx_mlp.cu", "sbx_turnover_batch.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FP_FLAGS = ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
@@ -35,19 +40,22 @@ def _deps():
     return files
 
 
-def up_to_date():
-    if not os.path.exists(LIB):
+def up_to_date(lib=LIB):
+    if not os.path.exists(lib):
         return False
-    t = os.path.getmtime(LIB)
+    t = os.path.getmtime(lib)
     return all(os.path.getmtime(f) <= t for f in _deps())
 
 
-def build(force=False, verbose_ptxas=False):
-    if not force and up_to_date():
-        return LIB
+def build(force=False, verbose_ptxas=False, check=False):
+    lib = LIB_CHECK if check else LIB
+    if not force and up_to_date(lib):
+        return lib
     os.makedirs(OUT_DIR, exist_ok=True)
     cmd = [nvcc_path(), "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC", "-lineinfo"] + ARCH + FP_FLAGS
-    cmd += ["-I" + os.path.join(ROOT, "include"), "-o", LIB + ".tmp"]
+    if check:
+        cmd += ["-DSBX_CHECK"]
+    cmd += ["-I" + os.path.join(ROOT, "include"), "-o", lib + ".tmp"]
     if verbose_ptxas:
         cmd += ["-Xptxas", "-v"]
     cmd += [os.path.join(CSRC, s) for s in SOURCES]
@@ -61,10 +69,10 @@ def build(force=False, verbose_ptxas=False):
         raise RuntimeError("nvcc failed")
     if verbose_ptxas:
         sys.stderr.write(r.stderr)
-    os.replace(LIB + ".tmp", LIB)
-    return LIB
+    os.replace(lib + ".tmp", lib)
+    return lib
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose_ptxas="--verbose-ptxas" in sys.argv)
-    print(LIB)
+    print(build(force="--force" in sys.argv, verbose_ptxas="--verbose-ptxas" in sys.argv,
+                check="--check" in sys.argv))

@@ -167,6 +167,7 @@ __device__ __forceinline__ void brownian_component(const FusedArgs& a, const sbx
 __device__ __forceinline__ int list_rank(const FusedArgs& a, int head, const int* next, int self, int bound) {
     int r = 0, it = 0;
     for (int j = head; j >= 0; j = next[j]) {
+        if (!SBX_IDX_OK(j, bound, CK_LIST_ENTRY)) break;
         r += j < self;
         if (++it > bound) {
             atomicOr(a.err, ERR_LIST);
@@ -272,8 +273,10 @@ __device__ void phase_publish_bin(const FusedArgs& a, int t) {
         } else {
             int k = i - cap;
             int la = xl.linkFilA[k], lb = xl.linkFilB[k];
-            if (la >= 0) overLink += row_insert(a.cntA, a.slotA, FUSED_ROW_SLOTS, a.rowUse, a.headA, a.nextA, la, k);
-            if (lb >= 0) overLink += row_insert(a.cntB, a.slotB, FUSED_ROW_SLOTS, a.rowUse, a.headB, a.nextB, lb, k);
+            if (la >= 0 && SBX_IDX_OK(la, nSeg, CK_LINK_END))
+                overLink += row_insert(a.cntA, a.slotA, FUSED_ROW_SLOTS, a.rowUse, a.headA, a.nextA, la, k);
+            if (lb >= 0 && SBX_IDX_OK(lb, nSeg, CK_LINK_END))
+                overLink += row_insert(a.cntB, a.slotB, FUSED_ROW_SLOTS, a.rowUse, a.headB, a.nextB, lb, k);
         }
     }
     stat_add(a, ST_CELL_LIST, overCell);
@@ -293,6 +296,7 @@ __device__ void link_unbind(const FusedArgs& a, int t, int firstWarp) {
     for (int k = (w - firstWarp) * 32 + (threadIdx.x & 31); k < a.nL; k += (nw - firstWarp) * 32) {
         int la = xl.linkFilA[k], lb = xl.linkFilB[k];
         int state = xl.linkState[k];
+        if (!SBX_IDX_OK_OR_NONE(la, a.nSeg, CK_LINK_END) || !SBX_IDX_OK_OR_NONE(lb, a.nSeg, CK_LINK_END)) continue;
         if (a.xlUnbind && state >= 0 &&
             unbind_one(k, a.nSeg, fb.uVec, fb.end1, la, lb, xl.loc1[k], xl.loc2[k], xl.strainHist, xl.strainPlace,
                        xl.offParams, t, sc.seed)) {
@@ -460,13 +464,14 @@ __device__ void phase_place(const FusedArgs& a) {
     for (int i = gtid(); i < total; i += gthreads()) {
         if (i < a.cap) {
             int c = g.bodyCell[i];
-            if (c < 0) continue;
+            if (c < 0 || !SBX_IDX_OK(c, a.C, CK_CELL)) continue;
             int rank = row_rank<FUSED_CELL_SLOTS>(a, a.cntCell, a.cellSlot, a.cellUse, a.cellHead, a.cellNext, c, i, a.cap);
+            if (!SBX_IDX_OK(g.gridCellOffsets[c] + rank, a.cap, CK_CSR_POS)) continue;
             g.gridCellContents[g.gridCellOffsets[c] + rank] = i;
             // segment endpoints in cell order for the reach walk: within a cell the segments
             // (slots below nSeg) precede the motor heads, so a segment's rank among the
             // segments of its cell equals its rank in the cell
-            if (i < nSeg) {
+            if (i < nSeg && SBX_IDX_OK(a.segCellOff[c] + rank, nSeg, CK_CSR_POS)) {
                 int q = a.segCellOff[c] + rank;
                 a.segE1[q] = make_float4(fb.end1[i], fb.end1[nSeg + i], fb.end1[2 * nSeg + i], __int_as_float(i));
                 a.segE2[q] = make_float4(fb.end2[i], fb.end2[nSeg + i], fb.end2[2 * nSeg + i], 0.f);
@@ -474,6 +479,7 @@ __device__ void phase_place(const FusedArgs& a) {
         } else {
             int k = i - a.cap;
             int la = xl.linkFilA[k], lb = xl.linkFilB[k];
+            if (!SBX_IDX_OK_OR_NONE(la, nSeg, CK_LINK_END) || !SBX_IDX_OK_OR_NONE(lb, nSeg, CK_LINK_END)) continue;
             if (la >= 0)
                 xl.segIdxA[xl.segOffsetsA[la] +
                            row_rank<FUSED_ROW_SLOTS>(a, a.cntA, a.slotA, a.rowUse, a.headA, a.nextA, la, k, a.nL)] = k;
@@ -541,11 +547,13 @@ __device__ int warp_reach_bind(const FusedArgs& a, int lane, float mx, float my,
 #pragma unroll
             for (int r = 1; r < 9; r++)
                 if (k >= preR[r]) idx = rsR[r] + (k - preR[r]);
-            e1 = a.segE1[idx];
-            e2 = a.segE2[idx];
-            d = reach_test_dist_sq(mx, my, mz, mux, muy, muz, rux, ruy, ruz, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z, tol,
-                                   align);
-            pass = d >= 0.f;
+            if (SBX_IDX_OK(idx, a.nSeg, CK_REACH_ENTRY)) {
+                e1 = a.segE1[idx];
+                e2 = a.segE2[idx];
+                d = reach_test_dist_sq(mx, my, mz, mux, muy, muz, rux, ruy, ruz, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z,
+                                       tol, align);
+                pass = d >= 0.f;
+            }
         }
         const unsigned mask = __ballot_sync(0xffffffffu, pass);
         const int pos = cnt + __popc(mask & lower);
@@ -623,7 +631,8 @@ __device__ void phase_bind(const FusedArgs& a, int t) {
             mot.capStats[myM] = cs;
             mot.nucleotideState[myM] = cycle_one(myM, mot.nucleotideState[myM], bs >= 0, mot.forceDotHist + 10 * myM,
                                                  mot.nucParams, t, sc.seed);
-            if (bs >= 0) listed += row_insert(a.cntM, a.slotM, FUSED_MOTOR_SLOTS, a.mRowUse, a.headM, a.nextM, bs, myM);
+            if (bs >= 0 && SBX_IDX_OK(bs, a.nSeg, CK_BOUND_SEG))
+                listed += row_insert(a.cntM, a.slotM, FUSED_MOTOR_SLOTS, a.mRowUse, a.headM, a.nextM, bs, myM);
         }
     }
     stat_add(a, ST_MOTOR_LIST, listed);
@@ -654,8 +663,10 @@ __device__ void mini_unit(const FusedArgs& a, MiniSmem& ms, int u, int t) {
             // CrossBridgeSystem.bondForces, then the head's sums: joint 1, then the bond
             int m = m0 + tid;
             float out[XB_STRIDE];
+            int bs = mot.boundSeg[m];
+            if (!SBX_IDX_OK_OR_NONE(bs, nSeg, CK_BOUND_SEG)) bs = -1;
             bond_one(m, nB, mb.coord, mb.uVec, mb.yVec, mb.bRotGam, nSeg, fb.coord, fb.uVec, fb.yVec, fb.bRotGam,
-                     fb.segLength, mot.boundSeg[m], mot.bindArc[m], mot.nucleotideState[m], sc.xbParams, out);
+                     fb.segLength, bs, mot.bindArc[m], mot.nucleotideState[m], sc.xbParams, out);
             for (int k = 0; k < XB_STRIDE; k++) sc.bondData[m * XB_STRIDE + k] = out[k];
             int hl = 3 * tid + 2;
             double f[3] = {0.0, 0.0, 0.0}, tq[3] = {0.0, 0.0, 0.0};
@@ -741,6 +752,7 @@ __device__ void link_item(const FusedArgs& a, int k) {
     const sbx_rigid_body& fb = sc.fil.body;
     float out[XL_STRIDE];
     int la = xl.linkFilA[k], lb = xl.linkFilB[k];
+    if (!SBX_IDX_OK_OR_NONE(la, a.nSeg, CK_LINK_END) || !SBX_IDX_OK_OR_NONE(lb, a.nSeg, CK_LINK_END)) return;
     link_forces_one(k, a.nSeg, fb.coord, fb.uVec, fb.end1, fb.bTransGam, la, lb, xl.loc1[k], xl.loc2[k], a.cntAct,
                     xl.xlParams, out);
     for (int j = 0; j < XL_STRIDE; j++) xl.xlinkData[k * XL_STRIDE + j] = out[j];
@@ -776,8 +788,10 @@ __device__ void phase_motors_links(const FusedArgs& a, FusedSmem& sm, int t) {
         for (int q = ((int)blockIdx.x - h0) * blockDim.x + threadIdx.x; q < total; q += helpers * blockDim.x) {
             if (q < nJ) {
                 const int i = q;
-                const int s2 = fs.end2NbrSlot[i], s1 = fs.end1NbrSlot[i];
+                int s2 = fs.end2NbrSlot[i], s1 = fs.end1NbrSlot[i];
                 const int d2 = fs.end2NbrSide[i], d1 = fs.end1NbrSide[i];
+                if (!SBX_IDX_OK_OR_NONE(s2, n, CK_NEIGHBOUR)) s2 = -1;
+                if (!SBX_IDX_OK_OR_NONE(s1, n, CK_NEIGHBOUR)) s1 = -1;
                 if (s2 > i || s1 > i) {
                     ChainParams cp = chain_params(fs.chainParams);
                     const RodGeom me = load_rod(n, i, fb.coord, fb.uVec, fb.segLength, fb.bTransGam, fb.bRotGam);
@@ -813,8 +827,8 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 // FP64 row sum of CSR c for local rod l, from the fetched entries (global past the cap);
 // the arithmetic of csr_gather_row
 __device__ __forceinline__ void gather_staged(const RodSmem& rs, int c, int l, int eBase, int entCap, const int* list,
-                                              const float* payload, int stride, int poff, const int* guard,
-                                              double f[3], double t[3]) {
+                                              int nItems, const float* payload, int stride, int poff,
+                                              const int* guard, double f[3], double t[3]) {
     f[0] = f[1] = f[2] = 0.0;
     t[0] = t[1] = t[2] = 0.0;
     int k0 = rs.off[c][0];
@@ -826,6 +840,7 @@ __device__ __forceinline__ void gather_staged(const RodSmem& rs, int c, int l, i
             p = rs.ent[e];
         } else {
             int li = list[k];
+            if (!SBX_IDX_OK(li, nItems, CK_LIST_ENTRY)) continue;
             if (guard && guard[li] < 0) continue;
             p = payload + (int64_t)li * stride + poff;
         }
@@ -896,6 +911,9 @@ __device__ bool rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
     if (tid < cnt) {
         s2 = f.end2NbrSlot[i]; n2 = f.end2NbrSide[i];
         s1 = f.end1NbrSlot[i]; n1 = f.end1NbrSide[i];
+        // a rod group holds whole filaments: both neighbours are staged rows of the group
+        if (s2 >= 0 && !SBX_IDX_OK(s2 - g0, cnt, CK_NEIGHBOUR)) s2 = -1;
+        if (s1 >= 0 && !SBX_IDX_OK(s1 - g0, cnt, CK_NEIGHBOUR)) s1 = -1;
     }
     if (tma) {
         // bounded wait on the transaction barrier, one verdict per CTA: the phase completed
@@ -946,11 +964,15 @@ __device__ bool rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
         bool ok;
         if (e < eA) {
             int li = xl.segIdxA[rs.off[0][0] + e];
-            ok = xl.linkState[li] >= 0;
+            const bool inb = SBX_IDX_OK(li, a.nL, CK_LIST_ENTRY);
+            if (!inb) li = 0;                     // (index-check build) stage zeros for it
+            ok = inb && xl.linkState[li] >= 0;
             p = xl.xlinkData + (int64_t)li * XL_STRIDE;
         } else {
             int li = xl.segIdxB[rs.off[1][0] + (e - eA)];
-            ok = xl.linkState[li] >= 0;
+            const bool inb = SBX_IDX_OK(li, a.nL, CK_LIST_ENTRY);
+            if (!inb) li = 0;
+            ok = inb && xl.linkState[li] >= 0;
             p = xl.xlinkData + (int64_t)li * XL_STRIDE + 6;
         }
         float v[6];
@@ -967,7 +989,10 @@ __device__ bool rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
     for (int k = tid; k < pairs; k += blockDim.x) {
         const int l = k / FUSED_MOTOR_SLOTS, j = k - l * FUSED_MOTOR_SLOTS;
         const int nm = rs.mLen[l];
-        if (j < nm && shortRow(nm)) rs.mRaw[l][j] = a.slotM[(size_t)(g0 + l) * FUSED_MOTOR_SLOTS + j];
+        if (j < nm && shortRow(nm)) {
+            const int m = a.slotM[(size_t)(g0 + l) * FUSED_MOTOR_SLOTS + j];
+            rs.mRaw[l][j] = SBX_IDX_OK(m, a.nM, CK_MOTOR_SLOT) ? m : 0;
+        }
     }
     for (int l = first; l < cnt; l += blockDim.x) {
         int* ids = rs.mIds[l];
@@ -980,6 +1005,7 @@ __device__ bool rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
         }
         int got = 0;
         auto put = [&](int m) {
+            if (!SBX_IDX_OK(m, a.nM, CK_MOTOR_SLOT)) m = 0;
             if (got < a.mIds) {
                 int q = got;
                 while (q > 0 && ids[q - 1] > m) { ids[q] = ids[q - 1]; q--; }
@@ -997,6 +1023,7 @@ __device__ bool rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
         if (nm > a.mRowUse) {
             int it = 0;
             for (int m = a.headM[r]; m >= 0; m = a.nextM[m]) {
+                if (!SBX_IDX_OK(m, a.nM, CK_MOTOR_SLOT)) break;
                 put(m);
                 if (++it > a.nM) { atomicOr(a.err, ERR_LIST); break; }
             }
@@ -1042,9 +1069,11 @@ __device__ bool rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
         for (int k = 0; k < 3; k++) { F[k] = (float)(0.0f + fd[k]); T[k] = (float)(0.0f + td[k]); }
         double gf[3], gt[3];
         if (a.xlOn) {
-            gather_staged(rs, 0, tid, 0, a.entCap, xl.segIdxA, xl.xlinkData, XL_STRIDE, 0, xl.linkState, gf, gt);
+            gather_staged(rs, 0, tid, 0, a.entCap, xl.segIdxA, a.nL, xl.xlinkData, XL_STRIDE, 0, xl.linkState, gf,
+                          gt);
             for (int k = 0; k < 3; k++) { F[k] = (float)(F[k] + gf[k]); T[k] = (float)(T[k] + gt[k]); }
-            gather_staged(rs, 1, tid, eA, a.entCap, xl.segIdxB, xl.xlinkData, XL_STRIDE, 6, xl.linkState, gf, gt);
+            gather_staged(rs, 1, tid, eA, a.entCap, xl.segIdxB, a.nL, xl.xlinkData, XL_STRIDE, 6, xl.linkState, gf,
+                          gt);
             for (int k = 0; k < 3; k++) { F[k] = (float)(F[k] + gf[k]); T[k] = (float)(T[k] + gt[k]); }
         }
         // CrossBridgeSystem.segGather: FP64 sums of the bound motors' reactions, ascending slot
@@ -1066,10 +1095,13 @@ __device__ bool rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
                 for (int j = 0; j < FUSED_MOTOR_SLOTS; j++) {
                     if (j >= nm || j >= a.mRowUse) break;
                     int m = a.slotM[(size_t)i * FUSED_MOTOR_SLOTS + j];
+                    if (!SBX_IDX_OK(m, a.nM, CK_MOTOR_SLOT)) continue;
                     if (m > last && m < next) next = m;
                 }
-                for (int m = a.headM[i]; m >= 0 && it <= a.nM; m = a.nextM[m], it++)
+                for (int m = a.headM[i]; m >= 0 && it <= a.nM; m = a.nextM[m], it++) {
+                    if (!SBX_IDX_OK(m, a.nM, CK_MOTOR_SLOT)) break;
                     if (m > last && m < next) next = m;
+                }
                 if (next == 0x7fffffff) {
                     atomicOr(a.err, ERR_LIST);
                     break;
@@ -1108,7 +1140,7 @@ __device__ void motor_csr(const FusedArgs& a, int h, int nH, unsigned long long&
     if (!counter_sync(a.bar + 1, hTarget, nH, a.err)) return;
     for (int m = h * blockDim.x + threadIdx.x; m < a.nM; m += nH * blockDim.x) {
         int bs = sc.mot.boundSeg[m];
-        if (bs < 0) continue;
+        if (bs < 0 || !SBX_IDX_OK(bs, a.nSeg, CK_BOUND_SEG)) continue;
         int pos = sc.segMotorOffsets[bs] +
                   row_rank<FUSED_MOTOR_SLOTS>(a, a.cntM, a.slotM, a.mRowUse, a.headM, a.nextM, bs, m, a.nM);
         if (pos < a.nM) sc.segMotorMyo[pos] = m;
@@ -1234,3 +1266,5 @@ int fused_max_blocks_per_sm() {
 }
 
 const void* fused_kernel_ptr() { return (const void*)k_dense_fused; }
+
+SBX_CHECK_EXPORT(fused)

@@ -42,6 +42,49 @@ static inline int blocks(int64_t n, int bs = 256) {
         (ctx)->launches++;                                              \
     } while (0)
 
+// ---------------------------------------------------------------- index checks (debug build)
+// Built with -DSBX_CHECK (python -m softbox_b200.build --check: libsoftbox_b200_check.so),
+// the kernels test every data-dependent index they follow (a chain neighbour, a bound
+// segment, a link end, a CSR list entry, a grid cell, a motor slot, a reach-walk entry)
+// against the length of the array it indexes. A bad index is counted, the first one's site
+// and value are kept, and the access is skipped; sbx_check_report returns them. In the
+// normal build every test is the constant `true` and compiles away.
+enum SbxCheckSite {
+    CK_NEIGHBOUR = 1, CK_BOUND_SEG = 2, CK_LINK_END = 3, CK_LIST_ENTRY = 4, CK_CELL = 5, CK_MOTOR_SLOT = 6,
+    CK_REACH_ENTRY = 7, CK_CSR_POS = 8
+};
+#ifdef SBX_CHECK
+static __device__ unsigned long long sbx_check_count;   // per translation unit
+static __device__ unsigned long long sbx_check_first;   // (site << 32) | index of the first bad index
+__device__ __forceinline__ bool sbx_idx_ok(long long i, long long n, int site) {
+    if (i >= 0 && i < n) return true;
+    if (atomicAdd(&sbx_check_count, 1ULL) == 0ULL)
+        sbx_check_first = ((unsigned long long)(unsigned)site << 32) | (unsigned long long)(unsigned)i;
+    return false;
+}
+#define SBX_IDX_OK(i, n, site) sbx_idx_ok((long long)(i), (long long)(n), (site))
+// each translation unit with checked kernels exports its counters
+#define SBX_CHECK_EXPORT(tu)                                                                        \
+    extern "C" int sbx_check_collect_##tu(unsigned long long* count, unsigned long long* first,     \
+                                          int reset) {                                              \
+        if (cudaMemcpyFromSymbol(count, sbx_check_count, sizeof(*count)) != cudaSuccess ||          \
+            cudaMemcpyFromSymbol(first, sbx_check_first, sizeof(*first)) != cudaSuccess)           \
+            return -1;                                                                              \
+        if (reset) {                                                                                \
+            const unsigned long long z = 0;                                                         \
+            if (cudaMemcpyToSymbol(sbx_check_count, &z, sizeof(z)) != cudaSuccess ||                \
+                cudaMemcpyToSymbol(sbx_check_first, &z, sizeof(z)) != cudaSuccess)                  \
+                return -1;                                                                          \
+        }                                                                                           \
+        return 0;                                                                                   \
+    }
+#else
+#define SBX_IDX_OK(i, n, site) true
+#define SBX_CHECK_EXPORT(tu)
+#endif
+// an index that may be negative (meaning "none") or must lie in [0, n)
+#define SBX_IDX_OK_OR_NONE(i, n, site) ((i) < 0 || SBX_IDX_OK((i), (n), (site)))
+
 // ---------------------------------------------------------------- counting sort
 // Stable counting sort of items [0, n) by key (keys < 0 are skipped; keys >= nRows are
 // skipped and set *errFlag) into row CSR form:

@@ -93,6 +93,43 @@ extern "C" int64_t sbx_ctx_launch_count(sbx_ctx* ctx) { return ctx ? ctx->launch
 
 extern "C" int64_t sbx_ctx_scratch_bytes(sbx_ctx* ctx) { return ctx ? (int64_t)ctx->scratch_bytes : -1; }
 
+#ifdef SBX_CHECK
+extern "C" int sbx_check_collect_systems(unsigned long long*, unsigned long long*, int);
+extern "C" int sbx_check_collect_fused(unsigned long long*, unsigned long long*, int);
+#endif
+
+extern "C" int32_t sbx_check_build(void) {
+#ifdef SBX_CHECK
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+extern "C" sbx_status sbx_check_report(int64_t* count, int32_t* site, int64_t* index, int32_t reset) {
+    if (!count || !site || !index) return SBX_EINVAL;
+    *count = 0;
+    *site = 0;
+    *index = 0;
+#ifdef SBX_CHECK
+    // the translation units with checked kernels, each with its own counters
+    int (*collect[])(unsigned long long*, unsigned long long*, int) = {sbx_check_collect_systems,
+                                                                      sbx_check_collect_fused};
+    for (auto fn : collect) {
+        unsigned long long c = 0, f = 0;
+        if (fn(&c, &f, reset) != 0) return SBX_ECUDA;
+        if (c && *count == 0) {
+            *site = (int32_t)(f >> 32);
+            *index = (int64_t)(int32_t)(unsigned)(f & 0xffffffffULL);
+        }
+        *count += (int64_t)c;
+    }
+#else
+    (void)reset;
+#endif
+    return SBX_OK;
+}
+
 sbx_status fail(sbx_ctx* ctx, sbx_status code, const std::string& msg) {
     if (ctx) ctx->err = msg;
     return code;
@@ -577,6 +614,8 @@ __global__ void __launch_bounds__(CHAIN_THREADS, 3) k_chain(int n, const float* 
     int s2 = -1, d2 = 0, s1 = -1, d1 = 0;
     if (i < n) {
         s2 = e2s[i]; d2 = e2d[i]; s1 = e1s[i]; d1 = e1d[i];
+        if (!SBX_IDX_OK_OR_NONE(s2, n, CK_NEIGHBOUR)) s2 = -1;
+        if (!SBX_IDX_OK_OR_NONE(s1, n, CK_NEIGHBOUR)) s1 = -1;
         if (s2 > i) {
             ChainParams cp = chain_params(chainParams);
             js[2 * tid] = chain_joint(cp, i, 0, s2, d2, load_rod(n, i, coord, uVec, segLength, bTG, bRG),
@@ -1039,7 +1078,9 @@ __global__ void k_bond(int nB, const float* mC, const float* mU, const float* mY
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= nB / 3) return;
     float out[XB_STRIDE];
-    bond_one(m, nB, mC, mU, mY, mBRG, nSeg, fC, fU, fY, fBRG, fLen, boundSeg[m], bindArc[m], nuc[m], xb, out);
+    int s = boundSeg[m];
+    if (!SBX_IDX_OK_OR_NONE(s, nSeg, CK_BOUND_SEG)) s = -1;
+    bond_one(m, nB, mC, mU, mY, mBRG, nSeg, fC, fU, fY, fBRG, fLen, s, bindArc[m], nuc[m], xb, out);
     for (int k = 0; k < XB_STRIDE; k++) bondData[m * XB_STRIDE + k] = out[k];
 }
 
@@ -1166,9 +1207,10 @@ extern "C" sbx_status sbx_xbridge_brute_gather(sbx_ctx* ctx, int32_t nSeg, int32
 }
 
 // ============================================================================ crosslinkers
-__global__ void k_xl_count(int nLinks, const int* state, const int* A, const int* B, int* count) {
+__global__ void k_xl_count(int nLinks, int nSeg, const int* state, const int* A, const int* B, int* count) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nLinks || state[k] < 0) return;
+    if (!SBX_IDX_OK(A[k], nSeg, CK_LINK_END) || !SBX_IDX_OK(B[k], nSeg, CK_LINK_END)) return;
     atomicAdd(&count[A[k]], 1);
     atomicAdd(&count[B[k]], 1);
 }
@@ -1179,7 +1221,7 @@ extern "C" sbx_status sbx_xlink_count_active(sbx_ctx* ctx, int32_t nLinks, const
     if (nSeg > 0 && cudaMemsetAsync(count, 0, sizeof(int) * nSeg, ctx->stream) != cudaSuccess)
         return fail(ctx, SBX_ECUDA, "sbx_xlink_count_active: memset");
     if (nLinks == 0) return SBX_OK;
-    SBX_LAUNCH(ctx, k_xl_count, blocks(nLinks), 256, nLinks, state, A, B, count);
+    SBX_LAUNCH(ctx, k_xl_count, blocks(nLinks), 256, nLinks, nSeg, state, A, B, count);
     return check_launch(ctx, "sbx_xlink_count_active");
 }
 
@@ -1188,6 +1230,7 @@ __global__ void k_xl_forces(int nSeg, const float* fC, const float* fU, const fl
                             const int* ct, float* xd, const float* xp) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nLinks) return;
+    if (!SBX_IDX_OK_OR_NONE(A[k], nSeg, CK_LINK_END) || !SBX_IDX_OK_OR_NONE(B[k], nSeg, CK_LINK_END)) return;
     float out[XL_STRIDE];
     link_forces_one(k, nSeg, fC, fU, fE1, fBTG, A[k], B[k], loc1[k], loc2[k], ct, xp, out);
     for (int j = 0; j < XL_STRIDE; j++) xd[k * XL_STRIDE + j] = out[j];
@@ -1209,6 +1252,7 @@ __global__ void k_xl_torsion(int nSeg, const float* fU, int nLinks, const int* A
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nLinks) return;
     if (tp[1] < 0.5f) return;
+    if (!SBX_IDX_OK_OR_NONE(A[k], nSeg, CK_LINK_END) || !SBX_IDX_OK_OR_NONE(B[k], nSeg, CK_LINK_END)) return;
     link_torsion_one(k, nSeg, fU, A[k], B[k], state[k], orient[k], hist, place, xd, tp[0]);
 }
 
@@ -1261,6 +1305,7 @@ __global__ void k_xl_unbind(int nSeg, const float* fU, const float* fE1, int nLi
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nLinks) return;
     if (state[k] < 0) return;
+    if (!SBX_IDX_OK_OR_NONE(A[k], nSeg, CK_LINK_END) || !SBX_IDX_OK_OR_NONE(B[k], nSeg, CK_LINK_END)) return;
     if (unbind_one(k, nSeg, fU, fE1, A[k], B[k], loc1[k], loc2[k], hist, place, op, counts[1], counts[2]))
         state[k] = LINK_FREE;
 }
@@ -1439,3 +1484,5 @@ extern "C" sbx_status sbx_deflection_pin_endpoints(sbx_ctx* ctx, int32_t n, floa
     SBX_LAUNCH(ctx, k_pin_endpoints, blocks(nPins), 256, n, coord, uVec, segLength, nPins, pinSeg, pinEnd, pinAnchor);
     return check_launch(ctx, "sbx_deflection_pin_endpoints");
 }
+
+SBX_CHECK_EXPORT(systems)

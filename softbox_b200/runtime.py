@@ -12,7 +12,9 @@ import re
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 HEADER = os.path.join(ROOT, "include", "softbox_b200.h")
-LIB_PATH = os.path.join(HERE, "_lib", "libsoftbox_b200.so")
+# SBX_LIB=check loads the index-checking debug build (python -m softbox_b200.build --check)
+LIB_PATH = os.path.join(HERE, "_lib", "libsoftbox_b200_check.so" if os.environ.get("SBX_LIB") == "check"
+                        else "libsoftbox_b200.so")
 
 STATUS = {0: "SBX_OK", -1: "SBX_EINVAL", -2: "SBX_ECUDA", -3: "SBX_EOVERFLOW", -4: "SBX_ETIMEOUT",
           -5: "SBX_ENOMEM", -6: "SBX_ENONFINITE", -7: "SBX_ESTATE"}

@@ -39,3 +39,21 @@ def test_ranges_reach_an_injected_tool(tmp_path):
     pushes, pops, names = out.read_text().split(" ", 2)
     assert int(pushes) == 1 and int(pops) == 1, (pushes, pops)
     assert names.strip().rstrip(",") == "sbx.free.run"
+
+
+def test_check_build_library():
+    """The index-checking debug twin is built beside the library, flags itself and exports
+    the same C ABI (its counters read as zeros through the normal build)."""
+    import ctypes as C
+    from softbox_b200.runtime import LIB, LIB_PATH, parse_header
+    check = os.path.join(os.path.dirname(LIB_PATH), "libsoftbox_b200_check.so")
+    assert os.path.exists(check)
+    lib = C.CDLL(check)
+    for name in parse_header():
+        getattr(lib, name)
+    lib.sbx_check_build.restype = C.c_int32
+    assert lib.sbx_check_build() == 1
+    assert LIB.sbx_check_build() == 0
+    c, s, i = C.c_int64(5), C.c_int32(5), C.c_int64(5)
+    assert LIB.sbx_check_report(C.byref(c), C.byref(s), C.byref(i), 0) == 0
+    assert (c.value, s.value, i.value) == (0, 0, 0)
