@@ -62,7 +62,8 @@ sbx_status sbx_ctx_set_stream(sbx_ctx* ctx, void* stream);
 void* sbx_ctx_stream(sbx_ctx* ctx);
 /* Waits for the context's stream. Also reports (SBX_EINVAL, then cleared) an input that a
  * kernel since the last sync found outside its documented range and skipped: a CSR key at
- * or past its row count (sbx_csr_build*, sbx_grid_build). */
+ * or past its row count (sbx_csr_build*, sbx_grid_build); and (SBX_ETIMEOUT, then cleared) a
+ * staged reach walk whose bulk copies did not complete in time. */
 sbx_status sbx_ctx_sync(sbx_ctx* ctx);
 /* number of kernels this context has launched (for launch accounting) */
 int64_t sbx_ctx_launch_count(sbx_ctx* ctx);
@@ -239,6 +240,22 @@ sbx_status sbx_fusion_grid_reachable(sbx_ctx* ctx, const float* head, const floa
                                      const int32_t* gridCellOffsets, const float* cellEnd1,
                                      const float* cellEnd2, int32_t* motorReachSeg, int32_t* motorReachCount,
                                      const float* kinParams, int32_t nM);
+/* The same walk (same reach lists and counts) with each tile of 64 x-cells of one y-row,
+ * every z, handled by one block that stages the tile's neighbourhood in shared memory: the
+ * cell offsets of the 3*nZ rows around it and their cell-ordered endpoint pairs (bulk copies);
+ * the heads binned in the tile then walk shared memory. Takes the grid dimensions on the
+ * host, the grid contents and owners (to find the tile's heads), bodyCell, cap and
+ * publishParams (heads in no cell take the plain walk). nZ > 16 falls back to
+ * sbx_fusion_grid_reachable. A bulk-copy wait past one second is reported as SBX_ETIMEOUT by
+ * the next sbx_ctx_sync (the tile's heads then take the plain walk). */
+sbx_status sbx_fusion_grid_reachable_staged(sbx_ctx* ctx, const float* head, const float* uVec,
+                                            const float* rodUVec, const float* gridParams,
+                                            const int32_t* gridDims, int32_t nX, int32_t nY, int32_t nZ,
+                                            const int32_t* gridCellOffsets, const int32_t* gridCellContents,
+                                            const int32_t* ownerStore, const int32_t* ownerSlot,
+                                            const int32_t* bodyCell, int32_t cap, const int32_t* publishParams,
+                                            const float* cellEnd1, const float* cellEnd2, int32_t* motorReachSeg,
+                                            int32_t* motorReachCount, const float* kinParams, int32_t nM);
 /* BindingDetectionSystem.bruteReachable (BindingDetectionSystem.java:260-283) */
 sbx_status sbx_binding_brute_reachable(sbx_ctx* ctx, const float* head, const float* uVec,
                                        const float* rodUVec, int32_t nSeg, const float* segEnd1,

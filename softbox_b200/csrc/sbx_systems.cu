@@ -83,7 +83,9 @@ extern "C" sbx_status sbx_ctx_sync(sbx_ctx* ctx) {
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return fail(ctx, SBX_ECUDA, std::string("sync: ") + cudaGetErrorString(e));
     if (ctx->err_host && *(volatile int*)ctx->err_host) {
+        const int w = *(volatile int*)ctx->err_host;
         *(volatile int*)ctx->err_host = 0;
+        if (w == 2) return fail(ctx, SBX_ETIMEOUT, "a staged reach walk's bulk copies did not complete in time");
         return fail(ctx, SBX_EINVAL, "a CSR key was >= its row count (the item was skipped)");
     }
     return SBX_OK;
@@ -980,6 +982,249 @@ extern "C" sbx_status sbx_fusion_grid_reachable(sbx_ctx* ctx, const float* head,
                reinterpret_cast<const float4*>(cellEnd1), reinterpret_cast<const float4*>(cellEnd2), reachSeg,
                reachCount, kp);
     return check_launch(ctx, "sbx_fusion_grid_reachable");
+}
+
+// ---------------------------------------------------------------- reach walk over staged cell rows
+// BindingDetectionSystem.gridReachable (BindingDetectionSystem.java:161-227) for the heads
+// binned in one tile of the grid (REACH_TILE_X consecutive x-cells of one y-row, every z),
+// with the tile's neighbourhood staged in shared memory: the cell offsets of the 3 nZ rows
+// around it (coalesced loads) and their cell-ordered endpoint pairs (cp.async.bulk, one
+// copy per row and array, completion on an mbarrier; no multicast, source in this GPU's
+// memory). Each head's walk then reads shared memory only, in the order of
+// grid_reach_walk_cells (the same rows, cells and entries): the same lists and counts. A
+// tile whose neighbourhood exceeds the staging capacity, a head past the tile's head list
+// and a head that is not binned (the blocks after the tiles look for those) take
+// grid_reach_walk_cells itself. A bulk-copy wait longer than one second sets bit 1 of the
+// context's error word (reported as SBX_ETIMEOUT by sbx_ctx_sync), waits once more for the
+// copies and leaves the tile's heads to the global walk.
+constexpr int REACH_TILE_X = 64, REACH_ZMAX = 16, REACH_CAP_E = 768, REACH_HCAP = 256;
+constexpr unsigned long long REACH_WAIT_NS = 1000000000ULL;
+
+static size_t reach_tile_smem(int nZ) {
+    return 2 * sizeof(float4) * REACH_CAP_E + sizeof(int) * ((size_t)3 * nZ * (REACH_TILE_X + 3) + 3 * nZ + 1) +
+           sizeof(int) * REACH_HCAP;
+}
+
+__device__ __forceinline__ bool reach_bulk_wait(unsigned long long* mbar, unsigned phase) {
+    unsigned mb = (unsigned)__cvta_generic_to_shared(mbar);
+    unsigned done = 0, it = 0;
+    unsigned long long t0 = 0;
+    while (!done) {
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(done) : "r"(mb), "r"(phase) : "memory");
+        if (!done && (++it & 15u) == 0) {
+            unsigned long long now;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+            if (t0 == 0) t0 = now;
+            else if (now - t0 > REACH_WAIT_NS) break;
+        }
+    }
+    return done != 0;
+}
+
+__global__ void __launch_bounds__(128) k_reach_tiles(int nM, const float* head, const float* uVec,
+                                                     const float* rodUVec, const float* gp, const int* gd, int nX,
+                                                     int nY, int nZ, const int* offsets, const int* contents,
+                                                     const int* ownerStore, const int* ownerSlot,
+                                                     const int* bodyCell, int cap, const int* publishParams,
+                                                     const float4* cellE1, const float4* cellE2, int* reachSeg,
+                                                     int* reachCount, const float* kp, int* errWord) {
+    extern __shared__ __align__(16) unsigned char rsm[];
+    float4* sE1 = reinterpret_cast<float4*>(rsm);
+    float4* sE2 = sE1 + REACH_CAP_E;
+    const int W = REACH_TILE_X + 3, R = 3 * nZ;
+    int* sOff = reinterpret_cast<int*>(sE2 + REACH_CAP_E);   // [R][W]: the staged rows' cell offsets
+    int* sBase = sOff + R * W;                                 // [R + 1]: each row's first staged entry
+    int* sHead = sBase + R + 1;                                // the tile's heads
+    __shared__ int sNHead, sStaged;
+    __shared__ __align__(8) unsigned long long mbar;
+    const float tol = kp[7], align = kp[8];
+    const int tilesX = (nX + REACH_TILE_X - 1) / REACH_TILE_X, nTiles = tilesX * nY;
+    if ((int)blockIdx.x >= nTiles) {
+        // heads that are in no grid cell: the global walk
+        const int m = ((int)blockIdx.x - nTiles) * blockDim.x + threadIdx.x;
+        if (m >= nM) return;
+        const int b = publishParams[0] + m;
+        if (b >= 0 && b < cap && bodyCell[b] >= 0) return;
+        reachCount[m] = grid_reach_walk_cells(m, nM, head, uVec, rodUVec, gp, gd, offsets, cellE1, cellE2,
+                                              reachSeg + (int64_t)m * MAX_CAND, tol, align);
+        return;
+    }
+    const int ty = blockIdx.x / tilesX, tx0 = (blockIdx.x - ty * tilesX) * REACH_TILE_X;
+    const int tx1 = min(tx0 + REACH_TILE_X, nX) - 1;             // the tile's last x-cell
+    const int xa = max(tx0 - 1, 0), xb = min(tx1 + 1, nX - 1);    // staged x-cells
+    const int nc = xb - xa + 2;                                   // offsets per staged row
+    const int nXY = nX * nY;
+    // (1) the staged rows' cell offsets (rows outside the grid hold zeros: no entries), eight
+    // loads per thread in flight together
+    for (int q0 = 0; q0 < R * nc; q0 += 8 * 128) {
+        int v[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int q = q0 + j * 128 + (int)threadIdx.x;
+            const int r = q / nc, k = q - r * nc;
+            const int yy = ty - 1 + r / nZ, zz = r - (r / nZ) * nZ;
+            v[j] = (q < R * nc && yy >= 0 && yy < nY) ? offsets[xa + k + yy * nX + zz * nXY] : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int q = q0 + j * 128 + (int)threadIdx.x;
+            if (q < R * nc) sOff[(q / nc) * W + (q - (q / nc) * nc)] = v[j];
+        }
+    }
+    if (threadIdx.x == 0) {
+        sNHead = 0;
+        unsigned mb = (unsigned)__cvta_generic_to_shared(&mbar);
+        asm volatile("mbarrier.init.shared.b64 [%0], 1;\n" :: "r"(mb) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    // (2) where each row lands in the staging buffer; the expected bytes before any copy
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int r = 0; r < R; r++) {
+            sBase[r] = acc;
+            acc += sOff[r * W + nc - 1] - sOff[r * W];
+        }
+        sBase[R] = acc;
+        const bool staged = acc > 0 && acc <= REACH_CAP_E;
+        sStaged = staged;
+        if (staged) {
+            unsigned mb = (unsigned)__cvta_generic_to_shared(&mbar);
+            asm volatile("mbarrier.arrive.expect_tx.shared.b64 _, [%0], %1;\n" :: "r"(mb), "r"((unsigned)acc * 32u)
+                         : "memory");
+        }
+    }
+    __syncthreads();
+    const bool staged = sStaged != 0;
+    // (3) one bulk copy per staged row and array
+    if (staged) {
+        for (int q = threadIdx.x; q < 2 * R; q += blockDim.x) {
+            const int r = q >> 1, n = sOff[r * W + nc - 1] - sOff[r * W];
+            if (n <= 0) continue;
+            float4* dst = ((q & 1) ? sE2 : sE1) + sBase[r];
+            const float4* src = ((q & 1) ? cellE2 : cellE1) + sOff[r * W];
+            unsigned d = (unsigned)__cvta_generic_to_shared(dst), mb = (unsigned)__cvta_generic_to_shared(&mbar);
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                         :: "r"(d), "l"(src), "r"((unsigned)n * 16u), "r"(mb) : "memory");
+        }
+    }
+    // (4) meanwhile, the heads binned in the tile's own cells (staged rows y = ty): the rows'
+    // entries as one sequence, four per thread in flight together
+    int ePre[REACH_ZMAX + 1];
+    ePre[0] = 0;
+    for (int z = 0; z < nZ; z++) {
+        const int r = nZ + z;
+        ePre[z + 1] = ePre[z] + sOff[r * W + (tx1 + 1 - xa)] - sOff[r * W + (tx0 - xa)];
+    }
+    const int nOwn = ePre[nZ];
+    for (int i0 = 0; i0 < nOwn; i0 += 4 * 128) {
+        int slot[4], own[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int i = i0 + j * 128 + (int)threadIdx.x;
+            slot[j] = -1;
+            if (i < nOwn) {
+                int z = 0;
+                while (i >= ePre[z + 1]) z++;
+                slot[j] = contents[sOff[(nZ + z) * W + (tx0 - xa)] + (i - ePre[z])];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) own[j] = slot[j] >= 0 ? ownerStore[slot[j]] : STORE_NONE;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if (own[j] != STORE_MOTOR) continue;
+            const int m = ownerSlot[slot[j]];
+            const int h = atomicAdd(&sNHead, 1);
+            if (h < REACH_HCAP) {
+                sHead[h] = m;
+            } else {
+                reachCount[m] = grid_reach_walk_cells(m, nM, head, uVec, rodUVec, gp, gd, offsets, cellE1, cellE2,
+                                                      reachSeg + (int64_t)m * MAX_CAND, tol, align);
+            }
+        }
+    }
+    bool ok = true;
+    if (staged) {
+        ok = __syncthreads_or(reach_bulk_wait(&mbar, 0)) != 0;
+        if (!ok && threadIdx.x == 0) {
+            *(volatile int*)errWord = 2;
+            reach_bulk_wait(&mbar, 0);     // the copies may still be landing: one more bounded wait
+        }
+    }
+    __syncthreads();
+    // (5) the walks: the staged rows when the tile is staged, else the global walk
+    const int nh = min(sNHead, REACH_HCAP);
+    for (int h = threadIdx.x; h < nh; h += blockDim.x) {
+        const int m = sHead[h];
+        int* outSlice = reachSeg + (int64_t)m * MAX_CAND;
+        const float hx = head[m], hy = head[nM + m];
+        const int hcx = cell_coord(hx, gp[0], gp[4], nX), hcy = cell_coord(hy, gp[1], gp[4], nY);
+        // (a head binned here lies in the tile's cells; anything else takes the global walk)
+        if (!staged || !ok || hcy != ty || hcx < tx0 || hcx > tx1) {
+            reachCount[m] = grid_reach_walk_cells(m, nM, head, uVec, rodUVec, gp, gd, offsets, cellE1, cellE2,
+                                                  outSlice, tol, align);
+            continue;
+        }
+        const float mx = head[m], my = head[nM + m], mz = head[2 * nM + m];
+        const float mux = uVec[m], muy = uVec[nM + m], muz = uVec[2 * nM + m];
+        const float rux = rodUVec[m], ruy = rodUVec[nM + m], ruz = rodUVec[2 * nM + m];
+        const int cx = cell_coord(mx, gp[0], gp[4], nX), cy = cell_coord(my, gp[1], gp[4], nY),
+                  cz = cell_coord(mz, gp[2], gp[4], nZ);
+        const int x0 = max(cx - 1, 0), x1 = min(cx + 1, nX - 1);
+        const int y0 = max(cy - 1, 0), y1 = min(cy + 1, nY - 1);
+        const int z0 = max(cz - 1, 0), z1 = min(cz + 1, nZ - 1);
+        int out = 0;
+        for (int rr = 0; rr < 9; rr++) {
+            const int zz = z0 + rr / 3, yy = y0 + rr % 3;
+            if (zz > z1 || yy > y1) continue;
+            const int r = (yy - (ty - 1)) * nZ + zz;           // the staged row (cy == ty)
+            const int* ro = sOff + r * W;
+            const int b0 = ro[x0 - xa], b1 = ro[x1 + 1 - xa];
+            const int base = sBase[r] - ro[0];
+            for (int e = b0; e < b1; e++) {
+                const float4 a1 = sE1[base + e], a2 = sE2[base + e];
+                const int sg = __float_as_int(a1.w);
+                if (sg < 0) continue;
+                const float d = reach_test_dist_sq(mx, my, mz, mux, muy, muz, rux, ruy, ruz, a1.x, a1.y, a1.z, a2.x,
+                                                   a2.y, a2.z, tol, align);
+                if (d >= 0.f) {
+                    if (out < MAX_CAND) outSlice[out] = sg;
+                    out++;
+                }
+            }
+        }
+        reachCount[m] = out;
+    }
+}
+
+extern "C" sbx_status sbx_fusion_grid_reachable_staged(
+    sbx_ctx* ctx, const float* head, const float* uVec, const float* rodUVec, const float* gp, const int32_t* gd,
+    int32_t nX, int32_t nY, int32_t nZ, const int32_t* gridCellOffsets, const int32_t* gridCellContents,
+    const int32_t* ownerStore, const int32_t* ownerSlot, const int32_t* bodyCell, int32_t cap,
+    const int32_t* publishParams, const float* cellEnd1, const float* cellEnd2, int32_t* reachSeg,
+    int32_t* reachCount, const float* kp, int32_t nM) {
+    SBX_REQUIRE(ctx && nM >= 0 && nX > 0 && nY > 0 && nZ > 0 && cap >= 0 &&
+                (nM == 0 || (head && uVec && rodUVec && gp && gd && gridCellOffsets && gridCellContents && ownerStore &&
+                             ownerSlot && bodyCell && publishParams && cellEnd1 && cellEnd2 && reachSeg &&
+                             reachCount && kp)));
+    if (nM == 0) return SBX_OK;
+    if (nZ > REACH_ZMAX)
+        return sbx_fusion_grid_reachable(ctx, head, uVec, rodUVec, gp, gd, gridCellOffsets, cellEnd1, cellEnd2,
+                                         reachSeg, reachCount, kp, nM);
+    const size_t smem = reach_tile_smem(nZ);
+    if (cudaFuncSetAttribute(k_reach_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return fail(ctx, SBX_ECUDA, "sbx_fusion_grid_reachable_staged: shared memory attribute");
+    const int64_t tiles = (int64_t)((nX + REACH_TILE_X - 1) / REACH_TILE_X) * nY;
+    const int64_t grid = tiles + (nM + 127) / 128;
+    if (grid > 0x7fffffff) return fail(ctx, SBX_EINVAL, "sbx_fusion_grid_reachable_staged: grid too large");
+    k_reach_tiles<<<(unsigned)grid, 128, smem, ctx->stream>>>(
+        nM, head, uVec, rodUVec, gp, gd, nX, nY, nZ, gridCellOffsets, gridCellContents, ownerStore, ownerSlot, bodyCell,
+        cap, publishParams, reinterpret_cast<const float4*>(cellEnd1), reinterpret_cast<const float4*>(cellEnd2),
+        reachSeg, reachCount, kp, ctx->err_dev);
+    ctx->launches++;
+    return check_launch(ctx, "sbx_fusion_grid_reachable_staged");
 }
 
 __global__ void k_brute_reachable(int nM, const float* head, const float* uVec, const float* rodUVec, int nSeg,

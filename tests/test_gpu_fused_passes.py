@@ -17,7 +17,7 @@ import numpy as np
 import pytest
 
 from helpers import assert_same, oracle_dense_run, small_dense
-from softbox_b200 import device as D
+from softbox_b200 import device as D, scenes
 
 pytestmark = pytest.mark.gpu
 
@@ -149,3 +149,73 @@ def test_cell_endpoint_walk_equals_grid_reachable(orc_dm, warm):
         k = min(int(hc[i]), want.shape[1])
         assert_same(want[i, :k], hs[i, :k], f"reachSeg row {i}")
     assert hc.sum() > 0
+
+
+def test_staged_tile_walk_equals_grid_reachable(orc_dm, warm):
+    """sbx_fusion_grid_reachable_staged (one block per tile of cells, the neighbourhood staged in
+    shared memory by bulk copies) gives the oracle's reach lists and counts."""
+    sc = copy.deepcopy(warm)
+    m, g, fb = sc["mot"], sc["grid"], sc["fil"]["body"]
+    nM, nSeg, cap = m["nMotors"], fb["n"], int(g["cap"])
+    d = D.to_device({"m": m, "g": g, "e1": fb["end1"], "e2": fb["end2"]})
+    dm, dg = d["m"], d["g"]
+    orc_dm.grid_reachable(nM, m["head"], m["uVec"], m["rodUVec"], nSeg, fb["end1"], fb["end2"], g["gridParams"],
+                          g["gridDims"], g["gridCellOffsets"], g["gridCellContents"], g["ownerStore"],
+                          g["ownerSlot"], g["reachSeg"], g["reachCount"], m["kinParams"])
+    ce1 = torch.zeros(4 * cap, dtype=torch.float32, device="cuda")
+    ce2 = torch.zeros(4 * cap, dtype=torch.float32, device="cuda")
+    dg["reachSeg"].fill_(-7)
+    dg["reachCount"].fill_(-7)
+    c = _ctx()
+    c("sbx_grid_cell_endpoints", cap, int(g["totalCells"]), dg["gridCellOffsets"], dg["gridCellContents"],
+      dg["ownerStore"], dg["ownerSlot"], nSeg, d["e1"], d["e2"], ce1, ce2)
+    nX, nY, nZ = (int(v) for v in g["gridDims"][:3])
+    c("sbx_fusion_grid_reachable_staged", dm["head"], dm["uVec"], dm["rodUVec"], dg["gridParams"], dg["gridDims"],
+      nX, nY, nZ, dg["gridCellOffsets"], dg["gridCellContents"], dg["ownerStore"], dg["ownerSlot"], dg["bodyCell"],
+      cap, dm["publishParams"], ce1, ce2, dg["reachSeg"], dg["reachCount"], dm["kinParams"], nM)
+    c.sync()
+    hc = D.to_host(dg["reachCount"])
+    assert_same(g["reachCount"], hc, "reachCount")
+    hs = D.to_host(dg["reachSeg"]).reshape(nM, -1)
+    want = g["reachSeg"].reshape(nM, -1)
+    for i in range(nM):
+        k = min(int(hc[i]), want.shape[1])
+        assert_same(want[i, :k], hs[i, :k], f"reachSeg row {i}")
+    assert hc.sum() > 0
+
+
+def test_staged_tile_walk_at_scale_equals_plain_walk():
+    """200,000 rods (about 18,000 tiles) after one step: the staged-tile walk and the per-head
+    walk over the same grid and endpoints give the same reach lists and counts."""
+    from softbox_b200.engine import DenseNetwork
+    sc = scenes.dense_contractile(scenes.dense_scaled(200000))
+    net = DenseNetwork(sc)
+    net.run(0, 1, mode="graph")
+    assert net.status() == 0
+    d = net.dev
+    m, g, fb = d["mot"], d["grid"], d["fil"]["body"]
+    nM, nSeg, cap = sc["mot"]["nMotors"], sc["fil"]["body"]["n"], int(sc["grid"]["cap"])
+    nX, nY, nZ = (int(v) for v in sc["grid"]["gridDims"][:3])
+    ce1 = torch.zeros(4 * cap, dtype=torch.float32, device="cuda")
+    ce2 = torch.zeros(4 * cap, dtype=torch.float32, device="cuda")
+    c = net.ctx
+    c("sbx_grid_cell_endpoints", cap, int(sc["grid"]["totalCells"]), g["gridCellOffsets"], g["gridCellContents"],
+      g["ownerStore"], g["ownerSlot"], nSeg, fb["end1"], fb["end2"], ce1, ce2)
+    out = []
+    for staged in (False, True):
+        seg = torch.full((nM * 256,), -7, dtype=torch.int32, device="cuda")
+        cnt = torch.full((nM,), -7, dtype=torch.int32, device="cuda")
+        if staged:
+            c("sbx_fusion_grid_reachable_staged", m["head"], m["uVec"], m["rodUVec"], g["gridParams"], g["gridDims"],
+              nX, nY, nZ, g["gridCellOffsets"], g["gridCellContents"], g["ownerStore"], g["ownerSlot"],
+              g["bodyCell"], cap, m["publishParams"], ce1, ce2, seg, cnt, m["kinParams"], nM)
+        else:
+            c("sbx_fusion_grid_reachable", m["head"], m["uVec"], m["rodUVec"], g["gridParams"], g["gridDims"],
+              g["gridCellOffsets"], ce1, ce2, seg, cnt, m["kinParams"], nM)
+        c.sync()
+        out.append((cnt.cpu().numpy(), seg.cpu().numpy().reshape(nM, 256)))
+    (c0, s0), (c1, s1) = out
+    assert_same(c0, c1, "reachCount")
+    assert c0.sum() > 0
+    filled = np.arange(256)[None, :] < np.minimum(c0, 256)[:, None]
+    assert_same(s0[filled], s1[filled], "reachSeg")
