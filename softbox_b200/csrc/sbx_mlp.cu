@@ -4,12 +4,15 @@
 // bias gradients, Adam).
 //
 // GEMM: C[M x N] = A[M x K] . B[N x K]^T, A and B row-major BF16 (K contiguous, "K-major"),
-// K <= 256. One CTA (4 warps) per 128-row tile of C and up to 256 columns: the A and B tiles
-// are staged in shared memory in the canonical no-swizzle K-major layout (8 x 16-byte core
-// matrices; core matrix (row group g, k group c) at ((g * Kp/8) + c) * 128 bytes), one
-// thread issues K/16 MMAs (M = 128, N = the tile width) into TMEM and commits them to an
-// mbarrier, and each warp reads its 32 accumulator lanes (rows) back with tcgen05.ld for the
-// epilogue. blockIdx.z selects an independent problem (an ensemble member) by strides.
+// K <= 256. One CTA (12 warps) per SM keeps its B tile (up to 256 columns) in shared memory
+// and loops over 128-row tiles of C: the A and B tiles are staged in shared memory in the
+// canonical no-swizzle K-major layout (8 x 16-byte core matrices; core matrix (row group g,
+// k group c) at ((g * Kp/8) + c) * 128 bytes), one thread issues K/16 MMAs (M = 128, N = the
+// tile width) into TMEM and commits them to an mbarrier, and the epilogue reads the
+// accumulators back with tcgen05.ld: warp w takes TMEM lanes (rows) 32 (w mod 4) .. +31 and
+// every third 16-column chunk from chunk w / 4, adds the bias, applies GELU and writes each
+// row's 16 values with vector stores (the transposed output by lanes along the rows).
+// blockIdx.z selects an independent problem (an ensemble member) by strides.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -21,10 +24,9 @@ namespace {
 constexpr int MT = 128;              // rows of a C tile (the MMA's M)
 constexpr int NT = 256;              // max columns of a C tile (the MMA's N)
 constexpr int KMAX = 256;            // max contraction length
-constexpr int GEMM_THREADS = 128;
+constexpr int GEMM_THREADS = 384;   // 12 warps: 4 TMEM lane quarters x 3 column groups
+constexpr int COL_GROUPS = GEMM_THREADS / 128;
 constexpr long long WAIT_NS = 1000000000LL;
-constexpr int STG_LD = 17;                           // padded row of the epilogue staging (floats)
-constexpr int STG_BYTES = 4 * 2 * 32 * STG_LD * 4;   // 4 warps x (values, activations) x 32 rows
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
@@ -112,7 +114,6 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm(GemmArgs g) {
     char* sB = smem + MT * Kp * 2;
     unsigned long long* mbar = reinterpret_cast<unsigned long long*>(sB + NT * Kp * 2);
     unsigned* tmemSlot = reinterpret_cast<unsigned*>(mbar + 1);
-    float* stage_base = reinterpret_cast<float*>(reinterpret_cast<char*>(mbar) + 16);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned ncolsAlloc = 32;
     while ((int)ncolsAlloc < Np) ncolsAlloc <<= 1;
@@ -133,10 +134,10 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm(GemmArgs g) {
     __nv_bfloat16* out = g.out ? g.out + z * g.sOut : nullptr;
     __nv_bfloat16* outT = g.outT ? g.outT + z * g.sOutT : nullptr;
     float* outF = g.outF ? g.outF + z * g.sOutF : nullptr;
-    // per-warp staging of a 32-row x 16-column chunk, so that the row-major outputs are
-    // written by lanes spanning columns (two rows of 16 per store instruction)
-    float* stV = stage_base + warp * (2 * 32 * STG_LD);
-    float* stA = stV + 32 * STG_LD;
+    // 16-byte row stores where every row start is 16-byte aligned
+    const bool vecOut = out && (g.ldo % 8 == 0) && (((uintptr_t)out & 15) == 0);
+    const bool vecOutF = outF && (g.ldf % 4 == 0) && (((uintptr_t)outF & 15) == 0);
+    const int quarter = warp & 3, cgroup = warp >> 2;
     bool ok = true;
     unsigned tmem = 0;
 
@@ -186,10 +187,10 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm(GemmArgs g) {
         if (!ok && threadIdx.x == 0 && g.err) atomicOr(g.err, 1);
         asm volatile("tcgen05.fence::after_thread_sync;");
         if (ok) {
-            const int row = m0 + warp * 32 + lane;
-            for (int c0 = 0; c0 < Np; c0 += 16) {
+            const int row = m0 + quarter * 32 + lane;
+            for (int c0 = cgroup * 16; c0 < Np; c0 += COL_GROUPS * 16) {
                 unsigned r[16];
-                unsigned taddr = tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0;
+                unsigned taddr = tmem + ((unsigned)(quarter * 32) << 16) + (unsigned)c0;
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
                     "[%16];"
@@ -198,27 +199,50 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm(GemmArgs g) {
                       "=r"(r[15])
                     : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;");
+                const int nb = n0 + c0;                    // this chunk's first column
+                float v[16], a[16];
+#pragma unroll
                 for (int j = 0; j < 16; j++) {
-                    int n = n0 + c0 + j;
-                    float v = __uint_as_float(r[j]);
-                    if (bias && n < g.N) v += bias[n];
-                    float a = g.act ? gelu(v) : v;
-                    stV[lane * STG_LD + j] = v;
-                    stA[lane * STG_LD + j] = a;
-                    if (outT && row < g.M && n < g.N) outT[(long long)n * g.ldt + row] = __float2bfloat16_rn(a);
+                    v[j] = __uint_as_float(r[j]);
+                    if (bias && nb + j < g.N) v[j] += bias[nb + j];
+                    a[j] = g.act ? gelu(v[j]) : v[j];
                 }
-                __syncwarp();
-                if (out || outF) {
-                    const int col = lane & 15, n = n0 + c0 + col;
-                    for (int rr = lane >> 4; rr < 32; rr += 2) {
-                        const int orow = m0 + warp * 32 + rr;
-                        if (orow < g.M && n < g.N) {
-                            if (outF) outF[(long long)orow * g.ldf + n] = stV[rr * STG_LD + col];
-                            if (out) out[(long long)orow * g.ldo + n] = __float2bfloat16_rn(stA[rr * STG_LD + col]);
+                if (outT) {
+#pragma unroll
+                    for (int j = 0; j < 16; j++)
+                        if (row < g.M && nb + j < g.N) outT[(long long)(nb + j) * g.ldt + row] = __float2bfloat16_rn(a[j]);
+                }
+                if (row < g.M) {
+                    const bool full = nb + 16 <= g.N;
+                    if (out) {
+                        __nv_bfloat16* o = out + (long long)row * g.ldo + nb;
+                        if (vecOut && full) {
+                            unsigned w[8];
+#pragma unroll
+                            for (int j = 0; j < 8; j++) {
+                                __nv_bfloat162 h = __floats2bfloat162_rn(a[2 * j], a[2 * j + 1]);
+                                w[j] = *reinterpret_cast<unsigned*>(&h);
+                            }
+                            reinterpret_cast<uint4*>(o)[0] = make_uint4(w[0], w[1], w[2], w[3]);
+                            reinterpret_cast<uint4*>(o)[1] = make_uint4(w[4], w[5], w[6], w[7]);
+                        } else {
+                            for (int j = 0; j < 16; j++)
+                                if (nb + j < g.N) o[j] = __float2bfloat16_rn(a[j]);
+                        }
+                    }
+                    if (outF) {
+                        float* o = outF + (long long)row * g.ldf + nb;
+                        if (vecOutF && full) {
+#pragma unroll
+                            for (int j = 0; j < 4; j++)
+                                reinterpret_cast<float4*>(o)[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2],
+                                                                              v[4 * j + 3]);
+                        } else {
+                            for (int j = 0; j < 16; j++)
+                                if (nb + j < g.N) o[j] = v[j];
                         }
                     }
                 }
-                __syncwarp();
             }
         }
         // every warp is done with sA and the accumulators before the next tile
@@ -316,10 +340,9 @@ extern "C" sbx_status sbx_mlp_gemm_bf16(sbx_ctx* ctx, int32_t nz, int32_t M, int
     if (M == 0) return SBX_OK;
     static bool attr = false;
     const int Kp = (K + 15) & ~15;
-    size_t smem = (size_t)(MT + NT) * Kp * 2 + 16 + STG_BYTES;
+    size_t smem = (size_t)(MT + NT) * Kp * 2 + 16;
     if (!attr) {
-        cudaFuncSetAttribute(k_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (MT + NT) * KMAX * 2 + 16 + STG_BYTES);
+        cudaFuncSetAttribute(k_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (MT + NT) * KMAX * 2 + 16);
         attr = true;
     }
     GemmArgs g{M, N, K, (const __nv_bfloat16*)A, lda, strideA, (const __nv_bfloat16*)B, ldb, strideB, bias,

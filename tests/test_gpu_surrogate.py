@@ -62,3 +62,40 @@ def test_training_fits_a_smooth_target():
     err = np.abs(mean - Y[3584:]) / np.abs(Y[3584:]).mean(axis=0)
     assert err.mean() < 0.05
     assert fallback_mask(mean, std, 0.10).mean() < 0.5
+
+
+@pytest.mark.parametrize("ldo_pad", [0, 3], ids=["vector-rows", "scalar-rows"])
+def test_gemm_epilogue_matches_torch(ldo_pad):
+    """sbx_mlp_gemm_bf16 on ragged sizes (M, N and K not multiples of the tiles), two problems
+    in one launch, with bias + GELU and all three outputs, against torch on the same BF16
+    operands: the FP32 pre-activations to FP32 accumulation-order tolerance, the BF16
+    activations and their transpose to one BF16 rounding. ldo_pad > 0 makes the row-major
+    outputs' rows unaligned (the element-wise store path)."""
+    from softbox_b200.runtime import Context
+    nz, M, N, K = 2, 1000, 200, 100
+    g = torch.Generator(device="cuda").manual_seed(3)
+    A = torch.randn(nz, M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = (0.1 * torch.randn(nz, N, K, device="cuda", generator=g)).to(torch.bfloat16)
+    bias = torch.randn(nz, N, device="cuda", generator=g)
+    ldo = N + ldo_pad
+    out = torch.zeros(nz, M, ldo, dtype=torch.bfloat16, device="cuda")
+    outF = torch.zeros(nz, M, ldo, dtype=torch.float32, device="cuda")
+    outT = torch.zeros(nz, N, M, dtype=torch.bfloat16, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ctx = Context(0)
+    ctx("sbx_mlp_gemm_bf16", nz, M, N, K, A, K, M * K, B, K, N * K, bias, N, 1, out, ldo, M * ldo, outT, M, N * M,
+        outF, ldo, M * ldo, err)
+    ctx.sync()
+    assert err.item() == 0
+    v = torch.matmul(A.float(), B.float().transpose(1, 2)) + bias[:, None, :]
+    a = torch.nn.functional.gelu(v)
+    got_v = outF[:, :, :N]
+    assert torch.allclose(got_v, v, rtol=1e-4, atol=1e-4), (got_v - v).abs().max()
+    ref = a.to(torch.bfloat16).float()
+    for got in (out[:, :, :N].float(), outT.transpose(1, 2).float()):
+        # one BF16 rounding of values that agree to FP32 accumulation order
+        assert torch.allclose(got, ref, rtol=1e-2, atol=1e-2), (got - ref).abs().max()
+    # padding columns of the row-major outputs stay untouched
+    if ldo_pad:
+        assert out[:, :, N:].float().abs().max().item() == 0
+        assert outF[:, :, N:].abs().max().item() == 0
