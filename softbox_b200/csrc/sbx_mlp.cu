@@ -4,13 +4,14 @@
 // bias gradients, Adam).
 //
 // GEMM: C[M x N] = A[M x K] . B[N x K]^T, A and B row-major BF16 (K contiguous, "K-major"),
-// K <= 256. One CTA (12 warps) per SM keeps its B tile (up to 256 columns) in shared memory
-// and loops over 128-row tiles of C: the A and B tiles are staged in shared memory in the
+// K <= 256. One CTA (16 warps) per SM keeps its B tile (up to 256 columns) in shared memory
+// and loops over 128-row tiles of C, staging the next tile's A while the current tile's
+// epilogue runs: the A and B tiles are staged in shared memory in the
 // canonical no-swizzle K-major layout (8 x 16-byte core matrices; core matrix (row group g,
 // k group c) at ((g * Kp/8) + c) * 128 bytes), one thread issues K/16 MMAs (M = 128, N = the
 // tile width) into TMEM and commits them to an mbarrier, and the epilogue reads the
 // accumulators back with tcgen05.ld: warp w takes TMEM lanes (rows) 32 (w mod 4) .. +31 and
-// every third 16-column chunk from chunk w / 4, adds the bias, applies GELU and writes each
+// every fourth 16-column chunk from chunk w / 4, adds the bias, applies GELU and writes each
 // row's 16 values with vector stores (the transposed output by lanes along the rows).
 // blockIdx.z selects an independent problem (an ensemble member) by strides.
 #include <cuda_bf16.h>
@@ -24,7 +25,7 @@ namespace {
 constexpr int MT = 128;              // rows of a C tile (the MMA's M)
 constexpr int NT = 256;              // max columns of a C tile (the MMA's N)
 constexpr int KMAX = 256;            // max contraction length
-constexpr int GEMM_THREADS = 384;   // 12 warps: 4 TMEM lane quarters x 3 column groups
+constexpr int GEMM_THREADS = 512;   // 16 warps: 4 TMEM lane quarters x 4 column groups
 constexpr int COL_GROUPS = GEMM_THREADS / 128;
 constexpr long long WAIT_NS = 1000000000LL;
 
@@ -142,9 +143,10 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm(GemmArgs g) {
     unsigned tmem = 0;
 
     int iter = 0;
+    if ((int)blockIdx.x < tilesM) stage(sA, A, g.lda, (int)blockIdx.x * MT, MT, g.M, g.K, Kp, vecA);
     for (int tile = blockIdx.x; tile < tilesM && ok; tile += gridDim.x, iter++) {
         const int m0 = tile * MT;
-        stage(sA, A, g.lda, m0, MT, g.M, g.K, Kp, vecA);
+        // this tile's A was staged before the previous tile's epilogue (or above)
         cp_async_wait_all();
         asm volatile("fence.proxy.async.shared::cta;");
         asm volatile("tcgen05.fence::before_thread_sync;");
@@ -186,6 +188,9 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm(GemmArgs g) {
         }
         if (!ok && threadIdx.x == 0 && g.err) atomicOr(g.err, 1);
         asm volatile("tcgen05.fence::after_thread_sync;");
+        // the MMAs have read A: stage the next tile's A while this tile's epilogue runs
+        if (ok && tile + (int)gridDim.x < tilesM)
+            stage(sA, A, g.lda, (tile + (int)gridDim.x) * MT, MT, g.M, g.K, Kp, vecA);
         if (ok) {
             const int row = m0 + quarter * 32 + lane;
             for (int c0 = cgroup * 16; c0 < Np; c0 += COL_GROUPS * 16) {
