@@ -1266,21 +1266,25 @@ SBX_DEV void integrate_derive_store(const sbx_rigid_body& b, int s, const float 
     const int n = b.n;
     Pose p, q;
     float rf[3], rt[3], gT[3], gR[3], dc[3];
+    // every input read up front, so that the loads are in flight together
+    double c64[3] = {0.0, 0.0, 0.0};
     for (int k = 0; k < 3; k++) {
         p.c[k] = b.coord[k * n + s]; p.u[k] = b.uVec[k * n + s]; p.y[k] = b.yVec[k * n + s];
         rf[k] = b.randForce[k * n + s]; rt[k] = b.randTorque[k * n + s];
         gT[k] = b.bTransGam[k * n + s]; gR[k] = b.bRotGam[k * n + s];
+        if (b.coord64) c64[k] = b.coord64[k * n + s];
     }
+    const float len = b.segLength[s];
     integrate_pose(p, F, T, rf, rt, gT, gR, dt, q, dc);
     if (b.coord64) {
         for (int k = 0; k < 3; k++) {
-            double c = b.coord64[k * n + s] + (double)dc[k];
+            double c = c64[k] + (double)dc[k];
             b.coord64[k * n + s] = c;
             q.c[k] = (float)c;
         }
     }
     float z[3], e1[3], e2[3];
-    derive_pose(q.c, q.u, q.y, z, e1, e2, b.segLength[s]);
+    derive_pose(q.c, q.u, q.y, z, e1, e2, len);
     for (int k = 0; k < 3; k++) {
         b.coord[k * n + s] = q.c[k]; b.uVec[k * n + s] = q.u[k]; b.yVec[k * n + s] = q.y[k];
         b.zVec[k * n + s] = z[k]; b.end1[k * n + s] = e1[k]; b.end2[k * n + s] = e2[k];
