@@ -46,9 +46,10 @@ WARM_STEPS = 3000      # untimed steps before the warm-up: bound heads have buil
 REF_MIN_STEPS = 200    # the reference arm times at least this many steps
 # DRAM bytes (read + write) of one launch of the fused kernel advancing one step of this
 # workload (FP64 centres, warmed state, L2 flushed before the launch), from one ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum, mean of three launches; the command is
-# in profiles/k_dense_fused_benchmark_network.md)
-FUSED_STEP_DRAM_BYTES = 11_140_000
+# (dram__bytes_read.sum + dram__bytes_write.sum, mean of three launches of
+# `python bench.py --steps 3 --warmup 3 --no-cpu --sweep-points 0` under
+# `ncu --clock-control none -k regex:k_dense_fused -s 1 -c 3`)
+FUSED_STEP_DRAM_BYTES = 12_198_000
 
 
 def workload_config(sc_host, warmup):
