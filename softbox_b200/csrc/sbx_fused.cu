@@ -495,25 +495,29 @@ __device__ void phase_place(const FusedArgs& a) {
 // segment-only cell-ordered endpoints, fused with bindNearest's selection
 // (BindingDetectionSystem.java:366-388): the same 27 cells in the same order (nine rows of
 // three consecutive x-cells), the same predicate, and the first nearest among the first
-// MAX_CAND candidates; one warp walks one head (every lane calls it with the same head):
-// lanes 0..8 read the nine stencil row ranges, then the entries are tested 32 at a
-// time, lane k taking entry k0 + k. Passing entries are appended in entry order (ballot, and
-// the popcount of the lower lanes' passes), so the list is the serial walk's list; the
-// nearest of the first MAX_CAND (strict <, the first in list order wins) is the serial
-// choice: a chunk's minimum with ties to its lowest lane replaces the running best only when
-// strictly smaller. Returns the reach count; best and arc are the same on every lane.
-__device__ int warp_reach_bind(const FusedArgs& a, int lane, float mx, float my, float mz, float mux, float muy,
-                               float muz, float rux, float ruy, float ruz, int* out, float tol, float align,
-                               int* bestSeg, float* bestArc) {
+// MAX_CAND candidates. One half-warp walks one head (the two halves of a warp walk two heads
+// side by side; every lane of a half calls it with its half's head, `valid` false for a
+// half without one): lanes 0..8 of the half read the nine stencil row ranges, then the
+// entries are tested 16 at a time, lane k of the half taking entry k0 + k. Passing entries
+// are appended in entry order (ballot, and the popcount of the half's lower lanes'
+// passes), so the list is the serial walk's list; the nearest of the first MAX_CAND (strict
+// <, the first in list order wins) is the serial choice: a chunk's minimum with ties to its
+// lowest lane replaces the running best only when strictly smaller. Both halves run the
+// same number of chunks (the longer walk's), so every shuffle has the whole warp. Returns
+// the reach count; best and arc are the same on every lane of the half.
+__device__ int half_reach_bind(const FusedArgs& a, int lane, bool valid, float mx, float my, float mz, float mux,
+                               float muy, float muz, float rux, float ruy, float ruz, int* out, float tol,
+                               float align, int* bestSeg, float* bestArc) {
     const float* gp = a.sc.grid.gridParams;
     const int* off = a.segCellOff;
+    const int hl = lane & 15, half = lane >> 4;
     const int nX = a.nX, nY = a.nY, nZ = a.nZ, nXY = nX * nY;
     const int cx = cell_coord(mx, gp[0], gp[4], nX), cy = cell_coord(my, gp[1], gp[4], nY),
               cz = cell_coord(mz, gp[2], gp[4], nZ);
     const int x0 = max(cx - 1, 0), x1 = min(cx + 1, nX - 1);
     int rs = 0, len = 0;
-    if (lane < 9) {
-        int zz = cz - 1 + lane / 3, yy = cy - 1 + lane % 3;
+    if (valid && hl < 9) {
+        int zz = cz - 1 + hl / 3, yy = cy - 1 + hl % 3;
         if (zz >= 0 && zz < nZ && yy >= 0 && yy < nY) {
             int c0 = x0 + yy * nX + zz * nXY;
             rs = off[c0];
@@ -523,22 +527,23 @@ __device__ int warp_reach_bind(const FusedArgs& a, int lane, float mx, float my,
     int inc = len;
 #pragma unroll
     for (int o = 1; o < 16; o <<= 1) {
-        int y = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += y;
+        int y = __shfl_up_sync(0xffffffffu, inc, o, 16);
+        if (hl >= o) inc += y;
     }
-    const int total = __shfl_sync(0xffffffffu, inc, 8);
-    // every lane holds the nine (start of row in the sequence, start of row in memory) pairs
+    const int total = __shfl_sync(0xffffffffu, inc, 8, 16);
+    const int totalMax = max(__shfl_sync(0xffffffffu, total, 0), __shfl_sync(0xffffffffu, total, 16));
+    // every lane holds its half's nine (start of row in the sequence, start of row in memory) pairs
     int preR[9], rsR[9];
 #pragma unroll
     for (int r = 0; r < 9; r++) {
-        preR[r] = __shfl_sync(0xffffffffu, inc - len, r);
-        rsR[r] = __shfl_sync(0xffffffffu, rs, r);
+        preR[r] = __shfl_sync(0xffffffffu, inc - len, r, 16);
+        rsR[r] = __shfl_sync(0xffffffffu, rs, r, 16);
     }
-    const unsigned lower = (1u << lane) - 1u;
+    const unsigned lower = (1u << hl) - 1u;
     int cnt = 0, best = -1;
     float bestD = 1.0e30f, arc = 0.f;
-    for (int k0 = 0; k0 < total; k0 += 32) {
-        const int k = k0 + lane;
+    for (int k0 = 0; k0 < totalMax; k0 += 16) {
+        const int k = k0 + hl;
         bool pass = false;
         float d = 0.f;
         float4 e1 = make_float4(0.f, 0.f, 0.f, 0.f), e2 = e1;
@@ -555,25 +560,27 @@ __device__ int warp_reach_bind(const FusedArgs& a, int lane, float mx, float my,
                 pass = d >= 0.f;
             }
         }
-        const unsigned mask = __ballot_sync(0xffffffffu, pass);
+        const unsigned mask = (__ballot_sync(0xffffffffu, pass) >> (16 * half)) & 0xffffu;
         const int pos = cnt + __popc(mask & lower);
         const int sg = __float_as_int(e1.w);
         const bool elig = pass && pos < MAX_CAND;
         if (elig) out[pos] = sg;
         float v = elig ? d : 3.0e38f;
-        int who = lane;
+        int who = hl;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
+        for (int o = 8; o > 0; o >>= 1) {
             float ov = __shfl_xor_sync(0xffffffffu, v, o);
             int ow = __shfl_xor_sync(0xffffffffu, who, o);
             if (ov < v || (ov == v && ow < who)) { v = ov; who = ow; }
         }
+        float myArc = 0.f;
+        if (v < bestD && hl == who) myArc = bind_arc(mx, my, mz, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z);
+        const int bw = __shfl_sync(0xffffffffu, sg, who, 16);
+        const float ba = __shfl_sync(0xffffffffu, myArc, who, 16);
         if (v < bestD) {
-            float myArc = 0.f;
-            if (lane == who) myArc = bind_arc(mx, my, mz, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z);
             bestD = v;
-            best = __shfl_sync(0xffffffffu, sg, who);
-            arc = __shfl_sync(0xffffffffu, myArc, who);
+            best = bw;
+            arc = ba;
         }
         cnt += __popc(mask);
     }
@@ -587,7 +594,8 @@ __device__ int warp_reach_bind(const FusedArgs& a, int lane, float mx, float my,
 // bindNearest's choice (BindingDetectionSystem.java:161-227, :366-388), the nucleotide cycle
 // (NucleotideCycleSystem.java:33-69) and the bound head's entry in its segment's motor row.
 // Warp w takes heads w, w + W, w + 2W, ... (W warps in the grid) in rounds of 32: lane j
-// releases and cycles the round's head j, all lanes walk each head in turn.
+// releases and cycles the round's head j; the two half-warps walk heads j and j + 1 side by
+// side.
 __device__ void phase_bind(const FusedArgs& a, int t) {
     const sbx_dense_scene& sc = a.sc;
     const sbx_motor_store& mot = sc.mot;
@@ -604,26 +612,35 @@ __device__ void phase_bind(const FusedArgs& a, int t) {
             cs = mot.capStats[myM];
             release_one(myM, bs, cd, sb, sr, cs, mot.forceDotFil[myM], mot.forceMag[myM], kp, t, sc.seed);
         }
-        for (int j = 0; j < 32; j++) {
-            const int m = base + j * nw;
-            if (m >= nM) break;
-            float mx = mot.head[m], my = mot.head[nM + m], mz = mot.head[2 * nM + m];
-            float mux = mot.uVec[m], muy = mot.uVec[nM + m], muz = mot.uVec[2 * nM + m];
-            float rux = mot.rodUVec[m], ruy = mot.rodUVec[nM + m], ruz = mot.rodUVec[2 * nM + m];
+        for (int j = 0; j < 32; j += 2) {
+            if (base + j * nw >= nM) break;
+            // half h walks head j + h (owned by lane j + h)
+            const int jh = j + (lane >> 4), m = base + jh * nw;
+            const bool valid = m < nM;
+            const int mm = valid ? m : base;
+            float mx = mot.head[mm], my = mot.head[nM + mm], mz = mot.head[2 * nM + mm];
+            float mux = mot.uVec[mm], muy = mot.uVec[nM + mm], muz = mot.uVec[2 * nM + mm];
+            float rux = mot.rodUVec[mm], ruy = mot.rodUVec[nM + mm], ruz = mot.rodUVec[2 * nM + mm];
             int best;
             float arc;
-            int rc = warp_reach_bind(a, lane, mx, my, mz, mux, muy, muz, rux, ruy, ruz,
-                                     sc.grid.reachSeg + (int64_t)m * MAX_CAND, kp[7], kp[8], &best, &arc);
-            if (lane == 0) {
+            int rc = half_reach_bind(a, lane, valid, mx, my, mz, mux, muy, muz, rux, ruy, ruz,
+                                     sc.grid.reachSeg + (int64_t)mm * MAX_CAND, kp[7], kp[8], &best, &arc);
+            if ((lane & 15) == 0 && valid) {
                 sc.grid.reachCount[m] = rc;
                 if (rc > MAX_CAND) {
                     atomicOr(a.err, ERR_REACH_OVERFLOW);
                     stat_add(a, ST_REACH_OVER, 1);
                 }
             }
-            if (lane == j && bs == FREE_BINDABLE && best >= 0) {
-                bs = best;
-                mot.bindArc[m] = arc;
+            // the owner lanes j and j + 1 take their half's choice
+            const int b0 = __shfl_sync(0xffffffffu, best, 0), b1 = __shfl_sync(0xffffffffu, best, 16);
+            const float a0 = __shfl_sync(0xffffffffu, arc, 0), a1 = __shfl_sync(0xffffffffu, arc, 16);
+            if (lane == j || lane == j + 1) {
+                const int bb = lane == j ? b0 : b1;
+                if (bs == FREE_BINDABLE && bb >= 0) {
+                    bs = bb;
+                    mot.bindArc[myM] = lane == j ? a0 : a1;
+                }
             }
         }
         if (mine) {
