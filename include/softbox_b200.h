@@ -749,6 +749,11 @@ int32_t sbx_dense_plan_kernels_per_step(sbx_dense_plan* plan);
 sbx_status sbx_dense_plan_status(sbx_dense_plan* plan, int32_t* flags);
 /* 1 when the fused persistent path is available for this scene (else mode 2 returns SBX_ESTATE) */
 int32_t sbx_dense_plan_fused_available(sbx_dense_plan* plan);
+/* Re-reads the chain topology for the fused path after the scene's filament topology changed
+ * (a turnover cadence: growth splits, deaths, births into FREE slots): rod groups, whether
+ * neighbours cross groups, joint sharing. Synchronises the plan's stream. The graph and
+ * per-system paths need no refresh. */
+sbx_status sbx_dense_plan_refresh(sbx_dense_plan* plan);
 /* cooperative grid size (CTAs) of the fused path */
 int32_t sbx_dense_plan_fused_grid(sbx_dense_plan* plan);
 /* Phase timing of the fused path: when dev_times (device int64 array of

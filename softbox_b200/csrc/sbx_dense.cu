@@ -394,6 +394,7 @@ struct sbx_dense_plan {
     int kernels_per_step = 0;
     // fused persistent path
     bool fused_ok = false;
+    bool fused_prepared = false;  // its scratch exists (the topology may still be refused)
     bool fused_dirty = true;     // scratch must be (re)initialised before the next fused run
     std::string fused_why;
     FusedArgs fa{};
@@ -463,6 +464,70 @@ bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
 // Checks that the scene has the harness's structure the fused kernel relies on and fills
 // the kernel arguments; on failure records why (the graph path remains available).
+// The fused kernel's view of the chain topology, read from the device (the plan's stream
+// is synchronised): rod groups (FUSED_MAX_ROD slots at most, a multiple of 4), whether every
+// chain neighbour lies in its own group (else the rod phase reads cross-group neighbours from
+// the step's start view), whether each joint can be computed once. FREE filament slots of
+// turnover are allowed: the body view leaves them out of the grid's segments. Called at plan
+// creation and by sbx_dense_plan_refresh after a topology change.
+bool fused_topology(sbx_dense_plan* p) {
+    const sbx_dense_scene& sc = p->scene;
+    cudaStream_t st = p->ctx->stream;
+    FusedArgs& a = p->fa;
+    auto why = [&](const char* w) { p->fused_why = w; return false; };
+    auto e1 = d2h(sc.fil.end1NbrSlot, a.nSeg, st), e2 = d2h(sc.fil.end2NbrSlot, a.nSeg, st);
+    auto d1 = d2h(sc.fil.end1NbrSide, a.nSeg, st), d2 = d2h(sc.fil.end2NbrSide, a.nSeg, st);
+    std::vector<int> lo(a.nSeg), hi(a.nSeg);
+    for (int i = 0; i < a.nSeg; i++) {
+        lo[i] = i; hi[i] = i;
+        int nb[2] = {e1[i], e2[i]};
+        for (int j : nb) {
+            if (j < -1 || j >= a.nSeg) return why("neighbour slot out of range");
+            if (j >= 0) { lo[i] = std::min(lo[i], j); hi[i] = std::max(hi[i], j); }
+        }
+    }
+    // filaments as contiguous slot ranges: a rod group is a run of whole filaments, the
+    // smallest group size whose groups fit one wave of CTAs, else the largest valid one
+    const int wave = p->fused_grid - FUSED_MIN_HELPERS;
+    a.G = 0;
+    int largest = 0;
+    for (int G = 4; G <= FUSED_MAX_ROD; G += 4) {
+        bool ok = true;
+        for (int i = 0; i < a.nSeg && ok; i++) ok = (lo[i] / G == i / G) && (hi[i] / G == i / G);
+        if (!ok) continue;
+        largest = G;
+        if (!a.G && (a.nSeg + G - 1) / G <= wave) a.G = G;
+    }
+    if (!a.G) a.G = largest;
+    a.nbrGlobal = 0;
+    if (!a.G) {
+        // neighbours across every grouping (births into free slots): groups of consecutive
+        // slots sized to one wave, cross-group neighbours read from the step's start view
+        a.nbrGlobal = 1;
+        int G = 4;
+        while (G < FUSED_MAX_ROD && (a.nSeg + G - 1) / G > wave) G += 4;
+        a.G = G;
+    }
+    // joint sharing needs every neighbour link to point back: rod i's side s (0 = end2) to
+    // slot j at nside means j's side 1 - nside points to i at nside 1 - s
+    a.jointShare = 1;
+    for (int i = 0; i < a.nSeg && a.jointShare; i++)
+        for (int side = 0; side < 2; side++) {
+            int j = side == 0 ? e2[i] : e1[i], ns = side == 0 ? d2[i] : d1[i];
+            if (j < 0) continue;
+            if (j == i || (ns != 0 && ns != 1)) { a.jointShare = 0; break; }
+            int back = ns == 0 ? e1[j] : e2[j], backSide = ns == 0 ? d1[j] : d2[j];
+            if (back != i || backSide != 1 - side) { a.jointShare = 0; break; }
+        }
+    a.nRodUnits = (a.nSeg + a.G - 1) / a.G;
+    // helper CTAs of the rod phase: those without a rod unit, at least FUSED_MIN_HELPERS
+    a.kHelp0 = std::max(0, std::min(a.nRodUnits, p->fused_grid - FUSED_MIN_HELPERS));
+    const sbx_rigid_body& fb = sc.fil.body;
+    a.useTma = (a.nSeg % 4 == 0) && (a.G % 4 == 0) && aligned16(fb.coord) && aligned16(fb.uVec) &&
+               aligned16(fb.segLength) && aligned16(fb.bTransGam) && aligned16(fb.bRotGam);
+    return true;
+}
+
 bool fused_prepare(sbx_dense_plan* p) {
     const sbx_dense_scene& sc = p->scene;
     cudaStream_t st = p->ctx->stream;
@@ -498,58 +563,11 @@ bool fused_prepare(sbx_dense_plan* p) {
     int per = fused_max_blocks_per_sm();
     if (!coop || per <= 0) return why("cooperative launch unavailable");
     p->fused_grid = sms * per;
-    // the fused kernel publishes every filament slot as live: no FREE slot may exist
-    if (sc.fil.filState) {
-        auto fs = d2h(sc.fil.filState, a.nSeg, st);
-        for (int i = 0; i < a.nSeg; i++)
-            if (fs[i] < 0) return why("FREE filament slots (turnover) need the per-system or graph path");
-    }
-    // chain topology: filaments must be contiguous slot ranges. A rod group is a run of
-    // whole filaments (a multiple of 4 segments, <= FUSED_MAX_ROD); the smallest group
-    // size whose groups fit one wave of CTAs, else the largest valid one.
-    auto e1 = d2h(sc.fil.end1NbrSlot, a.nSeg, st), e2 = d2h(sc.fil.end2NbrSlot, a.nSeg, st);
-    auto d1 = d2h(sc.fil.end1NbrSide, a.nSeg, st), d2 = d2h(sc.fil.end2NbrSide, a.nSeg, st);
-    std::vector<int> lo(a.nSeg), hi(a.nSeg);
-    for (int i = 0; i < a.nSeg; i++) {
-        lo[i] = i; hi[i] = i;
-        int nb[2] = {e1[i], e2[i]};
-        for (int j : nb) {
-            if (j < -1 || j >= a.nSeg) return why("neighbour slot out of range");
-            if (j >= 0) { lo[i] = std::min(lo[i], j); hi[i] = std::max(hi[i], j); }
-        }
-    }
-    a.G = 0;
-    int largest = 0;
-    for (int G = 4; G <= FUSED_MAX_ROD; G += 4) {
-        bool ok = true;
-        for (int i = 0; i < a.nSeg && ok; i++) ok = (lo[i] / G == i / G) && (hi[i] / G == i / G);
-        if (!ok) continue;
-        largest = G;
-        if (!a.G && (a.nSeg + G - 1) / G <= p->fused_grid - FUSED_MIN_HELPERS) a.G = G;
-    }
-    if (!a.G) a.G = largest;
-    if (!a.G) return why("chain neighbours cross every segment grouping");
-    // joint sharing needs every neighbour link to point back: rod i's side s (0 = end2) to
-    // slot j at nside means j's side 1 - nside points to i at nside 1 - s
-    a.jointShare = 1;
-    for (int i = 0; i < a.nSeg && a.jointShare; i++)
-        for (int side = 0; side < 2; side++) {
-            int j = side == 0 ? e2[i] : e1[i], ns = side == 0 ? d2[i] : d1[i];
-            if (j < 0) continue;
-            if (j == i || (ns != 0 && ns != 1)) { a.jointShare = 0; break; }
-            int back = ns == 0 ? e1[j] : e2[j], backSide = ns == 0 ? d1[j] : d2[j];
-            if (back != i || backSide != 1 - side) { a.jointShare = 0; break; }
-        }
-    a.nRodUnits = (a.nSeg + a.G - 1) / a.G;
-    // helper CTAs of the rod phase: those without a rod unit, at least FUSED_MIN_HELPERS
-    a.kHelp0 = std::max(0, std::min(a.nRodUnits, p->fused_grid - FUSED_MIN_HELPERS));
+    if (!fused_topology(p)) return false;
     a.tilesC = (a.C + SCAN_CHUNK - 1) / SCAN_CHUNK;
     a.tilesS = (a.nSeg + SCAN_CHUNK - 1) / SCAN_CHUNK;
     auto fc = d2h(sc.fil.counts, 4, st);
     a.filSeed = fc[2];
-    const sbx_rigid_body& fb = sc.fil.body;
-    a.useTma = (a.nSeg % 4 == 0) && (a.G % 4 == 0) && aligned16(fb.coord) && aligned16(fb.uVec) &&
-               aligned16(fb.segLength) && aligned16(fb.bTransGam) && aligned16(fb.bRotGam);
     // plan-owned scratch
     auto alloc = [&](size_t bytes) -> void* {
         void* q = nullptr;
@@ -576,6 +594,7 @@ bool fused_prepare(sbx_dense_plan* p) {
     a.segE1 = (float4*)alloc(16 * nS); a.segE2 = (float4*)alloc(16 * nS);
     a.joints = alloc(2 * nS * FUSED_JOINT_BYTES);
     a.terms = alloc((2 * (size_t)a.nM + 4 * (size_t)a.nD) * FUSED_TERM_BYTES);
+    a.uSnap = (float*)alloc(12 * nS);
     a.bar = (unsigned long long*)alloc(32);
     a.err = (int*)alloc(16);
     a.d_step = p->d_step;
@@ -591,6 +610,7 @@ bool fused_prepare(sbx_dense_plan* p) {
     // the error word and barrier counters are read by the plan status before any fused run
     cudaMemsetAsync(a.err, 0, 16, st);
     cudaMemsetAsync(a.bar, 0, 32, st);
+    p->fused_prepared = true;
     return true;
 }
 
@@ -793,6 +813,13 @@ extern "C" sbx_status sbx_dense_plan_status(sbx_dense_plan* p, int32_t* flags) {
 }
 
 extern "C" int32_t sbx_dense_plan_fused_available(sbx_dense_plan* p) { return p && p->fused_ok ? 1 : 0; }
+
+extern "C" sbx_status sbx_dense_plan_refresh(sbx_dense_plan* p) {
+    if (!p) return SBX_EINVAL;
+    if (p->batched || !p->fused_prepared) return SBX_OK;
+    p->fused_ok = fused_topology(p);
+    return SBX_OK;
+}
 
 extern "C" int32_t sbx_dense_plan_fused_grid(sbx_dense_plan* p) { return p ? p->fused_grid : 0; }
 

@@ -221,6 +221,7 @@ __device__ void phase_publish_bin(const FusedArgs& a, int t) {
     const int nX = a.nX, nY = a.nY, nZ = a.nZ;
     const int nLk = a.xlOn ? a.nL : 0;
     const int total = cap + nLk + nSeg;
+    const int* fb_state = sc.fil.filState;      // FREE (< 0) slots of turnover, or none
     int overCell = 0, overLink = 0;
     for (int i = gtid(); i < total; i += gthreads()) {
         if (i >= cap + nLk) {
@@ -234,7 +235,9 @@ __device__ void phase_publish_bin(const FusedArgs& a, int t) {
             float c[3] = {fb.coord[i], fb.coord[nSeg + i], fb.coord[2 * nSeg + i]};
             g.center[i] = c[0]; g.center[cap + i] = c[1]; g.center[2 * cap + i] = c[2];
             g.boundingRadius[i] = 0.5f * fb.segLength[i] + g.viewParams[0];
-            g.ownerStore[i] = STORE_FILAMENT;
+            g.ownerStore[i] = (fb_state && fb_state[i] < 0) ? STORE_NONE : STORE_FILAMENT;
+            if (a.nbrGlobal)
+                for (int k = 0; k < 3; k++) a.uSnap[k * nSeg + i] = fb.uVec[k * nSeg + i];
             g.ownerSlot[i] = i;
             if (i < a.S) {
                 int cell = cell_coord(c[0], gp[0], gp[4], nX) + cell_coord(c[1], gp[1], gp[4], nY) * nX +
@@ -473,8 +476,13 @@ __device__ void phase_place(const FusedArgs& a) {
             // segments of its cell equals its rank in the cell
             if (i < nSeg && SBX_IDX_OK(a.segCellOff[c] + rank, nSeg, CK_CSR_POS)) {
                 int q = a.segCellOff[c] + rank;
-                a.segE1[q] = make_float4(fb.end1[i], fb.end1[nSeg + i], fb.end1[2 * nSeg + i], __int_as_float(i));
-                a.segE2[q] = make_float4(fb.end2[i], fb.end2[nSeg + i], fb.end2[2 * nSeg + i], 0.f);
+                if (g.ownerStore[i] == STORE_FILAMENT) {
+                    a.segE1[q] = make_float4(fb.end1[i], fb.end1[nSeg + i], fb.end1[2 * nSeg + i], __int_as_float(i));
+                    a.segE2[q] = make_float4(fb.end2[i], fb.end2[nSeg + i], fb.end2[2 * nSeg + i], 0.f);
+                } else {
+                    a.segE1[q] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+                    a.segE2[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
             }
         } else {
             int k = i - a.cap;
@@ -557,7 +565,7 @@ __device__ int half_reach_bind(const FusedArgs& a, int lane, bool valid, float m
                 e2 = a.segE2[idx];
                 d = reach_test_dist_sq(mx, my, mz, mux, muy, muz, rux, ruy, ruz, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z,
                                        tol, align);
-                pass = d >= 0.f;
+                pass = d >= 0.f && __float_as_int(e1.w) >= 0;
             }
         }
         const unsigned mask = (__ballot_sync(0xffffffffu, pass) >> (16 * half)) & 0xffffu;
@@ -928,9 +936,15 @@ __device__ bool rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
     if (tid < cnt) {
         s2 = f.end2NbrSlot[i]; n2 = f.end2NbrSide[i];
         s1 = f.end1NbrSlot[i]; n1 = f.end1NbrSide[i];
-        // a rod group holds whole filaments: both neighbours are staged rows of the group
-        if (s2 >= 0 && !SBX_IDX_OK(s2 - g0, cnt, CK_NEIGHBOUR)) s2 = -1;
-        if (s1 >= 0 && !SBX_IDX_OK(s1 - g0, cnt, CK_NEIGHBOUR)) s1 = -1;
+        // a rod group holds whole filaments (both neighbours staged rows of the group) unless
+        // the topology has neighbours across groups
+        if (a.nbrGlobal) {
+            if (!SBX_IDX_OK_OR_NONE(s2, n, CK_NEIGHBOUR)) s2 = -1;
+            if (!SBX_IDX_OK_OR_NONE(s1, n, CK_NEIGHBOUR)) s1 = -1;
+        } else {
+            if (s2 >= 0 && !SBX_IDX_OK(s2 - g0, cnt, CK_NEIGHBOUR)) s2 = -1;
+            if (s1 >= 0 && !SBX_IDX_OK(s1 - g0, cnt, CK_NEIGHBOUR)) s1 = -1;
+        }
     }
     if (tma) {
         // bounded wait on the transaction barrier, one verdict per CTA: the phase completed
@@ -954,13 +968,25 @@ __device__ bool rod_unit(const FusedArgs& a, RodSmem& rs, int u, int t, uint64_t
     }
     __syncthreads();
     ChainParams cp = chain_params(f.chainParams);
+    // a rod of the group from the staging; a neighbour outside the group (turnover
+    // topologies) from the step's start view (phase A's centres and orientation snapshot:
+    // its own group may already have integrated it), the same values
     auto rod = [&](int j) {
         int l = j - g0;
         RodGeom r;
-        r.cx = sc_[0][l]; r.cy = sc_[1][l]; r.cz = sc_[2][l];
-        r.ux = sc_[3][l]; r.uy = sc_[4][l]; r.uz = sc_[5][l];
-        r.len = sc_[6][l];
-        r.bTGx = sc_[7][l]; r.bTGy = sc_[8][l]; r.bRGy = sc_[9][l];
+        if (l >= 0 && l < cnt) {
+            r.cx = sc_[0][l]; r.cy = sc_[1][l]; r.cz = sc_[2][l];
+            r.ux = sc_[3][l]; r.uy = sc_[4][l]; r.uz = sc_[5][l];
+            r.len = sc_[6][l];
+            r.bTGx = sc_[7][l]; r.bTGy = sc_[8][l]; r.bRGy = sc_[9][l];
+        } else {
+            const float* c = sc.grid.center;
+            const int cp_ = a.cap;
+            r.cx = c[j]; r.cy = c[cp_ + j]; r.cz = c[2 * cp_ + j];
+            r.ux = a.uSnap[j]; r.uy = a.uSnap[n + j]; r.uz = a.uSnap[2 * n + j];
+            r.len = fb.segLength[j];
+            r.bTGx = fb.bTransGam[j]; r.bTGy = fb.bTransGam[n + j]; r.bRGy = fb.bRotGam[n + j];
+        }
         return r;
     };
     // this rod's two joints (computed in the minifilament phase), loaded ahead of use

@@ -26,6 +26,8 @@ struct FusedArgs {
     int tilesC, tilesS;
     int xlOn, xlUnbind, useTma, filSeed;
     int jointShare;          // chain neighbours are symmetric: each joint computed once
+    int nbrGlobal;           // some chain neighbour lies outside its rod group (turnover topologies)
+    float* uSnap;            // with nbrGlobal: this step's start orientations (3 planes of nSeg), from phase A
     int kHelp0;              // first CTA of the rod phase's helpers (motor CSR build, resets)
     // private scratch (plan-owned)
     int *cntCell, *cntSeg, *cntAct, *cntA, *cntB, *cntM;   // cntSeg: segments per cell

@@ -136,8 +136,10 @@ class TurnoverNetwork(DenseNetwork):
     """A dense network with actin turnover (scenes.dense_turnover): at every biochem cadence
     the turnover block (growth, depolymerisation, death, severing, splits), the release of
     links and heads on dead slots, and constant-actin births run before that step's
-    mechanics, all on the library's stream with no host synchronisation. The mechanics run
-    on the graph or per-system path: the fused kernel assumes a static chain topology."""
+    mechanics, all on the library's stream. The mechanics run on any path; on the fused
+    path (mode "fused", or "auto" below the fused size limit) the plan re-reads the chain
+    topology after each cadence (sbx_dense_plan_refresh: one stream synchronisation per
+    cadence), since splits and births into FREE slots change the rod groups."""
 
     def __init__(self, host_scene, ctx=None, fp64_coords=False, device="cuda"):
         from .turnover import Turnover
@@ -150,14 +152,18 @@ class TurnoverNetwork(DenseNetwork):
                                  boundSeg=d["mot"]["boundSeg"])
 
     def run(self, t0, nsteps, mode="graph"):
-        if mode not in ("graph", "unfused"):
-            raise ValueError("turnover runs on the graph or per-system path")
+        if mode not in self.MODES:
+            raise ValueError(f"unknown mode {mode!r}")
         t, end = int(t0), int(t0) + int(nsteps)
         ci = self.tcfg.check_int
         while t < end:
             if self.tcfg.fires_at(t):
                 self.turnover.cadence(t)
                 self.turnover.births(t)
+                if mode in ("fused", "auto"):
+                    st = LIB.sbx_dense_plan_refresh(self.plan)
+                    if st != 0:
+                        raise SbxError(st, "sbx_dense_plan_refresh: " + self.ctx.last_error())
             nxt = min(end, (t // ci + 1) * ci)
             super().run(t, nxt - t, mode)
             t = nxt

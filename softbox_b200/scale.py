@@ -62,7 +62,7 @@ def measure(n_rods, steps=20, modes=("fused", "graph")):
     return out
 
 
-def measure_turnover(n_rods, steps=1000):
+def measure_turnover(n_rods, steps=1000, mode="graph"):
     import torch
     from .engine import TurnoverNetwork
     from .runtime import LIB
@@ -76,18 +76,22 @@ def measure_turnover(n_rods, steps=1000):
     ci = net.tcfg.check_int
     steps = max(ci, steps // ci * ci)
     stream = torch.cuda.ExternalStream(LIB.sbx_ctx_stream(net.ctx.h))
-    net.run(0, 3 * ci)
+    if mode == "fused" and not net.fused_available:
+        net.close()
+        return {"rods": n_rods, "mode": "fused+turnover", "unavailable": "fused path not available for this scene"}
+    net.run(0, 3 * ci, mode=mode)
     torch.cuda.synchronize()
     s, e = torch.cuda.Event(True), torch.cuda.Event(True)
     with torch.cuda.stream(stream):
         s.record(stream)
-        net.run(3 * ci, steps)
+        net.run(3 * ci, steps, mode=mode)
         e.record(stream)
     torch.cuda.synchronize()
+    net.status()
     ms = s.elapsed_time(e) / steps
     fs = net.pull("fil", "filState")
     conc, _, taken, returned = pool_fields(net.pull("turnover", "pool"))
-    out = {"rods": n_rods, "mode": "graph+turnover", "ms_per_step": ms, "rod_steps_per_s": n_rods / (ms / 1e3),
+    out = {"rods": n_rods, "mode": mode + "+turnover", "ms_per_step": ms, "rod_steps_per_s": n_rods / (ms / 1e3),
            "algorithmic_bytes_per_step": nbytes, "achieved_gbs": nbytes / (ms / 1e3) / 1e9, "hbm_peak_gbs": hbm,
            "frac": nbytes / (ms / 1e3) / 1e9 / hbm, "peak_source": how, "steps": steps, "cadence_steps": ci,
            "active_rods_end": int((fs >= 0).sum()), "pool_taken": taken, "pool_returned": returned,
@@ -107,7 +111,8 @@ def main():
     a = ap.parse_args()
     if a.turnover:
         for n in a.rods:
-            print(json.dumps(measure_turnover(n, a.steps)), flush=True)
+            for mode in a.modes:
+                print(json.dumps(measure_turnover(n, a.steps, mode)), flush=True)
         return
     for n in a.rods:
         for line in measure(n, a.steps, tuple(a.modes)):
