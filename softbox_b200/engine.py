@@ -151,7 +151,7 @@ class TurnoverNetwork(DenseNetwork):
                                  links=(xl["linkFilA"], xl["linkFilB"], xl["linkState"]),
                                  boundSeg=d["mot"]["boundSeg"])
 
-    def run(self, t0, nsteps, mode="graph"):
+    def run(self, t0, nsteps, mode="auto"):
         if mode not in self.MODES:
             raise ValueError(f"unknown mode {mode!r}")
         t, end = int(t0), int(t0) + int(nsteps)

@@ -49,8 +49,8 @@ def generate(points, steps, sample_every, batch=256, turnover=False):
 
 
 def per_run_seconds(points, steps, sample=8, turnover=False):
-    """Mean GPU seconds of one point's run alone (single-network plan: the auto path, or
-    the graph path with turnover)."""
+    """Mean GPU seconds of one point's run alone (single-network plan on the auto path,
+    with or without turnover)."""
     import torch
     from .engine import DenseNetwork, TurnoverNetwork
     from . import scenes

@@ -26,13 +26,14 @@ import ctypes as C, pickle, sys
 sys.path.insert(0, sys.argv[1])
 import torch
 from softbox_b200 import device as D
-from softbox_b200.engine import DenseNetwork
+from softbox_b200.engine import DenseNetwork, TurnoverNetwork
 from softbox_b200.runtime import LIB
 assert LIB.sbx_check_build() == 1
 job = pickle.load(open(sys.argv[2], "rb"))
 out = {}
 for mode in job["modes"]:
-    net = DenseNetwork(job["scene"], fp64_coords=job.get("fp64", False))
+    cls = TurnoverNetwork if job.get("turnover") else DenseNetwork
+    net = cls(job["scene"], fp64_coords=job.get("fp64", False))
     if mode == "unfused":
         for t in range(job["t0"], job["t0"] + job["n"]):
             net.step_unfused(t)
@@ -47,9 +48,10 @@ pickle.dump(out, open(sys.argv[3], "wb"))
 '''
 
 
-def run_checked(tmp_path, scene, t0, n, modes, fp64=False):
+def run_checked(tmp_path, scene, t0, n, modes, fp64=False, turnover=False):
     job, res = tmp_path / "job.pkl", tmp_path / "res.pkl"
-    pickle.dump({"scene": scene, "t0": t0, "n": n, "modes": modes, "fp64": fp64}, open(job, "wb"))
+    pickle.dump({"scene": scene, "t0": t0, "n": n, "modes": modes, "fp64": fp64, "turnover": turnover},
+                open(job, "wb"))
     env = dict(os.environ, SBX_LIB="check")
     subprocess.run([sys.executable, "-c", CHILD, ROOT, str(job), str(res)], check=True, env=env, cwd=ROOT,
                    timeout=600)
@@ -89,3 +91,18 @@ def test_check_build_benchmark_network_fused(tmp_path):
     torch.cuda.synchronize()
     names = compare_scenes({k: v for k, v in D.to_host(net.dev).items() if k != "cfg"}, out["fused"]["scene"])
     assert len(names) > 80
+
+
+@pytest.mark.skipif(not os.path.exists(CHECK_LIB), reason="check build missing")
+def test_check_build_turnover_network_fused(orc_dm, tmp_path):
+    """A turnover network (deaths, splits, births into FREE slots: chain neighbours across the
+    fused kernel's rod groups) for 500 fused steps in the check build: no bad index, and the
+    oracle's bits."""
+    from helpers import oracle_turnover_network_run
+    sc = scenes.dense_turnover(scenes.dense_small(0.05), growth_rate=400.0, sever_rate=5.0)
+    out = run_checked(tmp_path, copy.deepcopy(sc), 0, 500, ["fused"], turnover=True)
+    assert out["fused"]["bad"] == (0, 0, 0), out["fused"]["bad"]
+    ref = copy.deepcopy(sc)
+    oracle_turnover_network_run(orc_dm, ref, 0, 500)
+    names = compare_scenes({k: v for k, v in ref.items() if k != "tcfg"}, out["fused"]["scene"], skip=("coord64",))
+    assert "fil.body.coord" in names
