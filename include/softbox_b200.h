@@ -85,6 +85,15 @@ sbx_status sbx_malloc(sbx_ctx* ctx, size_t bytes, void** dptr);
 sbx_status sbx_free(sbx_ctx* ctx, void* dptr);
 sbx_status sbx_upload(sbx_ctx* ctx, void* dst_dev, const void* src_host, size_t bytes);
 sbx_status sbx_download(sbx_ctx* ctx, void* dst_host, const void* src_dev, size_t bytes);
+/* The same copy without the wait: the bytes are on the host once the stream has passed it
+ * (sbx_ctx_sync, or a marker recorded after it and waited for). */
+sbx_status sbx_download_async(sbx_ctx* ctx, void* dst_host, const void* src_dev, size_t bytes);
+/* Stream markers (slots 0..7): sbx_ctx_mark records the current end of the context's stream
+ * in a slot; sbx_ctx_wait_mark waits until the stream has passed it and reports the kernels'
+ * range errors like sbx_ctx_sync. A host can so keep the next step queued while it reads
+ * the previous step's results. */
+sbx_status sbx_ctx_mark(sbx_ctx* ctx, int32_t slot);
+sbx_status sbx_ctx_wait_mark(sbx_ctx* ctx, int32_t slot);
 sbx_status sbx_memset(sbx_ctx* ctx, void* dst_dev, int value, size_t bytes);
 
 /* ---------------------------------------------------------------- drag (host-init systems, run on device)

@@ -19,6 +19,9 @@ struct sbx_ctx {
     // >= its row count); sbx_ctx_sync reports and clears it. err_dev is its device address.
     int* err_host = nullptr;
     int* err_dev = nullptr;
+    // stream markers of sbx_ctx_mark / sbx_ctx_wait_mark (created on first use)
+    static constexpr int kMarks = 8;
+    cudaEvent_t marks[kMarks] = {};
 };
 
 sbx_status fail(sbx_ctx* ctx, sbx_status code, const std::string& msg);

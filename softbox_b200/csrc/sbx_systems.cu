@@ -58,6 +58,8 @@ extern "C" sbx_status sbx_ctx_destroy(sbx_ctx* ctx) {
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->host_flag) cudaFreeHost(ctx->host_flag);
     if (ctx->err_host) cudaFreeHost(ctx->err_host);
+    for (cudaEvent_t e : ctx->marks)
+        if (e) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SBX_OK;
@@ -180,6 +182,31 @@ extern "C" sbx_status sbx_download(sbx_ctx* ctx, void* dst, const void* src, siz
     if (cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess)
         return fail(ctx, SBX_ECUDA, "download failed");
     return sbx_ctx_sync(ctx);
+}
+extern "C" sbx_status sbx_download_async(sbx_ctx* ctx, void* dst, const void* src, size_t bytes) {
+    if (!ctx || (!dst && bytes) || (!src && bytes)) return SBX_EINVAL;
+    if (cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess)
+        return fail(ctx, SBX_ECUDA, "download failed");
+    return SBX_OK;
+}
+extern "C" sbx_status sbx_ctx_mark(sbx_ctx* ctx, int32_t slot) {
+    if (!ctx || slot < 0 || slot >= sbx_ctx::kMarks) return SBX_EINVAL;
+    if (!ctx->marks[slot] && cudaEventCreateWithFlags(&ctx->marks[slot], cudaEventDisableTiming) != cudaSuccess)
+        return fail(ctx, SBX_ECUDA, "sbx_ctx_mark: event");
+    if (cudaEventRecord(ctx->marks[slot], ctx->stream) != cudaSuccess) return fail(ctx, SBX_ECUDA, "sbx_ctx_mark: record");
+    return SBX_OK;
+}
+extern "C" sbx_status sbx_ctx_wait_mark(sbx_ctx* ctx, int32_t slot) {
+    if (!ctx || slot < 0 || slot >= sbx_ctx::kMarks || !ctx->marks[slot]) return SBX_EINVAL;
+    cudaError_t e = cudaEventSynchronize(ctx->marks[slot]);
+    if (e != cudaSuccess) return fail(ctx, SBX_ECUDA, std::string("wait: ") + cudaGetErrorString(e));
+    if (ctx->err_host && *(volatile int*)ctx->err_host) {
+        const int w = *(volatile int*)ctx->err_host;
+        *(volatile int*)ctx->err_host = 0;
+        if (w == 2) return fail(ctx, SBX_ETIMEOUT, "a staged reach walk's bulk copies did not complete in time");
+        return fail(ctx, SBX_EINVAL, "a CSR key was >= its row count (the item was skipped)");
+    }
+    return SBX_OK;
 }
 extern "C" sbx_status sbx_memset(sbx_ctx* ctx, void* dst, int value, size_t bytes) {
     if (!ctx || (!dst && bytes)) return SBX_EINVAL;

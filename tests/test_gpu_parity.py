@@ -630,3 +630,23 @@ def test_fused_barrier_timeout_reports_and_recovers(warm_scene):
     ref.run(300, 5, mode="graph")
     torch.cuda.synchronize()
     compare_scenes(host(ref.dev), host(fresh.dev))
+
+
+def test_async_download_and_stream_markers():
+    """sbx_download_async + sbx_ctx_mark / sbx_ctx_wait_mark: the bytes are on the host once
+    the marker recorded after the copy has been passed; invalid slots are refused."""
+    import ctypes as C
+    from softbox_b200.runtime import Context, LIB
+    ctx = Context(0)
+    src = torch.arange(4096, dtype=torch.int32, device="cuda")
+    dst = [torch.zeros(4096, dtype=torch.int32).pin_memory() for _ in range(2)]
+    for k in range(6):
+        b = k & 1
+        ctx("sbx_memset", C.c_void_p(src.data_ptr()), k, 4 * 4096)
+        ctx("sbx_download_async", C.c_void_p(dst[b].data_ptr()), C.c_void_p(src.data_ptr()), 4 * 4096)
+        ctx("sbx_ctx_mark", b)
+        ctx("sbx_ctx_wait_mark", b)
+        want = int.from_bytes(bytes([k]) * 4, "little")
+        assert (dst[b].numpy() == want).all()
+    assert LIB.sbx_ctx_mark(ctx.h, 8) != 0
+    assert LIB.sbx_ctx_wait_mark(ctx.h, 5) != 0          # never recorded
