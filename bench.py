@@ -374,7 +374,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=600)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--sweep-points", type=int, default=32, help="packed sweep points timed beside the step (0: off)")
+    ap.add_argument("--sweep-points", type=int, default=256,
+                    help="packed sweep points timed beside the step: 256, the batched ensemble's size (0: off)")
     ap.add_argument("--sweep-steps", type=int, default=200)
     args = ap.parse_args()
     if args.impl == "reference":
