@@ -249,8 +249,9 @@ def run_ours(args):
     value = ws * nrods * args.steps / (total_ms / 1e3)
 
     # e2e through the C ABI: per step, H2D of the step's counts blocks (the reference's
-    # EVERY_EXECUTION upload: motor, backbone and filament counts, 3 x 16 B) from pinned
-    # memory, one fused step, D2H of the step's binding state (boundSeg) into pinned memory.
+    # EVERY_EXECUTION upload: motor, backbone and filament counts, 3 x 16 B, contiguous on
+    # the device, so one copy) from pinned memory, one fused step, D2H of the step's binding
+    # state (boundSeg) into pinned memory.
     # Pipelined as a streaming host would run it: step k is queued (uploads, launch, result
     # copy, marker) before the host waits for step k - 1's result; two pinned buffers each.
     d = net.dev
@@ -270,8 +271,7 @@ def run_ours(args):
         c = counts_host[b].numpy()
         c[:] = [sc_host["mot"]["nMotors"], t, cfg.seed, nrods, sc_host["mini"]["nBackbones"], t, cfg.seed_bb,
                 sc_host["mini"]["nBackbones"], nrods, t, cfg.seed_fil, 1]
-        for j, dst in enumerate((d["mot"]["counts"], d["mini"]["bbCounts"], d["fil"]["counts"])):
-            ctx("sbx_upload", C.c_void_p(dst.data_ptr()), C.c_void_p(counts_host[b].data_ptr() + 16 * j), 16)
+        ctx("sbx_upload", C.c_void_p(net.counts_block.data_ptr()), C.c_void_p(counts_host[b].data_ptr()), h2d)
         st = LIB.sbx_dense_plan_run(net.plan, t, 1, 2)
         assert st == 0, ctx.last_error()
         ctx("sbx_download_async", C.c_void_p(bound_host[b].data_ptr()), C.c_void_p(d["mot"]["boundSeg"].data_ptr()),

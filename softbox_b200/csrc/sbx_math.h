@@ -16,12 +16,16 @@
 //     arithmetic), which reaches double accuracy with 6 to 11 terms where the
 //     truncated Taylor series of the same functions needs 10 to 14.
 //   * log(m) = 2*atanh(f/(2+f)), f = m - 1, m in [sqrt(1/2), sqrt(2)).
+//   * the Horner steps and the argument reductions are explicit fused multiply-adds
+//     (fmad below: one rounding of a*b + c). CUDA's __fma_rn and C99's fma are both
+//     correctly rounded, so they give the same bits; an FMA is one instruction where a
+//     multiply and an add are two dependent ones.
 //
 // Accuracy (checked in tests/test_math.py against libm and, on the GPU, against
 // CUDA's own functions): <= 2 ulp in double for |x| <= 2^20 (sin/cos), all positive
 // normal x (log), |x| <= 700 (exp). Compiled with contraction disabled
-// (-ffp-contract=off on the host, -fmad=false on the device) every operation is a
-// single IEEE-754 round-to-nearest step, so host and device agree bit for bit.
+// (-ffp-contract=off on the host, -fmad=false on the device) every other operation is
+// a single IEEE-754 round-to-nearest step, so host and device agree bit for bit.
 #pragma once
 #include <stdint.h>
 #include <string.h>
@@ -42,6 +46,15 @@
 #endif
 
 namespace sbxm {
+
+// fused multiply-add, one rounding (CUDA's fma and C99 fma are both correctly rounded)
+SBX_HD double fmad(double a, double b, double c) {
+#ifdef __CUDA_ARCH__
+    return __fma_rn(a, b, c);
+#else
+    return __builtin_fma(a, b, c);
+#endif
+}
 
 // ---- split constants (gen_math_constants.py) ----
 #define SBXM_PIO2_HI   0x1.921fb54400000p+0
@@ -102,33 +115,33 @@ SBX_HD int nearest_int(double x) {
 SBX_HD double sin_poly(double r) {
     double r2 = r * r;
     double p = SBXM_SIN5;
-    p = p * r2 + SBXM_SIN4;
-    p = p * r2 + SBXM_SIN3;
-    p = p * r2 + SBXM_SIN2;
-    p = p * r2 + SBXM_SIN1;
-    p = p * r2 + SBXM_SIN0;                       // ~ -1/3!
-    return r + r * (r2 * p);
+    p = fmad(p, r2, SBXM_SIN4);
+    p = fmad(p, r2, SBXM_SIN3);
+    p = fmad(p, r2, SBXM_SIN2);
+    p = fmad(p, r2, SBXM_SIN1);
+    p = fmad(p, r2, SBXM_SIN0);                       // ~ -1/3!
+    return fmad(r * r2, p, r);
 }
 
 SBX_HD double cos_poly(double r) {
     double r2 = r * r;
     double p = SBXM_COS5;
-    p = p * r2 + SBXM_COS4;
-    p = p * r2 + SBXM_COS3;
-    p = p * r2 + SBXM_COS2;
-    p = p * r2 + SBXM_COS1;
-    p = p * r2 + SBXM_COS0;                       // ~ 1/4!
-    p = p * r2 - 0.5;
-    return 1.0 + r2 * p;
+    p = fmad(p, r2, SBXM_COS4);
+    p = fmad(p, r2, SBXM_COS3);
+    p = fmad(p, r2, SBXM_COS2);
+    p = fmad(p, r2, SBXM_COS1);
+    p = fmad(p, r2, SBXM_COS0);                       // ~ 1/4!
+    p = fmad(p, r2, -0.5);
+    return fmad(r2, p, 1.0);
 }
 
 // x = k*(pi/2) + r, |r| <= pi/4 (+ tiny); returns r, writes the quadrant k & 3
 SBX_HD double reduce_pio2(double x, int* quadrant) {
     int k = nearest_int(x * SBXM_2_OVER_PI);
     double kd = (double)k;
-    double r = x - kd * SBXM_PIO2_HI;
-    r = r - kd * SBXM_PIO2_MID;
-    r = r - kd * SBXM_PIO2_LO;
+    double r = fmad(-kd, SBXM_PIO2_HI, x);
+    r = fmad(-kd, SBXM_PIO2_MID, r);
+    r = fmad(-kd, SBXM_PIO2_LO, r);
     *quadrant = k & 3;
     return r;
 }
@@ -194,15 +207,15 @@ SBX_HD_CALL double log(double x) {
     double s = f / (2.0 + f);
     double s2 = s * s;
     double q = SBXM_LOG6;
-    q = q * s2 + SBXM_LOG5;
-    q = q * s2 + SBXM_LOG4;
-    q = q * s2 + SBXM_LOG3;
-    q = q * s2 + SBXM_LOG2;
-    q = q * s2 + SBXM_LOG1;
-    q = q * s2 + SBXM_LOG0;                       // ~ 1/3
+    q = fmad(q, s2, SBXM_LOG5);
+    q = fmad(q, s2, SBXM_LOG4);
+    q = fmad(q, s2, SBXM_LOG3);
+    q = fmad(q, s2, SBXM_LOG2);
+    q = fmad(q, s2, SBXM_LOG1);
+    q = fmad(q, s2, SBXM_LOG0);                       // ~ 1/3
     double two_s = 2.0 * s;
     double ed = (double)e;
-    double lo = ed * SBXM_LN2_LO + two_s * (s2 * q);
+    double lo = fmad(ed, SBXM_LN2_LO, two_s * (s2 * q));
     return ed * SBXM_LN2_HI + (two_s + lo);
 }
 
@@ -213,20 +226,20 @@ SBX_HD_CALL double exp(double x) {
     if (x < -745.1332191019412) return 0.0;
     int k = nearest_int(x * SBXM_INV_LN2);
     double kd = (double)k;
-    double r = x - kd * SBXM_LN2_HI;
-    r = r - kd * SBXM_LN2_LO;
+    double r = fmad(-kd, SBXM_LN2_HI, x);
+    r = fmad(-kd, SBXM_LN2_LO, r);
     double p = SBXM_EXP10;
-    p = p * r + SBXM_EXP9;
-    p = p * r + SBXM_EXP8;
-    p = p * r + SBXM_EXP7;
-    p = p * r + SBXM_EXP6;
-    p = p * r + SBXM_EXP5;
-    p = p * r + SBXM_EXP4;
-    p = p * r + SBXM_EXP3;
-    p = p * r + SBXM_EXP2;
-    p = p * r + SBXM_EXP1;
-    p = p * r + SBXM_EXP0;                        // ~ 1/2
-    double er = 1.0 + (r + r * (r * p));
+    p = fmad(p, r, SBXM_EXP9);
+    p = fmad(p, r, SBXM_EXP8);
+    p = fmad(p, r, SBXM_EXP7);
+    p = fmad(p, r, SBXM_EXP6);
+    p = fmad(p, r, SBXM_EXP5);
+    p = fmad(p, r, SBXM_EXP4);
+    p = fmad(p, r, SBXM_EXP3);
+    p = fmad(p, r, SBXM_EXP2);
+    p = fmad(p, r, SBXM_EXP1);
+    p = fmad(p, r, SBXM_EXP0);                        // ~ 1/2
+    double er = 1.0 + fmad(r, r * p, r);
     // scale by 2^k in two halves so that k down to -1074 stays representable
     int k1 = k / 2, k2 = k - k1;
     double s1 = bitsd((uint64_t)(k1 + 1023) << 52);

@@ -30,6 +30,21 @@ def to_device(obj, device="cuda"):
     return obj
 
 
+def counts_block(dev):
+    """Moves the three per-execution counts blocks of a device dense scene (mot.counts,
+    mini.bbCounts, fil.counts: 4 int32 each, the reference's EVERY_EXECUTION uploads) into
+    one contiguous 12-int32 device tensor, points the scene at its three slices and returns
+    it, so that a host uploads one step's counts with one 48-byte copy."""
+    import torch
+    slots = ((dev["mot"], "counts"), (dev["mini"], "bbCounts"), (dev["fil"], "counts"))
+    assert all(s[k].numel() == 4 and s[k].dtype == torch.int32 for s, k in slots)
+    block = torch.empty(12, dtype=torch.int32, device=slots[0][0][slots[0][1]].device)
+    for j, (s, k) in enumerate(slots):
+        block[4 * j:4 * j + 4].copy_(s[k])
+        s[k] = block[4 * j:4 * j + 4]
+    return block
+
+
 def to_host(obj):
     if isinstance(obj, dict):
         return {k: to_host(v) for k, v in obj.items()}

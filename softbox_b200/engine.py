@@ -20,6 +20,9 @@ class DenseNetwork:
         self.ctx = ctx or default_context()
         self.host = host_scene
         self.dev = D.to_device({k: v for k, v in host_scene.items() if k not in ("cfg", "tcfg")}, device)
+        # motor, backbone and filament counts side by side: [nMotors, t, seed, nSeg,
+        # nBackbones, t, seedBb, nBackbones, nSeg, t, seedFil, 1]
+        self.counts_block = D.counts_block(self.dev)
         if fp64_coords:
             for path in (("fil", "body"), ("mot", "body"), ("mini", "backbone")):
                 D.add_coord64(self.dev[path[0]][path[1]])
