@@ -14,9 +14,9 @@
 //      Brownian forces of the motor sub-bodies and backbones
 //   E  stable placement by list rank -> gridCellContents, segIdxA, segIdxB and the
 //      segment endpoints in cell order (float4) for the reach walk
-//   B0 binding of every head, one warp per head: release, the reach walk fused with the
-//      nearest-segment choice (lanes test 32 candidates at a time, appended in order),
-//      nucleotide cycle; bound heads join their segment's motor list
+//   B0 binding of every head, 8 lanes per head: release, the reach walk fused with the
+//      nearest-segment choice (the group's lanes test 8 candidates at a time, appended in
+//      order), nucleotide cycle; bound heads join their segment's motor list
 //   F  one CTA per minifilament: every position-only myosin term, then the ordered sums,
 //      the cross-bridge bonds and integrate + derive of its 96 sub-bodies and backbone,
 //      all force sums in shared memory; other CTAs compute crosslinker forces + torsion,
@@ -503,54 +503,68 @@ __device__ void phase_place(const FusedArgs& a) {
 // segment-only cell-ordered endpoints, fused with bindNearest's selection
 // (BindingDetectionSystem.java:366-388): the same 27 cells in the same order (nine rows of
 // three consecutive x-cells), the same predicate, and the first nearest among the first
-// MAX_CAND candidates. One half-warp walks one head (the two halves of a warp walk two heads
-// side by side; every lane of a half calls it with its half's head, `valid` false for a
-// half without one): lanes 0..8 of the half read the nine stencil row ranges, then the
-// entries are tested 16 at a time, lane k of the half taking entry k0 + k. Passing entries
-// are appended in entry order (ballot, and the popcount of the half's lower lanes'
-// passes), so the list is the serial walk's list; the nearest of the first MAX_CAND (strict
-// <, the first in list order wins) is the serial choice: a chunk's minimum with ties to its
-// lowest lane replaces the running best only when strictly smaller. Both halves run the
-// same number of chunks (the longer walk's), so every shuffle has the whole warp. Returns
-// the reach count; best and arc are the same on every lane of the half.
-__device__ int half_reach_bind(const FusedArgs& a, int lane, bool valid, float mx, float my, float mz, float mux,
-                               float muy, float muz, float rux, float ruy, float ruz, int* out, float tol,
-                               float align, int* bestSeg, float* bestArc) {
+// MAX_CAND candidates. A group of W lanes (8 or 16) walks one head (the 32 / W groups of a
+// warp walk as many heads side by side; every lane of a group calls it with its group's
+// head, `valid` false for a group without one): lane r of the group reads stencil row r's
+// range (with 8 lanes, lane 0 also row 8), then the entries are tested W at a time, lane k
+// of the group taking entry k0 + k. Passing entries are appended in entry order (ballot,
+// and the popcount of the group's lower lanes' passes), so the list is the serial walk's
+// list; the nearest of the first MAX_CAND (strict <, the first in list order wins) is the
+// serial choice: a chunk's minimum with ties to its lowest lane replaces the running best
+// only when strictly smaller. Every group runs the same number of chunks (the longest
+// walk's), so every shuffle has the whole warp. Returns the reach count; best and arc are
+// the same on every lane of the group.
+template <int W>
+__device__ int group_reach_bind(const FusedArgs& a, int lane, bool valid, float mx, float my, float mz, float mux,
+                                float muy, float muz, float rux, float ruy, float ruz, int* out, float tol,
+                                float align, int* bestSeg, float* bestArc) {
+    static_assert(W == 8 || W == 16, "a group of 8 or 16 lanes walks one head");
     const float* gp = a.sc.grid.gridParams;
     const int* off = a.segCellOff;
-    const int hl = lane & 15, half = lane >> 4;
+    const int hl = lane & (W - 1), grp = lane / W;
     const int nX = a.nX, nY = a.nY, nZ = a.nZ, nXY = nX * nY;
     const int cx = cell_coord(mx, gp[0], gp[4], nX), cy = cell_coord(my, gp[1], gp[4], nY),
               cz = cell_coord(mz, gp[2], gp[4], nZ);
     const int x0 = max(cx - 1, 0), x1 = min(cx + 1, nX - 1);
-    int rs = 0, len = 0;
-    if (valid && hl < 9) {
-        int zz = cz - 1 + hl / 3, yy = cy - 1 + hl % 3;
+    // lane hl reads stencil row hl; with 8 lanes, lane 0 also reads row 8
+    int rs = 0, len = 0, rs8 = 0, len8 = 0;
+    auto row = [&](int r, int& s, int& l) {
+        int zz = cz - 1 + r / 3, yy = cy - 1 + r % 3;
         if (zz >= 0 && zz < nZ && yy >= 0 && yy < nY) {
             int c0 = x0 + yy * nX + zz * nXY;
-            rs = off[c0];
-            len = off[c0 + (x1 - x0) + 1] - rs;
+            s = off[c0];
+            l = off[c0 + (x1 - x0) + 1] - s;
         }
-    }
+    };
+    if (valid && hl < 9) row(hl, rs, len);
+    if (W == 8 && valid && hl == 0) row(8, rs8, len8);
     int inc = len;
 #pragma unroll
-    for (int o = 1; o < 16; o <<= 1) {
-        int y = __shfl_up_sync(0xffffffffu, inc, o, 16);
+    for (int o = 1; o < W; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, inc, o, W);
         if (hl >= o) inc += y;
     }
-    const int total = __shfl_sync(0xffffffffu, inc, 8, 16);
-    const int totalMax = max(__shfl_sync(0xffffffffu, total, 0), __shfl_sync(0xffffffffu, total, 16));
-    // every lane holds its half's nine (start of row in the sequence, start of row in memory) pairs
+    const int lanesTotal = __shfl_sync(0xffffffffu, inc, W - 1, W);     // rows 0 .. min(8, W - 1)
+    const int total = lanesTotal + (W == 8 ? __shfl_sync(0xffffffffu, len8, 0, W) : 0);
+    int totalMax = total;
+#pragma unroll
+    for (int o = W; o < 32; o <<= 1) totalMax = max(totalMax, __shfl_xor_sync(0xffffffffu, totalMax, o));
+    // every lane holds its group's nine (start of row in the sequence, start of row in memory) pairs
     int preR[9], rsR[9];
 #pragma unroll
     for (int r = 0; r < 9; r++) {
-        preR[r] = __shfl_sync(0xffffffffu, inc - len, r, 16);
-        rsR[r] = __shfl_sync(0xffffffffu, rs, r, 16);
+        if (r < W) {
+            preR[r] = __shfl_sync(0xffffffffu, inc - len, r, W);
+            rsR[r] = __shfl_sync(0xffffffffu, rs, r, W);
+        } else {
+            preR[r] = lanesTotal;
+            rsR[r] = __shfl_sync(0xffffffffu, rs8, 0, W);
+        }
     }
     const unsigned lower = (1u << hl) - 1u;
     int cnt = 0, best = -1;
     float bestD = 1.0e30f, arc = 0.f;
-    for (int k0 = 0; k0 < totalMax; k0 += 16) {
+    for (int k0 = 0; k0 < totalMax; k0 += W) {
         const int k = k0 + hl;
         bool pass = false;
         float d = 0.f;
@@ -568,7 +582,7 @@ __device__ int half_reach_bind(const FusedArgs& a, int lane, bool valid, float m
                 pass = d >= 0.f && __float_as_int(e1.w) >= 0;
             }
         }
-        const unsigned mask = (__ballot_sync(0xffffffffu, pass) >> (16 * half)) & 0xffffu;
+        const unsigned mask = (__ballot_sync(0xffffffffu, pass) >> (W * grp)) & ((1u << W) - 1u);
         const int pos = cnt + __popc(mask & lower);
         const int sg = __float_as_int(e1.w);
         const bool elig = pass && pos < MAX_CAND;
@@ -576,15 +590,15 @@ __device__ int half_reach_bind(const FusedArgs& a, int lane, bool valid, float m
         float v = elig ? d : 3.0e38f;
         int who = hl;
 #pragma unroll
-        for (int o = 8; o > 0; o >>= 1) {
+        for (int o = W / 2; o > 0; o >>= 1) {
             float ov = __shfl_xor_sync(0xffffffffu, v, o);
             int ow = __shfl_xor_sync(0xffffffffu, who, o);
             if (ov < v || (ov == v && ow < who)) { v = ov; who = ow; }
         }
         float myArc = 0.f;
         if (v < bestD && hl == who) myArc = bind_arc(mx, my, mz, e1.x, e1.y, e1.z, e2.x, e2.y, e2.z);
-        const int bw = __shfl_sync(0xffffffffu, sg, who, 16);
-        const float ba = __shfl_sync(0xffffffffu, myArc, who, 16);
+        const int bw = __shfl_sync(0xffffffffu, sg, who, W);
+        const float ba = __shfl_sync(0xffffffffu, myArc, who, W);
         if (v < bestD) {
             bestD = v;
             best = bw;
@@ -597,13 +611,15 @@ __device__ int half_reach_bind(const FusedArgs& a, int lane, bool valid, float m
     return cnt;
 }
 
-// BindingDetectionSystem / NucleotideCycleSystem for every head, one warp per head: the
+// BindingDetectionSystem / NucleotideCycleSystem for every head: the
 // catch-slip release (NucleotideCycleSystem.java:77-134), the reach walk fused with
 // bindNearest's choice (BindingDetectionSystem.java:161-227, :366-388), the nucleotide cycle
 // (NucleotideCycleSystem.java:33-69) and the bound head's entry in its segment's motor row.
-// Warp w takes heads w, w + W, w + 2W, ... (W warps in the grid) in rounds of 32: lane j
-// releases and cycles the round's head j; the two half-warps walk heads j and j + 1 side by
-// side.
+// Warp w takes heads w, w + N, w + 2N, ... (N warps in the grid) in rounds of 32: lane j
+// releases and cycles the round's head j; the four 8-lane groups walk heads j .. j + 3 side
+// by side. With 2,368 warps and 6,400 heads every warp walks its heads in one pass (16-lane
+// groups needed two passes in 70 % of the warps: 1 us more per step).
+constexpr int BIND_W = 8;     // lanes per walked head
 __device__ void phase_bind(const FusedArgs& a, int t) {
     const sbx_dense_scene& sc = a.sc;
     const sbx_motor_store& mot = sc.mot;
@@ -620,10 +636,10 @@ __device__ void phase_bind(const FusedArgs& a, int t) {
             cs = mot.capStats[myM];
             release_one(myM, bs, cd, sb, sr, cs, mot.forceDotFil[myM], mot.forceMag[myM], kp, t, sc.seed);
         }
-        for (int j = 0; j < 32; j += 2) {
+        for (int j = 0; j < 32; j += 32 / BIND_W) {
             if (base + j * nw >= nM) break;
-            // half h walks head j + h (owned by lane j + h)
-            const int jh = j + (lane >> 4), m = base + jh * nw;
+            // group q walks head j + q (owned by lane j + q)
+            const int jh = j + lane / BIND_W, m = base + jh * nw;
             const bool valid = m < nM;
             const int mm = valid ? m : base;
             float mx = mot.head[mm], my = mot.head[nM + mm], mz = mot.head[2 * nM + mm];
@@ -631,24 +647,23 @@ __device__ void phase_bind(const FusedArgs& a, int t) {
             float rux = mot.rodUVec[mm], ruy = mot.rodUVec[nM + mm], ruz = mot.rodUVec[2 * nM + mm];
             int best;
             float arc;
-            int rc = half_reach_bind(a, lane, valid, mx, my, mz, mux, muy, muz, rux, ruy, ruz,
+            int rc = group_reach_bind<BIND_W>(a, lane, valid, mx, my, mz, mux, muy, muz, rux, ruy, ruz,
                                      sc.grid.reachSeg + (int64_t)mm * MAX_CAND, kp[7], kp[8], &best, &arc);
-            if ((lane & 15) == 0 && valid) {
+            if ((lane & (BIND_W - 1)) == 0 && valid) {
                 sc.grid.reachCount[m] = rc;
                 if (rc > MAX_CAND) {
                     atomicOr(a.err, ERR_REACH_OVERFLOW);
                     stat_add(a, ST_REACH_OVER, 1);
                 }
             }
-            // the owner lanes j and j + 1 take their half's choice
-            const int b0 = __shfl_sync(0xffffffffu, best, 0), b1 = __shfl_sync(0xffffffffu, best, 16);
-            const float a0 = __shfl_sync(0xffffffffu, arc, 0), a1 = __shfl_sync(0xffffffffu, arc, 16);
-            if (lane == j || lane == j + 1) {
-                const int bb = lane == j ? b0 : b1;
-                if (bs == FREE_BINDABLE && bb >= 0) {
-                    bs = bb;
-                    mot.bindArc[myM] = lane == j ? a0 : a1;
-                }
+            // the owner lanes j .. j + 32 / BIND_W - 1 take their group's choice
+            const bool owner = lane >= j && lane < j + 32 / BIND_W;
+            const int src = owner ? (lane - j) * BIND_W : 0;
+            const int bb = __shfl_sync(0xffffffffu, best, src);
+            const float ab = __shfl_sync(0xffffffffu, arc, src);
+            if (owner && bs == FREE_BINDABLE && bb >= 0) {
+                bs = bb;
+                mot.bindArc[myM] = ab;
             }
         }
         if (mine) {
@@ -1277,7 +1292,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_dense_fused(const __grid_c
         phase_place(a);
         if (!counter_sync(a.bar, gTarget, nGrid, a.err)) return;
         stamp(s);
-        // B0: binding of every head (one warp per head)
+        // B0: binding of every head (8 lanes per head)
         phase_bind(a, t);
         if (!counter_sync(a.bar, gTarget, nGrid, a.err)) return;
         stamp(s);

@@ -18,7 +18,7 @@ from .runtime import LIB
 
 PHASES = ["A publish, bin, histograms + lists, crosslinker unbind",   # K(prev) -> A
           "B tile sums", "C scans + motor Brownian", "E stable placement",
-          "B0 binding (one warp per head)",
+          "B0 binding (8 lanes per head)",
           "F minifilaments + crosslinker forces + chain joints + filament Brownian",
           "K rods (+ motor CSR helpers, resets)"]
 
