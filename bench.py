@@ -49,7 +49,7 @@ REF_MIN_STEPS = 200    # the reference arm times at least this many steps
 # (dram__bytes_read.sum + dram__bytes_write.sum, mean of three launches of
 # `python bench.py --steps 3 --warmup 3 --no-cpu --sweep-points 0` under
 # `ncu --clock-control none -k regex:k_dense_fused -s 1 -c 3`)
-FUSED_STEP_DRAM_BYTES = 12_236_000
+FUSED_STEP_DRAM_BYTES = 12_302_000
 
 
 def workload_config(sc_host, warmup):
