@@ -252,8 +252,10 @@ def run_ours(args):
     # EVERY_EXECUTION upload: motor, backbone and filament counts, 3 x 16 B, contiguous on
     # the device, so one copy) from pinned memory, one fused step, D2H of the step's binding
     # state (boundSeg) into pinned memory.
-    # Pipelined as a streaming host would run it: step k is queued (uploads, launch, result
+    # Pipelined as a streaming host would run it: step k is queued (upload, launch, result
     # copy, marker) before the host waits for step k - 1's result; two pinned buffers each.
+    # The result copy runs on the context's copy stream, so it overlaps the next step's
+    # upload; the next step waits for it before it rewrites boundSeg.
     d = net.dev
     counts_host = [torch.zeros(12, dtype=torch.int32).pin_memory() for _ in range(2)]
     bound_host = [torch.empty(sc_host["mot"]["nMotors"], dtype=torch.int32).pin_memory() for _ in range(2)]
@@ -272,11 +274,13 @@ def run_ours(args):
         c[:] = [sc_host["mot"]["nMotors"], t, cfg.seed, nrods, sc_host["mini"]["nBackbones"], t, cfg.seed_bb,
                 sc_host["mini"]["nBackbones"], nrods, t, cfg.seed_fil, 1]
         ctx("sbx_upload", C.c_void_p(net.counts_block.data_ptr()), C.c_void_p(counts_host[b].data_ptr()), h2d)
+        if k > 0:
+            ctx("sbx_ctx_stream_wait_mark", 1 - b)       # the step rewrites boundSeg: after k - 1's copy
         st = LIB.sbx_dense_plan_run(net.plan, t, 1, 2)
         assert st == 0, ctx.last_error()
-        ctx("sbx_download_async", C.c_void_p(bound_host[b].data_ptr()), C.c_void_p(d["mot"]["boundSeg"].data_ptr()),
-            d2h)
-        ctx("sbx_ctx_mark", b)
+        ctx("sbx_download_async_side", C.c_void_p(bound_host[b].data_ptr()),
+            C.c_void_p(d["mot"]["boundSeg"].data_ptr()), d2h)
+        ctx("sbx_ctx_mark_side", b)
         if k > 0:
             ctx("sbx_ctx_wait_mark", 1 - b)              # step k - 1's result is on the host
             bound_sum += int(bound_host[1 - b].numpy()[0])
@@ -325,7 +329,7 @@ def run_ours(args):
                              "kernel": "k_dense_fused", "algorithmic_bytes_per_launch": bytes_step},
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e, "unit": "rod-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                        "host_loop": "C ABI from Python; each step's uploads, launch and result copy queued "
+                        "host_loop": "C ABI from Python; each step's upload, launch and result copy (on the copy stream) queued "
                                      "before the host waits for the previous step's result (L2 not flushed)"},
                 "gpu_launches": args.steps,
                 "clocks": clocks,

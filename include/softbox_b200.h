@@ -60,7 +60,7 @@ sbx_status sbx_ctx_destroy(sbx_ctx* ctx);
 const char* sbx_ctx_last_error(sbx_ctx* ctx);
 sbx_status sbx_ctx_set_stream(sbx_ctx* ctx, void* stream);
 void* sbx_ctx_stream(sbx_ctx* ctx);
-/* Waits for the context's stream. Also reports (SBX_EINVAL, then cleared) an input that a
+/* Waits for the context's stream (and its copy stream, if it has one). Also reports (SBX_EINVAL, then cleared) an input that a
  * kernel since the last sync found outside its documented range and skipped: a CSR key at
  * or past its row count (sbx_csr_build*, sbx_grid_build); and (SBX_ETIMEOUT, then cleared) a
  * staged reach walk whose bulk copies did not complete in time. */
@@ -94,6 +94,16 @@ sbx_status sbx_download_async(sbx_ctx* ctx, void* dst_host, const void* src_dev,
  * the previous step's results. */
 sbx_status sbx_ctx_mark(sbx_ctx* ctx, int32_t slot);
 sbx_status sbx_ctx_wait_mark(sbx_ctx* ctx, int32_t slot);
+/* A result copy off the context's stream: sbx_download_async_side queues the copy on the
+ * context's copy stream (created on first use), after everything queued on its stream so
+ * far, and returns; the stream moves on at once, so the copy overlaps the next uploads.
+ * sbx_ctx_mark_side records the copy stream's current end in a marker slot (wait for it on
+ * the host with sbx_ctx_wait_mark); sbx_ctx_stream_wait_mark makes work queued later on the
+ * context's stream start after a marker, e.g. a step that overwrites the copied array.
+ * sbx_ctx_mark_side before any side copy: SBX_EINVAL; so is a wait on an unrecorded slot. */
+sbx_status sbx_download_async_side(sbx_ctx* ctx, void* dst_host, const void* src_dev, size_t bytes);
+sbx_status sbx_ctx_mark_side(sbx_ctx* ctx, int32_t slot);
+sbx_status sbx_ctx_stream_wait_mark(sbx_ctx* ctx, int32_t slot);
 sbx_status sbx_memset(sbx_ctx* ctx, void* dst_dev, int value, size_t bytes);
 
 /* ---------------------------------------------------------------- drag (host-init systems, run on device)

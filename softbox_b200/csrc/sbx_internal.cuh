@@ -22,6 +22,10 @@ struct sbx_ctx {
     // stream markers of sbx_ctx_mark / sbx_ctx_wait_mark (created on first use)
     static constexpr int kMarks = 8;
     cudaEvent_t marks[kMarks] = {};
+    // the copy stream of sbx_download_async_side and the event that orders its copies after
+    // the work queued on `stream` (both created on first use)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copy_after = nullptr;
 };
 
 sbx_status fail(sbx_ctx* ctx, sbx_status code, const std::string& msg);

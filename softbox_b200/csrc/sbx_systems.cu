@@ -58,6 +58,11 @@ extern "C" sbx_status sbx_ctx_destroy(sbx_ctx* ctx) {
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->host_flag) cudaFreeHost(ctx->host_flag);
     if (ctx->err_host) cudaFreeHost(ctx->err_host);
+    if (ctx->copy_stream) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        cudaStreamDestroy(ctx->copy_stream);
+    }
+    if (ctx->copy_after) cudaEventDestroy(ctx->copy_after);
     for (cudaEvent_t e : ctx->marks)
         if (e) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
@@ -83,6 +88,7 @@ extern "C" void* sbx_ctx_stream(sbx_ctx* ctx) { return ctx ? (void*)ctx->stream 
 extern "C" sbx_status sbx_ctx_sync(sbx_ctx* ctx) {
     if (!ctx) return SBX_EINVAL;
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess && ctx->copy_stream) e = cudaStreamSynchronize(ctx->copy_stream);
     if (e != cudaSuccess) return fail(ctx, SBX_ECUDA, std::string("sync: ") + cudaGetErrorString(e));
     if (ctx->err_host && *(volatile int*)ctx->err_host) {
         const int w = *(volatile int*)ctx->err_host;
@@ -194,6 +200,35 @@ extern "C" sbx_status sbx_ctx_mark(sbx_ctx* ctx, int32_t slot) {
     if (!ctx->marks[slot] && cudaEventCreateWithFlags(&ctx->marks[slot], cudaEventDisableTiming) != cudaSuccess)
         return fail(ctx, SBX_ECUDA, "sbx_ctx_mark: event");
     if (cudaEventRecord(ctx->marks[slot], ctx->stream) != cudaSuccess) return fail(ctx, SBX_ECUDA, "sbx_ctx_mark: record");
+    return SBX_OK;
+}
+// the copy stream's copies start after everything queued on the context's stream so far;
+// the context's stream itself moves on at once
+extern "C" sbx_status sbx_download_async_side(sbx_ctx* ctx, void* dst, const void* src, size_t bytes) {
+    if (!ctx || (!dst && bytes) || (!src && bytes)) return SBX_EINVAL;
+    if (!ctx->copy_stream && cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(ctx, SBX_ECUDA, "sbx_download_async_side: stream");
+    if (!ctx->copy_after && cudaEventCreateWithFlags(&ctx->copy_after, cudaEventDisableTiming) != cudaSuccess)
+        return fail(ctx, SBX_ECUDA, "sbx_download_async_side: event");
+    if (cudaEventRecord(ctx->copy_after, ctx->stream) != cudaSuccess ||
+        cudaStreamWaitEvent(ctx->copy_stream, ctx->copy_after, 0) != cudaSuccess)
+        return fail(ctx, SBX_ECUDA, "sbx_download_async_side: order");
+    if (cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->copy_stream) != cudaSuccess)
+        return fail(ctx, SBX_ECUDA, "sbx_download_async_side: copy");
+    return SBX_OK;
+}
+extern "C" sbx_status sbx_ctx_mark_side(sbx_ctx* ctx, int32_t slot) {
+    if (!ctx || slot < 0 || slot >= sbx_ctx::kMarks || !ctx->copy_stream) return SBX_EINVAL;
+    if (!ctx->marks[slot] && cudaEventCreateWithFlags(&ctx->marks[slot], cudaEventDisableTiming) != cudaSuccess)
+        return fail(ctx, SBX_ECUDA, "sbx_ctx_mark_side: event");
+    if (cudaEventRecord(ctx->marks[slot], ctx->copy_stream) != cudaSuccess)
+        return fail(ctx, SBX_ECUDA, "sbx_ctx_mark_side: record");
+    return SBX_OK;
+}
+extern "C" sbx_status sbx_ctx_stream_wait_mark(sbx_ctx* ctx, int32_t slot) {
+    if (!ctx || slot < 0 || slot >= sbx_ctx::kMarks || !ctx->marks[slot]) return SBX_EINVAL;
+    if (cudaStreamWaitEvent(ctx->stream, ctx->marks[slot], 0) != cudaSuccess)
+        return fail(ctx, SBX_ECUDA, "sbx_ctx_stream_wait_mark");
     return SBX_OK;
 }
 extern "C" sbx_status sbx_ctx_wait_mark(sbx_ctx* ctx, int32_t slot) {

@@ -650,3 +650,33 @@ def test_async_download_and_stream_markers():
         assert (dst[b].numpy() == want).all()
     assert LIB.sbx_ctx_mark(ctx.h, 8) != 0
     assert LIB.sbx_ctx_wait_mark(ctx.h, 5) != 0          # never recorded
+
+
+def test_side_copy_and_stream_wait_markers():
+    """sbx_download_async_side + sbx_ctx_mark_side / sbx_ctx_stream_wait_mark /
+    sbx_ctx_wait_mark: each step's copy runs on the copy stream after the step; the next step
+    overwrites the source only after that copy (stream wait on its marker), so every copy
+    holds its own step's bytes; sbx_ctx_sync also waits for the copy stream."""
+    import ctypes as C
+    from softbox_b200.runtime import Context, LIB
+    ctx = Context(0)
+    assert LIB.sbx_ctx_mark_side(ctx.h, 0) != 0           # no copy stream yet
+    assert LIB.sbx_ctx_stream_wait_mark(ctx.h, 3) != 0     # never recorded
+    n = 16 << 20                                           # 64 MB: the copy outlasts the memset
+    src = torch.zeros(n, dtype=torch.int32, device="cuda")
+    dst = [torch.zeros(n, dtype=torch.int32).pin_memory() for _ in range(2)]
+    word = lambda k: int.from_bytes(bytes([k]) * 4, "little")
+    for k in range(6):
+        b = k & 1
+        if k > 0:
+            ctx("sbx_ctx_stream_wait_mark", 1 - b)         # after step k - 1's copy
+        ctx("sbx_memset", C.c_void_p(src.data_ptr()), k + 1, 4 * n)
+        ctx("sbx_download_async_side", C.c_void_p(dst[b].data_ptr()), C.c_void_p(src.data_ptr()), 4 * n)
+        ctx("sbx_ctx_mark_side", b)
+        if k > 0:
+            ctx("sbx_ctx_wait_mark", 1 - b)
+            v = dst[1 - b].numpy()
+            assert v[0] == word(k) and v[-1] == word(k) and (v == word(k)).all()
+    ctx("sbx_ctx_sync")
+    assert (dst[1].numpy() == word(6)).all()
+    assert LIB.sbx_ctx_mark_side(ctx.h, 8) != 0
