@@ -2,7 +2,7 @@
 
     net = DenseNetwork(scenes.dense_contractile(scenes.C1))
     net.run(t0=0, nsteps=100)          # CUDA-graph replay of the fused step
-    pose = net.pull("fil", "coord")    # UNDER_DEMAND host copy
+    pose = net.pull("fil", "coord", sub="body")    # UNDER_DEMAND host copy
 
     rods = FreeRods(scenes.free_rods_box())
     rods.run(0, 10000, noise="wang")   # one persistent launch, rods in registers
