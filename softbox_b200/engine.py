@@ -1,7 +1,7 @@
 """Device-resident networks: the public Python API over the fused step plans.
 
     net = DenseNetwork(scenes.dense_contractile(scenes.C1))
-    net.run(t0=0, nsteps=100)          # CUDA-graph replay of the fused step
+    net.run(t0=0, nsteps=100)          # "auto": one fused launch up to 40,960 rods, CUDA graphs above
     pose = net.pull("fil", "coord", sub="body")    # UNDER_DEMAND host copy
 
     rods = FreeRods(scenes.free_rods_box())
